@@ -1,0 +1,413 @@
+#!/usr/bin/env python3
+"""Benchmark of the fenix combustion-volume step on B200.
+
+One step = one full simulation step (injection, brick topology, advection,
+combustion, buoyancy, vorticity confinement, divergence, the 3-level pressure
+solve, projection) of the `plume_256` workload: 256^3 voxels, four floor plumes,
+a seeded synthetic developed-plume start state with ~18 % of bricks active.
+
+Metric: active-voxel-steps/s = sum over timed steps of the voxels in active
+bricks (the step's brick flags) / device time. Multi-GPU: one independent
+simulation per rank (replicas, weak scaling), time = max over ranks.
+
+`--impl reference` runs the reference's step on the host CPU instead: the f32
+CPU restatement of the WGSL step, with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "voxel-steps/s (256³ sparse fire) mixed vs FP32 plain at stated error; HBM %"
+UNIT = "active-voxel-steps/s"
+
+# Algorithmic bytes per voxel of each kernel (compulsory reads + writes of the
+# pass at f32 storage, velocity 12 B). "dense" kernels touch every voxel of
+# their level, "active" ones the voxels of active bricks.
+KERNEL_BYTES = {
+    "plain_inject_scalar": ("dense", 24.0),
+    "plain_inject_velocity": ("dense", 24.0),
+    "plain_inject_igniter": ("dense", 20.0),
+    "plain_advect_velocity": ("dense", 24.0),
+    "plain_advect_scalars": ("scalar_adv", None),
+    "plain_combustion": ("active", 32.0),
+    "plain_buoyancy": ("active", 36.0),
+    "plain_vorticity": ("dense", 28.0),
+    "plain_confinement": ("dense", 56.0),
+    "plain_divergence": ("dense", 16.0),
+    "plain_jacobi_fine": ("dense", 12.0),
+    "plain_jacobi_mid": ("mid", 12.0),
+    "plain_jacobi_coarse": ("coarse", 12.0),
+    "plain_restrict": ("restrict", None),
+    "plain_prolong": ("prolong", None),
+    "plain_project": ("dense", 28.0),
+    "plain_velocity_magnitude": ("dense", 16.0),
+    "plain_active_bricks": ("bricks", 780.0),
+}
+
+
+def kernel_bytes(name: str, n: int, active: float, nb: int, launches_per_step: float):
+    """Algorithmic bytes of one launch of `name` (None when not modelled)."""
+    from fenix_b200 import fused_bytes
+
+    spec = KERNEL_BYTES.get(name) or fused_bytes.KERNEL_BYTES.get(name)
+    if spec is None:
+        return None
+    kind, per = spec
+    n_mid, n_coarse = n / 8.0, n / 64.0
+    if kind == "dense":
+        return per * n
+    if kind == "active":
+        return per * active
+    if kind == "mid":
+        return per * n_mid
+    if kind == "coarse":
+        return per * n_coarse
+    if kind == "scalar_adv":
+        return 44.0 * active + 16.0 * (n - active)
+    if kind == "restrict":  # two launches per step: fine->mid and mid->coarse, averaged
+        return (36.0 * n_mid + 36.0 * n_coarse) / 2.0
+    if kind == "prolong":
+        return (8.0 * n_mid + 4.0 * n_coarse + 8.0 * n + 4.0 * n_mid) / 2.0
+    if kind == "bricks":
+        return per * nb
+    if kind == "fused":
+        return per(n, active, nb)
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    """The reference's step on the host CPU (the f32 restatement, all threads)."""
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    from fenix_b200 import workloads
+    from oracle import build as orc_build
+    from oracle.oracle import OracleSimulation, num_threads
+
+    orc_build.build()
+    wl = workloads.plume_256(size=args.size)
+    orc = OracleSimulation(wl.options, precision=32)
+    orc.updateSources(wl.sources)
+    workloads.load_state(orc, wl.state)
+    counts = workloads.brick_voxel_counts(wl.options["resolution"])
+    for k in range(args.warmup):
+        orc.step(k * wl.dt, wl.dt)
+    active = 0
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        orc.step((args.warmup + k) * wl.dt, wl.dt)
+        active += int(counts[orc.readField("brick_flags") != 0].sum())
+    el = time.perf_counter() - t0
+    value = active / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"plume_{args.size} (four floor plumes, {args.size}^3, 4/4/4/4/20 sweeps, dt 1/60)",
+                   "global_batch": 1, "seq_len": 0, "parallelism": "cpu"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": num_threads(), "kind": "port",
+                         "sample": f"{args.steps} full steps of plume_{args.size} after {args.warmup} warm-up steps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def cpu_baseline_and_parity(args, wl, counts, kernels):
+    """Times the oracle on a bounded sample and checks the CUDA step against it."""
+    from fenix_b200 import createCombustionVolumeSimulation, workloads
+    from oracle import build as orc_build
+    from oracle.oracle import OracleSimulation, num_threads
+
+    orc_build.build()
+    orc = OracleSimulation(wl.options, precision=32)
+    sim = createCombustionVolumeSimulation(wl.options, device=0, kernels=kernels)
+    for s in (orc, sim):
+        s.updateSources(wl.sources)
+        workloads.load_state(s, wl.state)
+    active = 0
+    el = 0.0
+    parity = True
+    for k in range(args.cpu_steps):
+        t0 = time.perf_counter()
+        orc.step(k * wl.dt, wl.dt)
+        el += time.perf_counter() - t0
+        sim.step(k * wl.dt, wl.dt)
+        flags = orc.readField("brick_flags")
+        active += int(counts[flags != 0].sum())
+        for name in ("density", "temperature", "fuel", "reaction", "velocity_x", "velocity_y", "velocity_z", "brick_flags", "pressure"):
+            a, b = sim.readField(name), orc.readField(name)
+            if not np.array_equal(a.view(np.uint32), b.view(np.uint32)):
+                parity = False
+    sim.dispose()
+    orc.dispose()
+    return {
+        "value": active / el, "unit": UNIT, "cores": num_threads(), "kind": "port",
+        "sample": f"{args.cpu_steps} full steps of the same workload from the same start state (f32 restatement, OpenMP)",
+    }, {"steps": args.cpu_steps, "bit_exact_vs_oracle": parity}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="fenix", choices=["fenix", "reference"])
+    ap.add_argument("--kernels", default="fused", choices=["fused", "plain"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        pg = dist
+
+    from fenix_b200 import build as fx_build
+    from fenix_b200 import createCombustionVolumeSimulation, workloads
+
+    if rank == 0:
+        fx_build.build()
+    if pg:
+        pg.barrier()
+
+    wl = workloads.plume_256(seed=1235 + rank, size=args.size)
+    res = wl.options["resolution"]
+    n = res[0] * res[1] * res[2]
+    counts = workloads.brick_voxel_counts(res)
+    nb = counts.size
+    sim = createCombustionVolumeSimulation(wl.options, device=local, kernels=args.kernels)
+    sim.updateSources(wl.sources)
+    workloads.load_state(sim, wl.state)
+    sim.setInstrumentation(count_active=True)
+    stream = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", local))
+    t = 0.0
+    for _ in range(args.warmup):
+        sim.step(t, wl.dt)
+        t += wl.dt
+    sim.synchronize()
+    sim.readActiveCounters()
+
+    # ---- timed region: K steps, device time on the simulation's stream ----
+    clocks = ClockSampler(local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        sim.step(t, wl.dt)
+        t += wl.dt
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    act = sim.readActiveCounters()
+    kernels_last = sim.stats()["kernelsPerStep"]
+    ms_max = ms
+    voxel_steps = act["voxelSteps"]
+    if pg:
+        tt = torch.tensor([ms], device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        ms_max = float(tt.item())
+        vv = torch.tensor([float(voxel_steps)], device="cuda", dtype=torch.float64)
+        pg.all_reduce(vv, op=pg.ReduceOp.SUM)
+        voxel_steps = int(vv.item())
+    value = voxel_steps / (ms_max / 1e3)
+    active_mean = act["voxelSteps"] / args.steps
+
+    # ---- per-kernel CUDA-event times over K more steps (roofline) ----
+    sim.setInstrumentation(kernel_times=True, count_active=True)
+    sim.readKernelTimes()
+    sim.readActiveCounters()
+    for _ in range(args.steps):
+        sim.step(t, wl.dt)
+        t += wl.dt
+    ktimes = sim.readKernelTimes()
+    act2 = sim.readActiveCounters()
+    active2 = act2["voxelSteps"] / args.steps
+    sim.setInstrumentation(count_active=True)
+    peak, peak_kind = measured_peak_hbm()
+    top = max(ktimes.items(), key=lambda kv: kv[1]["total_ms"]) if ktimes else None
+    total_kernel_ms = sum(v["total_ms"] for v in ktimes.values()) or 1.0
+    roofline = None
+    kernel_table = {}
+    for name, v in ktimes.items():
+        per_launch_ms = v["total_ms"] / max(v["launches"], 1)
+        b = kernel_bytes(name, n, active2, nb, v["launches"] / args.steps)
+        kernel_table[name] = {
+            "launches": v["launches"], "share": round(v["total_ms"] / total_kernel_ms, 4), "us_per_launch": round(per_launch_ms * 1e3, 2),
+            "GBps": round(b / (per_launch_ms / 1e3) / 1e9, 1) if b else None,
+        }
+    if top:
+        name, v = top
+        per_launch_ms = v["total_ms"] / max(v["launches"], 1)
+        b = kernel_bytes(name, n, active2, nb, v["launches"] / args.steps)
+        achieved = b / (per_launch_ms / 1e3) / 1e9 if b else None
+        roofline = {
+            "kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": None,
+            "bytes_per_launch": b, "us_per_launch": per_launch_ms * 1e3, "share_of_step": v["total_ms"] / total_kernel_ms,
+        }
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        from fenix_b200.emitters import packEmitterSources
+
+        packed = packEmitterSources(wl.sources)
+        params = sim.getRuntimeParams()
+        sim.synchronize()
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            sim.setRuntimeParams(params)                     # host -> step uniform
+            sim.updatePackedSources(packed, len(wl.sources))  # host -> device sources
+            sim.step(t, wl.dt)
+            t += wl.dt
+            sim.readActiveCounters()                          # device -> host result of the step (waits)
+        e2e_s = time.perf_counter() - t0
+        if pg:
+            tt = torch.tensor([e2e_s], device="cuda")
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        e2e = {"value": (active_mean * args.steps * world) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(packed.nbytes + 80),
+               "d2h_bytes_per_step": 16, "ms_per_step": e2e_s * 1e3 / args.steps}
+
+    sim.dispose()
+
+    cpu = None
+    parity = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu, parity = cpu_baseline_and_parity(args, wl, counts, args.kernels)
+
+    if pg:
+        pg.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {
+                "workload": f"plume_{args.size}: {args.size}^3 grid, 4 floor plumes (scalar+velocity+igniter each), seeded "
+                            f"developed-plume start, 4/4/4/4/20 sweeps, dt 1/60, f32, parity semantics",
+                "kernels": args.kernels, "active_fraction": active_mean / n, "global_batch": world, "seq_len": 0,
+                "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (about 2 GB of fields per step)",
+            },
+            "roofline": roofline, "kernels": kernel_table, "cpu_baseline": cpu, "parity_full_size": parity, "e2e": e2e,
+            "gpu_launches": int(kernels_last * args.steps), "clocks": clock_info,
+        }
+        print(json.dumps(line))
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

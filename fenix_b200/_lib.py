@@ -1,0 +1,229 @@
+"""ctypes binding of libfenixcuda.so (declarations in include/fenix_cuda.h).
+
+Loading fails loudly when the shared library has not been built: there is no
+CPU fallback for the simulation step.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, Structure, c_char_p, c_double, c_float, c_int32, c_int64, c_size_t, c_uint32, c_uint64, c_void_p
+
+PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PACKAGE_DIR, "libfenixcuda.so")
+
+FX_OK = 0
+FX_ERR_INVALID_ARGUMENT = -1
+FX_ERR_CUDA = -2
+FX_ERR_OUT_OF_MEMORY = -3
+FX_ERR_STATE = -4
+FX_ERR_TIMEOUT = -5
+FX_ERR_UNSUPPORTED = -6
+
+FX_ADVECT_SEMI_LAGRANGIAN = 0
+FX_ADVECT_MACCORMACK = 1
+
+FX_KERNELS_FUSED = 0
+FX_KERNELS_PLAIN = 1
+
+FX_OPT_DEBUG_FIELDS = 1 << 0
+FX_OPT_NO_GRAPHS = 1 << 1
+
+FX_PARAM_WIND = 1 << 0
+FX_PARAM_WIND_STRENGTH = 1 << 1
+FX_PARAM_GRAVITY = 1 << 2
+FX_PARAM_GRAVITY_STRENGTH = 1 << 3
+FX_PARAM_BUOYANCY = 1 << 4
+FX_PARAM_VORTICITY_STRENGTH = 1 << 5
+FX_PARAM_VORTICITY_CONSTANT_MASK = 1 << 6
+FX_PARAM_VORTICITY_VELOCITY_MASK = 1 << 7
+FX_PARAM_VORTICITY_HEAT_MASK = 1 << 8
+FX_PARAM_VORTICITY_DENSITY_MASK = 1 << 9
+FX_PARAM_WORLD_SIZE = 1 << 10
+FX_PARAM_ALL = 0x7FF
+
+FX_QUALITY_ALL = 0x7F
+
+FIELD_NAMES = [
+    "density", "temperature", "fuel", "reaction",
+    "prev_density", "prev_temperature", "prev_fuel", "prev_reaction",
+    "velocity_x", "velocity_y", "velocity_z",
+    "velocity_scratch_x", "velocity_scratch_y", "velocity_scratch_z",
+    "vorticity_x", "vorticity_y", "vorticity_z",
+    "vorticity_magnitude", "confinement_magnitude", "velocity_magnitude",
+    "brick_flags", "prev_brick_flags",
+    "fine_divergence", "fine_pressure_a", "fine_pressure_b",
+    "mid_divergence", "mid_pressure_a", "mid_pressure_b",
+    "coarse_divergence", "coarse_pressure_a", "coarse_pressure_b",
+    "pressure",
+]
+FIELD_IDS = {name: i for i, name in enumerate(FIELD_NAMES)}
+UINT_FIELDS = {"brick_flags", "prev_brick_flags"}
+
+
+class FxQuality(Structure):
+    _fields_ = [
+        ("pressure_interval", c_double),
+        ("vorticity_interval", c_double),
+        ("fine_pre_iterations", c_double),
+        ("fine_post_iterations", c_double),
+        ("mid_pre_iterations", c_double),
+        ("mid_post_iterations", c_double),
+        ("coarse_iterations", c_double),
+    ]
+
+
+class FxRuntimeParams(Structure):
+    _fields_ = [
+        ("wind", c_double * 3),
+        ("wind_strength", c_double),
+        ("gravity", c_double * 3),
+        ("gravity_strength", c_double),
+        ("buoyancy", c_double),
+        ("vorticity_strength", c_double),
+        ("vorticity_constant_mask", c_double),
+        ("vorticity_velocity_mask", c_double),
+        ("vorticity_heat_mask", c_double),
+        ("vorticity_density_mask", c_double),
+        ("world_size", c_double),
+    ]
+
+
+class FxSimOptions(Structure):
+    _fields_ = [
+        ("struct_size", c_uint32),
+        ("width", c_uint32),
+        ("height", c_uint32),
+        ("depth", c_uint32),
+        ("scalar_advection_mode", c_int32),
+        ("runtime_mask", c_uint32),
+        ("runtime", FxRuntimeParams),
+        ("quality_mask", c_uint32),
+        ("quality", FxQuality),
+        ("device", c_int32),
+        ("kernels", c_int32),
+        ("flags", c_uint32),
+        ("stream", c_void_p),
+    ]
+
+
+class FxRenderBuffers(Structure):
+    _fields_ = [
+        ("density", c_uint64),
+        ("temperature", c_uint64),
+        ("fuel", c_uint64),
+        ("reaction", c_uint64),
+        ("active_brick_flags", c_uint64),
+        ("active_brick_info", c_uint32 * 8),
+        ("width", c_uint32),
+        ("height", c_uint32),
+        ("depth", c_uint32),
+        ("dtype", c_int32),
+    ]
+
+
+class FxDebugBuffers(Structure):
+    _fields_ = [
+        ("render", FxRenderBuffers),
+        ("velocity_magnitude", c_uint64),
+        ("divergence", c_uint64),
+        ("pressure", c_uint64),
+        ("vorticity_magnitude", c_uint64),
+        ("confinement_force_magnitude", c_uint64),
+    ]
+
+
+class FxStats(Structure):
+    _fields_ = [
+        ("step_index", c_int64),
+        ("current_scalar_set", c_int32),
+        ("last_pressure_buffer", c_int32),
+        ("brick_count", c_uint32),
+        ("active_bricks", c_uint32),
+        ("kernels_per_step", c_uint32),
+        ("reserved", c_uint32),
+    ]
+
+
+class FxKernelTime(Structure):
+    _fields_ = [("name", ctypes.c_char * 48), ("launches", c_uint32), ("reserved", c_uint32), ("total_ms", c_double)]
+
+
+FX_INSTR_KERNEL_TIMES = 1 << 0
+FX_INSTR_COUNT_ACTIVE = 1 << 1
+
+
+# (name, restype, argtypes) of every function include/fenix_cuda.h declares.
+PROTOTYPES = [
+    ("fx_abi_version", c_int32, []),
+    ("fx_last_error", c_char_p, []),
+    ("fx_sim_options_default", None, [POINTER(FxSimOptions)]),
+    ("fx_sim_create", c_int32, [POINTER(FxSimOptions), POINTER(c_void_p)]),
+    ("fx_sim_destroy", None, [c_void_p]),
+    ("fx_sim_step", c_int32, [c_void_p, c_double, c_double]),
+    ("fx_sim_get_render_buffers", c_int32, [c_void_p, POINTER(FxRenderBuffers)]),
+    ("fx_sim_get_debug_buffers", c_int32, [c_void_p, POINTER(FxDebugBuffers)]),
+    ("fx_sim_get_scalar_advection_mode", c_int32, [c_void_p, POINTER(c_int32)]),
+    ("fx_sim_set_scalar_advection_mode", c_int32, [c_void_p, c_int32]),
+    ("fx_sim_get_runtime_params", c_int32, [c_void_p, POINTER(FxRuntimeParams)]),
+    ("fx_sim_set_runtime_params", c_int32, [c_void_p, POINTER(FxRuntimeParams), c_uint32]),
+    ("fx_sim_get_quality", c_int32, [c_void_p, POINTER(FxQuality)]),
+    ("fx_sim_set_quality", c_int32, [c_void_p, POINTER(FxQuality), c_uint32]),
+    ("fx_sim_update_sources", c_int32, [c_void_p, POINTER(c_float), c_uint32]),
+    ("fx_sim_reset", c_int32, [c_void_p]),
+    ("fx_sim_get_resolution", c_int32, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_uint32)]),
+    ("fx_sim_field_size", c_int32, [c_void_p, c_int32, POINTER(c_size_t)]),
+    ("fx_sim_read_field", c_int32, [c_void_p, c_int32, c_void_p, c_size_t]),
+    ("fx_sim_write_field", c_int32, [c_void_p, c_int32, c_void_p, c_size_t]),
+    ("fx_sim_synchronize", c_int32, [c_void_p]),
+    ("fx_sim_get_stats", c_int32, [c_void_p, POINTER(FxStats)]),
+    ("fx_sim_set_instrumentation", c_int32, [c_void_p, c_uint32]),
+    ("fx_sim_read_kernel_times", c_int32, [c_void_p, POINTER(FxKernelTime), c_uint32, POINTER(c_uint32)]),
+    ("fx_sim_read_active_counters", c_int32, [c_void_p, POINTER(c_uint64), POINTER(c_uint64)]),
+    ("fx_sim_get_stream", c_int32, [c_void_p, POINTER(c_void_p)]),
+    ("fx_sim_last_error", c_char_p, [c_void_p]),
+]
+
+# Test hooks exported beside the ABI (not declared in the public header).
+TEST_PROTOTYPES = [
+    ("fx_test_pinned_sincos", c_int32, [POINTER(c_float), POINTER(c_float), c_uint32, c_int32]),
+]
+
+_LIB = None
+
+
+class FenixError(RuntimeError):
+    """A C-ABI call returned a negative fx_status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"fenix_cuda status {status}: {message}")
+        self.status = status
+
+
+def load(path: str | None = None) -> ctypes.CDLL:
+    """Loads the CUDA library once. Raises if it is missing: no fallback exists."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"libfenixcuda.so not found at {p}: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+            "(nvcc, sm_100a). The simulation has no CPU fallback."
+        )
+    lib = ctypes.CDLL(p)
+    for name, res, args in PROTOTYPES + TEST_PROTOTYPES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _LIB = lib
+    return lib
+
+
+def check(status: int, sim_handle=None) -> None:
+    if status == FX_OK:
+        return
+    lib = load()
+    msg = lib.fx_sim_last_error(sim_handle) if sim_handle else lib.fx_last_error()
+    raise FenixError(status, (msg or b"").decode(errors="replace"))

@@ -1,0 +1,62 @@
+"""Build recipe of libfenixcuda.so (nvcc, sm_100a, built in-tree).
+
+Flags that the bit-exact parity of the kernels depends on:
+  -fmad=false                 no contraction of a*b+c into FMA (explicit fmaf stays)
+  -prec-div=true -prec-sqrt=true -ftz=false   IEEE division, square root, denormals
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(PACKAGE_DIR, "csrc")
+SOURCES = ["fx_sim.cu", "fx_plain.cu", "fx_fused.cu"]
+OUTPUT = os.path.join(PACKAGE_DIR, "libfenixcuda.so")
+
+NVCC_FLAGS = [
+    "-std=c++17",
+    "-O3",
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo",
+    "-fmad=false",
+    "-prec-div=true",
+    "-prec-sqrt=true",
+    "-ftz=false",
+    "-Xcompiler", "-fPIC,-ffp-contract=off",
+    "-shared",
+]
+
+
+def nvcc() -> str:
+    if os.environ.get("NVCC"):
+        return os.environ["NVCC"]
+    return "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc"
+
+
+def sources() -> list[str]:
+    return [os.path.join(CSRC, s) for s in SOURCES]
+
+
+def needs_build() -> bool:
+    if not os.path.exists(OUTPUT):
+        return True
+    out_m = os.path.getmtime(OUTPUT)
+    deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
+    deps.append(os.path.join(PACKAGE_DIR, "..", "include", "fenix_cuda.h"))
+    return any(os.path.getmtime(d) > out_m for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not needs_build():
+        return OUTPUT
+    cmd = [nvcc(), *NVCC_FLAGS, "-o", OUTPUT, *sources()]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    return OUTPUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

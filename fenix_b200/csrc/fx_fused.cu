@@ -1,0 +1,884 @@
+// Fused kernel path (see fx_fused.h).
+//
+// The step is the reference's (runtime/createCombustionVolumeSimulation.ts:270-301)
+// with the same per-voxel arithmetic as the plain path, reorganised for B200:
+//  - Injection visits only the bricks that intersect an emitter's reach (host-culled
+//    list). The reference clamps the whole velocity field to +-80/dx inside its
+//    velocity-injection pass (inject-velocity.wgsl.ts:94-95); the only reader of
+//    that field before projection rewrites it is velocity advection, so the clamp
+//    is applied there, on every value read, which gives identical results.
+//  - Brick flags (compute-active-bricks.wgsl.ts) are built from per-brick summaries
+//    (bit 0: a sample is above 0.012, bit 1: the brick dilates) that the kernels
+//    writing a scalar set emit as a by-product, then dilated in gather form:
+//    flag[b] = active[b] OR any neighbour n (Chebyshev distance 1) with
+//    active[n] AND dilate[n]. That is the reference's clamped scatter.
+//  - Scalar advection, combustion and buoyancy run over compacted brick lists.
+//    Per-brick "may be non-zero" bits of each scalar buffer let the kernels skip
+//    bricks that are already zero where the reference rewrites zeros.
+//  - Combustion writes the next set from the advected scratch set, so every
+//    neighbour read sees the state before the pass.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fx_fused.h"
+
+namespace fx {
+namespace {
+
+inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+constexpr int kBrickThreads = 256;
+
+__global__ void k_count_flags(const uint32_t* __restrict__ flags, uint32_t nb, uint32_t* __restrict__ out) {
+  uint32_t local = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x) local += flags[i] != 0u;
+  for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(out, local);
+}
+
+// One thread per brick; block-level sums, one atomic pair per block.
+__global__ void k_accumulate_active(Dims dm, uint3 bc, const uint32_t* __restrict__ flags, unsigned long long* __restrict__ acc) {
+  const uint32_t nb = bc.x * bc.y * bc.z;
+  unsigned long long bricks = 0, voxels = 0;
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    if (flags[b] == 0u) continue;
+    const uint32_t bx = b % bc.x, by = (b / bc.x) % bc.y, bz = b / (bc.x * bc.y);
+    const uint32_t ex = min(8u, dm.w - 8u * bx), ey = min(8u, dm.h - 8u * by), ez = min(8u, dm.d - 8u * bz);
+    bricks += 1;
+    voxels += (unsigned long long)ex * ey * ez;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    bricks += __shfl_down_sync(0xffffffffu, bricks, o);
+    voxels += __shfl_down_sync(0xffffffffu, voxels, o);
+  }
+  __shared__ unsigned long long sb[32], sv[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sb[warp] = bricks;
+    sv[warp] = voxels;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    bricks = lane < nw ? sb[lane] : 0;
+    voxels = lane < nw ? sv[lane] : 0;
+    for (int o = 16; o > 0; o >>= 1) {
+      bricks += __shfl_down_sync(0xffffffffu, bricks, o);
+      voxels += __shfl_down_sync(0xffffffffu, voxels, o);
+    }
+    if (lane == 0 && bricks) {
+      atomicAdd(acc, bricks);
+      atomicAdd(acc + 1, voxels);
+    }
+  }
+}
+
+// Brick geometry of a list entry and the two voxels each thread owns.
+struct BrickCtx {
+  uint32_t bx, by, bz;
+  uint32_t x0, y0, z0;
+  uint32_t cx, cy, cz;  // flag centre (compute-active-bricks.wgsl.ts:52)
+};
+
+FX_DEV BrickCtx brick_ctx(const Dims& dm, uint3 bc, uint32_t b) {
+  BrickCtx c;
+  c.bx = b % bc.x;
+  c.by = (b / bc.x) % bc.y;
+  c.bz = b / (bc.x * bc.y);
+  c.x0 = c.bx * 8u;
+  c.y0 = c.by * 8u;
+  c.z0 = c.bz * 8u;
+  c.cx = min(c.x0 + 4u, dm.w - 1u);
+  c.cy = min(c.y0 + 4u, dm.h - 1u);
+  c.cz = min(c.z0 + 4u, dm.d - 1u);
+  return c;
+}
+
+// Sample-point test of compute-active-bricks.wgsl.ts:35-58 for one voxel of a
+// brick: local coordinates all even are samples, plus the brick's flag centre.
+struct Energy {
+  bool over_active;  // some sample or the centre > 0.012
+  bool over_peak;    // peak > 0.05 (over samples and centre)
+  bool center_hot;   // centre > 0.035
+};
+
+FX_DEV void energy_vote(const BrickCtx& c, uint32_t x, uint32_t y, uint32_t z, bool inside, float d, float t, float r, Energy& e) {
+  if (!inside) return;
+  const bool sample = ((x - c.x0) & 1u) == 0u && ((y - c.y0) & 1u) == 0u && ((z - c.z0) & 1u) == 0u;
+  const bool center = x == c.cx && y == c.cy && z == c.cz;
+  if (!sample && !center) return;
+  const float en = d + t * 0.7f + r * 0.9f;
+  if (en > 0.012f) e.over_active = true;
+  if (en > 0.05f) e.over_peak = true;
+  if (center && en > 0.035f) e.center_hot = true;
+}
+
+// Block-wide OR of the votes into the brick summary (bit 0 active, bit 1 dilate).
+FX_DEV uint8_t summary_of(const Energy& e) {
+  const int a = __syncthreads_or(e.over_active ? 1 : 0);
+  const int p = __syncthreads_or(e.over_peak ? 1 : 0);
+  const int h = __syncthreads_or(e.center_hot ? 1 : 0);
+  if (!a) return 0;
+  return (uint8_t)(1u | ((p || h) ? 2u : 0u));
+}
+
+// ------------------------------------------------------------------ injection
+__global__ void __launch_bounds__(kBrickThreads) k_inject(Dims dm, uint3 bc, const Params* __restrict__ Pp, const float* __restrict__ src,
+                                                          uint32_t nsrc, const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
+                                                          ScalarSet set, VelField v, uint8_t* __restrict__ summary, uint8_t* __restrict__ nz) {
+  const Params P = *Pp;
+  const uint32_t n = *count;
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t b = list[li];
+    const BrickCtx c = brick_ctx(dm, bc, b);
+    Energy e{false, false, false};
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const uint32_t lv = threadIdx.x + kBrickThreads * j;
+      const uint32_t x = c.x0 + (lv & 7u), y = c.y0 + ((lv >> 3) & 7u), z = c.z0 + (lv >> 6);
+      const bool inside = x < dm.w && y < dm.h && z < dm.d;
+      float d = 0.f, t = 0.f, f = 0.f, r = 0.f;
+      if (inside) {
+        const uint32_t i = flat(dm, x, y, z);
+        const float px = ((float)x + 0.5f) / (float)dm.w, py = ((float)y + 0.5f) / (float)dm.h, pz = ((float)z + 0.5f) / (float)dm.d;
+        d = set.f[0][i];
+        t = set.f[1][i];
+        f = set.f[2][i];
+        r = set.f[3][i];
+        inject_scalar_voxel(P, src, nsrc, px, py, pz, d, t, f);
+        float vx = v.c[0][i], vy = v.c[1][i], vz = v.c[2][i];
+        inject_velocity_voxel(P, src, nsrc, px, py, pz, vx, vy, vz);
+        const float lim = speed_limit(P);
+        v.c[0][i] = clampv(vx, -lim, lim);
+        v.c[1][i] = clampv(vy, -lim, lim);
+        v.c[2][i] = clampv(vz, -lim, lim);
+        inject_igniter_voxel(P, src, nsrc, px, py, pz, f, r, t);
+        set.f[0][i] = d;
+        set.f[1][i] = t;
+        set.f[2][i] = f;
+        set.f[3][i] = r;
+        any = any || d != 0.f || t != 0.f || f != 0.f || r != 0.f;
+      }
+      energy_vote(c, x, y, z, inside, d, t, r, e);
+    }
+    const uint8_t s = summary_of(e);
+    const int nzb = __syncthreads_or(any ? 1 : 0);
+    if (threadIdx.x == 0) {
+      summary[b] = s;
+      if (nzb) nz[b] = 1;
+    }
+  }
+}
+
+// ------------------------------------------------------------------- dilation
+// flags[b] = active[b] || any neighbour within Chebyshev distance 1 that is
+// active and dilates. Appends to `list` every brick with a flag or with any of
+// the given "may be non-zero" bits set.
+__global__ void k_dilate(uint3 bc, const uint8_t* __restrict__ summary, uint32_t* __restrict__ flags, const uint8_t* __restrict__ nz_a,
+                         const uint8_t* __restrict__ nz_b, uint32_t* __restrict__ list, uint32_t* __restrict__ count) {
+  const uint32_t nb = bc.x * bc.y * bc.z;
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  bool take = false;
+  if (b < nb) {
+    const uint32_t bx = b % bc.x, by = (b / bc.x) % bc.y, bz = b / (bc.x * bc.y);
+    bool flag = (summary[b] & 1u) != 0u;
+    if (!flag) {
+      const uint32_t zlo = bz ? bz - 1 : 0, zhi = min(bz + 1, bc.z - 1);
+      const uint32_t ylo = by ? by - 1 : 0, yhi = min(by + 1, bc.y - 1);
+      const uint32_t xlo = bx ? bx - 1 : 0, xhi = min(bx + 1, bc.x - 1);
+      for (uint32_t z = zlo; z <= zhi && !flag; ++z)
+        for (uint32_t y = ylo; y <= yhi && !flag; ++y)
+          for (uint32_t x = xlo; x <= xhi; ++x)
+            if (summary[x + bc.x * (y + bc.y * z)] == 3u) {
+              flag = true;
+              break;
+            }
+    }
+    flags[b] = flag ? 1u : 0u;
+    take = flag || (nz_a && nz_a[b]) || (nz_b && nz_b[b]);
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, take);
+  if (mask) {
+    const int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == __ffs(mask) - 1) base = atomicAdd(count, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
+    if (take) list[base + __popc(mask & ((1u << lane) - 1u))] = b;
+  }
+}
+
+FX_DEV bool flag_at(const uint32_t* __restrict__ flags, uint3 bc, uint32_t b) { return __ldg(flags + b) != 0u; }
+
+// ------------------------------------------------------------ velocity advection
+// advect-velocity-semilagrangian.wgsl.ts:23-41 over vCurrent clamped to +-lim on read.
+FX_DEV float tri_interp_clamped(const float* __restrict__ f, const Tri& c, float lim) {
+  const float x00 = mixv(clampv(__ldg(f + c.i000), -lim, lim), clampv(__ldg(f + c.i100), -lim, lim), c.fx);
+  const float x10 = mixv(clampv(__ldg(f + c.i010), -lim, lim), clampv(__ldg(f + c.i110), -lim, lim), c.fx);
+  const float x01 = mixv(clampv(__ldg(f + c.i001), -lim, lim), clampv(__ldg(f + c.i101), -lim, lim), c.fx);
+  const float x11 = mixv(clampv(__ldg(f + c.i011), -lim, lim), clampv(__ldg(f + c.i111), -lim, lim), c.fx);
+  return mixv(mixv(x00, x10, c.fy), mixv(x01, x11, c.fy), c.fz);
+}
+
+__global__ void __launch_bounds__(256) k_advect_velocity(Dims dm, const Params* __restrict__ Pp, VelField src, VelField dst) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+  const uint32_t z = blockIdx.z * blockDim.z + threadIdx.z;
+  if (x >= dm.w || y >= dm.h || z >= dm.d) return;
+  const uint32_t i = flat(dm, x, y, z);
+  if (is_boundary(dm, x, y, z)) {
+    dst.c[0][i] = 0.0f;
+    dst.c[1][i] = 0.0f;
+    dst.c[2][i] = 0.0f;
+    return;
+  }
+  const float dt = Pp->dt;
+  const float lim = speed_limit(*Pp);
+  const float cx = (float)x + 0.5f, cy = (float)y + 0.5f, cz = (float)z + 0.5f;
+  const Tri c0 = tri_corners(dm, cx - 0.5f, cy - 0.5f, cz - 0.5f);
+  const float v0x = tri_interp_clamped(src.c[0], c0, lim), v0y = tri_interp_clamped(src.c[1], c0, lim), v0z = tri_interp_clamped(src.c[2], c0, lim);
+  const float bx = cx - v0x * dt, by = cy - v0y * dt, bz = cz - v0z * dt;
+  const Tri c1 = tri_corners(dm, bx - 0.5f, by - 0.5f, bz - 0.5f);
+  const float damp = 1.0f - dt * 0.025f;
+  dst.c[0][i] = tri_interp_clamped(src.c[0], c1, lim) * damp;
+  dst.c[1][i] = tri_interp_clamped(src.c[1], c1, lim) * damp;
+  dst.c[2][i] = tri_interp_clamped(src.c[2], c1, lim) * damp;
+}
+
+// -------------------------------------------------------------- scalar advection
+// advect-scalar-maccormack.wgsl.ts:33-101 / advect-scalar-semilagrangian.wgsl.ts
+// over the bricks of list_adv: flagged bricks are advected into T, the others
+// (T may hold old values there) are zeroed. Emits T's brick summary and non-zero bit.
+__global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3 bc, const Params* __restrict__ Pp, int mode, ScalarSet src,
+                                                                  VelField vel, const uint32_t* __restrict__ flags,
+                                                                  const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
+                                                                  ScalarSet dst, uint8_t* __restrict__ summary, uint8_t* __restrict__ nz) {
+  const Params P = *Pp;
+  const uint32_t n = *count;
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t b = list[li];
+    const BrickCtx c = brick_ctx(dm, bc, b);
+    const bool active = flag_at(flags, bc, b);
+    Energy e{false, false, false};
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const uint32_t lv = threadIdx.x + kBrickThreads * j;
+      const uint32_t x = c.x0 + (lv & 7u), y = c.y0 + ((lv >> 3) & 7u), z = c.z0 + (lv >> 6);
+      const bool inside = x < dm.w && y < dm.h && z < dm.d;
+      float out[4] = {0.f, 0.f, 0.f, 0.f};
+      if (inside && active) {
+        const float dt = P.dt;
+        const float cx = (float)x + 0.5f, cy = (float)y + 0.5f, cz = (float)z + 0.5f;
+        const Tri c0 = tri_corners(dm, cx - 0.5f, cy - 0.5f, cz - 0.5f);
+        const float vx = tri_interp(vel.c[0], c0), vy = tri_interp(vel.c[1], c0), vz = tri_interp(vel.c[2], c0);
+        const float bxp = cx - vx * dt, byp = cy - vy * dt, bzp = cz - vz * dt;
+        const float spx = bxp - 0.5f, spy = byp - 0.5f, spz = bzp - 0.5f;
+        const Tri cs = tri_corners(dm, spx, spy, spz);
+        float noise;
+        if (mode == 1) {
+          const float fvx = tri_interp(vel.c[0], cs), fvy = tri_interp(vel.c[1], cs), fvz = tri_interp(vel.c[2], cs);
+          const float rx = bxp + fvx * dt, ry = byp + fvy * dt, rz = bzp + fvz * dt;
+          const Tri cr = tri_corners(dm, rx - 0.5f, ry - 0.5f, rz - 0.5f);
+#pragma unroll
+          for (int f = 0; f < 4; ++f) {
+            const float predicted = tri_interp(src.f[f], cs);
+            const float recovered = tri_interp(src.f[f], cr);
+            const float original = tri_interp(src.f[f], c0);
+            const float corrected = predicted + 0.5f * (original - recovered);
+            out[f] = clampv(corrected, mn(original, predicted), mx(original, predicted));
+          }
+          noise = thermal_noise(P, cx, cy, cz);
+        } else {
+#pragma unroll
+          for (int f = 0; f < 4; ++f) out[f] = tri_interp(src.f[f], cs);
+          noise = thermal_noise(P, spx, spy, spz);
+        }
+        const float ny = ((float)y + 0.5f) / (float)dm.h;
+        decay_scalars(P, ny, noise, out[0], out[1], out[2], out[3]);
+        any = any || out[0] != 0.f || out[1] != 0.f || out[2] != 0.f || out[3] != 0.f;
+      }
+      if (inside) {
+        const uint32_t i = flat(dm, x, y, z);
+        dst.f[0][i] = out[0];
+        dst.f[1][i] = out[1];
+        dst.f[2][i] = out[2];
+        dst.f[3][i] = out[3];
+      }
+      energy_vote(c, x, y, z, inside, out[0], out[1], out[3], e);
+    }
+    const uint8_t s = summary_of(e);
+    const int nzb = __syncthreads_or(any ? 1 : 0);
+    if (threadIdx.x == 0) {
+      summary[b] = s;
+      nz[b] = nzb ? 1 : 0;
+    }
+  }
+}
+
+// -------------------------------------------------------------------- combustion
+// combustion-update.wgsl.ts:42-93 from T into the next set over list_next:
+// flagged bricks get the combustion update, the others copy T. Emits the next
+// set's brick summary and non-zero bit.
+__global__ void __launch_bounds__(kBrickThreads) k_combustion(Dims dm, uint3 bc, const Params* __restrict__ Pp, ScalarSet tset,
+                                                              const uint32_t* __restrict__ flags, const uint32_t* __restrict__ list,
+                                                              const uint32_t* __restrict__ count, const uint8_t* __restrict__ nz_t,
+                                                              const uint8_t* __restrict__ summary_t, ScalarSet dst,
+                                                              uint8_t* __restrict__ summary, uint8_t* __restrict__ nz) {
+  const Params P = *Pp;
+  const uint32_t n = *count;
+  const uint32_t W1 = dm.w - 1u, H1 = dm.h - 1u, D1 = dm.d - 1u;
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t b = list[li];
+    const BrickCtx c = brick_ctx(dm, bc, b);
+    const bool active = flag_at(flags, bc, b);
+    const bool t_nonzero = nz_t[b] != 0;
+    Energy e{false, false, false};
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const uint32_t lv = threadIdx.x + kBrickThreads * j;
+      const uint32_t x = c.x0 + (lv & 7u), y = c.y0 + ((lv >> 3) & 7u), z = c.z0 + (lv >> 6);
+      const bool inside = x < dm.w && y < dm.h && z < dm.d;
+      if (!inside) continue;
+      const uint32_t i = flat(dm, x, y, z);
+      float d = 0.f, t = 0.f, f = 0.f, r = 0.f;
+      if (t_nonzero || active) {
+        d = __ldg(tset.f[0] + i);
+        t = __ldg(tset.f[1] + i);
+        f = __ldg(tset.f[2] + i);
+        r = __ldg(tset.f[3] + i);
+      }
+      if (active) {
+        auto hot = [&](uint32_t xx, uint32_t yy, uint32_t zz) {
+          const uint32_t k = flat(dm, xx, yy, zz);
+          return comb_hot(__ldg(tset.f[1] + k), __ldg(tset.f[2] + k), __ldg(tset.f[3] + k));
+        };
+        const float nsum = hot(inc(x, W1), y, z) + hot(dec(x), y, z) + hot(x, inc(y, H1), z) + hot(x, dec(y), z) + hot(x, y, inc(z, D1)) +
+                           hot(x, y, dec(z));
+        const float ny = ((float)y + 0.5f) / (float)dm.h;
+        combustion_voxel(P, x, y, z, ny, nsum, d, t, f, r);
+        energy_vote(c, x, y, z, true, d, t, r, e);
+      }
+      dst.f[0][i] = d;
+      dst.f[1][i] = t;
+      dst.f[2][i] = f;
+      dst.f[3][i] = r;
+      any = any || d != 0.f || t != 0.f || f != 0.f || r != 0.f;
+    }
+    const uint8_t s = summary_of(e);
+    const int nzb = __syncthreads_or(any ? 1 : 0);
+    if (threadIdx.x == 0) {
+      summary[b] = active ? s : summary_t[b];
+      nz[b] = nzb ? 1 : 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------- buoyancy
+// apply-buoyancy.wgsl.ts:37-110 over the flagged bricks of list_next.
+__global__ void __launch_bounds__(kBrickThreads) k_buoyancy(Dims dm, uint3 bc, const Params* __restrict__ Pp, ScalarSet set,
+                                                            const uint32_t* __restrict__ flags, const uint32_t* __restrict__ list,
+                                                            const uint32_t* __restrict__ count, VelField v) {
+  const Params P = *Pp;
+  const uint32_t n = *count;
+  const uint32_t W1 = dm.w - 1u, H1 = dm.h - 1u, D1 = dm.d - 1u;
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t b = list[li];
+    if (!flag_at(flags, bc, b)) continue;
+    const BrickCtx c = brick_ctx(dm, bc, b);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const uint32_t lv = threadIdx.x + kBrickThreads * j;
+      const uint32_t x = c.x0 + (lv & 7u), y = c.y0 + ((lv >> 3) & 7u), z = c.z0 + (lv >> 6);
+      if (x >= dm.w || y >= dm.h || z >= dm.d) continue;
+      const uint32_t i = flat(dm, x, y, z);
+      const float* D = set.f[0];
+      auto hot = [&](uint32_t xx, uint32_t yy, uint32_t zz) {
+        const uint32_t k = flat(dm, xx, yy, zz);
+        return buoy_hot(__ldg(set.f[1] + k), __ldg(set.f[3] + k));
+      };
+      const float hot_gas = hot(x, y, z);
+      const float tgx = (hot(inc(x, W1), y, z) - hot(dec(x), y, z)) * 0.5f;
+      const float tgy = (hot(x, inc(y, H1), z) - hot(x, dec(y), z)) * 0.5f;
+      const float tgz = (hot(x, y, inc(z, D1)) - hot(x, y, dec(z))) * 0.5f;
+      const float dgx = (__ldg(D + flat(dm, inc(x, W1), y, z)) - __ldg(D + flat(dm, dec(x), y, z))) * 0.5f;
+      const float dgy = (__ldg(D + flat(dm, x, inc(y, H1), z)) - __ldg(D + flat(dm, x, dec(y), z))) * 0.5f;
+      const float dgz = (__ldg(D + flat(dm, x, y, inc(z, D1))) - __ldg(D + flat(dm, x, y, dec(z)))) * 0.5f;
+      float vx = v.c[0][i], vy = v.c[1][i], vz = v.c[2][i];
+      buoyancy_voxel(P, dm, x, y, z, __ldg(D + i), hot_gas, tgx, tgy, tgz, dgx, dgy, dgz, vx, vy, vz);
+      v.c[0][i] = vx;
+      v.c[1][i] = vy;
+      v.c[2][i] = vz;
+    }
+  }
+}
+
+// ------------------------------------------------------------ vorticity magnitude
+// compute-vorticity.wgsl.ts:23-50: |w| for every voxel (w itself only when the
+// debug fields are wanted; the confinement kernel recomputes w at its voxel).
+FX_DEV void curl_at(const Dims& dm, const VelField& v, uint32_t x, uint32_t y, uint32_t z, float& cx, float& cy, float& cz) {
+  const uint32_t W1 = dm.w - 1u, H1 = dm.h - 1u, D1 = dm.d - 1u;
+  const uint32_t x0 = flat(dm, dec(x), y, z), x1 = flat(dm, inc(x, W1), y, z);
+  const uint32_t y0 = flat(dm, x, dec(y), z), y1 = flat(dm, x, inc(y, H1), z);
+  const uint32_t z0 = flat(dm, x, y, dec(z)), z1 = flat(dm, x, y, inc(z, D1));
+  cx = ((__ldg(v.c[2] + y1) - __ldg(v.c[2] + y0)) - (__ldg(v.c[1] + z1) - __ldg(v.c[1] + z0))) * 0.5f;
+  cy = ((__ldg(v.c[0] + z1) - __ldg(v.c[0] + z0)) - (__ldg(v.c[2] + x1) - __ldg(v.c[2] + x0))) * 0.5f;
+  cz = ((__ldg(v.c[1] + x1) - __ldg(v.c[1] + x0)) - (__ldg(v.c[0] + y1) - __ldg(v.c[0] + y0))) * 0.5f;
+}
+
+__global__ void __launch_bounds__(256) k_vorticity(Dims dm, VelField v, float* __restrict__ wmag, VelField w, int write_w) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+  const uint32_t z = blockIdx.z * blockDim.z + threadIdx.z;
+  if (x >= dm.w || y >= dm.h || z >= dm.d) return;
+  const uint32_t i = flat(dm, x, y, z);
+  float cx = 0.f, cy = 0.f, cz = 0.f;
+  if (!is_boundary(dm, x, y, z)) curl_at(dm, v, x, y, z, cx, cy, cz);
+  wmag[i] = is_boundary(dm, x, y, z) ? 0.0f : length3(cx, cy, cz);
+  if (write_w) {
+    w.c[0][i] = cx;
+    w.c[1][i] = cy;
+    w.c[2][i] = cz;
+  }
+}
+
+// apply-vorticity-confinement.wgsl.ts:30-66 from vScratch into vScratch2, with w
+// recomputed at the voxel and the scalars read only from bricks that may be
+// non-zero.
+__global__ void __launch_bounds__(256) k_confinement(Dims dm, uint3 bc, const Params* __restrict__ Pp, VelField v, const float* __restrict__ wmag,
+                                                     ScalarSet set, const uint8_t* __restrict__ nz, VelField out, float* __restrict__ fmag,
+                                                     int write_fmag) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+  const uint32_t z = blockIdx.z * blockDim.z + threadIdx.z;
+  if (x >= dm.w || y >= dm.h || z >= dm.d) return;
+  const uint32_t i = flat(dm, x, y, z);
+  float vx = __ldg(v.c[0] + i), vy = __ldg(v.c[1] + i), vz = __ldg(v.c[2] + i);
+  if (is_boundary(dm, x, y, z)) {
+    out.c[0][i] = vx;
+    out.c[1][i] = vy;
+    out.c[2][i] = vz;
+    if (write_fmag) fmag[i] = 0.0f;
+    return;
+  }
+  const Params P = *Pp;
+  const uint32_t W1 = dm.w - 1u, H1 = dm.h - 1u, D1 = dm.d - 1u;
+  const float gx = (__ldg(wmag + flat(dm, inc(x, W1), y, z)) - __ldg(wmag + flat(dm, dec(x), y, z))) * 0.5f;
+  const float gy = (__ldg(wmag + flat(dm, x, inc(y, H1), z)) - __ldg(wmag + flat(dm, x, dec(y), z))) * 0.5f;
+  const float gz = (__ldg(wmag + flat(dm, x, y, inc(z, D1))) - __ldg(wmag + flat(dm, x, y, dec(z)))) * 0.5f;
+  float wx, wy, wz;
+  curl_at(dm, v, x, y, z, wx, wy, wz);
+  const uint32_t b = (x >> 3) + bc.x * ((y >> 3) + bc.y * (z >> 3));
+  float d = 0.f, t = 0.f, r = 0.f;
+  if (__ldg(nz + b)) {
+    d = __ldg(set.f[0] + i);
+    t = __ldg(set.f[1] + i);
+    r = __ldg(set.f[3] + i);
+  }
+  const float fm = confinement_voxel(P, gx, gy, gz, wx, wy, wz, __ldg(wmag + i), d, t, r, vx, vy, vz);
+  out.c[0][i] = vx;
+  out.c[1][i] = vy;
+  out.c[2][i] = vz;
+  if (write_fmag) fmag[i] = fm;
+}
+
+// Projection (project-velocity.wgsl.ts:21-43) with |v|
+// (compute-debug-fields.wgsl.ts:18-25) fused when it is due.
+__global__ void __launch_bounds__(256) k_project(Dims dm, VelField vs, const float* __restrict__ p, VelField vd, float* __restrict__ vmag,
+                                                 int write_vmag) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+  const uint32_t z = blockIdx.z * blockDim.z + threadIdx.z;
+  if (x >= dm.w || y >= dm.h || z >= dm.d) return;
+  const uint32_t i = flat(dm, x, y, z);
+  float ox = 0.f, oy = 0.f, oz = 0.f;
+  if (!is_boundary(dm, x, y, z)) {
+    const uint32_t W1 = dm.w - 1u, H1 = dm.h - 1u, D1 = dm.d - 1u;
+    const float gx = (__ldg(p + flat(dm, inc(x, W1), y, z)) - __ldg(p + flat(dm, dec(x), y, z))) * 0.5f;
+    const float gy = (__ldg(p + flat(dm, x, inc(y, H1), z)) - __ldg(p + flat(dm, x, dec(y), z))) * 0.5f;
+    const float gz = (__ldg(p + flat(dm, x, y, inc(z, D1))) - __ldg(p + flat(dm, x, y, dec(z)))) * 0.5f;
+    ox = __ldg(vs.c[0] + i) - gx;
+    oy = __ldg(vs.c[1] + i) - gy;
+    oz = __ldg(vs.c[2] + i) - gz;
+  }
+  vd.c[0][i] = ox;
+  vd.c[1][i] = oy;
+  vd.c[2][i] = oz;
+  if (write_vmag) vmag[i] = length3(ox, oy, oz);
+}
+
+// Rebuilds the per-brick bookkeeping after the fields were written from the host:
+// the non-zero bits of the three scalar buffers and the summary of the current set.
+__global__ void __launch_bounds__(kBrickThreads) k_rebuild(Dims dm, uint3 bc, ScalarSet cur, ScalarSet other, ScalarSet tset,
+                                                           uint8_t* __restrict__ summary_cur, uint8_t* __restrict__ nz_cur,
+                                                           uint8_t* __restrict__ nz_other, uint8_t* __restrict__ nz_t) {
+  const uint32_t nb = bc.x * bc.y * bc.z;
+  for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+    const BrickCtx c = brick_ctx(dm, bc, b);
+    Energy e{false, false, false};
+    bool a0 = false, a1 = false, a2 = false;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const uint32_t lv = threadIdx.x + kBrickThreads * j;
+      const uint32_t x = c.x0 + (lv & 7u), y = c.y0 + ((lv >> 3) & 7u), z = c.z0 + (lv >> 6);
+      const bool inside = x < dm.w && y < dm.h && z < dm.d;
+      float d = 0.f, t = 0.f, r = 0.f;
+      if (inside) {
+        const uint32_t i = flat(dm, x, y, z);
+        d = cur.f[0][i];
+        t = cur.f[1][i];
+        r = cur.f[3][i];
+        a0 = a0 || d != 0.f || t != 0.f || cur.f[2][i] != 0.f || r != 0.f;
+        a1 = a1 || other.f[0][i] != 0.f || other.f[1][i] != 0.f || other.f[2][i] != 0.f || other.f[3][i] != 0.f;
+        a2 = a2 || tset.f[0][i] != 0.f || tset.f[1][i] != 0.f || tset.f[2][i] != 0.f || tset.f[3][i] != 0.f;
+      }
+      energy_vote(c, x, y, z, inside, d, t, r, e);
+    }
+    const uint8_t s = summary_of(e);
+    const int n0 = __syncthreads_or(a0 ? 1 : 0);
+    const int n1 = __syncthreads_or(a1 ? 1 : 0);
+    const int n2 = __syncthreads_or(a2 ? 1 : 0);
+    if (threadIdx.x == 0) {
+      summary_cur[b] = s;
+      nz_cur[b] = n0 ? 1 : 0;
+      nz_other[b] = n1 ? 1 : 0;
+      nz_t[b] = n2 ? 1 : 0;
+    }
+  }
+}
+
+inline dim3 dense_grid(Dims d) { return dim3((d.w + 31) / 32, (d.h + 3) / 4, (d.d + 1) / 2); }
+const dim3 kDenseBlock(32, 4, 2);
+
+// Host: bricks whose voxels an emitter can reach this step (conservative).
+void injection_bricks(const FusedStep& st, std::vector<uint8_t>& mark, std::vector<uint32_t>& out) {
+  out.clear();
+  if (!st.host_sources || st.host_nsrc == 0) return;
+  const Dims dm = st.dm;
+  const uint3 bc = st.bricks;
+  mark.assign((size_t)bc.x * bc.y * bc.z, 0);
+  const double dxw = (double)st.host_params.dx / std::max((double)st.host_params.world_size, 1e-4);
+  const double t = st.host_params.time;
+  for (uint32_t e = 0; e < st.host_nsrc; ++e) {
+    const float* s = st.host_sources + 32 * (size_t)e;
+    const double start = s[4], duration = s[5];
+    const double age = t - start;
+    // activeGate (inject-source-common.wgsl.ts:24-27) with a margin for f32 rounding
+    if (!(age >= -1e-3 * (1.0 + std::fabs(t)) && age <= duration + 1e-3 * (1.0 + std::fabs(duration)))) {
+      if (std::isfinite(age) && std::isfinite(duration)) continue;
+    }
+    const double r = s[3];
+    double reach = r + std::max(r * 0.24, dxw * 3.0);
+    if (!std::isfinite(reach)) reach = 4.0;
+    reach = std::max(reach, 0.0) * 1.0001 + 1e-6;
+    uint32_t lo[3], hi[3];
+    const uint32_t dims[3] = {dm.w, dm.h, dm.d};
+    bool empty = false;
+    for (int a = 0; a < 3; ++a) {
+      const double c = s[a];
+      double l = std::floor((c - reach) * dims[a] - 0.5) - 1.0, h = std::ceil((c + reach) * dims[a] - 0.5) + 1.0;
+      if (!std::isfinite(l)) l = 0;
+      if (!std::isfinite(h)) h = dims[a] - 1.0;
+      l = std::max(l, 0.0);
+      h = std::min(h, dims[a] - 1.0);
+      if (h < l) {
+        empty = true;
+        break;
+      }
+      lo[a] = (uint32_t)l;
+      hi[a] = (uint32_t)h;
+    }
+    if (empty) continue;
+    for (uint32_t bz = lo[2] / 8; bz <= hi[2] / 8; ++bz)
+      for (uint32_t by = lo[1] / 8; by <= hi[1] / 8; ++by)
+        for (uint32_t bx = lo[0] / 8; bx <= hi[0] / 8; ++bx) {
+          const uint32_t b = bx + bc.x * (by + bc.y * bz);
+          if (!mark[b]) {
+            mark[b] = 1;
+            out.push_back(b);
+          }
+        }
+  }
+}
+
+}  // namespace
+
+size_t fused_work_bytes(Dims, uint3 bricks) {
+  const size_t nb = (size_t)bricks.x * bricks.y * bricks.z;
+  return 8 * align256(nb) + 3 * align256(nb * 4) + align256(16 * 4);
+}
+
+void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks) {
+  w.dm = dm;
+  w.bricks = bricks;
+  w.nb = bricks.x * bricks.y * bricks.z;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char* p = base + off;
+    off += align256(bytes);
+    return p;
+  };
+  w.summary_set[0] = (uint8_t*)take(w.nb);
+  w.summary_set[1] = (uint8_t*)take(w.nb);
+  w.summary_t = (uint8_t*)take(w.nb);
+  w.nz_set[0] = (uint8_t*)take(w.nb);
+  w.nz_set[1] = (uint8_t*)take(w.nb);
+  w.nz_t = (uint8_t*)take(w.nb);
+  take(w.nb);
+  take(w.nb);
+  w.list_adv = (uint32_t*)take((size_t)w.nb * 4);
+  w.list_next = (uint32_t*)take((size_t)w.nb * 4);
+  w.list_inj = (uint32_t*)take((size_t)w.nb * 4);
+  w.counters = (uint32_t*)take(16 * 4);
+}
+
+fx_status fused_init(FusedWork& w, cudaStream_t) {
+  if (cudaEventCreateWithFlags(&w.inj_event, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
+  if (cudaMallocHost(&w.host_list_inj, ((size_t)w.nb + 1) * 4) != cudaSuccess) return FX_ERR_OUT_OF_MEMORY;
+  w.valid = true;  // the arena starts cleared: every brick is zero
+  return FX_OK;
+}
+
+fx_status fused_reset(FusedWork& w, cudaStream_t) {
+  w.valid = true;
+  return FX_OK;
+}
+
+fx_status fused_invalidate(FusedWork& w, cudaStream_t) {
+  w.valid = false;
+  return FX_OK;
+}
+
+void fused_release(FusedWork& w) {
+  if (w.inj_event) cudaEventDestroy(w.inj_event);
+  w.inj_event = nullptr;
+  if (w.host_list_inj) cudaFreeHost(w.host_list_inj);
+  w.host_list_inj = nullptr;
+  for (auto& ev : w.timing_events) cudaEventDestroy(ev);
+  w.timing_events.clear();
+}
+
+void fused_set_timing(FusedWork& w, bool on) { w.timing = on; }
+
+void fused_drain_timing(FusedWork& w, const std::function<void(const char*, uint32_t, double)>& sink) {
+  for (auto& p : w.timing_pending) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, w.timing_events[p.a], w.timing_events[p.b]);
+    sink(p.name, 1, ms);
+  }
+  w.timing_pending.clear();
+  w.timing_next = 0;
+}
+
+namespace {
+
+struct Timed {
+  FusedWork& w;
+  cudaStream_t s;
+  int a = -1;
+  const char* name;
+  Timed(FusedWork& w_, cudaStream_t s_, const char* n) : w(w_), s(s_), name(n) {
+    if (!w.timing) return;
+    a = w.next_event();
+    cudaEventRecord(w.timing_events[a], s);
+  }
+  ~Timed() {
+    if (!w.timing) return;
+    const int b = w.next_event();
+    cudaEventRecord(w.timing_events[b], s);
+    w.timing_pending.push_back({name, a, b});
+  }
+};
+
+}  // namespace
+
+int FusedWork::next_event() {
+  if (timing_next >= (int)timing_events.size()) {
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    timing_events.push_back(e);
+  }
+  return timing_next++;
+}
+
+fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
+  cudaStream_t s = st.stream;
+  const Dims dm = st.dm;
+  const uint3 bc = st.bricks;
+  const uint32_t nb = w.nb;
+  const int cur = st.cur_index, next = cur ^ 1;
+  uint32_t launches = 0;
+  const uint32_t brick_grid = std::max<uint32_t>(1, std::min<uint32_t>(nb, 148u * 8u));
+  uint32_t* c_adv = w.counters + 0;
+  uint32_t* c_next = w.counters + 1;
+  uint32_t* c_inj = w.counters + 3;
+#define FX_CK(call)                              \
+  do {                                           \
+    cudaError_t e_ = (call);                     \
+    if (e_ != cudaSuccess) {                     \
+      out.error = std::string(#call) + ": " + cudaGetErrorString(e_); \
+      return FX_ERR_CUDA;                        \
+    }                                            \
+  } while (0)
+
+  if (!w.valid) {
+    Timed tm(w, s, "fused_rebuild");
+    k_rebuild<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.cur, st.next, st.scratch, w.summary_set[cur], w.nz_set[cur], w.nz_set[next], w.nz_t);
+    ++launches;
+    w.valid = true;
+  }
+
+  // 1. injection over the reachable bricks
+  injection_bricks(st, w.host_mark, w.host_list);
+  const uint32_t ninj = (uint32_t)w.host_list.size();
+  if (ninj) {
+    FX_CK(cudaEventSynchronize(w.inj_event));
+    std::memcpy(w.host_list_inj, w.host_list.data(), ninj * 4);
+    w.host_list_inj[nb] = ninj;
+    FX_CK(cudaMemcpyAsync(w.list_inj, w.host_list_inj, ninj * 4, cudaMemcpyHostToDevice, s));
+    FX_CK(cudaMemcpyAsync(c_inj, w.host_list_inj + nb, 4, cudaMemcpyHostToDevice, s));
+    FX_CK(cudaEventRecord(w.inj_event, s));
+    Timed tm(w, s, "fused_inject");
+    k_inject<<<std::min<uint32_t>(ninj, brick_grid), kBrickThreads, 0, s>>>(dm, bc, st.params, st.sources, st.nsrc, w.list_inj, c_inj, st.cur,
+                                                                            st.vcur, w.summary_set[cur], w.nz_set[cur]);
+    ++launches;
+  }
+
+  // 2. flags of the current set, list of bricks for scalar advection
+  FX_CK(cudaMemsetAsync(w.counters, 0, 3 * sizeof(uint32_t), s));
+  {
+    Timed tm(w, s, "fused_dilate");
+    k_dilate<<<(nb + 255) / 256, 256, 0, s>>>(bc, w.summary_set[cur], st.flags_cur, w.nz_t, nullptr, w.list_adv, c_adv);
+    ++launches;
+  }
+  // 3. velocity advection (dense)
+  {
+    Timed tm(w, s, "fused_advect_velocity");
+    k_advect_velocity<<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, st.params, st.vcur, st.vscr);
+    ++launches;
+  }
+  // 4. scalar advection over the list
+  FX_CK(cudaMemsetAsync(w.summary_t, 0, nb, s));
+  {
+    Timed tm(w, s, "fused_advect_scalars");
+    k_advect_scalars<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.advect_mode, st.cur, st.vscr, st.flags_cur, w.list_adv, c_adv,
+                                                          st.scratch, w.summary_t, w.nz_t);
+    ++launches;
+  }
+  // 5. flags of the advected set
+  {
+    Timed tm(w, s, "fused_dilate");
+    k_dilate<<<(nb + 255) / 256, 256, 0, s>>>(bc, w.summary_t, st.flags_next, w.nz_t, w.nz_set[next], w.list_next, c_next);
+    ++launches;
+  }
+  // 6. combustion T -> next set, 7. buoyancy
+  FX_CK(cudaMemsetAsync(w.summary_set[next], 0, nb, s));
+  {
+    Timed tm(w, s, "fused_combustion");
+    k_combustion<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.scratch, st.flags_next, w.list_next, c_next, w.nz_t, w.summary_t,
+                                                      st.next, w.summary_set[next], w.nz_set[next]);
+    ++launches;
+  }
+  {
+    Timed tm(w, s, "fused_buoyancy");
+    k_buoyancy<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.next, st.flags_next, w.list_next, c_next, st.vscr);
+    ++launches;
+  }
+  // 8. vorticity confinement
+  const VelField* vfinal = &st.vscr;
+  if (st.vort_on) {
+    {
+      Timed tm(w, s, "fused_vorticity");
+      k_vorticity<<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, st.vscr, st.vort_mag, st.vort, st.debug_fields ? 1 : 0);
+      ++launches;
+    }
+    {
+      Timed tm(w, s, "fused_confinement");
+      k_confinement<<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, bc, st.params, st.vscr, st.vort_mag, st.next, w.nz_set[next], st.vscr2,
+                                                           st.conf_mag, st.debug_fields ? 1 : 0);
+      ++launches;
+    }
+    vfinal = &st.vscr2;
+  }
+  // 9. pressure
+  int last_p = st.last_p;
+  if (st.pressure_on) {
+    for (int l = 0; l < 3; ++l)
+      FX_CK(cudaMemsetAsync(st.lv[l].p[0], 0, (size_t)st.lv[l].dm.w * st.lv[l].dm.h * st.lv[l].dm.d * sizeof(float), s));
+    {
+      Timed tm(w, s, "fused_divergence");
+      plain_divergence(s, dm, *vfinal, st.lv[0].div);
+      ++launches;
+    }
+    auto smooth = [&](const LevelBuf& L, int iters, int start, const char* name) {
+      int a = start;
+      for (int k = 0; k < iters; ++k) {
+        Timed tm(w, s, name);
+        plain_jacobi(s, L.dm, L.div, L.p[a], L.p[a ^ 1]);
+        a ^= 1;
+        ++launches;
+      }
+      return a;
+    };
+    const int fine_pre = smooth(st.lv[0], st.q[2], 0, "fused_jacobi_fine");
+    {
+      Timed tm(w, s, "fused_restrict");
+      plain_restrict(s, st.lv[0].dm, st.lv[1].dm, st.lv[0].div, st.lv[1].div);
+      ++launches;
+    }
+    const int mid_pre = smooth(st.lv[1], st.q[4], 0, "fused_jacobi_mid");
+    {
+      Timed tm(w, s, "fused_restrict");
+      plain_restrict(s, st.lv[1].dm, st.lv[2].dm, st.lv[1].div, st.lv[2].div);
+      ++launches;
+    }
+    const int coarse = smooth(st.lv[2], st.q[6], 0, "fused_jacobi_coarse");
+    {
+      Timed tm(w, s, "fused_prolong");
+      plain_prolong(s, st.lv[2].dm, st.lv[1].dm, st.lv[2].p[coarse], st.lv[1].p[0]);
+      ++launches;
+    }
+    const int mid = smooth(st.lv[1], st.q[5], mid_pre, "fused_jacobi_mid");
+    {
+      Timed tm(w, s, "fused_prolong");
+      plain_prolong(s, st.lv[1].dm, st.lv[0].dm, st.lv[1].p[mid], st.lv[0].p[0]);
+      ++launches;
+    }
+    last_p = smooth(st.lv[0], st.q[3], fine_pre, "fused_jacobi_fine");
+  }
+  // 10. projection (+ |v|)
+  {
+    Timed tm(w, s, "fused_project");
+    k_project<<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0);
+    ++launches;
+  }
+  FX_CK(cudaGetLastError());
+#undef FX_CK
+  out.last_p = last_p;
+  out.final_vscr_is_2 = st.vort_on;
+  out.launches = launches;
+  return FX_OK;
+}
+
+fx_status fused_count_active(FusedWork& w, cudaStream_t s, const uint32_t* flags, uint32_t nb, uint32_t* out) {
+  uint32_t* c = w.counters + 2;
+  if (cudaMemsetAsync(c, 0, 4, s) != cudaSuccess) return FX_ERR_CUDA;
+  k_count_flags<<<148, 256, 0, s>>>(flags, nb, c);
+  uint32_t h = 0;
+  if (cudaMemcpyAsync(&h, c, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return FX_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return FX_ERR_CUDA;
+  *out = h;
+  return FX_OK;
+}
+
+cudaError_t fused_accumulate_active(cudaStream_t s, Dims dm, uint3 bricks, const uint32_t* flags, unsigned long long* acc) {
+  const uint32_t nb = bricks.x * bricks.y * bricks.z;
+  const uint32_t blocks = std::min<uint32_t>((nb + 255) / 256, 148);
+  k_accumulate_active<<<blocks, 256, 0, s>>>(dm, bricks, flags, acc);
+  return cudaGetLastError();
+}
+
+}  // namespace fx

@@ -1,0 +1,87 @@
+// The fused kernel path: the same step as the plain path with the same bits,
+// computed by fewer, brick-list-driven kernels captured in a CUDA graph.
+#pragma once
+
+#include <cstdint>
+#include <functional>
+#include <string>
+#include <cuda_runtime.h>
+
+#include "../../include/fenix_cuda.h"
+#include "fx_kernels.h"
+
+namespace fx {
+
+// Device work buffers of the fused path, carved from the simulation's arena.
+struct FusedWork {
+  Dims dm{};
+  uint3 bricks{};
+  uint32_t nb = 0;
+  // Per-brick energy summary of a scalar set at the reference's flag sample
+  // points: bit 0 = some sample above the activity threshold, bit 1 = dilate.
+  uint8_t* summary_cur = nullptr;   // summary of the current set (after injection)
+  uint8_t* summary_next = nullptr;  // summary of the advected set
+  // Bricks whose voxels may be non-zero in the advected scratch set (T) and in
+  // the current set (S).
+  uint8_t* maybe_nz_t = nullptr;
+  uint8_t* maybe_nz_s = nullptr;
+  // Compacted brick lists and their counts.
+  uint32_t* list_adv = nullptr;   // bricks the scalar advection kernel visits
+  uint32_t* list_next = nullptr;  // bricks the combustion/buoyancy kernels visit
+  uint32_t* list_inj = nullptr;   // bricks the injection kernel visits (host-filled)
+  uint32_t* counters = nullptr;   // [0] adv count, [1] next count, [2] scratch
+  uint32_t* host_list_inj = nullptr;  // pinned staging for list_inj
+  uint32_t inj_count = 0;
+  cudaEvent_t inj_event = nullptr;
+  // CUDA graph cache of the step.
+  cudaGraphExec_t graph = nullptr;
+  uint64_t graph_key = ~0ull;
+  bool graph_ok = true;
+  bool valid = false;  // false: maybe-non-zero masks must be rebuilt
+};
+
+struct FusedStep {
+  cudaStream_t stream;
+  Dims dm;
+  uint3 bricks;
+  const Params* params;
+  Params host_params;
+  const float* sources;
+  uint32_t nsrc;
+  const float* host_sources;  // packed sources (NULL when none)
+  uint32_t host_nsrc;
+  int advect_mode;
+  ScalarSet cur, next, scratch;
+  uint32_t *flags_cur, *flags_next;
+  VelField vcur, vscr, vscr2, vort;
+  float *vort_mag, *conf_mag, *vel_mag;
+  LevelBuf lv[3];
+  int q[7];
+  bool vort_on, pressure_on, debug_on, debug_fields;
+  int last_p;
+};
+
+struct FusedResult {
+  int last_p = 0;
+  bool final_vscr_is_2 = false;
+  uint32_t launches = 0;
+  std::string error;
+};
+
+size_t fused_work_bytes(Dims dm, uint3 bricks);
+void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks);
+fx_status fused_init(FusedWork& w, cudaStream_t s);
+fx_status fused_reset(FusedWork& w, cudaStream_t s);
+fx_status fused_invalidate(FusedWork& w, cudaStream_t s);
+void fused_release(FusedWork& w);
+fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out);
+fx_status fused_count_active(FusedWork& w, cudaStream_t s, const uint32_t* flags, uint32_t nb, uint32_t* out);
+
+// Adds the active bricks of `flags` and their voxel count to acc[0] and acc[1].
+cudaError_t fused_accumulate_active(cudaStream_t s, Dims dm, uint3 bricks, const uint32_t* flags, unsigned long long* acc);
+
+// Kernel timing of the fused path (events recorded inside its graphs).
+void fused_set_timing(FusedWork& w, bool on);
+void fused_drain_timing(FusedWork& w, const std::function<void(const char*, uint32_t, double)>& sink);
+
+}  // namespace fx

@@ -1,0 +1,50 @@
+// Host-side declarations of the kernel launchers used by the simulation object.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "fx_math.cuh"
+
+namespace fx {
+
+struct ScalarSet {
+  float* f[4];  // density, temperature, fuel, reaction
+};
+
+struct VelField {
+  float* c[3];  // x, y, z planes
+};
+
+struct LevelBuf {
+  Dims dm;
+  float* div;
+  float* p[2];  // pressureA, pressureB
+};
+
+// ---------------------------------------------------------------- plain path
+// One launcher per reference WGSL pass (shaders/passes/*.wgsl.ts).
+void plain_inject_scalar(cudaStream_t s, Dims dm, const Params* P, const float* src, uint32_t nsrc, ScalarSet set);
+void plain_inject_velocity(cudaStream_t s, Dims dm, const Params* P, const float* src, uint32_t nsrc, VelField v);
+void plain_inject_igniter(cudaStream_t s, Dims dm, const Params* P, const float* src, uint32_t nsrc, ScalarSet set);
+void plain_active_bricks(cudaStream_t s, Dims dm, uint3 bricks, ScalarSet set, uint32_t* flags);
+void plain_advect_velocity(cudaStream_t s, Dims dm, const Params* P, VelField src, VelField dst);
+void plain_advect_scalars(cudaStream_t s, Dims dm, uint3 bricks, const Params* P, int mode, ScalarSet src, VelField vel,
+                          const uint32_t* flags, ScalarSet dst);
+void plain_combustion(cudaStream_t s, Dims dm, uint3 bricks, const Params* P, ScalarSet snapshot, const uint32_t* flags,
+                      ScalarSet dst);
+void plain_buoyancy(cudaStream_t s, Dims dm, uint3 bricks, const Params* P, ScalarSet set, const uint32_t* flags, VelField v);
+void plain_vorticity(cudaStream_t s, Dims dm, VelField v, VelField w, float* wmag);
+void plain_confinement(cudaStream_t s, Dims dm, const Params* P, VelField w, const float* wmag, ScalarSet set, VelField v,
+                       float* fmag);
+void plain_divergence(cudaStream_t s, Dims dm, VelField v, float* div);
+void plain_jacobi(cudaStream_t s, Dims dm, const float* div, const float* src, float* dst);
+void plain_restrict(cudaStream_t s, Dims fine, Dims coarse, const float* src, float* dst);
+void plain_prolong(cudaStream_t s, Dims coarse, Dims fine, const float* coarse_p, float* fine_pa);
+void plain_project(cudaStream_t s, Dims dm, VelField vsrc, const float* p, VelField vdst);
+void plain_velocity_magnitude(cudaStream_t s, Dims dm, VelField v, float* out);
+
+// Pinned sin/cos over an array (tests compare it with the oracle bit for bit).
+void pinned_sincos_array(cudaStream_t s, const float* x, float* out, uint32_t n, int cosine);
+
+}  // namespace fx

@@ -1,0 +1,918 @@
+// The simulation object behind the C ABI of include/fenix_cuda.h: buffer
+// ownership, the reference's per-step schedule
+// (runtime/createCombustionVolumeSimulation.ts:230-305), its parameter and
+// quality handling, and the multilevel pressure schedule
+// (runtime/passes/PressureSolvePass.ts:62-158).
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/fenix_cuda.h"
+#include "fx_fused.h"
+#include "fx_kernels.h"
+
+using namespace fx;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+constexpr int kParamSlots = 32;
+
+// Per-kernel CUDA-event timing on the simulation's stream (FX_INSTR_KERNEL_TIMES).
+struct KernelTimer {
+  bool on = false;
+  struct Pending {
+    const char* name;
+    cudaEvent_t a, b;
+  };
+  std::vector<cudaEvent_t> pool;
+  std::vector<Pending> pending;
+  std::map<std::string, std::pair<uint32_t, double>> acc;
+  const char* open_name = nullptr;
+  cudaEvent_t open_a = nullptr;
+
+  cudaEvent_t take() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void begin(cudaStream_t s, const char* name) {
+    if (!on) return;
+    open_name = name;
+    open_a = take();
+    cudaEventRecord(open_a, s);
+  }
+  void end(cudaStream_t s) {
+    if (!on || !open_name) return;
+    cudaEvent_t b = take();
+    cudaEventRecord(b, s);
+    pending.push_back({open_name, open_a, b});
+    open_name = nullptr;
+  }
+  void drain() {
+    for (auto& p : pending) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, p.a, p.b);
+      auto& e = acc[p.name];
+      e.first += 1;
+      e.second += ms;
+      pool.push_back(p.a);
+      pool.push_back(p.b);
+    }
+    pending.clear();
+  }
+  void release() {
+    drain();
+    for (auto e : pool) cudaEventDestroy(e);
+    pool.clear();
+  }
+};
+
+}  // namespace
+
+struct fx_sim {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  Dims dm{};
+  uint32_t n = 0;
+  uint3 bricks{};
+  uint32_t nb = 0;
+  int kernels = FX_KERNELS_FUSED;
+  uint32_t opt_flags = 0;
+
+  // device memory
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+  ScalarSet sets[3]{};  // [0], [1]: the reference's two sets; [2]: scratch (snapshot / advected)
+  VelField vcur{}, vscr{}, vscr2{}, vort{};
+  float* vort_mag = nullptr;
+  float* conf_mag = nullptr;
+  float* vel_mag = nullptr;
+  uint32_t* flags[2]{};
+  LevelBuf lv[3]{};
+  Params* d_params = nullptr;
+  FusedWork fw{};
+
+  // sources
+  float* d_sources = nullptr;
+  uint32_t src_cap = 0;   // in sources
+  uint32_t src_count = 0; // as given (0 -> one zero "phantom" source on device)
+  float* h_src_stage = nullptr;
+  uint32_t h_src_cap = 0;
+  cudaEvent_t src_event = nullptr;
+  std::vector<float> host_sources;  // packed copy, used for the injection bounds
+
+  // pinned parameter ring
+  Params* h_params = nullptr;
+  cudaEvent_t param_events[kParamSlots]{};
+  uint64_t param_counter = 0;
+
+  // reference host state (createCombustionVolumeSimulation.ts:180-204)
+  int cur = 0;
+  int64_t step_index = 0;
+  bool initialized = false;
+  double start_s = 0, last_elapsed_s = 0;
+  int last_p = 0;
+  bool debug_requested = false;
+  int advect_mode = FX_ADVECT_MACCORMACK;
+  fx_quality quality{};
+  int qi[7]{};  // clamped integers of `quality`
+  fx_runtime_params rp{};
+  uint32_t last_kernel_count = 0;
+  uint32_t instr = 0;
+  KernelTimer timer;
+  unsigned long long* d_active_acc = nullptr;  // [0] brick-steps, [1] voxel-steps
+  // In the fused path the final velocity of the step may live in vscr2.
+  VelField* final_vscr = nullptr;
+
+  std::string err;
+};
+
+namespace {
+
+fx_status fail(fx_sim* s, fx_status code, const std::string& msg) {
+  if (s) {
+    if (s->err.empty()) s->err = msg;
+  } else {
+    g_last_error = msg;
+  }
+  return code;
+}
+
+#define FX_CUDA(sim, call)                                                                  \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail((sim), e_ == cudaErrorMemoryAllocation ? FX_ERR_OUT_OF_MEMORY : FX_ERR_CUDA, \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                      \
+  } while (0)
+
+// clampInteger of types.ts:26-28 with JavaScript Math.round (half toward +inf).
+double js_round(double v) {
+  const double f = std::floor(v);
+  return (v - f >= 0.5) ? f + 1.0 : f;
+}
+int clamp_integer(double v, int lo, int hi) { return (int)std::max<double>(lo, std::min<double>(hi, js_round(v))); }
+
+void apply_quality_clamps(fx_sim* s) {
+  const fx_quality& q = s->quality;
+  s->qi[0] = clamp_integer(q.pressure_interval, 1, 16);
+  s->qi[1] = clamp_integer(q.vorticity_interval, 1, 16);
+  s->qi[2] = clamp_integer(q.fine_pre_iterations, 0, 32);
+  s->qi[3] = clamp_integer(q.fine_post_iterations, 0, 32);
+  s->qi[4] = clamp_integer(q.mid_pre_iterations, 0, 32);
+  s->qi[5] = clamp_integer(q.mid_post_iterations, 0, 32);
+  s->qi[6] = clamp_integer(q.coarse_iterations, 0, 64);
+  // Store the clamped values back, as createSimulationQualitySettings returns them.
+  s->quality.pressure_interval = s->qi[0];
+  s->quality.vorticity_interval = s->qi[1];
+  s->quality.fine_pre_iterations = s->qi[2];
+  s->quality.fine_post_iterations = s->qi[3];
+  s->quality.mid_pre_iterations = s->qi[4];
+  s->quality.mid_post_iterations = s->qi[5];
+  s->quality.coarse_iterations = s->qi[6];
+}
+
+bool merge_quality(fx_quality& dst, const fx_quality& src, uint32_t mask) {
+  const double* sv = &src.pressure_interval;
+  double* dv = &dst.pressure_interval;
+  for (int k = 0; k < 7; ++k)
+    if (mask & (1u << k)) {
+      if (std::isnan(sv[k])) return false;
+      dv[k] = sv[k];
+    }
+  return true;
+}
+
+void merge_params(fx_runtime_params& d, const fx_runtime_params& s, uint32_t m) {
+  if (m & FX_PARAM_WIND) std::memcpy(d.wind, s.wind, sizeof d.wind);
+  if (m & FX_PARAM_WIND_STRENGTH) d.wind_strength = s.wind_strength;
+  if (m & FX_PARAM_GRAVITY) std::memcpy(d.gravity, s.gravity, sizeof d.gravity);
+  if (m & FX_PARAM_GRAVITY_STRENGTH) d.gravity_strength = s.gravity_strength;
+  if (m & FX_PARAM_BUOYANCY) d.buoyancy = s.buoyancy;
+  if (m & FX_PARAM_VORTICITY_STRENGTH) d.vorticity_strength = s.vorticity_strength;
+  if (m & FX_PARAM_VORTICITY_CONSTANT_MASK) d.vorticity_constant_mask = s.vorticity_constant_mask;
+  if (m & FX_PARAM_VORTICITY_VELOCITY_MASK) d.vorticity_velocity_mask = s.vorticity_velocity_mask;
+  if (m & FX_PARAM_VORTICITY_HEAT_MASK) d.vorticity_heat_mask = s.vorticity_heat_mask;
+  if (m & FX_PARAM_VORTICITY_DENSITY_MASK) d.vorticity_density_mask = s.vorticity_density_mask;
+  if (m & FX_PARAM_WORLD_SIZE) d.world_size = s.world_size;
+}
+
+Dims halve(Dims a) {
+  return Dims{std::max<uint32_t>(4, a.w / 2), std::max<uint32_t>(4, a.h / 2), std::max<uint32_t>(4, a.d / 2)};
+}
+
+size_t count_of(Dims d) { return (size_t)d.w * d.h * d.d; }
+
+fx_status zero_state(fx_sim* s) {
+  // doReset (createCombustionVolumeSimulation.ts:213-225) clears everything the
+  // step reads; clearing the whole arena is a superset.
+  FX_CUDA(s, cudaMemsetAsync(s->arena, 0, s->arena_bytes, s->stream));
+  return FX_OK;
+}
+
+fx_status upload_sources(fx_sim* s) {
+  // SourceInjectionPass.ts:13-23,71-83: a buffer of max(bytes, 128); with no
+  // sources the kernels see one all-zero entry.
+  const uint32_t dev_count = std::max<uint32_t>(s->src_count, 1);
+  if (dev_count > s->src_cap) {
+    FX_CUDA(s, cudaStreamSynchronize(s->stream));
+    if (s->d_sources) FX_CUDA(s, cudaFree(s->d_sources));
+    s->d_sources = nullptr;
+    const uint32_t cap = std::max<uint32_t>(dev_count, 2 * s->src_cap);
+    FX_CUDA(s, cudaMalloc(&s->d_sources, (size_t)cap * 32 * sizeof(float)));
+    s->src_cap = cap;
+  }
+  if (dev_count > s->h_src_cap) {
+    FX_CUDA(s, cudaEventSynchronize(s->src_event));
+    if (s->h_src_stage) FX_CUDA(s, cudaFreeHost(s->h_src_stage));
+    s->h_src_stage = nullptr;
+    FX_CUDA(s, cudaMallocHost(&s->h_src_stage, (size_t)dev_count * 32 * sizeof(float)));
+    s->h_src_cap = dev_count;
+  }
+  FX_CUDA(s, cudaEventSynchronize(s->src_event));
+  if (s->src_count == 0) std::memset(s->h_src_stage, 0, 32 * sizeof(float));
+  else std::memcpy(s->h_src_stage, s->host_sources.data(), (size_t)s->src_count * 32 * sizeof(float));
+  FX_CUDA(s, cudaMemcpyAsync(s->d_sources, s->h_src_stage, (size_t)dev_count * 32 * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  FX_CUDA(s, cudaEventRecord(s->src_event, s->stream));
+  return FX_OK;
+}
+
+// Fills the 80-byte uniform exactly as createCombustionVolumeSimulation.ts:237-266
+// does: doubles computed on the host, then rounded to f32.
+Params make_params(const fx_sim* s, double elapsed, double step_s) {
+  const double effective = std::min(step_s, 1.0 / 15.0);
+  const double local_time = elapsed - s->start_s;
+  const double prev_local = s->last_elapsed_s - s->start_s;
+  const double dx = s->rp.world_size / (double)std::max(s->dm.w, s->dm.d);
+  Params P;
+  P.time = (float)local_time;
+  P.dt = (float)effective;
+  P.prev_time = (float)prev_local;
+  P.scalar_set = (float)s->cur;
+  for (int k = 0; k < 3; ++k) P.wind[k] = (float)s->rp.wind[k];
+  P.wind[3] = (float)s->rp.wind_strength;
+  for (int k = 0; k < 3; ++k) P.gravity[k] = (float)s->rp.gravity[k];
+  P.gravity[3] = (float)s->rp.gravity_strength;
+  P.buoyancy = (float)s->rp.buoyancy;
+  P.vorticity_strength = (float)s->rp.vorticity_strength;
+  P.dx = (float)dx;
+  P.world_size = (float)s->rp.world_size;
+  P.vmask[0] = (float)s->rp.vorticity_constant_mask;
+  P.vmask[1] = (float)s->rp.vorticity_velocity_mask;
+  P.vmask[2] = (float)s->rp.vorticity_heat_mask;
+  P.vmask[3] = (float)s->rp.vorticity_density_mask;
+  return P;
+}
+
+// PressureSolvePass.smooth (:129-143) for the plain path.
+int plain_smooth(fx_sim* s, LevelBuf& L, int iters, int start, uint32_t& launches, const char* name) {
+  int active = start;
+  for (int k = 0; k < iters; ++k) {
+    s->timer.begin(s->stream, name);
+    plain_jacobi(s->stream, L.dm, L.div, L.p[active], L.p[active ^ 1]);
+    s->timer.end(s->stream);
+    active ^= 1;
+    ++launches;
+  }
+  return active;
+}
+
+#define FX_TIMED(sim, name, call)            \
+  do {                                       \
+    (sim)->timer.begin((sim)->stream, name); \
+    call;                                    \
+    (sim)->timer.end((sim)->stream);         \
+  } while (0)
+
+// The plain FP32 step: one kernel per reference dispatch, in the reference order.
+fx_status step_plain(fx_sim* s, bool vort_on, bool pressure_on, bool debug_on) {
+  cudaStream_t st = s->stream;
+  const int cur = s->cur, next = cur ^ 1;
+  const uint32_t nsrc = std::max<uint32_t>(s->src_count, 1);
+  uint32_t launches = 0;
+  FX_TIMED(s, "plain_inject_scalar", plain_inject_scalar(st, s->dm, s->d_params, s->d_sources, nsrc, s->sets[cur]));
+  FX_TIMED(s, "plain_inject_velocity", plain_inject_velocity(st, s->dm, s->d_params, s->d_sources, nsrc, s->vcur));
+  FX_TIMED(s, "plain_inject_igniter", plain_inject_igniter(st, s->dm, s->d_params, s->d_sources, nsrc, s->sets[cur]));
+  FX_CUDA(s, cudaMemsetAsync(s->flags[cur], 0, s->nb * sizeof(uint32_t), st));
+  FX_TIMED(s, "plain_active_bricks", plain_active_bricks(st, s->dm, s->bricks, s->sets[cur], s->flags[cur]));
+  FX_TIMED(s, "plain_advect_velocity", plain_advect_velocity(st, s->dm, s->d_params, s->vcur, s->vscr));
+  FX_TIMED(s, "plain_advect_scalars", plain_advect_scalars(st, s->dm, s->bricks, s->d_params, s->advect_mode, s->sets[cur], s->vscr, s->flags[cur], s->sets[next]));
+  FX_CUDA(s, cudaMemsetAsync(s->flags[next], 0, s->nb * sizeof(uint32_t), st));
+  FX_TIMED(s, "plain_active_bricks", plain_active_bricks(st, s->dm, s->bricks, s->sets[next], s->flags[next]));
+  launches += 7;
+  // Combustion reads a snapshot of the set so that every neighbour read sees the
+  // state before the pass (see the note at plain k_combustion).
+  for (int f = 0; f < 4; ++f)
+    FX_CUDA(s, cudaMemcpyAsync(s->sets[2].f[f], s->sets[next].f[f], (size_t)s->n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  FX_TIMED(s, "plain_combustion", plain_combustion(st, s->dm, s->bricks, s->d_params, s->sets[2], s->flags[next], s->sets[next]));
+  FX_TIMED(s, "plain_buoyancy", plain_buoyancy(st, s->dm, s->bricks, s->d_params, s->sets[next], s->flags[next], s->vscr));
+  launches += 2;
+  if (vort_on) {
+    FX_TIMED(s, "plain_vorticity", plain_vorticity(st, s->dm, s->vscr, s->vort, s->vort_mag));
+    FX_TIMED(s, "plain_confinement", plain_confinement(st, s->dm, s->d_params, s->vort, s->vort_mag, s->sets[next], s->vscr, s->conf_mag));
+    launches += 2;
+  }
+  if (pressure_on) {
+    for (auto& L : s->lv) FX_CUDA(s, cudaMemsetAsync(L.p[0], 0, count_of(L.dm) * sizeof(float), st));
+    FX_TIMED(s, "plain_divergence", plain_divergence(st, s->dm, s->vscr, s->lv[0].div));
+    ++launches;
+    const int* q = s->qi;
+    const int fine_pre = plain_smooth(s, s->lv[0], q[2], 0, launches, "plain_jacobi_fine");
+    FX_TIMED(s, "plain_restrict", plain_restrict(st, s->lv[0].dm, s->lv[1].dm, s->lv[0].div, s->lv[1].div));
+    const int mid_pre = plain_smooth(s, s->lv[1], q[4], 0, launches, "plain_jacobi_mid");
+    FX_TIMED(s, "plain_restrict", plain_restrict(st, s->lv[1].dm, s->lv[2].dm, s->lv[1].div, s->lv[2].div));
+    const int coarse = plain_smooth(s, s->lv[2], q[6], 0, launches, "plain_jacobi_coarse");
+    FX_TIMED(s, "plain_prolong", plain_prolong(st, s->lv[2].dm, s->lv[1].dm, s->lv[2].p[coarse], s->lv[1].p[0]));
+    const int mid = plain_smooth(s, s->lv[1], q[5], mid_pre, launches, "plain_jacobi_mid");
+    FX_TIMED(s, "plain_prolong", plain_prolong(st, s->lv[1].dm, s->lv[0].dm, s->lv[1].p[mid], s->lv[0].p[0]));
+    s->last_p = plain_smooth(s, s->lv[0], q[3], fine_pre, launches, "plain_jacobi_fine");
+    launches += 4;
+  }
+  FX_TIMED(s, "plain_project", plain_project(st, s->dm, s->vscr, s->lv[0].p[s->last_p], s->vcur));
+  ++launches;
+  if (debug_on) {
+    FX_TIMED(s, "plain_velocity_magnitude", plain_velocity_magnitude(st, s->dm, s->vcur, s->vel_mag));
+    ++launches;
+  }
+  s->final_vscr = &s->vscr;
+  s->last_kernel_count = launches;
+  FX_CUDA(s, cudaGetLastError());
+  return FX_OK;
+}
+
+// Pointer of a field for read/write, with its element count and element size.
+bool field_ref(fx_sim* s, int id, void** ptr, size_t* count) {
+  const int prev = s->cur ^ 1;
+  *count = s->n;
+  switch (id) {
+    case FX_FIELD_DENSITY: case FX_FIELD_TEMPERATURE: case FX_FIELD_FUEL: case FX_FIELD_REACTION:
+      *ptr = s->sets[s->cur].f[id - FX_FIELD_DENSITY]; return true;
+    case FX_FIELD_PREV_DENSITY: case FX_FIELD_PREV_TEMPERATURE: case FX_FIELD_PREV_FUEL: case FX_FIELD_PREV_REACTION:
+      *ptr = s->sets[prev].f[id - FX_FIELD_PREV_DENSITY]; return true;
+    case FX_FIELD_VELOCITY_X: case FX_FIELD_VELOCITY_Y: case FX_FIELD_VELOCITY_Z:
+      *ptr = s->vcur.c[id - FX_FIELD_VELOCITY_X]; return true;
+    case FX_FIELD_VELOCITY_SCRATCH_X: case FX_FIELD_VELOCITY_SCRATCH_Y: case FX_FIELD_VELOCITY_SCRATCH_Z:
+      *ptr = s->final_vscr->c[id - FX_FIELD_VELOCITY_SCRATCH_X]; return true;
+    case FX_FIELD_VORTICITY_X: case FX_FIELD_VORTICITY_Y: case FX_FIELD_VORTICITY_Z:
+      *ptr = s->vort.c[id - FX_FIELD_VORTICITY_X]; return true;
+    case FX_FIELD_VORTICITY_MAGNITUDE: *ptr = s->vort_mag; return true;
+    case FX_FIELD_CONFINEMENT_MAGNITUDE: *ptr = s->conf_mag; return true;
+    case FX_FIELD_VELOCITY_MAGNITUDE: *ptr = s->vel_mag; return true;
+    case FX_FIELD_BRICK_FLAGS: *ptr = s->flags[s->cur]; *count = s->nb; return true;
+    case FX_FIELD_PREV_BRICK_FLAGS: *ptr = s->flags[prev]; *count = s->nb; return true;
+    case FX_FIELD_FINE_DIVERGENCE: case FX_FIELD_FINE_PRESSURE_A: case FX_FIELD_FINE_PRESSURE_B:
+    case FX_FIELD_MID_DIVERGENCE: case FX_FIELD_MID_PRESSURE_A: case FX_FIELD_MID_PRESSURE_B:
+    case FX_FIELD_COARSE_DIVERGENCE: case FX_FIELD_COARSE_PRESSURE_A: case FX_FIELD_COARSE_PRESSURE_B: {
+      const int l = (id - FX_FIELD_FINE_DIVERGENCE) / 3, k = (id - FX_FIELD_FINE_DIVERGENCE) % 3;
+      *count = count_of(s->lv[l].dm);
+      *ptr = k == 0 ? s->lv[l].div : s->lv[l].p[k - 1];
+      return true;
+    }
+    case FX_FIELD_PRESSURE: *ptr = s->lv[0].p[s->last_p]; return true;
+    default: return false;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t fx_abi_version(void) { return FX_ABI_VERSION; }
+
+const char* fx_last_error(void) { return g_last_error.c_str(); }
+
+void fx_sim_options_default(fx_sim_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->struct_size = sizeof *o;
+  o->width = 128;
+  o->height = 256;
+  o->depth = 128;
+  o->scalar_advection_mode = FX_ADVECT_MACCORMACK;
+  o->runtime_mask = 0;
+  o->runtime.gravity[1] = -1.0;
+  o->runtime.gravity_strength = 0.45;
+  o->runtime.buoyancy = 3.6;
+  o->runtime.vorticity_strength = 2.15;
+  o->runtime.vorticity_constant_mask = 1.0;
+  o->runtime.vorticity_velocity_mask = 0.4;
+  o->runtime.vorticity_heat_mask = 0.8;
+  o->runtime.vorticity_density_mask = 0.35;
+  o->runtime.world_size = 10.0;
+  o->quality_mask = 0;
+  o->quality.pressure_interval = 1;
+  o->quality.vorticity_interval = 1;
+  o->quality.fine_pre_iterations = 2;
+  o->quality.fine_post_iterations = 3;
+  o->quality.mid_pre_iterations = 2;
+  o->quality.mid_post_iterations = 3;
+  o->quality.coarse_iterations = 10;
+  o->device = 0;
+  o->kernels = FX_KERNELS_PLAIN;
+  o->flags = 0;
+  o->stream = nullptr;
+}
+
+fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
+  g_last_error.clear();
+  if (!out) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_create: out is NULL");
+  *out = nullptr;
+  fx_sim_options opt;
+  fx_sim_options_default(&opt);
+  if (opt_in) {
+    if (opt_in->struct_size != sizeof(fx_sim_options))
+      return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_create: struct_size does not match this library's fx_sim_options");
+    opt = *opt_in;
+  }
+  uint32_t w = opt.width ? opt.width : 128, h = opt.height ? opt.height : 256, d = opt.depth ? opt.depth : 128;
+  if (w < 2 || h < 2 || d < 2) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_create: every dimension must be >= 2");
+  if ((double)w * h * d >= 4294967296.0) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_create: grid must hold fewer than 2^32 voxels");
+  if (opt.scalar_advection_mode != FX_ADVECT_SEMI_LAGRANGIAN && opt.scalar_advection_mode != FX_ADVECT_MACCORMACK)
+    return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_create: unknown scalar_advection_mode");
+  if (opt.kernels != FX_KERNELS_FUSED && opt.kernels != FX_KERNELS_PLAIN)
+    return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_create: unknown kernels path");
+
+  fx_sim* s = new (std::nothrow) fx_sim;
+  if (!s) return fail(nullptr, FX_ERR_OUT_OF_MEMORY, "fx_sim_create: host allocation failed");
+  auto bail = [&](fx_status code) {
+    g_last_error = s->err;
+    fx_sim_destroy(s);
+    return code;
+  };
+  s->device = opt.device;
+  s->kernels = opt.kernels;
+  s->opt_flags = opt.flags;
+  s->dm = Dims{w, h, d};
+  s->n = w * h * d;
+  s->bricks = make_uint3((w + 7) / 8, (h + 7) / 8, (d + 7) / 8);
+  s->nb = s->bricks.x * s->bricks.y * s->bricks.z;
+  s->advect_mode = opt.scalar_advection_mode;
+  fx_sim_options defaults;
+  fx_sim_options_default(&defaults);
+  s->rp = defaults.runtime;
+  merge_params(s->rp, opt.runtime, opt.runtime_mask);
+  s->quality = defaults.quality;
+  if (!merge_quality(s->quality, opt.quality, opt.quality_mask)) {
+    s->err = "fx_sim_create: NaN quality setting";
+    return bail(FX_ERR_INVALID_ARGUMENT);
+  }
+  apply_quality_clamps(s);
+
+  fx_status st;
+  if (cudaSetDevice(s->device) != cudaSuccess) {
+    s->err = "fx_sim_create: cudaSetDevice failed (no CUDA device?)";
+    return bail(FX_ERR_CUDA);
+  }
+  if (opt.stream) {
+    s->stream = (cudaStream_t)opt.stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      s->err = "fx_sim_create: cudaStreamCreate failed";
+      return bail(FX_ERR_CUDA);
+    }
+    s->own_stream = true;
+  }
+  s->lv[0].dm = s->dm;
+  s->lv[1].dm = halve(s->lv[0].dm);
+  s->lv[2].dm = halve(s->lv[1].dm);
+
+  // One arena; every buffer starts on a 256-byte boundary.
+  const size_t n = s->n;
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    const size_t o = off;
+    off += (bytes + 255) & ~(size_t)255;
+    return o;
+  };
+  size_t o_sets[3][4], o_vcur[3], o_vscr[3], o_vscr2[3], o_vort[3], o_wmag, o_fmag, o_vmag, o_flags[2], o_lv[3][3], o_params;
+  for (auto& set : o_sets)
+    for (auto& f : set) f = carve(n * 4);
+  for (int c = 0; c < 3; ++c) {
+    o_vcur[c] = carve(n * 4);
+    o_vscr[c] = carve(n * 4);
+    o_vscr2[c] = carve(n * 4);
+    o_vort[c] = carve(n * 4);
+  }
+  o_wmag = carve(n * 4);
+  o_fmag = carve(n * 4);
+  o_vmag = carve(n * 4);
+  o_flags[0] = carve((size_t)s->nb * 4);
+  o_flags[1] = carve((size_t)s->nb * 4);
+  for (int l = 0; l < 3; ++l)
+    for (int k = 0; k < 3; ++k) o_lv[l][k] = carve(count_of(s->lv[l].dm) * 4);
+  o_params = carve(sizeof(Params));
+  const size_t o_acc = carve(2 * sizeof(unsigned long long));
+  const size_t o_fused = off;
+  off += fused_work_bytes(s->dm, s->bricks);
+  s->arena_bytes = off;
+  {
+    cudaError_t e = cudaMalloc(&s->arena, s->arena_bytes);
+    if (e != cudaSuccess) {
+      s->err = std::string("fx_sim_create: cudaMalloc of the field arena failed: ") + cudaGetErrorString(e);
+      return bail(e == cudaErrorMemoryAllocation ? FX_ERR_OUT_OF_MEMORY : FX_ERR_CUDA);
+    }
+  }
+  char* base = (char*)s->arena;
+  for (int k = 0; k < 3; ++k)
+    for (int f = 0; f < 4; ++f) s->sets[k].f[f] = (float*)(base + o_sets[k][f]);
+  for (int c = 0; c < 3; ++c) {
+    s->vcur.c[c] = (float*)(base + o_vcur[c]);
+    s->vscr.c[c] = (float*)(base + o_vscr[c]);
+    s->vscr2.c[c] = (float*)(base + o_vscr2[c]);
+    s->vort.c[c] = (float*)(base + o_vort[c]);
+  }
+  s->vort_mag = (float*)(base + o_wmag);
+  s->conf_mag = (float*)(base + o_fmag);
+  s->vel_mag = (float*)(base + o_vmag);
+  s->flags[0] = (uint32_t*)(base + o_flags[0]);
+  s->flags[1] = (uint32_t*)(base + o_flags[1]);
+  for (int l = 0; l < 3; ++l) {
+    s->lv[l].div = (float*)(base + o_lv[l][0]);
+    s->lv[l].p[0] = (float*)(base + o_lv[l][1]);
+    s->lv[l].p[1] = (float*)(base + o_lv[l][2]);
+  }
+  s->d_params = (Params*)(base + o_params);
+  s->d_active_acc = (unsigned long long*)(base + o_acc);
+  fused_work_carve(s->fw, base + o_fused, s->dm, s->bricks);
+  s->final_vscr = &s->vscr;
+
+  if (cudaMallocHost(&s->h_params, kParamSlots * sizeof(Params)) != cudaSuccess) {
+    s->err = "fx_sim_create: cudaMallocHost failed";
+    return bail(FX_ERR_OUT_OF_MEMORY);
+  }
+  for (auto& ev : s->param_events)
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+      s->err = "fx_sim_create: cudaEventCreate failed";
+      return bail(FX_ERR_CUDA);
+    }
+  if (cudaEventCreateWithFlags(&s->src_event, cudaEventDisableTiming) != cudaSuccess) {
+    s->err = "fx_sim_create: cudaEventCreate failed";
+    return bail(FX_ERR_CUDA);
+  }
+  if ((st = zero_state(s)) != FX_OK) return bail(st);
+  if ((st = upload_sources(s)) != FX_OK) return bail(st);
+  if ((st = fused_init(s->fw, s->stream)) != FX_OK) {
+    s->err = "fx_sim_create: fused path initialisation failed";
+    return bail(st);
+  }
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
+    s->err = "fx_sim_create: initial clear failed";
+    return bail(FX_ERR_CUDA);
+  }
+  *out = s;
+  return FX_OK;
+}
+
+void fx_sim_destroy(fx_sim* s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  fused_release(s->fw);
+  s->timer.release();
+  if (s->arena) cudaFree(s->arena);
+  if (s->d_sources) cudaFree(s->d_sources);
+  if (s->h_src_stage) cudaFreeHost(s->h_src_stage);
+  if (s->h_params) cudaFreeHost(s->h_params);
+  for (auto& ev : s->param_events)
+    if (ev) cudaEventDestroy(ev);
+  if (s->src_event) cudaEventDestroy(s->src_event);
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+fx_status fx_sim_step(fx_sim* s, double elapsed, double step_s) {
+  if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_step: NULL handle");
+  if (!s->err.empty()) return FX_ERR_STATE;
+  FX_CUDA(s, cudaSetDevice(s->device));
+  if (!s->initialized) {
+    s->initialized = true;
+    s->start_s = elapsed;
+    s->last_elapsed_s = elapsed;
+  }
+  const Params P = make_params(s, elapsed, step_s);
+  const int slot = (int)(s->param_counter % kParamSlots);
+  FX_CUDA(s, cudaEventSynchronize(s->param_events[slot]));
+  s->h_params[slot] = P;
+  FX_CUDA(s, cudaMemcpyAsync(s->d_params, &s->h_params[slot], sizeof(Params), cudaMemcpyHostToDevice, s->stream));
+  FX_CUDA(s, cudaEventRecord(s->param_events[slot], s->stream));
+  ++s->param_counter;
+
+  const bool vort_on = s->step_index % s->qi[1] == 0;
+  const bool pressure_on = s->step_index % s->qi[0] == 0;
+  const bool debug_on = s->n < 1800000u || s->debug_requested;
+  fx_status st;
+  if (s->kernels == FX_KERNELS_PLAIN) {
+    st = step_plain(s, vort_on, pressure_on, debug_on);
+  } else {
+    FusedStep fs;
+    fs.stream = s->stream;
+    fs.dm = s->dm;
+    fs.bricks = s->bricks;
+    fs.params = s->d_params;
+    fs.host_params = P;
+    fs.sources = s->d_sources;
+    fs.nsrc = std::max<uint32_t>(s->src_count, 1);
+    fs.host_sources = s->src_count ? s->host_sources.data() : nullptr;
+    fs.host_nsrc = s->src_count;
+    fs.advect_mode = s->advect_mode;
+    fs.cur = s->sets[s->cur];
+    fs.next = s->sets[s->cur ^ 1];
+    fs.scratch = s->sets[2];
+    fs.flags_cur = s->flags[s->cur];
+    fs.flags_next = s->flags[s->cur ^ 1];
+    fs.vcur = s->vcur;
+    fs.vscr = s->vscr;
+    fs.vscr2 = s->vscr2;
+    fs.vort = s->vort;
+    fs.vort_mag = s->vort_mag;
+    fs.conf_mag = s->conf_mag;
+    fs.vel_mag = s->vel_mag;
+    for (int l = 0; l < 3; ++l) fs.lv[l] = s->lv[l];
+    for (int k = 0; k < 7; ++k) fs.q[k] = s->qi[k];
+    fs.vort_on = vort_on;
+    fs.pressure_on = pressure_on;
+    fs.debug_on = debug_on;
+    fs.debug_fields = (s->opt_flags & FX_OPT_DEBUG_FIELDS) != 0;
+    fs.last_p = s->last_p;
+    FusedResult fr;
+    st = fused_step(s->fw, fs, fr);
+    if (st == FX_OK) {
+      s->last_p = fr.last_p;
+      s->final_vscr = fr.final_vscr_is_2 ? &s->vscr2 : &s->vscr;
+      s->last_kernel_count = fr.launches;
+    } else {
+      fail(s, st, "fx_sim_step: fused step failed: " + fr.error);
+    }
+  }
+  if (st != FX_OK) return st;
+  if (s->instr & FX_INSTR_COUNT_ACTIVE) {
+    // flags of the step's advected set: the render flags once the step is done
+    FX_CUDA(s, fused_accumulate_active(s->stream, s->dm, s->bricks, s->flags[s->cur ^ 1], s->d_active_acc));
+    s->last_kernel_count += 1;
+  }
+  if (debug_on) s->debug_requested = false;
+  s->cur ^= 1;
+  s->last_elapsed_s = elapsed;
+  s->step_index += 1;
+  return FX_OK;
+}
+
+fx_status fx_sim_get_render_buffers(fx_sim* s, fx_render_buffers* o) {
+  if (!s || !o) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_render_buffers: NULL argument");
+  std::memset(o, 0, sizeof *o);
+  const ScalarSet& set = s->sets[s->cur];
+  o->density = (uint64_t)(uintptr_t)set.f[0];
+  o->temperature = (uint64_t)(uintptr_t)set.f[1];
+  o->fuel = (uint64_t)(uintptr_t)set.f[2];
+  o->reaction = (uint64_t)(uintptr_t)set.f[3];
+  o->active_brick_flags = (uint64_t)(uintptr_t)s->flags[s->cur];
+  o->active_brick_info[0] = s->bricks.x;
+  o->active_brick_info[1] = s->bricks.y;
+  o->active_brick_info[2] = s->bricks.z;
+  o->active_brick_info[3] = s->nb;
+  o->active_brick_info[4] = 8;
+  o->width = s->dm.w;
+  o->height = s->dm.h;
+  o->depth = s->dm.d;
+  o->dtype = FX_DTYPE_F32;
+  return FX_OK;
+}
+
+fx_status fx_sim_get_debug_buffers(fx_sim* s, fx_debug_buffers* o) {
+  if (!s || !o) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_debug_buffers: NULL argument");
+  fx_status st = fx_sim_get_render_buffers(s, &o->render);
+  if (st != FX_OK) return st;
+  s->debug_requested = true;
+  o->velocity_magnitude = (uint64_t)(uintptr_t)s->vel_mag;
+  o->divergence = (uint64_t)(uintptr_t)s->lv[0].div;
+  o->pressure = (uint64_t)(uintptr_t)s->lv[0].p[s->last_p];
+  o->vorticity_magnitude = (uint64_t)(uintptr_t)s->vort_mag;
+  o->confinement_force_magnitude = (uint64_t)(uintptr_t)s->conf_mag;
+  return FX_OK;
+}
+
+fx_status fx_sim_get_scalar_advection_mode(fx_sim* s, int32_t* mode) {
+  if (!s || !mode) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_scalar_advection_mode: NULL argument");
+  *mode = s->advect_mode;
+  return FX_OK;
+}
+
+fx_status fx_sim_set_scalar_advection_mode(fx_sim* s, int32_t mode) {
+  if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_scalar_advection_mode: NULL handle");
+  if (mode != FX_ADVECT_SEMI_LAGRANGIAN && mode != FX_ADVECT_MACCORMACK)
+    return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_scalar_advection_mode: unknown mode");
+  s->advect_mode = mode;
+  return FX_OK;
+}
+
+fx_status fx_sim_get_runtime_params(fx_sim* s, fx_runtime_params* o) {
+  if (!s || !o) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_runtime_params: NULL argument");
+  *o = s->rp;
+  return FX_OK;
+}
+
+fx_status fx_sim_set_runtime_params(fx_sim* s, const fx_runtime_params* p, uint32_t mask) {
+  if (!s || (!p && mask)) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_runtime_params: NULL argument");
+  if (mask & ~FX_PARAM_ALL) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_runtime_params: unknown mask bits");
+  if (p) merge_params(s->rp, *p, mask);
+  return FX_OK;
+}
+
+fx_status fx_sim_get_quality(fx_sim* s, fx_quality* o) {
+  if (!s || !o) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_quality: NULL argument");
+  *o = s->quality;
+  return FX_OK;
+}
+
+fx_status fx_sim_set_quality(fx_sim* s, const fx_quality* q, uint32_t mask) {
+  if (!s || (!q && mask)) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_quality: NULL argument");
+  if (mask & ~FX_QUALITY_ALL) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_quality: unknown mask bits");
+  fx_quality merged = s->quality;
+  if (q && !merge_quality(merged, *q, mask)) return FX_ERR_INVALID_ARGUMENT;
+  s->quality = merged;
+  apply_quality_clamps(s);
+  return FX_OK;
+}
+
+fx_status fx_sim_update_sources(fx_sim* s, const float* packed, uint32_t count) {
+  if (!s || (count && !packed)) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_update_sources: NULL argument");
+  if (!s->err.empty()) return FX_ERR_STATE;
+  FX_CUDA(s, cudaSetDevice(s->device));
+  s->host_sources.assign(packed, packed + (size_t)count * 32);
+  s->src_count = count;
+  return upload_sources(s);
+}
+
+fx_status fx_sim_reset(fx_sim* s) {
+  if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_reset: NULL handle");
+  if (!s->err.empty()) return FX_ERR_STATE;
+  FX_CUDA(s, cudaSetDevice(s->device));
+  // doReset(lastElapsedSeconds), createCombustionVolumeSimulation.ts:206-226,381-383
+  s->cur = 0;
+  s->step_index = 0;
+  s->last_p = 0;
+  s->initialized = false;
+  s->start_s = s->last_elapsed_s;
+  fx_status st = zero_state(s);
+  if (st != FX_OK) return st;
+  return fused_reset(s->fw, s->stream);
+}
+
+fx_status fx_sim_get_resolution(fx_sim* s, uint32_t* w, uint32_t* h, uint32_t* d) {
+  if (!s || !w || !h || !d) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_resolution: NULL argument");
+  *w = s->dm.w;
+  *h = s->dm.h;
+  *d = s->dm.d;
+  return FX_OK;
+}
+
+fx_status fx_sim_field_size(fx_sim* s, int32_t id, size_t* bytes) {
+  if (!s || !bytes) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_field_size: NULL argument");
+  void* p;
+  size_t count;
+  if (!field_ref(s, id, &p, &count)) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_field_size: unknown field id");
+  *bytes = count * 4;
+  return FX_OK;
+}
+
+fx_status fx_sim_read_field(fx_sim* s, int32_t id, void* dst, size_t bytes) {
+  if (!s || !dst) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_read_field: NULL argument");
+  void* p;
+  size_t count;
+  if (!field_ref(s, id, &p, &count)) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_read_field: unknown field id");
+  if (bytes != count * 4) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_read_field: byte count does not match the field");
+  FX_CUDA(s, cudaSetDevice(s->device));
+  FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  FX_CUDA(s, cudaMemcpy(dst, p, bytes, cudaMemcpyDeviceToHost));
+  return FX_OK;
+}
+
+fx_status fx_sim_write_field(fx_sim* s, int32_t id, const void* src, size_t bytes) {
+  if (!s || !src) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_write_field: NULL argument");
+  void* p;
+  size_t count;
+  if (!field_ref(s, id, &p, &count)) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_write_field: unknown field id");
+  if (bytes != count * 4) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_write_field: byte count does not match the field");
+  FX_CUDA(s, cudaSetDevice(s->device));
+  FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  FX_CUDA(s, cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice));
+  // A scratch velocity written here is what the next read returns.
+  return fused_invalidate(s->fw, s->stream);
+}
+
+fx_status fx_sim_synchronize(fx_sim* s) {
+  if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_synchronize: NULL handle");
+  FX_CUDA(s, cudaSetDevice(s->device));
+  FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  return FX_OK;
+}
+
+fx_status fx_sim_get_stats(fx_sim* s, fx_stats* o) {
+  if (!s || !o) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_stats: NULL argument");
+  std::memset(o, 0, sizeof *o);
+  o->step_index = s->step_index;
+  o->current_scalar_set = s->cur;
+  o->last_pressure_buffer = s->last_p;
+  o->brick_count = s->nb;
+  o->kernels_per_step = s->last_kernel_count;
+  FX_CUDA(s, cudaSetDevice(s->device));
+  uint32_t active = 0;
+  fx_status st = fused_count_active(s->fw, s->stream, s->flags[s->cur], s->nb, &active);
+  if (st != FX_OK) return fail(s, st, "fx_sim_get_stats: counting active bricks failed");
+  o->active_bricks = active;
+  return FX_OK;
+}
+
+fx_status fx_sim_set_instrumentation(fx_sim* s, uint32_t flags) {
+  if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_instrumentation: NULL handle");
+  if (flags & ~(FX_INSTR_KERNEL_TIMES | FX_INSTR_COUNT_ACTIVE))
+    return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_instrumentation: unknown flags");
+  s->instr = flags;
+  s->timer.on = (flags & FX_INSTR_KERNEL_TIMES) != 0;
+  fused_set_timing(s->fw, s->timer.on);
+  return FX_OK;
+}
+
+fx_status fx_sim_read_kernel_times(fx_sim* s, fx_kernel_time* out, uint32_t capacity, uint32_t* count) {
+  if (!s || !count || (capacity && !out)) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_read_kernel_times: NULL argument");
+  FX_CUDA(s, cudaSetDevice(s->device));
+  FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  s->timer.drain();
+  fused_drain_timing(s->fw, [&](const char* name, uint32_t launches, double ms) {
+    auto& e = s->timer.acc[name];
+    e.first += launches;
+    e.second += ms;
+  });
+  uint32_t k = 0;
+  for (auto& kv : s->timer.acc) {
+    if (k < capacity) {
+      std::memset(&out[k], 0, sizeof out[k]);
+      std::snprintf(out[k].name, sizeof out[k].name, "%s", kv.first.c_str());
+      out[k].launches = kv.second.first;
+      out[k].total_ms = kv.second.second;
+    }
+    ++k;
+  }
+  *count = k;
+  s->timer.acc.clear();
+  return FX_OK;
+}
+
+fx_status fx_sim_read_active_counters(fx_sim* s, uint64_t* brick_steps, uint64_t* voxel_steps) {
+  if (!s || !brick_steps || !voxel_steps) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_read_active_counters: NULL argument");
+  FX_CUDA(s, cudaSetDevice(s->device));
+  unsigned long long h[2] = {0, 0};
+  FX_CUDA(s, cudaMemcpyAsync(h, s->d_active_acc, sizeof h, cudaMemcpyDeviceToHost, s->stream));
+  FX_CUDA(s, cudaMemsetAsync(s->d_active_acc, 0, sizeof h, s->stream));
+  FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  *brick_steps = h[0];
+  *voxel_steps = h[1];
+  return FX_OK;
+}
+
+fx_status fx_sim_get_stream(fx_sim* s, void** stream) {
+  if (!s || !stream) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_stream: NULL argument");
+  *stream = (void*)s->stream;
+  return FX_OK;
+}
+
+const char* fx_sim_last_error(fx_sim* s) {
+  if (!s) return g_last_error.c_str();
+  return s->err.c_str();
+}
+
+// Test hook (declared in fenix_b200/csrc/fx_testing.h, not part of the public
+// ABI): evaluates the pinned sin/cos on the device.
+fx_status fx_test_pinned_sincos(const float* host_x, float* host_out, uint32_t n, int cosine) {
+  if (n == 0) return FX_OK;
+  float *dx = nullptr, *dout = nullptr;
+  if (cudaMalloc(&dx, n * sizeof(float)) != cudaSuccess) return FX_ERR_OUT_OF_MEMORY;
+  if (cudaMalloc(&dout, n * sizeof(float)) != cudaSuccess) {
+    cudaFree(dx);
+    return FX_ERR_OUT_OF_MEMORY;
+  }
+  fx_status st = FX_OK;
+  if (cudaMemcpy(dx, host_x, n * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) st = FX_ERR_CUDA;
+  if (st == FX_OK) {
+    pinned_sincos_array(0, dx, dout, n, cosine);
+    if (cudaMemcpy(host_out, dout, n * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) st = FX_ERR_CUDA;
+  }
+  cudaFree(dx);
+  cudaFree(dout);
+  return st;
+}
+
+}  // extern "C"

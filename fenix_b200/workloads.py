@@ -1,0 +1,186 @@
+"""Seeded synthetic plume workloads for the benchmark and the full-size tests.
+
+The reference publishes no benchmark and ships no scenes that run outside the
+browser, so these stand in for them. They are synthetic inputs with the shapes of
+the benchmark configurations:
+- `plume_256`: a 256^3 domain (32,768 bricks of 8^3) with four floor plumes.
+  Each plume is a scalar emitter, an upward velocity emitter and an igniter.
+  The emitters have radii of 8-14 voxels at seeded floor positions
+  x, z in [40, 216], y = 8 voxels. The step starts from a seeded synthetic
+  developed-plume state, so about 15-25 % of the bricks are active from the
+  first timed step.
+- `plume_64`: the 64^3 single-emitter case (voxel size 1/64).
+Solver settings for both: 4 fine/mid pre and post sweeps, 20 coarse sweeps;
+gravity strength 0.1, buoyancy 1.0, vorticity strength 0.3; dt = 1/60 s.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Dict, List
+
+import numpy as np
+
+from .emitters import IgniterEmitter, ScalarEmitter, VelocityEmitter
+
+QUALITY_C0 = {
+    "finePreIterations": 4,
+    "finePostIterations": 4,
+    "midPreIterations": 4,
+    "midPostIterations": 4,
+    "coarseIterations": 20,
+}
+
+DT = 1.0 / 60.0
+
+
+@dataclass
+class Workload:
+    name: str
+    options: Dict
+    sources: List
+    state: Dict[str, np.ndarray]
+    dt: float = DT
+
+
+class Pcg32:
+    """PCG-XSH-RR 32-bit generator (O'Neill 2014), for seeded workload draws."""
+
+    MULT = 6364136223846793005
+    MASK = (1 << 64) - 1
+
+    def __init__(self, seed: int, seq: int = 54):
+        self.inc = ((seq << 1) | 1) & self.MASK
+        self.state = 0
+        self.next_u32()
+        self.state = (self.state + seed) & self.MASK
+        self.next_u32()
+
+    def next_u32(self) -> int:
+        old = self.state
+        self.state = (old * self.MULT + self.inc) & self.MASK
+        xorshifted = (((old >> 18) ^ old) >> 27) & 0xFFFFFFFF
+        rot = old >> 59
+        return ((xorshifted >> rot) | (xorshifted << ((-rot) & 31))) & 0xFFFFFFFF
+
+    def uniform(self, lo: float, hi: float) -> float:
+        return lo + (hi - lo) * (self.next_u32() / 4294967296.0)
+
+
+def _plume_sources(res, centers_vox, radii_vox, rng: Pcg32):
+    w, h, d = res
+    out = []
+    for (cx, cy, cz), r in zip(centers_vox, radii_vox):
+        pos = (cx / w, cy / h, cz / d)
+        rn = r / max(w, d)
+        seed = float(int(rng.uniform(1, 4000)))
+        out.append(ScalarEmitter(position=pos, radius=rn, startTime=0.0, duration=1.0e4, densityRate=1.2, heatRate=3.5,
+                                 fuelRate=4.0, noiseScale=9.0, noiseMix=0.45, seed=seed))
+        out.append(VelocityEmitter(position=pos, radius=rn * 1.3, startTime=0.0, duration=1.0e4, mode="directional", speed=24.0,
+                                   direction=(0.0, 1.0, 0.0), falloff=0.7, seed=seed + 1.0, tightness=0.25))
+        out.append(IgniterEmitter(position=pos, radius=rn, startTime=0.0, duration=1.0e4, intensity=0.8, seed=seed + 2.0))
+    return out
+
+
+def _plume_state(res, centers_vox, radii_vox, heights, seed: int) -> Dict[str, np.ndarray]:
+    """A developed-plume state: cones of smoke and heat rising from each source,
+    with seeded lateral wobble and noise. Returned arrays are (D, H, W) float32."""
+    w, h, d = res
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid(np.arange(d, dtype=np.float32), np.arange(h, dtype=np.float32), np.arange(w, dtype=np.float32), indexing="ij")
+    dens = np.zeros((d, h, w), np.float32)
+    temp = np.zeros_like(dens)
+    fuel = np.zeros_like(dens)
+    reac = np.zeros_like(dens)
+    vy = np.zeros_like(dens)
+    vx = np.zeros_like(dens)
+    vz = np.zeros_like(dens)
+    for (cx, cy, cz), r, top in zip(centers_vox, radii_vox, heights):
+        phase = rng.uniform(0, 2 * np.pi, size=2)
+        t = np.clip((y - cy) / max(top - cy, 1.0), 0.0, 1.0)
+        wob_x = cx + 6.0 * np.sin(0.045 * y + phase[0]) * t
+        wob_z = cz + 6.0 * np.cos(0.038 * y + phase[1]) * t
+        rad = r * (1.0 + 2.4 * t)
+        dist = np.sqrt((x - wob_x) ** 2 + (z - wob_z) ** 2)
+        inside = (y >= cy - r) & (y <= top)
+        core = np.clip(1.0 - dist / rad, 0.0, 1.0) * inside
+        dens = np.maximum(dens, (0.55 * core * (0.4 + 0.6 * t)).astype(np.float32))
+        temp = np.maximum(temp, (0.9 * core * (1.0 - 0.7 * t)).astype(np.float32))
+        fuel = np.maximum(fuel, (0.6 * core * np.clip(1.0 - 3.0 * t, 0, 1)).astype(np.float32))
+        reac = np.maximum(reac, (0.5 * core * np.clip(1.0 - 2.0 * t, 0, 1)).astype(np.float32))
+        vy = np.maximum(vy, (18.0 * core * (1.0 - 0.5 * t)).astype(np.float32))
+        vx += (2.0 * core * np.sin(0.05 * y + phase[0])).astype(np.float32)
+        vz += (2.0 * core * np.cos(0.05 * y + phase[1])).astype(np.float32)
+    noise = rng.uniform(0.85, 1.0, size=dens.shape).astype(np.float32)
+    out = {
+        "density": np.clip(dens * noise, 0, 1),
+        "temperature": np.clip(temp * noise, 0, 1),
+        "fuel": np.clip(fuel * noise, 0, 1),
+        "reaction": np.clip(reac * noise, 0, 1),
+        "velocity_x": vx,
+        "velocity_y": vy,
+        "velocity_z": vz,
+    }
+    return {k: v.astype(np.float32) for k, v in out.items()}
+
+
+def plume_256(seed: int = 1235, size: int = 256) -> Workload:
+    """Four-plume sparse fire on a size^3 grid (size 256 by default)."""
+    rng = Pcg32(seed)
+    s = size / 256.0
+    centers = []
+    radii = []
+    heights = []
+    for _ in range(4):
+        cx = rng.uniform(40, 216) * s
+        cz = rng.uniform(40, 216) * s
+        r = rng.uniform(8, 14) * s
+        centers.append((cx, 8.0 * s, cz))
+        radii.append(r)
+        heights.append(rng.uniform(150, 230) * s)
+    res = (size, size, size)
+    options = {
+        "resolution": res,
+        "worldSize": 10.0,
+        "gravityStrength": 0.1,
+        "buoyancy": 1.0,
+        "vorticityStrength": 0.3,
+        "qualitySettings": dict(QUALITY_C0),
+    }
+    return Workload(f"plume_{size}", options, _plume_sources(res, centers, radii, rng), _plume_state(res, centers, radii, heights, seed))
+
+
+def plume_64(seed: int = 1234) -> Workload:
+    """One emitter at (32, 6, 32) voxels of a 64^3 grid with radius 6 voxels, voxel size 1/64."""
+    res = (64, 64, 64)
+    options = {
+        "resolution": res,
+        "worldSize": 1.0,
+        "gravityStrength": 0.1,
+        "buoyancy": 1.0,
+        "vorticityStrength": 0.3,
+        "qualitySettings": dict(QUALITY_C0),
+    }
+    pos = (32 / 64, 6 / 64, 32 / 64)
+    sources = [
+        ScalarEmitter(position=pos, radius=6 / 64, startTime=0.0, duration=1.0e4, densityRate=0.0, heatRate=60.0, fuelRate=60.0,
+                      noiseScale=1.0, noiseMix=0.0, seed=float(seed)),
+        VelocityEmitter(position=pos, radius=6 / 64, startTime=0.0, duration=1.0e4, mode="directional", speed=2.0,
+                        direction=(0.0, 1.0, 0.0), falloff=0.0, seed=float(seed + 1), tightness=1.0),
+    ]
+    return Workload("plume_64", options, sources, {})
+
+
+def load_state(sim, state: Dict[str, np.ndarray]) -> None:
+    """Writes a workload's initial fields into the current set and velocity."""
+    for name, arr in state.items():
+        sim.writeField(name, arr.ravel())
+
+
+def brick_voxel_counts(res) -> np.ndarray:
+    """Voxels of each brick (x fastest), for grids that are not multiples of 8."""
+    w, h, d = res
+    bx, by, bz = (w + 7) // 8, (h + 7) // 8, (d + 7) // 8
+    cx = np.minimum(8, w - 8 * np.arange(bx))
+    cy = np.minimum(8, h - 8 * np.arange(by))
+    cz = np.minimum(8, d - 8 * np.arange(bz))
+    return (cz[:, None, None] * cy[None, :, None] * cx[None, None, :]).ravel().astype(np.int64)

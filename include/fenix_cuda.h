@@ -1,0 +1,286 @@
+/*
+ * fenix_cuda.h — C ABI of libfenixcuda.so, a B200 (sm_100a) CUDA implementation of
+ * fenix's per-frame combustion-volume simulation step.
+ *
+ * Each entry point replaces one member of the reference's simulation object,
+ * `CombustionVolumeSimulation`
+ * (src/engine/simulation/runtime/combustion-volume-simulation/types.ts:62-76),
+ * created by `createCombustionVolumeSimulation(device, options)`
+ * (src/engine/simulation/runtime/createCombustionVolumeSimulation.ts:39-53).
+ * Each declaration below cites the reference member it replaces.
+ *
+ * Conventions
+ *  - All functions are `extern "C"`. They take plain pointers and sizes and return
+ *    fx_status (0 = FX_OK, < 0 = FX_ERR_*). No C++ exception crosses the ABI.
+ *  - A handle is thread-affine: use one host thread per fx_sim.
+ *  - fx_sim_step only enqueues work on the simulation's CUDA stream and does not
+ *    wait for it. This matches the reference, where step() records into the
+ *    caller's encoder and the caller submits. Calls that return data to the host
+ *    (read_field, get_stats with counts, synchronize) wait for the stream.
+ *  - After the first failure a handle keeps a sticky error string
+ *    (fx_sim_last_error). Failures before a handle exists are reported through
+ *    fx_last_error().
+ *  - Device pointers are returned as uint64_t (a bigint under bun:ffi).
+ *  - Parameters are latched at the next fx_sim_step, as in the reference.
+ */
+#ifndef FENIX_CUDA_H
+#define FENIX_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FX_ABI_VERSION 1
+
+typedef int32_t fx_status;
+#define FX_OK 0
+#define FX_ERR_INVALID_ARGUMENT (-1)
+#define FX_ERR_CUDA (-2)
+#define FX_ERR_OUT_OF_MEMORY (-3)
+#define FX_ERR_STATE (-4)
+#define FX_ERR_TIMEOUT (-5)
+#define FX_ERR_UNSUPPORTED (-6)
+
+typedef struct fx_sim fx_sim;
+
+/* ScalarAdvectionMode (types.ts:4): 'semi-lagrangian' | 'maccormack'. */
+#define FX_ADVECT_SEMI_LAGRANGIAN 0
+#define FX_ADVECT_MACCORMACK 1
+
+/* SimulationQualitySettings (types.ts:6-14). Values are JS numbers in the
+ * reference, so they are doubles here. Setters round and clamp them exactly as
+ * createSimulationQualitySettings does (types.ts:26-44). A NaN is rejected with
+ * FX_ERR_INVALID_ARGUMENT. */
+typedef struct fx_quality {
+  double pressure_interval;    /* 1..16 */
+  double vorticity_interval;   /* 1..16 */
+  double fine_pre_iterations;  /* 0..32 */
+  double fine_post_iterations; /* 0..32 */
+  double mid_pre_iterations;   /* 0..32 */
+  double mid_post_iterations;  /* 0..32 */
+  double coarse_iterations;    /* 0..64 */
+} fx_quality;
+
+#define FX_QUALITY_PRESSURE_INTERVAL (1u << 0)
+#define FX_QUALITY_VORTICITY_INTERVAL (1u << 1)
+#define FX_QUALITY_FINE_PRE (1u << 2)
+#define FX_QUALITY_FINE_POST (1u << 3)
+#define FX_QUALITY_MID_PRE (1u << 4)
+#define FX_QUALITY_MID_POST (1u << 5)
+#define FX_QUALITY_COARSE (1u << 6)
+#define FX_QUALITY_ALL (0x7Fu)
+
+/* SimulationRuntimeParams (types.ts:46-58). A field mask stands for Partial<>. */
+typedef struct fx_runtime_params {
+  double wind[3];
+  double wind_strength;
+  double gravity[3];
+  double gravity_strength;
+  double buoyancy;
+  double vorticity_strength;
+  double vorticity_constant_mask;
+  double vorticity_velocity_mask;
+  double vorticity_heat_mask;
+  double vorticity_density_mask;
+  double world_size;
+} fx_runtime_params;
+
+#define FX_PARAM_WIND (1u << 0)
+#define FX_PARAM_WIND_STRENGTH (1u << 1)
+#define FX_PARAM_GRAVITY (1u << 2)
+#define FX_PARAM_GRAVITY_STRENGTH (1u << 3)
+#define FX_PARAM_BUOYANCY (1u << 4)
+#define FX_PARAM_VORTICITY_STRENGTH (1u << 5)
+#define FX_PARAM_VORTICITY_CONSTANT_MASK (1u << 6)
+#define FX_PARAM_VORTICITY_VELOCITY_MASK (1u << 7)
+#define FX_PARAM_VORTICITY_HEAT_MASK (1u << 8)
+#define FX_PARAM_VORTICITY_DENSITY_MASK (1u << 9)
+#define FX_PARAM_WORLD_SIZE (1u << 10)
+#define FX_PARAM_ALL (0x7FFu)
+
+/* Kernel paths. Both compute the reference step and give identical results. */
+#define FX_KERNELS_FUSED 0 /* default: fused, brick-list-driven kernels */
+#define FX_KERNELS_PLAIN 1 /* one kernel per reference WGSL pass (the plain FP32 step) */
+
+/* Option flags (extensions; none changes results). */
+#define FX_OPT_DEBUG_FIELDS (1u << 0) /* always write vorticity, |vorticity|, |F_conf| */
+#define FX_OPT_NO_GRAPHS (1u << 1)    /* launch kernels directly instead of CUDA graphs */
+
+/* CombustionVolumeSimulationOptions (createCombustionVolumeSimulation.ts:39-48).
+ * Fill with fx_sim_options_default() and then override fields. */
+typedef struct fx_sim_options {
+  uint32_t struct_size;           /* sizeof(fx_sim_options) */
+  uint32_t width, height, depth;  /* resolution; 0 = reference default 128 x 256 x 128 */
+  int32_t scalar_advection_mode;  /* FX_ADVECT_*; default maccormack */
+  uint32_t runtime_mask;          /* FX_PARAM_* bits of `runtime` that are given */
+  fx_runtime_params runtime;      /* options.wind/windStrength/gravity/gravityStrength/worldSize (+ the rest) */
+  uint32_t quality_mask;          /* FX_QUALITY_* bits of `quality` that are given */
+  fx_quality quality;             /* options.qualitySettings */
+  int32_t device;                 /* CUDA device ordinal */
+  int32_t kernels;                /* FX_KERNELS_* */
+  uint32_t flags;                 /* FX_OPT_* */
+  void* stream;                   /* cudaStream_t to enqueue on; NULL = the simulation's own stream */
+} fx_sim_options;
+
+/* getRenderBuffers() (createCombustionVolumeSimulation.ts:306-312): the current
+ * scalar set, the current brick flags and the packed brick layout
+ * (sim/sparse/createSparseBrickLayout.ts:28-38). Device pointers stay valid until
+ * fx_sim_destroy; which buffers form the current set alternates every step. */
+typedef struct fx_render_buffers {
+  uint64_t density;
+  uint64_t temperature;
+  uint64_t fuel;
+  uint64_t reaction;
+  uint64_t active_brick_flags; /* uint32 per brick, 1 = active */
+  uint32_t active_brick_info[8];
+  uint32_t width, height, depth;
+  int32_t dtype; /* FX_DTYPE_F32 */
+} fx_render_buffers;
+
+#define FX_DTYPE_F32 0
+
+/* getDebugBuffers() (createCombustionVolumeSimulation.ts:313-326). */
+typedef struct fx_debug_buffers {
+  fx_render_buffers render;
+  uint64_t velocity_magnitude;
+  uint64_t divergence;
+  uint64_t pressure;
+  uint64_t vorticity_magnitude;
+  uint64_t confinement_force_magnitude;
+} fx_debug_buffers;
+
+/* Field ids for fx_sim_read_field / fx_sim_write_field. Scalar and velocity fields
+ * are f32 of width*height*depth voxels (x fastest); flags are uint32 per brick;
+ * pressure-level fields have the level's own voxel count. */
+enum {
+  FX_FIELD_DENSITY = 0, FX_FIELD_TEMPERATURE, FX_FIELD_FUEL, FX_FIELD_REACTION,
+  FX_FIELD_PREV_DENSITY, FX_FIELD_PREV_TEMPERATURE, FX_FIELD_PREV_FUEL, FX_FIELD_PREV_REACTION,
+  FX_FIELD_VELOCITY_X, FX_FIELD_VELOCITY_Y, FX_FIELD_VELOCITY_Z,
+  FX_FIELD_VELOCITY_SCRATCH_X, FX_FIELD_VELOCITY_SCRATCH_Y, FX_FIELD_VELOCITY_SCRATCH_Z,
+  FX_FIELD_VORTICITY_X, FX_FIELD_VORTICITY_Y, FX_FIELD_VORTICITY_Z,
+  FX_FIELD_VORTICITY_MAGNITUDE, FX_FIELD_CONFINEMENT_MAGNITUDE, FX_FIELD_VELOCITY_MAGNITUDE,
+  FX_FIELD_BRICK_FLAGS, FX_FIELD_PREV_BRICK_FLAGS,
+  FX_FIELD_FINE_DIVERGENCE, FX_FIELD_FINE_PRESSURE_A, FX_FIELD_FINE_PRESSURE_B,
+  FX_FIELD_MID_DIVERGENCE, FX_FIELD_MID_PRESSURE_A, FX_FIELD_MID_PRESSURE_B,
+  FX_FIELD_COARSE_DIVERGENCE, FX_FIELD_COARSE_PRESSURE_A, FX_FIELD_COARSE_PRESSURE_B,
+  FX_FIELD_PRESSURE,
+  FX_FIELD_COUNT
+};
+
+/* Host-visible counters of a simulation. */
+typedef struct fx_stats {
+  int64_t step_index;          /* simulationStepIndex */
+  int32_t current_scalar_set;  /* currentScalarSet (0 or 1) */
+  int32_t last_pressure_buffer;/* lastPressureBuffer: 0 = 'a', 1 = 'b' */
+  uint32_t brick_count;        /* bricks of 8^3 voxels */
+  uint32_t active_bricks;      /* bricks flagged in the current flags (waits for the stream) */
+  uint32_t kernels_per_step;   /* kernels the last step launched */
+  uint32_t reserved;
+} fx_stats;
+
+/* Version of this ABI (FX_ABI_VERSION). */
+int32_t fx_abi_version(void);
+
+/* Message of the last failure on this thread that had no handle to record it. */
+const char* fx_last_error(void);
+
+/* Fills `opt` with the reference defaults (createCombustionVolumeSimulation.ts:54,
+ * 181,194-204; types.ts:16-24). */
+void fx_sim_options_default(fx_sim_options* opt);
+
+/* createCombustionVolumeSimulation(device, options)
+ * (createCombustionVolumeSimulation.ts:50-401). Allocates and zeroes every buffer. */
+fx_status fx_sim_create(const fx_sim_options* opt, fx_sim** out);
+
+/* dispose() (createCombustionVolumeSimulation.ts:384-399). NULL is ignored. */
+void fx_sim_destroy(fx_sim* sim);
+
+/* step(encoder, elapsedSeconds, stepSeconds) (createCombustionVolumeSimulation.ts:230-305).
+ * Enqueues one step on the simulation's stream. */
+fx_status fx_sim_step(fx_sim* sim, double elapsed_seconds, double step_seconds);
+
+/* getRenderBuffers() (createCombustionVolumeSimulation.ts:306-312). */
+fx_status fx_sim_get_render_buffers(fx_sim* sim, fx_render_buffers* out);
+
+/* getDebugBuffers() (createCombustionVolumeSimulation.ts:313-326). Like the
+ * reference, this requests the |v| debug pass on the next step. */
+fx_status fx_sim_get_debug_buffers(fx_sim* sim, fx_debug_buffers* out);
+
+/* getScalarAdvectionMode() / setScalarAdvectionMode(mode)
+ * (createCombustionVolumeSimulation.ts:327-337). */
+fx_status fx_sim_get_scalar_advection_mode(fx_sim* sim, int32_t* mode);
+fx_status fx_sim_set_scalar_advection_mode(fx_sim* sim, int32_t mode);
+
+/* getRuntimeParams() / setRuntimeParams(Partial<params>)
+ * (createCombustionVolumeSimulation.ts:338-365). `mask` selects the given fields. */
+fx_status fx_sim_get_runtime_params(fx_sim* sim, fx_runtime_params* out);
+fx_status fx_sim_set_runtime_params(fx_sim* sim, const fx_runtime_params* params, uint32_t mask);
+
+/* getQualitySettings() / setQualitySettings(Partial<settings>)
+ * (createCombustionVolumeSimulation.ts:366-377). */
+fx_status fx_sim_get_quality(fx_sim* sim, fx_quality* out);
+fx_status fx_sim_set_quality(fx_sim* sim, const fx_quality* quality, uint32_t mask);
+
+/* updateSources(sources) (createCombustionVolumeSimulation.ts:378-380 →
+ * runtime/passes/SourceInjectionPass.ts:71-83). `packed` holds count * 32 floats in
+ * the layout of sim/emitters/packEmitterSources.ts:13-77 (128 bytes per source). */
+fx_status fx_sim_update_sources(fx_sim* sim, const float* packed, uint32_t count);
+
+/* reset() (createCombustionVolumeSimulation.ts:381-383 → doReset :206-226). */
+fx_status fx_sim_reset(fx_sim* sim);
+
+/* resolution (types.ts:63). */
+fx_status fx_sim_get_resolution(fx_sim* sim, uint32_t* width, uint32_t* height, uint32_t* depth);
+
+/* Readback and upload of one field (no reference counterpart: the reference
+ * reads buffers only through its renderer). Waits for the stream. `bytes` must
+ * equal the field's size. */
+fx_status fx_sim_field_size(fx_sim* sim, int32_t field_id, size_t* bytes);
+fx_status fx_sim_read_field(fx_sim* sim, int32_t field_id, void* host_dst, size_t bytes);
+fx_status fx_sim_write_field(fx_sim* sim, int32_t field_id, const void* host_src, size_t bytes);
+
+/* Waits until all enqueued work of the simulation has finished. */
+fx_status fx_sim_synchronize(fx_sim* sim);
+
+/* Counters; active_bricks waits for the stream. */
+fx_status fx_sim_get_stats(fx_sim* sim, fx_stats* out);
+
+/* Instrumentation (no reference counterpart; the reference's only timing is a
+ * stats-gl overlay, src/engine/render/renderer/createViewportRuntime.ts:236-268).
+ * FX_INSTR_KERNEL_TIMES brackets every kernel with CUDA events on the
+ * simulation's stream; FX_INSTR_COUNT_ACTIVE adds, after every step, the step's
+ * active bricks and their voxels to device-side counters. */
+#define FX_INSTR_KERNEL_TIMES (1u << 0)
+#define FX_INSTR_COUNT_ACTIVE (1u << 1)
+
+typedef struct fx_kernel_time {
+  char name[48];
+  uint32_t launches;
+  uint32_t reserved;
+  double total_ms;
+} fx_kernel_time;
+
+fx_status fx_sim_set_instrumentation(fx_sim* sim, uint32_t flags);
+
+/* Per-kernel totals since the last call (waits for the stream, then resets).
+ * Writes up to `capacity` entries and the number of distinct kernels to *count. */
+fx_status fx_sim_read_kernel_times(fx_sim* sim, fx_kernel_time* out, uint32_t capacity, uint32_t* count);
+
+/* Active bricks and active voxels summed over the steps since the last call
+ * (waits for the stream, then resets). */
+fx_status fx_sim_read_active_counters(fx_sim* sim, uint64_t* brick_steps, uint64_t* voxel_steps);
+
+/* The CUDA stream the simulation enqueues on (cudaStream_t). */
+fx_status fx_sim_get_stream(fx_sim* sim, void** stream);
+
+/* The sticky error message of a handle ("" when none). */
+const char* fx_sim_last_error(fx_sim* sim);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FENIX_CUDA_H */

@@ -1,0 +1,210 @@
+"""ORACLE — test infrastructure, not product code.
+
+ctypes wrapper of liboracle_fenix.so, the CPU restatement of fenix's
+combustion-volume step (fenix_oracle.cpp). Only the tests, the smoke check and
+the CPU-baseline leg of bench.py use it, as the checker. Parity against the
+reference itself is UNPINNED (the reference has no runnable CPU path, tests or
+golden vectors); see fenix_oracle.cpp.
+
+`OracleSimulation` takes the same calls as fenix_b200's
+`CombustionVolumeSimulation`, so a test can drive both with one script.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_double, c_float, c_int, c_long, c_uint32, c_void_p
+from typing import Any, Mapping, Optional, Sequence
+
+import numpy as np
+
+from fenix_b200 import _lib as fxlib
+from fenix_b200.emitters import packEmitterSources
+from fenix_b200.simulation import QUALITY_KEYS, _resolution_tuple, createSimulationQualitySettings
+
+ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(ORACLE_DIR, "liboracle_fenix.so")
+
+_LIB = None
+
+
+def load() -> ctypes.CDLL:
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python oracle/build.py`")
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.orc_create.restype = c_void_p
+        lib.orc_create.argtypes = [c_int, c_uint32, c_uint32, c_uint32]
+        lib.orc_destroy.argtypes = [c_void_p]
+        lib.orc_set_runtime_params.argtypes = [c_void_p, POINTER(c_double)]
+        lib.orc_set_quality.argtypes = [c_void_p, POINTER(c_int)]
+        lib.orc_set_advection_mode.argtypes = [c_void_p, c_int]
+        lib.orc_set_emit_dead_residual.argtypes = [c_void_p, c_int]
+        lib.orc_update_sources.argtypes = [c_void_p, POINTER(c_float), c_uint32]
+        lib.orc_step.argtypes = [c_void_p, c_double, c_double]
+        lib.orc_reset.argtypes = [c_void_p]
+        lib.orc_request_debug.argtypes = [c_void_p]
+        lib.orc_get_state.argtypes = [c_void_p, POINTER(c_long)]
+        lib.orc_read_field.restype = c_long
+        lib.orc_read_field.argtypes = [c_void_p, c_int, POINTER(c_double), c_long]
+        lib.orc_write_field.restype = c_long
+        lib.orc_write_field.argtypes = [c_void_p, c_int, POINTER(c_double), c_long]
+        lib.orc_pinned_sin.argtypes = [POINTER(c_float), POINTER(c_float), c_long]
+        lib.orc_pinned_cos.argtypes = [POINTER(c_float), POINTER(c_float), c_long]
+        lib.orc_num_threads.restype = c_int
+        lib.orc_set_num_threads.argtypes = [c_int]
+        _LIB = lib
+    return _LIB
+
+
+_PARAM_ORDER = [
+    ("wind", 3), ("windStrength", 1), ("gravity", 3), ("gravityStrength", 1), ("buoyancy", 1),
+    ("vorticityStrength", 1), ("vorticityConstantMask", 1), ("vorticityVelocityMask", 1),
+    ("vorticityHeatMask", 1), ("vorticityDensityMask", 1), ("worldSize", 1),
+]
+
+DEFAULT_RUNTIME = {
+    "wind": (0.0, 0.0, 0.0), "windStrength": 0.0, "gravity": (0.0, -1.0, 0.0), "gravityStrength": 0.45,
+    "buoyancy": 3.6, "vorticityStrength": 2.15, "vorticityConstantMask": 1.0, "vorticityVelocityMask": 0.4,
+    "vorticityHeatMask": 0.8, "vorticityDensityMask": 0.35, "worldSize": 10.0,
+}
+
+
+def pinned_sin(x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty_like(x)
+    load().orc_pinned_sin(x.ctypes.data_as(POINTER(c_float)), out.ctypes.data_as(POINTER(c_float)), x.size)
+    return out
+
+
+def pinned_cos(x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty_like(x)
+    load().orc_pinned_cos(x.ctypes.data_as(POINTER(c_float)), out.ctypes.data_as(POINTER(c_float)), x.size)
+    return out
+
+
+def set_threads(n: int) -> None:
+    load().orc_set_num_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(load().orc_num_threads())
+
+
+class OracleSimulation:
+    """The reference step on the CPU, in f32 (precision=32) or f64 (precision=64)."""
+
+    def __init__(self, options: Optional[Mapping[str, Any]] = None, precision: int = 32):
+        self._lib = load()
+        options = dict(options or {})
+        w, h, d = _resolution_tuple(options.pop("resolution", None))
+        self.resolution = {"width": w, "height": h, "depth": d}
+        self.precision = precision
+        self._h = self._lib.orc_create(precision, w, h, d)
+        if not self._h:
+            raise ValueError("orc_create rejected the arguments")
+        self._runtime = dict(DEFAULT_RUNTIME)
+        mode = options.pop("scalarAdvectionMode", None)
+        self._mode = "maccormack"
+        if mode is not None:
+            self.setScalarAdvectionMode(mode)
+        quality = options.pop("qualitySettings", None)
+        self._quality = createSimulationQualitySettings(quality or {})
+        self._push_quality()
+        self.setRuntimeParams(options)
+
+    def _push_quality(self) -> None:
+        q = (c_int * 7)(*[self._quality[k] for k in QUALITY_KEYS])
+        self._lib.orc_set_quality(self._h, q)
+
+    def step(self, elapsedSeconds: float, stepSeconds: float) -> None:
+        self._lib.orc_step(self._h, float(elapsedSeconds), float(stepSeconds))
+
+    def setRuntimeParams(self, params: Mapping[str, Any]) -> None:
+        for k, v in params.items():
+            if k not in self._runtime:
+                raise KeyError(f"unknown runtime parameter {k!r}")
+            if v is not None:
+                self._runtime[k] = tuple(float(x) for x in v) if k in ("wind", "gravity") else float(v)
+        flat = []
+        for k, n in _PARAM_ORDER:
+            v = self._runtime[k]
+            flat.extend(v if n == 3 else [v])
+        arr = (c_double * 15)(*flat)
+        self._lib.orc_set_runtime_params(self._h, arr)
+
+    def getRuntimeParams(self) -> dict:
+        return dict(self._runtime)
+
+    def setQualitySettings(self, settings: Mapping[str, Any]) -> None:
+        merged = dict(self._quality)
+        merged.update({k: v for k, v in settings.items() if v is not None})
+        self._quality = createSimulationQualitySettings(merged)
+        self._push_quality()
+
+    def getQualitySettings(self) -> dict:
+        return dict(self._quality)
+
+    def setScalarAdvectionMode(self, mode: str) -> None:
+        self._lib.orc_set_advection_mode(self._h, {"semi-lagrangian": 0, "maccormack": 1}[mode])
+        self._mode = mode
+
+    def getScalarAdvectionMode(self) -> str:
+        return self._mode
+
+    def updateSources(self, sources: Sequence[Any]) -> None:
+        self.updatePackedSources(packEmitterSources(sources), len(sources))
+
+    def updatePackedSources(self, packed: np.ndarray, count: int) -> None:
+        arr = np.ascontiguousarray(packed, dtype=np.float32)
+        self._lib.orc_update_sources(self._h, arr.ctypes.data_as(POINTER(c_float)), count)
+
+    def setEmitDeadResidual(self, on: bool) -> None:
+        self._lib.orc_set_emit_dead_residual(self._h, 1 if on else 0)
+
+    def getDebugBuffers(self) -> None:
+        """Like the reference, asks for the |v| debug pass on the next step."""
+        self._lib.orc_request_debug(self._h)
+
+    def reset(self) -> None:
+        self._lib.orc_reset(self._h)
+
+    def state(self) -> dict:
+        out = (c_long * 4)()
+        self._lib.orc_get_state(self._h, out)
+        return {"currentScalarSet": out[0], "stepIndex": out[1], "lastPressureBuffer": out[2], "brickCount": out[3]}
+
+    def readField(self, name: str) -> np.ndarray:
+        fid = fxlib.FIELD_IDS[name]
+        cap = self._field_count(fid)
+        buf = np.empty(cap, dtype=np.float64)
+        n = self._lib.orc_read_field(self._h, fid, buf.ctypes.data_as(POINTER(c_double)), cap)
+        if n <= 0:
+            raise KeyError(name)
+        if name in fxlib.UINT_FIELDS:
+            return buf[:n].astype(np.uint32)
+        return buf[:n].astype(np.float32) if self.precision == 32 else buf[:n]
+
+    def writeField(self, name: str, values: np.ndarray) -> None:
+        fid = fxlib.FIELD_IDS[name]
+        arr = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        n = self._lib.orc_write_field(self._h, fid, arr.ctypes.data_as(POINTER(c_double)), arr.size)
+        if n != arr.size:
+            raise ValueError(f"writeField({name}): size mismatch")
+
+    def _field_count(self, fid: int) -> int:
+        n = self._lib.orc_read_field(self._h, fid, None, 0)
+        return -n if n < 0 else n
+
+    def dispose(self) -> None:
+        if self._h:
+            self._lib.orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.dispose()
+        except Exception:
+            pass
