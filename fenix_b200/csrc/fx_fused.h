@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <functional>
 #include <string>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "../../include/fenix_cuda.h"
@@ -17,27 +18,34 @@ struct FusedWork {
   Dims dm{};
   uint3 bricks{};
   uint32_t nb = 0;
-  // Per-brick energy summary of a scalar set at the reference's flag sample
-  // points: bit 0 = some sample above the activity threshold, bit 1 = dilate.
-  uint8_t* summary_cur = nullptr;   // summary of the current set (after injection)
-  uint8_t* summary_next = nullptr;  // summary of the advected set
-  // Bricks whose voxels may be non-zero in the advected scratch set (T) and in
-  // the current set (S).
-  uint8_t* maybe_nz_t = nullptr;
-  uint8_t* maybe_nz_s = nullptr;
-  // Compacted brick lists and their counts.
+  // Per-brick energy summary of a scalar buffer at the reference's flag sample
+  // points (bit 0: some sample above the activity threshold, bit 1: the brick
+  // dilates), for the two scalar sets and the advected scratch set T.
+  uint8_t* summary_set[2] = {nullptr, nullptr};
+  uint8_t* summary_t = nullptr;
+  // Bricks whose voxels may be non-zero, per scalar buffer.
+  uint8_t* nz_set[2] = {nullptr, nullptr};
+  uint8_t* nz_t = nullptr;
+  // Compacted brick lists.
   uint32_t* list_adv = nullptr;   // bricks the scalar advection kernel visits
   uint32_t* list_next = nullptr;  // bricks the combustion/buoyancy kernels visit
   uint32_t* list_inj = nullptr;   // bricks the injection kernel visits (host-filled)
-  uint32_t* counters = nullptr;   // [0] adv count, [1] next count, [2] scratch
-  uint32_t* host_list_inj = nullptr;  // pinned staging for list_inj
-  uint32_t inj_count = 0;
+  uint32_t* counters = nullptr;   // [0] adv count, [1] next count, [2] scratch, [3] inject count
+  uint32_t* host_list_inj = nullptr;  // pinned staging for list_inj (+ count at [nb])
   cudaEvent_t inj_event = nullptr;
-  // CUDA graph cache of the step.
-  cudaGraphExec_t graph = nullptr;
-  uint64_t graph_key = ~0ull;
-  bool graph_ok = true;
-  bool valid = false;  // false: maybe-non-zero masks must be rebuilt
+  std::vector<uint8_t> host_mark;
+  std::vector<uint32_t> host_list;
+  bool valid = false;  // false: the per-brick bookkeeping must be rebuilt from the fields
+  // kernel timing
+  bool timing = false;
+  struct TimedPair {
+    const char* name;
+    int a, b;
+  };
+  std::vector<cudaEvent_t> timing_events;
+  std::vector<TimedPair> timing_pending;
+  int timing_next = 0;
+  int next_event();
 };
 
 struct FusedStep {
@@ -51,6 +59,7 @@ struct FusedStep {
   const float* host_sources;  // packed sources (NULL when none)
   uint32_t host_nsrc;
   int advect_mode;
+  int cur_index;  // index of the current scalar set (0 or 1)
   ScalarSet cur, next, scratch;
   uint32_t *flags_cur, *flags_next;
   VelField vcur, vscr, vscr2, vort;

@@ -421,7 +421,7 @@ void fx_sim_options_default(fx_sim_options* o) {
   o->quality.mid_post_iterations = 3;
   o->quality.coarse_iterations = 10;
   o->device = 0;
-  o->kernels = FX_KERNELS_PLAIN;
+  o->kernels = FX_KERNELS_FUSED;
   o->flags = 0;
   o->stream = nullptr;
 }
@@ -628,6 +628,7 @@ fx_status fx_sim_step(fx_sim* s, double elapsed, double step_s) {
     fs.host_sources = s->src_count ? s->host_sources.data() : nullptr;
     fs.host_nsrc = s->src_count;
     fs.advect_mode = s->advect_mode;
+    fs.cur_index = s->cur;
     fs.cur = s->sets[s->cur];
     fs.next = s->sets[s->cur ^ 1];
     fs.scratch = s->sets[2];
