@@ -343,9 +343,14 @@ template <class R> class Sim {
     return mx(r * K(0.24), voxel_width * K(3.0));
   }
   R source_outer_limit(R r) const { return r + source_feather(r); }
-  static R hash31(R x, R y, R z) {  // :102-104
-    const R d = x * K(127.1) + y * K(311.7) + z * K(74.7);
-    return fractv(Mth<R>::sin(d) * K(43758.5453123));
+  // hash31 (:102-104). The hash is a discrete pseudo-random function of integer
+  // lattice points, not a physical quantity: both instantiations evaluate it in
+  // f32 so that they produce the same noise pattern (an f64 evaluation of
+  // fract(sin(.) * 43758.5) gives unrelated values, not more accurate ones).
+  static R hash31(R x, R y, R z) {
+    const float xf = (float)x, yf = (float)y, zf = (float)z;
+    const float d = xf * 127.1f + yf * 311.7f + zf * 74.7f;
+    return (R)fractv(pinned_sincos(d, 0) * 43758.5453123f);
   }
   static R value_noise3(R px, R py, R pz) {  // :106-117
     const R cx = std::floor(px), cy = std::floor(py), cz = std::floor(pz);
@@ -1027,13 +1032,8 @@ template <class R> class Sim {
     });
   }
 
-  // createCombustionVolumeSimulation.ts:230-305
-  void step(double elapsed, double step_s) {
-    if (!initialized) {
-      initialized = true;
-      start_s = elapsed;
-      last_elapsed_s = elapsed;
-    }
+  // The uniform of createCombustionVolumeSimulation.ts:237-266 (doubles rounded to f32).
+  void prepare_params(double elapsed, double step_s) {
     const double effective = std::min(step_s, 1.0 / 15.0);
     const double local_time = elapsed - start_s;
     const double prev_local = last_elapsed_s - start_s;
@@ -1051,7 +1051,16 @@ template <class R> class Sim {
     P.dx = (float)dx;
     P.world_size = (float)world_size;
     for (int k = 0; k < 4; ++k) P.vmask[k] = (float)vmask[k];
+  }
 
+  // createCombustionVolumeSimulation.ts:230-305
+  void step(double elapsed, double step_s) {
+    if (!initialized) {
+      initialized = true;
+      start_s = elapsed;
+      last_elapsed_s = elapsed;
+    }
+    prepare_params(elapsed, step_s);
     const int next = cur == 0 ? 1 : 0;
     inject_scalar(cur);
     inject_velocity();
@@ -1198,6 +1207,55 @@ void orc_update_sources(void* hv, const float* packed, uint32_t count) {
     if (count == 0) s->sources.assign(32, 0.0f);
     else s->sources.assign(packed, packed + (size_t)count * 32);
     return 0;
+  });
+}
+
+// Sets the step uniform for (elapsed, step) without running a step.
+void orc_prepare_params(void* hv, double elapsed, double step_s) {
+  dispatch(static_cast<Handle*>(hv), [&](auto* s) {
+    if (!s->initialized) {
+      s->initialized = true;
+      s->start_s = elapsed;
+      s->last_elapsed_s = elapsed;
+    }
+    s->prepare_params(elapsed, step_s);
+    return 0;
+  });
+}
+
+// Runs one pass on the current state (tests). Scalar sets are addressed by
+// index 0/1, levels by 0 (fine), 1 (mid), 2 (coarse). Returns 0, or -1 for an
+// unknown pass.
+//   0 inject-scalar(set a)   1 inject-velocity          2 inject-igniter(set a)
+//   3 active-bricks(set a)   4 advect-velocity          5 maccormack(a -> b)
+//   6 semi-lagrangian(a -> b) 7 combustion(set a)       8 buoyancy(set a)
+//   9 vorticity             10 confinement(set a)      11 divergence
+//  12 jacobi(level a, p[b] -> p[1-b])                   13 restrict(level a -> a+1)
+//  14 prolong(level a+1 p[b] -> level a pA)             15 project(fine p[a])
+//  16 velocity magnitude    17 pressure solve (returns the final buffer id)
+int orc_run_pass(void* hv, int pass, int a, int b) {
+  return dispatch(static_cast<Handle*>(hv), [&](auto* s) -> int {
+    switch (pass) {
+      case 0: s->inject_scalar(a); return 0;
+      case 1: s->inject_velocity(); return 0;
+      case 2: s->inject_igniter(a); return 0;
+      case 3: s->active_bricks(a); return 0;
+      case 4: s->advect_velocity(); return 0;
+      case 5: s->advect_scalars_maccormack(a, b); return 0;
+      case 6: s->advect_scalars_semilagrangian(a, b); return 0;
+      case 7: s->combustion(a); return 0;
+      case 8: s->buoyancy_pass(a); return 0;
+      case 9: s->vorticity_pass(); return 0;
+      case 10: s->confinement_pass(a); return 0;
+      case 11: s->divergence_pass(); return 0;
+      case 12: s->jacobi(s->lv[a], s->pbuf(s->lv[a], b), s->pbuf(s->lv[a], b ^ 1)); return 0;
+      case 13: s->restrict_div(s->lv[a], s->lv[a + 1]); return 0;
+      case 14: s->prolong(s->lv[a + 1], s->pbuf(s->lv[a + 1], b), s->lv[a]); return 0;
+      case 15: s->project(s->pbuf(s->lv[0], a)); return 0;
+      case 16: s->debug_fields(); return 0;
+      case 17: return s->solve();
+      default: return -1;
+    }
   });
 }
 

@@ -43,6 +43,9 @@ def load() -> ctypes.CDLL:
         lib.orc_set_emit_dead_residual.argtypes = [c_void_p, c_int]
         lib.orc_update_sources.argtypes = [c_void_p, POINTER(c_float), c_uint32]
         lib.orc_step.argtypes = [c_void_p, c_double, c_double]
+        lib.orc_prepare_params.argtypes = [c_void_p, c_double, c_double]
+        lib.orc_run_pass.restype = c_int
+        lib.orc_run_pass.argtypes = [c_void_p, c_int, c_int, c_int]
         lib.orc_reset.argtypes = [c_void_p]
         lib.orc_request_debug.argtypes = [c_void_p]
         lib.orc_get_state.argtypes = [c_void_p, POINTER(c_long)]
@@ -160,6 +163,21 @@ class OracleSimulation:
     def updatePackedSources(self, packed: np.ndarray, count: int) -> None:
         arr = np.ascontiguousarray(packed, dtype=np.float32)
         self._lib.orc_update_sources(self._h, arr.ctypes.data_as(POINTER(c_float)), count)
+
+    PASSES = {
+        "inject_scalar": 0, "inject_velocity": 1, "inject_igniter": 2, "active_bricks": 3, "advect_velocity": 4,
+        "maccormack": 5, "semi_lagrangian": 6, "combustion": 7, "buoyancy": 8, "vorticity": 9, "confinement": 10,
+        "divergence": 11, "jacobi": 12, "restrict": 13, "prolong": 14, "project": 15, "velocity_magnitude": 16, "solve": 17,
+    }
+
+    def prepareParams(self, elapsedSeconds: float, stepSeconds: float) -> None:
+        self._lib.orc_prepare_params(self._h, float(elapsedSeconds), float(stepSeconds))
+
+    def runPass(self, name: str, a: int = 0, b: int = 0) -> int:
+        r = self._lib.orc_run_pass(self._h, self.PASSES[name], a, b)
+        if r < 0:
+            raise ValueError(name)
+        return r
 
     def setEmitDeadResidual(self, on: bool) -> None:
         self._lib.orc_set_emit_dead_residual(self._h, 1 if on else 0)
