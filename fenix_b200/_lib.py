@@ -187,6 +187,7 @@ PROTOTYPES = [
 # Test hooks exported beside the ABI (not declared in the public header).
 TEST_PROTOTYPES = [
     ("fx_test_pinned_sincos", c_int32, [POINTER(c_float), POINTER(c_float), c_uint32, c_int32]),
+    ("fx_test_div6_exhaustive", c_int32, [POINTER(c_uint64)]),
 ]
 
 _LIB = None

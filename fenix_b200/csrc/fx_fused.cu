@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "fx_fused.h"
+#include "fx_pressure.h"
 
 namespace fx {
 namespace {
@@ -803,16 +804,90 @@ fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
     }
     vfinal = &st.vscr2;
   }
-  // 9. pressure
+  // 9. pressure (PressureSolvePass.solve, :68-84) and 10. projection
   int last_p = st.last_p;
   if (st.pressure_on) {
-    for (int l = 0; l < 3; ++l)
-      FX_CK(cudaMemsetAsync(st.lv[l].p[0], 0, (size_t)st.lv[l].dm.w * st.lv[l].dm.h * st.lv[l].dm.d * sizeof(float), s));
+    const int m = st.q[2], n = st.q[3];
+    const LevelBuf& F = st.lv[0];
+    const LevelBuf& M = st.lv[1];
+    const LevelBuf& C = st.lv[2];
+    const bool fuse_restrict = dm.w >= 16 && dm.h >= 16 && dm.d >= 16;
+    // The reference's buffer ids: the pre-smoothed pressure ends in 'a' after an
+    // even number of sweeps, and the post smoothing flips it once per sweep.
+    const int fine_pre_id = m & 1;
+    last_p = fine_pre_id ^ (n & 1);
+    // Mid and coarse start from cleared pressureA (PressureSolvePass.clear). The
+    // fine passes never read the cleared fine buffer, so it is not cleared.
+    FX_CK(cudaMemsetAsync(M.p[0], 0, (size_t)M.dm.w * M.dm.h * M.dm.d * sizeof(float), s));
+    FX_CK(cudaMemsetAsync(C.p[0], 0, (size_t)C.dm.w * C.dm.h * C.dm.d * sizeof(float), s));
+
+    // Plan the fine passes: pre-smoothing in groups of <= 4 sweeps (the first one
+    // also computes the divergence), post-smoothing in groups of <= 4 sweeps (the
+    // first adds the prolongation, the last finishes with the projection).
+    struct Plan {
+      int sweeps;
+      ZInput input;
+      bool divv, proj;
+    };
+    std::vector<Plan> pre, post;
+    const int kmax = zpass_max_sweeps();
+    for (int left = m; left > 0;) {
+      const int k = std::min(left, kmax);
+      pre.push_back({k, pre.empty() ? ZIN_ZERO : ZIN_BUF, pre.empty(), false});
+      left -= k;
+    }
     {
+      const ZInput first_in = (m & 1) ? ZIN_BUF : (m == 0 ? ZIN_ZERO_PROLONG : ZIN_BUF_PROLONG);
+      if (n == 0) {
+        post.push_back({0, first_in, false, true});
+      } else {
+        for (int left = n; left > 0;) {
+          const int k = std::min(left, kmax);
+          post.push_back({k, post.empty() ? first_in : ZIN_BUF, false, left - k == 0});
+          left -= k;
+        }
+      }
+    }
+    // Output buffers: the last pass writes p[last]; going backwards the passes
+    // alternate with the other buffer, so no pass reads the buffer it writes.
+    const size_t npass = pre.size() + post.size();
+    std::vector<float*> outs(npass);
+    for (size_t i = npass; i-- > 0;)
+      outs[i] = (i + 1 == npass) ? F.p[last_p] : (outs[i + 1] == F.p[last_p] ? F.p[last_p ^ 1] : F.p[last_p]);
+    size_t pi = 0;
+    const float* chain = nullptr;  // the latest fine pressure (nullptr: the cleared buffer)
+    if (m == 0) {
       Timed tm(w, s, "fused_divergence");
-      plain_divergence(s, dm, *vfinal, st.lv[0].div);
+      plain_divergence(s, dm, *vfinal, F.div);
       ++launches;
     }
+    for (const Plan& pl : pre) {
+      ZPass zp{};
+      zp.dm = dm;
+      zp.mid = M.dm;
+      zp.sweeps = pl.sweeps;
+      zp.zchunk = zpass_zchunk();
+      zp.input = pl.input;
+      zp.div_from_velocity = pl.divv;
+      zp.project = false;
+      zp.restrict_mid = (pl.divv && fuse_restrict) ? 1 : 0;
+      zp.p_in = chain;
+      zp.div_in = F.div;
+      zp.div_out = F.div;
+      zp.mid_div = M.div;
+      zp.p_out = outs[pi];
+      zp.vfin = *vfinal;
+      Timed tm(w, s, pl.divv ? "fused_zpass_div_pre" : "fused_zpass_pre");
+      FX_CK(zpass_launch(s, zp));
+      ++launches;
+      chain = outs[pi++];
+    }
+    if (m == 0 || !fuse_restrict) {
+      Timed tm(w, s, "fused_restrict");
+      plain_restrict(s, F.dm, M.dm, F.div, M.div);
+      ++launches;
+    }
+    // mid and coarse levels (sweep by sweep)
     auto smooth = [&](const LevelBuf& L, int iters, int start, const char* name) {
       int a = start;
       for (int k = 0; k < iters; ++k) {
@@ -823,34 +898,43 @@ fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
       }
       return a;
     };
-    const int fine_pre = smooth(st.lv[0], st.q[2], 0, "fused_jacobi_fine");
+    const int mid_pre = smooth(M, st.q[4], 0, "fused_jacobi_mid");
     {
       Timed tm(w, s, "fused_restrict");
-      plain_restrict(s, st.lv[0].dm, st.lv[1].dm, st.lv[0].div, st.lv[1].div);
+      plain_restrict(s, M.dm, C.dm, M.div, C.div);
       ++launches;
     }
-    const int mid_pre = smooth(st.lv[1], st.q[4], 0, "fused_jacobi_mid");
-    {
-      Timed tm(w, s, "fused_restrict");
-      plain_restrict(s, st.lv[1].dm, st.lv[2].dm, st.lv[1].div, st.lv[2].div);
-      ++launches;
-    }
-    const int coarse = smooth(st.lv[2], st.q[6], 0, "fused_jacobi_coarse");
+    const int coarse = smooth(C, st.q[6], 0, "fused_jacobi_coarse");
     {
       Timed tm(w, s, "fused_prolong");
-      plain_prolong(s, st.lv[2].dm, st.lv[1].dm, st.lv[2].p[coarse], st.lv[1].p[0]);
+      plain_prolong(s, C.dm, M.dm, C.p[coarse], M.p[0]);
       ++launches;
     }
-    const int mid = smooth(st.lv[1], st.q[5], mid_pre, "fused_jacobi_mid");
-    {
-      Timed tm(w, s, "fused_prolong");
-      plain_prolong(s, st.lv[1].dm, st.lv[0].dm, st.lv[1].p[mid], st.lv[0].p[0]);
+    const int mid = smooth(M, st.q[5], mid_pre, "fused_jacobi_mid");
+    for (const Plan& pl : post) {
+      ZPass zp{};
+      zp.dm = dm;
+      zp.mid = M.dm;
+      zp.sweeps = pl.sweeps;
+      zp.zchunk = zpass_zchunk();
+      zp.input = pl.input;
+      zp.div_from_velocity = false;
+      zp.project = pl.proj;
+      zp.p_in = chain;
+      zp.div_in = F.div;
+      zp.mid_p = M.p[mid];
+      zp.p_out = outs[pi];
+      zp.vfin = *vfinal;
+      zp.vcur = st.vcur;
+      zp.vmag = st.vel_mag;
+      zp.write_vmag = st.debug_on ? 1 : 0;
+      Timed tm(w, s, pl.proj ? "fused_zpass_post_project" : "fused_zpass_post");
+      FX_CK(zpass_launch(s, zp));
       ++launches;
+      chain = outs[pi++];
     }
-    last_p = smooth(st.lv[0], st.q[3], fine_pre, "fused_jacobi_fine");
-  }
-  // 10. projection (+ |v|)
-  {
+  } else {
+    // 10. projection with the pressure of the last solve (+ |v|)
     Timed tm(w, s, "fused_project");
     k_project<<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0);
     ++launches;

@@ -1,0 +1,431 @@
+// Fine-level pressure passes of the fused path: up to four Jacobi sweeps
+// (pressure-jacobi.wgsl.ts:15-36) temporally blocked on chip, with the
+// divergence (compute-divergence.wgsl.ts:22-42), the fine->mid restriction
+// (pressure-restriction.wgsl.ts:27-50), the mid->fine prolongation
+// (pressure-prolongation.wgsl.ts:29-44) and the projection
+// (project-velocity.wgsl.ts:21-43) fused where the reference runs them next to
+// the sweeps.
+//
+// A block owns a TX x TY column of the grid and marches along z through a chunk
+// of planes. Stage 0 is the pass input and stage j the j-th sweep; stage j at
+// plane z needs stage j-1 at planes z-1..z+1, so stage j runs j planes behind
+// the input (one more when the divergence is computed in the block). Each thread
+// owns fixed (x, y) positions of a frame = the column widened by H voxels (H =
+// number of stencil stages after stage 0). For its positions it keeps every
+// stage's last three planes in registers (the z neighbours) and publishes the
+// newest plane to a double-buffered shared plane (the x and y neighbours).
+// Stage j is valid on the frame shrunk by j, which is all the next stage needs.
+// A stage at clock t reads only planes published at clock t-1, so one barrier
+// per plane suffices.
+//
+// Every value is computed with the reference's operations in its order: the
+// result equals the sweep-by-sweep evaluation bit for bit. The division by 6 is
+// the exact IEEE quotient (div6 below).
+#include <algorithm>
+#include <cstdlib>
+
+#include "fx_fused.h"
+#include "fx_pressure.h"
+
+namespace fx {
+namespace {
+
+constexpr int TX = 32, TY = 16, NT = TX * TY;
+
+enum { IN_ZERO = 0, IN_BUF = 1, IN_BUF_PROLONG = 2, IN_ZERO_PROLONG = 3 };
+
+struct ZArgs {
+  Dims dm;
+  Dims mid;
+  int zchunk;
+  const float* p_in;
+  const float* div_in;
+  float* div_out;
+  float* mid_div;
+  const float* mid_p;
+  float* p_out;
+  VelField vfin;
+  VelField vcur;
+  float* vmag;
+  int write_vmag;
+  int restrict_mid;
+};
+
+// x / 6 rounded to nearest, for every float x. For |x| in [2^-125, FLT_MAX] the
+// quotient is q0 = x * RN(1/6) corrected once by its exact residual (Markstein,
+// "IA-64 and Elementary Functions", 2000): r = fma(-q0, 6, x), q = fma(r, RN(1/6), q0).
+// An exhaustive check over all 2^32 inputs shows this equals the IEEE quotient on
+// that range; tiny, infinite and NaN inputs take the IEEE division.
+FX_DEV float div6(float x) {
+  const float ax = fabsf(x);
+  if (ax >= 0x1p-125f && ax <= 0x1.fffffep127f) {
+    const float r6 = 0x1.555556p-3f;  // RN(1/6)
+    const float q0 = x * r6;
+    const float e = fmaf(-q0, 6.0f, x);
+    return fmaf(e, r6, q0);
+  }
+  return x / 6.0f;
+}
+
+// Prolongation term of pressure-prolongation.wgsl.ts:42-43 at fine voxel (x,y,z).
+FX_DEV float prolong_sample(const Dims& mid, const float* __restrict__ mp, int x, int y, int z) {
+  const float px = ((float)x + 0.5f) * 0.5f - 0.5f;
+  const float py = ((float)y + 0.5f) * 0.5f - 0.5f;
+  const float pz = ((float)z + 0.5f) * 0.5f - 0.5f;
+  return tri_interp(mp, tri_corners(mid, px, py, pz));
+}
+
+template <int S, int IN, bool DIVV, bool PROJ>
+struct Frame {
+  static constexpr int H = S + (PROJ ? 1 : 0);
+  static constexpr int EX = TX + 2 * H;
+  static constexpr int EY = TY + 2 * H;
+  static constexpr int P = EX * EY;
+  static constexpr int RP = (P + NT - 1) / NT;
+  static constexpr bool stage0 = IN != IN_ZERO;
+  static constexpr int first = stage0 ? 0 : 1;  // first stage held in registers
+  // Shared planes (P floats each): 2 per published stage (stages first..S-1, and
+  // S when projecting), 2 each for vx and vy and 3 for the divergence when it is
+  // computed in the block.
+  static constexpr int pub_last = PROJ ? S : S - 1;
+  static constexpr int npub = pub_last >= first ? pub_last - first + 1 : 0;
+  static constexpr int floats = P * (2 * npub + (DIVV ? 7 : 0));
+};
+
+template <int S, int IN, bool DIVV, bool PROJ>
+__global__ void __launch_bounds__(NT, 1) k_zjacobi(ZArgs a) {
+  using Fr = Frame<S, IN, DIVV, PROJ>;
+  constexpr int H = Fr::H, EX = Fr::EX, EY = Fr::EY, P = Fr::P, RP = Fr::RP;
+  constexpr int dl = DIVV ? 1 : 0;
+  constexpr int L = S + (PROJ ? 1 : 0);
+  extern __shared__ float sm[];
+  const Dims dm = a.dm;
+  const int W = (int)dm.w, Hh = (int)dm.h, D = (int)dm.d;
+  const int tid = threadIdx.x + TX * threadIdx.y;
+  const int gx0 = (int)blockIdx.x * TX - H, gy0 = (int)blockIdx.y * TY - H;
+  const int za = (int)blockIdx.z * a.zchunk;
+  const int zb = min(za + a.zchunk, D);
+  const size_t plane = (size_t)W * (size_t)Hh;
+
+  // shared planes
+  auto pub = [&](int j, int buf) -> float* { return sm + ((j - Fr::first) * 2 + buf) * P; };
+  float* vxs = sm + 2 * Fr::npub * P;  // [2][P]
+  float* vys = vxs + 2 * P;            // [2][P]
+  float* dvs = vys + 2 * P;            // [3][P]
+
+  // per-position constants
+  int pidx[RP], dist[RP], gxr[RP], gyr[RP], gxy[RP];
+  bool valid[RP], indom[RP], xyint[RP];
+#pragma unroll
+  for (int r = 0; r < RP; ++r) {
+    const int p = tid + NT * r;
+    valid[r] = p < P;
+    const int lx = p % EX, ly = p / EX;
+    pidx[r] = p;
+    dist[r] = min(min(lx, EX - 1 - lx), min(ly, EY - 1 - ly));
+    const int gx = gx0 + lx, gy = gy0 + ly;
+    indom[r] = valid[r] && gx >= 0 && gy >= 0 && gx < W && gy < Hh;
+    xyint[r] = valid[r] && gx > 0 && gy > 0 && gx < W - 1 && gy < Hh - 1;
+    gxy[r] = indom[r] ? gx + W * gy : 0;
+    gxr[r] = gx;
+    gyr[r] = gy;
+  }
+  for (int k = tid; k < Fr::floats; k += NT) sm[k] = 0.0f;
+
+  // register rings: ring[j][r][0..2] = stage j at planes q_j-2, q_j-1, q_j
+  float ring[S + 1][RP][3];
+  float divr[RP][S + 1];  // divr[r][k] = divergence at plane (t - dl - k)
+  float vzr[RP][3];       // vz at planes t-2, t-1, t (divergence in block)
+#pragma unroll
+  for (int j = 0; j <= S; ++j)
+#pragma unroll
+    for (int r = 0; r < RP; ++r) ring[j][r][0] = ring[j][r][1] = ring[j][r][2] = 0.0f;
+#pragma unroll
+  for (int r = 0; r < RP; ++r) {
+#pragma unroll
+    for (int k = 0; k <= S; ++k) divr[r][k] = 0.0f;
+    vzr[r][0] = vzr[r][1] = vzr[r][2] = 0.0f;
+  }
+  __syncthreads();
+
+  const int t_begin = za - L;
+  const int t_end = zb - 1 + L + dl;
+
+  // Raw inputs of plane tt for this thread's positions, loaded one clock ahead.
+  float pre_v[RP], pre_a[RP], pre_b[RP], pre_c[RP];
+  auto fetch = [&](int tt) {
+    const bool t_in = tt >= 0 && tt < D;
+    const bool zint = tt > 0 && tt < D - 1;
+#pragma unroll
+    for (int r = 0; r < RP; ++r) {
+      pre_a[r] = pre_b[r] = pre_c[r] = pre_v[r] = 0.0f;
+      if (!(t_in && indom[r])) continue;
+      const size_t i = (size_t)gxy[r] + plane * (size_t)tt;
+      if (DIVV) {
+        pre_a[r] = __ldg(a.vfin.c[0] + i);
+        pre_b[r] = __ldg(a.vfin.c[1] + i);
+        pre_c[r] = __ldg(a.vfin.c[2] + i);
+      } else if (S >= 1) {
+        pre_a[r] = __ldg(a.div_in + i);
+      }
+      if (Fr::stage0) {
+        if (IN == IN_BUF) {
+          pre_v[r] = __ldg(a.p_in + i);
+        } else if (zint && xyint[r]) {
+          const float ps = prolong_sample(a.mid, a.mid_p, gxr[r], gyr[r], tt);
+          pre_v[r] = (IN == IN_BUF_PROLONG) ? __ldg(a.p_in + i) + ps : 0.0f + ps;
+        }
+      }
+    }
+  };
+  fetch(t_begin);
+
+  for (int t = t_begin; t <= t_end; ++t) {
+    const int b = t & 1;
+
+    // ---- consume the prefetched plane t
+    if (DIVV) {
+#pragma unroll
+      for (int r = 0; r < RP; ++r) {
+        if (valid[r]) {
+          vxs[b * P + pidx[r]] = pre_a[r];
+          vys[b * P + pidx[r]] = pre_b[r];
+        }
+        vzr[r][0] = vzr[r][1];
+        vzr[r][1] = vzr[r][2];
+        vzr[r][2] = pre_c[r];
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < RP; ++r) {
+#pragma unroll
+        for (int k = S; k > 0; --k) divr[r][k] = divr[r][k - 1];
+        divr[r][0] = pre_a[r];
+      }
+    }
+    if (Fr::stage0) {
+#pragma unroll
+      for (int r = 0; r < RP; ++r) {
+        ring[0][r][0] = ring[0][r][1];
+        ring[0][r][1] = ring[0][r][2];
+        ring[0][r][2] = pre_v[r];
+        if (valid[r] && Fr::pub_last >= 0) pub(0, b)[pidx[r]] = pre_v[r];
+      }
+    }
+    // ---- issue the loads of plane t + 1; they complete while this clock computes
+    if (t < t_end) fetch(t + 1);
+
+    // ---- divergence at plane t - 1 (in block)
+    if (DIVV) {
+      const int q = t - 1;
+      const int qb = q & 1;
+      const bool qint = q > 0 && q < D - 1;
+      const int slot = ((q % 3) + 3) % 3;
+#pragma unroll
+      for (int r = 0; r < RP; ++r) {
+        float d = 0.0f;
+        if (qint && xyint[r] && dist[r] >= 1) {
+          const int c = pidx[r];
+          const float* vx = vxs + qb * P;
+          const float* vy = vys + qb * P;
+          const float ddx = vx[c + 1] - vx[c - 1];
+          const float ddy = vy[c + EX] - vy[c - EX];
+          const float ddz = vzr[r][2] - vzr[r][0];
+          d = (ddx + ddy + ddz) * 0.5f;
+        }
+#pragma unroll
+        for (int k = S; k > 0; --k) divr[r][k] = divr[r][k - 1];
+        divr[r][0] = d;
+        if (valid[r]) dvs[slot * P + pidx[r]] = d;
+        if (q >= za && q < zb && dist[r] >= H && indom[r]) a.div_out[(size_t)gxy[r] + plane * (size_t)q] = d;
+      }
+      // restriction of fine planes q-2, q-1 (published at clocks t-2, t-1)
+      const int q1 = q - 1;
+      if (a.restrict_mid && q1 >= za && q1 < zb && (q1 & 1) == 1 && tid < (TX / 2) * (TY / 2)) {
+        const int mx_ = (gx0 + H) / 2 + (tid % (TX / 2)), my_ = (gy0 + H) / 2 + (tid / (TX / 2)), mz_ = q1 / 2;
+        if (mx_ < (int)a.mid.w && my_ < (int)a.mid.h && mz_ < (int)a.mid.d) {
+          float out = 0.0f;
+          if (!(mx_ == 0 || my_ == 0 || mz_ == 0 || mx_ == (int)a.mid.w - 1 || my_ == (int)a.mid.h - 1 || mz_ == (int)a.mid.d - 1)) {
+            const float* d0 = dvs + (((q1 - 1) % 3 + 3) % 3) * P;
+            const float* d1 = dvs + ((q1 % 3 + 3) % 3) * P;
+            const int c = (2 * mx_ - gx0) + (2 * my_ - gy0) * EX;
+            float sum = 0.0f;
+            sum += d0[c];
+            sum += d0[c + 1];
+            sum += d0[c + EX];
+            sum += d0[c + EX + 1];
+            sum += d1[c];
+            sum += d1[c + 1];
+            sum += d1[c + EX];
+            sum += d1[c + EX + 1];
+            out = sum * 0.125f;
+          }
+          a.mid_div[flat(a.mid, (uint32_t)mx_, (uint32_t)my_, (uint32_t)mz_)] = out;
+        }
+      }
+    }
+
+    // ---- sweeps: stage j at plane q_j = t - dl - j
+#pragma unroll
+    for (int j = 1; j <= S; ++j) {
+      const int q = t - dl - j;
+      const bool qint = q > 0 && q < D - 1;
+      const float* xy = (j - 1 >= Fr::first) ? pub(j - 1, (q & 1)) : nullptr;
+#pragma unroll
+      for (int r = 0; r < RP; ++r) {
+        float v = 0.0f;
+        if (qint && xyint[r] && dist[r] >= j) {
+          const float dd = divr[r][j];
+          if (j == 1 && !Fr::stage0) {
+            v = div6(0.0f - dd);
+          } else {
+            const int c = pidx[r];
+            const float s = xy[c + 1] + xy[c - 1] + xy[c + EX] + xy[c - EX] + ring[j - 1][r][2] + ring[j - 1][r][0];
+            v = div6(s - dd);
+          }
+        }
+        ring[j][r][0] = ring[j][r][1];
+        ring[j][r][1] = ring[j][r][2];
+        ring[j][r][2] = v;
+        if (j <= Fr::pub_last && valid[r]) pub(j, q & 1)[pidx[r]] = v;
+      }
+    }
+
+    // ---- last stage to global, projection
+    {
+      const int q = t - dl - S;
+      if (q >= za && q < zb) {
+#pragma unroll
+        for (int r = 0; r < RP; ++r)
+          if (dist[r] >= H && indom[r]) a.p_out[(size_t)gxy[r] + plane * (size_t)q] = ring[S][r][2];
+      }
+    }
+    if (PROJ) {
+      const int q = t - dl - S - 1;
+      if (q >= za && q < zb) {
+        const bool qint = q > 0 && q < D - 1;
+        const float* xy = pub(S, q & 1);
+#pragma unroll
+        for (int r = 0; r < RP; ++r) {
+          if (dist[r] >= H && indom[r]) {
+            const size_t i = (size_t)gxy[r] + plane * (size_t)q;
+            float ox = 0.f, oy = 0.f, oz = 0.f;
+            if (qint && xyint[r]) {
+              const int c = pidx[r];
+              const float gx = (xy[c + 1] - xy[c - 1]) * 0.5f;
+              const float gy = (xy[c + EX] - xy[c - EX]) * 0.5f;
+              const float gz = (ring[S][r][2] - ring[S][r][0]) * 0.5f;
+              ox = __ldg(a.vfin.c[0] + i) - gx;
+              oy = __ldg(a.vfin.c[1] + i) - gy;
+              oz = __ldg(a.vfin.c[2] + i) - gz;
+            }
+            a.vcur.c[0][i] = ox;
+            a.vcur.c[1][i] = oy;
+            a.vcur.c[2][i] = oz;
+            if (a.write_vmag) a.vmag[i] = length3(ox, oy, oz);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int S, int IN, bool DIVV, bool PROJ>
+cudaError_t launch_z(cudaStream_t s, const ZArgs& a) {
+  using Fr = Frame<S, IN, DIVV, PROJ>;
+  const size_t smem = (size_t)Fr::floats * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(k_zjacobi<S, IN, DIVV, PROJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((a.dm.w + TX - 1) / TX, (a.dm.h + TY - 1) / TY, (a.dm.d + a.zchunk - 1) / a.zchunk);
+  k_zjacobi<S, IN, DIVV, PROJ><<<grid, dim3(TX, TY), smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <int IN, bool DIVV, bool PROJ>
+cudaError_t launch_s(cudaStream_t s, int sweeps, const ZArgs& a) {
+  switch (sweeps) {
+    case 0: return launch_z<0, IN, DIVV, PROJ>(s, a);
+    case 1: return launch_z<1, IN, DIVV, PROJ>(s, a);
+    case 2: return launch_z<2, IN, DIVV, PROJ>(s, a);
+    case 3: return launch_z<3, IN, DIVV, PROJ>(s, a);
+    default: return launch_z<4, IN, DIVV, PROJ>(s, a);
+  }
+}
+
+__global__ void k_div6_check(uint32_t hi_base, unsigned long long* bad) {
+  const uint32_t u = hi_base + blockIdx.x * blockDim.x + threadIdx.x;
+  const float x = __uint_as_float(u);
+  if (x != x) return;
+  const float a = div6(x), b = x / 6.0f;
+  if (__float_as_uint(a) != __float_as_uint(b)) atomicAdd(bad, 1ull);
+}
+
+}  // namespace
+
+cudaError_t zpass_launch(cudaStream_t s, const ZPass& p) {
+  ZArgs a{};
+  a.dm = p.dm;
+  a.mid = p.mid;
+  a.zchunk = p.zchunk > 0 ? p.zchunk : 64;
+  a.p_in = p.p_in;
+  a.div_in = p.div_in;
+  a.div_out = p.div_out;
+  a.mid_div = p.mid_div;
+  a.mid_p = p.mid_p;
+  a.p_out = p.p_out;
+  a.vfin = p.vfin;
+  a.vcur = p.vcur;
+  a.vmag = p.vmag;
+  a.write_vmag = p.write_vmag;
+  a.restrict_mid = p.restrict_mid;
+  const int S = std::min(p.sweeps, 4);
+  if (p.div_from_velocity) {
+    if (p.input != ZIN_ZERO || p.project || S < 1) return cudaErrorInvalidValue;
+    return launch_s<IN_ZERO, true, false>(s, S, a);
+  }
+  switch (p.input) {
+    case ZIN_BUF:
+      return p.project ? launch_s<IN_BUF, false, true>(s, S, a) : launch_s<IN_BUF, false, false>(s, S, a);
+    case ZIN_BUF_PROLONG:
+      return p.project ? launch_s<IN_BUF_PROLONG, false, true>(s, S, a) : launch_s<IN_BUF_PROLONG, false, false>(s, S, a);
+    case ZIN_ZERO_PROLONG:
+      return p.project ? launch_s<IN_ZERO_PROLONG, false, true>(s, S, a) : launch_s<IN_ZERO_PROLONG, false, false>(s, S, a);
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+namespace {
+int env_int(const char* name, int dflt, int lo, int hi) {
+  const char* v = std::getenv(name);
+  if (!v || !*v) return dflt;
+  const int x = std::atoi(v);
+  return (x >= lo && x <= hi) ? x : dflt;
+}
+}  // namespace
+
+int zpass_max_sweeps() {
+  static const int k = env_int("FENIX_ZPASS_SWEEPS", 4, 1, 4);
+  return k;
+}
+
+int zpass_zchunk() {
+  static const int z = env_int("FENIX_ZPASS_ZCHUNK", 64, 8, 4096) & ~1;
+  return z;
+}
+
+cudaError_t div6_exhaustive_check(unsigned long long* host_bad) {
+  unsigned long long* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(unsigned long long));
+  if (e != cudaSuccess) return e;
+  cudaMemset(d, 0, sizeof(unsigned long long));
+  // 2^32 inputs in 256 launches of 2^24 (65536 blocks of 256 threads)
+  for (uint32_t k = 0; k < 256; ++k) k_div6_check<<<65536, 256>>>(k << 24, d);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(host_bad, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return e;
+}
+
+}  // namespace fx

@@ -1,0 +1,50 @@
+// Fine-level pressure passes of the fused path (fx_pressure.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fx_kernels.h"
+
+namespace fx {
+
+// Stage-0 input of a pass.
+enum ZInput {
+  ZIN_ZERO = 0,          // the cleared buffer: the first sweep is (0 - div) / 6
+  ZIN_BUF = 1,           // p_in
+  ZIN_BUF_PROLONG = 2,   // p_in + prolongation of mid_p (boundary 0)
+  ZIN_ZERO_PROLONG = 3,  // 0 + prolongation of mid_p (boundary 0)
+};
+
+struct ZPass {
+  Dims dm;
+  Dims mid;
+  int zchunk;            // planes per block (0 = default)
+  int sweeps;            // 0..4
+  ZInput input;
+  bool div_from_velocity;  // compute the divergence of vfin (and write div_out, mid_div)
+  bool project;            // finish with the projection of vfin into vcur
+  int restrict_mid;        // with div_from_velocity: also write the fine->mid restriction
+  const float* p_in;
+  const float* div_in;
+  float* div_out;
+  float* mid_div;
+  const float* mid_p;
+  float* p_out;
+  VelField vfin;
+  VelField vcur;
+  float* vmag;
+  int write_vmag;
+};
+
+cudaError_t zpass_launch(cudaStream_t s, const ZPass& p);
+
+// Tuning of the fine passes: sweeps fused per pass (1..4) and planes per block.
+// Defaults come from measurement; FENIX_ZPASS_SWEEPS / FENIX_ZPASS_ZCHUNK override.
+int zpass_max_sweeps();
+int zpass_zchunk();
+
+// Counts the floats x (all 2^32 bit patterns, NaNs excluded) for which the
+// pressure kernels' division by 6 differs from the IEEE quotient x / 6.0f.
+cudaError_t div6_exhaustive_check(unsigned long long* host_bad);
+
+}  // namespace fx

@@ -15,6 +15,7 @@
 #include "../../include/fenix_cuda.h"
 #include "fx_fused.h"
 #include "fx_kernels.h"
+#include "fx_pressure.h"
 
 using namespace fx;
 
@@ -914,6 +915,13 @@ fx_status fx_test_pinned_sincos(const float* host_x, float* host_out, uint32_t n
   cudaFree(dx);
   cudaFree(dout);
   return st;
+}
+
+// Test hook: exhaustive comparison of the pressure kernels' division by 6 with
+// the IEEE division on the device. Returns the mismatch count in *bad.
+fx_status fx_test_div6_exhaustive(unsigned long long* bad) {
+  if (!bad) return FX_ERR_INVALID_ARGUMENT;
+  return div6_exhaustive_check(bad) == cudaSuccess ? FX_OK : FX_ERR_CUDA;
 }
 
 }  // extern "C"

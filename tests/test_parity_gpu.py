@@ -173,3 +173,16 @@ def test_pinned_sincos_matches_oracle():
                                        out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), x.size, cosine)
         assert st == 0
         np.testing.assert_array_equal(out.view(np.uint32), ref(x).view(np.uint32))
+
+
+def test_division_by_six_is_exact_for_every_float():
+    """The pressure kernels divide by 6 with a residual-corrected product; it must
+    equal the IEEE quotient x / 6.0f for all 2^32 inputs (NaNs excluded)."""
+    import ctypes
+
+    from fenix_b200 import _lib
+
+    lib = _lib.load()
+    bad = ctypes.c_uint64(123)
+    assert lib.fx_test_div6_exhaustive(ctypes.byref(bad)) == 0
+    assert bad.value == 0
