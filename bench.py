@@ -308,7 +308,8 @@ def main():
     clock_info = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     act = sim.readActiveCounters()
-    kernels_last = sim.stats()["kernelsPerStep"]
+    st_timed = sim.stats()
+    kernels_last = st_timed["kernelsPerStep"]
     ms_max = ms
     voxel_steps = act["voxelSteps"]
     if pg:
@@ -397,7 +398,7 @@ def main():
             "config": {
                 "workload": f"plume_{args.size}: {args.size}^3 grid, 4 floor plumes (scalar+velocity+igniter each), seeded "
                             f"developed-plume start, 4/4/4/4/20 sweeps, dt 1/60, f32, parity semantics",
-                "kernels": args.kernels, "active_fraction": active_mean / n, "global_batch": world, "seq_len": 0,
+                "kernels": args.kernels, "cuda_graph": bool(st_timed.get("graphReplay")), "active_fraction": active_mean / n, "global_batch": world, "seq_len": 0,
                 "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (about 2 GB of fields per step)",
             },
             "roofline": roofline, "kernels": kernel_table, "cpu_baseline": cpu, "parity_full_size": parity, "e2e": e2e,

@@ -141,7 +141,7 @@ class FxStats(Structure):
         ("brick_count", c_uint32),
         ("active_bricks", c_uint32),
         ("kernels_per_step", c_uint32),
-        ("reserved", c_uint32),
+        ("flags", c_uint32),
     ]
 
 

@@ -223,29 +223,40 @@ FX_DEV float tri_interp_clamped(const float* __restrict__ f, const Tri& c, float
   return mixv(mixv(x00, x10, c.fy), mixv(x01, x11, c.fy), c.fz);
 }
 
+// The start sample of the back-trace sits on the voxel centre: every weight of
+// the trilinear mix is 0, so the mix equals the voxel's own (clamped) value up to
+// the sign of a zero, and c - v*dt comes out the same (c >= 0.5). For fields
+// without NaN this reads one value instead of eight.
+constexpr int kAdvZ = 4;
+
 __global__ void __launch_bounds__(256) k_advect_velocity(Dims dm, const Params* __restrict__ Pp, VelField src, VelField dst) {
-  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
-  const uint32_t z = blockIdx.z * blockDim.z + threadIdx.z;
-  if (x >= dm.w || y >= dm.h || z >= dm.d) return;
-  const uint32_t i = flat(dm, x, y, z);
-  if (is_boundary(dm, x, y, z)) {
-    dst.c[0][i] = 0.0f;
-    dst.c[1][i] = 0.0f;
-    dst.c[2][i] = 0.0f;
-    return;
-  }
+  const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z0 = blockIdx.z * kAdvZ;
+  if (x >= dm.w || y >= dm.h) return;
   const float dt = Pp->dt;
   const float lim = speed_limit(*Pp);
-  const float cx = (float)x + 0.5f, cy = (float)y + 0.5f, cz = (float)z + 0.5f;
-  const Tri c0 = tri_corners(dm, cx - 0.5f, cy - 0.5f, cz - 0.5f);
-  const float v0x = tri_interp_clamped(src.c[0], c0, lim), v0y = tri_interp_clamped(src.c[1], c0, lim), v0z = tri_interp_clamped(src.c[2], c0, lim);
-  const float bx = cx - v0x * dt, by = cy - v0y * dt, bz = cz - v0z * dt;
-  const Tri c1 = tri_corners(dm, bx - 0.5f, by - 0.5f, bz - 0.5f);
   const float damp = 1.0f - dt * 0.025f;
-  dst.c[0][i] = tri_interp_clamped(src.c[0], c1, lim) * damp;
-  dst.c[1][i] = tri_interp_clamped(src.c[1], c1, lim) * damp;
-  dst.c[2][i] = tri_interp_clamped(src.c[2], c1, lim) * damp;
+  const bool xyint = x > 0 && y > 0 && x < dm.w - 1 && y < dm.h - 1;
+#pragma unroll
+  for (int k = 0; k < kAdvZ; ++k) {
+    const uint32_t z = z0 + k;
+    if (z >= dm.d) break;
+    const uint32_t i = flat(dm, x, y, z);
+    if (!xyint || z == 0 || z == dm.d - 1) {
+      dst.c[0][i] = 0.0f;
+      dst.c[1][i] = 0.0f;
+      dst.c[2][i] = 0.0f;
+      continue;
+    }
+    const float cx = (float)x + 0.5f, cy = (float)y + 0.5f, cz = (float)z + 0.5f;
+    const float v0x = clampv(__ldg(src.c[0] + i), -lim, lim);
+    const float v0y = clampv(__ldg(src.c[1] + i), -lim, lim);
+    const float v0z = clampv(__ldg(src.c[2] + i), -lim, lim);
+    const float bx = cx - v0x * dt, by = cy - v0y * dt, bz = cz - v0z * dt;
+    const Tri c1 = tri_corners(dm, bx - 0.5f, by - 0.5f, bz - 0.5f);
+    dst.c[0][i] = tri_interp_clamped(src.c[0], c1, lim) * damp;
+    dst.c[1][i] = tri_interp_clamped(src.c[1], c1, lim) * damp;
+    dst.c[2][i] = tri_interp_clamped(src.c[2], c1, lim) * damp;
+  }
 }
 
 // -------------------------------------------------------------- scalar advection
@@ -273,8 +284,11 @@ __global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3
       if (inside && active) {
         const float dt = P.dt;
         const float cx = (float)x + 0.5f, cy = (float)y + 0.5f, cz = (float)z + 0.5f;
-        const Tri c0 = tri_corners(dm, cx - 0.5f, cy - 0.5f, cz - 0.5f);
-        const float vx = tri_interp(vel.c[0], c0), vy = tri_interp(vel.c[1], c0), vz = tri_interp(vel.c[2], c0);
+        // Samples at the voxel centre (the back-trace start and `original`) equal the
+        // voxel's values up to the sign of a zero, which neither c - v*dt nor the
+        // max(0, .) of every output can see (NaN-free fields).
+        const uint32_t ic = flat(dm, x, y, z);
+        const float vx = __ldg(vel.c[0] + ic), vy = __ldg(vel.c[1] + ic), vz = __ldg(vel.c[2] + ic);
         const float bxp = cx - vx * dt, byp = cy - vy * dt, bzp = cz - vz * dt;
         const float spx = bxp - 0.5f, spy = byp - 0.5f, spz = bzp - 0.5f;
         const Tri cs = tri_corners(dm, spx, spy, spz);
@@ -287,7 +301,7 @@ __global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3
           for (int f = 0; f < 4; ++f) {
             const float predicted = tri_interp(src.f[f], cs);
             const float recovered = tri_interp(src.f[f], cr);
-            const float original = tri_interp(src.f[f], c0);
+            const float original = __ldg(src.f[f] + ic);
             const float corrected = predicted + 0.5f * (original - recovered);
             out[f] = clampv(corrected, mn(original, predicted), mx(original, predicted));
           }
@@ -487,29 +501,47 @@ __global__ void __launch_bounds__(256) k_confinement(Dims dm, uint3 bc, const Pa
 }
 
 // Projection (project-velocity.wgsl.ts:21-43) with |v|
-// (compute-debug-fields.wgsl.ts:18-25) fused when it is due.
+// (compute-debug-fields.wgsl.ts:18-25) fused when it is due. A thread computes
+// a column of kProjZ voxels and reuses the z neighbours of the pressure.
+constexpr int kProjZ = 8;
+
 __global__ void __launch_bounds__(256) k_project(Dims dm, VelField vs, const float* __restrict__ p, VelField vd, float* __restrict__ vmag,
                                                  int write_vmag) {
-  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
-  const uint32_t z = blockIdx.z * blockDim.z + threadIdx.z;
-  if (x >= dm.w || y >= dm.h || z >= dm.d) return;
-  const uint32_t i = flat(dm, x, y, z);
-  float ox = 0.f, oy = 0.f, oz = 0.f;
-  if (!is_boundary(dm, x, y, z)) {
-    const uint32_t W1 = dm.w - 1u, H1 = dm.h - 1u, D1 = dm.d - 1u;
-    const float gx = (__ldg(p + flat(dm, inc(x, W1), y, z)) - __ldg(p + flat(dm, dec(x), y, z))) * 0.5f;
-    const float gy = (__ldg(p + flat(dm, x, inc(y, H1), z)) - __ldg(p + flat(dm, x, dec(y), z))) * 0.5f;
-    const float gz = (__ldg(p + flat(dm, x, y, inc(z, D1))) - __ldg(p + flat(dm, x, y, dec(z)))) * 0.5f;
-    ox = __ldg(vs.c[0] + i) - gx;
-    oy = __ldg(vs.c[1] + i) - gy;
-    oz = __ldg(vs.c[2] + i) - gz;
+  const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z0 = blockIdx.z * kProjZ;
+  if (x >= dm.w || y >= dm.h) return;
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  const uint32_t base = x + dm.w * y;
+  const bool xyint = x > 0 && y > 0 && x < dm.w - 1 && y < dm.h - 1;
+  float pz[kProjZ + 2];
+  if (xyint) {
+#pragma unroll
+    for (int k = 0; k < kProjZ + 2; ++k) {
+      const int z = (int)z0 + k - 1;
+      pz[k] = (z >= 0 && z < (int)dm.d) ? __ldg(p + base + sz * (uint32_t)z) : 0.0f;
+    }
   }
-  vd.c[0][i] = ox;
-  vd.c[1][i] = oy;
-  vd.c[2][i] = oz;
-  if (write_vmag) vmag[i] = length3(ox, oy, oz);
+#pragma unroll
+  for (int k = 0; k < kProjZ; ++k) {
+    const uint32_t z = z0 + k;
+    if (z >= dm.d) break;
+    const uint32_t i = base + sz * z;
+    float ox = 0.f, oy = 0.f, oz = 0.f;
+    if (xyint && z > 0 && z < dm.d - 1) {
+      const float gx = (__ldg(p + i + 1) - __ldg(p + i - 1)) * 0.5f;
+      const float gy = (__ldg(p + i + sy) - __ldg(p + i - sy)) * 0.5f;
+      const float gz = (pz[k + 2] - pz[k]) * 0.5f;
+      ox = __ldg(vs.c[0] + i) - gx;
+      oy = __ldg(vs.c[1] + i) - gy;
+      oz = __ldg(vs.c[2] + i) - gz;
+    }
+    vd.c[0][i] = ox;
+    vd.c[1][i] = oy;
+    vd.c[2][i] = oz;
+    if (write_vmag) vmag[i] = length3(ox, oy, oz);
+  }
 }
+
+inline dim3 proj_grid(Dims d) { return dim3((d.w + 31) / 32, (d.h + 7) / 8, (d.d + kProjZ - 1) / kProjZ); }
 
 // Rebuilds the per-brick bookkeeping after the fields were written from the host:
 // the non-zero bits of the three scalar buffers and the summary of the current set.
@@ -609,7 +641,7 @@ void injection_bricks(const FusedStep& st, std::vector<uint8_t>& mark, std::vect
 
 size_t fused_work_bytes(Dims, uint3 bricks) {
   const size_t nb = (size_t)bricks.x * bricks.y * bricks.z;
-  return 8 * align256(nb) + 3 * align256(nb * 4) + align256(16 * 4);
+  return 8 * align256(nb) + 3 * align256(nb * 4) + align256(16 * 4) + align256(96 * 4);
 }
 
 void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks) {
@@ -634,6 +666,7 @@ void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks) {
   w.list_next = (uint32_t*)take((size_t)w.nb * 4);
   w.list_inj = (uint32_t*)take((size_t)w.nb * 4);
   w.counters = (uint32_t*)take(16 * 4);
+  w.mg_bar = (unsigned*)take(96 * 4);
 }
 
 fx_status fused_init(FusedWork& w, cudaStream_t) {
@@ -644,7 +677,10 @@ fx_status fused_init(FusedWork& w, cudaStream_t) {
 }
 
 fx_status fused_reset(FusedWork& w, cudaStream_t) {
+  // The arena was cleared: every brick is zero, and the device copy of the
+  // injection list is gone.
   w.valid = true;
+  w.uploaded_list.clear();
   return FX_OK;
 }
 
@@ -654,6 +690,8 @@ fx_status fused_invalidate(FusedWork& w, cudaStream_t) {
 }
 
 void fused_release(FusedWork& w) {
+  for (auto& kv : w.graphs) cudaGraphExecDestroy(kv.second.exec);
+  w.graphs.clear();
   if (w.inj_event) cudaEventDestroy(w.inj_event);
   w.inj_event = nullptr;
   if (w.host_list_inj) cudaFreeHost(w.host_list_inj);
@@ -705,7 +743,102 @@ int FusedWork::next_event() {
   return timing_next++;
 }
 
+#define FX_CK(call)                              \
+  do {                                           \
+    cudaError_t e_ = (call);                     \
+    if (e_ != cudaSuccess) {                     \
+      out.error = std::string(#call) + ": " + cudaGetErrorString(e_); \
+      return FX_ERR_CUDA;                        \
+    }                                            \
+  } while (0)
+
+fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, FusedResult& out);
+
 fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
+  cudaStream_t s = st.stream;
+  const Dims dm = st.dm;
+  const uint3 bc = st.bricks;
+  const uint32_t nb = w.nb;
+  const int cur = st.cur_index, next = cur ^ 1;
+  uint32_t launches = 0;
+  const uint32_t brick_grid = std::max<uint32_t>(1, std::min<uint32_t>(nb, 148u * 8u));
+  uint32_t* c_inj = w.counters + 3;
+
+  if (!w.valid) {
+    Timed tm(w, s, "fused_rebuild");
+    k_rebuild<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.cur, st.next, st.scratch, w.summary_set[cur], w.nz_set[cur], w.nz_set[next], w.nz_t);
+    ++launches;
+    w.valid = true;
+  }
+
+  // 1. injection over the reachable bricks: the list is built on the host and
+  // uploaded only when it changes.
+  injection_bricks(st, w.host_mark, w.host_list);
+  const uint32_t ninj = (uint32_t)w.host_list.size();
+  if (ninj && w.host_list != w.uploaded_list) {
+    FX_CK(cudaEventSynchronize(w.inj_event));
+    std::memcpy(w.host_list_inj, w.host_list.data(), ninj * 4);
+    w.host_list_inj[nb] = ninj;
+    FX_CK(cudaMemcpyAsync(w.list_inj, w.host_list_inj, ninj * 4, cudaMemcpyHostToDevice, s));
+    FX_CK(cudaMemcpyAsync(c_inj, w.host_list_inj + nb, 4, cudaMemcpyHostToDevice, s));
+    FX_CK(cudaEventRecord(w.inj_event, s));
+    w.uploaded_list = w.host_list;
+  }
+
+  // The device part of the step, captured once per configuration and replayed.
+  const bool graphs = w.use_graphs && !w.timing;
+  uint64_t key = 0;
+  auto mix_key = [&](uint64_t v) { key = (key ^ v) * 0x100000001b3ull; };
+  key = 0xcbf29ce484222325ull;
+  mix_key((uint64_t)st.cur_index);
+  mix_key(ninj > 0);
+  mix_key((uint64_t)(uintptr_t)st.sources);
+  mix_key(st.nsrc);
+  mix_key((uint64_t)st.advect_mode);
+  mix_key(st.vort_on);
+  mix_key(st.pressure_on);
+  mix_key(st.debug_on);
+  mix_key(st.debug_fields);
+  mix_key((uint64_t)st.last_p);
+  for (int k = 0; k < 7; ++k) mix_key((uint64_t)st.q[k]);
+  if (graphs) {
+    auto it = w.graphs.find(key);
+    if (it == w.graphs.end()) {
+      cudaGraph_t g = nullptr;
+      FX_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+      FusedResult tmp;
+      const fx_status cst = fused_sequence(w, st, ninj, tmp);
+      const cudaError_t ce = cudaStreamEndCapture(s, &g);
+      if (cst != FX_OK || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        w.use_graphs = false;  // capture unsupported here: launch directly from now on
+        w.graph_note = "capture failed: " + (cst != FX_OK ? tmp.error : std::string(cudaGetErrorString(ce)));
+        return fused_sequence(w, st, ninj, out);
+      }
+      cudaGraphExec_t ex = nullptr;
+      const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) {
+        cudaGetLastError();
+        w.use_graphs = false;
+        w.graph_note = std::string("instantiate failed: ") + cudaGetErrorString(ie);
+        return fused_sequence(w, st, ninj, out);
+      }
+      it = w.graphs.emplace(key, FusedWork::GraphEntry{ex, tmp}).first;
+    }
+    FX_CK(cudaGraphLaunch(it->second.exec, s));
+    out = it->second.result;
+    out.launches += launches;
+    out.graph = true;
+    return FX_OK;
+  }
+  const fx_status r = fused_sequence(w, st, ninj, out);
+  out.launches += launches;
+  return r;
+}
+
+fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, FusedResult& out) {
   cudaStream_t s = st.stream;
   const Dims dm = st.dm;
   const uint3 bc = st.bricks;
@@ -716,35 +849,10 @@ fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
   uint32_t* c_adv = w.counters + 0;
   uint32_t* c_next = w.counters + 1;
   uint32_t* c_inj = w.counters + 3;
-#define FX_CK(call)                              \
-  do {                                           \
-    cudaError_t e_ = (call);                     \
-    if (e_ != cudaSuccess) {                     \
-      out.error = std::string(#call) + ": " + cudaGetErrorString(e_); \
-      return FX_ERR_CUDA;                        \
-    }                                            \
-  } while (0)
-
-  if (!w.valid) {
-    Timed tm(w, s, "fused_rebuild");
-    k_rebuild<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.cur, st.next, st.scratch, w.summary_set[cur], w.nz_set[cur], w.nz_set[next], w.nz_t);
-    ++launches;
-    w.valid = true;
-  }
-
-  // 1. injection over the reachable bricks
-  injection_bricks(st, w.host_mark, w.host_list);
-  const uint32_t ninj = (uint32_t)w.host_list.size();
   if (ninj) {
-    FX_CK(cudaEventSynchronize(w.inj_event));
-    std::memcpy(w.host_list_inj, w.host_list.data(), ninj * 4);
-    w.host_list_inj[nb] = ninj;
-    FX_CK(cudaMemcpyAsync(w.list_inj, w.host_list_inj, ninj * 4, cudaMemcpyHostToDevice, s));
-    FX_CK(cudaMemcpyAsync(c_inj, w.host_list_inj + nb, 4, cudaMemcpyHostToDevice, s));
-    FX_CK(cudaEventRecord(w.inj_event, s));
     Timed tm(w, s, "fused_inject");
-    k_inject<<<std::min<uint32_t>(ninj, brick_grid), kBrickThreads, 0, s>>>(dm, bc, st.params, st.sources, st.nsrc, w.list_inj, c_inj, st.cur,
-                                                                            st.vcur, w.summary_set[cur], w.nz_set[cur]);
+    k_inject<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.sources, st.nsrc, w.list_inj, c_inj, st.cur, st.vcur,
+                                                   w.summary_set[cur], w.nz_set[cur]);
     ++launches;
   }
 
@@ -758,7 +866,7 @@ fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
   // 3. velocity advection (dense)
   {
     Timed tm(w, s, "fused_advect_velocity");
-    k_advect_velocity<<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, st.params, st.vcur, st.vscr);
+    k_advect_velocity<<<dim3((dm.w + 31) / 32, (dm.h + 7) / 8, (dm.d + kAdvZ - 1) / kAdvZ), dim3(32, 8, 1), 0, s>>>(dm, st.params, st.vcur, st.vscr);
     ++launches;
   }
   // 4. scalar advection over the list
@@ -821,130 +929,193 @@ fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
     FX_CK(cudaMemsetAsync(M.p[0], 0, (size_t)M.dm.w * M.dm.h * M.dm.d * sizeof(float), s));
     FX_CK(cudaMemsetAsync(C.p[0], 0, (size_t)C.dm.w * C.dm.h * C.dm.d * sizeof(float), s));
 
-    // Plan the fine passes: pre-smoothing in groups of <= 4 sweeps (the first one
-    // also computes the divergence), post-smoothing in groups of <= 4 sweeps (the
-    // first adds the prolongation, the last finishes with the projection).
-    struct Plan {
-      int sweeps;
-      ZInput input;
-      bool divv, proj;
-    };
-    std::vector<Plan> pre, post;
-    const int kmax = zpass_max_sweeps();
-    for (int left = m; left > 0;) {
-      const int k = std::min(left, kmax);
-      pre.push_back({k, pre.empty() ? ZIN_ZERO : ZIN_BUF, pre.empty(), false});
-      left -= k;
-    }
-    {
-      const ZInput first_in = (m & 1) ? ZIN_BUF : (m == 0 ? ZIN_ZERO_PROLONG : ZIN_BUF_PROLONG);
-      if (n == 0) {
-        post.push_back({0, first_in, false, true});
-      } else {
-        for (int left = n; left > 0;) {
-          const int k = std::min(left, kmax);
-          post.push_back({k, post.empty() ? first_in : ZIN_BUF, false, left - k == 0});
-          left -= k;
-        }
-      }
-    }
-    // Output buffers: the last pass writes p[last]; going backwards the passes
-    // alternate with the other buffer, so no pass reads the buffer it writes.
-    const size_t npass = pre.size() + post.size();
-    std::vector<float*> outs(npass);
-    for (size_t i = npass; i-- > 0;)
-      outs[i] = (i + 1 == npass) ? F.p[last_p] : (outs[i + 1] == F.p[last_p] ? F.p[last_p ^ 1] : F.p[last_p]);
-    size_t pi = 0;
-    const float* chain = nullptr;  // the latest fine pressure (nullptr: the cleared buffer)
-    if (m == 0) {
-      Timed tm(w, s, "fused_divergence");
-      plain_divergence(s, dm, *vfinal, F.div);
-      ++launches;
-    }
-    for (const Plan& pl : pre) {
-      ZPass zp{};
-      zp.dm = dm;
-      zp.mid = M.dm;
-      zp.sweeps = pl.sweeps;
-      zp.zchunk = zpass_zchunk();
-      zp.input = pl.input;
-      zp.div_from_velocity = pl.divv;
-      zp.project = false;
-      zp.restrict_mid = (pl.divv && fuse_restrict) ? 1 : 0;
-      zp.p_in = chain;
-      zp.div_in = F.div;
-      zp.div_out = F.div;
-      zp.mid_div = M.div;
-      zp.p_out = outs[pi];
-      zp.vfin = *vfinal;
-      Timed tm(w, s, pl.divv ? "fused_zpass_div_pre" : "fused_zpass_pre");
-      FX_CK(zpass_launch(s, zp));
-      ++launches;
-      chain = outs[pi++];
-    }
-    if (m == 0 || !fuse_restrict) {
-      Timed tm(w, s, "fused_restrict");
-      plain_restrict(s, F.dm, M.dm, F.div, M.div);
-      ++launches;
-    }
-    // mid and coarse levels (sweep by sweep)
-    auto smooth = [&](const LevelBuf& L, int iters, int start, const char* name) {
-      int a = start;
-      for (int k = 0; k < iters; ++k) {
-        Timed tm(w, s, name);
-        plain_jacobi(s, L.dm, L.div, L.p[a], L.p[a ^ 1]);
-        a ^= 1;
+    if (pressure_plan() == 0) {
+      // Per-voxel plan. Fine writes in order: the first sweep (fused into the
+      // divergence kernel), the remaining pre sweeps (the last one adds the
+      // prolongation when the reference prolongs into it), the prolongation alone
+      // when there is no pre sweep, then the post sweeps. The last write lands in
+      // p[last]; going backwards the writes alternate with the other buffer, so no
+      // sweep reads the buffer it writes.
+      const bool prolong_live = (m & 1) == 0;  // odd m: the correction lands in a buffer never read
+      const int nwrites = std::max(m, 0) + (m == 0 ? 1 : 0) + n;
+      std::vector<float*> outs(nwrites);
+      for (int i = nwrites; i-- > 0;)
+        outs[i] = (i + 1 == nwrites) ? F.p[last_p] : (outs[i + 1] == F.p[last_p] ? F.p[last_p ^ 1] : F.p[last_p]);
+      int wi = 0;
+      const float* chain = nullptr;
+      {
+        Timed tm(w, s, "fused_div_first_sweep");
+        FX_CK(lean_div_first(s, dm, *vfinal, F.div, m >= 1 ? outs[0] : nullptr, M.dm, M.div, fuse_restrict));
         ++launches;
       }
-      return a;
-    };
-    const int mid_pre = smooth(M, st.q[4], 0, "fused_jacobi_mid");
-    {
-      Timed tm(w, s, "fused_restrict");
-      plain_restrict(s, M.dm, C.dm, M.div, C.div);
-      ++launches;
-    }
-    const int coarse = smooth(C, st.q[6], 0, "fused_jacobi_coarse");
-    {
-      Timed tm(w, s, "fused_prolong");
-      plain_prolong(s, C.dm, M.dm, C.p[coarse], M.p[0]);
-      ++launches;
-    }
-    const int mid = smooth(M, st.q[5], mid_pre, "fused_jacobi_mid");
-    for (const Plan& pl : post) {
-      ZPass zp{};
-      zp.dm = dm;
-      zp.mid = M.dm;
-      zp.sweeps = pl.sweeps;
-      zp.zchunk = zpass_zchunk();
-      zp.input = pl.input;
-      zp.div_from_velocity = false;
-      zp.project = pl.proj;
-      zp.p_in = chain;
-      zp.div_in = F.div;
-      zp.mid_p = M.p[mid];
-      zp.p_out = outs[pi];
-      zp.vfin = *vfinal;
-      zp.vcur = st.vcur;
-      zp.vmag = st.vel_mag;
-      zp.write_vmag = st.debug_on ? 1 : 0;
-      Timed tm(w, s, pl.proj ? "fused_zpass_post_project" : "fused_zpass_post");
-      FX_CK(zpass_launch(s, zp));
-      ++launches;
-      chain = outs[pi++];
+      if (m >= 1) chain = outs[wi++];
+      if (!fuse_restrict) {
+        Timed tm(w, s, "fused_restrict");
+        plain_restrict(s, F.dm, M.dm, F.div, M.div);
+        ++launches;
+      }
+      int mid = 0;
+      if (prolong_live) {
+        Timed tm(w, s, "fused_multigrid_lower");
+        FX_CK(mg_lower_launch(s, M, C, st.q[4], st.q[6], st.q[5], w.mg_bar, &mid));
+        ++launches;
+      }
+      for (int k = 2; k <= m; ++k) {
+        const bool add = prolong_live && k == m;
+        Timed tm(w, s, add ? "fused_sweep_prolong" : "fused_sweep");
+        FX_CK(lean_sweep(s, dm, F.div, chain, outs[wi], M.dm, add ? M.p[mid] : nullptr));
+        chain = outs[wi++];
+        ++launches;
+      }
+      if (m == 0) {
+        Timed tm(w, s, "fused_prolong_fine");
+        FX_CK(lean_prolong_zero(s, dm, outs[wi], M.dm, M.p[mid]));
+        chain = outs[wi++];
+        ++launches;
+      }
+      for (int k = 1; k <= n; ++k) {
+        Timed tm(w, s, "fused_sweep");
+        FX_CK(lean_sweep(s, dm, F.div, chain, outs[wi], M.dm, nullptr));
+        chain = outs[wi++];
+        ++launches;
+      }
+      {
+        Timed tm(w, s, "fused_project");
+        k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, F.p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0);
+        ++launches;
+      }
+    } else {
+      // Plan the fine passes: pre-smoothing in groups of <= 4 sweeps (the first one
+      // also computes the divergence), post-smoothing in groups of <= 4 sweeps (the
+      // first adds the prolongation, the last finishes with the projection).
+      struct Plan {
+        int sweeps;
+        ZInput input;
+        bool divv, proj;
+      };
+      std::vector<Plan> pre, post;
+      const int kmax = zpass_max_sweeps();
+      for (int left = m; left > 0;) {
+        const int k = std::min(left, kmax);
+        pre.push_back({k, pre.empty() ? ZIN_ZERO : ZIN_BUF, pre.empty(), false});
+        left -= k;
+      }
+      {
+        const ZInput first_in = (m & 1) ? ZIN_BUF : (m == 0 ? ZIN_ZERO_PROLONG : ZIN_BUF_PROLONG);
+        if (n == 0) {
+          post.push_back({0, first_in, false, true});
+        } else {
+          for (int left = n; left > 0;) {
+            const int k = std::min(left, kmax);
+            post.push_back({k, post.empty() ? first_in : ZIN_BUF, false, left - k == 0});
+            left -= k;
+          }
+        }
+      }
+      // Output buffers: the last pass writes p[last]; going backwards the passes
+      // alternate with the other buffer, so no pass reads the buffer it writes.
+      const size_t npass = pre.size() + post.size();
+      std::vector<float*> outs(npass);
+      for (size_t i = npass; i-- > 0;)
+        outs[i] = (i + 1 == npass) ? F.p[last_p] : (outs[i + 1] == F.p[last_p] ? F.p[last_p ^ 1] : F.p[last_p]);
+      size_t pi = 0;
+      const float* chain = nullptr;  // the latest fine pressure (nullptr: the cleared buffer)
+      if (m == 0) {
+        Timed tm(w, s, "fused_divergence");
+        plain_divergence(s, dm, *vfinal, F.div);
+        ++launches;
+      }
+      for (const Plan& pl : pre) {
+        ZPass zp{};
+        zp.dm = dm;
+        zp.mid = M.dm;
+        zp.sweeps = pl.sweeps;
+        zp.zchunk = zpass_zchunk();
+        zp.input = pl.input;
+        zp.div_from_velocity = pl.divv;
+        zp.project = false;
+        zp.restrict_mid = (pl.divv && fuse_restrict) ? 1 : 0;
+        zp.p_in = chain;
+        zp.div_in = F.div;
+        zp.div_out = F.div;
+        zp.mid_div = M.div;
+        zp.p_out = outs[pi];
+        zp.vfin = *vfinal;
+        Timed tm(w, s, pl.divv ? "fused_zpass_div_pre" : "fused_zpass_pre");
+        FX_CK(zpass_launch(s, zp));
+        ++launches;
+        chain = outs[pi++];
+      }
+      if (m == 0 || !fuse_restrict) {
+        Timed tm(w, s, "fused_restrict");
+        plain_restrict(s, F.dm, M.dm, F.div, M.div);
+        ++launches;
+      }
+      // mid and coarse levels (sweep by sweep)
+      auto smooth = [&](const LevelBuf& L, int iters, int start, const char* name) {
+        int a = start;
+        for (int k = 0; k < iters; ++k) {
+          Timed tm(w, s, name);
+          plain_jacobi(s, L.dm, L.div, L.p[a], L.p[a ^ 1]);
+          a ^= 1;
+          ++launches;
+        }
+        return a;
+      };
+      const int mid_pre = smooth(M, st.q[4], 0, "fused_jacobi_mid");
+      {
+        Timed tm(w, s, "fused_restrict");
+        plain_restrict(s, M.dm, C.dm, M.div, C.div);
+        ++launches;
+      }
+      const int coarse = smooth(C, st.q[6], 0, "fused_jacobi_coarse");
+      {
+        Timed tm(w, s, "fused_prolong");
+        plain_prolong(s, C.dm, M.dm, C.p[coarse], M.p[0]);
+        ++launches;
+      }
+      const int mid = smooth(M, st.q[5], mid_pre, "fused_jacobi_mid");
+      for (const Plan& pl : post) {
+        ZPass zp{};
+        zp.dm = dm;
+        zp.mid = M.dm;
+        zp.sweeps = pl.sweeps;
+        zp.zchunk = zpass_zchunk();
+        zp.input = pl.input;
+        zp.div_from_velocity = false;
+        zp.project = pl.proj;
+        zp.p_in = chain;
+        zp.div_in = F.div;
+        zp.mid_p = M.p[mid];
+        zp.p_out = outs[pi];
+        zp.vfin = *vfinal;
+        zp.vcur = st.vcur;
+        zp.vmag = st.vel_mag;
+        zp.write_vmag = st.debug_on ? 1 : 0;
+        Timed tm(w, s, pl.proj ? "fused_zpass_post_project" : "fused_zpass_post");
+        FX_CK(zpass_launch(s, zp));
+        ++launches;
+        chain = outs[pi++];
+      }
     }
   } else {
     // 10. projection with the pressure of the last solve (+ |v|)
     Timed tm(w, s, "fused_project");
-    k_project<<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0);
+    k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0);
     ++launches;
   }
   FX_CK(cudaGetLastError());
-#undef FX_CK
   out.last_p = last_p;
   out.final_vscr_is_2 = st.vort_on;
   out.launches = launches;
   return FX_OK;
+}
+
+fx_status fused_check_device_error(FusedWork& w, cudaStream_t s) {
+  unsigned h = 0;
+  if (cudaMemcpyAsync(&h, w.mg_bar + 64, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess) return FX_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return FX_ERR_CUDA;
+  return h ? FX_ERR_TIMEOUT : FX_OK;
 }
 
 fx_status fused_count_active(FusedWork& w, cudaStream_t s, const uint32_t* flags, uint32_t nb, uint32_t* out) {

@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <functional>
+#include <map>
 #include <string>
 #include <vector>
 #include <cuda_runtime.h>
@@ -12,6 +13,14 @@
 #include "fx_kernels.h"
 
 namespace fx {
+
+struct FusedResult {
+  int last_p = 0;
+  bool final_vscr_is_2 = false;
+  uint32_t launches = 0;
+  bool graph = false;  // the step was a replay of a captured CUDA graph
+  std::string error;
+};
 
 // Device work buffers of the fused path, carved from the simulation's arena.
 struct FusedWork {
@@ -31,11 +40,21 @@ struct FusedWork {
   uint32_t* list_next = nullptr;  // bricks the combustion/buoyancy kernels visit
   uint32_t* list_inj = nullptr;   // bricks the injection kernel visits (host-filled)
   uint32_t* counters = nullptr;   // [0] adv count, [1] next count, [2] scratch, [3] inject count
+  unsigned* mg_bar = nullptr;      // grid barrier of the lower multigrid kernel: arrivals, generation, error flag
   uint32_t* host_list_inj = nullptr;  // pinned staging for list_inj (+ count at [nb])
   cudaEvent_t inj_event = nullptr;
   std::vector<uint8_t> host_mark;
   std::vector<uint32_t> host_list;
   bool valid = false;  // false: the per-brick bookkeeping must be rebuilt from the fields
+  std::vector<uint32_t> uploaded_list;  // injection list currently on the device
+  // CUDA graphs of the device part of the step, keyed by its configuration.
+  struct GraphEntry {
+    cudaGraphExec_t exec;
+    FusedResult result;
+  };
+  bool use_graphs = true;
+  std::string graph_note;
+  std::map<uint64_t, GraphEntry> graphs;
   // kernel timing
   bool timing = false;
   struct TimedPair {
@@ -70,12 +89,6 @@ struct FusedStep {
   int last_p;
 };
 
-struct FusedResult {
-  int last_p = 0;
-  bool final_vscr_is_2 = false;
-  uint32_t launches = 0;
-  std::string error;
-};
 
 size_t fused_work_bytes(Dims dm, uint3 bricks);
 void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks);
@@ -85,6 +98,10 @@ fx_status fused_invalidate(FusedWork& w, cudaStream_t s);
 void fused_release(FusedWork& w);
 fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out);
 fx_status fused_count_active(FusedWork& w, cudaStream_t s, const uint32_t* flags, uint32_t nb, uint32_t* out);
+
+// FX_ERR_TIMEOUT when a grid barrier of the fused path gave up waiting
+// (waits for the stream), FX_OK otherwise.
+fx_status fused_check_device_error(FusedWork& w, cudaStream_t s);
 
 // Adds the active bricks of `flags` and their voxel count to acc[0] and acc[1].
 cudaError_t fused_accumulate_active(cudaStream_t s, Dims dm, uint3 bricks, const uint32_t* flags, unsigned long long* acc);

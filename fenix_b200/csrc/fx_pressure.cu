@@ -32,6 +32,14 @@ namespace {
 
 constexpr int TX = 32, TY = 16, NT = TX * TY;
 
+// Integer tuning knob from the environment (defaults come from measurement).
+int env_int(const char* name, int dflt, int lo, int hi) {
+  const char* v = std::getenv(name);
+  if (!v || !*v) return dflt;
+  const int x = std::atoi(v);
+  return (x >= lo && x <= hi) ? x : dflt;
+}
+
 enum { IN_ZERO = 0, IN_BUF = 1, IN_BUF_PROLONG = 2, IN_ZERO_PROLONG = 3 };
 
 struct ZArgs {
@@ -353,6 +361,337 @@ cudaError_t launch_s(cudaStream_t s, int sweeps, const ZArgs& a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Lean per-voxel kernels (one thread per voxel, blocks of 32 x 4 x 2).
+// ---------------------------------------------------------------------------
+
+// Divergence (compute-divergence.wgsl.ts:22-42) with, pointwise, the first
+// Jacobi sweep from the cleared buffer, (0 - div) / 6, and the fine->mid
+// restriction (pressure-restriction.wgsl.ts:27-50) of each 2x2x2 group of the
+// block through shared memory. The restriction needs every fine dimension >= 16.
+__global__ void __launch_bounds__(256) k_div_first(Dims dm, VelField v, float* __restrict__ div, float* __restrict__ p1, Dims mid,
+                                                   float* __restrict__ mid_div, int restrict_mid) {
+  __shared__ float sd[2][4][32];
+  const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 4 + threadIdx.y, z = blockIdx.z * 2 + threadIdx.z;
+  const bool in = x < dm.w && y < dm.h && z < dm.d;
+  float d = 0.0f;
+  if (in) {
+    const uint32_t i = flat(dm, x, y, z);
+    if (!is_boundary(dm, x, y, z)) {
+      const uint32_t sy = dm.w, sz = dm.w * dm.h;
+      const float ddx = __ldg(v.c[0] + i + 1) - __ldg(v.c[0] + i - 1);
+      const float ddy = __ldg(v.c[1] + i + sy) - __ldg(v.c[1] + i - sy);
+      const float ddz = __ldg(v.c[2] + i + sz) - __ldg(v.c[2] + i - sz);
+      d = (ddx + ddy + ddz) * 0.5f;
+      if (p1) p1[i] = div6(0.0f - d);
+    } else if (p1) {
+      p1[i] = 0.0f;
+    }
+    div[i] = d;
+  }
+  if (!restrict_mid) return;
+  sd[threadIdx.z][threadIdx.y][threadIdx.x] = d;
+  __syncthreads();
+  if (threadIdx.z == 0 && (threadIdx.y & 1) == 0 && (threadIdx.x & 1) == 0) {
+    const uint32_t mx_ = x >> 1, my_ = y >> 1, mz_ = z >> 1;
+    if (mx_ < mid.w && my_ < mid.h && mz_ < mid.d) {
+      float out = 0.0f;
+      if (!(mx_ == 0 || my_ == 0 || mz_ == 0 || mx_ == mid.w - 1 || my_ == mid.h - 1 || mz_ == mid.d - 1)) {
+        const int tx = threadIdx.x, ty = threadIdx.y;
+        float sum = 0.0f;
+        sum += sd[0][ty][tx];
+        sum += sd[0][ty][tx + 1];
+        sum += sd[0][ty + 1][tx];
+        sum += sd[0][ty + 1][tx + 1];
+        sum += sd[1][ty][tx];
+        sum += sd[1][ty][tx + 1];
+        sum += sd[1][ty + 1][tx];
+        sum += sd[1][ty + 1][tx + 1];
+        out = sum * 0.125f;
+      }
+      mid_div[flat(mid, mx_, my_, mz_)] = out;
+    }
+  }
+}
+
+// One Jacobi sweep (pressure-jacobi.wgsl.ts:15-36). With `mid_p`, the result
+// then gets the prolongation added (pressure-prolongation.wgsl.ts:36-43: the
+// boundary stays 0, the interior becomes p + sample), as when the reference
+// prolongs into the buffer this sweep wrote. With `src` NULL the input is the
+// cleared buffer.
+//
+// A thread computes a column of ZB voxels along z, reusing the z neighbours in
+// registers; all loads of the column are independent, which keeps enough bytes
+// in flight per SM to stream HBM.
+// A warp holds 32 consecutive x of one row. The x neighbours come from the
+// coalesced centre row by shuffles (the two row ends load their outer
+// neighbour), the z neighbours from the column in registers; every load of the
+// column is issued before the arithmetic. The sum keeps the reference order
+// +x, -x, +y, -y, +z, -z.
+template <int ZB>
+__global__ void __launch_bounds__(256) k_sweep(Dims dm, const float* __restrict__ div, const float* __restrict__ src, float* __restrict__ dst,
+                                               Dims mid, const float* __restrict__ mid_p) {
+  const uint32_t lane = threadIdx.x;
+  const uint32_t x = blockIdx.x * 32 + lane, y = blockIdx.y * 8 + threadIdx.y, z0 = blockIdx.z * ZB;
+  if (y >= dm.h) return;  // whole warp
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  const bool xin = x < dm.w;
+  const uint32_t base = (xin ? x : dm.w - 1) + dm.w * y;
+  const bool yint = y > 0 && y < dm.h - 1;
+  const bool xint = x > 0 && x < dm.w - 1;
+  const int nz = min(ZB, (int)dm.d - (int)z0);
+  if (!yint) {
+    if (xin)
+      for (int k = 0; k < nz; ++k) dst[base + sz * (z0 + k)] = 0.0f;
+    return;
+  }
+  float c[ZB + 2], yp[ZB], ym[ZB], dv[ZB], xe[ZB];
+  const bool left_end = lane == 0 && x > 0, right_end = (lane == 31 || x == dm.w - 1) && x + 1 < dm.w;
+#pragma unroll
+  for (int k = 0; k < ZB + 2; ++k) {
+    const int z = (int)z0 + k - 1;
+    c[k] = (src && z >= 0 && z < (int)dm.d) ? __ldg(src + base + sz * (uint32_t)z) : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < ZB; ++k) {
+    const uint32_t z = min(z0 + k, dm.d - 1);
+    const uint32_t i = base + sz * z;
+    dv[k] = __ldg(div + i);
+    yp[k] = src ? __ldg(src + i + sy) : 0.0f;
+    ym[k] = src ? __ldg(src + i - sy) : 0.0f;
+    xe[k] = 0.0f;
+    if (src && left_end) xe[k] = __ldg(src + i - 1);
+    if (src && right_end) xe[k] = __ldg(src + i + 1);
+  }
+#pragma unroll
+  for (int k = 0; k < ZB; ++k) {
+    const float cm = c[k + 1];
+    float xr = __shfl_down_sync(0xffffffffu, cm, 1);
+    float xl = __shfl_up_sync(0xffffffffu, cm, 1);
+    if (right_end) xr = xe[k];
+    if (left_end) xl = xe[k];
+    const uint32_t z = z0 + k;
+    if (k >= nz || !xin) continue;
+    float v = 0.0f;
+    if (xint && z > 0 && z < dm.d - 1) {
+      if (src) {
+        const float s = xr + xl + yp[k] + ym[k] + c[k + 2] + c[k];
+        v = div6(s - dv[k]);
+      } else {
+        v = div6(0.0f - dv[k]);
+      }
+      if (mid_p) v = v + prolong_sample(mid, mid_p, (int)x, (int)y, (int)z);
+    }
+    dst[base + sz * z] = v;
+  }
+}
+
+// The cleared buffer plus the prolongation (finePre = 0): boundary 0, interior 0 + sample.
+__global__ void __launch_bounds__(256) k_prolong_zero(Dims dm, float* __restrict__ dst, Dims mid, const float* __restrict__ mid_p) {
+  const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 4 + threadIdx.y, z = blockIdx.z * 2 + threadIdx.z;
+  if (x >= dm.w || y >= dm.h || z >= dm.d) return;
+  const uint32_t i = flat(dm, x, y, z);
+  dst[i] = is_boundary(dm, x, y, z) ? 0.0f : 0.0f + prolong_sample(mid, mid_p, (int)x, (int)y, (int)z);
+}
+
+inline dim3 lean_grid(Dims d) { return dim3((d.w + 31) / 32, (d.h + 3) / 4, (d.d + 1) / 2); }
+
+// ---------------------------------------------------------------------------
+// The mid and coarse levels of PressureSolvePass.solve (:73-82) in one
+// cooperative launch: mid pre-smoothing, restriction to coarse, coarse
+// smoothing, prolongation into mid pressureA and mid post-smoothing, separated
+// by grid-wide barriers. The levels are small enough to stay in L2, so the
+// launch-per-sweep cost of the reference schedule dominates without this.
+// ---------------------------------------------------------------------------
+struct MgArgs {
+  Dims mid, coarse;
+  float* mdiv;
+  float* mp[2];
+  float* cdiv;
+  float* cp[2];
+  int mid_pre, coarse_n, mid_post;
+  unsigned* bar;  // [0] arrivals, [1] generation, [2] error flag
+};
+
+// Grid barrier with a bounded wait: after 2^24 polls of at least 64 ns (about a
+// second; a correct barrier takes microseconds) the waiting block records an
+// error and every block leaves the kernel.
+FX_DEV bool grid_sync(unsigned* bar) {
+  // bar[0]: arrivals, bar[32]: generation, bar[64]: error flag (separate 128-byte lines)
+  __syncthreads();
+  __shared__ int failed;
+  if (threadIdx.x == 0) {
+    failed = 0;
+    volatile unsigned* vgen = bar + 32;
+    volatile unsigned* verr = bar + 64;
+    const unsigned gen = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 32, 1u);
+    } else {
+      unsigned polls = 0;
+      while (*vgen == gen) {
+        __nanosleep(64);
+        if (++polls > (1u << 24) || *verr) {
+          atomicExch(bar + 64, 1u);
+          failed = 1;
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return failed == 0 && *((volatile unsigned*)bar + 64) == 0;
+}
+
+// Grid-stride walk over a level's voxels keeping (x, y, z) by carry instead of
+// dividing each linear index by the dimensions.
+struct Walk {
+  uint32_t i, x, y, z, step, sx, sy, sz;
+  FX_DEV Walk(const Dims& d) {
+    i = blockIdx.x * blockDim.x + threadIdx.x;
+    step = gridDim.x * blockDim.x;
+    x = i % d.w;
+    y = (i / d.w) % d.h;
+    z = i / (d.w * d.h);
+    sx = step % d.w;
+    sy = (step / d.w) % d.h;
+    sz = step / (d.w * d.h);
+  }
+  FX_DEV void next(const Dims& d) {
+    i += step;
+    x += sx;
+    uint32_t cy = 0;
+    if (x >= d.w) {
+      x -= d.w;
+      cy = 1;
+    }
+    y += sy + cy;
+    uint32_t cz = 0;
+    if (y >= d.h) {
+      y -= d.h;
+      cz = 1;
+    }
+    z += sz + cz;
+  }
+};
+
+// A warp owns chunks of 32*MG_RUN consecutive voxels, lane-interleaved (so the
+// accesses stay coalesced); each lane loads its MG_RUN voxels' operands before
+// computing, which keeps MG_RUN independent loads in flight per thread.
+constexpr int MG_RUN = 8;
+
+FX_DEV void mg_sweep(const Dims& d, const float* __restrict__ div, const float* __restrict__ src, float* __restrict__ dst) {
+  const uint32_t n = d.w * d.h * d.d;
+  const uint32_t sy = d.w, sz = d.w * d.h;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t chunk = 32u * MG_RUN;
+  for (uint32_t c0 = warp * chunk; c0 < n; c0 += nwarps * chunk) {
+    uint32_t i0 = c0 + lane;
+    uint32_t x = i0 % d.w, y = (i0 / d.w) % d.h, z = i0 / sz;
+    float nb[MG_RUN][6], dv[MG_RUN];
+    bool live[MG_RUN], interior[MG_RUN];
+    uint32_t idx[MG_RUN];
+#pragma unroll
+    for (int k = 0; k < MG_RUN; ++k) {
+      const uint32_t i = i0 + 32u * k;
+      idx[k] = i;
+      live[k] = i < n;
+      interior[k] = live[k] && !is_boundary(d, x, y, z);
+      if (interior[k]) {
+        nb[k][0] = src[i + 1];
+        nb[k][1] = src[i - 1];
+        nb[k][2] = src[i + sy];
+        nb[k][3] = src[i - sy];
+        nb[k][4] = src[i + sz];
+        nb[k][5] = src[i - sz];
+        dv[k] = div[i];
+      }
+      // advance (x, y, z) by 32 voxels
+      x += 32u;
+      while (x >= d.w) {
+        x -= d.w;
+        if (++y >= d.h) {
+          y = 0;
+          ++z;
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < MG_RUN; ++k) {
+      if (!live[k]) continue;
+      float v = 0.0f;
+      if (interior[k]) {
+        const float s = nb[k][0] + nb[k][1] + nb[k][2] + nb[k][3] + nb[k][4] + nb[k][5];
+        v = div6(s - dv[k]);
+      }
+      dst[idx[k]] = v;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(512) k_mg_lower(MgArgs a) {
+  int m = 0;
+  for (int k = 0; k < a.mid_pre; ++k, m ^= 1) {
+    mg_sweep(a.mid, a.mdiv, a.mp[m], a.mp[m ^ 1]);
+    if (!grid_sync(a.bar)) return;
+  }
+  const int mid_pre = m;
+  {  // restriction mid -> coarse (pressure-restriction.wgsl.ts:27-50)
+    const Dims& t = a.coarse;
+    const Dims& sdm = a.mid;
+    const uint32_t n = t.w * t.h * t.d;
+    for (Walk w(t); w.i < n; w.next(t)) {
+      const uint32_t i = w.i, x = w.x, y = w.y, z = w.z;
+      if (x == 0u || y == 0u || z == 0u || x == t.w - 1u || y == t.h - 1u || z == t.d - 1u) {
+        a.cdiv[i] = 0.0f;
+        continue;
+      }
+      float sum = 0.0f;
+      for (uint32_t dz = 0; dz < 2u; ++dz)
+        for (uint32_t dy = 0; dy < 2u; ++dy)
+          for (uint32_t dx = 0; dx < 2u; ++dx) {
+            const uint32_t sx = min(2u * x + dx, sdm.w - 1u), sy = min(2u * y + dy, sdm.h - 1u), sz = min(2u * z + dz, sdm.d - 1u);
+            sum += a.mdiv[flat(sdm, sx, sy, sz)];
+          }
+      a.cdiv[i] = sum * 0.125f;
+    }
+    if (!grid_sync(a.bar)) return;
+  }
+  int c = 0;
+  for (int k = 0; k < a.coarse_n; ++k, c ^= 1) {
+    mg_sweep(a.coarse, a.cdiv, a.cp[c], a.cp[c ^ 1]);
+    if (!grid_sync(a.bar)) return;
+  }
+  {  // prolongation coarse -> mid pressureA (pressure-prolongation.wgsl.ts:29-44)
+    const Dims& t = a.mid;
+    const uint32_t n = t.w * t.h * t.d;
+    for (Walk w(t); w.i < n; w.next(t)) {
+      const uint32_t i = w.i, x = w.x, y = w.y, z = w.z;
+      if (x == 0u || y == 0u || z == 0u || x == t.w - 1u || y == t.h - 1u || z == t.d - 1u) {
+        a.mp[0][i] = 0.0f;
+        continue;
+      }
+      const float px = ((float)x + 0.5f) * 0.5f - 0.5f;
+      const float py = ((float)y + 0.5f) * 0.5f - 0.5f;
+      const float pz = ((float)z + 0.5f) * 0.5f - 0.5f;
+      a.mp[0][i] += tri_interp(a.cp[c], tri_corners(a.coarse, px, py, pz));
+    }
+    if (!grid_sync(a.bar)) return;
+  }
+  m = mid_pre;
+  for (int k = 0; k < a.mid_post; ++k, m ^= 1) {
+    mg_sweep(a.mid, a.mdiv, a.mp[m], a.mp[m ^ 1]);
+    if (k + 1 < a.mid_post && !grid_sync(a.bar)) return;
+  }
+}
+
 __global__ void k_div6_check(uint32_t hi_base, unsigned long long* bad) {
   const uint32_t u = hi_base + blockIdx.x * blockDim.x + threadIdx.x;
   const float x = __uint_as_float(u);
@@ -396,14 +735,6 @@ cudaError_t zpass_launch(cudaStream_t s, const ZPass& p) {
   }
 }
 
-namespace {
-int env_int(const char* name, int dflt, int lo, int hi) {
-  const char* v = std::getenv(name);
-  if (!v || !*v) return dflt;
-  const int x = std::atoi(v);
-  return (x >= lo && x <= hi) ? x : dflt;
-}
-}  // namespace
 
 int zpass_max_sweeps() {
   static const int k = env_int("FENIX_ZPASS_SWEEPS", 4, 1, 4);
@@ -413,6 +744,75 @@ int zpass_max_sweeps() {
 int zpass_zchunk() {
   static const int z = env_int("FENIX_ZPASS_ZCHUNK", 64, 8, 4096) & ~1;
   return z;
+}
+
+cudaError_t lean_div_first(cudaStream_t s, Dims dm, VelField v, float* div, float* p1, Dims mid, float* mid_div, bool restrict_mid) {
+  k_div_first<<<lean_grid(dm), dim3(32, 4, 2), 0, s>>>(dm, v, div, p1, mid, mid_div, restrict_mid ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t lean_sweep(cudaStream_t s, Dims dm, const float* div, const float* src, float* dst, Dims mid, const float* mid_p) {
+  static const int zb = env_int("FENIX_SWEEP_ZB", 4, 1, 8);
+  auto grid = [&](int z) { return dim3((dm.w + 31) / 32, (dm.h + 7) / 8, (dm.d + z - 1) / z); };
+  if (zb <= 2) k_sweep<2><<<grid(2), dim3(32, 8, 1), 0, s>>>(dm, div, src, dst, mid, mid_p);
+  else if (zb <= 4) k_sweep<4><<<grid(4), dim3(32, 8, 1), 0, s>>>(dm, div, src, dst, mid, mid_p);
+  else k_sweep<8><<<grid(8), dim3(32, 8, 1), 0, s>>>(dm, div, src, dst, mid, mid_p);
+  return cudaGetLastError();
+}
+
+cudaError_t lean_prolong_zero(cudaStream_t s, Dims dm, float* dst, Dims mid, const float* mid_p) {
+  k_prolong_zero<<<lean_grid(dm), dim3(32, 4, 2), 0, s>>>(dm, dst, mid, mid_p);
+  return cudaGetLastError();
+}
+
+cudaError_t mg_lower_launch(cudaStream_t s, const LevelBuf& mid, const LevelBuf& coarse, int mid_pre, int coarse_n, int mid_post,
+                            unsigned* bar, int* mid_result) {
+  static int grid = 0;
+  static int grid_dev = -1;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (grid == 0 || grid_dev != dev) {
+    int per_sm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_lower, 512, 0);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    grid = std::max(1, std::min(per_sm, 2) * sms);
+    grid_dev = dev;
+  }
+  MgArgs a;
+  a.mid = mid.dm;
+  a.coarse = coarse.dm;
+  a.mdiv = mid.div;
+  a.mp[0] = mid.p[0];
+  a.mp[1] = mid.p[1];
+  a.cdiv = coarse.div;
+  a.cp[0] = coarse.p[0];
+  a.cp[1] = coarse.p[1];
+  a.mid_pre = mid_pre;
+  a.coarse_n = coarse_n;
+  a.mid_post = mid_post;
+  a.bar = bar;
+  *mid_result = (mid_pre & 1) ^ (mid_post & 1);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(512);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  e = cudaLaunchKernelEx(&cfg, k_mg_lower, a);
+  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+int pressure_plan() {
+  static const int p = env_int("FENIX_PRESSURE_PLAN", 0, 0, 1);
+  return p;
 }
 
 cudaError_t div6_exhaustive_check(unsigned long long* host_bad) {

@@ -43,6 +43,21 @@ cudaError_t zpass_launch(cudaStream_t s, const ZPass& p);
 int zpass_max_sweeps();
 int zpass_zchunk();
 
+// Lean per-voxel kernels of the default pressure plan.
+cudaError_t lean_div_first(cudaStream_t s, Dims dm, VelField v, float* div, float* p1, Dims mid, float* mid_div, bool restrict_mid);
+cudaError_t lean_sweep(cudaStream_t s, Dims dm, const float* div, const float* src, float* dst, Dims mid, const float* mid_p);
+cudaError_t lean_prolong_zero(cudaStream_t s, Dims dm, float* dst, Dims mid, const float* mid_p);
+
+// The mid/coarse part of the solve in one cooperative launch. `bar` is 96
+// zeroed device words: [0] arrivals, [32] generation, [64] error flag (set when
+// a grid barrier times out). *mid_result gets the id of the mid buffer
+// holding the result.
+cudaError_t mg_lower_launch(cudaStream_t s, const LevelBuf& mid, const LevelBuf& coarse, int mid_pre, int coarse_n, int mid_post,
+                            unsigned* bar, int* mid_result);
+
+// 0: per-voxel sweeps (default); 1: z-march passes (FENIX_PRESSURE_PLAN=1).
+int pressure_plan();
+
 // Counts the floats x (all 2^32 bit patterns, NaNs excluded) for which the
 // pressure kernels' division by 6 differs from the IEEE quotient x / 6.0f.
 cudaError_t div6_exhaustive_check(unsigned long long* host_bad);

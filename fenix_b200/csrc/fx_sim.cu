@@ -132,6 +132,7 @@ struct fx_sim {
   int qi[7]{};  // clamped integers of `quality`
   fx_runtime_params rp{};
   uint32_t last_kernel_count = 0;
+  bool last_step_graph = false;
   uint32_t instr = 0;
   KernelTimer timer;
   unsigned long long* d_active_acc = nullptr;  // [0] brick-steps, [1] voxel-steps
@@ -548,6 +549,7 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
   s->d_params = (Params*)(base + o_params);
   s->d_active_acc = (unsigned long long*)(base + o_acc);
   fused_work_carve(s->fw, base + o_fused, s->dm, s->bricks);
+  s->fw.use_graphs = (s->opt_flags & FX_OPT_NO_GRAPHS) == 0;
   s->final_vscr = &s->vscr;
 
   if (cudaMallocHost(&s->h_params, kParamSlots * sizeof(Params)) != cudaSuccess) {
@@ -655,6 +657,7 @@ fx_status fx_sim_step(fx_sim* s, double elapsed, double step_s) {
       s->last_p = fr.last_p;
       s->final_vscr = fr.final_vscr_is_2 ? &s->vscr2 : &s->vscr;
       s->last_kernel_count = fr.launches;
+      s->last_step_graph = fr.graph;
     } else {
       fail(s, st, "fx_sim_step: fused step failed: " + fr.error);
     }
@@ -798,6 +801,8 @@ fx_status fx_sim_read_field(fx_sim* s, int32_t id, void* dst, size_t bytes) {
   if (bytes != count * 4) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_read_field: byte count does not match the field");
   FX_CUDA(s, cudaSetDevice(s->device));
   FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  if (fused_check_device_error(s->fw, s->stream) == FX_ERR_TIMEOUT)
+    return fail(s, FX_ERR_TIMEOUT, "a grid barrier of the pressure solve timed out; the results of that step are invalid");
   FX_CUDA(s, cudaMemcpy(dst, p, bytes, cudaMemcpyDeviceToHost));
   return FX_OK;
 }
@@ -819,6 +824,8 @@ fx_status fx_sim_synchronize(fx_sim* s) {
   if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_synchronize: NULL handle");
   FX_CUDA(s, cudaSetDevice(s->device));
   FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  if (fused_check_device_error(s->fw, s->stream) == FX_ERR_TIMEOUT)
+    return fail(s, FX_ERR_TIMEOUT, "a grid barrier of the pressure solve timed out; the results of that step are invalid");
   return FX_OK;
 }
 
@@ -830,6 +837,7 @@ fx_status fx_sim_get_stats(fx_sim* s, fx_stats* o) {
   o->last_pressure_buffer = s->last_p;
   o->brick_count = s->nb;
   o->kernels_per_step = s->last_kernel_count;
+  o->flags = (s->last_step_graph ? FX_STATS_GRAPH : 0u) | (s->fw.use_graphs ? 0u : FX_STATS_GRAPHS_OFF);
   FX_CUDA(s, cudaSetDevice(s->device));
   uint32_t active = 0;
   fx_status st = fused_count_active(s->fw, s->stream, s->flags[s->cur], s->nb, &active);

@@ -268,6 +268,8 @@ class CombustionVolumeSimulation:
             "brickCount": st.brick_count,
             "activeBricks": st.active_bricks,
             "kernelsPerStep": st.kernels_per_step,
+            "graphReplay": bool(st.flags & 1),
+            "graphsOff": bool(st.flags & 2),
         }
 
     def setInstrumentation(self, kernel_times: bool = False, count_active: bool = False) -> None:

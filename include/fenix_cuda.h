@@ -178,8 +178,11 @@ typedef struct fx_stats {
   uint32_t brick_count;        /* bricks of 8^3 voxels */
   uint32_t active_bricks;      /* bricks flagged in the current flags (waits for the stream) */
   uint32_t kernels_per_step;   /* kernels the last step launched */
-  uint32_t reserved;
+  uint32_t flags;              /* FX_STATS_* */
 } fx_stats;
+
+#define FX_STATS_GRAPH (1u << 0)      /* the last step replayed a captured CUDA graph */
+#define FX_STATS_GRAPHS_OFF (1u << 1) /* graphs are off (FX_OPT_NO_GRAPHS, or capture failed) */
 
 /* Version of this ABI (FX_ABI_VERSION). */
 int32_t fx_abi_version(void);
