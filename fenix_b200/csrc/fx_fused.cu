@@ -955,10 +955,53 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
         ++launches;
       }
       int mid = 0;
-      if (prolong_live) {
+      if (prolong_live && multigrid_plan() == 1) {
         Timed tm(w, s, "fused_multigrid_lower");
         FX_CK(mg_lower_launch(s, M, C, st.q[4], st.q[6], st.q[5], w.mg_bar, &mid));
         ++launches;
+      } else if (prolong_live) {
+        // Mid and coarse levels sweep by sweep (inside the step's CUDA graph the
+        // launch gaps are short). The first sweep of a level reads the cleared
+        // buffer, so it is computed from the divergence alone.
+        int mid_pre = 0;
+        {
+          int a = 0;
+          for (int k = 0; k < st.q[4]; ++k) {
+            Timed tm(w, s, "fused_sweep_mid");
+            FX_CK(lean_sweep(s, M.dm, M.div, k == 0 ? nullptr : M.p[a], M.p[a ^ 1], M.dm, nullptr));
+            a ^= 1;
+            ++launches;
+          }
+          mid_pre = a;
+        }
+        {
+          Timed tm(w, s, "fused_restrict");
+          plain_restrict(s, M.dm, C.dm, M.div, C.div);
+          ++launches;
+        }
+        int coarse = 0;
+        {
+          int a = 0;
+          for (int k = 0; k < st.q[6]; ++k) {
+            Timed tm(w, s, "fused_sweep_coarse");
+            FX_CK(lean_sweep(s, C.dm, C.div, k == 0 ? nullptr : C.p[a], C.p[a ^ 1], C.dm, nullptr));
+            a ^= 1;
+            ++launches;
+          }
+          coarse = a;
+        }
+        {
+          Timed tm(w, s, "fused_prolong");
+          plain_prolong(s, C.dm, M.dm, C.p[coarse], M.p[0]);
+          ++launches;
+        }
+        mid = mid_pre;
+        for (int k = 0; k < st.q[5]; ++k) {
+          Timed tm(w, s, "fused_sweep_mid");
+          FX_CK(lean_sweep(s, M.dm, M.div, M.p[mid], M.p[mid ^ 1], M.dm, nullptr));
+          mid ^= 1;
+          ++launches;
+        }
       }
       for (int k = 2; k <= m; ++k) {
         const bool add = prolong_live && k == m;

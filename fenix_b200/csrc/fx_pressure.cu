@@ -810,6 +810,11 @@ cudaError_t mg_lower_launch(cudaStream_t s, const LevelBuf& mid, const LevelBuf&
   return cudaGetLastError();
 }
 
+int multigrid_plan() {
+  static const int p = env_int("FENIX_MG_PLAN", 0, 0, 1);
+  return p;
+}
+
 int pressure_plan() {
   static const int p = env_int("FENIX_PRESSURE_PLAN", 0, 0, 1);
   return p;

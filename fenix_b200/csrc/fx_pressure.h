@@ -55,6 +55,9 @@ cudaError_t lean_prolong_zero(cudaStream_t s, Dims dm, float* dst, Dims mid, con
 cudaError_t mg_lower_launch(cudaStream_t s, const LevelBuf& mid, const LevelBuf& coarse, int mid_pre, int coarse_n, int mid_post,
                             unsigned* bar, int* mid_result);
 
+// Mid/coarse levels: 0 = kernel per sweep (default), 1 = one cooperative launch (FENIX_MG_PLAN=1).
+int multigrid_plan();
+
 // 0: per-voxel sweeps (default); 1: z-march passes (FENIX_PRESSURE_PLAN=1).
 int pressure_plan();
 

@@ -122,3 +122,23 @@ def test_partial_structs_and_masks():
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         _lib.load(str(tmp_path / "libfenixcuda.so"))
+
+
+def test_struct_layouts_match_the_c_compiler(tmp_path):
+    """The ctypes mirrors have the sizes and field offsets gcc gives the header's structs."""
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "fenix_cuda.h"\n'
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\","
+        "sizeof(fx_sim_options), sizeof(fx_runtime_params), sizeof(fx_quality), sizeof(fx_render_buffers),"
+        "sizeof(fx_debug_buffers), sizeof(fx_stats), sizeof(fx_kernel_time), offsetof(fx_sim_options, quality),"
+        "offsetof(fx_sim_options, stream), offsetof(fx_render_buffers, active_brick_info), offsetof(fx_stats, flags));return 0;}\n"
+    )
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [ctypes.sizeof(_lib.FxSimOptions), ctypes.sizeof(_lib.FxRuntimeParams), ctypes.sizeof(_lib.FxQuality),
+            ctypes.sizeof(_lib.FxRenderBuffers), ctypes.sizeof(_lib.FxDebugBuffers), ctypes.sizeof(_lib.FxStats),
+            ctypes.sizeof(_lib.FxKernelTime), _lib.FxSimOptions.quality.offset, _lib.FxSimOptions.stream.offset,
+            _lib.FxRenderBuffers.active_brick_info.offset, _lib.FxStats.flags.offset]
+    assert got == want
