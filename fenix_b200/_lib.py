@@ -182,6 +182,7 @@ PROTOTYPES = [
     ("fx_sim_read_active_counters", c_int32, [c_void_p, POINTER(c_uint64), POINTER(c_uint64)]),
     ("fx_sim_get_stream", c_int32, [c_void_p, POINTER(c_void_p)]),
     ("fx_sim_last_error", c_char_p, [c_void_p]),
+    ("fx_brick_flags_noalloc", c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_void_p, c_void_p]),
 ]
 
 # Test hooks exported beside the ABI (not declared in the public header).

@@ -390,6 +390,11 @@ bool field_ref(fx_sim* s, int id, void** ptr, size_t* count) {
 
 }  // namespace
 
+namespace fx {
+// The calling thread's fx_last_error message, for entry points outside this file.
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace fx
+
 extern "C" {
 
 int32_t fx_abi_version(void) { return FX_ABI_VERSION; }

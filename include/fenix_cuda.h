@@ -282,6 +282,27 @@ fx_status fx_sim_get_stream(fx_sim* sim, void** stream);
 /* The sticky error message of a handle ("" when none). */
 const char* fx_sim_last_error(fx_sim* sim);
 
+/* Brick flags of caller-owned fields, allocating nothing. No counterpart in the
+ * reference. It computes what compute-active-bricks.wgsl.ts:35-58 computes, for
+ * the density, temperature and reaction fields (width*height*depth floats each,
+ * x fastest) on the current device. It writes one uint32 flag (0 or 1) per 8^3
+ * brick to `flags` (ceil(w/8)*ceil(h/8)*ceil(d/8) entries, x fastest) and
+ * enqueues on `stream` (cudaStream_t, NULL for the legacy stream).
+ *
+ * It is for callers that cannot allocate device memory at the time of the
+ * call: a per-frame loop, where a cudaFree would wait for the whole device, or
+ * a process whose device memory its own arena has already reserved. It calls no
+ * cudaMalloc or cudaFree and no allocating library routine. Its scratch is a
+ * 1 MiB static device array, one summary byte per brick, so grids above
+ * 1,048,576 bricks are rejected with FX_ERR_INVALID_ARGUMENT before any CUDA
+ * call. The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress), with the device current, and should come before any
+ * stream capture. Nothing has to start at zero. There is one scratch array per
+ * device, so two calls in flight at once on one device race; calls on one
+ * stream are ordered. Errors go to fx_last_error(). */
+fx_status fx_brick_flags_noalloc(const float* density, const float* temperature, const float* reaction, uint32_t width,
+                                 uint32_t height, uint32_t depth, uint32_t* flags, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
