@@ -7,8 +7,12 @@ solve, projection) of the `plume_256` workload: 256^3 voxels, four floor plumes,
 a seeded synthetic developed-plume start state with ~18 % of bricks active.
 
 Metric: active-voxel-steps/s = sum over timed steps of the voxels in active
-bricks (the step's brick flags) / device time. Multi-GPU: one independent
-simulation per rank (replicas, weak scaling), time = max over ranks.
+bricks (the step's brick flags) / device time. The headline is the mixed
+precision step (fused kernels, scalar sets stored in FP16, f32 arithmetic);
+the line also times the plain FP32 step (one kernel per reference pass) and
+the fused FP32 step on the same workload, and states the error of the mixed
+and FP32 steps against the f64 oracle. Multi-GPU: one independent simulation
+per rank (replicas, weak scaling), time = max over ranks.
 
 `--impl reference` runs the reference's step on the host CPU instead: the f32
 CPU restatement of the WGSL step, with all host threads.
@@ -58,11 +62,11 @@ KERNEL_BYTES = {
 }
 
 
-def kernel_bytes(name: str, n: int, active: float, nb: int, launches_per_step: float):
+def kernel_bytes(name: str, n: int, active: float, nb: int, launches_per_step: float, storage: str = "f32"):
     """Algorithmic bytes of one launch of `name` (None when not modelled)."""
     from fenix_b200 import fused_bytes
 
-    spec = KERNEL_BYTES.get(name) or fused_bytes.KERNEL_BYTES.get(name)
+    spec = KERNEL_BYTES.get(name) or fused_bytes.kernel_bytes_table(storage).get(name)
     if spec is None:
         return None
     kind, per = spec
@@ -199,16 +203,26 @@ def run_reference(args):
     return 0
 
 
-def cpu_baseline_and_parity(args, wl, counts, kernels):
-    """Times the oracle on a bounded sample and checks the CUDA step against it."""
+PARITY_FIELDS = ("density", "temperature", "fuel", "reaction", "velocity_x", "velocity_y", "velocity_z", "brick_flags", "pressure")
+ERROR_FIELDS = ("density", "temperature", "fuel", "reaction", "velocity_x", "velocity_y", "velocity_z")
+
+
+def cpu_baseline_and_parity(args, wl, counts, kernels, storage):
+    """Times the f32 oracle on a bounded sample, checks the CUDA step bit for bit
+    against the oracle of the same storage, and states the error of the CUDA
+    step (and of the f32 fused step) against the f64 oracle."""
     from fenix_b200 import createCombustionVolumeSimulation, workloads
     from oracle import build as orc_build
     from oracle.oracle import OracleSimulation, num_threads
 
     orc_build.build()
     orc = OracleSimulation(wl.options, precision=32)
-    sim = createCombustionVolumeSimulation(wl.options, device=0, kernels=kernels)
-    for s in (orc, sim):
+    orc64 = OracleSimulation(wl.options, precision=64)
+    orc_same = orc if storage == "f32" else OracleSimulation(wl.options, precision=32, storage=storage)
+    sim = createCombustionVolumeSimulation(wl.options, device=0, kernels=kernels, storage=storage)
+    sim32 = None if storage == "f32" else createCombustionVolumeSimulation(wl.options, device=0, kernels="fused")
+    everyone = [s for s in (orc, orc64, orc_same, sim, sim32) if s is not None]
+    for s in set(everyone):
         s.updateSources(wl.sources)
         workloads.load_state(s, wl.state)
     active = 0
@@ -218,19 +232,75 @@ def cpu_baseline_and_parity(args, wl, counts, kernels):
         t0 = time.perf_counter()
         orc.step(k * wl.dt, wl.dt)
         el += time.perf_counter() - t0
-        sim.step(k * wl.dt, wl.dt)
+        for s in (orc64, sim, sim32) + (() if orc_same is orc else (orc_same,)):
+            if s is not None:
+                s.step(k * wl.dt, wl.dt)
         flags = orc.readField("brick_flags")
         active += int(counts[flags != 0].sum())
-        for name in ("density", "temperature", "fuel", "reaction", "velocity_x", "velocity_y", "velocity_z", "brick_flags", "pressure"):
-            a, b = sim.readField(name), orc.readField(name)
+        for name in PARITY_FIELDS:
+            a, b = sim.readField(name), orc_same.readField(name)
             if not np.array_equal(a.view(np.uint32), b.view(np.uint32)):
                 parity = False
-    sim.dispose()
-    orc.dispose()
+
+    def errors(s):
+        out = {}
+        for name in ERROR_FIELDS:
+            a, r = s.readField(name).astype(np.float64), orc64.readField(name).astype(np.float64)
+            out[name] = {"rel_l2": float(np.linalg.norm(a - r) / max(np.linalg.norm(r), 1e-300)), "max_abs": float(np.max(np.abs(a - r)))}
+        return out
+
+    err = {f"{storage}_{kernels}": errors(sim)}
+    if sim32 is not None:
+        err["f32_fused"] = errors(sim32)
+    for s in set(everyone):
+        s.dispose()
     return {
         "value": active / el, "unit": UNIT, "cores": num_threads(), "kind": "port",
         "sample": f"{args.cpu_steps} full steps of the same workload from the same start state (f32 restatement, OpenMP)",
-    }, {"steps": args.cpu_steps, "bit_exact_vs_oracle": parity}
+    }, {"steps": args.cpu_steps, "bit_exact_vs_oracle": parity, "oracle": f"f32 arithmetic, {storage} storage"}, {
+        "steps": args.cpu_steps, "against": "f64 oracle (same start state and steps)", "fields": err}
+
+
+def time_steps(args, wl, local, kernels, storage, pg):
+    """K steps of (kernels, storage) on a fresh simulation, device time on its
+    stream (max over ranks), after the warm-up steps."""
+    import torch
+
+    from fenix_b200 import createCombustionVolumeSimulation, workloads
+
+    sim = createCombustionVolumeSimulation(wl.options, device=local, kernels=kernels, storage=storage)
+    sim.updateSources(wl.sources)
+    workloads.load_state(sim, wl.state)
+    sim.setInstrumentation(count_active=True)
+    stream = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", local))
+    t = 0.0
+    for _ in range(args.warmup):
+        sim.step(t, wl.dt)
+        t += wl.dt
+    sim.synchronize()
+    sim.readActiveCounters()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        sim.step(t, wl.dt)
+        t += wl.dt
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    voxel_steps = sim.readActiveCounters()["voxelSteps"]
+    sim.dispose()
+    if pg:
+        tt = torch.tensor([ms], device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        ms = float(tt.item())
+        vv = torch.tensor([float(voxel_steps)], device="cuda", dtype=torch.float64)
+        pg.all_reduce(vv, op=pg.ReduceOp.SUM)
+        voxel_steps = int(vv.item())
+    return {"value": voxel_steps / (ms / 1e3), "ms_per_step": ms / args.steps, "kernels": kernels, "storage": storage}
 
 
 def main():
@@ -240,6 +310,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="fenix", choices=["fenix", "reference"])
     ap.add_argument("--kernels", default="fused", choices=["fused", "plain"])
+    ap.add_argument("--storage", default="f16", choices=["f16", "f32"], help="scalar-set storage of the headline step")
+    ap.add_argument("--no-compare", action="store_true", help="skip timing the FP32 plain and fused steps")
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
@@ -277,7 +349,9 @@ def main():
     n = res[0] * res[1] * res[2]
     counts = workloads.brick_voxel_counts(res)
     nb = counts.size
-    sim = createCombustionVolumeSimulation(wl.options, device=local, kernels=args.kernels)
+    if args.storage == "f16" and args.kernels != "fused":
+        raise SystemExit("FP16 storage runs on the fused kernels only")
+    sim = createCombustionVolumeSimulation(wl.options, device=local, kernels=args.kernels, storage=args.storage)
     sim.updateSources(wl.sources)
     workloads.load_state(sim, wl.state)
     sim.setInstrumentation(count_active=True)
@@ -340,7 +414,7 @@ def main():
     kernel_table = {}
     for name, v in ktimes.items():
         per_launch_ms = v["total_ms"] / max(v["launches"], 1)
-        b = kernel_bytes(name, n, active2, nb, v["launches"] / args.steps)
+        b = kernel_bytes(name, n, active2, nb, v["launches"] / args.steps, args.storage)
         kernel_table[name] = {
             "launches": v["launches"], "share": round(v["total_ms"] / total_kernel_ms, 4), "us_per_launch": round(per_launch_ms * 1e3, 2),
             "GBps": round(b / (per_launch_ms / 1e3) / 1e9, 1) if b else None,
@@ -348,7 +422,7 @@ def main():
     if top:
         name, v = top
         per_launch_ms = v["total_ms"] / max(v["launches"], 1)
-        b = kernel_bytes(name, n, active2, nb, v["launches"] / args.steps)
+        b = kernel_bytes(name, n, active2, nb, v["launches"] / args.steps, args.storage)
         achieved = b / (per_launch_ms / 1e3) / 1e9 if b else None
         roofline = {
             "kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
@@ -383,10 +457,20 @@ def main():
 
     sim.dispose()
 
+    # ---- the FP32 plain and fused steps on the same workload ----
+    compare = {}
+    if not args.no_compare:
+        for kernels, storage in (("plain", "f32"), ("fused", "f32")):
+            if (kernels, storage) != (args.kernels, args.storage):
+                r = time_steps(args, wl, local, kernels, storage, pg)
+                r["ratio"] = value / r["value"]
+                compare[f"{storage}_{kernels}"] = r
+
     cpu = None
     parity = None
+    error = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu, parity = cpu_baseline_and_parity(args, wl, counts, args.kernels)
+        cpu, parity, error = cpu_baseline_and_parity(args, wl, counts, args.kernels, args.storage)
 
     if pg:
         pg.barrier()
@@ -397,11 +481,13 @@ def main():
             "dtype": "f32", "data": "synthetic",
             "config": {
                 "workload": f"plume_{args.size}: {args.size}^3 grid, 4 floor plumes (scalar+velocity+igniter each), seeded "
-                            f"developed-plume start, 4/4/4/4/20 sweeps, dt 1/60, f32, parity semantics",
-                "kernels": args.kernels, "cuda_graph": bool(st_timed.get("graphReplay")), "active_fraction": active_mean / n, "global_batch": world, "seq_len": 0,
+                            f"developed-plume start, 4/4/4/4/20 sweeps, dt 1/60, f32 arithmetic, {args.storage} scalar storage, "
+                            f"reference semantics",
+                "kernels": args.kernels, "scalar_storage": args.storage, "cuda_graph": bool(st_timed.get("graphReplay")), "active_fraction": active_mean / n, "global_batch": world, "seq_len": 0,
                 "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (about 2 GB of fields per step)",
             },
             "roofline": roofline, "kernels": kernel_table, "cpu_baseline": cpu, "parity_full_size": parity, "e2e": e2e,
+            "compare": compare, "error_vs_f64": error,
             "gpu_launches": int(kernels_last * args.steps), "clocks": clock_info,
         }
         print(json.dumps(line))

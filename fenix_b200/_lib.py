@@ -28,6 +28,10 @@ FX_KERNELS_PLAIN = 1
 
 FX_OPT_DEBUG_FIELDS = 1 << 0
 FX_OPT_NO_GRAPHS = 1 << 1
+FX_OPT_SCALARS_F16 = 1 << 2
+
+FX_DTYPE_F32 = 0
+FX_DTYPE_F16 = 1
 
 FX_PARAM_WIND = 1 << 0
 FX_PARAM_WIND_STRENGTH = 1 << 1

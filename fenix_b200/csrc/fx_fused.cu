@@ -22,6 +22,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cuda_fp16.h>
+
 #include "fx_fused.h"
 #include "fx_pressure.h"
 
@@ -31,6 +33,63 @@ namespace {
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 constexpr int kBrickThreads = 256;
+
+// ------------------------------------------------------------- scalar storage
+// The scalar sets (density, temperature, fuel, reaction) are stored as float or,
+// with FP16 storage, as binary16. The kernels compute in f32 either way. Each
+// value the reference stores into one of those buffers goes through qS first
+// (round to the storage type and back), so everything read afterwards (the
+// brick summaries, the non-zero bits, later fields) sees the stored value.
+template <typename S>
+struct SSet {
+  S* f[4];
+};
+
+template <typename S>
+SSet<S> sset(const ScalarSet& s) {
+  SSet<S> o;
+  for (int k = 0; k < 4; ++k) o.f[k] = reinterpret_cast<S*>(s.f[k]);
+  return o;
+}
+
+FX_DEV float ldS(const float* p, uint32_t i) { return __ldg(p + i); }
+FX_DEV float ldS(const __half* p, uint32_t i) { return __half2float(__ldg(p + i)); }
+FX_DEV float rdS(const float* p, uint32_t i) { return p[i]; }
+FX_DEV float rdS(const __half* p, uint32_t i) { return __half2float(p[i]); }
+FX_DEV void stS(float* p, uint32_t i, float v) { p[i] = v; }
+FX_DEV void stS(__half* p, uint32_t i, float v) { p[i] = __float2half_rn(v); }
+
+template <typename S>
+FX_DEV float qS(float v);
+template <>
+FX_DEV float qS<float>(float v) {
+  return v;
+}
+template <>
+FX_DEV float qS<__half>(float v) {
+  return __half2float(__float2half_rn(v));
+}
+
+// tri_interp (sampling-scalar.wgsl.ts:11-34) over a stored scalar field.
+template <typename S>
+FX_DEV float tri_interp_s(const S* __restrict__ f, const Tri& c) {
+  const float x00 = mixv(ldS(f, c.i000), ldS(f, c.i100), c.fx);
+  const float x10 = mixv(ldS(f, c.i010), ldS(f, c.i110), c.fx);
+  const float x01 = mixv(ldS(f, c.i001), ldS(f, c.i101), c.fx);
+  const float x11 = mixv(ldS(f, c.i011), ldS(f, c.i111), c.fx);
+  return mixv(mixv(x00, x10, c.fy), mixv(x01, x11, c.fy), c.fz);
+}
+
+// Calls f(tag) where decltype(tag)::type is the storage type (float or __half).
+template <typename S>
+struct StorageTag {
+  using type = S;
+};
+template <typename F>
+void by_storage(bool half, F&& f) {
+  if (half) f(StorageTag<__half>{});
+  else f(StorageTag<float>{});
+}
 
 __global__ void k_count_flags(const uint32_t* __restrict__ flags, uint32_t nb, uint32_t* __restrict__ out) {
   uint32_t local = 0;
@@ -126,9 +185,10 @@ FX_DEV uint8_t summary_of(const Energy& e) {
 }
 
 // ------------------------------------------------------------------ injection
+template <typename S>
 __global__ void __launch_bounds__(kBrickThreads) k_inject(Dims dm, uint3 bc, const Params* __restrict__ Pp, const float* __restrict__ src,
                                                           uint32_t nsrc, const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
-                                                          ScalarSet set, VelField v, uint8_t* __restrict__ summary, uint8_t* __restrict__ nz) {
+                                                          SSet<S> set, VelField v, uint8_t* __restrict__ summary, uint8_t* __restrict__ nz) {
   const Params P = *Pp;
   const uint32_t n = *count;
   for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
@@ -145,11 +205,15 @@ __global__ void __launch_bounds__(kBrickThreads) k_inject(Dims dm, uint3 bc, con
       if (inside) {
         const uint32_t i = flat(dm, x, y, z);
         const float px = ((float)x + 0.5f) / (float)dm.w, py = ((float)y + 0.5f) / (float)dm.h, pz = ((float)z + 0.5f) / (float)dm.d;
-        d = set.f[0][i];
-        t = set.f[1][i];
-        f = set.f[2][i];
-        r = set.f[3][i];
+        d = rdS(set.f[0], i);
+        t = rdS(set.f[1], i);
+        f = rdS(set.f[2], i);
+        r = rdS(set.f[3], i);
         inject_scalar_voxel(P, src, nsrc, px, py, pz, d, t, f);
+        // inject-scalar stores d, T, f here; inject-igniter reads them back
+        d = qS<S>(d);
+        t = qS<S>(t);
+        f = qS<S>(f);
         float vx = v.c[0][i], vy = v.c[1][i], vz = v.c[2][i];
         inject_velocity_voxel(P, src, nsrc, px, py, pz, vx, vy, vz);
         const float lim = speed_limit(P);
@@ -157,10 +221,12 @@ __global__ void __launch_bounds__(kBrickThreads) k_inject(Dims dm, uint3 bc, con
         v.c[1][i] = clampv(vy, -lim, lim);
         v.c[2][i] = clampv(vz, -lim, lim);
         inject_igniter_voxel(P, src, nsrc, px, py, pz, f, r, t);
-        set.f[0][i] = d;
-        set.f[1][i] = t;
-        set.f[2][i] = f;
-        set.f[3][i] = r;
+        r = qS<S>(r);
+        t = qS<S>(t);
+        stS(set.f[0], i, d);
+        stS(set.f[1], i, t);
+        stS(set.f[2], i, f);
+        stS(set.f[3], i, r);
         any = any || d != 0.f || t != 0.f || f != 0.f || r != 0.f;
       }
       energy_vote(c, x, y, z, inside, d, t, r, e);
@@ -263,10 +329,11 @@ __global__ void __launch_bounds__(256) k_advect_velocity(Dims dm, const Params* 
 // advect-scalar-maccormack.wgsl.ts:33-101 / advect-scalar-semilagrangian.wgsl.ts
 // over the bricks of list_adv: flagged bricks are advected into T, the others
 // (T may hold old values there) are zeroed. Emits T's brick summary and non-zero bit.
-__global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3 bc, const Params* __restrict__ Pp, int mode, ScalarSet src,
+template <typename S>
+__global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3 bc, const Params* __restrict__ Pp, int mode, SSet<S> src,
                                                                   VelField vel, const uint32_t* __restrict__ flags,
                                                                   const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
-                                                                  ScalarSet dst, uint8_t* __restrict__ summary, uint8_t* __restrict__ nz) {
+                                                                  SSet<S> dst, uint8_t* __restrict__ summary, uint8_t* __restrict__ nz) {
   const Params P = *Pp;
   const uint32_t n = *count;
   for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
@@ -299,28 +366,30 @@ __global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3
           const Tri cr = tri_corners(dm, rx - 0.5f, ry - 0.5f, rz - 0.5f);
 #pragma unroll
           for (int f = 0; f < 4; ++f) {
-            const float predicted = tri_interp(src.f[f], cs);
-            const float recovered = tri_interp(src.f[f], cr);
-            const float original = __ldg(src.f[f] + ic);
+            const float predicted = tri_interp_s(src.f[f], cs);
+            const float recovered = tri_interp_s(src.f[f], cr);
+            const float original = ldS(src.f[f], ic);
             const float corrected = predicted + 0.5f * (original - recovered);
             out[f] = clampv(corrected, mn(original, predicted), mx(original, predicted));
           }
           noise = thermal_noise(P, cx, cy, cz);
         } else {
 #pragma unroll
-          for (int f = 0; f < 4; ++f) out[f] = tri_interp(src.f[f], cs);
+          for (int f = 0; f < 4; ++f) out[f] = tri_interp_s(src.f[f], cs);
           noise = thermal_noise(P, spx, spy, spz);
         }
         const float ny = ((float)y + 0.5f) / (float)dm.h;
         decay_scalars(P, ny, noise, out[0], out[1], out[2], out[3]);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) out[f] = qS<S>(out[f]);
         any = any || out[0] != 0.f || out[1] != 0.f || out[2] != 0.f || out[3] != 0.f;
       }
       if (inside) {
         const uint32_t i = flat(dm, x, y, z);
-        dst.f[0][i] = out[0];
-        dst.f[1][i] = out[1];
-        dst.f[2][i] = out[2];
-        dst.f[3][i] = out[3];
+        stS(dst.f[0], i, out[0]);
+        stS(dst.f[1], i, out[1]);
+        stS(dst.f[2], i, out[2]);
+        stS(dst.f[3], i, out[3]);
       }
       energy_vote(c, x, y, z, inside, out[0], out[1], out[3], e);
     }
@@ -337,10 +406,11 @@ __global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3
 // combustion-update.wgsl.ts:42-93 from T into the next set over list_next:
 // flagged bricks get the combustion update, the others copy T. Emits the next
 // set's brick summary and non-zero bit.
-__global__ void __launch_bounds__(kBrickThreads) k_combustion(Dims dm, uint3 bc, const Params* __restrict__ Pp, ScalarSet tset,
+template <typename S>
+__global__ void __launch_bounds__(kBrickThreads) k_combustion(Dims dm, uint3 bc, const Params* __restrict__ Pp, SSet<S> tset,
                                                               const uint32_t* __restrict__ flags, const uint32_t* __restrict__ list,
                                                               const uint32_t* __restrict__ count, const uint8_t* __restrict__ nz_t,
-                                                              const uint8_t* __restrict__ summary_t, ScalarSet dst,
+                                                              const uint8_t* __restrict__ summary_t, SSet<S> dst,
                                                               uint8_t* __restrict__ summary, uint8_t* __restrict__ nz) {
   const Params P = *Pp;
   const uint32_t n = *count;
@@ -361,26 +431,30 @@ __global__ void __launch_bounds__(kBrickThreads) k_combustion(Dims dm, uint3 bc,
       const uint32_t i = flat(dm, x, y, z);
       float d = 0.f, t = 0.f, f = 0.f, r = 0.f;
       if (t_nonzero || active) {
-        d = __ldg(tset.f[0] + i);
-        t = __ldg(tset.f[1] + i);
-        f = __ldg(tset.f[2] + i);
-        r = __ldg(tset.f[3] + i);
+        d = ldS(tset.f[0], i);
+        t = ldS(tset.f[1], i);
+        f = ldS(tset.f[2], i);
+        r = ldS(tset.f[3], i);
       }
       if (active) {
         auto hot = [&](uint32_t xx, uint32_t yy, uint32_t zz) {
           const uint32_t k = flat(dm, xx, yy, zz);
-          return comb_hot(__ldg(tset.f[1] + k), __ldg(tset.f[2] + k), __ldg(tset.f[3] + k));
+          return comb_hot(ldS(tset.f[1], k), ldS(tset.f[2], k), ldS(tset.f[3], k));
         };
         const float nsum = hot(inc(x, W1), y, z) + hot(dec(x), y, z) + hot(x, inc(y, H1), z) + hot(x, dec(y), z) + hot(x, y, inc(z, D1)) +
                            hot(x, y, dec(z));
         const float ny = ((float)y + 0.5f) / (float)dm.h;
         combustion_voxel(P, x, y, z, ny, nsum, d, t, f, r);
+        d = qS<S>(d);
+        t = qS<S>(t);
+        f = qS<S>(f);
+        r = qS<S>(r);
         energy_vote(c, x, y, z, true, d, t, r, e);
       }
-      dst.f[0][i] = d;
-      dst.f[1][i] = t;
-      dst.f[2][i] = f;
-      dst.f[3][i] = r;
+      stS(dst.f[0], i, d);
+      stS(dst.f[1], i, t);
+      stS(dst.f[2], i, f);
+      stS(dst.f[3], i, r);
       any = any || d != 0.f || t != 0.f || f != 0.f || r != 0.f;
     }
     const uint8_t s = summary_of(e);
@@ -394,7 +468,8 @@ __global__ void __launch_bounds__(kBrickThreads) k_combustion(Dims dm, uint3 bc,
 
 // ---------------------------------------------------------------------- buoyancy
 // apply-buoyancy.wgsl.ts:37-110 over the flagged bricks of list_next.
-__global__ void __launch_bounds__(kBrickThreads) k_buoyancy(Dims dm, uint3 bc, const Params* __restrict__ Pp, ScalarSet set,
+template <typename S>
+__global__ void __launch_bounds__(kBrickThreads) k_buoyancy(Dims dm, uint3 bc, const Params* __restrict__ Pp, SSet<S> set,
                                                             const uint32_t* __restrict__ flags, const uint32_t* __restrict__ list,
                                                             const uint32_t* __restrict__ count, VelField v) {
   const Params P = *Pp;
@@ -410,20 +485,20 @@ __global__ void __launch_bounds__(kBrickThreads) k_buoyancy(Dims dm, uint3 bc, c
       const uint32_t x = c.x0 + (lv & 7u), y = c.y0 + ((lv >> 3) & 7u), z = c.z0 + (lv >> 6);
       if (x >= dm.w || y >= dm.h || z >= dm.d) continue;
       const uint32_t i = flat(dm, x, y, z);
-      const float* D = set.f[0];
+      const S* D = set.f[0];
       auto hot = [&](uint32_t xx, uint32_t yy, uint32_t zz) {
         const uint32_t k = flat(dm, xx, yy, zz);
-        return buoy_hot(__ldg(set.f[1] + k), __ldg(set.f[3] + k));
+        return buoy_hot(ldS(set.f[1], k), ldS(set.f[3], k));
       };
       const float hot_gas = hot(x, y, z);
       const float tgx = (hot(inc(x, W1), y, z) - hot(dec(x), y, z)) * 0.5f;
       const float tgy = (hot(x, inc(y, H1), z) - hot(x, dec(y), z)) * 0.5f;
       const float tgz = (hot(x, y, inc(z, D1)) - hot(x, y, dec(z))) * 0.5f;
-      const float dgx = (__ldg(D + flat(dm, inc(x, W1), y, z)) - __ldg(D + flat(dm, dec(x), y, z))) * 0.5f;
-      const float dgy = (__ldg(D + flat(dm, x, inc(y, H1), z)) - __ldg(D + flat(dm, x, dec(y), z))) * 0.5f;
-      const float dgz = (__ldg(D + flat(dm, x, y, inc(z, D1))) - __ldg(D + flat(dm, x, y, dec(z)))) * 0.5f;
+      const float dgx = (ldS(D, flat(dm, inc(x, W1), y, z)) - ldS(D, flat(dm, dec(x), y, z))) * 0.5f;
+      const float dgy = (ldS(D, flat(dm, x, inc(y, H1), z)) - ldS(D, flat(dm, x, dec(y), z))) * 0.5f;
+      const float dgz = (ldS(D, flat(dm, x, y, inc(z, D1))) - ldS(D, flat(dm, x, y, dec(z)))) * 0.5f;
       float vx = v.c[0][i], vy = v.c[1][i], vz = v.c[2][i];
-      buoyancy_voxel(P, dm, x, y, z, __ldg(D + i), hot_gas, tgx, tgy, tgz, dgx, dgy, dgz, vx, vy, vz);
+      buoyancy_voxel(P, dm, x, y, z, ldS(D, i), hot_gas, tgx, tgy, tgz, dgx, dgy, dgz, vx, vy, vz);
       v.c[0][i] = vx;
       v.c[1][i] = vy;
       v.c[2][i] = vz;
@@ -463,8 +538,9 @@ __global__ void __launch_bounds__(256) k_vorticity(Dims dm, VelField v, float* _
 // apply-vorticity-confinement.wgsl.ts:30-66 from vScratch into vScratch2, with w
 // recomputed at the voxel and the scalars read only from bricks that may be
 // non-zero.
+template <typename S>
 __global__ void __launch_bounds__(256) k_confinement(Dims dm, uint3 bc, const Params* __restrict__ Pp, VelField v, const float* __restrict__ wmag,
-                                                     ScalarSet set, const uint8_t* __restrict__ nz, VelField out, float* __restrict__ fmag,
+                                                     SSet<S> set, const uint8_t* __restrict__ nz, VelField out, float* __restrict__ fmag,
                                                      int write_fmag) {
   const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -489,9 +565,9 @@ __global__ void __launch_bounds__(256) k_confinement(Dims dm, uint3 bc, const Pa
   const uint32_t b = (x >> 3) + bc.x * ((y >> 3) + bc.y * (z >> 3));
   float d = 0.f, t = 0.f, r = 0.f;
   if (__ldg(nz + b)) {
-    d = __ldg(set.f[0] + i);
-    t = __ldg(set.f[1] + i);
-    r = __ldg(set.f[3] + i);
+    d = ldS(set.f[0], i);
+    t = ldS(set.f[1], i);
+    r = ldS(set.f[3], i);
   }
   const float fm = confinement_voxel(P, gx, gy, gz, wx, wy, wz, __ldg(wmag + i), d, t, r, vx, vy, vz);
   out.c[0][i] = vx;
@@ -545,7 +621,8 @@ inline dim3 proj_grid(Dims d) { return dim3((d.w + 31) / 32, (d.h + 7) / 8, (d.d
 
 // Rebuilds the per-brick bookkeeping after the fields were written from the host:
 // the non-zero bits of the three scalar buffers and the summary of the current set.
-__global__ void __launch_bounds__(kBrickThreads) k_rebuild(Dims dm, uint3 bc, ScalarSet cur, ScalarSet other, ScalarSet tset,
+template <typename S>
+__global__ void __launch_bounds__(kBrickThreads) k_rebuild(Dims dm, uint3 bc, SSet<S> cur, SSet<S> other, SSet<S> tset,
                                                            uint8_t* __restrict__ summary_cur, uint8_t* __restrict__ nz_cur,
                                                            uint8_t* __restrict__ nz_other, uint8_t* __restrict__ nz_t) {
   const uint32_t nb = bc.x * bc.y * bc.z;
@@ -561,12 +638,12 @@ __global__ void __launch_bounds__(kBrickThreads) k_rebuild(Dims dm, uint3 bc, Sc
       float d = 0.f, t = 0.f, r = 0.f;
       if (inside) {
         const uint32_t i = flat(dm, x, y, z);
-        d = cur.f[0][i];
-        t = cur.f[1][i];
-        r = cur.f[3][i];
-        a0 = a0 || d != 0.f || t != 0.f || cur.f[2][i] != 0.f || r != 0.f;
-        a1 = a1 || other.f[0][i] != 0.f || other.f[1][i] != 0.f || other.f[2][i] != 0.f || other.f[3][i] != 0.f;
-        a2 = a2 || tset.f[0][i] != 0.f || tset.f[1][i] != 0.f || tset.f[2][i] != 0.f || tset.f[3][i] != 0.f;
+        d = rdS(cur.f[0], i);
+        t = rdS(cur.f[1], i);
+        r = rdS(cur.f[3], i);
+        a0 = a0 || d != 0.f || t != 0.f || rdS(cur.f[2], i) != 0.f || r != 0.f;
+        a1 = a1 || rdS(other.f[0], i) != 0.f || rdS(other.f[1], i) != 0.f || rdS(other.f[2], i) != 0.f || rdS(other.f[3], i) != 0.f;
+        a2 = a2 || rdS(tset.f[0], i) != 0.f || rdS(tset.f[1], i) != 0.f || rdS(tset.f[2], i) != 0.f || rdS(tset.f[3], i) != 0.f;
       }
       energy_vote(c, x, y, z, inside, d, t, r, e);
     }
@@ -766,7 +843,11 @@ fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
 
   if (!w.valid) {
     Timed tm(w, s, "fused_rebuild");
-    k_rebuild<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.cur, st.next, st.scratch, w.summary_set[cur], w.nz_set[cur], w.nz_set[next], w.nz_t);
+    by_storage(st.half_storage, [&](auto tag) {
+      using S = typename decltype(tag)::type;
+      k_rebuild<S><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, sset<S>(st.cur), sset<S>(st.next), sset<S>(st.scratch), w.summary_set[cur],
+                                                        w.nz_set[cur], w.nz_set[next], w.nz_t);
+    });
     ++launches;
     w.valid = true;
   }
@@ -851,8 +932,11 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   uint32_t* c_inj = w.counters + 3;
   if (ninj) {
     Timed tm(w, s, "fused_inject");
-    k_inject<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.sources, st.nsrc, w.list_inj, c_inj, st.cur, st.vcur,
-                                                   w.summary_set[cur], w.nz_set[cur]);
+    by_storage(st.half_storage, [&](auto tag) {
+      using S = typename decltype(tag)::type;
+      k_inject<S><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.sources, st.nsrc, w.list_inj, c_inj, sset<S>(st.cur), st.vcur,
+                                                       w.summary_set[cur], w.nz_set[cur]);
+    });
     ++launches;
   }
 
@@ -873,8 +957,11 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   FX_CK(cudaMemsetAsync(w.summary_t, 0, nb, s));
   {
     Timed tm(w, s, "fused_advect_scalars");
-    k_advect_scalars<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.advect_mode, st.cur, st.vscr, st.flags_cur, w.list_adv, c_adv,
-                                                          st.scratch, w.summary_t, w.nz_t);
+    by_storage(st.half_storage, [&](auto tag) {
+      using S = typename decltype(tag)::type;
+      k_advect_scalars<S><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.advect_mode, sset<S>(st.cur), st.vscr, st.flags_cur,
+                                                               w.list_adv, c_adv, sset<S>(st.scratch), w.summary_t, w.nz_t);
+    });
     ++launches;
   }
   // 5. flags of the advected set
@@ -887,13 +974,19 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   FX_CK(cudaMemsetAsync(w.summary_set[next], 0, nb, s));
   {
     Timed tm(w, s, "fused_combustion");
-    k_combustion<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.scratch, st.flags_next, w.list_next, c_next, w.nz_t, w.summary_t,
-                                                      st.next, w.summary_set[next], w.nz_set[next]);
+    by_storage(st.half_storage, [&](auto tag) {
+      using S = typename decltype(tag)::type;
+      k_combustion<S><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, sset<S>(st.scratch), st.flags_next, w.list_next, c_next, w.nz_t,
+                                                           w.summary_t, sset<S>(st.next), w.summary_set[next], w.nz_set[next]);
+    });
     ++launches;
   }
   {
     Timed tm(w, s, "fused_buoyancy");
-    k_buoyancy<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.next, st.flags_next, w.list_next, c_next, st.vscr);
+    by_storage(st.half_storage, [&](auto tag) {
+      using S = typename decltype(tag)::type;
+      k_buoyancy<S><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, sset<S>(st.next), st.flags_next, w.list_next, c_next, st.vscr);
+    });
     ++launches;
   }
   // 8. vorticity confinement
@@ -906,8 +999,11 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     }
     {
       Timed tm(w, s, "fused_confinement");
-      k_confinement<<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, bc, st.params, st.vscr, st.vort_mag, st.next, w.nz_set[next], st.vscr2,
-                                                           st.conf_mag, st.debug_fields ? 1 : 0);
+      by_storage(st.half_storage, [&](auto tag) {
+        using S = typename decltype(tag)::type;
+        k_confinement<S><<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, bc, st.params, st.vscr, st.vort_mag, sset<S>(st.next), w.nz_set[next],
+                                                                st.vscr2, st.conf_mag, st.debug_fields ? 1 : 0);
+      });
       ++launches;
     }
     vfinal = &st.vscr2;

@@ -79,7 +79,8 @@ struct FusedStep {
   uint32_t host_nsrc;
   int advect_mode;
   int cur_index;  // index of the current scalar set (0 or 1)
-  ScalarSet cur, next, scratch;
+  ScalarSet cur, next, scratch;  // float* each, or binary16 buffers when half_storage
+  bool half_storage;
   uint32_t *flags_cur, *flags_next;
   VelField vcur, vscr, vscr2, vort;
   float *vort_mag, *conf_mag, *vel_mag;

@@ -12,6 +12,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda_fp16.h>
+
 #include "../../include/fenix_cuda.h"
 #include "fx_fused.h"
 #include "fx_kernels.h"
@@ -92,6 +94,7 @@ struct fx_sim {
   uint32_t nb = 0;
   int kernels = FX_KERNELS_FUSED;
   uint32_t opt_flags = 0;
+  bool half = false;  // FX_OPT_SCALARS_F16: the scalar sets are binary16 buffers
 
   // device memory
   void* arena = nullptr;
@@ -355,7 +358,9 @@ fx_status step_plain(fx_sim* s, bool vort_on, bool pressure_on, bool debug_on) {
   return FX_OK;
 }
 
-// Pointer of a field for read/write, with its element count and element size.
+bool is_scalar_field(int id) { return id >= FX_FIELD_DENSITY && id <= FX_FIELD_PREV_REACTION; }
+
+// Pointer of a field for read/write, with its element count.
 bool field_ref(fx_sim* s, int id, void** ptr, size_t* count) {
   const int prev = s->cur ^ 1;
   *count = s->n;
@@ -451,6 +456,8 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
     return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_create: unknown scalar_advection_mode");
   if (opt.kernels != FX_KERNELS_FUSED && opt.kernels != FX_KERNELS_PLAIN)
     return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_create: unknown kernels path");
+  if ((opt.flags & FX_OPT_SCALARS_F16) && opt.kernels != FX_KERNELS_FUSED)
+    return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_sim_create: FP16 scalar storage needs the fused kernels");
 
   fx_sim* s = new (std::nothrow) fx_sim;
   if (!s) return fail(nullptr, FX_ERR_OUT_OF_MEMORY, "fx_sim_create: host allocation failed");
@@ -462,6 +469,7 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
   s->device = opt.device;
   s->kernels = opt.kernels;
   s->opt_flags = opt.flags;
+  s->half = (opt.flags & FX_OPT_SCALARS_F16) != 0;
   s->dm = Dims{w, h, d};
   s->n = w * h * d;
   s->bricks = make_uint3((w + 7) / 8, (h + 7) / 8, (d + 7) / 8);
@@ -506,7 +514,7 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
   };
   size_t o_sets[3][4], o_vcur[3], o_vscr[3], o_vscr2[3], o_vort[3], o_wmag, o_fmag, o_vmag, o_flags[2], o_lv[3][3], o_params;
   for (auto& set : o_sets)
-    for (auto& f : set) f = carve(n * 4);
+    for (auto& f : set) f = carve(n * (s->half ? 2 : 4));
   for (int c = 0; c < 3; ++c) {
     o_vcur[c] = carve(n * 4);
     o_vscr[c] = carve(n * 4);
@@ -640,6 +648,7 @@ fx_status fx_sim_step(fx_sim* s, double elapsed, double step_s) {
     fs.cur = s->sets[s->cur];
     fs.next = s->sets[s->cur ^ 1];
     fs.scratch = s->sets[2];
+    fs.half_storage = s->half;
     fs.flags_cur = s->flags[s->cur];
     fs.flags_next = s->flags[s->cur ^ 1];
     fs.vcur = s->vcur;
@@ -697,7 +706,7 @@ fx_status fx_sim_get_render_buffers(fx_sim* s, fx_render_buffers* o) {
   o->width = s->dm.w;
   o->height = s->dm.h;
   o->depth = s->dm.d;
-  o->dtype = FX_DTYPE_F32;
+  o->dtype = s->half ? FX_DTYPE_F16 : FX_DTYPE_F32;
   return FX_OK;
 }
 
@@ -808,6 +817,14 @@ fx_status fx_sim_read_field(fx_sim* s, int32_t id, void* dst, size_t bytes) {
   FX_CUDA(s, cudaStreamSynchronize(s->stream));
   if (fused_check_device_error(s->fw, s->stream) == FX_ERR_TIMEOUT)
     return fail(s, FX_ERR_TIMEOUT, "a grid barrier of the pressure solve timed out; the results of that step are invalid");
+  if (s->half && is_scalar_field(id)) {
+    // binary16 on the device, f32 at the ABI (exact widening)
+    std::vector<__half> tmp(count);
+    FX_CUDA(s, cudaMemcpy(tmp.data(), p, count * sizeof(__half), cudaMemcpyDeviceToHost));
+    float* out = static_cast<float*>(dst);
+    for (size_t i = 0; i < count; ++i) out[i] = __half2float(tmp[i]);
+    return FX_OK;
+  }
   FX_CUDA(s, cudaMemcpy(dst, p, bytes, cudaMemcpyDeviceToHost));
   return FX_OK;
 }
@@ -820,7 +837,15 @@ fx_status fx_sim_write_field(fx_sim* s, int32_t id, const void* src, size_t byte
   if (bytes != count * 4) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_write_field: byte count does not match the field");
   FX_CUDA(s, cudaSetDevice(s->device));
   FX_CUDA(s, cudaStreamSynchronize(s->stream));
-  FX_CUDA(s, cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice));
+  if (s->half && is_scalar_field(id)) {
+    // f32 at the ABI, rounded to the nearest binary16 (ties to even) on the device
+    std::vector<__half> tmp(count);
+    const float* in = static_cast<const float*>(src);
+    for (size_t i = 0; i < count; ++i) tmp[i] = __float2half_rn(in[i]);
+    FX_CUDA(s, cudaMemcpy(p, tmp.data(), count * sizeof(__half), cudaMemcpyHostToDevice));
+  } else {
+    FX_CUDA(s, cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice));
+  }
   // A scratch velocity written here is what the next read returns.
   return fused_invalidate(s->fw, s->stream);
 }

@@ -157,6 +157,7 @@ def _pointer_dict(rb: FxRenderBuffers) -> Dict[str, Any]:
         "reaction": rb.reaction,
         "activeBrickFlags": rb.active_brick_flags,
         "activeBrickInfo": list(rb.active_brick_info),
+        "dtype": "f16" if rb.dtype == _lib.FX_DTYPE_F16 else "f32",
     }
 
 
@@ -303,9 +304,15 @@ class CombustionVolumeSimulation:
             pass
 
 
+STORAGE = {"f32": 0, "f16": _lib.FX_OPT_SCALARS_F16}
+
+
 def build_options(options: Optional[Mapping[str, Any]] = None, *, device: int = 0, kernels: str = "fused",
-                  debug_fields: bool = False, use_graphs: bool = True) -> FxSimOptions:
-    """CombustionVolumeSimulationOptions -> fx_sim_options."""
+                  debug_fields: bool = False, use_graphs: bool = True, storage: str = "f32") -> FxSimOptions:
+    """CombustionVolumeSimulationOptions -> fx_sim_options. storage="f16" stores the
+    scalar sets in binary16 (fused kernels only)."""
+    if storage not in STORAGE:
+        raise ValueError(f"unknown storage {storage!r}; expected one of {sorted(STORAGE)}")
     lib = _lib.load()
     opt = FxSimOptions()
     lib.fx_sim_options_default(ctypes.byref(opt))
@@ -331,15 +338,15 @@ def build_options(options: Optional[Mapping[str, Any]] = None, *, device: int = 
         opt.runtime_mask = rmask
     opt.device = device
     opt.kernels = KERNEL_PATHS[kernels]
-    opt.flags = (_lib.FX_OPT_DEBUG_FIELDS if debug_fields else 0) | (0 if use_graphs else _lib.FX_OPT_NO_GRAPHS)
+    opt.flags = (_lib.FX_OPT_DEBUG_FIELDS if debug_fields else 0) | (0 if use_graphs else _lib.FX_OPT_NO_GRAPHS) | STORAGE[storage]
     return opt
 
 
 def createCombustionVolumeSimulation(options: Optional[Mapping[str, Any]] = None, *, device: int = 0, kernels: str = "fused",
-                                     debug_fields: bool = False, use_graphs: bool = True) -> CombustionVolumeSimulation:
+                                     debug_fields: bool = False, use_graphs: bool = True, storage: str = "f32") -> CombustionVolumeSimulation:
     """createCombustionVolumeSimulation.ts:50-401 on CUDA device `device`."""
     lib = _lib.load()
-    opt = build_options(options, device=device, kernels=kernels, debug_fields=debug_fields, use_graphs=use_graphs)
+    opt = build_options(options, device=device, kernels=kernels, debug_fields=debug_fields, use_graphs=use_graphs, storage=storage)
     handle = ctypes.c_void_p()
     check(lib.fx_sim_create(ctypes.byref(opt), ctypes.byref(handle)))
     return CombustionVolumeSimulation(handle, lib)

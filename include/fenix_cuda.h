@@ -105,9 +105,16 @@ typedef struct fx_runtime_params {
 #define FX_KERNELS_FUSED 0 /* default: fused, brick-list-driven kernels */
 #define FX_KERNELS_PLAIN 1 /* one kernel per reference WGSL pass (the plain FP32 step) */
 
-/* Option flags (extensions; none changes results). */
+/* Option flags (extensions). The first two do not change results. */
 #define FX_OPT_DEBUG_FIELDS (1u << 0) /* always write vorticity, |vorticity|, |F_conf| */
 #define FX_OPT_NO_GRAPHS (1u << 1)    /* launch kernels directly instead of CUDA graphs */
+/* FP16 storage of the scalar sets (density, temperature, fuel, reaction); fused
+ * kernels only (FX_ERR_UNSUPPORTED with FX_KERNELS_PLAIN). Arithmetic stays f32;
+ * every value a reference pass stores into a scalar buffer is rounded to the
+ * nearest binary16 (ties to even). Velocity and pressure stay f32. Field reads
+ * and writes still exchange f32 (writes are rounded), and the render buffers
+ * report FX_DTYPE_F16. */
+#define FX_OPT_SCALARS_F16 (1u << 2)
 
 /* CombustionVolumeSimulationOptions (createCombustionVolumeSimulation.ts:39-48).
  * Fill with fx_sim_options_default() and then override fields. */
@@ -137,10 +144,11 @@ typedef struct fx_render_buffers {
   uint64_t active_brick_flags; /* uint32 per brick, 1 = active */
   uint32_t active_brick_info[8];
   uint32_t width, height, depth;
-  int32_t dtype; /* FX_DTYPE_F32 */
+  int32_t dtype; /* FX_DTYPE_F32, or FX_DTYPE_F16 (IEEE binary16) with FX_OPT_SCALARS_F16 */
 } fx_render_buffers;
 
 #define FX_DTYPE_F32 0
+#define FX_DTYPE_F16 1
 
 /* getDebugBuffers() (createCombustionVolumeSimulation.ts:313-326). */
 typedef struct fx_debug_buffers {

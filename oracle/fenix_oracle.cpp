@@ -20,6 +20,9 @@
 //                   for bit. This instantiation is also the timed CPU baseline.
 //   Real = double : the accuracy reference (libm sin/cos), used to state the f32
 //                   and f16-storage error of the CUDA path.
+// Either instantiation can store the scalar sets in binary16 (orc_set_half_storage):
+// each value a reference pass writes to density, temperature, fuel or reaction is
+// rounded to the nearest binary16, ties to even, as the CUDA FP16-storage path does.
 //
 // WGSL builtin semantics used throughout (WGSL spec formulas):
 //   mix(a,b,t) = a*(1-t) + b*t;  smoothstep(e0,e1,x) = t*t*(3-2t), t=clamp((x-e0)/(e1-e0),0,1)
@@ -246,6 +249,11 @@ template <class R> class Sim {
   Quality q;
   int advect_mode = 1;         // 0 semi-lagrangian, 1 maccormack
   bool emit_dead_residual = false;
+  // FP16 storage of the scalar sets (density, temperature, fuel, reaction): every
+  // value a reference pass stores into one of those buffers is rounded to the
+  // nearest binary16 (ties to even) and read back as R. Arithmetic stays in R.
+  bool half_storage = false;
+  R qs(R v) const { return half_storage ? (R)(_Float16)v : v; }
   // runtime params (createCombustionVolumeSimulation.ts:194-204)
   double wind[3] = {0, 0, 0}, wind_strength = 0, gravity[3] = {0, -1, 0}, gravity_strength = 0.45;
   double buoyancy = 3.6, vorticity_strength = 2.15;
@@ -435,9 +443,9 @@ template <class R> class Sim {
         tt = clamp01(tt + s.yt * contribution);
         ff = clamp01(ff + s.yf * contribution);
       }
-      D[i] = dd;
-      T[i] = tt;
-      Fu[i] = ff;
+      D[i] = qs(dd);
+      T[i] = qs(tt);
+      Fu[i] = qs(ff);
     });
   }
 
@@ -534,8 +542,8 @@ template <class R> class Sim {
         rr = clamp01(rr + seed);
         tt = clamp01(tt + intensity * weight * R(P.dt) * K(4.0));
       }
-      Re[i] = rr;
-      T[i] = tt;
+      Re[i] = qs(rr);
+      T[i] = qs(tt);
     });
   }
 
@@ -641,10 +649,10 @@ template <class R> class Sim {
     const R cold_breakup = dt * density * (R(1) - smoothstepv(K(0.2), K(0.86), hot)) * smoothstepv(K(0.18), K(0.72), density) *
                            smoothstepv(K(0.34), K(0.92), noise) * K(0.34);
     const R clearing = dt * density * hot * mixv(K(0.1), K(0.72), noise);
-    sc[dst][0][i] = clamp01(mx(R(0), density * (R(1) - smoke_loss) - clearing - cold_breakup));
-    sc[dst][1][i] = clamp01(mx(R(0), temperature - cooling));
-    sc[dst][2][i] = clamp01(mx(R(0), fuel - dt * mixv(K(0.012), K(0.034), noise)));
-    sc[dst][3][i] = clamp01(mx(R(0), reaction - dt * mixv(K(0.46), K(0.82), noise)));
+    sc[dst][0][i] = qs(clamp01(mx(R(0), density * (R(1) - smoke_loss) - clearing - cold_breakup)));
+    sc[dst][1][i] = qs(clamp01(mx(R(0), temperature - cooling)));
+    sc[dst][2][i] = qs(clamp01(mx(R(0), fuel - dt * mixv(K(0.012), K(0.034), noise))));
+    sc[dst][3][i] = qs(clamp01(mx(R(0), reaction - dt * mixv(K(0.46), K(0.82), noise))));
   }
 
   // shaders/passes/advect-scalar-maccormack.wgsl.ts:33-101 (set src -> set dst,
@@ -750,10 +758,10 @@ template <class R> class Sim {
       const R clearing = d * smoothstepv(K(0.18), K(0.82), t + r * K(0.22) + f * K(0.1)) * dt * mixv(K(0.55), K(2.45), hot_pocket);
       const R cooling_smoke = d * t * (cooling_pocket + hot_soot * K(0.32)) * dt * K(0.16);
       const R reaction_decay = r * (R(1) - dt * mixv(K(0.68), K(0.22), hot_pocket));
-      sc[set][2][i] = clamp01(f - burn);
-      sc[set][1][i] = clamp01(t + burn * mixv(K(2.1), K(3.25), hot_pocket) + radiative - heat_loss);
-      sc[set][0][i] = clamp01(mx(R(0), d + smoke_yield + cooling_smoke - density_loss - clearing * K(0.72)));
-      sc[set][3][i] = clamp01(mx(reaction_decay, burn * mixv(K(4.0), K(7.5), hot_pocket) + radiative * K(1.8)));
+      sc[set][2][i] = qs(clamp01(f - burn));
+      sc[set][1][i] = qs(clamp01(t + burn * mixv(K(2.1), K(3.25), hot_pocket) + radiative - heat_loss));
+      sc[set][0][i] = qs(clamp01(mx(R(0), d + smoke_yield + cooling_smoke - density_loss - clearing * K(0.72))));
+      sc[set][3][i] = qs(clamp01(mx(reaction_decay, burn * mixv(K(4.0), K(7.5), hot_pocket) + radiative * K(1.8))));
     });
   }
 
@@ -1302,7 +1310,17 @@ long orc_read_field(void* hv, int id, double* dst, long cap) {
   });
 }
 
-// Overwrites field `id` from float64 values (rounded to the oracle precision).
+// Switches FP16 storage of the scalar sets on (1) or off (0); set it before the
+// first step or field write.
+void orc_set_half_storage(void* hv, int on) {
+  dispatch(static_cast<Handle*>(hv), [&](auto* s) {
+    s->half_storage = on != 0;
+    return 0;
+  });
+}
+
+// Overwrites field `id` from float64 values (rounded to the oracle precision,
+// and to binary16 for scalar fields under FP16 storage).
 long orc_write_field(void* hv, int id, const double* src, long count) {
   return dispatch(static_cast<Handle*>(hv), [&](auto* s) -> long {
     size_t n = 0;
@@ -1315,7 +1333,8 @@ long orc_write_field(void* hv, int id, const double* src, long count) {
     }
     auto* p = s->field_ptr(id, &n);
     if (!p || (long)n != count) return 0;
-    for (size_t i = 0; i < n; ++i) p[i] = (R)src[i];
+    const bool scalar = id >= F_DENSITY && id <= F_PREV_REACTION;
+    for (size_t i = 0; i < n; ++i) p[i] = scalar ? s->qs((R)src[i]) : (R)src[i];
     return (long)n;
   });
 }

@@ -41,6 +41,7 @@ def load() -> ctypes.CDLL:
         lib.orc_set_quality.argtypes = [c_void_p, POINTER(c_int)]
         lib.orc_set_advection_mode.argtypes = [c_void_p, c_int]
         lib.orc_set_emit_dead_residual.argtypes = [c_void_p, c_int]
+        lib.orc_set_half_storage.argtypes = [c_void_p, c_int]
         lib.orc_update_sources.argtypes = [c_void_p, POINTER(c_float), c_uint32]
         lib.orc_step.argtypes = [c_void_p, c_double, c_double]
         lib.orc_prepare_params.argtypes = [c_void_p, c_double, c_double]
@@ -97,9 +98,12 @@ def num_threads() -> int:
 
 
 class OracleSimulation:
-    """The reference step on the CPU, in f32 (precision=32) or f64 (precision=64)."""
+    """The reference step on the CPU, in f32 (precision=32) or f64 (precision=64).
 
-    def __init__(self, options: Optional[Mapping[str, Any]] = None, precision: int = 32):
+    storage="f16" stores the scalar sets in binary16: every value a pass writes to
+    density, temperature, fuel or reaction is rounded to the nearest binary16."""
+
+    def __init__(self, options: Optional[Mapping[str, Any]] = None, precision: int = 32, storage: str = "f32"):
         self._lib = load()
         options = dict(options or {})
         w, h, d = _resolution_tuple(options.pop("resolution", None))
@@ -108,6 +112,10 @@ class OracleSimulation:
         self._h = self._lib.orc_create(precision, w, h, d)
         if not self._h:
             raise ValueError("orc_create rejected the arguments")
+        if storage not in ("f32", "f16"):
+            raise ValueError(f"unknown storage {storage!r}")
+        self.storage = storage
+        self._lib.orc_set_half_storage(self._h, 1 if storage == "f16" else 0)
         self._runtime = dict(DEFAULT_RUNTIME)
         mode = options.pop("scalarAdvectionMode", None)
         self._mode = "maccormack"

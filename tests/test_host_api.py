@@ -142,3 +142,18 @@ def test_struct_layouts_match_the_c_compiler(tmp_path):
             ctypes.sizeof(_lib.FxKernelTime), _lib.FxSimOptions.quality.offset, _lib.FxSimOptions.stream.offset,
             _lib.FxRenderBuffers.active_brick_info.offset, _lib.FxStats.flags.offset]
     assert got == want
+
+
+@pytest.mark.skipif(not os.path.exists(_lib.LIB_PATH), reason="libfenixcuda.so not built on this machine")
+def test_f16_storage_needs_the_fused_kernels():
+    """Checked before any CUDA call, so it runs without a GPU."""
+    from fenix_b200.simulation import build_options
+
+    lib = _lib.load()
+    opt = build_options({"resolution": (16, 16, 16)}, kernels="plain", storage="f16")
+    assert opt.flags & _lib.FX_OPT_SCALARS_F16
+    h = ctypes.c_void_p()
+    assert lib.fx_sim_create(ctypes.byref(opt), ctypes.byref(h)) == _lib.FX_ERR_UNSUPPORTED
+    assert b"FP16" in lib.fx_last_error()
+    with pytest.raises(ValueError):
+        build_options(storage="bf16")
