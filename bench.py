@@ -261,9 +261,9 @@ def cpu_baseline_and_parity(args, wl, counts, kernels, storage):
         "steps": args.cpu_steps, "against": "f64 oracle (same start state and steps)", "fields": err}
 
 
-def time_steps(args, wl, local, kernels, storage, pg):
-    """K steps of (kernels, storage) on a fresh simulation, device time on its
-    stream (max over ranks), after the warm-up steps."""
+def time_steps(args, wl, local, kernels, storage, pg, solver=None):
+    """K steps of (kernels, storage[, solver]) on a fresh simulation, device time
+    on its stream (max over ranks), after the warm-up steps."""
     import torch
 
     from fenix_b200 import createCombustionVolumeSimulation, workloads
@@ -272,6 +272,8 @@ def time_steps(args, wl, local, kernels, storage, pg):
     sim.updateSources(wl.sources)
     workloads.load_state(sim, wl.state)
     sim.setInstrumentation(count_active=True)
+    if solver:
+        sim.setSolver(solver)
     stream = torch.cuda.ExternalStream(sim.stream, device=torch.device("cuda", local))
     t = 0.0
     for _ in range(args.warmup):
@@ -292,6 +294,7 @@ def time_steps(args, wl, local, kernels, storage, pg):
     ev1.synchronize()
     ms = ev0.elapsed_time(ev1)
     voxel_steps = sim.readActiveCounters()["voxelSteps"]
+    solver_stats = sim.readSolverStats() if solver else None
     sim.dispose()
     if pg:
         tt = torch.tensor([ms], device="cuda")
@@ -300,7 +303,11 @@ def time_steps(args, wl, local, kernels, storage, pg):
         vv = torch.tensor([float(voxel_steps)], device="cuda", dtype=torch.float64)
         pg.all_reduce(vv, op=pg.ReduceOp.SUM)
         voxel_steps = int(vv.item())
-    return {"value": voxel_steps / (ms / 1e3), "ms_per_step": ms / args.steps, "kernels": kernels, "storage": storage}
+    out = {"value": voxel_steps / (ms / 1e3), "ms_per_step": ms / args.steps, "kernels": kernels, "storage": storage}
+    if solver:
+        out["solver"] = dict(solver)
+        out["last_step_solver_stats"] = solver_stats
+    return out
 
 
 def main():
@@ -465,6 +472,10 @@ def main():
                 r = time_steps(args, wl, local, kernels, storage, pg)
                 r["ratio"] = value / r["value"]
                 compare[f"{storage}_{kernels}"] = r
+        # config C2 in full: FP16 storage with the FP64-norm V-cycle stopping at 1e-5
+        r = time_steps(args, wl, local, "fused", "f16", pg, solver={"mode": "vcycle", "tolerance": 1e-5})
+        r["ratio"] = value / r["value"]
+        compare["f16_fused_vcycle"] = r
 
     cpu = None
     parity = None

@@ -155,6 +155,25 @@ class FxKernelTime(Structure):
 
 FX_INSTR_KERNEL_TIMES = 1 << 0
 FX_INSTR_COUNT_ACTIVE = 1 << 1
+FX_INSTR_SOLVER_NORMS = 1 << 2
+
+FX_SOLVER_REFERENCE = 0
+FX_SOLVER_VCYCLE = 1
+
+
+class FxSolverSettings(Structure):
+    _fields_ = [
+        ("mode", c_int32), ("levels", c_int32), ("pre_sweeps", c_int32), ("post_sweeps", c_int32),
+        ("coarse_sweeps", c_int32), ("max_cycles", c_int32), ("warm_start", c_int32), ("reserved", c_int32),
+        ("omega", c_double), ("tolerance", c_double),
+    ]
+
+
+class FxSolverStats(Structure):
+    _fields_ = [
+        ("rhs_l2", c_double), ("residual_l2", c_double), ("relative_residual", c_double), ("max_abs_divergence", c_double),
+        ("cycles", c_int32), ("converged", c_int32),
+    ]
 
 
 # (name, restype, argtypes) of every function include/fenix_cuda.h declares.
@@ -186,6 +205,10 @@ PROTOTYPES = [
     ("fx_sim_read_active_counters", c_int32, [c_void_p, POINTER(c_uint64), POINTER(c_uint64)]),
     ("fx_sim_get_stream", c_int32, [c_void_p, POINTER(c_void_p)]),
     ("fx_sim_last_error", c_char_p, [c_void_p]),
+    ("fx_solver_settings_default", None, [POINTER(FxSolverSettings)]),
+    ("fx_sim_set_solver", c_int32, [c_void_p, POINTER(FxSolverSettings)]),
+    ("fx_sim_get_solver", c_int32, [c_void_p, POINTER(FxSolverSettings)]),
+    ("fx_sim_read_solver_stats", c_int32, [c_void_p, POINTER(FxSolverStats)]),
     ("fx_brick_flags_noalloc", c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_void_p, c_void_p]),
 ]
 

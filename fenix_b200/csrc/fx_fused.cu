@@ -718,7 +718,7 @@ void injection_bricks(const FusedStep& st, std::vector<uint8_t>& mark, std::vect
 
 size_t fused_work_bytes(Dims, uint3 bricks) {
   const size_t nb = (size_t)bricks.x * bricks.y * bricks.z;
-  return 8 * align256(nb) + 3 * align256(nb * 4) + align256(16 * 4) + align256(96 * 4);
+  return 8 * align256(nb) + 3 * align256(nb * 4) + align256(16 * 4) + align256(96 * 4) + align256(sizeof(SolverDev));
 }
 
 void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks) {
@@ -744,11 +744,14 @@ void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks) {
   w.list_inj = (uint32_t*)take((size_t)w.nb * 4);
   w.counters = (uint32_t*)take(16 * 4);
   w.mg_bar = (unsigned*)take(96 * 4);
+  w.solver = (SolverDev*)take(sizeof(SolverDev));
 }
 
 fx_status fused_init(FusedWork& w, cudaStream_t) {
   if (cudaEventCreateWithFlags(&w.inj_event, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
   if (cudaMallocHost(&w.host_list_inj, ((size_t)w.nb + 1) * 4) != cudaSuccess) return FX_ERR_OUT_OF_MEMORY;
+  if (cudaMallocHost(&w.host_cont, sizeof(int)) != cudaSuccess) return FX_ERR_OUT_OF_MEMORY;
+  if (cudaStreamCreateWithFlags(&w.aux, cudaStreamNonBlocking) != cudaSuccess) return FX_ERR_CUDA;
   w.valid = true;  // the arena starts cleared: every brick is zero
   return FX_OK;
 }
@@ -773,6 +776,10 @@ void fused_release(FusedWork& w) {
   w.inj_event = nullptr;
   if (w.host_list_inj) cudaFreeHost(w.host_list_inj);
   w.host_list_inj = nullptr;
+  if (w.host_cont) cudaFreeHost(w.host_cont);
+  w.host_cont = nullptr;
+  if (w.aux) cudaStreamDestroy(w.aux);
+  w.aux = nullptr;
   for (auto& ev : w.timing_events) cudaEventDestroy(ev);
   w.timing_events.clear();
 }
@@ -882,6 +889,18 @@ fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
   mix_key(st.debug_fields);
   mix_key((uint64_t)st.last_p);
   for (int k = 0; k < 7; ++k) mix_key((uint64_t)st.q[k]);
+  mix_key((uint64_t)st.solver_mode);
+  mix_key(st.solver_norms);
+  if (st.solver_mode == 1) {
+    const VCycleConfig& c = st.vc;
+    for (int v : {c.levels, c.pre, c.post, c.coarse, c.max_cycles, (int)c.warm, (int)c.omega_one}) mix_key((uint64_t)v);
+    uint32_t wb;
+    std::memcpy(&wb, &c.omega, 4);
+    uint64_t tb;
+    std::memcpy(&tb, &c.tol, 8);
+    mix_key(wb);
+    mix_key(tb);
+  }
   if (graphs) {
     auto it = w.graphs.find(key);
     if (it == w.graphs.end()) {
@@ -917,6 +936,73 @@ fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
   const fx_status r = fused_sequence(w, st, ninj, out);
   out.launches += launches;
   return r;
+}
+
+// The V-cycle solve: the divergence, the prologue (norms, first decision) and
+// the loop. Under stream capture the loop is a WHILE conditional node whose
+// body graph (one cycle + norm + decision) is captured on the auxiliary stream;
+// without capture the host reads the decision after every cycle.
+fx_status vcycle_solve(FusedWork& w, const FusedStep& st, const VelField& vfin, uint32_t& launches, FusedResult& out) {
+  cudaStream_t s = st.stream;
+  const LevelBuf& F = st.lv[0];
+  {
+    Timed tm(w, s, "fused_divergence");
+    FX_CK(lean_div_first(s, st.dm, vfin, F.div, nullptr, st.lv[1].dm, st.lv[1].div, false));
+    ++launches;
+  }
+  VCycleLevels L;
+  for (int k = 0; k < 3; ++k) {
+    L.lv[k] = st.lv[k];
+    L.lv[3 + k] = st.xlv[k];
+  }
+  const int start = st.last_p;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  FX_CK(cudaStreamIsCapturing(s, &cs));
+  if (cs == cudaStreamCaptureStatusActive) {
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    FX_CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &ndeps));
+    cudaGraphConditionalHandle h = 0;
+    FX_CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    FX_CK(vcycle_prologue(s, L, st.vc, start, w.solver, h));
+    launches += 3;
+    FX_CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &ndeps));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    FX_CK(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    FX_CK(cudaStreamBeginCaptureToGraph(w.aux, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    uint32_t body_launches = 0;
+    const cudaError_t be = vcycle_body(w.aux, L, st.vc, start, w.solver, h, &body_launches);
+    cudaGraph_t body_out = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(w.aux, &body_out);
+    FX_CK(be);
+    FX_CK(ee);
+    FX_CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    out.cycle_launches = body_launches;
+  } else {
+    {
+      Timed tm(w, s, "fused_vcycle_prologue");
+      FX_CK(vcycle_prologue(s, L, st.vc, start, w.solver, 0));
+      launches += 3;
+    }
+    uint32_t body_launches = 0;
+    for (int c = 0; c < st.vc.max_cycles; ++c) {
+      FX_CK(cudaMemcpyAsync(w.host_cont, &w.solver->cont, sizeof(int), cudaMemcpyDeviceToHost, s));
+      FX_CK(cudaStreamSynchronize(s));
+      if (!*w.host_cont) break;
+      Timed tm(w, s, "fused_vcycle");
+      body_launches = 0;
+      FX_CK(vcycle_body(s, L, st.vc, start, w.solver, 0, &body_launches));
+    }
+    out.cycle_launches = body_launches;
+  }
+  return FX_OK;
 }
 
 fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, FusedResult& out) {
@@ -1010,7 +1096,13 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   }
   // 9. pressure (PressureSolvePass.solve, :68-84) and 10. projection
   int last_p = st.last_p;
-  if (st.pressure_on) {
+  if (st.pressure_on && st.solver_mode == 1) {
+    const fx_status vs = vcycle_solve(w, st, *vfinal, launches, out);
+    if (vs != FX_OK) return vs;
+    Timed tm(w, s, "fused_project");
+    k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0);
+    ++launches;
+  } else if (st.pressure_on) {
     const int m = st.q[2], n = st.q[3];
     const LevelBuf& F = st.lv[0];
     const LevelBuf& M = st.lv[1];
@@ -1241,6 +1333,17 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     // 10. projection with the pressure of the last solve (+ |v|)
     Timed tm(w, s, "fused_project");
     k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0);
+    ++launches;
+  }
+  // FP64 statistics of the solve: ||div||, ||div - A p|| (the V-cycle has them
+  // already) and max |div u| of the projected velocity.
+  if (st.pressure_on && (st.solver_mode == 1 || st.solver_norms)) {
+    Timed tm(w, s, "fused_solver_norms");
+    if (st.solver_mode == 0) {
+      FX_CK(solver_norms(s, dm, st.lv[0].div, st.lv[0].p[last_p], st.vc.tol, w.solver));
+      launches += 3;
+    }
+    FX_CK(max_divergence(s, dm, st.vcur, w.solver));
     ++launches;
   }
   FX_CK(cudaGetLastError());

@@ -11,6 +11,7 @@
 
 #include "../../include/fenix_cuda.h"
 #include "fx_kernels.h"
+#include "fx_vcycle.h"
 
 namespace fx {
 
@@ -19,6 +20,7 @@ struct FusedResult {
   bool final_vscr_is_2 = false;
   uint32_t launches = 0;
   bool graph = false;  // the step was a replay of a captured CUDA graph
+  uint32_t cycle_launches = 0;  // kernels per V-cycle (not counted in `launches`, which covers the rest)
   std::string error;
 };
 
@@ -41,6 +43,9 @@ struct FusedWork {
   uint32_t* list_inj = nullptr;   // bricks the injection kernel visits (host-filled)
   uint32_t* counters = nullptr;   // [0] adv count, [1] next count, [2] scratch, [3] inject count
   unsigned* mg_bar = nullptr;      // grid barrier of the lower multigrid kernel: arrivals, generation, error flag
+  SolverDev* solver = nullptr;     // FP64 solver statistics and the V-cycle loop state
+  cudaStream_t aux = nullptr;      // captures the V-cycle body graph
+  int* host_cont = nullptr;        // pinned: the continue flag, read by the host loop without graphs
   uint32_t* host_list_inj = nullptr;  // pinned staging for list_inj (+ count at [nb])
   cudaEvent_t inj_event = nullptr;
   std::vector<uint8_t> host_mark;
@@ -85,7 +90,11 @@ struct FusedStep {
   VelField vcur, vscr, vscr2, vort;
   float *vort_mag, *conf_mag, *vel_mag;
   LevelBuf lv[3];
+  LevelBuf xlv[3];  // V-cycle levels 3..5
   int q[7];
+  int solver_mode;    // 0: the reference schedule, 1: the V-cycle
+  VCycleConfig vc;
+  bool solver_norms;  // FP64 statistics after the reference schedule too
   bool vort_on, pressure_on, debug_on, debug_fields;
   int last_p;
 };

@@ -20,7 +20,7 @@
 //
 // Every value is computed with the reference's operations in its order: the
 // result equals the sweep-by-sweep evaluation bit for bit. The division by 6 is
-// the exact IEEE quotient (div6 below).
+// the exact IEEE quotient (div6, fx_math.cuh).
 #include <algorithm>
 #include <cstdlib>
 
@@ -58,22 +58,6 @@ struct ZArgs {
   int write_vmag;
   int restrict_mid;
 };
-
-// x / 6 rounded to nearest, for every float x. For |x| in [2^-125, FLT_MAX] the
-// quotient is q0 = x * RN(1/6) corrected once by its exact residual (Markstein,
-// "IA-64 and Elementary Functions", 2000): r = fma(-q0, 6, x), q = fma(r, RN(1/6), q0).
-// An exhaustive check over all 2^32 inputs shows this equals the IEEE quotient on
-// that range; tiny, infinite and NaN inputs take the IEEE division.
-FX_DEV float div6(float x) {
-  const float ax = fabsf(x);
-  if (ax >= 0x1p-125f && ax <= 0x1.fffffep127f) {
-    const float r6 = 0x1.555556p-3f;  // RN(1/6)
-    const float q0 = x * r6;
-    const float e = fmaf(-q0, 6.0f, x);
-    return fmaf(e, r6, q0);
-  }
-  return x / 6.0f;
-}
 
 // Prolongation term of pressure-prolongation.wgsl.ts:42-43 at fine voxel (x,y,z).
 FX_DEV float prolong_sample(const Dims& mid, const float* __restrict__ mp, int x, int y, int z) {

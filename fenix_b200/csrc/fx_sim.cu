@@ -95,6 +95,9 @@ struct fx_sim {
   int kernels = FX_KERNELS_FUSED;
   uint32_t opt_flags = 0;
   bool half = false;  // FX_OPT_SCALARS_F16: the scalar sets are binary16 buffers
+  fx_solver_settings solver{};
+  uint32_t last_cycle_launches = 0;  // kernels per V-cycle in the latest step
+  int last_solver_mode = 0;
 
   // device memory
   void* arena = nullptr;
@@ -106,6 +109,7 @@ struct fx_sim {
   float* vel_mag = nullptr;
   uint32_t* flags[2]{};
   LevelBuf lv[3]{};
+  LevelBuf xlv[3]{};  // V-cycle levels 3..5
   Params* d_params = nullptr;
   FusedWork fw{};
 
@@ -503,6 +507,10 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
   s->lv[0].dm = s->dm;
   s->lv[1].dm = halve(s->lv[0].dm);
   s->lv[2].dm = halve(s->lv[1].dm);
+  s->xlv[0].dm = halve(s->lv[2].dm);
+  s->xlv[1].dm = halve(s->xlv[0].dm);
+  s->xlv[2].dm = halve(s->xlv[1].dm);
+  fx_solver_settings_default(&s->solver);
 
   // One arena; every buffer starts on a 256-byte boundary.
   const size_t n = s->n;
@@ -512,7 +520,7 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
     off += (bytes + 255) & ~(size_t)255;
     return o;
   };
-  size_t o_sets[3][4], o_vcur[3], o_vscr[3], o_vscr2[3], o_vort[3], o_wmag, o_fmag, o_vmag, o_flags[2], o_lv[3][3], o_params;
+  size_t o_sets[3][4], o_vcur[3], o_vscr[3], o_vscr2[3], o_vort[3], o_wmag, o_fmag, o_vmag, o_flags[2], o_lv[3][3], o_xlv[3][3], o_params;
   for (auto& set : o_sets)
     for (auto& f : set) f = carve(n * (s->half ? 2 : 4));
   for (int c = 0; c < 3; ++c) {
@@ -528,6 +536,8 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
   o_flags[1] = carve((size_t)s->nb * 4);
   for (int l = 0; l < 3; ++l)
     for (int k = 0; k < 3; ++k) o_lv[l][k] = carve(count_of(s->lv[l].dm) * 4);
+  for (int l = 0; l < 3; ++l)
+    for (int k = 0; k < 3; ++k) o_xlv[l][k] = carve(count_of(s->xlv[l].dm) * 4);
   o_params = carve(sizeof(Params));
   const size_t o_acc = carve(2 * sizeof(unsigned long long));
   const size_t o_fused = off;
@@ -558,6 +568,9 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
     s->lv[l].div = (float*)(base + o_lv[l][0]);
     s->lv[l].p[0] = (float*)(base + o_lv[l][1]);
     s->lv[l].p[1] = (float*)(base + o_lv[l][2]);
+    s->xlv[l].div = (float*)(base + o_xlv[l][0]);
+    s->xlv[l].p[0] = (float*)(base + o_xlv[l][1]);
+    s->xlv[l].p[1] = (float*)(base + o_xlv[l][2]);
   }
   s->d_params = (Params*)(base + o_params);
   s->d_active_acc = (unsigned long long*)(base + o_acc);
@@ -659,7 +672,19 @@ fx_status fx_sim_step(fx_sim* s, double elapsed, double step_s) {
     fs.conf_mag = s->conf_mag;
     fs.vel_mag = s->vel_mag;
     for (int l = 0; l < 3; ++l) fs.lv[l] = s->lv[l];
+    for (int l = 0; l < 3; ++l) fs.xlv[l] = s->xlv[l];
     for (int k = 0; k < 7; ++k) fs.q[k] = s->qi[k];
+    fs.solver_mode = s->solver.mode;
+    fs.vc.levels = s->solver.levels;
+    fs.vc.pre = s->solver.pre_sweeps;
+    fs.vc.post = s->solver.post_sweeps;
+    fs.vc.coarse = s->solver.coarse_sweeps;
+    fs.vc.max_cycles = s->solver.max_cycles;
+    fs.vc.omega = (float)s->solver.omega;
+    fs.vc.omega_one = s->solver.omega == 1.0;
+    fs.vc.tol = s->solver.tolerance;
+    fs.vc.warm = s->solver.warm_start != 0;
+    fs.solver_norms = (s->instr & FX_INSTR_SOLVER_NORMS) != 0;
     fs.vort_on = vort_on;
     fs.pressure_on = pressure_on;
     fs.debug_on = debug_on;
@@ -672,6 +697,8 @@ fx_status fx_sim_step(fx_sim* s, double elapsed, double step_s) {
       s->final_vscr = fr.final_vscr_is_2 ? &s->vscr2 : &s->vscr;
       s->last_kernel_count = fr.launches;
       s->last_step_graph = fr.graph;
+      s->last_cycle_launches = pressure_on && s->solver.mode == FX_SOLVER_VCYCLE ? fr.cycle_launches : 0;
+      s->last_solver_mode = s->solver.mode;
     } else {
       fail(s, st, "fx_sim_step: fused step failed: " + fr.error);
     }
@@ -869,6 +896,13 @@ fx_status fx_sim_get_stats(fx_sim* s, fx_stats* o) {
   o->kernels_per_step = s->last_kernel_count;
   o->flags = (s->last_step_graph ? FX_STATS_GRAPH : 0u) | (s->fw.use_graphs ? 0u : FX_STATS_GRAPHS_OFF);
   FX_CUDA(s, cudaSetDevice(s->device));
+  if (s->last_cycle_launches) {
+    // the V-cycle loop ran a device-decided number of cycles
+    SolverDev d{};
+    FX_CUDA(s, cudaMemcpyAsync(&d, s->fw.solver, sizeof d, cudaMemcpyDeviceToHost, s->stream));
+    FX_CUDA(s, cudaStreamSynchronize(s->stream));
+    o->kernels_per_step += (uint32_t)d.cycles * s->last_cycle_launches;
+  }
   uint32_t active = 0;
   fx_status st = fused_count_active(s->fw, s->stream, s->flags[s->cur], s->nb, &active);
   if (st != FX_OK) return fail(s, st, "fx_sim_get_stats: counting active bricks failed");
@@ -878,8 +912,10 @@ fx_status fx_sim_get_stats(fx_sim* s, fx_stats* o) {
 
 fx_status fx_sim_set_instrumentation(fx_sim* s, uint32_t flags) {
   if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_instrumentation: NULL handle");
-  if (flags & ~(FX_INSTR_KERNEL_TIMES | FX_INSTR_COUNT_ACTIVE))
+  if (flags & ~(FX_INSTR_KERNEL_TIMES | FX_INSTR_COUNT_ACTIVE | FX_INSTR_SOLVER_NORMS))
     return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_instrumentation: unknown flags");
+  if ((flags & FX_INSTR_SOLVER_NORMS) && s->kernels != FX_KERNELS_FUSED)
+    return fail(s, FX_ERR_UNSUPPORTED, "fx_sim_set_instrumentation: solver statistics need the fused kernels");
   s->instr = flags;
   s->timer.on = (flags & FX_INSTR_KERNEL_TIMES) != 0;
   fused_set_timing(s->fw, s->timer.on);
@@ -953,6 +989,61 @@ fx_status fx_test_pinned_sincos(const float* host_x, float* host_out, uint32_t n
   cudaFree(dx);
   cudaFree(dout);
   return st;
+}
+
+void fx_solver_settings_default(fx_solver_settings* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->mode = FX_SOLVER_REFERENCE;
+  o->levels = 5;
+  o->pre_sweeps = 4;
+  o->post_sweeps = 4;
+  o->coarse_sweeps = 20;
+  o->max_cycles = 30;
+  o->warm_start = 1;
+  o->omega = 2.0 / 3.0;
+  o->tolerance = 1e-5;
+}
+
+fx_status fx_sim_set_solver(fx_sim* s, const fx_solver_settings* v) {
+  if (!s || !v) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_solver: NULL argument");
+  if (v->mode != FX_SOLVER_REFERENCE && v->mode != FX_SOLVER_VCYCLE)
+    return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_solver: unknown mode");
+  if (v->levels < 2 || v->levels > kMaxVLevels || v->pre_sweeps < 0 || v->pre_sweeps > 32 || v->post_sweeps < 0 || v->post_sweeps > 32 ||
+      v->coarse_sweeps < 0 || v->coarse_sweeps > 256 || v->max_cycles < 1 || v->max_cycles > 1000)
+    return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_solver: a count is out of range");
+  if (!(v->omega > 0.0 && v->omega <= 1.0) || !(v->tolerance >= 0.0) || !std::isfinite(v->tolerance))
+    return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_solver: omega must be in (0, 1] and tolerance finite and >= 0");
+  if (v->mode == FX_SOLVER_VCYCLE && s->kernels != FX_KERNELS_FUSED)
+    return fail(s, FX_ERR_UNSUPPORTED, "fx_sim_set_solver: the V-cycle needs the fused kernels");
+  s->solver = *v;
+  s->solver.reserved = 0;
+  return FX_OK;
+}
+
+fx_status fx_sim_get_solver(fx_sim* s, fx_solver_settings* o) {
+  if (!s || !o) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_solver: NULL argument");
+  *o = s->solver;
+  return FX_OK;
+}
+
+fx_status fx_sim_read_solver_stats(fx_sim* s, fx_solver_stats* o) {
+  if (!s || !o) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_read_solver_stats: NULL argument");
+  std::memset(o, 0, sizeof *o);
+  if (s->kernels != FX_KERNELS_FUSED) return FX_OK;
+  FX_CUDA(s, cudaSetDevice(s->device));
+  SolverDev d{};
+  FX_CUDA(s, cudaMemcpyAsync(&d, s->fw.solver, sizeof d, cudaMemcpyDeviceToHost, s->stream));
+  FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  o->rhs_l2 = std::sqrt(d.rhs2);
+  o->residual_l2 = std::sqrt(d.res2);
+  o->relative_residual = o->rhs_l2 > 0 ? o->residual_l2 / o->rhs_l2 : (o->residual_l2 > 0 ? INFINITY : 0.0);
+  double m;
+  std::memcpy(&m, &d.maxdiv_bits, sizeof m);
+  o->max_abs_divergence = m;
+  o->cycles = d.cycles;
+  o->converged = d.converged;
+  return FX_OK;
 }
 
 // Test hook: exhaustive comparison of the pressure kernels' division by 6 with

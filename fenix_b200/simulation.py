@@ -273,9 +273,29 @@ class CombustionVolumeSimulation:
             "graphsOff": bool(st.flags & 2),
         }
 
-    def setInstrumentation(self, kernel_times: bool = False, count_active: bool = False) -> None:
-        flags = (_lib.FX_INSTR_KERNEL_TIMES if kernel_times else 0) | (_lib.FX_INSTR_COUNT_ACTIVE if count_active else 0)
+    def setInstrumentation(self, kernel_times: bool = False, count_active: bool = False, solver_norms: bool = False) -> None:
+        flags = ((_lib.FX_INSTR_KERNEL_TIMES if kernel_times else 0) | (_lib.FX_INSTR_COUNT_ACTIVE if count_active else 0)
+                 | (_lib.FX_INSTR_SOLVER_NORMS if solver_norms else 0))
         check(self._lib.fx_sim_set_instrumentation(self._h, flags), self._h)
+
+    # -- pressure solver (extension) ---------------------------------------------
+    def setSolver(self, settings: Mapping[str, Any]) -> None:
+        """Partial solver settings (keys of SOLVER_DEFAULTS); the rest keep their values."""
+        cur = self.getSolver()
+        cur.update(settings)
+        check(self._lib.fx_sim_set_solver(self._h, ctypes.byref(solver_struct(cur))), self._h)
+
+    def getSolver(self) -> Dict[str, Any]:
+        st = _lib.FxSolverSettings()
+        check(self._lib.fx_sim_get_solver(self._h, ctypes.byref(st)), self._h)
+        return solver_dict(st)
+
+    def readSolverStats(self) -> Dict[str, Any]:
+        """FP64 statistics of the latest solve (waits for the stream)."""
+        st = _lib.FxSolverStats()
+        check(self._lib.fx_sim_read_solver_stats(self._h, ctypes.byref(st)), self._h)
+        return {"rhsL2": st.rhs_l2, "residualL2": st.residual_l2, "relativeResidual": st.relative_residual,
+                "maxAbsDivergence": st.max_abs_divergence, "cycles": st.cycles, "converged": bool(st.converged)}
 
     def readKernelTimes(self) -> Dict[str, Dict[str, float]]:
         """{kernel: {launches, total_ms}} since the last call (waits for the stream)."""
@@ -305,6 +325,48 @@ class CombustionVolumeSimulation:
 
 
 STORAGE = {"f32": 0, "f16": _lib.FX_OPT_SCALARS_F16}
+
+# Pressure solver settings (extension): "reference" is PressureSolvePass's fixed
+# schedule, "vcycle" the weighted-Jacobi V-cycle with an FP64 stopping test.
+SOLVER_MODES = {"reference": _lib.FX_SOLVER_REFERENCE, "vcycle": _lib.FX_SOLVER_VCYCLE}
+SOLVER_DEFAULTS = {"mode": "reference", "levels": 5, "preSweeps": 4, "postSweeps": 4, "coarseSweeps": 20, "maxCycles": 30,
+                   "warmStart": True, "omega": 2.0 / 3.0, "tolerance": 1e-5}
+_SOLVER_FIELDS = {"levels": "levels", "preSweeps": "pre_sweeps", "postSweeps": "post_sweeps", "coarseSweeps": "coarse_sweeps",
+                  "maxCycles": "max_cycles"}
+
+
+def solver_settings(settings: Optional[Mapping[str, Any]] = None) -> Dict[str, Any]:
+    """SOLVER_DEFAULTS updated with `settings` (unknown keys raise KeyError)."""
+    out = dict(SOLVER_DEFAULTS)
+    for k, v in (settings or {}).items():
+        if k not in out:
+            raise KeyError(f"unknown solver setting {k!r}")
+        out[k] = v
+    if out["mode"] not in SOLVER_MODES:
+        raise ValueError(f"unknown solver mode {out['mode']!r}")
+    return out
+
+
+def solver_struct(settings: Mapping[str, Any]) -> "_lib.FxSolverSettings":
+    full = solver_settings(settings)
+    st = _lib.FxSolverSettings()
+    st.mode = SOLVER_MODES[full["mode"]]
+    for key, name in _SOLVER_FIELDS.items():
+        setattr(st, name, int(full[key]))
+    st.warm_start = 1 if full["warmStart"] else 0
+    st.omega = float(full["omega"])
+    st.tolerance = float(full["tolerance"])
+    return st
+
+
+def solver_dict(st: "_lib.FxSolverSettings") -> Dict[str, Any]:
+    out = {"mode": "vcycle" if st.mode == _lib.FX_SOLVER_VCYCLE else "reference"}
+    for key, name in _SOLVER_FIELDS.items():
+        out[key] = getattr(st, name)
+    out["warmStart"] = bool(st.warm_start)
+    out["omega"] = st.omega
+    out["tolerance"] = st.tolerance
+    return out
 
 
 def build_options(options: Optional[Mapping[str, Any]] = None, *, device: int = 0, kernels: str = "fused",

@@ -266,6 +266,7 @@ fx_status fx_sim_get_stats(fx_sim* sim, fx_stats* out);
  * active bricks and their voxels to device-side counters. */
 #define FX_INSTR_KERNEL_TIMES (1u << 0)
 #define FX_INSTR_COUNT_ACTIVE (1u << 1)
+#define FX_INSTR_SOLVER_NORMS (1u << 2) /* FP64 solver statistics after the reference schedule too */
 
 typedef struct fx_kernel_time {
   char name[48];
@@ -289,6 +290,52 @@ fx_status fx_sim_get_stream(fx_sim* sim, void** stream);
 
 /* The sticky error message of a handle ("" when none). */
 const char* fx_sim_last_error(fx_sim* sim);
+
+/* Pressure solver (extension; no counterpart in the reference, whose solve is the
+ * fixed schedule of sim/runtime/passes/PressureSolvePass.ts:68-84, set through
+ * fx_quality). FX_SOLVER_VCYCLE runs weighted-Jacobi V-cycles over `levels`
+ * levels (the reference's level sizes, buffers.ts:10-16): `pre_sweeps` and
+ * `post_sweeps` per level, `coarse_sweeps` on the coarsest, the coarse
+ * right-hand side 4 x the mean of the 8 fine residuals, the reference's
+ * trilinear prolongation. It stops when ||div - A p||_2 <= tolerance * ||div||_2
+ * (both FP64, on the device) or after max_cycles cycles, and can start from the
+ * previous step's pressure. Fused kernels only. Under CUDA graphs the loop is a
+ * conditional WHILE node decided on the device. */
+#define FX_SOLVER_REFERENCE 0
+#define FX_SOLVER_VCYCLE 1
+
+typedef struct fx_solver_settings {
+  int32_t mode;          /* FX_SOLVER_*; default FX_SOLVER_REFERENCE */
+  int32_t levels;        /* 2..6; default 5 */
+  int32_t pre_sweeps;    /* 0..32; default 4 */
+  int32_t post_sweeps;   /* 0..32; default 4 */
+  int32_t coarse_sweeps; /* 0..256; default 20 */
+  int32_t max_cycles;    /* 1..1000; default 30 */
+  int32_t warm_start;    /* 1: start from the previous pressure; default 1 */
+  int32_t reserved;
+  double omega;          /* Jacobi weight in (0, 1]; default 2/3 */
+  double tolerance;      /* relative residual; default 1e-5 */
+} fx_solver_settings;
+
+void fx_solver_settings_default(fx_solver_settings* out);
+fx_status fx_sim_set_solver(fx_sim* sim, const fx_solver_settings* settings);
+fx_status fx_sim_get_solver(fx_sim* sim, fx_solver_settings* out);
+
+/* FP64 statistics of the latest pressure solve (waits for the stream): the
+ * norms of the divergence and of the final residual, their ratio, the max
+ * |div u| of the projected velocity over interior voxels, and the V-cycles run.
+ * Filled by FX_SOLVER_VCYCLE steps, and by reference-schedule steps while
+ * FX_INSTR_SOLVER_NORMS is set. */
+typedef struct fx_solver_stats {
+  double rhs_l2;
+  double residual_l2;
+  double relative_residual;
+  double max_abs_divergence;
+  int32_t cycles;
+  int32_t converged;
+} fx_solver_stats;
+
+fx_status fx_sim_read_solver_stats(fx_sim* sim, fx_solver_stats* out);
 
 /* Brick flags of caller-owned fields, allocating nothing. No counterpart in the
  * reference. It computes what compute-active-bricks.wgsl.ts:35-58 computes, for

@@ -236,6 +236,23 @@ struct Quality {
   int fine_pre = 2, fine_post = 3, mid_pre = 2, mid_post = 3, coarse = 10;
 };
 
+// Pressure solver selection. mode 0 is the reference's fixed schedule
+// (PressureSolvePass.ts:68-84). mode 1 is an extension with no counterpart in the
+// reference: a weighted-Jacobi V-cycle over `levels` levels (the reference's
+// level sizes, buffers.ts:10-16) that runs until ||div - A p||_2 <= tol * ||div||_2
+// in FP64, or max_cycles.
+struct SolverSettings {
+  int mode = 0, levels = 5, pre = 4, post = 4, coarse = 20, max_cycles = 30, warm = 1;
+  double omega = 2.0 / 3.0, tol = 1e-5;
+};
+
+// FP64 diagnostics of the last solve: squared norms of the divergence and of the
+// final residual, the max |div u| of the projected velocity, and the V-cycles run.
+struct SolverStats {
+  double rhs2 = 0, res2 = 0, maxdiv = 0;
+  int cycles = 0, converged = 0;
+};
+
 template <class R> class Sim {
  public:
   Dims dm;
@@ -245,6 +262,10 @@ template <class R> class Sim {
   std::vector<R> vc[3], vs[3], vort[3], vort_mag, conf_mag, vel_mag;
   std::vector<uint32_t> flags[2];
   Level<R> lv[3];
+  Level<R> xl[3];  // V-cycle levels 3..5
+  SolverSettings sv;
+  SolverStats stats;
+  bool norms = false;  // compute SolverStats in the reference mode too
   std::vector<float> sources;  // packed, >= 32 floats (phantom emitter when empty)
   Quality q;
   int advect_mode = 1;         // 0 semi-lagrangian, 1 maccormack
@@ -294,11 +315,25 @@ template <class R> class Sim {
       l.pa.assign(l.dm.n, R(0));
       l.pb.assign(l.dm.n, R(0));
     }
+    xl[0].dm = halve(lv[2].dm);
+    xl[1].dm = halve(xl[0].dm);
+    xl[2].dm = halve(xl[1].dm);
+    for (auto& l : xl) {
+      l.div.assign(l.dm.n, R(0));
+      l.pa.assign(l.dm.n, R(0));
+      l.pb.assign(l.dm.n, R(0));
+    }
     sources.assign(32, 0.0f);
   }
 
   // createCombustionVolumeSimulation.ts:206-226
   void reset() {
+    for (auto& l : xl) {
+      std::fill(l.div.begin(), l.div.end(), R(0));
+      std::fill(l.pa.begin(), l.pa.end(), R(0));
+      std::fill(l.pb.begin(), l.pb.end(), R(0));
+    }
+    stats = SolverStats{};
     cur = 0;
     step_index = 0;
     last_p = 0;
@@ -1014,6 +1049,164 @@ template <class R> class Sim {
     return smooth(lv[0], q.fine_post, fine_pre);
   }
 
+  // ------------------------------------------------ V-cycle solver (extension)
+  // Level k of the V-cycle: the reference's fine, mid and coarse levels, then
+  // three more halvings. `div` holds the level's right-hand side, pa/pb its
+  // iterate (the pressure on level 0, a correction below).
+  Level<R>& vlev(int k) { return k < 3 ? lv[k] : xl[k - 3]; }
+
+  // Weighted Jacobi: j = (sum of the 6 neighbours - rhs) / 6 in the reference's
+  // order, dst = src + w (j - src) (dst = j when w is 1); boundary voxels 0.
+  void wjacobi(Level<R>& L, const std::vector<R>& src, std::vector<R>& dst) {
+    const Dims& d = L.dm;
+    const uint32_t W1 = d.w - 1, H1 = d.h - 1, D1 = d.d - 1;
+    const R w = R(sv.omega);
+    const bool one = sv.omega == 1.0;
+    for_voxels(d, [&](uint32_t x, uint32_t y, uint32_t z) {
+      const size_t i = flat(d, x, y, z);
+      if (is_boundary(d, x, y, z)) {
+        dst[i] = R(0);
+        return;
+      }
+      const R s = src[flat(d, inc(x, W1), y, z)] + src[flat(d, dec(x), y, z)] + src[flat(d, x, inc(y, H1), z)] +
+                  src[flat(d, x, dec(y), z)] + src[flat(d, x, y, inc(z, D1))] + src[flat(d, x, y, dec(z))];
+      const R j = (s - L.div[i]) / R(6);
+      dst[i] = one ? j : src[i] + w * (j - src[i]);
+    });
+  }
+
+  int wsmooth(Level<R>& L, int iters, int start) {
+    int a = start;
+    for (int k = 0; k < iters; ++k) {
+      wjacobi(L, pbuf(L, a), pbuf(L, a ^ 1));
+      a ^= 1;
+    }
+    return a;
+  }
+
+  // rhs - (sum of the 6 neighbours - 6 e) at an interior voxel, 0 on the boundary.
+  R resid_at(const Level<R>& L, const std::vector<R>& e, uint32_t x, uint32_t y, uint32_t z) const {
+    const Dims& d = L.dm;
+    if (is_boundary(d, x, y, z)) return R(0);
+    const uint32_t W1 = d.w - 1, H1 = d.h - 1, D1 = d.d - 1;
+    const size_t i = flat(d, x, y, z);
+    const R s = e[flat(d, inc(x, W1), y, z)] + e[flat(d, dec(x), y, z)] + e[flat(d, x, inc(y, H1), z)] + e[flat(d, x, dec(y), z)] +
+                e[flat(d, x, y, inc(z, D1))] + e[flat(d, x, y, dec(z))];
+    const R lap = s - e[i] * R(6);
+    return L.div[i] - lap;
+  }
+
+  // Coarse right-hand side: 4 x the mean of the 8 fine residuals under a coarse
+  // voxel (children clamped as in pressure-restriction.wgsl.ts:27-50); the 4
+  // rescales the unscaled 7-point operator to the doubled spacing.
+  void restrict_residual(const Level<R>& F, const std::vector<R>& e, Level<R>& C) {
+    const Dims& s = F.dm;
+    const Dims& t = C.dm;
+    for_voxels(t, [&](uint32_t x, uint32_t y, uint32_t z) {
+      const size_t i = flat(t, x, y, z);
+      if (x == 0 || y == 0 || z == 0 || x == t.w - 1 || y == t.h - 1 || z == t.d - 1) {
+        C.div[i] = R(0);
+        return;
+      }
+      R sum = R(0);
+      for (uint32_t dz = 0; dz < 2; ++dz)
+        for (uint32_t dy = 0; dy < 2; ++dy)
+          for (uint32_t dx = 0; dx < 2; ++dx)
+            sum += resid_at(F, e, std::min(2 * x + dx, s.w - 1), std::min(2 * y + dy, s.h - 1), std::min(2 * z + dz, s.d - 1));
+      C.div[i] = (sum * K(0.125)) * R(4);
+    });
+  }
+
+  // dst = src + trilinear(coarse e) at interior fine voxels (the sample position
+  // of pressure-prolongation.wgsl.ts:29-44); boundary voxels copy src.
+  void prolong_add(const Level<R>& C, const std::vector<R>& ec, const Level<R>& F, const std::vector<R>& src, std::vector<R>& dst) {
+    const Dims& t = F.dm;
+    for_voxels(t, [&](uint32_t x, uint32_t y, uint32_t z) {
+      const size_t i = flat(t, x, y, z);
+      if (x == 0 || y == 0 || z == 0 || x == t.w - 1 || y == t.h - 1 || z == t.d - 1) {
+        dst[i] = src[i];
+        return;
+      }
+      const R px = (R(x) + K(0.5)) * K(0.5) - K(0.5);
+      const R py = (R(y) + K(0.5)) * K(0.5) - K(0.5);
+      const R pz = (R(z) + K(0.5)) * K(0.5) - K(0.5);
+      dst[i] = src[i] + interp(ec.data(), corners(C.dm, px, py, pz));
+    });
+  }
+
+  // One V-cycle on level k from buffer `start`; returns the buffer of the result.
+  // When pre + post is odd the prolongation writes the other buffer, so the fine
+  // level always ends in the buffer it started from.
+  int vcycle(int k, int start) {
+    Level<R>& L = vlev(k);
+    if (k == sv.levels - 1) return wsmooth(L, sv.coarse, start);
+    const int a = wsmooth(L, sv.pre, start);
+    Level<R>& C = vlev(k + 1);
+    restrict_residual(L, pbuf(L, a), C);
+    std::fill(C.pa.begin(), C.pa.end(), R(0));
+    const int ce = vcycle(k + 1, 0);
+    const int b = ((sv.pre + sv.post) & 1) ? a ^ 1 : a;
+    prolong_add(C, pbuf(C, ce), L, pbuf(L, a), pbuf(L, b));
+    return wsmooth(L, sv.post, b);
+  }
+
+  // Squared FP64 norms: sum of div^2, and of the residual computed in double from
+  // the stored values (neighbour sum in the reference's order).
+  double rhs_norm2() const {
+    double acc = 0;
+    for (const R v : lv[0].div) acc += (double)v * (double)v;
+    return acc;
+  }
+  double residual_norm2(const std::vector<R>& p) const {
+    const Dims& d = lv[0].dm;
+    const auto& div = lv[0].div;
+    const uint32_t W1 = d.w - 1, H1 = d.h - 1, D1 = d.d - 1;
+    double acc = 0;
+#pragma omp parallel for collapse(2) reduction(+ : acc) schedule(static)
+    for (uint32_t z = 1; z < d.d - 1; ++z)
+      for (uint32_t y = 1; y < d.h - 1; ++y)
+        for (uint32_t x = 1; x + 1 < d.w; ++x) {
+          const size_t i = flat(d, x, y, z);
+          const double s = (double)p[flat(d, inc(x, W1), y, z)] + (double)p[flat(d, dec(x), y, z)] + (double)p[flat(d, x, inc(y, H1), z)] +
+                           (double)p[flat(d, x, dec(y), z)] + (double)p[flat(d, x, y, inc(z, D1))] + (double)p[flat(d, x, y, dec(z))];
+          const double r = (double)div[i] - (s - 6.0 * (double)p[i]);
+          acc += r * r;
+        }
+    return acc;
+  }
+  // max |0.5 (central differences of v)| over interior voxels, in FP64.
+  double max_abs_divergence() const {
+    double m = 0;
+#pragma omp parallel for collapse(2) reduction(max : m) schedule(static)
+    for (uint32_t z = 1; z < dm.d - 1; ++z)
+      for (uint32_t y = 1; y < dm.h - 1; ++y)
+        for (uint32_t x = 1; x + 1 < dm.w; ++x) {
+          const double ddx = (double)vc[0][flat(dm, x + 1, y, z)] - (double)vc[0][flat(dm, x - 1, y, z)];
+          const double ddy = (double)vc[1][flat(dm, x, y + 1, z)] - (double)vc[1][flat(dm, x, y - 1, z)];
+          const double ddz = (double)vc[2][flat(dm, x, y, z + 1)] - (double)vc[2][flat(dm, x, y, z - 1)];
+          m = std::max(m, std::fabs(0.5 * (ddx + ddy + ddz)));
+        }
+    return m;
+  }
+
+  bool vcycle_done() const { return std::sqrt(stats.res2) <= sv.tol * std::sqrt(stats.rhs2); }
+
+  int solve_vcycle() {
+    Level<R>& F = lv[0];
+    int pid = last_p;
+    if (!sv.warm) std::fill(pbuf(F, pid).begin(), pbuf(F, pid).end(), R(0));
+    stats = SolverStats{};
+    stats.rhs2 = rhs_norm2();
+    stats.res2 = residual_norm2(pbuf(F, pid));
+    while (!vcycle_done() && stats.cycles < sv.max_cycles) {
+      pid = vcycle(0, pid);
+      stats.cycles += 1;
+      stats.res2 = residual_norm2(pbuf(F, pid));
+    }
+    stats.converged = vcycle_done() ? 1 : 0;
+    return pid;
+  }
+
   // shaders/passes/project-velocity.wgsl.ts:21-43 (vScratch, p -> vCurrent)
   void project(const std::vector<R>& p) {
     const uint32_t W1 = dm.w - 1, H1 = dm.h - 1, D1 = dm.d - 1;
@@ -1084,12 +1277,23 @@ template <class R> class Sim {
       vorticity_pass();
       confinement_pass(next);
     }
-    if (step_index % q.pressure_interval == 0) {
+    const bool solved = step_index % q.pressure_interval == 0;
+    if (solved && sv.mode == 1) {
+      divergence_pass();
+      last_p = solve_vcycle();
+    } else if (solved) {
       for (auto& l : lv) std::fill(l.pa.begin(), l.pa.end(), R(0));
       divergence_pass();
       last_p = solve();
+      if (norms) {
+        stats = SolverStats{};
+        stats.rhs2 = rhs_norm2();
+        stats.res2 = residual_norm2(pbuf(lv[0], last_p));
+        stats.converged = vcycle_done() ? 1 : 0;
+      }
     }
     project(pbuf(lv[0], last_p));
+    if (solved && (sv.mode == 1 || norms)) stats.maxdiv = max_abs_divergence();
     if (dm.n < 1800000 || debug_requested) {
       debug_fields();
       debug_requested = false;
@@ -1307,6 +1511,38 @@ long orc_read_field(void* hv, int id, double* dst, long cap) {
     if ((long)n > cap) return -(long)n;
     for (size_t i = 0; i < n; ++i) dst[i] = (double)p[i];
     return (long)n;
+  });
+}
+
+// Pressure solver: iv = mode, levels, pre, post, coarse, max_cycles, warm_start;
+// dv = omega, tolerance. norms = 1 computes the FP64 statistics in mode 0 too.
+void orc_set_solver(void* hv, const int* iv, const double* dv, int norms) {
+  dispatch(static_cast<Handle*>(hv), [&](auto* s) {
+    s->sv.mode = iv[0];
+    s->sv.levels = iv[1];
+    s->sv.pre = iv[2];
+    s->sv.post = iv[3];
+    s->sv.coarse = iv[4];
+    s->sv.max_cycles = iv[5];
+    s->sv.warm = iv[6];
+    s->sv.omega = dv[0];
+    s->sv.tol = dv[1];
+    s->norms = norms != 0;
+    return 0;
+  });
+}
+
+// out: rhs_l2, residual_l2, relative residual, max |div u|; iout: cycles, converged.
+void orc_get_solver_stats(void* hv, double* out, int* iout) {
+  dispatch(static_cast<Handle*>(hv), [&](auto* s) {
+    const double rhs = std::sqrt(s->stats.rhs2), res = std::sqrt(s->stats.res2);
+    out[0] = rhs;
+    out[1] = res;
+    out[2] = rhs > 0 ? res / rhs : (res > 0 ? INFINITY : 0.0);
+    out[3] = s->stats.maxdiv;
+    iout[0] = s->stats.cycles;
+    iout[1] = s->stats.converged;
+    return 0;
   });
 }
 

@@ -20,7 +20,7 @@ import numpy as np
 
 from fenix_b200 import _lib as fxlib
 from fenix_b200.emitters import packEmitterSources
-from fenix_b200.simulation import QUALITY_KEYS, _resolution_tuple, createSimulationQualitySettings
+from fenix_b200.simulation import QUALITY_KEYS, SOLVER_MODES, _resolution_tuple, createSimulationQualitySettings, solver_settings
 
 ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(ORACLE_DIR, "liboracle_fenix.so")
@@ -42,6 +42,8 @@ def load() -> ctypes.CDLL:
         lib.orc_set_advection_mode.argtypes = [c_void_p, c_int]
         lib.orc_set_emit_dead_residual.argtypes = [c_void_p, c_int]
         lib.orc_set_half_storage.argtypes = [c_void_p, c_int]
+        lib.orc_set_solver.argtypes = [c_void_p, POINTER(c_int), POINTER(c_double), c_int]
+        lib.orc_get_solver_stats.argtypes = [c_void_p, POINTER(c_double), POINTER(c_int)]
         lib.orc_update_sources.argtypes = [c_void_p, POINTER(c_float), c_uint32]
         lib.orc_step.argtypes = [c_void_p, c_double, c_double]
         lib.orc_prepare_params.argtypes = [c_void_p, c_double, c_double]
@@ -129,6 +131,22 @@ class OracleSimulation:
     def _push_quality(self) -> None:
         q = (c_int * 7)(*[self._quality[k] for k in QUALITY_KEYS])
         self._lib.orc_set_quality(self._h, q)
+
+    def setSolver(self, settings: Mapping[str, Any], norms: bool = False) -> None:
+        """Pressure solver settings (the keys of fenix_b200.simulation.SOLVER_DEFAULTS)."""
+        full = solver_settings({**getattr(self, "_solver", {}), **settings})
+        self._solver = full
+        iv = (c_int * 7)(SOLVER_MODES[full["mode"]], int(full["levels"]), int(full["preSweeps"]), int(full["postSweeps"]),
+                         int(full["coarseSweeps"]), int(full["maxCycles"]), 1 if full["warmStart"] else 0)
+        dv = (c_double * 2)(float(full["omega"]), float(full["tolerance"]))
+        self._lib.orc_set_solver(self._h, iv, dv, 1 if norms else 0)
+
+    def readSolverStats(self) -> dict:
+        out = (c_double * 4)()
+        iout = (c_int * 2)()
+        self._lib.orc_get_solver_stats(self._h, out, iout)
+        return {"rhsL2": out[0], "residualL2": out[1], "relativeResidual": out[2], "maxAbsDivergence": out[3],
+                "cycles": iout[0], "converged": bool(iout[1])}
 
     def step(self, elapsedSeconds: float, stepSeconds: float) -> None:
         self._lib.orc_step(self._h, float(elapsedSeconds), float(stepSeconds))

@@ -157,3 +157,17 @@ def test_f16_storage_needs_the_fused_kernels():
     assert b"FP16" in lib.fx_last_error()
     with pytest.raises(ValueError):
         build_options(storage="bf16")
+
+
+def test_solver_struct_layout_and_defaults():
+    from fenix_b200.simulation import solver_dict, solver_struct
+
+    assert ctypes.sizeof(_lib.FxSolverSettings) == 48 and ctypes.sizeof(_lib.FxSolverStats) == 40
+    st = solver_struct({"mode": "vcycle", "levels": 3, "warmStart": False})
+    d = solver_dict(st)
+    assert d["mode"] == "vcycle" and d["levels"] == 3 and d["warmStart"] is False and d["preSweeps"] == 4
+    if os.path.exists(_lib.LIB_PATH):
+        lib = _lib.load()
+        dflt = _lib.FxSolverSettings()
+        lib.fx_solver_settings_default(ctypes.byref(dflt))
+        assert solver_dict(dflt) == solver_dict(solver_struct({}))
