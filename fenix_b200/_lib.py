@@ -209,6 +209,14 @@ PROTOTYPES = [
     ("fx_sim_set_solver", c_int32, [c_void_p, POINTER(FxSolverSettings)]),
     ("fx_sim_get_solver", c_int32, [c_void_p, POINTER(FxSolverSettings)]),
     ("fx_sim_read_solver_stats", c_int32, [c_void_p, POINTER(FxSolverStats)]),
+    ("fx_batch_create", c_int32, [POINTER(POINTER(FxSimOptions)), c_uint32, POINTER(c_void_p)]),
+    ("fx_batch_destroy", None, [c_void_p]),
+    ("fx_batch_size", c_int32, [c_void_p, POINTER(c_uint32)]),
+    ("fx_batch_get_sim", c_int32, [c_void_p, c_uint32, POINTER(c_void_p)]),
+    ("fx_batch_step", c_int32, [c_void_p, c_double, c_double]),
+    ("fx_batch_synchronize", c_int32, [c_void_p]),
+    ("fx_batch_get_stream", c_int32, [c_void_p, POINTER(c_void_p)]),
+    ("fx_batch_last_error", c_char_p, [c_void_p]),
     ("fx_brick_flags_noalloc", c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_void_p, c_void_p]),
 ]
 

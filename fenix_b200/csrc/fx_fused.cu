@@ -838,7 +838,7 @@ int FusedWork::next_event() {
 
 fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, FusedResult& out);
 
-fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
+fx_status fused_prepare(FusedWork& w, const FusedStep& st, uint32_t* ninj_out, FusedResult& out) {
   cudaStream_t s = st.stream;
   const Dims dm = st.dm;
   const uint3 bc = st.bricks;
@@ -872,9 +872,12 @@ fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
     FX_CK(cudaEventRecord(w.inj_event, s));
     w.uploaded_list = w.host_list;
   }
+  *ninj_out = ninj;
+  out.launches = launches;
+  return FX_OK;
+}
 
-  // The device part of the step, captured once per configuration and replayed.
-  const bool graphs = w.use_graphs && !w.timing;
+uint64_t fused_key(const FusedStep& st, uint32_t ninj) {
   uint64_t key = 0;
   auto mix_key = [&](uint64_t v) { key = (key ^ v) * 0x100000001b3ull; };
   key = 0xcbf29ce484222325ull;
@@ -901,6 +904,23 @@ fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
     mix_key(wb);
     mix_key(tb);
   }
+  return key;
+}
+
+fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
+  cudaStream_t s = st.stream;
+  uint32_t ninj = 0;
+  FusedResult prep;
+  const fx_status ps = fused_prepare(w, st, &ninj, prep);
+  if (ps != FX_OK) {
+    out.error = prep.error;
+    return ps;
+  }
+  const uint32_t launches = prep.launches;
+
+  // The device part of the step, captured once per configuration and replayed.
+  const bool graphs = w.use_graphs && !w.timing;
+  const uint64_t key = fused_key(st, ninj);
   if (graphs) {
     auto it = w.graphs.find(key);
     if (it == w.graphs.end()) {

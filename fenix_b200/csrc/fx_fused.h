@@ -107,6 +107,14 @@ fx_status fused_reset(FusedWork& w, cudaStream_t s);
 fx_status fused_invalidate(FusedWork& w, cudaStream_t s);
 void fused_release(FusedWork& w);
 fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out);
+
+// The parts of fused_step, for callers that build their own graphs (batches):
+// host-side preparation on st.stream outside any graph (bookkeeping rebuild,
+// injection-list upload; *ninj = bricks to inject), the configuration key of the
+// device sequence, and the device sequence itself (capturable on st.stream).
+fx_status fused_prepare(FusedWork& w, const FusedStep& st, uint32_t* ninj, FusedResult& out);
+uint64_t fused_key(const FusedStep& st, uint32_t ninj);
+fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, FusedResult& out);
 fx_status fused_count_active(FusedWork& w, cudaStream_t s, const uint32_t* flags, uint32_t nb, uint32_t* out);
 
 // FX_ERR_TIMEOUT when a grid barrier of the fused path gave up waiting

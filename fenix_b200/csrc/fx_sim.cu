@@ -397,6 +397,102 @@ bool field_ref(fx_sim* s, int id, void** ptr, size_t* count) {
   }
 }
 
+// The host side of a step around its device work, shared by fx_sim_step and the
+// batch step: step_begin latches the parameters (createCombustionVolumeSimulation.ts:
+// 236-266) into the device uniform and describes the fused step; step_finish
+// records the result and advances the host state (:293-305).
+struct StepPlan {
+  bool vort_on = false, pressure_on = false, debug_on = false;
+  FusedStep fs{};
+};
+
+fx_status step_begin(fx_sim* s, double elapsed, double step_s, StepPlan& sp) {
+  if (!s->initialized) {
+    s->initialized = true;
+    s->start_s = elapsed;
+    s->last_elapsed_s = elapsed;
+  }
+  const Params P = make_params(s, elapsed, step_s);
+  const int slot = (int)(s->param_counter % kParamSlots);
+  FX_CUDA(s, cudaEventSynchronize(s->param_events[slot]));
+  s->h_params[slot] = P;
+  FX_CUDA(s, cudaMemcpyAsync(s->d_params, &s->h_params[slot], sizeof(Params), cudaMemcpyHostToDevice, s->stream));
+  FX_CUDA(s, cudaEventRecord(s->param_events[slot], s->stream));
+  ++s->param_counter;
+
+  sp.vort_on = s->step_index % s->qi[1] == 0;
+  sp.pressure_on = s->step_index % s->qi[0] == 0;
+  sp.debug_on = s->n < 1800000u || s->debug_requested;
+  if (s->kernels != FX_KERNELS_FUSED) return FX_OK;
+  FusedStep& fs = sp.fs;
+  fs.stream = s->stream;
+  fs.dm = s->dm;
+  fs.bricks = s->bricks;
+  fs.params = s->d_params;
+  fs.host_params = P;
+  fs.sources = s->d_sources;
+  fs.nsrc = std::max<uint32_t>(s->src_count, 1);
+  fs.host_sources = s->src_count ? s->host_sources.data() : nullptr;
+  fs.host_nsrc = s->src_count;
+  fs.advect_mode = s->advect_mode;
+  fs.cur_index = s->cur;
+  fs.cur = s->sets[s->cur];
+  fs.next = s->sets[s->cur ^ 1];
+  fs.scratch = s->sets[2];
+  fs.half_storage = s->half;
+  fs.flags_cur = s->flags[s->cur];
+  fs.flags_next = s->flags[s->cur ^ 1];
+  fs.vcur = s->vcur;
+  fs.vscr = s->vscr;
+  fs.vscr2 = s->vscr2;
+  fs.vort = s->vort;
+  fs.vort_mag = s->vort_mag;
+  fs.conf_mag = s->conf_mag;
+  fs.vel_mag = s->vel_mag;
+  for (int l = 0; l < 3; ++l) fs.lv[l] = s->lv[l];
+  for (int l = 0; l < 3; ++l) fs.xlv[l] = s->xlv[l];
+  for (int k = 0; k < 7; ++k) fs.q[k] = s->qi[k];
+  fs.solver_mode = s->solver.mode;
+  fs.vc.levels = s->solver.levels;
+  fs.vc.pre = s->solver.pre_sweeps;
+  fs.vc.post = s->solver.post_sweeps;
+  fs.vc.coarse = s->solver.coarse_sweeps;
+  fs.vc.max_cycles = s->solver.max_cycles;
+  fs.vc.omega = (float)s->solver.omega;
+  fs.vc.omega_one = s->solver.omega == 1.0;
+  fs.vc.tol = s->solver.tolerance;
+  fs.vc.warm = s->solver.warm_start != 0;
+  fs.solver_norms = (s->instr & FX_INSTR_SOLVER_NORMS) != 0;
+  fs.vort_on = sp.vort_on;
+  fs.pressure_on = sp.pressure_on;
+  fs.debug_on = sp.debug_on;
+  fs.debug_fields = (s->opt_flags & FX_OPT_DEBUG_FIELDS) != 0;
+  fs.last_p = s->last_p;
+  return FX_OK;
+}
+
+fx_status step_finish(fx_sim* s, fx_status st, const FusedResult* fr, const StepPlan& sp, double elapsed) {
+  if (st != FX_OK) return st;
+  if (fr) {
+    s->last_p = fr->last_p;
+    s->final_vscr = fr->final_vscr_is_2 ? &s->vscr2 : &s->vscr;
+    s->last_kernel_count = fr->launches;
+    s->last_step_graph = fr->graph;
+    s->last_cycle_launches = sp.pressure_on && s->solver.mode == FX_SOLVER_VCYCLE ? fr->cycle_launches : 0;
+    s->last_solver_mode = s->solver.mode;
+  }
+  if (s->instr & FX_INSTR_COUNT_ACTIVE) {
+    // flags of the step's advected set: the render flags once the step is done
+    FX_CUDA(s, fused_accumulate_active(s->stream, s->dm, s->bricks, s->flags[s->cur ^ 1], s->d_active_acc));
+    s->last_kernel_count += 1;
+  }
+  if (sp.debug_on) s->debug_requested = false;
+  s->cur ^= 1;
+  s->last_elapsed_s = elapsed;
+  s->step_index += 1;
+  return FX_OK;
+}
+
 }  // namespace
 
 namespace fx {
@@ -626,94 +722,14 @@ fx_status fx_sim_step(fx_sim* s, double elapsed, double step_s) {
   if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_step: NULL handle");
   if (!s->err.empty()) return FX_ERR_STATE;
   FX_CUDA(s, cudaSetDevice(s->device));
-  if (!s->initialized) {
-    s->initialized = true;
-    s->start_s = elapsed;
-    s->last_elapsed_s = elapsed;
-  }
-  const Params P = make_params(s, elapsed, step_s);
-  const int slot = (int)(s->param_counter % kParamSlots);
-  FX_CUDA(s, cudaEventSynchronize(s->param_events[slot]));
-  s->h_params[slot] = P;
-  FX_CUDA(s, cudaMemcpyAsync(s->d_params, &s->h_params[slot], sizeof(Params), cudaMemcpyHostToDevice, s->stream));
-  FX_CUDA(s, cudaEventRecord(s->param_events[slot], s->stream));
-  ++s->param_counter;
-
-  const bool vort_on = s->step_index % s->qi[1] == 0;
-  const bool pressure_on = s->step_index % s->qi[0] == 0;
-  const bool debug_on = s->n < 1800000u || s->debug_requested;
-  fx_status st;
-  if (s->kernels == FX_KERNELS_PLAIN) {
-    st = step_plain(s, vort_on, pressure_on, debug_on);
-  } else {
-    FusedStep fs;
-    fs.stream = s->stream;
-    fs.dm = s->dm;
-    fs.bricks = s->bricks;
-    fs.params = s->d_params;
-    fs.host_params = P;
-    fs.sources = s->d_sources;
-    fs.nsrc = std::max<uint32_t>(s->src_count, 1);
-    fs.host_sources = s->src_count ? s->host_sources.data() : nullptr;
-    fs.host_nsrc = s->src_count;
-    fs.advect_mode = s->advect_mode;
-    fs.cur_index = s->cur;
-    fs.cur = s->sets[s->cur];
-    fs.next = s->sets[s->cur ^ 1];
-    fs.scratch = s->sets[2];
-    fs.half_storage = s->half;
-    fs.flags_cur = s->flags[s->cur];
-    fs.flags_next = s->flags[s->cur ^ 1];
-    fs.vcur = s->vcur;
-    fs.vscr = s->vscr;
-    fs.vscr2 = s->vscr2;
-    fs.vort = s->vort;
-    fs.vort_mag = s->vort_mag;
-    fs.conf_mag = s->conf_mag;
-    fs.vel_mag = s->vel_mag;
-    for (int l = 0; l < 3; ++l) fs.lv[l] = s->lv[l];
-    for (int l = 0; l < 3; ++l) fs.xlv[l] = s->xlv[l];
-    for (int k = 0; k < 7; ++k) fs.q[k] = s->qi[k];
-    fs.solver_mode = s->solver.mode;
-    fs.vc.levels = s->solver.levels;
-    fs.vc.pre = s->solver.pre_sweeps;
-    fs.vc.post = s->solver.post_sweeps;
-    fs.vc.coarse = s->solver.coarse_sweeps;
-    fs.vc.max_cycles = s->solver.max_cycles;
-    fs.vc.omega = (float)s->solver.omega;
-    fs.vc.omega_one = s->solver.omega == 1.0;
-    fs.vc.tol = s->solver.tolerance;
-    fs.vc.warm = s->solver.warm_start != 0;
-    fs.solver_norms = (s->instr & FX_INSTR_SOLVER_NORMS) != 0;
-    fs.vort_on = vort_on;
-    fs.pressure_on = pressure_on;
-    fs.debug_on = debug_on;
-    fs.debug_fields = (s->opt_flags & FX_OPT_DEBUG_FIELDS) != 0;
-    fs.last_p = s->last_p;
-    FusedResult fr;
-    st = fused_step(s->fw, fs, fr);
-    if (st == FX_OK) {
-      s->last_p = fr.last_p;
-      s->final_vscr = fr.final_vscr_is_2 ? &s->vscr2 : &s->vscr;
-      s->last_kernel_count = fr.launches;
-      s->last_step_graph = fr.graph;
-      s->last_cycle_launches = pressure_on && s->solver.mode == FX_SOLVER_VCYCLE ? fr.cycle_launches : 0;
-      s->last_solver_mode = s->solver.mode;
-    } else {
-      fail(s, st, "fx_sim_step: fused step failed: " + fr.error);
-    }
-  }
+  StepPlan sp;
+  fx_status st = step_begin(s, elapsed, step_s, sp);
   if (st != FX_OK) return st;
-  if (s->instr & FX_INSTR_COUNT_ACTIVE) {
-    // flags of the step's advected set: the render flags once the step is done
-    FX_CUDA(s, fused_accumulate_active(s->stream, s->dm, s->bricks, s->flags[s->cur ^ 1], s->d_active_acc));
-    s->last_kernel_count += 1;
-  }
-  if (debug_on) s->debug_requested = false;
-  s->cur ^= 1;
-  s->last_elapsed_s = elapsed;
-  s->step_index += 1;
-  return FX_OK;
+  if (s->kernels == FX_KERNELS_PLAIN) return step_finish(s, step_plain(s, sp.vort_on, sp.pressure_on, sp.debug_on), nullptr, sp, elapsed);
+  FusedResult fr;
+  st = fused_step(s->fw, sp.fs, fr);
+  if (st != FX_OK) fail(s, st, "fx_sim_step: fused step failed: " + fr.error);
+  return step_finish(s, st, &fr, sp, elapsed);
 }
 
 fx_status fx_sim_get_render_buffers(fx_sim* s, fx_render_buffers* o) {
@@ -1045,6 +1061,210 @@ fx_status fx_sim_read_solver_stats(fx_sim* s, fx_solver_stats* o) {
   o->converged = d.converged;
   return FX_OK;
 }
+
+}  // extern "C"
+
+// ------------------------------------------------------------------- batches
+// Independent simulations stepped together: each step is one CUDA graph in
+// which every simulation's device sequence is a separate branch (captured on
+// its own stream, forked from and joined to the batch stream), so the GPU runs
+// them concurrently from a single launch. Host preparation (parameters,
+// injection lists) is enqueued on the batch stream before the launch.
+struct fx_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<fx_sim*> sims;
+  std::vector<cudaStream_t> branch;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  bool use_graphs = true;
+  struct Entry {
+    cudaGraphExec_t exec;
+    std::vector<FusedResult> results;
+  };
+  std::map<uint64_t, Entry> graphs;
+  std::string err;
+};
+
+namespace {
+
+fx_status batch_fail(fx_batch* b, fx_status code, const std::string& msg) {
+  if (b) {
+    if (b->err.empty()) b->err = msg;
+  } else {
+    g_last_error = msg;
+  }
+  return code;
+}
+
+// Enqueues every simulation's device sequence on its branch stream between the
+// fork and join events (captured when the batch stream is capturing).
+fx_status batch_sequences(fx_batch* b, std::vector<StepPlan>& sps, const std::vector<uint32_t>& ninj, std::vector<FusedResult>& res) {
+  if (cudaEventRecord(b->fork, b->stream) != cudaSuccess) return batch_fail(b, FX_ERR_CUDA, "fx_batch_step: fork event failed");
+  for (size_t i = 0; i < b->sims.size(); ++i) {
+    FusedStep fs = sps[i].fs;
+    fs.stream = b->branch[i];
+    if (cudaStreamWaitEvent(b->branch[i], b->fork, 0) != cudaSuccess) return batch_fail(b, FX_ERR_CUDA, "fx_batch_step: fork wait failed");
+    const fx_status st = fused_sequence(b->sims[i]->fw, fs, ninj[i], res[i]);
+    if (st != FX_OK) return batch_fail(b, st, "fx_batch_step: simulation " + std::to_string(i) + ": " + res[i].error);
+    if (cudaEventRecord(b->join[i], b->branch[i]) != cudaSuccess || cudaStreamWaitEvent(b->stream, b->join[i], 0) != cudaSuccess)
+      return batch_fail(b, FX_ERR_CUDA, "fx_batch_step: join failed");
+  }
+  return FX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fx_status fx_batch_create(const fx_sim_options* const* options, uint32_t count, fx_batch** out) {
+  g_last_error.clear();
+  if (!out || !options || count == 0 || count > 4096)
+    return batch_fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_batch_create: need 1..4096 option structs and an out pointer");
+  *out = nullptr;
+  for (uint32_t i = 0; i < count; ++i) {
+    if (!options[i]) return batch_fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_batch_create: NULL options");
+    if (options[i]->struct_size != sizeof(fx_sim_options))
+      return batch_fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_batch_create: struct_size does not match this library's fx_sim_options");
+    if (options[i]->kernels != FX_KERNELS_FUSED)
+      return batch_fail(nullptr, FX_ERR_UNSUPPORTED, "fx_batch_create: batches run the fused kernels");
+    if (options[i]->device != options[0]->device)
+      return batch_fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_batch_create: every simulation of a batch is on one device");
+  }
+  fx_batch* b = new (std::nothrow) fx_batch;
+  if (!b) return batch_fail(nullptr, FX_ERR_OUT_OF_MEMORY, "fx_batch_create: host allocation failed");
+  b->device = options[0]->device;
+  auto bail = [&](fx_status code, const std::string& msg) {
+    fx_batch_destroy(b);
+    return batch_fail(nullptr, code, msg);
+  };
+  if (cudaSetDevice(b->device) != cudaSuccess) return bail(FX_ERR_CUDA, "fx_batch_create: cudaSetDevice failed (no CUDA device?)");
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(FX_ERR_CUDA, "fx_batch_create: stream creation failed");
+  if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) return bail(FX_ERR_CUDA, "fx_batch_create: event creation failed");
+  for (uint32_t i = 0; i < count; ++i) {
+    fx_sim_options o = *options[i];
+    o.stream = b->stream;
+    fx_sim* sim = nullptr;
+    const fx_status st = fx_sim_create(&o, &sim);
+    if (st != FX_OK) return bail(st, "fx_batch_create: simulation " + std::to_string(i) + ": " + g_last_error);
+    b->sims.push_back(sim);
+    if ((o.flags & FX_OPT_NO_GRAPHS) != 0) b->use_graphs = false;
+    cudaStream_t br = nullptr;
+    cudaEvent_t ev = nullptr;
+    if (cudaStreamCreateWithFlags(&br, cudaStreamNonBlocking) != cudaSuccess) return bail(FX_ERR_CUDA, "fx_batch_create: stream creation failed");
+    b->branch.push_back(br);
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return bail(FX_ERR_CUDA, "fx_batch_create: event creation failed");
+    b->join.push_back(ev);
+  }
+  *out = b;
+  return FX_OK;
+}
+
+void fx_batch_destroy(fx_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second.exec);
+  for (fx_sim* sim : b->sims) fx_sim_destroy(sim);
+  for (cudaStream_t br : b->branch) cudaStreamDestroy(br);
+  for (cudaEvent_t ev : b->join) cudaEventDestroy(ev);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+fx_status fx_batch_size(fx_batch* b, uint32_t* count) {
+  if (!b || !count) return batch_fail(b, FX_ERR_INVALID_ARGUMENT, "fx_batch_size: NULL argument");
+  *count = (uint32_t)b->sims.size();
+  return FX_OK;
+}
+
+fx_status fx_batch_get_sim(fx_batch* b, uint32_t index, fx_sim** sim) {
+  if (!b || !sim) return batch_fail(b, FX_ERR_INVALID_ARGUMENT, "fx_batch_get_sim: NULL argument");
+  if (index >= b->sims.size()) return batch_fail(b, FX_ERR_INVALID_ARGUMENT, "fx_batch_get_sim: index out of range");
+  *sim = b->sims[index];
+  return FX_OK;
+}
+
+fx_status fx_batch_step(fx_batch* b, double elapsed, double step_s) {
+  if (!b) return batch_fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_batch_step: NULL handle");
+  if (!b->err.empty()) return FX_ERR_STATE;
+  if (cudaSetDevice(b->device) != cudaSuccess) return batch_fail(b, FX_ERR_CUDA, "fx_batch_step: cudaSetDevice failed");
+  const size_t n = b->sims.size();
+  std::vector<StepPlan> sps(n);
+  std::vector<uint32_t> ninj(n, 0);
+  std::vector<uint32_t> prep_launches(n, 0);
+  bool timing = false;
+  uint64_t key = 0xcbf29ce484222325ull;
+  for (size_t i = 0; i < n; ++i) {
+    fx_sim* sim = b->sims[i];
+    if (!sim->err.empty()) return batch_fail(b, FX_ERR_STATE, "fx_batch_step: simulation " + std::to_string(i) + " has an error: " + sim->err);
+    fx_status st = step_begin(sim, elapsed, step_s, sps[i]);
+    if (st != FX_OK) return batch_fail(b, st, "fx_batch_step: simulation " + std::to_string(i) + ": " + sim->err);
+    FusedResult prep;
+    st = fused_prepare(sim->fw, sps[i].fs, &ninj[i], prep);
+    if (st != FX_OK) return batch_fail(b, st, "fx_batch_step: simulation " + std::to_string(i) + ": " + prep.error);
+    prep_launches[i] = prep.launches;
+    timing = timing || sim->fw.timing;
+    key = (key ^ (fused_key(sps[i].fs, ninj[i]) + 0x9e3779b97f4a7c15ull * (i + 1))) * 0x100000001b3ull;
+  }
+  std::vector<FusedResult> res(n);
+  bool replay = false;
+  if (b->use_graphs && !timing) {
+    auto it = b->graphs.find(key);
+    if (it == b->graphs.end()) {
+      cudaGraph_t g = nullptr;
+      if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+        return batch_fail(b, FX_ERR_CUDA, "fx_batch_step: stream capture failed to start");
+      std::vector<FusedResult> tmp(n);
+      const std::string before = b->err;
+      const fx_status cst = batch_sequences(b, sps, ninj, tmp);
+      const cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+      cudaGraphExec_t ex = nullptr;
+      cudaError_t ie = cudaErrorUnknown;
+      if (cst == FX_OK && ce == cudaSuccess) ie = cudaGraphInstantiate(&ex, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (cst != FX_OK || ce != cudaSuccess || ie != cudaSuccess) {
+        cudaGetLastError();
+        b->err = before;  // a capture problem falls back to direct launches
+        b->use_graphs = false;
+      } else {
+        it = b->graphs.emplace(key, fx_batch::Entry{ex, tmp}).first;
+      }
+    }
+    if (b->use_graphs) {
+      if (cudaGraphLaunch(it->second.exec, b->stream) != cudaSuccess) return batch_fail(b, FX_ERR_CUDA, "fx_batch_step: graph launch failed");
+      res = it->second.results;
+      replay = true;
+    }
+  }
+  if (!replay) {
+    const fx_status st = batch_sequences(b, sps, ninj, res);
+    if (st != FX_OK) return st;
+  }
+  for (size_t i = 0; i < n; ++i) {
+    res[i].launches += prep_launches[i];
+    res[i].graph = replay;
+    const fx_status st = step_finish(b->sims[i], FX_OK, &res[i], sps[i], elapsed);
+    if (st != FX_OK) return batch_fail(b, st, "fx_batch_step: simulation " + std::to_string(i) + ": " + b->sims[i]->err);
+  }
+  return FX_OK;
+}
+
+fx_status fx_batch_synchronize(fx_batch* b) {
+  if (!b) return batch_fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_batch_synchronize: NULL handle");
+  if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamSynchronize(b->stream) != cudaSuccess)
+    return batch_fail(b, FX_ERR_CUDA, "fx_batch_synchronize: the batch stream failed");
+  return FX_OK;
+}
+
+fx_status fx_batch_get_stream(fx_batch* b, void** stream) {
+  if (!b || !stream) return batch_fail(b, FX_ERR_INVALID_ARGUMENT, "fx_batch_get_stream: NULL argument");
+  *stream = (void*)b->stream;
+  return FX_OK;
+}
+
+const char* fx_batch_last_error(fx_batch* b) { return b ? b->err.c_str() : g_last_error.c_str(); }
 
 // Test hook: exhaustive comparison of the pressure kernels' division by 6 with
 // the IEEE division on the device. Returns the mismatch count in *bad.

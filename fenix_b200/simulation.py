@@ -164,9 +164,10 @@ def _pointer_dict(rb: FxRenderBuffers) -> Dict[str, Any]:
 class CombustionVolumeSimulation:
     """types.ts:62-76, backed by a `fx_sim` handle."""
 
-    def __init__(self, handle: ctypes.c_void_p, lib: ctypes.CDLL):
+    def __init__(self, handle: ctypes.c_void_p, lib: ctypes.CDLL, owned: bool = True):
         self._h = handle
         self._lib = lib
+        self._owned = owned  # False for the members of a batch, which the batch destroys
         w, h, d = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
         check(lib.fx_sim_get_resolution(self._h, ctypes.byref(w), ctypes.byref(h), ctypes.byref(d)), self._h)
         self.resolution = {"width": w.value, "height": h.value, "depth": d.value}
@@ -227,7 +228,8 @@ class CombustionVolumeSimulation:
 
     def dispose(self) -> None:
         if self._h:
-            self._lib.fx_sim_destroy(self._h)
+            if self._owned:
+                self._lib.fx_sim_destroy(self._h)
             self._h = None
 
     # -- extensions --------------------------------------------------------------

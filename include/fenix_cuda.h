@@ -337,6 +337,26 @@ typedef struct fx_solver_stats {
 
 fx_status fx_sim_read_solver_stats(fx_sim* sim, fx_solver_stats* out);
 
+/* Batches (extension; the reference steps one simulation per device): many
+ * independent simulations, each with its own options (sizes may differ), stepped
+ * together. Every fx_batch_step is one CUDA graph in which each simulation's
+ * device work is a separate branch, so they run concurrently from one launch.
+ * The members are ordinary fx_sim handles owned by the batch: use them for
+ * params, quality, sources, solver, field reads and writes; do not destroy them.
+ * fx_sim_step on a member steps that member alone. Fused kernels only. */
+typedef struct fx_batch fx_batch;
+
+fx_status fx_batch_create(const fx_sim_options* const* options, uint32_t count, fx_batch** out);
+void fx_batch_destroy(fx_batch* batch);
+fx_status fx_batch_size(fx_batch* batch, uint32_t* count);
+fx_status fx_batch_get_sim(fx_batch* batch, uint32_t index, fx_sim** sim);
+/* One step of every member (each member's reference schedule, parameters and
+ * sources), enqueued on the batch stream. */
+fx_status fx_batch_step(fx_batch* batch, double elapsed_seconds, double step_seconds);
+fx_status fx_batch_synchronize(fx_batch* batch);
+fx_status fx_batch_get_stream(fx_batch* batch, void** stream);
+const char* fx_batch_last_error(fx_batch* batch);
+
 /* Brick flags of caller-owned fields, allocating nothing. No counterpart in the
  * reference. It computes what compute-active-bricks.wgsl.ts:35-58 computes, for
  * the density, temperature and reaction fields (width*height*depth floats each,
