@@ -310,6 +310,90 @@ def time_steps(args, wl, local, kernels, storage, pg, solver=None):
     return out
 
 
+def run_batch_c3(args, local, rank, world, pg):
+    """The batched configuration: 64 simulations of uneven size and activity,
+    partitioned over the ranks by LPT on their active bricks. Each rank times
+    its share as one FP16-storage batch (one CUDA graph per step), then the same
+    share as sequential plain-FP32 steps on one stream. Device time, max over
+    ranks; value = active voxel-steps of all ranks / that time (strong scaling:
+    the 64 simulations are fixed)."""
+    import torch
+
+    from fenix_b200 import batch as fxb
+    from fenix_b200 import createCombustionVolumeSimulation, workloads
+
+    wls = workloads.batch_c3(count=64, processes=min(16, os.cpu_count() or 1))
+    costs = [fxb.workload_cost(w) for w in wls]
+    share = fxb.lpt_partition(costs, world)[rank]
+    mine = [wls[i] for i in share]
+    dt = wls[0].dt
+    steps = args.c3_steps
+
+    def timed(step_all, stream, sims):
+        t = 0.0
+        for _ in range(args.warmup):
+            step_all(t)
+            t += dt
+        torch.cuda.synchronize()
+        for s in sims:
+            s.readActiveCounters()
+        if pg:
+            pg.barrier()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            step_all(t)
+            t += dt
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        vox = sum(s.readActiveCounters()["voxelSteps"] for s in sims)
+        if pg:
+            tt = torch.tensor([ms], device="cuda")
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+            ms = float(tt.item())
+            vv = torch.tensor([float(vox)], device="cuda", dtype=torch.float64)
+            pg.all_reduce(vv, op=pg.ReduceOp.SUM)
+            vox = int(vv.item())
+        return {"value": vox / (ms / 1e3), "ms_per_step": ms / steps}
+
+    dev = torch.device("cuda", local)
+    batch = fxb.SimulationBatch([w.options for w in mine], device=local, storage="f16")
+    for sim, wl in zip(batch.sims, mine):
+        sim.updateSources(wl.sources)
+        workloads.load_state(sim, wl.state)
+        sim.setInstrumentation(count_active=True)
+    bstream = torch.cuda.ExternalStream(batch.stream, device=dev)
+    batched = timed(lambda t: batch.step(t, dt), bstream, batch.sims)
+    batch.dispose()
+
+    seq_stream = torch.cuda.Stream(device=dev)
+    sims = []
+    for wl in mine:
+        s = createCombustionVolumeSimulation(wl.options, device=local, kernels="plain", stream=seq_stream.cuda_stream)
+        s.updateSources(wl.sources)
+        workloads.load_state(s, wl.state)
+        s.setInstrumentation(count_active=True)
+        sims.append(s)
+
+    def step_seq(t):
+        for s in sims:
+            s.step(t, dt)
+
+    sequential = timed(step_seq, seq_stream, sims)
+    for s in sims:
+        s.dispose()
+    total_vox = sum(w.options["resolution"][0] * w.options["resolution"][1] * w.options["resolution"][2] for w in wls)
+    return {
+        "workload": "64 simulations, seeded boxes with sides in {32..192} step 8, 1-3 emitters (inflow 1-3, burn 0.2-1.0), "
+                    f"start active fraction 0.1-0.6; {total_vox / 1e6:.1f} M voxels in all; {steps} steps after {args.warmup} warm-up",
+        "metric": "active-voxel-steps/s", "scaling": "strong", "ranks": world,
+        "batched_f16": batched, "sequential_plain_f32": sequential, "ratio": batched["value"] / sequential["value"],
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -319,6 +403,8 @@ def main():
     ap.add_argument("--kernels", default="fused", choices=["fused", "plain"])
     ap.add_argument("--storage", default="f16", choices=["f16", "f32"], help="scalar-set storage of the headline step")
     ap.add_argument("--no-compare", action="store_true", help="skip timing the FP32 plain and fused steps")
+    ap.add_argument("--no-c3", action="store_true", help="skip the batched 64-simulation configuration")
+    ap.add_argument("--c3-steps", type=int, default=100)
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
@@ -477,6 +563,8 @@ def main():
         r["ratio"] = value / r["value"]
         compare["f16_fused_vcycle"] = r
 
+    batch_c3 = None if args.no_c3 else run_batch_c3(args, local, rank, world, pg)
+
     cpu = None
     parity = None
     error = None
@@ -498,7 +586,7 @@ def main():
                 "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (about 2 GB of fields per step)",
             },
             "roofline": roofline, "kernels": kernel_table, "cpu_baseline": cpu, "parity_full_size": parity, "e2e": e2e,
-            "compare": compare, "error_vs_f64": error,
+            "compare": compare, "error_vs_f64": error, "batch_c3": batch_c3,
             "gpu_launches": int(kernels_last * args.steps), "clocks": clock_info,
         }
         print(json.dumps(line))

@@ -372,7 +372,7 @@ def solver_dict(st: "_lib.FxSolverSettings") -> Dict[str, Any]:
 
 
 def build_options(options: Optional[Mapping[str, Any]] = None, *, device: int = 0, kernels: str = "fused",
-                  debug_fields: bool = False, use_graphs: bool = True, storage: str = "f32") -> FxSimOptions:
+                  debug_fields: bool = False, use_graphs: bool = True, storage: str = "f32", stream: int = 0) -> FxSimOptions:
     """CombustionVolumeSimulationOptions -> fx_sim_options. storage="f16" stores the
     scalar sets in binary16 (fused kernels only)."""
     if storage not in STORAGE:
@@ -403,14 +403,18 @@ def build_options(options: Optional[Mapping[str, Any]] = None, *, device: int = 
     opt.device = device
     opt.kernels = KERNEL_PATHS[kernels]
     opt.flags = (_lib.FX_OPT_DEBUG_FIELDS if debug_fields else 0) | (0 if use_graphs else _lib.FX_OPT_NO_GRAPHS) | STORAGE[storage]
+    opt.stream = stream or None
     return opt
 
 
 def createCombustionVolumeSimulation(options: Optional[Mapping[str, Any]] = None, *, device: int = 0, kernels: str = "fused",
-                                     debug_fields: bool = False, use_graphs: bool = True, storage: str = "f32") -> CombustionVolumeSimulation:
-    """createCombustionVolumeSimulation.ts:50-401 on CUDA device `device`."""
+                                     debug_fields: bool = False, use_graphs: bool = True, storage: str = "f32",
+                                     stream: int = 0) -> CombustionVolumeSimulation:
+    """createCombustionVolumeSimulation.ts:50-401 on CUDA device `device`. `stream`
+    (a cudaStream_t as an integer, 0 = the simulation's own) is where it enqueues."""
     lib = _lib.load()
-    opt = build_options(options, device=device, kernels=kernels, debug_fields=debug_fields, use_graphs=use_graphs, storage=storage)
+    opt = build_options(options, device=device, kernels=kernels, debug_fields=debug_fields, use_graphs=use_graphs, storage=storage,
+                        stream=stream)
     handle = ctypes.c_void_p()
     check(lib.fx_sim_create(ctypes.byref(opt), ctypes.byref(handle)))
     return CombustionVolumeSimulation(handle, lib)

@@ -40,6 +40,7 @@ class Workload:
     sources: List
     state: Dict[str, np.ndarray]
     dt: float = DT
+    target_fraction: float = 0.0
 
 
 class Pcg32:
@@ -81,13 +82,15 @@ def _plume_sources(res, centers_vox, radii_vox, rng: Pcg32):
     return out
 
 
-def _plume_state(res, centers_vox, radii_vox, heights, seed: int) -> Dict[str, np.ndarray]:
+def _plume_state(res, centers_vox, radii_vox, heights, seed: int, stride: int = 1) -> Dict[str, np.ndarray]:
     """A developed-plume state: cones of smoke and heat rising from each source,
-    with seeded lateral wobble and noise. Returned arrays are (D, H, W) float32."""
+    with seeded lateral wobble and noise. Returned arrays are (D, H, W) float32
+    (every `stride`-th voxel along each axis when stride > 1)."""
     w, h, d = res
     rng = np.random.default_rng(seed)
-    z, y, x = np.meshgrid(np.arange(d, dtype=np.float32), np.arange(h, dtype=np.float32), np.arange(w, dtype=np.float32), indexing="ij")
-    dens = np.zeros((d, h, w), np.float32)
+    z, y, x = np.meshgrid(np.arange(0, d, stride, dtype=np.float32), np.arange(0, h, stride, dtype=np.float32),
+                          np.arange(0, w, stride, dtype=np.float32), indexing="ij")
+    dens = np.zeros(x.shape, np.float32)
     temp = np.zeros_like(dens)
     fuel = np.zeros_like(dens)
     reac = np.zeros_like(dens)
@@ -184,3 +187,113 @@ def brick_voxel_counts(res) -> np.ndarray:
     cy = np.minimum(8, h - 8 * np.arange(by))
     cz = np.minimum(8, d - 8 * np.arange(bz))
     return (cz[:, None, None] * cy[None, :, None] * cx[None, None, :]).ravel().astype(np.int64)
+
+
+def _flags_from_samples(e: np.ndarray) -> np.ndarray:
+    """Brick flags from the energy at every second voxel of a grid whose sides are
+    multiples of 8: each brick's 4^3 samples include its centre (local 4, 4, 4)."""
+    d2, h2, w2 = e.shape
+    bz, by, bx = d2 // 4, h2 // 4, w2 // 4
+    peak = e.reshape(bz, 4, by, 4, bx, 4).max(axis=(1, 3, 5))
+    centre = e[2::4, 2::4, 2::4]
+    active = peak > np.float32(0.012)
+    dilate = active & ((peak > np.float32(0.05)) | (centre > np.float32(0.035)))
+    pad = np.pad(dilate, 1)
+    grown = np.zeros_like(active)
+    for dz in range(3):
+        for dy in range(3):
+            for dx in range(3):
+                grown |= pad[dz:dz + bz, dy:dy + by, dx:dx + bx]
+    return (active | grown).astype(np.uint8)
+
+
+def brick_flags_estimate(state: Dict[str, np.ndarray]) -> np.ndarray:
+    """The reference's brick flags (compute-active-bricks.wgsl.ts:35-58) of a
+    state whose sides are multiples of 8, evaluated with numpy in float32:
+    samples at even local coordinates (the centre is one of them), threshold
+    0.012, dilation by one brick when the peak exceeds 0.05 or the centre 0.035.
+    Returns uint8 flags of shape (bz, by, bx)."""
+    e = (state["density"] + state["temperature"] * np.float32(0.7)) + state["reaction"] * np.float32(0.9)
+    return _flags_from_samples(np.ascontiguousarray(e[::2, ::2, ::2]))
+
+
+def _batch_draw(index: int, rng: Pcg32, seed: int) -> Dict:
+    """The seeded parameters of one simulation of the batched configuration."""
+    w, h, d = (8 * int(rng.uniform(4, 25)) for _ in range(3))
+    target = rng.uniform(0.1, 0.6)
+    count = 1 + int(rng.uniform(0, 3))
+    emitters = []
+    for _ in range(count):
+        emitters.append({
+            "center": (rng.uniform(0.2, 0.8) * w, 4.0, rng.uniform(0.2, 0.8) * d),
+            "radius": rng.uniform(0.04, 0.1) * min(w, d),
+            "speed": rng.uniform(1.0, 3.0),
+            "burn": rng.uniform(0.2, 1.0),
+            "seed": float(int(rng.uniform(1, 4000))),
+        })
+    return {"index": index, "res": (w, h, d), "target": target, "emitters": emitters, "seed": seed + index}
+
+
+def _batch_build(p: Dict) -> Workload:
+    """Bisects the cone width so the start state's brick flags cover the target
+    fraction (evaluated on every second voxel), then builds the state."""
+    res = p["res"]
+    w, h, d = res
+    em = p["emitters"]
+    centers = [e["center"] for e in em]
+    radii = [e["radius"] for e in em]
+    heights = [0.92 * h] * len(em)
+
+    def fraction(scale):
+        st = _plume_state(res, centers, [r * scale for r in radii], heights, p["seed"], stride=2)
+        e = (st["density"] + st["temperature"] * np.float32(0.7)) + st["reaction"] * np.float32(0.9)
+        return float(_flags_from_samples(e).mean())
+
+    lo, hi = 0.05, 12.0
+    for _ in range(9):
+        mid = 0.5 * (lo + hi)
+        if fraction(mid) < p["target"]:
+            lo = mid
+        else:
+            hi = mid
+    scale = 0.5 * (lo + hi)
+    sources = []
+    for e in em:
+        cx, cy, cz = e["center"]
+        pos = (cx / w, cy / h, cz / d)
+        rn = e["radius"] * scale / max(w, d)
+        sd = e["seed"]
+        sources.append(ScalarEmitter(position=pos, radius=rn, startTime=0.0, duration=1.0e4, densityRate=1.2, heatRate=3.5,
+                                     fuelRate=4.0, noiseScale=9.0, noiseMix=0.45, seed=sd))
+        sources.append(VelocityEmitter(position=pos, radius=rn * 1.3, startTime=0.0, duration=1.0e4, mode="directional",
+                                       speed=e["speed"], direction=(0.0, 1.0, 0.0), falloff=0.7, seed=sd + 1.0, tightness=0.25))
+        # the reference's combustion has no burn-rate knob: the burn rate sets the igniter intensity
+        sources.append(IgniterEmitter(position=pos, radius=rn, startTime=0.0, duration=1.0e4, intensity=e["burn"], seed=sd + 2.0))
+    options = {
+        "resolution": res,
+        "worldSize": max(w, d) / 64.0,
+        "gravityStrength": 0.1,
+        "buoyancy": 1.0,
+        "vorticityStrength": 0.3,
+        "qualitySettings": dict(QUALITY_C0),
+    }
+    state = _plume_state(res, centers, [r * scale for r in radii], heights, p["seed"])
+    return Workload(f"batch_{p['index']}", options, sources, state, target_fraction=p["target"])
+
+
+def batch_c3(seed: int = 1237, count: int = 64, processes: int = 0) -> List[Workload]:
+    """The batched configuration: `count` independent simulations, each with a
+    bounding box of seeded sides in {32, 40, ..., 192}, 1-3 floor emitters with
+    seeded radius, inflow speed in [1, 3] and burn rate in [0.2, 1.0], and a
+    developed-plume start state whose brick flags cover a seeded fraction in
+    [0.1, 0.6]. processes > 1 builds the states in a spawn-started process pool
+    (safe after CUDA initialisation); the result does not depend on it."""
+    rng = Pcg32(seed)
+    params = [_batch_draw(i, rng, seed) for i in range(count)]
+    if processes and processes > 1:
+        import multiprocessing
+        from concurrent.futures import ProcessPoolExecutor
+
+        with ProcessPoolExecutor(max_workers=processes, mp_context=multiprocessing.get_context("spawn")) as ex:
+            return list(ex.map(_batch_build, params))
+    return [_batch_build(p) for p in params]
