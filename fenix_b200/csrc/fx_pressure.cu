@@ -470,6 +470,72 @@ __global__ void __launch_bounds__(256) k_sweep(Dims dm, const float* __restrict_
   }
 }
 
+// k_sweep with two consecutive x per thread (even widths): a warp covers 64 x,
+// the column loads are float2, and one shuffle per voxel brings the outer x
+// neighbour of each pair from the next lane. Each voxel's sum, division and
+// prolongation are those of k_sweep, in the same order, so the results are the
+// same bits.
+template <int ZB>
+__global__ void __launch_bounds__(256) k_sweep_v2(Dims dm, const float* __restrict__ div, const float* __restrict__ src, float* __restrict__ dst,
+                                                  Dims mid, const float* __restrict__ mid_p) {
+  const uint32_t lane = threadIdx.x;
+  const uint32_t x0 = blockIdx.x * 64 + 2 * lane, y = blockIdx.y * 8 + threadIdx.y, z0 = blockIdx.z * ZB;
+  if (y >= dm.h) return;  // whole warp
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  const bool xin = x0 < dm.w;  // dm.w is even: x0 + 1 < dm.w too
+  const uint32_t base = (xin ? x0 : dm.w - 2) + dm.w * y;
+  const bool yint = y > 0 && y < dm.h - 1;
+  const int nz = min(ZB, (int)dm.d - (int)z0);
+  const float2* __restrict__ src2 = reinterpret_cast<const float2*>(src);
+  const float2* __restrict__ div2 = reinterpret_cast<const float2*>(div);
+  float2* __restrict__ dst2 = reinterpret_cast<float2*>(dst);
+  if (!yint) {
+    if (xin)
+      for (int k = 0; k < nz; ++k) dst2[(base + sz * (z0 + k)) >> 1] = make_float2(0.0f, 0.0f);
+    return;
+  }
+  const bool int0 = x0 > 0 && x0 < dm.w - 1, int1 = x0 + 1 < dm.w - 1;
+  const bool left_end = lane == 0 && x0 > 0, right_end = lane == 31 && x0 + 2 < dm.w;
+  float2 c[ZB + 2], yp[ZB], ym[ZB], dv[ZB];
+  float xl_e[ZB], xr_e[ZB];
+#pragma unroll
+  for (int k = 0; k < ZB + 2; ++k) {
+    const int z = (int)z0 + k - 1;
+    c[k] = (src && z >= 0 && z < (int)dm.d) ? __ldg(src2 + ((base + sz * (uint32_t)z) >> 1)) : make_float2(0.0f, 0.0f);
+  }
+#pragma unroll
+  for (int k = 0; k < ZB; ++k) {
+    const uint32_t z = min(z0 + k, dm.d - 1);
+    const uint32_t i = base + sz * z;
+    dv[k] = __ldg(div2 + (i >> 1));
+    yp[k] = src ? __ldg(src2 + ((i + sy) >> 1)) : make_float2(0.0f, 0.0f);
+    ym[k] = src ? __ldg(src2 + ((i - sy) >> 1)) : make_float2(0.0f, 0.0f);
+    xl_e[k] = (src && left_end) ? __ldg(src + i - 1) : 0.0f;
+    xr_e[k] = (src && right_end) ? __ldg(src + i + 2) : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < ZB; ++k) {
+    const float2 cm = c[k + 1];
+    float left = __shfl_up_sync(0xffffffffu, cm.y, 1);     // x0 - 1
+    float right = __shfl_down_sync(0xffffffffu, cm.x, 1);  // x0 + 2
+    if (left_end) left = xl_e[k];
+    if (right_end) right = xr_e[k];
+    const uint32_t z = z0 + k;
+    if (k >= nz || !xin) continue;
+    const bool zint = z > 0 && z < dm.d - 1;
+    float v0 = 0.0f, v1 = 0.0f;
+    if (zint && int0) {
+      v0 = src ? div6(cm.y + left + yp[k].x + ym[k].x + c[k + 2].x + c[k].x - dv[k].x) : div6(0.0f - dv[k].x);
+      if (mid_p) v0 = v0 + prolong_sample(mid, mid_p, (int)x0, (int)y, (int)z);
+    }
+    if (zint && int1) {
+      v1 = src ? div6(right + cm.x + yp[k].y + ym[k].y + c[k + 2].y + c[k].y - dv[k].y) : div6(0.0f - dv[k].y);
+      if (mid_p) v1 = v1 + prolong_sample(mid, mid_p, (int)x0 + 1, (int)y, (int)z);
+    }
+    dst2[(base + sz * z) >> 1] = make_float2(v0, v1);
+  }
+}
+
 // The cleared buffer plus the prolongation (finePre = 0): boundary 0, interior 0 + sample.
 __global__ void __launch_bounds__(256) k_prolong_zero(Dims dm, float* __restrict__ dst, Dims mid, const float* __restrict__ mid_p) {
   const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 4 + threadIdx.y, z = blockIdx.z * 2 + threadIdx.z;
@@ -737,6 +803,16 @@ cudaError_t lean_div_first(cudaStream_t s, Dims dm, VelField v, float* div, floa
 
 cudaError_t lean_sweep(cudaStream_t s, Dims dm, const float* div, const float* src, float* dst, Dims mid, const float* mid_p) {
   static const int zb = env_int("FENIX_SWEEP_ZB", 4, 1, 8);
+  static const int vec = env_int("FENIX_SWEEP_VEC", 1, 0, 1);
+  static const int vzb = env_int("FENIX_SWEEP_VEC_ZB", 2, 2, 4);
+  if (vec && dm.w % 2 == 0 && dm.w >= 4) {
+    if (vzb <= 2) {
+      k_sweep_v2<2><<<dim3((dm.w + 63) / 64, (dm.h + 7) / 8, (dm.d + 1) / 2), dim3(32, 8, 1), 0, s>>>(dm, div, src, dst, mid, mid_p);
+    } else {
+      k_sweep_v2<4><<<dim3((dm.w + 63) / 64, (dm.h + 7) / 8, (dm.d + 3) / 4), dim3(32, 8, 1), 0, s>>>(dm, div, src, dst, mid, mid_p);
+    }
+    return cudaGetLastError();
+  }
   auto grid = [&](int z) { return dim3((dm.w + 31) / 32, (dm.h + 7) / 8, (dm.d + z - 1) / z); };
   if (zb <= 2) k_sweep<2><<<grid(2), dim3(32, 8, 1), 0, s>>>(dm, div, src, dst, mid, mid_p);
   else if (zb <= 4) k_sweep<4><<<grid(4), dim3(32, 8, 1), 0, s>>>(dm, div, src, dst, mid, mid_p);
