@@ -137,6 +137,35 @@ class FxDebugBuffers(Structure):
     ]
 
 
+FX_MAX_RENDER_LIGHTS = 3
+FX_LIGHT_DIRECTIONAL = 0
+FX_LIGHT_POINT = 1
+FX_RM_STEP_COUNT = 1 << 0
+FX_RM_LIGHTS = 1 << 1
+FX_RM_SCATTER_FORWARD = 1 << 2
+FX_RM_SCATTER_BACK = 1 << 3
+FX_DISPLAY_TEMPERATURE = 0
+FX_DISPLAY_DENSITY = 1
+FX_DISPLAY_FUEL = 2
+FX_PIXELS_RGBA16F = 0
+FX_PIXELS_RGBA32F = 1
+
+
+class FxCamera(Structure):
+    _fields_ = [("position", c_double * 3), ("target", c_double * 3), ("forward", c_double * 3), ("right", c_double * 3),
+                ("up", c_double * 3), ("aspect", c_double), ("tan_half_fov_y", c_double)]
+
+
+class FxRenderLight(Structure):
+    _fields_ = [("type", c_int32), ("reserved", c_int32), ("direction", c_double * 3), ("position", c_double * 3),
+                ("color", c_double * 3), ("intensity", c_double)]
+
+
+class FxRaymarchParams(Structure):
+    _fields_ = [("mask", c_uint32), ("light_count", c_uint32), ("step_count", c_double), ("scattering_forward", c_double),
+                ("scattering_back", c_double), ("lights", FxRenderLight * FX_MAX_RENDER_LIGHTS)]
+
+
 class FxStats(Structure):
     _fields_ = [
         ("step_index", c_int64),
@@ -217,6 +246,10 @@ PROTOTYPES = [
     ("fx_batch_synchronize", c_int32, [c_void_p]),
     ("fx_batch_get_stream", c_int32, [c_void_p, POINTER(c_void_p)]),
     ("fx_batch_last_error", c_char_p, [c_void_p]),
+    ("fx_raymarch_create", c_int32, [c_uint32, c_uint32, c_uint32, POINTER(c_void_p)]),
+    ("fx_raymarch_destroy", None, [c_void_p]),
+    ("fx_raymarch_set_params", c_int32, [c_void_p, POINTER(FxRaymarchParams)]),
+    ("fx_raymarch_render", c_int32, [c_void_p, c_void_p, POINTER(FxCamera), c_int32, c_uint32, c_uint32, c_double, c_void_p, c_int32]),
     ("fx_brick_flags_noalloc", c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_void_p, c_void_p]),
 ]
 
@@ -224,6 +257,7 @@ PROTOTYPES = [
 TEST_PROTOTYPES = [
     ("fx_test_pinned_sincos", c_int32, [POINTER(c_float), POINTER(c_float), c_uint32, c_int32]),
     ("fx_test_div6_exhaustive", c_int32, [POINTER(c_uint64)]),
+    ("fx_test_pinned_exp_pow", c_int32, [POINTER(c_float), POINTER(c_float), POINTER(c_float), POINTER(c_float), c_uint32]),
 ]
 
 _LIB = None

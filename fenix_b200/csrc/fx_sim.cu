@@ -498,6 +498,30 @@ fx_status step_finish(fx_sim* s, fx_status st, const FusedResult* fr, const Step
 namespace fx {
 // The calling thread's fx_last_error message, for entry points outside this file.
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+// The state a render reads: the current scalar set and brick flags (what
+// getRenderBuffers returns), on the simulation's stream.
+struct SimView {
+  Dims dm;
+  uint3 bricks;
+  const void* f[4];
+  const uint32_t* flags;
+  bool half;
+  cudaStream_t stream;
+  int device;
+};
+
+bool sim_view(fx_sim* s, SimView* out) {
+  if (!s || !s->err.empty()) return false;
+  out->dm = s->dm;
+  out->bricks = s->bricks;
+  for (int k = 0; k < 4; ++k) out->f[k] = s->sets[s->cur].f[k];
+  out->flags = s->flags[s->cur];
+  out->half = s->half;
+  out->stream = s->stream;
+  out->device = s->device;
+  return true;
+}
 }  // namespace fx
 
 extern "C" {

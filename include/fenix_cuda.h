@@ -357,6 +357,77 @@ fx_status fx_batch_synchronize(fx_batch* batch);
 fx_status fx_batch_get_stream(fx_batch* batch, void** stream);
 const char* fx_batch_last_error(fx_batch* batch);
 
+/* Volume raymarch: the reference's VolumeRaymarchPass
+ * (src/engine/render/passes/createVolumeRaymarchPass.ts:15-29), whose fragment
+ * shader (:300-726) runs as a CUDA kernel into a headless RGBA device buffer
+ * instead of a WebGPU render target. It reads a simulation's render buffers
+ * (the current scalar set and brick flags, f32 or FP16) and skips inactive
+ * bricks as the shader does. */
+#define FX_MAX_RENDER_LIGHTS 3
+#define FX_LIGHT_DIRECTIONAL 0
+#define FX_LIGHT_POINT 1
+
+/* OrbitCameraSnapshot (src/engine/scene/camera/createOrbitCameraController.ts:11-19). */
+typedef struct fx_camera {
+  double position[3];
+  double target[3];
+  double forward[3];
+  double right[3];
+  double up[3];
+  double aspect;
+  double tan_half_fov_y;
+} fx_camera;
+
+/* RenderLight (src/engine/render/lighting/renderLight.ts:3-9). */
+typedef struct fx_render_light {
+  int32_t type; /* FX_LIGHT_* */
+  int32_t reserved;
+  double direction[3];
+  double position[3];
+  double color[3];
+  double intensity;
+} fx_render_light;
+
+/* RaymarchRenderParams (createVolumeRaymarchPass.ts:8-13); the mask stands for
+ * Partial<>, and the values are clamped as setRenderParams does (:268-281). */
+typedef struct fx_raymarch_params {
+  uint32_t mask;        /* FX_RM_* */
+  uint32_t light_count; /* with FX_RM_LIGHTS: lights[0..light_count) (at most 3 are kept) */
+  double step_count;    /* rounded, then clamped to [32, 4096] (the reference has no upper bound) */
+  double scattering_forward; /* clamped to [0, 0.98] */
+  double scattering_back;    /* clamped to [-0.98, 0] */
+  fx_render_light lights[FX_MAX_RENDER_LIGHTS];
+} fx_raymarch_params;
+
+#define FX_RM_STEP_COUNT (1u << 0)
+#define FX_RM_LIGHTS (1u << 1)
+#define FX_RM_SCATTER_FORWARD (1u << 2)
+#define FX_RM_SCATTER_BACK (1u << 3)
+
+/* VolumeDisplayMode (src/engine/render/volumetrics/volumeDisplayMode.ts). */
+#define FX_DISPLAY_TEMPERATURE 0
+#define FX_DISPLAY_DENSITY 1
+#define FX_DISPLAY_FUEL 2
+
+#define FX_PIXELS_RGBA16F 0 /* 4 x IEEE binary16 per pixel */
+#define FX_PIXELS_RGBA32F 1 /* 4 x float per pixel */
+
+typedef struct fx_raymarch fx_raymarch;
+
+/* createVolumeRaymarchPass(device, format, resolution) (:81-91): world bounds
+ * and the default step count of the resolution, the default light. */
+fx_status fx_raymarch_create(uint32_t width, uint32_t height, uint32_t depth, fx_raymarch** out);
+void fx_raymarch_destroy(fx_raymarch* pass);
+/* setRenderParams (:268-281). */
+fx_status fx_raymarch_set_params(fx_raymarch* pass, const fx_raymarch_params* params);
+/* render(encoder, view, buffers, camera, displayMode, width, height, elapsed)
+ * (:184-266): fills `pixels`, a device buffer of render_width * render_height
+ * RGBA pixels (row 0 at the top, premultiplied colour; (0, 0, 0, 0) where the
+ * reference's fragment discards), on the simulation's stream. The simulation
+ * must have the pass's resolution. */
+fx_status fx_raymarch_render(fx_raymarch* pass, fx_sim* sim, const fx_camera* camera, int32_t display_mode, uint32_t render_width,
+                             uint32_t render_height, double elapsed_seconds, void* pixels, int32_t pixel_format);
+
 /* Brick flags of caller-owned fields, allocating nothing. No counterpart in the
  * reference. It computes what compute-active-bricks.wgsl.ts:35-58 computes, for
  * the density, temperature and reaction fields (width*height*depth floats each,

@@ -13,6 +13,7 @@ import sys
 
 ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
 SOURCE = os.path.join(ORACLE_DIR, "fenix_oracle.cpp")
+SOURCES = [SOURCE, os.path.join(ORACLE_DIR, "raymarch.cpp")]
 OUTPUT = os.path.join(ORACLE_DIR, "liboracle_fenix.so")
 
 CXX_FLAGS = ["-O3", "-std=c++17", "-march=x86-64-v3", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared"]
@@ -26,13 +27,13 @@ def compiler() -> str:
 
 
 def needs_build() -> bool:
-    return not os.path.exists(OUTPUT) or os.path.getmtime(SOURCE) > os.path.getmtime(OUTPUT)
+    return not os.path.exists(OUTPUT) or any(os.path.getmtime(src) > os.path.getmtime(OUTPUT) for src in SOURCES)
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return OUTPUT
-    cmd = [compiler(), *CXX_FLAGS, "-o", OUTPUT, SOURCE]
+    cmd = [compiler(), *CXX_FLAGS, "-o", OUTPUT, *SOURCES]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -42,6 +42,10 @@ def load() -> ctypes.CDLL:
         lib.orc_set_advection_mode.argtypes = [c_void_p, c_int]
         lib.orc_set_emit_dead_residual.argtypes = [c_void_p, c_int]
         lib.orc_set_half_storage.argtypes = [c_void_p, c_int]
+        lib.orc_raymarch.argtypes = [POINTER(c_float)] * 4 + [POINTER(c_uint32), c_uint32, c_uint32, c_uint32, POINTER(c_double), c_int,
+                                                             c_uint32, c_uint32, c_double, POINTER(c_double), c_int, POINTER(c_double),
+                                                             POINTER(c_float)]
+        lib.orc_pinned_exp_pow.argtypes = [POINTER(c_float), POINTER(c_float), POINTER(c_float), POINTER(c_float), c_long]
         lib.orc_set_solver.argtypes = [c_void_p, POINTER(c_int), POINTER(c_double), c_int]
         lib.orc_get_solver_stats.argtypes = [c_void_p, POINTER(c_double), POINTER(c_int)]
         lib.orc_update_sources.argtypes = [c_void_p, POINTER(c_float), c_uint32]
@@ -252,3 +256,46 @@ class OracleSimulation:
             self.dispose()
         except Exception:
             pass
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_float))
+
+
+def raymarch(orc: "OracleSimulation", camera: Mapping[str, Any], displayMode: str, width: int, height: int, elapsed: float = 0.0,
+             params: Optional[Mapping[str, Any]] = None) -> np.ndarray:
+    """The reference's volume raymarch of the oracle's current render buffers
+    (oracle/raymarch.cpp), as float32 RGBA of shape (height, width, 4)."""
+    lib = load()
+    params = dict(params or {})
+    w, h, d = orc.resolution["width"], orc.resolution["height"], orc.resolution["depth"]
+    fields = [np.ascontiguousarray(orc.readField(n), dtype=np.float32) for n in ("density", "temperature", "fuel", "reaction")]
+    flags = np.ascontiguousarray(orc.readField("brick_flags"), dtype=np.uint32)
+    cam = (c_double * 17)(*[float(v) for k in ("position", "target", "forward", "right", "up") for v in camera[k]],
+                          float(camera["aspect"]), float(camera["tanHalfFovY"]))
+    st = params.get("stepCount")
+    sf, sb = params.get("scatteringForward"), params.get("scatteringBack")
+    settings = (c_double * 6)(1.0 if st is not None else 0.0, float(st or 0.0), 1.0 if sf is not None else 0.0, float(sf or 0.0),
+                              1.0 if sb is not None else 0.0, float(sb or 0.0))
+    lights = params.get("lights")
+    flat = []
+    for l in (lights or [])[:3]:
+        flat += [1.0 if l.get("type") == "point" else 0.0, *map(float, l.get("direction", (0.0, 1.0, 0.0))),
+                 *map(float, l.get("position", (0.0, 0.0, 0.0))), *map(float, l.get("color", (1.0, 1.0, 1.0))), float(l.get("intensity", 1.0))]
+    larr = (c_double * max(len(flat), 1))(*flat) if flat else (c_double * 1)(0.0)
+    mode = {"temperature": 0, "density": 1, "fuel": 2}[displayMode]
+    out = np.zeros((height, width, 4), dtype=np.float32)
+    lib.orc_raymarch(*[_fptr(f) for f in fields], flags.ctypes.data_as(POINTER(c_uint32)), w, h, d, cam, mode, width, height,
+                     float(elapsed), settings, -1 if lights is None else len(lights[:3]), larr, _fptr(out))
+    return out
+
+
+def pinned_exp_pow(x: np.ndarray, y: np.ndarray):
+    """The pinned f32 exp(x) and pow(x, y) of the raymarch."""
+    lib = load()
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    oe = np.empty_like(x)
+    op = np.empty_like(x)
+    lib.orc_pinned_exp_pow(_fptr(x), _fptr(y), _fptr(oe), _fptr(op), x.size)
+    return oe, op
