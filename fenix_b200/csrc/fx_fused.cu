@@ -295,13 +295,13 @@ FX_DEV float tri_interp_clamped(const float* __restrict__ f, const Tri& c, float
 // without NaN this reads one value instead of eight.
 constexpr int kAdvZ = 4;
 
-__global__ void __launch_bounds__(256) k_advect_velocity(Dims dm, const Params* __restrict__ Pp, VelField src, VelField dst) {
-  const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z0 = blockIdx.z * kAdvZ;
-  if (x >= dm.w || y >= dm.h) return;
-  const float dt = Pp->dt;
-  const float lim = speed_limit(*Pp);
-  const float damp = 1.0f - dt * 0.025f;
-  const bool xyint = x > 0 && y > 0 && x < dm.w - 1 && y < dm.h - 1;
+// The clamp is the identity on every value when the largest |v| of the field is
+// within the limit: `vmax` holds that bound (float bits, written by the
+// projection that produced the field; all ones when unknown), and the kernel
+// then reads the values as they are, with the same results.
+template <bool CLAMP>
+FX_DEV void advect_velocity_column(Dims dm, uint32_t x, uint32_t y, uint32_t z0, float dt, float lim, float damp, bool xyint,
+                                   const VelField& src, const VelField& dst) {
 #pragma unroll
   for (int k = 0; k < kAdvZ; ++k) {
     const uint32_t z = z0 + k;
@@ -314,15 +314,36 @@ __global__ void __launch_bounds__(256) k_advect_velocity(Dims dm, const Params* 
       continue;
     }
     const float cx = (float)x + 0.5f, cy = (float)y + 0.5f, cz = (float)z + 0.5f;
-    const float v0x = clampv(__ldg(src.c[0] + i), -lim, lim);
-    const float v0y = clampv(__ldg(src.c[1] + i), -lim, lim);
-    const float v0z = clampv(__ldg(src.c[2] + i), -lim, lim);
+    float v0x = __ldg(src.c[0] + i), v0y = __ldg(src.c[1] + i), v0z = __ldg(src.c[2] + i);
+    if (CLAMP) {
+      v0x = clampv(v0x, -lim, lim);
+      v0y = clampv(v0y, -lim, lim);
+      v0z = clampv(v0z, -lim, lim);
+    }
     const float bx = cx - v0x * dt, by = cy - v0y * dt, bz = cz - v0z * dt;
     const Tri c1 = tri_corners(dm, bx - 0.5f, by - 0.5f, bz - 0.5f);
-    dst.c[0][i] = tri_interp_clamped(src.c[0], c1, lim) * damp;
-    dst.c[1][i] = tri_interp_clamped(src.c[1], c1, lim) * damp;
-    dst.c[2][i] = tri_interp_clamped(src.c[2], c1, lim) * damp;
+    if (CLAMP) {
+      dst.c[0][i] = tri_interp_clamped(src.c[0], c1, lim) * damp;
+      dst.c[1][i] = tri_interp_clamped(src.c[1], c1, lim) * damp;
+      dst.c[2][i] = tri_interp_clamped(src.c[2], c1, lim) * damp;
+    } else {
+      dst.c[0][i] = tri_interp(src.c[0], c1) * damp;
+      dst.c[1][i] = tri_interp(src.c[1], c1) * damp;
+      dst.c[2][i] = tri_interp(src.c[2], c1) * damp;
+    }
   }
+}
+
+__global__ void __launch_bounds__(256) k_advect_velocity(Dims dm, const Params* __restrict__ Pp, VelField src, VelField dst,
+                                                         const unsigned* __restrict__ vmax) {
+  const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z0 = blockIdx.z * kAdvZ;
+  if (x >= dm.w || y >= dm.h) return;
+  const float dt = Pp->dt;
+  const float lim = speed_limit(*Pp);
+  const float damp = 1.0f - dt * 0.025f;
+  const bool xyint = x > 0 && y > 0 && x < dm.w - 1 && y < dm.h - 1;
+  if (__uint_as_float(__ldg(vmax)) <= lim) advect_velocity_column<false>(dm, x, y, z0, dt, lim, damp, xyint, src, dst);
+  else advect_velocity_column<true>(dm, x, y, z0, dt, lim, damp, xyint, src, dst);
 }
 
 // -------------------------------------------------------------- scalar advection
@@ -581,10 +602,8 @@ __global__ void __launch_bounds__(256) k_confinement(Dims dm, uint3 bc, const Pa
 // a column of kProjZ voxels and reuses the z neighbours of the pressure.
 constexpr int kProjZ = 8;
 
-__global__ void __launch_bounds__(256) k_project(Dims dm, VelField vs, const float* __restrict__ p, VelField vd, float* __restrict__ vmag,
-                                                 int write_vmag) {
-  const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z0 = blockIdx.z * kProjZ;
-  if (x >= dm.w || y >= dm.h) return;
+FX_DEV void project_column(Dims dm, uint32_t x, uint32_t y, uint32_t z0, const VelField& vs, const float* __restrict__ p, const VelField& vd,
+                           float* __restrict__ vmag, int write_vmag, float& m) {
   const uint32_t sy = dm.w, sz = dm.w * dm.h;
   const uint32_t base = x + dm.w * y;
   const bool xyint = x > 0 && y > 0 && x < dm.w - 1 && y < dm.h - 1;
@@ -614,6 +633,27 @@ __global__ void __launch_bounds__(256) k_project(Dims dm, VelField vs, const flo
     vd.c[1][i] = oy;
     vd.c[2][i] = oz;
     if (write_vmag) vmag[i] = length3(ox, oy, oz);
+    m = fmaxf(m, fmaxf(fabsf(ox), fmaxf(fabsf(oy), fabsf(oz))));
+  }
+}
+
+// Also records max |v| of the result in *vmax (float bits; reset to 0 before
+// the launch) for the next step's velocity advection.
+__global__ void __launch_bounds__(256) k_project(Dims dm, VelField vs, const float* __restrict__ p, VelField vd, float* __restrict__ vmag,
+                                                 int write_vmag, unsigned* __restrict__ vmax) {
+  const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z0 = blockIdx.z * kProjZ;
+  const bool live = x < dm.w && y < dm.h;
+  float m = 0.0f;
+  if (live) project_column(dm, x, y, z0, vs, p, vd, vmag, write_vmag, m);
+  // block maximum, then one atomic per block when it raises the bound
+  unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(m));
+  __shared__ unsigned part[8];
+  const int warp = threadIdx.y;
+  if (threadIdx.x == 0) part[warp] = bits;
+  __syncthreads();
+  if (threadIdx.x == 0 && warp == 0) {
+    for (int k = 1; k < 8; ++k) bits = max(bits, part[k]);
+    if (bits > __ldcg(vmax)) atomicMax(vmax, bits);
   }
 }
 
@@ -718,7 +758,7 @@ void injection_bricks(const FusedStep& st, std::vector<uint8_t>& mark, std::vect
 
 size_t fused_work_bytes(Dims, uint3 bricks) {
   const size_t nb = (size_t)bricks.x * bricks.y * bricks.z;
-  return 8 * align256(nb) + 3 * align256(nb * 4) + align256(16 * 4) + align256(96 * 4) + align256(sizeof(SolverDev));
+  return 8 * align256(nb) + 3 * align256(nb * 4) + align256(16 * 4) + align256(96 * 4) + align256(sizeof(SolverDev)) + align256(4);
 }
 
 void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks) {
@@ -745,6 +785,7 @@ void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks) {
   w.counters = (uint32_t*)take(16 * 4);
   w.mg_bar = (unsigned*)take(96 * 4);
   w.solver = (SolverDev*)take(sizeof(SolverDev));
+  w.vmax = (unsigned*)take(4);
 }
 
 fx_status fused_init(FusedWork& w, cudaStream_t) {
@@ -849,6 +890,8 @@ fx_status fused_prepare(FusedWork& w, const FusedStep& st, uint32_t* ninj_out, F
   uint32_t* c_inj = w.counters + 3;
 
   if (!w.valid) {
+    // the fields came from the host: their largest |v| is unknown
+    FX_CK(cudaMemsetAsync(w.vmax, 0xFF, sizeof(unsigned), s));
     Timed tm(w, s, "fused_rebuild");
     by_storage(st.half_storage, [&](auto tag) {
       using S = typename decltype(tag)::type;
@@ -1056,7 +1099,8 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   // 3. velocity advection (dense)
   {
     Timed tm(w, s, "fused_advect_velocity");
-    k_advect_velocity<<<dim3((dm.w + 31) / 32, (dm.h + 7) / 8, (dm.d + kAdvZ - 1) / kAdvZ), dim3(32, 8, 1), 0, s>>>(dm, st.params, st.vcur, st.vscr);
+    k_advect_velocity<<<dim3((dm.w + 31) / 32, (dm.h + 7) / 8, (dm.d + kAdvZ - 1) / kAdvZ), dim3(32, 8, 1), 0, s>>>(dm, st.params, st.vcur, st.vscr,
+                                                                                                                 w.vmax);
     ++launches;
   }
   // 4. scalar advection over the list
@@ -1120,7 +1164,8 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     const fx_status vs = vcycle_solve(w, st, *vfinal, launches, out);
     if (vs != FX_OK) return vs;
     Timed tm(w, s, "fused_project");
-    k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0);
+    FX_CK(cudaMemsetAsync(w.vmax, 0, sizeof(unsigned), s));
+    k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax);
     ++launches;
   } else if (st.pressure_on) {
     const int m = st.q[2], n = st.q[3];
@@ -1232,10 +1277,13 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       }
       {
         Timed tm(w, s, "fused_project");
-        k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, F.p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0);
+        FX_CK(cudaMemsetAsync(w.vmax, 0, sizeof(unsigned), s));
+        k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, F.p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax);
         ++launches;
       }
     } else {
+      // The projection of these passes does not record max |v|: mark it unknown.
+      FX_CK(cudaMemsetAsync(w.vmax, 0xFF, sizeof(unsigned), s));
       // Plan the fine passes: pre-smoothing in groups of <= 4 sweeps (the first one
       // also computes the divergence), post-smoothing in groups of <= 4 sweeps (the
       // first adds the prolongation, the last finishes with the projection).
@@ -1352,7 +1400,8 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   } else {
     // 10. projection with the pressure of the last solve (+ |v|)
     Timed tm(w, s, "fused_project");
-    k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0);
+    FX_CK(cudaMemsetAsync(w.vmax, 0, sizeof(unsigned), s));
+    k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax);
     ++launches;
   }
   // FP64 statistics of the solve: ||div||, ||div - A p|| (the V-cycle has them

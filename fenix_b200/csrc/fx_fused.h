@@ -44,6 +44,7 @@ struct FusedWork {
   uint32_t* counters = nullptr;   // [0] adv count, [1] next count, [2] scratch, [3] inject count
   unsigned* mg_bar = nullptr;      // grid barrier of the lower multigrid kernel: arrivals, generation, error flag
   SolverDev* solver = nullptr;     // FP64 solver statistics and the V-cycle loop state
+  unsigned* vmax = nullptr;        // max |v| of the current velocity (float bits; all ones = unknown)
   cudaStream_t aux = nullptr;      // captures the V-cycle body graph
   int* host_cont = nullptr;        // pinned: the continue flag, read by the host loop without graphs
   uint32_t* host_list_inj = nullptr;  // pinned staging for list_inj (+ count at [nb])
