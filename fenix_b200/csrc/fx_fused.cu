@@ -135,6 +135,25 @@ __global__ void k_accumulate_active(Dims dm, uint3 bc, const uint32_t* __restric
   }
 }
 
+// The six neighbours of voxel (x, y, z) at flat index i, clamped as the
+// reference's inc/dec (clamp-utils.wgsl.ts:12-22): i -+ 1, i -+ sy, i -+ sz, or
+// i itself at the grid edge.
+struct Nbr {
+  uint32_t xp, xm, yp, ym, zp, zm;
+};
+
+FX_DEV Nbr neighbours(const Dims& dm, uint32_t x, uint32_t y, uint32_t z, uint32_t i) {
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  Nbr n;
+  n.xp = x + 1u < dm.w ? i + 1u : i;
+  n.xm = x > 0u ? i - 1u : i;
+  n.yp = y + 1u < dm.h ? i + sy : i;
+  n.ym = y > 0u ? i - sy : i;
+  n.zp = z + 1u < dm.d ? i + sz : i;
+  n.zm = z > 0u ? i - sz : i;
+  return n;
+}
+
 // Brick geometry of a list entry and the two voxels each thread owns.
 struct BrickCtx {
   uint32_t bx, by, bz;
@@ -458,12 +477,9 @@ __global__ void __launch_bounds__(kBrickThreads) k_combustion(Dims dm, uint3 bc,
         r = ldS(tset.f[3], i);
       }
       if (active) {
-        auto hot = [&](uint32_t xx, uint32_t yy, uint32_t zz) {
-          const uint32_t k = flat(dm, xx, yy, zz);
-          return comb_hot(ldS(tset.f[1], k), ldS(tset.f[2], k), ldS(tset.f[3], k));
-        };
-        const float nsum = hot(inc(x, W1), y, z) + hot(dec(x), y, z) + hot(x, inc(y, H1), z) + hot(x, dec(y), z) + hot(x, y, inc(z, D1)) +
-                           hot(x, y, dec(z));
+        auto hot = [&](uint32_t k) { return comb_hot(ldS(tset.f[1], k), ldS(tset.f[2], k), ldS(tset.f[3], k)); };
+        const Nbr n = neighbours(dm, x, y, z, i);
+        const float nsum = hot(n.xp) + hot(n.xm) + hot(n.yp) + hot(n.ym) + hot(n.zp) + hot(n.zm);
         const float ny = ((float)y + 0.5f) / (float)dm.h;
         combustion_voxel(P, x, y, z, ny, nsum, d, t, f, r);
         d = qS<S>(d);
@@ -507,17 +523,15 @@ __global__ void __launch_bounds__(kBrickThreads) k_buoyancy(Dims dm, uint3 bc, c
       if (x >= dm.w || y >= dm.h || z >= dm.d) continue;
       const uint32_t i = flat(dm, x, y, z);
       const S* D = set.f[0];
-      auto hot = [&](uint32_t xx, uint32_t yy, uint32_t zz) {
-        const uint32_t k = flat(dm, xx, yy, zz);
-        return buoy_hot(ldS(set.f[1], k), ldS(set.f[3], k));
-      };
-      const float hot_gas = hot(x, y, z);
-      const float tgx = (hot(inc(x, W1), y, z) - hot(dec(x), y, z)) * 0.5f;
-      const float tgy = (hot(x, inc(y, H1), z) - hot(x, dec(y), z)) * 0.5f;
-      const float tgz = (hot(x, y, inc(z, D1)) - hot(x, y, dec(z))) * 0.5f;
-      const float dgx = (ldS(D, flat(dm, inc(x, W1), y, z)) - ldS(D, flat(dm, dec(x), y, z))) * 0.5f;
-      const float dgy = (ldS(D, flat(dm, x, inc(y, H1), z)) - ldS(D, flat(dm, x, dec(y), z))) * 0.5f;
-      const float dgz = (ldS(D, flat(dm, x, y, inc(z, D1))) - ldS(D, flat(dm, x, y, dec(z)))) * 0.5f;
+      auto hot = [&](uint32_t k) { return buoy_hot(ldS(set.f[1], k), ldS(set.f[3], k)); };
+      const Nbr n = neighbours(dm, x, y, z, i);
+      const float hot_gas = hot(i);
+      const float tgx = (hot(n.xp) - hot(n.xm)) * 0.5f;
+      const float tgy = (hot(n.yp) - hot(n.ym)) * 0.5f;
+      const float tgz = (hot(n.zp) - hot(n.zm)) * 0.5f;
+      const float dgx = (ldS(D, n.xp) - ldS(D, n.xm)) * 0.5f;
+      const float dgy = (ldS(D, n.yp) - ldS(D, n.ym)) * 0.5f;
+      const float dgz = (ldS(D, n.zp) - ldS(D, n.zm)) * 0.5f;
       float vx = v.c[0][i], vy = v.c[1][i], vz = v.c[2][i];
       buoyancy_voxel(P, dm, x, y, z, ldS(D, i), hot_gas, tgx, tgy, tgz, dgx, dgy, dgz, vx, vy, vz);
       v.c[0][i] = vx;
@@ -530,11 +544,11 @@ __global__ void __launch_bounds__(kBrickThreads) k_buoyancy(Dims dm, uint3 bc, c
 // ------------------------------------------------------------ vorticity magnitude
 // compute-vorticity.wgsl.ts:23-50: |w| for every voxel (w itself only when the
 // debug fields are wanted; the confinement kernel recomputes w at its voxel).
-FX_DEV void curl_at(const Dims& dm, const VelField& v, uint32_t x, uint32_t y, uint32_t z, float& cx, float& cy, float& cz) {
-  const uint32_t W1 = dm.w - 1u, H1 = dm.h - 1u, D1 = dm.d - 1u;
-  const uint32_t x0 = flat(dm, dec(x), y, z), x1 = flat(dm, inc(x, W1), y, z);
-  const uint32_t y0 = flat(dm, x, dec(y), z), y1 = flat(dm, x, inc(y, H1), z);
-  const uint32_t z0 = flat(dm, x, y, dec(z)), z1 = flat(dm, x, y, inc(z, D1));
+// At an interior voxel i the reference's clamped neighbours (clamp-utils.wgsl.ts
+// dec/inc) are i -+ 1, i -+ sy, i -+ sz: the curl and gradients there read
+// them directly.
+FX_DEV void curl_at(const VelField& v, uint32_t i, uint32_t sy, uint32_t sz, float& cx, float& cy, float& cz) {
+  const uint32_t x0 = i - 1u, x1 = i + 1u, y0 = i - sy, y1 = i + sy, z0 = i - sz, z1 = i + sz;
   cx = ((__ldg(v.c[2] + y1) - __ldg(v.c[2] + y0)) - (__ldg(v.c[1] + z1) - __ldg(v.c[1] + z0))) * 0.5f;
   cy = ((__ldg(v.c[0] + z1) - __ldg(v.c[0] + z0)) - (__ldg(v.c[2] + x1) - __ldg(v.c[2] + x0))) * 0.5f;
   cz = ((__ldg(v.c[1] + x1) - __ldg(v.c[1] + x0)) - (__ldg(v.c[0] + y1) - __ldg(v.c[0] + y0))) * 0.5f;
@@ -547,7 +561,7 @@ __global__ void __launch_bounds__(256) k_vorticity(Dims dm, VelField v, float* _
   if (x >= dm.w || y >= dm.h || z >= dm.d) return;
   const uint32_t i = flat(dm, x, y, z);
   float cx = 0.f, cy = 0.f, cz = 0.f;
-  if (!is_boundary(dm, x, y, z)) curl_at(dm, v, x, y, z, cx, cy, cz);
+  if (!is_boundary(dm, x, y, z)) curl_at(v, i, dm.w, dm.w * dm.h, cx, cy, cz);
   wmag[i] = is_boundary(dm, x, y, z) ? 0.0f : length3(cx, cy, cz);
   if (write_w) {
     w.c[0][i] = cx;
@@ -577,12 +591,12 @@ __global__ void __launch_bounds__(256) k_confinement(Dims dm, uint3 bc, const Pa
     return;
   }
   const Params P = *Pp;
-  const uint32_t W1 = dm.w - 1u, H1 = dm.h - 1u, D1 = dm.d - 1u;
-  const float gx = (__ldg(wmag + flat(dm, inc(x, W1), y, z)) - __ldg(wmag + flat(dm, dec(x), y, z))) * 0.5f;
-  const float gy = (__ldg(wmag + flat(dm, x, inc(y, H1), z)) - __ldg(wmag + flat(dm, x, dec(y), z))) * 0.5f;
-  const float gz = (__ldg(wmag + flat(dm, x, y, inc(z, D1))) - __ldg(wmag + flat(dm, x, y, dec(z)))) * 0.5f;
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  const float gx = (__ldg(wmag + i + 1u) - __ldg(wmag + i - 1u)) * 0.5f;
+  const float gy = (__ldg(wmag + i + sy) - __ldg(wmag + i - sy)) * 0.5f;
+  const float gz = (__ldg(wmag + i + sz) - __ldg(wmag + i - sz)) * 0.5f;
   float wx, wy, wz;
-  curl_at(dm, v, x, y, z, wx, wy, wz);
+  curl_at(v, i, sy, sz, wx, wy, wz);
   const uint32_t b = (x >> 3) + bc.x * ((y >> 3) + bc.y * (z >> 3));
   float d = 0.f, t = 0.f, r = 0.f;
   if (__ldg(nz + b)) {
