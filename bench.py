@@ -381,6 +381,8 @@ def run_batch_c3(args, local, rank, world, pg):
         sim.updateSources(wl.sources)
         workloads.load_state(sim, wl.state)
         sim.setInstrumentation(count_active=True)
+        if not args.no_autotune:
+            sim.autotune()  # sweeps per level, chosen per simulation size
     bstream = torch.cuda.ExternalStream(batch.stream, device=dev)
     batched = timed(lambda t: batch.step(t, dt), bstream, batch.sims)
     batch.dispose()
@@ -421,6 +423,7 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip timing the FP32 plain and fused steps")
     ap.add_argument("--no-c3", action="store_true", help="skip the batched 64-simulation configuration")
     ap.add_argument("--c3-steps", type=int, default=100)
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default sweep kernels")
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
@@ -469,6 +472,7 @@ def main():
     for _ in range(args.warmup):
         sim.step(t, wl.dt)
         t += wl.dt
+    tuned = None if args.no_autotune or args.kernels != "fused" else sim.autotune()
     sim.synchronize()
     sim.readActiveCounters()
 
@@ -602,7 +606,7 @@ def main():
                 "workload": f"plume_{args.size}: {args.size}^3 grid, 4 floor plumes (scalar+velocity+igniter each), seeded "
                             f"developed-plume start, 4/4/4/4/20 sweeps, dt 1/60, f32 arithmetic, {args.storage} scalar storage, "
                             f"reference semantics",
-                "kernels": args.kernels, "scalar_storage": args.storage, "cuda_graph": bool(st_timed.get("graphReplay")), "active_fraction": active_mean / n, "global_batch": world, "seq_len": 0,
+                "kernels": args.kernels, "scalar_storage": args.storage, "autotune": tuned, "cuda_graph": bool(st_timed.get("graphReplay")), "active_fraction": active_mean / n, "global_batch": world, "seq_len": 0,
                 "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (about 2 GB of fields per step)",
             },
             "roofline": roofline, "kernels": kernel_table, "cpu_baseline": cpu, "parity_full_size": parity, "e2e": e2e,

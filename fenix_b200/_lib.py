@@ -166,6 +166,10 @@ class FxRaymarchParams(Structure):
                 ("scattering_back", c_double), ("lights", FxRenderLight * FX_MAX_RENDER_LIGHTS)]
 
 
+class FxAutotuneReport(Structure):
+    _fields_ = [("sweep_variant", c_int32 * 3), ("sweep_us", c_float * 3), ("default_us", c_float * 3)]
+
+
 class FxStats(Structure):
     _fields_ = [
         ("step_index", c_int64),
@@ -238,6 +242,7 @@ PROTOTYPES = [
     ("fx_sim_set_solver", c_int32, [c_void_p, POINTER(FxSolverSettings)]),
     ("fx_sim_get_solver", c_int32, [c_void_p, POINTER(FxSolverSettings)]),
     ("fx_sim_read_solver_stats", c_int32, [c_void_p, POINTER(FxSolverStats)]),
+    ("fx_sim_autotune", c_int32, [c_void_p, POINTER(FxAutotuneReport)]),
     ("fx_batch_create", c_int32, [POINTER(POINTER(FxSimOptions)), c_uint32, POINTER(c_void_p)]),
     ("fx_batch_destroy", None, [c_void_p]),
     ("fx_batch_size", c_int32, [c_void_p, POINTER(c_uint32)]),

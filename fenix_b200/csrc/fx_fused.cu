@@ -950,6 +950,7 @@ uint64_t fused_key(const FusedStep& st, uint32_t ninj) {
   mix_key((uint64_t)st.last_p);
   for (int k = 0; k < 7; ++k) mix_key((uint64_t)st.q[k]);
   mix_key((uint64_t)st.solver_mode);
+  for (int l = 0; l < 3; ++l) mix_key((uint64_t)(st.sweep_variant[l] + 1));
   mix_key(st.solver_norms);
   if (st.solver_mode == 1) {
     const VCycleConfig& c = st.vc;
@@ -1235,7 +1236,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
           int a = 0;
           for (int k = 0; k < st.q[4]; ++k) {
             Timed tm(w, s, "fused_sweep_mid");
-            FX_CK(lean_sweep(s, M.dm, M.div, k == 0 ? nullptr : M.p[a], M.p[a ^ 1], M.dm, nullptr));
+            FX_CK(lean_sweep_variant(s, st.sweep_variant[1], M.dm, M.div, k == 0 ? nullptr : M.p[a], M.p[a ^ 1], M.dm, nullptr));
             a ^= 1;
             ++launches;
           }
@@ -1251,7 +1252,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
           int a = 0;
           for (int k = 0; k < st.q[6]; ++k) {
             Timed tm(w, s, "fused_sweep_coarse");
-            FX_CK(lean_sweep(s, C.dm, C.div, k == 0 ? nullptr : C.p[a], C.p[a ^ 1], C.dm, nullptr));
+            FX_CK(lean_sweep_variant(s, st.sweep_variant[2], C.dm, C.div, k == 0 ? nullptr : C.p[a], C.p[a ^ 1], C.dm, nullptr));
             a ^= 1;
             ++launches;
           }
@@ -1265,7 +1266,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
         mid = mid_pre;
         for (int k = 0; k < st.q[5]; ++k) {
           Timed tm(w, s, "fused_sweep_mid");
-          FX_CK(lean_sweep(s, M.dm, M.div, M.p[mid], M.p[mid ^ 1], M.dm, nullptr));
+          FX_CK(lean_sweep_variant(s, st.sweep_variant[1], M.dm, M.div, M.p[mid], M.p[mid ^ 1], M.dm, nullptr));
           mid ^= 1;
           ++launches;
         }
@@ -1273,7 +1274,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       for (int k = 2; k <= m; ++k) {
         const bool add = prolong_live && k == m;
         Timed tm(w, s, add ? "fused_sweep_prolong" : "fused_sweep");
-        FX_CK(lean_sweep(s, dm, F.div, chain, outs[wi], M.dm, add ? M.p[mid] : nullptr));
+        FX_CK(lean_sweep_variant(s, st.sweep_variant[0], dm, F.div, chain, outs[wi], M.dm, add ? M.p[mid] : nullptr));
         chain = outs[wi++];
         ++launches;
       }
@@ -1285,7 +1286,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       }
       for (int k = 1; k <= n; ++k) {
         Timed tm(w, s, "fused_sweep");
-        FX_CK(lean_sweep(s, dm, F.div, chain, outs[wi], M.dm, nullptr));
+        FX_CK(lean_sweep_variant(s, st.sweep_variant[0], dm, F.div, chain, outs[wi], M.dm, nullptr));
         chain = outs[wi++];
         ++launches;
       }

@@ -93,6 +93,7 @@ struct FusedStep {
   LevelBuf lv[3];
   LevelBuf xlv[3];  // V-cycle levels 3..5
   int q[7];
+  int sweep_variant[3];  // sweep kernel of the fine, mid and coarse level (-1 = default)
   int solver_mode;    // 0: the reference schedule, 1: the V-cycle
   VCycleConfig vc;
   bool solver_norms;  // FP64 statistics after the reference schedule too

@@ -801,23 +801,36 @@ cudaError_t lean_div_first(cudaStream_t s, Dims dm, VelField v, float* div, floa
   return cudaGetLastError();
 }
 
-cudaError_t lean_sweep(cudaStream_t s, Dims dm, const float* div, const float* src, float* dst, Dims mid, const float* mid_p) {
+bool sweep_variant_valid(int variant, Dims dm) {
+  if (variant < 0 || variant >= kSweepVariants) return false;
+  return variant < SWEEP_VEC_Z2 || (dm.w % 2 == 0 && dm.w >= 4);
+}
+
+int sweep_variant_default(Dims dm) {
   static const int zb = env_int("FENIX_SWEEP_ZB", 4, 1, 8);
   static const int vec = env_int("FENIX_SWEEP_VEC", 1, 0, 1);
   static const int vzb = env_int("FENIX_SWEEP_VEC_ZB", 2, 2, 4);
-  if (vec && dm.w % 2 == 0 && dm.w >= 4) {
-    if (vzb <= 2) {
-      k_sweep_v2<2><<<dim3((dm.w + 63) / 64, (dm.h + 7) / 8, (dm.d + 1) / 2), dim3(32, 8, 1), 0, s>>>(dm, div, src, dst, mid, mid_p);
-    } else {
-      k_sweep_v2<4><<<dim3((dm.w + 63) / 64, (dm.h + 7) / 8, (dm.d + 3) / 4), dim3(32, 8, 1), 0, s>>>(dm, div, src, dst, mid, mid_p);
-    }
-    return cudaGetLastError();
+  if (vec && sweep_variant_valid(SWEEP_VEC_Z2, dm)) return vzb <= 2 ? SWEEP_VEC_Z2 : SWEEP_VEC_Z4;
+  return zb <= 2 ? SWEEP_Z2 : (zb <= 4 ? SWEEP_Z4 : SWEEP_Z8);
+}
+
+cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float* div, const float* src, float* dst, Dims mid,
+                               const float* mid_p) {
+  if (!sweep_variant_valid(variant, dm)) variant = sweep_variant_default(dm);
+  auto grid = [&](int x_per_block, int z) { return dim3((dm.w + x_per_block - 1) / x_per_block, (dm.h + 7) / 8, (dm.d + z - 1) / z); };
+  const dim3 block(32, 8, 1);
+  switch (variant) {
+    case SWEEP_Z2: k_sweep<2><<<grid(32, 2), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
+    case SWEEP_Z4: k_sweep<4><<<grid(32, 4), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
+    case SWEEP_Z8: k_sweep<8><<<grid(32, 8), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
+    case SWEEP_VEC_Z2: k_sweep_v2<2><<<grid(64, 2), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
+    default: k_sweep_v2<4><<<grid(64, 4), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
   }
-  auto grid = [&](int z) { return dim3((dm.w + 31) / 32, (dm.h + 7) / 8, (dm.d + z - 1) / z); };
-  if (zb <= 2) k_sweep<2><<<grid(2), dim3(32, 8, 1), 0, s>>>(dm, div, src, dst, mid, mid_p);
-  else if (zb <= 4) k_sweep<4><<<grid(4), dim3(32, 8, 1), 0, s>>>(dm, div, src, dst, mid, mid_p);
-  else k_sweep<8><<<grid(8), dim3(32, 8, 1), 0, s>>>(dm, div, src, dst, mid, mid_p);
   return cudaGetLastError();
+}
+
+cudaError_t lean_sweep(cudaStream_t s, Dims dm, const float* div, const float* src, float* dst, Dims mid, const float* mid_p) {
+  return lean_sweep_variant(s, -1, dm, div, src, dst, mid, mid_p);
 }
 
 cudaError_t lean_prolong_zero(cudaStream_t s, Dims dm, float* dst, Dims mid, const float* mid_p) {

@@ -46,6 +46,15 @@ int zpass_zchunk();
 // Lean per-voxel kernels of the default pressure plan.
 cudaError_t lean_div_first(cudaStream_t s, Dims dm, VelField v, float* div, float* p1, Dims mid, float* mid_div, bool restrict_mid);
 cudaError_t lean_sweep(cudaStream_t s, Dims dm, const float* div, const float* src, float* dst, Dims mid, const float* mid_p);
+
+// Sweep kernel variants (all give the same bits): one x per thread with z-depth
+// 2, 4 or 8, or two x per thread (even widths) with z-depth 2 or 4. An invalid
+// variant (-1, or a two-x variant on an odd width) takes the default.
+enum SweepVariant { SWEEP_Z2 = 0, SWEEP_Z4 = 1, SWEEP_Z8 = 2, SWEEP_VEC_Z2 = 3, SWEEP_VEC_Z4 = 4, kSweepVariants = 5 };
+bool sweep_variant_valid(int variant, Dims dm);
+int sweep_variant_default(Dims dm);
+cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float* div, const float* src, float* dst, Dims mid,
+                               const float* mid_p);
 cudaError_t lean_prolong_zero(cudaStream_t s, Dims dm, float* dst, Dims mid, const float* mid_p);
 
 // The mid/coarse part of the solve in one cooperative launch. `bar` is 96

@@ -97,6 +97,7 @@ struct fx_sim {
   bool half = false;  // FX_OPT_SCALARS_F16: the scalar sets are binary16 buffers
   fx_solver_settings solver{};
   uint32_t last_cycle_launches = 0;  // kernels per V-cycle in the latest step
+  int sweep_variant[3] = {-1, -1, -1};  // sweep kernel per pressure level, chosen by fx_sim_autotune
   int last_solver_mode = 0;
 
   // device memory
@@ -452,6 +453,7 @@ fx_status step_begin(fx_sim* s, double elapsed, double step_s, StepPlan& sp) {
   for (int l = 0; l < 3; ++l) fs.lv[l] = s->lv[l];
   for (int l = 0; l < 3; ++l) fs.xlv[l] = s->xlv[l];
   for (int k = 0; k < 7; ++k) fs.q[k] = s->qi[k];
+  for (int l = 0; l < 3; ++l) fs.sweep_variant[l] = s->sweep_variant[l];
   fs.solver_mode = s->solver.mode;
   fs.vc.levels = s->solver.levels;
   fs.vc.pre = s->solver.pre_sweeps;
@@ -1064,6 +1066,58 @@ fx_status fx_sim_set_solver(fx_sim* s, const fx_solver_settings* v) {
 fx_status fx_sim_get_solver(fx_sim* s, fx_solver_settings* o) {
   if (!s || !o) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_solver: NULL argument");
   *o = s->solver;
+  return FX_OK;
+}
+
+fx_status fx_sim_autotune(fx_sim* s, fx_autotune_report* o) {
+  if (!s || !o) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_autotune: NULL argument");
+  if (s->kernels != FX_KERNELS_FUSED) return fail(s, FX_ERR_UNSUPPORTED, "fx_sim_autotune: the plain kernels have nothing to tune");
+  std::memset(o, 0, sizeof *o);
+  FX_CUDA(s, cudaSetDevice(s->device));
+  FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  FX_CUDA(s, cudaEventCreate(&ev[0]));
+  if (cudaEventCreate(&ev[1]) != cudaSuccess) {
+    cudaEventDestroy(ev[0]);
+    return fail(s, FX_ERR_CUDA, "fx_sim_autotune: cudaEventCreate failed");
+  }
+  fx_status st = FX_OK;
+  for (int l = 0; l < 3 && st == FX_OK; ++l) {
+    // Sweeps from the level's current iterate into the buffer that is dead
+    // between steps (the non-current fine pressure; the mid and coarse buffers
+    // restart from zero every solve).
+    const LevelBuf& L = s->lv[l];
+    const float* src = l == 0 ? L.p[s->last_p] : L.p[0];
+    float* dst = l == 0 ? L.p[s->last_p ^ 1] : L.p[1];
+    const int dflt = sweep_variant_default(L.dm);
+    int best = dflt;
+    float best_us = 0.0f;
+    for (int v = 0; v < kSweepVariants && st == FX_OK; ++v) {
+      if (!sweep_variant_valid(v, L.dm)) continue;
+      float ms = 0.0f;
+      for (int k = 0; k < 3; ++k) lean_sweep_variant(s->stream, v, L.dm, L.div, src, dst, L.dm, nullptr);
+      cudaEventRecord(ev[0], s->stream);
+      for (int k = 0; k < 20; ++k) lean_sweep_variant(s->stream, v, L.dm, L.div, src, dst, L.dm, nullptr);
+      cudaEventRecord(ev[1], s->stream);
+      if (cudaEventSynchronize(ev[1]) != cudaSuccess || cudaEventElapsedTime(&ms, ev[0], ev[1]) != cudaSuccess) {
+        st = fail(s, FX_ERR_CUDA, "fx_sim_autotune: timing failed");
+        break;
+      }
+      const float us = ms * 1000.0f / 20.0f;
+      if (v == dflt) o->default_us[l] = us;
+      if (best_us == 0.0f || us < best_us) {
+        best_us = us;
+        best = v;
+      }
+    }
+    s->sweep_variant[l] = best;
+    o->sweep_variant[l] = best;
+    o->sweep_us[l] = best_us;
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (st != FX_OK) return st;
+  FX_CUDA(s, cudaGetLastError());
   return FX_OK;
 }
 

@@ -292,6 +292,13 @@ class CombustionVolumeSimulation:
         check(self._lib.fx_sim_get_solver(self._h, ctypes.byref(st)), self._h)
         return solver_dict(st)
 
+    def autotune(self) -> Dict[str, Any]:
+        """Times the pressure sweep kernels on this grid's levels and keeps the
+        fastest per level (same results; waits for the stream)."""
+        r = _lib.FxAutotuneReport()
+        check(self._lib.fx_sim_autotune(self._h, ctypes.byref(r)), self._h)
+        return {"sweepVariant": list(r.sweep_variant), "sweepUs": list(r.sweep_us), "defaultUs": list(r.default_us)}
+
     def readSolverStats(self) -> Dict[str, Any]:
         """FP64 statistics of the latest solve (waits for the stream)."""
         st = _lib.FxSolverStats()

@@ -337,6 +337,20 @@ typedef struct fx_solver_stats {
 
 fx_status fx_sim_read_solver_stats(fx_sim* sim, fx_solver_stats* out);
 
+/* Autotuning (extension): times every sweep kernel variant of the pressure
+ * solve on each level (fine, mid, coarse) of this simulation's grid and keeps
+ * the fastest for its later steps. All variants give the same bits. Waits for
+ * the stream; overwrites the pressure buffers that are not current (the
+ * non-current fine buffer and the mid/coarse levels, which every solve
+ * rewrites from zero). */
+typedef struct fx_autotune_report {
+  int32_t sweep_variant[3]; /* chosen variant per level (0..4) */
+  float sweep_us[3];        /* its time per sweep */
+  float default_us[3];      /* the default variant's time per sweep */
+} fx_autotune_report;
+
+fx_status fx_sim_autotune(fx_sim* sim, fx_autotune_report* out);
+
 /* Batches (extension; the reference steps one simulation per device): many
  * independent simulations, each with its own options (sizes may differ), stepped
  * together. Every fx_batch_step is one CUDA graph in which each simulation's

@@ -1,0 +1,44 @@
+"""fx_sim_autotune: the sweep variant per pressure level, timed on the grid.
+
+Every variant gives the same bits, so a tuned simulation must still equal the
+oracle; the vector variants need an even width."""
+import pytest
+
+from fenix_b200 import createCombustionVolumeSimulation, workloads
+from oracle.oracle import OracleSimulation
+
+from parity_util import EXPOSED_FIELDS, all_kind_sources, compare
+
+pytestmark = pytest.mark.gpu
+
+VECTOR_VARIANTS = (3, 4)
+
+
+@pytest.mark.parametrize("opts,sources", [
+    ({"resolution": (37, 45, 29), "worldSize": 1.7}, "all"),   # odd width: no vector variant on the fine level
+    ("plume64", None),
+])
+def test_autotuned_steps_equal_the_oracle(opts, sources):
+    if opts == "plume64":
+        wl = workloads.plume_64()
+        opts, srcs = wl.options, wl.sources
+    else:
+        srcs = all_kind_sources(seed=23.0)
+    sim = createCombustionVolumeSimulation(opts, device=0)
+    orc = OracleSimulation(opts, precision=32)
+    for s in (sim, orc):
+        s.updateSources(srcs)
+    for k in range(3):
+        sim.step(k / 60, 1 / 60)
+        orc.step(k / 60, 1 / 60)
+    rep = sim.autotune()
+    assert all(0 <= v <= 4 for v in rep["sweepVariant"]) and all(t > 0 for t in rep["sweepUs"])
+    assert all(rep["sweepUs"][l] <= rep["defaultUs"][l] * 1.0001 for l in range(3))
+    if opts["resolution"][0] % 2:
+        assert rep["sweepVariant"][0] not in VECTOR_VARIANTS
+    # the tuning left the state alone, and the tuned steps give the same bits
+    compare(sim, orc, EXPOSED_FIELDS, "after autotune")
+    for k in range(3, 9):
+        sim.step(k / 60, 1 / 60)
+        orc.step(k / 60, 1 / 60)
+        compare(sim, orc, EXPOSED_FIELDS, f"tuned step {k + 1}")
