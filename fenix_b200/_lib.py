@@ -149,6 +149,7 @@ FX_DISPLAY_DENSITY = 1
 FX_DISPLAY_FUEL = 2
 FX_PIXELS_RGBA16F = 0
 FX_PIXELS_RGBA32F = 1
+FX_PIXELS_RGBA8 = 2
 
 
 class FxCamera(Structure):
@@ -168,6 +169,10 @@ class FxRaymarchParams(Structure):
 
 class FxAutotuneReport(Structure):
     _fields_ = [("sweep_variant", c_int32 * 3), ("sweep_us", c_float * 3), ("default_us", c_float * 3)]
+
+
+class FxBloomParams(Structure):
+    _fields_ = [("enabled", c_int32), ("reserved", c_int32), ("threshold", c_double), ("strength", c_double), ("radius", c_double)]
 
 
 class FxStats(Structure):
@@ -255,6 +260,9 @@ PROTOTYPES = [
     ("fx_raymarch_destroy", None, [c_void_p]),
     ("fx_raymarch_set_params", c_int32, [c_void_p, POINTER(FxRaymarchParams)]),
     ("fx_raymarch_render", c_int32, [c_void_p, c_void_p, POINTER(FxCamera), c_int32, c_uint32, c_uint32, c_double, c_void_p, c_int32]),
+    ("fx_bloom_create", c_int32, [POINTER(c_void_p)]),
+    ("fx_bloom_destroy", None, [c_void_p]),
+    ("fx_bloom_render", c_int32, [c_void_p, c_void_p, c_int32, c_uint32, c_uint32, POINTER(FxBloomParams), c_void_p, c_int32, c_void_p]),
     ("fx_brick_flags_noalloc", c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_void_p, c_void_p]),
 ]
 

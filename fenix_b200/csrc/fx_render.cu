@@ -420,6 +420,113 @@ __global__ void __launch_bounds__(128) k_raymarch(Uniform U, Fields<S> F, uint32
   }
 }
 
+// ---------------------------------------------------------------------- bloom
+// createBloomPass.ts: soft threshold into a half-resolution texture, a 9-tap
+// gaussian blur along x then y, and the composite with pow(., 0.92) into the
+// canvas (:224-297). Textures are RGBA16F (values rounded to nearest); a
+// textureSample with the linear sampler is bilinear with exact f32 weights and
+// clamp-to-edge addressing; the fragment uv at pixel (x, y) of a W x H target
+// is ((x + 0.5) / W, (y + 0.5) / H).
+struct Px4 {
+  float v[4];
+};
+
+template <typename T>
+FX_DEV float texel(const T* t, uint32_t i) {
+  if constexpr (sizeof(T) == 2) return __half2float(t[i]);
+  else return t[i];
+}
+
+template <typename T>
+FX_DEV Px4 sample_bilinear(const T* tex, uint32_t tw, uint32_t th, float u, float v) {
+  const float x = u * (float)tw - 0.5f, y = v * (float)th - 0.5f;
+  const float x0 = floorf(x), y0 = floorf(y);
+  const float fx = x - x0, fy = y - y0;
+  const int ix = (int)x0, iy = (int)y0;
+  const uint32_t xa = (uint32_t)min(max(ix, 0), (int)tw - 1), xb = (uint32_t)min(max(ix + 1, 0), (int)tw - 1);
+  const uint32_t ya = (uint32_t)min(max(iy, 0), (int)th - 1), yb = (uint32_t)min(max(iy + 1, 0), (int)th - 1);
+  Px4 o;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const float t00 = texel(tex, (ya * tw + xa) * 4 + c), t10 = texel(tex, (ya * tw + xb) * 4 + c);
+    const float t01 = texel(tex, (yb * tw + xa) * 4 + c), t11 = texel(tex, (yb * tw + xb) * 4 + c);
+    o.v[c] = mixv(mixv(t00, t10, fx), mixv(t01, t11, fx), fy);
+  }
+  return o;
+}
+
+struct BloomU {
+  float threshold, strength, radius;
+  float texel_hx, texel_hy;  // 1 / half width, 1 / half height (paramsData[4..5])
+};
+
+template <typename T>
+__global__ void k_bloom_threshold(const T* __restrict__ src, uint32_t w, uint32_t h, uint32_t hw, uint32_t hh, BloomU U, __half* __restrict__ out) {
+  const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= hw || py >= hh) return;
+  const float u = ((float)px + 0.5f) / (float)hw, v = ((float)py + 0.5f) / (float)hh;
+  const Px4 c = sample_bilinear(src, w, h, u, v);
+  const float lum = c.v[0] * 0.2126f + c.v[1] * 0.7152f + c.v[2] * 0.0722f;
+  const float knee = U.threshold * 0.5f;
+  const float rq = clampv(lum - U.threshold + knee, 0.0f, 2.0f * knee);
+  const float wgt = (rq * rq) / (4.0f * knee * knee + 0.00001f);
+  const float mask = mx(wgt, stepv(U.threshold, lum));
+  const size_t o = ((size_t)py * hw + px) * 4;
+  out[o + 0] = __float2half_rn(c.v[0] * mask * c.v[3]);
+  out[o + 1] = __float2half_rn(c.v[1] * mask * c.v[3]);
+  out[o + 2] = __float2half_rn(c.v[2] * mask * c.v[3]);
+  out[o + 3] = __float2half_rn(c.v[3] * mask);
+}
+
+__global__ void k_bloom_blur(const __half* __restrict__ src, uint32_t hw, uint32_t hh, float sx, float sy, __half* __restrict__ out) {
+  const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= hw || py >= hh) return;
+  const float u = ((float)px + 0.5f) / (float)hw, v = ((float)py + 0.5f) / (float)hh;
+  const float wts[5] = {0.2270270270f, 0.1945945946f, 0.1216216216f, 0.0540540541f, 0.0162162162f};
+  Px4 col = sample_bilinear(src, hw, hh, u, v);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) col.v[c] = col.v[c] * wts[0];
+#pragma unroll
+  for (int k = 1; k <= 4; ++k) {
+    const float ox = sx * (float)k, oy = sy * (float)k;
+    const Px4 a = sample_bilinear(src, hw, hh, u + ox, v + oy);
+    const Px4 b = sample_bilinear(src, hw, hh, u - ox, v - oy);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) col.v[c] = col.v[c] + a.v[c] * wts[k];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) col.v[c] = col.v[c] + b.v[c] * wts[k];
+  }
+  const size_t o = ((size_t)py * hw + px) * 4;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) out[o + c] = __float2half_rn(col.v[c]);
+}
+
+FX_DEV uint8_t unorm8(float x) { return (uint8_t)rintf(clampv(x, 0.0f, 1.0f) * 255.0f); }
+
+template <typename T, typename P>
+__global__ void k_bloom_composite(const T* __restrict__ src, uint32_t w, uint32_t h, const __half* __restrict__ glow_tex, uint32_t hw,
+                                  uint32_t hh, BloomU U, int enabled, P* __restrict__ out) {
+  const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y * blockDim.y + threadIdx.y;
+  if (px >= w || py >= h) return;
+  const float u = ((float)px + 0.5f) / (float)w, v = ((float)py + 0.5f) / (float)h;
+  const Px4 base = sample_bilinear(src, w, h, u, v);
+  float r[4];
+  if (enabled) {
+    const Px4 glow = sample_bilinear(glow_tex, hw, hh, u, v);
+    for (int c = 0; c < 3; ++c) r[c] = ppow(mx(base.v[c] + mx(glow.v[c], 0.0f) * U.strength, 0.0f), 0.92f);
+    const float glow_alpha = clampv(glow.v[3] * U.strength, 0.0f, 1.0f);
+    r[3] = clampv(base.v[3] + glow_alpha * (1.0f - base.v[3]), 0.0f, 1.0f);
+  } else {  // the blit shader (:284-296)
+    for (int c = 0; c < 3; ++c) r[c] = ppow(mx(base.v[c], 0.0f), 0.92f);
+    r[3] = clampv(base.v[3], 0.0f, 1.0f);
+  }
+  const size_t o = ((size_t)py * w + px) * 4;
+  for (int c = 0; c < 4; ++c) {
+    if constexpr (sizeof(P) == 1) out[o + c] = unorm8(r[c]);
+    else out[o + c] = r[c];
+  }
+}
+
 __global__ void k_exp_pow(const float* x, const float* y, float* oe, float* op, uint32_t n) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -450,6 +557,12 @@ void sanitize_light(const fx_render_light& in, fx_render_light& out) {
 }  // namespace fx
 
 using namespace fx;
+
+struct fx_bloom {
+  int device = 0;
+  uint32_t hw = 0, hh = 0;
+  __half* tex[3] = {nullptr, nullptr, nullptr};  // bright, blur x, blur y (half resolution)
+};
 
 struct fx_raymarch {
   uint32_t w, h, d;
@@ -602,6 +715,77 @@ fx_status fx_raymarch_render(fx_raymarch* r, fx_sim* sim, const fx_camera* cam, 
   else launch(float{});
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return rm_fail(FX_ERR_CUDA, std::string("fx_raymarch_render: launch failed: ") + cudaGetErrorString(e));
+  return FX_OK;
+}
+
+fx_status fx_bloom_create(fx_bloom** out) {
+  if (!out) return rm_fail(FX_ERR_INVALID_ARGUMENT, "fx_bloom_create: out is NULL");
+  *out = new (std::nothrow) fx_bloom;
+  if (!*out) return rm_fail(FX_ERR_OUT_OF_MEMORY, "fx_bloom_create: host allocation failed");
+  if (cudaGetDevice(&(*out)->device) != cudaSuccess) (*out)->device = 0;
+  return FX_OK;
+}
+
+void fx_bloom_destroy(fx_bloom* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  for (auto& t : b->tex)
+    if (t) cudaFree(t);
+  delete b;
+}
+
+fx_status fx_bloom_render(fx_bloom* b, const void* hdr, int32_t hdr_format, uint32_t width, uint32_t height, const fx_bloom_params* p,
+                          void* out, int32_t out_format, void* stream) {
+  if (!b || !hdr || !p || !out) return rm_fail(FX_ERR_INVALID_ARGUMENT, "fx_bloom_render: NULL argument");
+  if (width == 0 || height == 0 || (uint64_t)width * height > (1ull << 28))
+    return rm_fail(FX_ERR_INVALID_ARGUMENT, "fx_bloom_render: image size out of range");
+  if ((hdr_format != FX_PIXELS_RGBA16F && hdr_format != FX_PIXELS_RGBA32F) || (out_format != FX_PIXELS_RGBA8 && out_format != FX_PIXELS_RGBA32F))
+    return rm_fail(FX_ERR_INVALID_ARGUMENT, "fx_bloom_render: unknown pixel format");
+  if (cudaSetDevice(b->device) != cudaSuccess) return rm_fail(FX_ERR_CUDA, "fx_bloom_render: cudaSetDevice failed");
+  // rebuildTextures (:84-94): half resolution, at least 1 x 1
+  const uint32_t hw = std::max(1u, width / 2), hh = std::max(1u, height / 2);
+  if (hw != b->hw || hh != b->hh) {
+    b->hw = b->hh = 0;  // a failed allocation leaves no size that matches
+    for (auto& t : b->tex) {
+      if (t) cudaFree(t);
+      t = nullptr;
+    }
+    for (auto& t : b->tex)
+      if (cudaMalloc(&t, (size_t)hw * hh * 4 * sizeof(__half)) != cudaSuccess)
+        return rm_fail(FX_ERR_OUT_OF_MEMORY, "fx_bloom_render: texture allocation failed");
+    b->hw = hw;
+    b->hh = hh;
+  }
+  // paramsData (:103-111), as f32
+  BloomU U;
+  U.threshold = (float)p->threshold;
+  U.strength = (float)p->strength;
+  U.radius = (float)p->radius;
+  U.texel_hx = (float)(1.0 / hw);
+  U.texel_hy = (float)(1.0 / hh);
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const dim3 block(16, 16, 1), half_grid((hw + 15) / 16, (hh + 15) / 16, 1), full_grid((width + 15) / 16, (height + 15) / 16, 1);
+  // blur step: texel * (1 + radius * 2) along one axis (:247)
+  const float spread = 1.0f + U.radius * 2.0f;
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    const T* src = static_cast<const T*>(hdr);
+    if (p->enabled) {
+      k_bloom_threshold<T><<<half_grid, block, 0, s>>>(src, width, height, hw, hh, U, b->tex[0]);
+      k_bloom_blur<<<half_grid, block, 0, s>>>(b->tex[0], hw, hh, U.texel_hx * spread, 0.0f * spread, b->tex[1]);
+      k_bloom_blur<<<half_grid, block, 0, s>>>(b->tex[1], hw, hh, 0.0f * spread, U.texel_hy * spread, b->tex[2]);
+    }
+    if (out_format == FX_PIXELS_RGBA8)
+      k_bloom_composite<T, uint8_t><<<full_grid, block, 0, s>>>(src, width, height, b->tex[2], hw, hh, U, p->enabled ? 1 : 0,
+                                                                 static_cast<uint8_t*>(out));
+    else
+      k_bloom_composite<T, float><<<full_grid, block, 0, s>>>(src, width, height, b->tex[2], hw, hh, U, p->enabled ? 1 : 0,
+                                                               static_cast<float*>(out));
+  };
+  if (hdr_format == FX_PIXELS_RGBA16F) run(__half{});
+  else run(float{});
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return rm_fail(FX_ERR_CUDA, std::string("fx_bloom_render: launch failed: ") + cudaGetErrorString(e));
   return FX_OK;
 }
 

@@ -4,11 +4,13 @@ flipbook spritesheet.
 The reference's exporter (src/ui/components/toolbar/ExportPopover.tsx:369-373,
 425-433) resets the simulation and, for frame i, steps it at
 t = (startFrame + i) / fps with dt = 1 / fps and renders the frame
-(createViewportRuntime.ts:205-232), then draws the canvas over the background
-colour into an MP4 or a spritesheet. Here a frame is the raymarch's
-premultiplied RGBA composited over the background (the reference's bloom and
-overlay passes are not part of this library), clamped, and written as 8-bit
-PNG; the spritesheet lays frames out row by row in `columns` columns.
+(createViewportRuntime.ts:205-232: raymarch into the HDR texture, bloom into
+the premultiplied 8-bit canvas), then draws the canvas over the background
+colour into an MP4 or a spritesheet. Here a frame is that canvas from the CUDA
+raymarch and bloom passes (the overlay pass, gizmos and grid, is not part of
+this library) composited over the background and written as 8-bit PNG; with
+`bloom=None` the raymarch's image is composited directly. The spritesheet lays
+frames out row by row in `columns` columns.
 """
 from __future__ import annotations
 
@@ -18,6 +20,8 @@ import zlib
 from typing import Any, Dict, List, Mapping, Optional, Sequence
 
 import numpy as np
+
+from .render import BLOOM_DEFAULTS
 
 
 def write_png(path: str, rgb: np.ndarray) -> None:
@@ -74,6 +78,16 @@ def composite(rgba: np.ndarray, background: Optional[str]) -> np.ndarray:
     return np.rint(out * 255.0).astype(np.uint8)
 
 
+def composite_canvas(canvas: np.ndarray, background: Optional[str]) -> np.ndarray:
+    """A premultiplied RGBA8 canvas drawn over a background colour (None keeps
+    the canvas), as uint8."""
+    c = np.asarray(canvas, dtype=np.float32) / 255.0
+    if background is None:
+        return np.asarray(canvas, dtype=np.uint8).copy()
+    out = np.clip(c[..., :3] + hex_color(background) * (1.0 - c[..., 3:4]), 0.0, 1.0)
+    return np.rint(out * 255.0).astype(np.uint8)
+
+
 def spritesheet(frames: Sequence[np.ndarray], columns: int, background: Optional[str] = None) -> np.ndarray:
     """Frames (equal H x W x C uint8) laid out row by row in `columns` columns."""
     if not frames:
@@ -92,10 +106,13 @@ def spritesheet(frames: Sequence[np.ndarray], columns: int, background: Optional
 def export_frames(sim, raymarch, camera: Mapping[str, Any], out_dir: str, *, start_frame: int = 0, end_frame: int = 59,
                   fps: float = 30.0, width: int = 512, height: int = 512, display_mode: str = "temperature",
                   background: Optional[str] = "#0b0d12", columns: int = 8, reset: bool = True,
-                  prefix: str = "frame") -> Dict[str, Any]:
+                  prefix: str = "frame", bloom: Optional[Mapping[str, Any]] = BLOOM_DEFAULTS) -> Dict[str, Any]:
     """Steps `sim` at fixed dt = 1/fps from a reset and writes each frame as
-    `<prefix>_NNNN.png` plus `flipbook.png`; returns the file names."""
+    `<prefix>_NNNN.png` plus `flipbook.png`; returns the file names. `bloom`
+    holds the BloomParams of the frame's bloom pass (None skips the pass)."""
     import torch
+
+    from .render import createBloomPass
 
     os.makedirs(out_dir, exist_ok=True)
     if reset:
@@ -103,18 +120,27 @@ def export_frames(sim, raymarch, camera: Mapping[str, Any], out_dir: str, *, sta
     dt = 1.0 / fps
     dev = torch.device("cuda", torch.cuda.current_device())
     buf = torch.empty((height, width, 4), dtype=torch.float16, device=dev)
+    bloom_pass = createBloomPass() if bloom is not None else None
+    canvas = torch.empty((height, width, 4), dtype=torch.uint8, device=dev) if bloom_pass else None
     frames: List[np.ndarray] = []
     names: List[str] = []
     for i in range(end_frame - start_frame + 1):
         t = (start_frame + i) * dt
         sim.step(t, dt)
         raymarch.render(sim, camera, display_mode, width, height, t, out=buf)
+        if bloom_pass:
+            bloom_pass.render(buf, bloom, out=canvas, stream=sim.stream)
         sim.synchronize()
-        img = composite(buf.float().cpu().numpy(), background)
+        if bloom_pass:
+            img = composite_canvas(canvas.cpu().numpy(), background)
+        else:
+            img = composite(buf.float().cpu().numpy(), background)
         name = os.path.join(out_dir, f"{prefix}_{start_frame + i:04d}.png")
         write_png(name, img)
         frames.append(img)
         names.append(name)
+    if bloom_pass:
+        bloom_pass.dispose()
     sheet = os.path.join(out_dir, "flipbook.png")
     write_png(sheet, spritesheet(frames, columns, background))
     return {"frames": names, "flipbook": sheet, "dt": dt}

@@ -133,3 +133,53 @@ class VolumeRaymarchPass:
 
 def createVolumeRaymarchPass(resolution: Sequence[int]) -> VolumeRaymarchPass:
     return VolumeRaymarchPass(resolution)
+
+
+BLOOM_DEFAULTS = {"enabled": True, "threshold": 0.6, "strength": 0.9, "radius": 0.4}  # createViewportRuntime.ts:43
+
+
+class BloomPass:
+    """createBloomPass (createBloomPass.ts): HDR image -> canvas image."""
+
+    def __init__(self):
+        self._lib = _lib.load()
+        h = ctypes.c_void_p()
+        check(self._lib.fx_bloom_create(ctypes.byref(h)))
+        self._h = h
+
+    def render(self, hdr, params: Optional[Mapping[str, Any]] = None, out=None, out_format: str = "rgba8", stream: int = 0):
+        """hdr: a CUDA tensor (H x W x 4, float16 or float32); returns `out`
+        (uint8 or float32 H x W x 4), allocated when None. Runs on `stream`
+        (a cudaStream_t; 0 is the legacy default stream), which must be ordered
+        after the writer of `hdr`: pass the simulation's stream for an image
+        its raymarch just rendered."""
+        import torch
+
+        p = dict(BLOOM_DEFAULTS)
+        p.update(params or {})
+        st = _lib.FxBloomParams()
+        st.enabled = 1 if p["enabled"] else 0
+        st.threshold, st.strength, st.radius = float(p["threshold"]), float(p["strength"]), float(p["radius"])
+        h, w = int(hdr.shape[0]), int(hdr.shape[1])
+        in_fmt = _lib.FX_PIXELS_RGBA16F if hdr.dtype == torch.float16 else _lib.FX_PIXELS_RGBA32F
+        out_fmt = _lib.FX_PIXELS_RGBA8 if out_format == "rgba8" else _lib.FX_PIXELS_RGBA32F
+        if out is None:
+            out = torch.empty((h, w, 4), dtype=torch.uint8 if out_fmt == _lib.FX_PIXELS_RGBA8 else torch.float32, device=hdr.device)
+        check(self._lib.fx_bloom_render(self._h, ctypes.c_void_p(hdr.data_ptr()), in_fmt, w, h, ctypes.byref(st), ctypes.c_void_p(out.data_ptr()),
+                                        out_fmt, ctypes.c_void_p(stream or 0)))
+        return out
+
+    def dispose(self) -> None:
+        if self._h:
+            self._lib.fx_bloom_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.dispose()
+        except Exception:
+            pass
+
+
+def createBloomPass() -> BloomPass:
+    return BloomPass()

@@ -425,6 +425,7 @@ typedef struct fx_raymarch_params {
 
 #define FX_PIXELS_RGBA16F 0 /* 4 x IEEE binary16 per pixel */
 #define FX_PIXELS_RGBA32F 1 /* 4 x float per pixel */
+#define FX_PIXELS_RGBA8 2   /* 4 x unorm8 per pixel (the canvas): round(clamp(x, 0, 1) * 255) */
 
 typedef struct fx_raymarch fx_raymarch;
 
@@ -441,6 +442,30 @@ fx_status fx_raymarch_set_params(fx_raymarch* pass, const fx_raymarch_params* pa
  * must have the pass's resolution. */
 fx_status fx_raymarch_render(fx_raymarch* pass, fx_sim* sim, const fx_camera* camera, int32_t display_mode, uint32_t render_width,
                              uint32_t render_height, double elapsed_seconds, void* pixels, int32_t pixel_format);
+
+/* Bloom: the reference's BloomPass (src/engine/render/passes/createBloomPass.ts),
+ * from the raymarch's HDR image (RGBA16F, or RGBA32F) to the canvas image: a
+ * soft threshold into a half-resolution RGBA16F texture, a 9-tap gaussian blur
+ * along x then y, and the composite with pow(., 0.92) (or the blit when
+ * disabled). textureSample is bilinear with exact f32 weights and clamp-to-edge
+ * addressing. The pass owns its half-resolution textures (allocated on the
+ * first render of a size). */
+typedef struct fx_bloom_params { /* BloomParams (createBloomPass.ts:1-6) */
+  int32_t enabled;
+  int32_t reserved;
+  double threshold;
+  double strength;
+  double radius;
+} fx_bloom_params;
+
+typedef struct fx_bloom fx_bloom;
+fx_status fx_bloom_create(fx_bloom** out);  /* createBloomPass(device, canvasFormat), on the current device */
+void fx_bloom_destroy(fx_bloom* pass);
+/* render(encoder, sourceView, targetView, width, height, params) (:96-130):
+ * `hdr` and `out` are device buffers of width * height pixels (row 0 at the
+ * top); out_format FX_PIXELS_RGBA8 or FX_PIXELS_RGBA32F; stream: cudaStream_t. */
+fx_status fx_bloom_render(fx_bloom* pass, const void* hdr, int32_t hdr_format, uint32_t width, uint32_t height,
+                          const fx_bloom_params* params, void* out, int32_t out_format, void* stream);
 
 /* Brick flags of caller-owned fields, allocating nothing. No counterpart in the
  * reference. It computes what compute-active-bricks.wgsl.ts:35-58 computes, for

@@ -46,6 +46,8 @@ def load() -> ctypes.CDLL:
                                                              c_uint32, c_uint32, c_double, POINTER(c_double), c_int, POINTER(c_double),
                                                              POINTER(c_float)]
         lib.orc_pinned_exp_pow.argtypes = [POINTER(c_float), POINTER(c_float), POINTER(c_float), POINTER(c_float), c_long]
+        lib.orc_bloom.argtypes = [POINTER(c_float), c_uint32, c_uint32, c_int, c_double, c_double, c_double, POINTER(c_float),
+                                  POINTER(ctypes.c_uint8)]
         lib.orc_set_solver.argtypes = [c_void_p, POINTER(c_int), POINTER(c_double), c_int]
         lib.orc_get_solver_stats.argtypes = [c_void_p, POINTER(c_double), POINTER(c_int)]
         lib.orc_update_sources.argtypes = [c_void_p, POINTER(c_float), c_uint32]
@@ -299,3 +301,20 @@ def pinned_exp_pow(x: np.ndarray, y: np.ndarray):
     op = np.empty_like(x)
     lib.orc_pinned_exp_pow(_fptr(x), _fptr(y), _fptr(oe), _fptr(op), x.size)
     return oe, op
+
+
+def bloom(hdr: np.ndarray, params: Optional[Mapping[str, Any]] = None):
+    """The bloom pass over an H x W x 4 HDR image (float16 or float32): returns
+    (RGBA f32, RGBA uint8), both H x W x 4."""
+    from fenix_b200.render import BLOOM_DEFAULTS
+
+    p = dict(BLOOM_DEFAULTS)
+    p.update(params or {})
+    lib = load()
+    src = np.ascontiguousarray(np.asarray(hdr).astype(np.float32))
+    h, w = src.shape[:2]
+    out = np.empty((h, w, 4), dtype=np.float32)
+    out8 = np.empty((h, w, 4), dtype=np.uint8)
+    lib.orc_bloom(_fptr(src), w, h, 1 if p["enabled"] else 0, float(p["threshold"]), float(p["strength"]), float(p["radius"]), _fptr(out),
+                  out8.ctypes.data_as(POINTER(ctypes.c_uint8)))
+    return out, out8

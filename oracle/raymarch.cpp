@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <vector>
 
 namespace {
 
@@ -419,6 +420,100 @@ void orc_raymarch(const float* density, const float* temperature, const float* f
       float o[4] = {0.0f, 0.0f, 0.0f, 0.0f};
       s.fragment(u, v, o);
       std::memcpy(rgba + ((size_t)py * width + px) * 4, o, sizeof o);
+    }
+}
+
+// Bloom: createBloomPass.ts (:216-297) with render() (:93-130). `hdr` holds
+// width x height RGBA f32 pixels (an RGBA16F source converted exactly), row 0 at
+// the top; the three half-resolution textures are RGBA16F (each value rounded to
+// nearest f16 on store). The fragment uv at pixel (x, y) of a W x H target is
+// ((x + 0.5) / W, (y + 0.5) / H); textureSample with the linear sampler is
+// bilinear with exact f32 weights, clamp-to-edge. Writes out_f32 (RGBA f32) and,
+// when non-NULL, out_u8 (round(clamp(x, 0, 1) * 255), half to even).
+void orc_bloom(const float* hdr, uint32_t width, uint32_t height, int enabled, double threshold, double strength, double radius,
+               float* out_f32, uint8_t* out_u8) {
+  struct Tex {
+    const float* px;
+    uint32_t w, h;
+    float at(int x, int y, int c) const {
+      x = std::min(std::max(x, 0), (int)w - 1);
+      y = std::min(std::max(y, 0), (int)h - 1);
+      return px[((size_t)y * w + x) * 4 + c];
+    }
+    void sample(float u, float v, float o[4]) const {
+      const float fx = u * (float)w - 0.5f, fy = v * (float)h - 0.5f;
+      const float bx = std::floor(fx), by = std::floor(fy);
+      const float tx = fx - bx, ty = fy - by;
+      const int x = (int)bx, y = (int)by;
+      for (int c = 0; c < 4; ++c) {
+        const float top = fmix(at(x, y, c), at(x + 1, y, c), tx);
+        const float bottom = fmix(at(x, y + 1, c), at(x + 1, y + 1, c), tx);
+        o[c] = fmix(top, bottom, ty);
+      }
+    }
+  };
+  auto f16 = [](float x) { return (float)(_Float16)x; };
+  const float thr = (float)threshold, str = (float)strength, rad = (float)radius;
+  const uint32_t hw = std::max(1u, width / 2), hh = std::max(1u, height / 2);
+  const Tex src{hdr, width, height};
+  std::vector<float> bright((size_t)hw * hh * 4), blur_h(bright.size()), blur_v(bright.size());
+  if (enabled) {
+    for (uint32_t y = 0; y < hh; ++y)  // threshold (:224-233)
+      for (uint32_t x = 0; x < hw; ++x) {
+        float c[4];
+        src.sample(((float)x + 0.5f) / (float)hw, ((float)y + 0.5f) / (float)hh, c);
+        const float lum = c[0] * 0.2126f + c[1] * 0.7152f + c[2] * 0.0722f;
+        const float knee = thr * 0.5f;
+        const float rq = fclamp(lum - thr + knee, 0.0f, 2.0f * knee);
+        const float wq = (rq * rq) / (4.0f * knee * knee + 0.00001f);
+        const float mask = fmax_(wq, lum >= thr ? 1.0f : 0.0f);
+        float* o = &bright[((size_t)y * hw + x) * 4];
+        for (int k = 0; k < 3; ++k) o[k] = f16(c[k] * mask * c[3]);
+        o[3] = f16(c[3] * mask);
+      }
+    static const float g[5] = {0.2270270270f, 0.1945945946f, 0.1216216216f, 0.0540540541f, 0.0162162162f};
+    const float spread = 1.0f + rad * 2.0f;
+    for (int pass = 0; pass < 2; ++pass) {  // blur along x, then y (:246-263)
+      const Tex in{pass == 0 ? bright.data() : blur_h.data(), hw, hh};
+      std::vector<float>& outv = pass == 0 ? blur_h : blur_v;
+      const float step_x = (pass == 0 ? 1.0f / (float)hw : 0.0f) * spread, step_y = (pass == 0 ? 0.0f : 1.0f / (float)hh) * spread;
+      for (uint32_t y = 0; y < hh; ++y)
+        for (uint32_t x = 0; x < hw; ++x) {
+          const float u = ((float)x + 0.5f) / (float)hw, v = ((float)y + 0.5f) / (float)hh;
+          float acc[4], t[4];
+          in.sample(u, v, t);
+          for (int c = 0; c < 4; ++c) acc[c] = t[c] * g[0];
+          for (int k = 1; k <= 4; ++k)
+            for (int sign = 1; sign >= -1; sign -= 2) {
+              const float du = step_x * (float)k, dv = step_y * (float)k;
+              in.sample(sign > 0 ? u + du : u - du, sign > 0 ? v + dv : v - dv, t);
+              for (int c = 0; c < 4; ++c) acc[c] = acc[c] + t[c] * g[k];
+            }
+          for (int c = 0; c < 4; ++c) outv[((size_t)y * hw + x) * 4 + c] = f16(acc[c]);
+        }
+    }
+  }
+  const Tex glow_tex{blur_v.data(), hw, hh};
+  for (uint32_t y = 0; y < height; ++y)  // composite (:290-297) or blit (:273-277)
+    for (uint32_t x = 0; x < width; ++x) {
+      const float u = ((float)x + 0.5f) / (float)width, v = ((float)y + 0.5f) / (float)height;
+      float base[4], r[4];
+      src.sample(u, v, base);
+      if (enabled) {
+        float glow[4];
+        glow_tex.sample(u, v, glow);
+        for (int c = 0; c < 3; ++c) r[c] = fpow(fmax_(base[c] + fmax_(glow[c], 0.0f) * str, 0.0f), 0.92f);
+        const float ga = fclamp(glow[3] * str, 0.0f, 1.0f);
+        r[3] = fclamp(base[3] + ga * (1.0f - base[3]), 0.0f, 1.0f);
+      } else {
+        for (int c = 0; c < 3; ++c) r[c] = fpow(fmax_(base[c], 0.0f), 0.92f);
+        r[3] = fclamp(base[3], 0.0f, 1.0f);
+      }
+      const size_t o = ((size_t)y * width + x) * 4;
+      for (int c = 0; c < 4; ++c) {
+        if (out_f32) out_f32[o + c] = r[c];
+        if (out_u8) out_u8[o + c] = (uint8_t)std::nearbyint(fclamp(r[c], 0.0f, 1.0f) * 255.0f);
+      }
     }
 }
 
