@@ -412,6 +412,78 @@ def run_batch_c3(args, local, rank, world, pg):
     }
 
 
+def run_adjoint_c4(args, local, pg):
+    """The differentiation configuration: 64 plain FP32 steps at 128^3 with a
+    16 x 16 inflow patch as the control, loss = |density_64 - target|^2, a
+    checkpoint every 8 steps. Times the forward (with checkpoints) and the
+    backward (segment recomputation, tape re-runs and the adjoint kernels) with
+    CUDA events on the simulation's stream, host copies of the control, loss and
+    gradients included; checks the gradient against the committed oracle
+    references of this workload (f32-trajectory tangents, f64 central
+    differences) when present."""
+    import torch
+
+    from fenix_b200 import createCombustionVolumeSimulation, workloads
+    from fenix_b200.adjoint import Rollout, start_from
+
+    aw = workloads.adjoint_c4(size=args.adjoint_size, steps=args.adjoint_steps)
+    dev = torch.device("cuda", local)
+    sim = createCombustionVolumeSimulation(aw.workload.options, device=local, kernels="plain")
+    sim.updateSources(aw.workload.sources)
+    ro = Rollout(sim, steps=aw.steps, checkpoint_interval=aw.checkpoint_interval, patch=aw.patch)
+    ro.setTarget(aw.target)
+    stream = torch.cuda.ExternalStream(sim.stream, device=dev)
+    fwd, bwd = [], []
+    gi = gv = None
+    loss = 0.0
+    for rep in range(1 + args.adjoint_reps):
+        start_from(sim, aw.workload.state)
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(stream)
+        loss = ro.forward(aw.inflow)
+        ev[1].record(stream)
+        gi, gv = ro.backward(velocity=True)
+        ev[2].record(stream)
+        ev[2].synchronize()
+        if rep:  # the first repetition is the warm-up
+            fwd.append(ev[0].elapsed_time(ev[1]))
+            bwd.append(ev[1].elapsed_time(ev[2]))
+    ro.dispose()
+    sim.dispose()
+    f_ms, b_ms = float(np.median(fwd)), float(np.median(bwd))
+    if pg:
+        tt = torch.tensor([f_ms, b_ms], device=dev)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        f_ms, b_ms = (float(v) for v in tt.tolist())
+    n = int(np.prod(aw.target.shape))
+    out = {
+        "workload": f"adjoint_{args.adjoint_size}: {args.adjoint_size}^3 four-plume start (about 30 % of bricks active), "
+                    f"16 x 16 inflow patch at y = 1 (2 + N(0, 0.1^2)), {aw.steps} plain f32 steps at dt 1/60, "
+                    f"loss |density - target|^2 (3 seeded Gaussians), checkpoint every {aw.checkpoint_interval}",
+        "loss": loss, "forward_ms": f_ms, "backward_ms": b_ms, "backward_over_forward": b_ms / f_ms,
+        "voxel_steps_per_s_forward": n * aw.steps / (f_ms / 1e3),
+        "voxel_steps_per_s_forward_backward": n * aw.steps / ((f_ms + b_ms) / 1e3), "repetitions": args.adjoint_reps,
+        "h2d_bytes": int(aw.inflow.nbytes), "d2h_bytes": int(8 + gi.nbytes + gv.nbytes),
+    }
+    ref_path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", f"adjoint_c4_{args.adjoint_size}.json")
+    if os.path.exists(ref_path) and aw.steps == 64:
+        with open(ref_path) as f:
+            ref = json.load(f)
+        scale = float(np.abs(gi).max())
+        g = [float(gi.ravel()[j]) for j in ref["picks"]]
+
+        def worst(vals):
+            return max(abs(a - b) / max(abs(b), 1e-3 * scale) for a, b in zip(g, vals))
+
+        out["gradient_check"] = {
+            "parameters": len(g), "max_rel_vs_f32_tangent": worst(ref["tan32"]),
+            "max_rel_vs_f64_central_differences": worst(ref["fd64"]), "h": ref["h"],
+            "loss_rel_vs_oracle_f32": abs(loss - ref["loss32"]) / ref["loss32"],
+        }
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -428,6 +500,12 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiation configuration")
+    ap.add_argument("--adjoint-size", type=int, default=128)
+    ap.add_argument("--adjoint-reps", type=int, default=2)
+    ap.add_argument("--adjoint-steps", type=int, default=64)
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="run only the differentiation configuration (one GPU) and print its JSON object (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -439,6 +517,9 @@ def main():
 
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
+    if args.adjoint_only:
+        print(json.dumps({"adjoint_c4": run_adjoint_c4(args, local, None)}))
+        return 0
     pg = None
     if world > 1:
         import datetime
@@ -588,6 +669,7 @@ def main():
         compare["f16_fused_vcycle"] = r
 
     batch_c3 = None if args.no_c3 else run_batch_c3(args, local, rank, world, pg)
+    adjoint = None if args.no_adjoint else run_adjoint_c4(args, local, pg)
 
     cpu = None
     parity = None
@@ -610,7 +692,7 @@ def main():
                 "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (about 2 GB of fields per step)",
             },
             "roofline": roofline, "kernels": kernel_table, "cpu_baseline": cpu, "parity_full_size": parity, "e2e": e2e,
-            "compare": compare, "error_vs_f64": error, "batch_c3": batch_c3,
+            "compare": compare, "error_vs_f64": error, "batch_c3": batch_c3, "adjoint_c4": adjoint,
             "gpu_launches": int(kernels_last * args.steps), "clocks": clock_info,
         }
         print(json.dumps(line))

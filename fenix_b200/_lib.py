@@ -171,6 +171,12 @@ class FxAutotuneReport(Structure):
     _fields_ = [("sweep_variant", c_int32 * 3), ("sweep_us", c_float * 3), ("default_us", c_float * 3)]
 
 
+class FxRolloutDesc(Structure):
+    _fields_ = [("struct_size", c_uint32), ("steps", c_uint32), ("checkpoint_interval", c_uint32), ("reserved0", c_uint32),
+                ("start_elapsed", c_double), ("step_seconds", c_double), ("inflow_x0", c_uint32), ("inflow_y", c_uint32),
+                ("inflow_z0", c_uint32), ("inflow_nx", c_uint32), ("inflow_nz", c_uint32), ("reserved1", c_uint32)]
+
+
 class FxBloomParams(Structure):
     _fields_ = [("enabled", c_int32), ("reserved", c_int32), ("threshold", c_double), ("strength", c_double), ("radius", c_double)]
 
@@ -248,6 +254,12 @@ PROTOTYPES = [
     ("fx_sim_get_solver", c_int32, [c_void_p, POINTER(FxSolverSettings)]),
     ("fx_sim_read_solver_stats", c_int32, [c_void_p, POINTER(FxSolverStats)]),
     ("fx_sim_autotune", c_int32, [c_void_p, POINTER(FxAutotuneReport)]),
+    ("fx_rollout_desc_default", None, [POINTER(FxRolloutDesc)]),
+    ("fx_rollout_create", c_int32, [c_void_p, POINTER(FxRolloutDesc), POINTER(c_void_p)]),
+    ("fx_rollout_destroy", None, [c_void_p]),
+    ("fx_rollout_set_target", c_int32, [c_void_p, POINTER(c_float)]),
+    ("fx_rollout_forward", c_int32, [c_void_p, POINTER(c_float), POINTER(c_double)]),
+    ("fx_rollout_backward", c_int32, [c_void_p, POINTER(c_float), POINTER(c_float)]),
     ("fx_batch_create", c_int32, [POINTER(POINTER(FxSimOptions)), c_uint32, POINTER(c_void_p)]),
     ("fx_batch_destroy", None, [c_void_p]),
     ("fx_batch_size", c_int32, [c_void_p, POINTER(c_uint32)]),

@@ -12,7 +12,7 @@ import sys
 
 PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PACKAGE_DIR, "csrc")
-SOURCES = ["fx_sim.cu", "fx_plain.cu", "fx_fused.cu", "fx_pressure.cu", "fx_vcycle.cu", "fx_render.cu", "fx_noalloc.cu"]
+SOURCES = ["fx_sim.cu", "fx_plain.cu", "fx_fused.cu", "fx_pressure.cu", "fx_vcycle.cu", "fx_render.cu", "fx_noalloc.cu", "fx_adjoint.cu"]
 OUTPUT = os.path.join(PACKAGE_DIR, "libfenixcuda.so")
 
 NVCC_FLAGS = [

@@ -239,8 +239,13 @@ FX_DEV void turbulent_dir(float px, float py, float pz, float seed, float& ox, f
 
 // The per-voxel emitter loops of inject-scalar.wgsl.ts:44-65,
 // inject-velocity.wgsl.ts:56-95 and inject-igniter.wgsl.ts:43-62.
-FX_DEV void inject_scalar_voxel(const Params& P, const float* __restrict__ src, uint32_t nsrc, float px, float py, float pz,
-                                float& dd, float& tt, float& ff) {
+//
+// These and the per-voxel source terms below are templates over the number
+// type of the state values: the kernels use float; the adjoint kernels evaluate
+// the same code with dual numbers (fx_dual.cuh) to obtain its local Jacobian.
+template <class T>
+FX_DEV void inject_scalar_voxel(const Params& P, const float* __restrict__ src, uint32_t nsrc, float px, float py, float pz, T& dd,
+                                T& tt, T& ff) {
   for (uint32_t e = 0; e < nsrc; ++e) {
     const Src s = load_src(src + 32u * e);
     const bool burst = s.kind == 3.0f;
@@ -261,8 +266,9 @@ FX_DEV void inject_scalar_voxel(const Params& P, const float* __restrict__ src, 
   }
 }
 
-FX_DEV void inject_velocity_voxel(const Params& P, const float* __restrict__ src, uint32_t nsrc, float px, float py, float pz,
-                                  float& vx, float& vy, float& vz) {
+template <class T>
+FX_DEV void inject_velocity_voxel(const Params& P, const float* __restrict__ src, uint32_t nsrc, float px, float py, float pz, T& vx,
+                                  T& vy, T& vz) {
   for (uint32_t e = 0; e < nsrc; ++e) {
     const Src s = load_src(src + 32u * e);
     const bool burst = s.kind == 3.0f;
@@ -325,8 +331,9 @@ FX_DEV void inject_velocity_voxel(const Params& P, const float* __restrict__ src
 
 FX_DEV float speed_limit(const Params& P) { return 80.0f / mx(P.dx, 0.001f); }
 
-FX_DEV void inject_igniter_voxel(const Params& P, const float* __restrict__ src, uint32_t nsrc, float px, float py, float pz,
-                                 float fuel, float& rr, float& tt) {
+template <class T>
+FX_DEV void inject_igniter_voxel(const Params& P, const float* __restrict__ src, uint32_t nsrc, float px, float py, float pz, T fuel,
+                                 T& rr, T& tt) {
   for (uint32_t e = 0; e < nsrc; ++e) {
     const Src s = load_src(src + 32u * e);
     const bool burst = s.kind == 3.0f;
@@ -337,9 +344,9 @@ FX_DEV void inject_igniter_voxel(const Params& P, const float* __restrict__ src,
     if (dist > (burst ? source_outer_limit(P, radius) : radius)) continue;
     const float weight = burst ? eruptive_falloff(P, px, py, pz, dist, s, 0.6f) : sphere_falloff(dist, radius, 0.6f);
     const float intensity = s.intensity;
-    const float fuel_avail = burst ? 1.0f : smoothstepv(0.02f, 0.22f, fuel);
+    const T fuel_avail = burst ? T(1.0f) : smoothstepv(0.02f, 0.22f, fuel);
     const float release = burst ? 1.0f / source_duration(s) : 1.6f;
-    const float seed = intensity * weight * fuel_avail * P.dt * release;
+    const T seed = intensity * weight * fuel_avail * P.dt * release;
     rr = clamp01(rr + seed);
     tt = clamp01(tt + intensity * weight * P.dt * 4.0f);
   }
@@ -359,20 +366,20 @@ FX_DEV float thermal_noise(const Params& P, float px, float py, float pz) {
 }
 
 // The decay block of advect-scalar-maccormack.wgsl.ts:80-100.
-FX_DEV void decay_scalars(const Params& P, float ny, float noise, float& density, float& temperature, float& fuel, float& reaction) {
+template <class T>
+FX_DEV void decay_scalars(const Params& P, float ny, float noise, T& density, T& temperature, T& fuel, T& reaction) {
   const float dt = P.dt;
-  const float hot = smoothstepv(0.22f, 0.78f, temperature + fuel * 0.2f + reaction * 0.26f);
-  const float cooling_pocket =
-      smoothstepv(0.44f, 0.9f, 1.0f - noise) * smoothstepv(0.08f, 0.74f, density) * (1.0f - hot * 0.72f);
-  const float cooling = dt * (0.016f + ny * 0.052f) * mixv(1.28f, 0.58f, hot) * mixv(0.86f, 1.9f, cooling_pocket);
+  const T hot = smoothstepv(0.22f, 0.78f, temperature + fuel * 0.2f + reaction * 0.26f);
+  const T cooling_pocket = smoothstepv(0.44f, 0.9f, 1.0f - noise) * smoothstepv(0.08f, 0.74f, density) * (1.0f - hot * 0.72f);
+  const T cooling = dt * (0.016f + ny * 0.052f) * mixv(1.28f, 0.58f, hot) * mixv(0.86f, 1.9f, cooling_pocket);
   const float smoke_loss = dt * (0.008f + ny * 0.026f) * mixv(0.75f, 1.38f, noise);
-  const float cold_breakup = dt * density * (1.0f - smoothstepv(0.2f, 0.86f, hot)) * smoothstepv(0.18f, 0.72f, density) *
-                             smoothstepv(0.34f, 0.92f, noise) * 0.34f;
-  const float clearing = dt * density * hot * mixv(0.1f, 0.72f, noise);
-  const float d = clamp01(mx(0.0f, density * (1.0f - smoke_loss) - clearing - cold_breakup));
-  const float t = clamp01(mx(0.0f, temperature - cooling));
-  const float f = clamp01(mx(0.0f, fuel - dt * mixv(0.012f, 0.034f, noise)));
-  const float r = clamp01(mx(0.0f, reaction - dt * mixv(0.46f, 0.82f, noise)));
+  const T cold_breakup = dt * density * (1.0f - smoothstepv(0.2f, 0.86f, hot)) * smoothstepv(0.18f, 0.72f, density) *
+                         smoothstepv(0.34f, 0.92f, noise) * 0.34f;
+  const T clearing = dt * density * hot * mixv(0.1f, 0.72f, noise);
+  const T d = clamp01(mx(0.0f, density * (1.0f - smoke_loss) - clearing - cold_breakup));
+  const T t = clamp01(mx(0.0f, temperature - cooling));
+  const T f = clamp01(mx(0.0f, fuel - dt * mixv(0.012f, 0.034f, noise)));
+  const T r = clamp01(mx(0.0f, reaction - dt * mixv(0.46f, 0.82f, noise)));
   density = d;
   temperature = t;
   fuel = f;
@@ -390,35 +397,38 @@ FX_DEV float thermal_cluster(const Params& P, float px, float py, float pz) {
 }
 
 // localHotGas of combustion-update.wgsl.ts:36-40.
-FX_DEV float comb_hot(float t, float f, float r) { return clampv(t * 1.55f + f * 0.26f + r * 0.44f, 0.0f, 1.0f); }
+template <class T>
+FX_DEV T comb_hot(T t, T f, T r) {
+  return clampv(t * 1.55f + f * 0.26f + r * 0.44f, 0.0f, 1.0f);
+}
 
 // combustion-update.wgsl.ts:52-92, given the six neighbour hot-gas values summed
 // in the reference order (+x, -x, +y, -y, +z, -z).
-FX_DEV void combustion_voxel(const Params& P, uint32_t x, uint32_t y, uint32_t z, float ny, float neighbor_sum, float& d,
-                             float& t, float& f, float& r) {
+template <class T>
+FX_DEV void combustion_voxel(const Params& P, uint32_t x, uint32_t y, uint32_t z, float ny, T neighbor_sum, T& d, T& t, T& f, T& r) {
   const float dt = P.dt;
   const float cluster = thermal_cluster(P, (float)x, (float)y, (float)z);
-  const float neighbor = neighbor_sum * 0.16666667f;
-  const float local_before = comb_hot(t, f, r);
-  const float radiative =
+  const T neighbor = neighbor_sum * 0.16666667f;
+  const T local_before = comb_hot(t, f, r);
+  const T radiative =
       mx(neighbor - local_before * 0.55f, 0.0f) * smoothstepv(0.04f, 0.76f, d) * (0.45f + (1.0f - cluster) * 0.55f) * dt * 2.6f;
-  const float hot_pocket = smoothstepv(0.58f, 0.92f, cluster + r * 0.22f);
-  const float cooling_pocket =
+  const T hot_pocket = smoothstepv(0.58f, 0.92f, cluster + r * 0.22f);
+  const T cooling_pocket =
       smoothstepv(0.42f, 0.82f, 1.0f - cluster) * smoothstepv(0.08f, 0.68f, d) * (1.0f - smoothstepv(0.54f, 0.94f, r));
-  const float ignition = smoothstepv(0.1f, 0.55f, t);
-  const float burn = mn(f, f * ignition * dt * mixv(4.2f, 8.6f, hot_pocket));
-  const float hot_soot = smoothstepv(0.24f, 0.88f, t + r * 0.2f) * smoothstepv(0.36f, 0.9f, 1.0f - cluster + d * 0.18f);
-  const float smoke_yield = burn * mixv(0.16f, 0.58f, cooling_pocket + (1.0f - ignition) * 0.5f + hot_soot * 0.45f);
-  const float hot_cooling = mixv(1.3f, 0.62f, hot_pocket);
-  const float heat_loss = dt * (0.018f + ny * 0.052f) * hot_cooling * mixv(1.0f, 2.25f, cooling_pocket);
-  const float density_loss = dt * d * (0.02f + ny * 0.07f);
-  const float clearing = d * smoothstepv(0.18f, 0.82f, t + r * 0.22f + f * 0.1f) * dt * mixv(0.55f, 2.45f, hot_pocket);
-  const float cooling_smoke = d * t * (cooling_pocket + hot_soot * 0.32f) * dt * 0.16f;
-  const float reaction_decay = r * (1.0f - dt * mixv(0.68f, 0.22f, hot_pocket));
-  const float nf = clamp01(f - burn);
-  const float nt = clamp01(t + burn * mixv(2.1f, 3.25f, hot_pocket) + radiative - heat_loss);
-  const float nd = clamp01(mx(0.0f, d + smoke_yield + cooling_smoke - density_loss - clearing * 0.72f));
-  const float nr = clamp01(mx(reaction_decay, burn * mixv(4.0f, 7.5f, hot_pocket) + radiative * 1.8f));
+  const T ignition = smoothstepv(0.1f, 0.55f, t);
+  const T burn = mn(f, f * ignition * dt * mixv(4.2f, 8.6f, hot_pocket));
+  const T hot_soot = smoothstepv(0.24f, 0.88f, t + r * 0.2f) * smoothstepv(0.36f, 0.9f, 1.0f - cluster + d * 0.18f);
+  const T smoke_yield = burn * mixv(0.16f, 0.58f, cooling_pocket + (1.0f - ignition) * 0.5f + hot_soot * 0.45f);
+  const T hot_cooling = mixv(1.3f, 0.62f, hot_pocket);
+  const T heat_loss = dt * (0.018f + ny * 0.052f) * hot_cooling * mixv(1.0f, 2.25f, cooling_pocket);
+  const T density_loss = dt * d * (0.02f + ny * 0.07f);
+  const T clearing = d * smoothstepv(0.18f, 0.82f, t + r * 0.22f + f * 0.1f) * dt * mixv(0.55f, 2.45f, hot_pocket);
+  const T cooling_smoke = d * t * (cooling_pocket + hot_soot * 0.32f) * dt * 0.16f;
+  const T reaction_decay = r * (1.0f - dt * mixv(0.68f, 0.22f, hot_pocket));
+  const T nf = clamp01(f - burn);
+  const T nt = clamp01(t + burn * mixv(2.1f, 3.25f, hot_pocket) + radiative - heat_loss);
+  const T nd = clamp01(mx(0.0f, d + smoke_yield + cooling_smoke - density_loss - clearing * 0.72f));
+  const T nr = clamp01(mx(reaction_decay, burn * mixv(4.0f, 7.5f, hot_pocket) + radiative * 1.8f));
   f = nf;
   t = nt;
   d = nd;
@@ -426,39 +436,43 @@ FX_DEV void combustion_voxel(const Params& P, uint32_t x, uint32_t y, uint32_t z
 }
 
 // hotGasAt of apply-buoyancy.wgsl.ts:31-35.
-FX_DEV float buoy_hot(float t, float r) { return clampv(t * 1.0f + r * 0.85f, 0.0f, 1.0f); }
+template <class T>
+FX_DEV T buoy_hot(T t, T r) {
+  return clampv(t * 1.0f + r * 0.85f, 0.0f, 1.0f);
+}
 
 // apply-buoyancy.wgsl.ts:47-109 given the voxel's own density/hot gas, the
 // central differences of hot gas (tg*) and density (dg*), and its velocity.
-FX_DEV void buoyancy_voxel(const Params& P, const Dims& dm, uint32_t x, uint32_t y, uint32_t z, float d, float hot_gas, float tgx,
-                           float tgy, float tgz, float dgx, float dgy, float dgz, float& vx, float& vy, float& vz) {
+template <class T>
+FX_DEV void buoyancy_voxel(const Params& P, const Dims& dm, uint32_t x, uint32_t y, uint32_t z, T d, T hot_gas, T tgx, T tgy, T tgz,
+                           T dgx, T dgy, T dgz, T& vx, T& vy, T& vz) {
   const float dt = P.dt;
   const float b = P.buoyancy;
   const float response = b * (1.0f + smoothstepv(6.0f, 24.0f, fabsf(b)) * 0.38f);
-  const float lift = hot_gas * response;
+  const T lift = hot_gas * response;
   const float gw = P.gravity[3];
-  const float gfx = P.gravity[0] * d * gw, gfy = P.gravity[1] * d * gw, gfz = P.gravity[2] * d * gw;
-  const float entrain = d * smoothstepv(0.04f, 0.3f, hot_gas);
+  const T gfx = P.gravity[0] * d * gw, gfy = P.gravity[1] * d * gw, gfz = P.gravity[2] * d * gw;
+  const T entrain = d * smoothstepv(0.04f, 0.3f, hot_gas);
   const float ny = ((float)y + 0.5f) / (float)dm.h;
   const float t = P.time;
   const float fxv = (float)x, fyv = (float)y, fzv = (float)z;
   const float shear = psin(fyv * 0.073f + t * 0.9f) * 0.35f + psin(fxv * 0.041f - fzv * 0.052f + t * 0.43f) * 0.22f;
   const float ww = P.wind[3];
   const float wx = P.wind[0], wy = P.wind[1], wz = P.wind[2];
-  const float amount = ww * (0.18f + d * 0.55f + ny * 0.45f);
-  const float windx = wx * amount + (-wz) * amount * shear;
-  const float windy = wy * amount + 0.0f * amount * shear;
-  const float windz = wz * amount + wx * amount * shear;
-  const float dgl = mx(length3(dgx, dgy, dgz), 0.0001f);
-  const float cold = d * (1.0f - smoothstepv(0.12f, 0.72f, hot_gas));
-  const float breakup = smoothstepv(0.008f, 0.06f, dgl) * cold;
+  const T amount = ww * (0.18f + d * 0.55f + ny * 0.45f);
+  const T windx = wx * amount + (-wz) * amount * shear;
+  const T windy = wy * amount + 0.0f * amount * shear;
+  const T windz = wz * amount + wx * amount * shear;
+  const T dgl = mx(length3(dgx, dgy, dgz), 0.0001f);
+  const T cold = d * (1.0f - smoothstepv(0.12f, 0.72f, hot_gas));
+  const T breakup = smoothstepv(0.008f, 0.06f, dgl) * cold;
   const float s1 = psin(fyv * 0.117f + t * 1.9f);
   const float s2 = psin(fxv * 0.071f - fzv * 0.083f + t * 1.35f) * 0.35f;
   const float s3 = pcos(fxv * 0.061f + fyv * 0.049f - t * 1.6f);
   const float sl = length3(s1, s2, s3);
   const float shx = s1 / sl, shy = s2 / sl, shz = s3 / sl;
-  const float collapse = d * (1.0f - smoothstepv(0.16f, 0.64f, hot_gas));
-  const float drag = d * smoothstepv(0.03f, 0.45f, hot_gas);
+  const T collapse = d * (1.0f - smoothstepv(0.16f, 0.64f, hot_gas));
+  const T drag = d * smoothstepv(0.03f, 0.45f, hot_gas);
   const float keep = 1.0f - dt * 0.08f;
   vx = vx * keep;
   vy = vy * keep;
@@ -470,7 +484,7 @@ FX_DEV void buoyancy_voxel(const Params& P, const Dims& dm, uint32_t x, uint32_t
   vx += (-dgx) / dgl * breakup * dt * 2.8f;
   vy += (-dgy) / dgl * breakup * dt * 2.8f;
   vz += (-dgz) / dgl * breakup * dt * 2.8f;
-  const float sk = 0.72f + breakup * 2.4f;
+  const T sk = 0.72f + breakup * 2.4f;
   vx += shx * cold * dt * sk; vy += shy * cold * dt * sk; vz += shz * cold * dt * sk;
   vx += wx * cold * ww * dt * 0.9f; vy += wy * cold * ww * dt * 0.9f; vz += wz * cold * ww * dt * 0.9f;
   vx += 0.0f * dt; vy += drag * response * 0.55f * dt; vz += 0.0f * dt;
@@ -485,18 +499,18 @@ FX_DEV void buoyancy_voxel(const Params& P, const Dims& dm, uint32_t x, uint32_t
 
 // apply-vorticity-confinement.wgsl.ts:42-65 given the |w| central differences,
 // the voxel's w, |w| and scalars. Returns |F|.
-FX_DEV float confinement_voxel(const Params& P, float gx, float gy, float gz, float wx, float wy, float wz, float wmag, float d,
-                               float t, float r, float& vx, float& vy, float& vz) {
-  const float gl = mx(length3(gx, gy, gz), 0.0001f);
-  const float nx = gx / gl, ny = gy / gl, nz = gz / gl;
-  const float hot_gas = clampv(t + r * 0.85f, 0.0f, 1.0f);
-  const float mask = clampv(P.vmask[0] + smoothstepv(0.02f, 0.38f, wmag) * P.vmask[1] + smoothstepv(0.04f, 0.7f, hot_gas) * P.vmask[2] +
-                                smoothstepv(0.04f, 0.65f, d) * P.vmask[3],
-                            0.0f, 4.0f);
+template <class T>
+FX_DEV T confinement_voxel(const Params& P, T gx, T gy, T gz, T wx, T wy, T wz, T wmag, T d, T t, T r, T& vx, T& vy, T& vz) {
+  const T gl = mx(length3(gx, gy, gz), 0.0001f);
+  const T nx = gx / gl, ny = gy / gl, nz = gz / gl;
+  const T hot_gas = clampv(t + r * 0.85f, 0.0f, 1.0f);
+  const T mask = clampv(P.vmask[0] + smoothstepv(0.02f, 0.38f, wmag) * P.vmask[1] + smoothstepv(0.04f, 0.7f, hot_gas) * P.vmask[2] +
+                            smoothstepv(0.04f, 0.65f, d) * P.vmask[3],
+                        0.0f, 4.0f);
   const float k = P.vorticity_strength;
-  const float fx = (ny * wz - nz * wy) * k * mask * 1.45f;
-  const float fy = (nz * wx - nx * wz) * k * mask * 1.45f;
-  const float fz = (nx * wy - ny * wx) * k * mask * 1.45f;
+  const T fx = (ny * wz - nz * wy) * k * mask * 1.45f;
+  const T fy = (nz * wx - nx * wz) * k * mask * 1.45f;
+  const T fz = (nx * wy - ny * wx) * k * mask * 1.45f;
   const float lim = speed_limit(P);
   vx = clampv(vx + fx * P.dt, -lim, lim);
   vy = clampv(vy + fy * P.dt, -lim, lim);

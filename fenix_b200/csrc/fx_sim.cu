@@ -15,6 +15,7 @@
 #include <cuda_fp16.h>
 
 #include "../../include/fenix_cuda.h"
+#include "fx_adjoint.h"
 #include "fx_fused.h"
 #include "fx_kernels.h"
 #include "fx_pressure.h"
@@ -307,18 +308,45 @@ int plain_smooth(fx_sim* s, LevelBuf& L, int iters, int start, uint32_t& launche
     (sim)->timer.end((sim)->stream);         \
   } while (0)
 
+// Additions to a plain step used by the differentiable rollout: the inflow
+// patch (applied after inject-velocity), and copies of the intermediate fields
+// its adjoint reads (a null pointer skips a copy).
+struct PlainHooks {
+  const float* inflow = nullptr;
+  InflowPatch patch{};
+  float* t1 = nullptr;  // temperature after inject-scalar
+  float* r1 = nullptr;  // reaction after inject-scalar
+  VelField v1{};        // velocity after inject-velocity and the inflow
+  VelField a{};         // velocity after advect-velocity
+  VelField b{};         // velocity after buoyancy
+};
+
+fx_status copy_vel(fx_sim* s, VelField dst, VelField src) {
+  if (!dst.c[0]) return FX_OK;
+  for (int c = 0; c < 3; ++c)
+    FX_CUDA(s, cudaMemcpyAsync(dst.c[c], src.c[c], (size_t)s->n * sizeof(float), cudaMemcpyDeviceToDevice, s->stream));
+  return FX_OK;
+}
+
 // The plain FP32 step: one kernel per reference dispatch, in the reference order.
-fx_status step_plain(fx_sim* s, bool vort_on, bool pressure_on, bool debug_on) {
+fx_status step_plain(fx_sim* s, bool vort_on, bool pressure_on, bool debug_on, const PlainHooks* hk = nullptr) {
   cudaStream_t st = s->stream;
   const int cur = s->cur, next = cur ^ 1;
   const uint32_t nsrc = std::max<uint32_t>(s->src_count, 1);
   uint32_t launches = 0;
   FX_TIMED(s, "plain_inject_scalar", plain_inject_scalar(st, s->dm, s->d_params, s->d_sources, nsrc, s->sets[cur]));
   FX_TIMED(s, "plain_inject_velocity", plain_inject_velocity(st, s->dm, s->d_params, s->d_sources, nsrc, s->vcur));
+  if (hk) {
+    if (hk->inflow) plain_inflow(st, s->dm, hk->patch, hk->inflow, s->vcur);
+    if (hk->t1) FX_CUDA(s, cudaMemcpyAsync(hk->t1, s->sets[cur].f[1], (size_t)s->n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    if (hk->r1) FX_CUDA(s, cudaMemcpyAsync(hk->r1, s->sets[cur].f[3], (size_t)s->n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    if (copy_vel(s, hk->v1, s->vcur) != FX_OK) return FX_ERR_CUDA;
+  }
   FX_TIMED(s, "plain_inject_igniter", plain_inject_igniter(st, s->dm, s->d_params, s->d_sources, nsrc, s->sets[cur]));
   FX_CUDA(s, cudaMemsetAsync(s->flags[cur], 0, s->nb * sizeof(uint32_t), st));
   FX_TIMED(s, "plain_active_bricks", plain_active_bricks(st, s->dm, s->bricks, s->sets[cur], s->flags[cur]));
   FX_TIMED(s, "plain_advect_velocity", plain_advect_velocity(st, s->dm, s->d_params, s->vcur, s->vscr));
+  if (hk && copy_vel(s, hk->a, s->vscr) != FX_OK) return FX_ERR_CUDA;
   FX_TIMED(s, "plain_advect_scalars", plain_advect_scalars(st, s->dm, s->bricks, s->d_params, s->advect_mode, s->sets[cur], s->vscr, s->flags[cur], s->sets[next]));
   FX_CUDA(s, cudaMemsetAsync(s->flags[next], 0, s->nb * sizeof(uint32_t), st));
   FX_TIMED(s, "plain_active_bricks", plain_active_bricks(st, s->dm, s->bricks, s->sets[next], s->flags[next]));
@@ -330,6 +358,7 @@ fx_status step_plain(fx_sim* s, bool vort_on, bool pressure_on, bool debug_on) {
   FX_TIMED(s, "plain_combustion", plain_combustion(st, s->dm, s->bricks, s->d_params, s->sets[2], s->flags[next], s->sets[next]));
   FX_TIMED(s, "plain_buoyancy", plain_buoyancy(st, s->dm, s->bricks, s->d_params, s->sets[next], s->flags[next], s->vscr));
   launches += 2;
+  if (hk && copy_vel(s, hk->b, s->vscr) != FX_OK) return FX_ERR_CUDA;
   if (vort_on) {
     FX_TIMED(s, "plain_vorticity", plain_vorticity(st, s->dm, s->vscr, s->vort, s->vort_mag));
     FX_TIMED(s, "plain_confinement", plain_confinement(st, s->dm, s->d_params, s->vort, s->vort_mag, s->sets[next], s->vscr, s->conf_mag));
@@ -1349,6 +1378,396 @@ const char* fx_batch_last_error(fx_batch* b) { return b ? b->err.c_str() : g_las
 fx_status fx_test_div6_exhaustive(unsigned long long* bad) {
   if (!bad) return FX_ERR_INVALID_ARGUMENT;
   return div6_exhaustive_check(bad) == cudaSuccess ? FX_OK : FX_ERR_CUDA;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------
+// Differentiable rollout: K plain FP32 steps from the simulation's state with an
+// inflow patch as the control, the loss sum (density_K - target)^2, and its
+// gradient with respect to the inflow values and the initial velocity by the
+// adjoint kernels of fx_adjoint.cu. The forward keeps a state checkpoint every
+// `checkpoint_interval` steps; the backward recomputes each segment from its
+// checkpoint, then steps back through it, re-running each step with the copies
+// its adjoint reads.
+// ------------------------------------------------------------------------------
+namespace {
+
+struct HostState {
+  int cur = 0;
+  int64_t step_index = 0;
+  bool initialized = false;
+  double start_s = 0, last_elapsed_s = 0;
+  int last_p = 0;
+  bool debug_requested = false;
+};
+
+}  // namespace
+
+struct fx_rollout {
+  fx_sim* s = nullptr;
+  int device = 0;
+  fx_rollout_desc d{};
+  InflowPatch patch{};
+  size_t n = 0;
+  uint32_t npatch = 0, nck = 0;
+  void* arena = nullptr;
+  float* inflow = nullptr;
+  float* target = nullptr;
+  float* grad_inflow = nullptr;
+  double* loss = nullptr;
+  float* ck = nullptr;   // nck states of 7 n floats: density, temperature, fuel, reaction, velocity x, y, z
+  float* seg = nullptr;  // checkpoint_interval states
+  float* fin = nullptr;  // the final state of the latest forward
+  std::vector<HostState> ck_host, seg_host;
+  HostState fin_host;
+  float* t1 = nullptr;
+  float* r1 = nullptr;
+  VelField v1{}, a{}, b{};
+  ScalarSet lam_s[2]{};
+  VelField lam_v[2]{};
+  VelField lam_c{}, lam_w{}, lam_g{};
+  float* lam_wmag = nullptr;
+  float* hot = nullptr;
+  float* dens = nullptr;
+  float* lam_p[3][2]{};
+  float* lam_div[3]{};
+  bool have_target = false;
+  bool forward_done = false;
+};
+
+namespace {
+
+// Configuration and argument errors of the rollout are reported through
+// fx_last_error and leave the simulation usable; CUDA failures are recorded on
+// the simulation (sticky), like its own.
+fx_status rollout_check(fx_rollout* r) {
+  fx_sim* s = r->s;
+  if (!s->err.empty()) return fail(nullptr, FX_ERR_STATE, "fx_rollout: the simulation has an error: " + s->err);
+  if (s->kernels != FX_KERNELS_PLAIN || s->half)
+    return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_rollout: the simulation must use the plain kernels with f32 storage");
+  if (s->solver.mode != FX_SOLVER_REFERENCE || s->advect_mode != FX_ADVECT_MACCORMACK)
+    return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_rollout: needs the reference pressure schedule and MacCormack advection");
+  if (s->qi[0] != 1 || s->qi[1] != 1)
+    return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_rollout: needs pressure and vorticity intervals of 1");
+  return FX_OK;
+}
+
+HostState host_state(const fx_sim* s) {
+  HostState h;
+  h.cur = s->cur;
+  h.step_index = s->step_index;
+  h.initialized = s->initialized;
+  h.start_s = s->start_s;
+  h.last_elapsed_s = s->last_elapsed_s;
+  h.last_p = s->last_p;
+  h.debug_requested = s->debug_requested;
+  return h;
+}
+
+fx_status save_state(fx_rollout* r, float* dst, HostState& h) {
+  fx_sim* s = r->s;
+  h = host_state(s);
+  const size_t b = r->n * sizeof(float);
+  for (int k = 0; k < 4; ++k) FX_CUDA(s, cudaMemcpyAsync(dst + k * r->n, s->sets[s->cur].f[k], b, cudaMemcpyDeviceToDevice, s->stream));
+  for (int k = 0; k < 3; ++k) FX_CUDA(s, cudaMemcpyAsync(dst + (4 + k) * r->n, s->vcur.c[k], b, cudaMemcpyDeviceToDevice, s->stream));
+  return FX_OK;
+}
+
+fx_status restore_state(fx_rollout* r, const float* src, const HostState& h) {
+  fx_sim* s = r->s;
+  s->cur = h.cur;
+  s->step_index = h.step_index;
+  s->initialized = h.initialized;
+  s->start_s = h.start_s;
+  s->last_elapsed_s = h.last_elapsed_s;
+  s->last_p = h.last_p;
+  s->debug_requested = h.debug_requested;
+  const size_t b = r->n * sizeof(float);
+  for (int k = 0; k < 4; ++k) FX_CUDA(s, cudaMemcpyAsync(s->sets[s->cur].f[k], src + k * r->n, b, cudaMemcpyDeviceToDevice, s->stream));
+  for (int k = 0; k < 3; ++k) FX_CUDA(s, cudaMemcpyAsync(s->vcur.c[k], src + (4 + k) * r->n, b, cudaMemcpyDeviceToDevice, s->stream));
+  return FX_OK;
+}
+
+fx_status rollout_step(fx_rollout* r, uint32_t k, const PlainHooks& hk) {
+  fx_sim* s = r->s;
+  const double elapsed = r->d.start_elapsed + (double)k * r->d.step_seconds;
+  StepPlan sp;
+  fx_status st = step_begin(s, elapsed, r->d.step_seconds, sp);
+  if (st != FX_OK) return st;
+  return step_finish(s, step_plain(s, sp.vort_on, sp.pressure_on, sp.debug_on, &hk), nullptr, sp, elapsed);
+}
+
+// PressureSolvePass.smooth (:129-143) in reverse.
+void reverse_smooth(fx_rollout* r, int l, int iters, int start) {
+  fx_sim* s = r->s;
+  const Dims dm = s->lv[l].dm;
+  for (int k = iters - 1; k >= 0; --k) {
+    const int a = start ^ (k & 1);
+    adj_jacobi(s->stream, dm, r->lam_p[l][a ^ 1], r->lam_p[l][a], r->lam_div[l]);
+    cudaMemsetAsync(r->lam_p[l][a ^ 1], 0, count_of(dm) * sizeof(float), s->stream);
+  }
+}
+
+// PressureSolvePass.solve (:68-84) in reverse: from the adjoint of the final
+// fine pressure buffer to the adjoint of the fine divergence (lam_div[0]).
+void reverse_pressure(fx_rollout* r) {
+  fx_sim* s = r->s;
+  const int* q = s->qi;
+  const int fine_pre = q[2] & 1, mid_pre = q[4] & 1, coarse = q[6] & 1;
+  const int mid = mid_pre ^ (q[5] & 1);
+  reverse_smooth(r, 0, q[3], fine_pre);
+  adj_prolong(s->stream, s->lv[1].dm, s->lv[0].dm, r->lam_p[0][0], r->lam_p[1][mid]);
+  reverse_smooth(r, 1, q[5], mid_pre);
+  adj_prolong(s->stream, s->lv[2].dm, s->lv[1].dm, r->lam_p[1][0], r->lam_p[2][coarse]);
+  reverse_smooth(r, 2, q[6], 0);
+  adj_restrict(s->stream, s->lv[1].dm, s->lv[2].dm, r->lam_div[2], r->lam_div[1]);
+  reverse_smooth(r, 1, q[4], 0);
+  adj_restrict(s->stream, s->lv[0].dm, s->lv[1].dm, r->lam_div[1], r->lam_div[0]);
+  reverse_smooth(r, 0, q[2], 0);
+}
+
+// The adjoint of one step that was just re-run with the tape hooks from the
+// state `state0` (whose current set index was `cur`): lam_s[o], lam_v[o] hold
+// the adjoint of the step's output state; lam_s[o ^ 1], lam_v[o ^ 1] receive
+// the adjoint of its input state.
+fx_status reverse_step(fx_rollout* r, int cur, const float* state0, int o) {
+  fx_sim* s = r->s;
+  cudaStream_t st = s->stream;
+  const Dims dm = s->dm;
+  const int next = cur ^ 1;
+  const size_t n = r->n;
+  const Params* P = s->d_params;
+  const uint32_t nsrc = std::max<uint32_t>(s->src_count, 1);
+  ScalarSet S0;
+  for (int k = 0; k < 4; ++k) S0.f[k] = const_cast<float*>(state0) + k * n;
+  VelField V0;
+  for (int k = 0; k < 3; ++k) V0.c[k] = const_cast<float*>(state0) + (4 + k) * n;
+  const ScalarSet lo = r->lam_s[o], li = r->lam_s[o ^ 1];
+  const VelField lvo = r->lam_v[o], lvi = r->lam_v[o ^ 1];
+  for (int l = 0; l < 3; ++l) {
+    const size_t c = count_of(s->lv[l].dm) * sizeof(float);
+    FX_CUDA(s, cudaMemsetAsync(r->lam_p[l][0], 0, c, st));
+    FX_CUDA(s, cudaMemsetAsync(r->lam_p[l][1], 0, c, st));
+    FX_CUDA(s, cudaMemsetAsync(r->lam_div[l], 0, c, st));
+  }
+  adj_project(st, dm, lvo, r->lam_c, r->lam_p[0][s->last_p]);
+  reverse_pressure(r);
+  adj_divergence(st, dm, r->lam_div[0], r->lam_c);
+  adj_confinement(st, dm, P, s->vort, s->vort_mag, s->sets[next], r->b, r->lam_c, r->lam_w, r->lam_wmag, r->lam_g, lo);
+  adj_vorticity(st, dm, s->vort, s->vort_mag, r->lam_w, r->lam_wmag, r->lam_g, r->lam_c);
+  adj_buoyancy(st, dm, s->bricks, P, s->sets[next], s->flags[next], r->a, r->lam_c, lo, r->hot, r->dens);
+  adj_combustion(st, dm, s->bricks, P, s->sets[2], s->flags[next], lo, r->hot);
+  for (int k = 0; k < 4; ++k) FX_CUDA(s, cudaMemsetAsync(li.f[k], 0, n * sizeof(float), st));
+  for (int k = 0; k < 3; ++k) FX_CUDA(s, cudaMemsetAsync(lvi.c[k], 0, n * sizeof(float), st));
+  adj_advect_scalars(st, dm, s->bricks, P, s->sets[cur], r->a, s->flags[cur], lo, li, r->lam_c);
+  adj_advect_velocity(st, dm, P, r->v1, r->lam_c, lvi);
+  adj_inject_igniter(st, dm, P, s->d_sources, nsrc, r->t1, s->sets[cur].f[2], r->r1, li);
+  adj_inflow(st, dm, r->patch, lvi, r->grad_inflow);
+  adj_inject_velocity(st, dm, P, s->d_sources, nsrc, V0, lvi);
+  adj_inject_scalar(st, dm, P, s->d_sources, nsrc, S0, li);
+  FX_CUDA(s, cudaGetLastError());
+  return FX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void fx_rollout_desc_default(fx_rollout_desc* d) {
+  if (!d) return;
+  std::memset(d, 0, sizeof *d);
+  d->struct_size = sizeof *d;
+  d->steps = 64;
+  d->checkpoint_interval = 8;
+  d->step_seconds = 1.0 / 60.0;
+}
+
+fx_status fx_rollout_create(fx_sim* s, const fx_rollout_desc* d, fx_rollout** out) {
+  if (!s || !d || !out) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_rollout_create: NULL argument");
+  *out = nullptr;
+  if (d->struct_size < sizeof(fx_rollout_desc)) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_rollout_create: struct_size too small");
+  if (d->steps == 0 || d->checkpoint_interval == 0 || !(d->step_seconds > 0.0) || !std::isfinite(d->start_elapsed))
+    return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_rollout_create: steps, checkpoint_interval and step_seconds must be positive");
+  if ((uint64_t)d->inflow_x0 + d->inflow_nx > s->dm.w || d->inflow_y >= s->dm.h || (uint64_t)d->inflow_z0 + d->inflow_nz > s->dm.d)
+    return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_rollout_create: the inflow patch leaves the grid");
+  auto r = new (std::nothrow) fx_rollout;
+  if (!r) return fail(nullptr, FX_ERR_OUT_OF_MEMORY, "fx_rollout_create: host allocation failed");
+  r->s = s;
+  r->device = s->device;
+  r->d = *d;
+  r->patch = InflowPatch{d->inflow_x0, d->inflow_y, d->inflow_z0, d->inflow_nx, d->inflow_nz};
+  r->n = s->n;
+  r->npatch = d->inflow_nx * d->inflow_nz;
+  r->nck = (d->steps + d->checkpoint_interval - 1) / d->checkpoint_interval;
+  fx_status st = rollout_check(r);
+  if (st != FX_OK) {
+    delete r;
+    return st;
+  }
+  const size_t n = r->n;
+  const size_t n1 = count_of(s->lv[1].dm), n2 = count_of(s->lv[2].dm);
+  const size_t ints = (size_t)r->npatch * 2 + 64;
+  // floats: target, checkpoints, segment, final state, tape (11 n), adjoint (26 n), pressure adjoints
+  const size_t floats = n + (size_t)r->nck * 7 * n + (size_t)d->checkpoint_interval * 7 * n + 7 * n + 11 * n + 26 * n +
+                        3 * (n + n1 + n2) + ints;
+  const size_t bytes = floats * sizeof(float) + 64 * 256 + sizeof(double) * 2;
+  if (cudaSetDevice(s->device) != cudaSuccess || cudaMalloc(&r->arena, bytes) != cudaSuccess) {
+    delete r;
+    return fail(nullptr, FX_ERR_OUT_OF_MEMORY, "fx_rollout_create: device allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  char* p = static_cast<char*>(r->arena);
+  auto take = [&](size_t count) {
+    float* q = reinterpret_cast<float*>(p);
+    p += (count * sizeof(float) + 255) / 256 * 256;
+    return q;
+  };
+  r->loss = reinterpret_cast<double*>(take(4));
+  r->inflow = take(r->npatch + 1);
+  r->grad_inflow = take(r->npatch + 1);
+  r->target = take(n);
+  r->ck = take((size_t)r->nck * 7 * n);
+  r->seg = take((size_t)d->checkpoint_interval * 7 * n);
+  r->fin = take(7 * n);
+  r->t1 = take(n);
+  r->r1 = take(n);
+  for (int k = 0; k < 3; ++k) {
+    r->v1.c[k] = take(n);
+    r->a.c[k] = take(n);
+    r->b.c[k] = take(n);
+  }
+  for (int o = 0; o < 2; ++o) {
+    for (int k = 0; k < 4; ++k) r->lam_s[o].f[k] = take(n);
+    for (int k = 0; k < 3; ++k) r->lam_v[o].c[k] = take(n);
+  }
+  for (int k = 0; k < 3; ++k) {
+    r->lam_c.c[k] = take(n);
+    r->lam_w.c[k] = take(n);
+    r->lam_g.c[k] = take(n);
+  }
+  r->lam_wmag = take(n);
+  r->hot = take(n);
+  r->dens = take(n);
+  for (int l = 0; l < 3; ++l) {
+    const size_t c = count_of(s->lv[l].dm);
+    r->lam_p[l][0] = take(c);
+    r->lam_p[l][1] = take(c);
+    r->lam_div[l] = take(c);
+  }
+  if ((size_t)(p - static_cast<char*>(r->arena)) > bytes) {
+    cudaFree(r->arena);
+    delete r;
+    return fail(nullptr, FX_ERR_STATE, "fx_rollout_create: internal layout error");
+  }
+  r->ck_host.resize(r->nck);
+  r->seg_host.resize(d->checkpoint_interval);
+  if (cudaMemsetAsync(r->arena, 0, bytes, s->stream) != cudaSuccess) {
+    cudaFree(r->arena);
+    delete r;
+    return fail(nullptr, FX_ERR_CUDA, "fx_rollout_create: cudaMemsetAsync failed");
+  }
+  *out = r;
+  return FX_OK;
+}
+
+// Touches only the rollout's own memory (cudaFree waits for the device), so it
+// may run after the simulation was destroyed.
+void fx_rollout_destroy(fx_rollout* r) {
+  if (!r) return;
+  cudaSetDevice(r->device);
+  if (r->arena) cudaFree(r->arena);
+  delete r;
+}
+
+fx_status fx_rollout_set_target(fx_rollout* r, const float* target) {
+  if (!r || !target) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_rollout_set_target: NULL argument");
+  fx_sim* s = r->s;
+  FX_CUDA(s, cudaSetDevice(s->device));
+  FX_CUDA(s, cudaMemcpyAsync(r->target, target, r->n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  r->have_target = true;
+  return FX_OK;
+}
+
+fx_status fx_rollout_forward(fx_rollout* r, const float* inflow, double* loss) {
+  if (!r || (!inflow && r->npatch) || !loss) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_rollout_forward: NULL argument");
+  fx_sim* s = r->s;
+  fx_status st = rollout_check(r);
+  if (st != FX_OK) return st;
+  if (!r->have_target) return fail(nullptr, FX_ERR_STATE, "fx_rollout_forward: no target (fx_rollout_set_target)");
+  FX_CUDA(s, cudaSetDevice(s->device));
+  r->forward_done = false;
+  if (r->npatch)
+    FX_CUDA(s, cudaMemcpyAsync(r->inflow, inflow, r->npatch * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  PlainHooks hk;
+  hk.inflow = r->npatch ? r->inflow : nullptr;
+  hk.patch = r->patch;
+  const uint32_t every = r->d.checkpoint_interval;
+  for (uint32_t k = 0; k < r->d.steps; ++k) {
+    if (k % every == 0 && save_state(r, r->ck + (size_t)(k / every) * 7 * r->n, r->ck_host[k / every]) != FX_OK) return FX_ERR_CUDA;
+    st = rollout_step(r, k, hk);
+    if (st != FX_OK) return st;
+  }
+  if (save_state(r, r->fin, r->fin_host) != FX_OK) return FX_ERR_CUDA;
+  FX_CUDA(s, cudaMemsetAsync(r->loss, 0, sizeof(double), s->stream));
+  adj_loss(s->stream, (uint32_t)r->n, s->sets[s->cur].f[0], r->target, nullptr, r->loss);
+  FX_CUDA(s, cudaMemcpyAsync(loss, r->loss, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  r->forward_done = true;
+  return FX_OK;
+}
+
+fx_status fx_rollout_backward(fx_rollout* r, float* grad_inflow, float* grad_velocity) {
+  if (!r || (!grad_inflow && r->npatch)) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_rollout_backward: NULL argument");
+  fx_sim* s = r->s;
+  if (!r->forward_done) return fail(nullptr, FX_ERR_STATE, "fx_rollout_backward: no forward to differentiate");
+  fx_status st = rollout_check(r);
+  if (st != FX_OK) return st;
+  FX_CUDA(s, cudaSetDevice(s->device));
+  cudaStream_t cs = s->stream;
+  const size_t n = r->n;
+  int o = 0;
+  for (int k = 0; k < 4; ++k) FX_CUDA(s, cudaMemsetAsync(r->lam_s[0].f[k], 0, n * sizeof(float), cs));
+  for (int k = 0; k < 3; ++k) FX_CUDA(s, cudaMemsetAsync(r->lam_v[0].c[k], 0, n * sizeof(float), cs));
+  FX_CUDA(s, cudaMemsetAsync(r->grad_inflow, 0, (r->npatch + 1) * sizeof(float), cs));
+  FX_CUDA(s, cudaMemsetAsync(r->hot, 0, n * sizeof(float), cs));
+  FX_CUDA(s, cudaMemsetAsync(r->dens, 0, n * sizeof(float), cs));
+  FX_CUDA(s, cudaMemsetAsync(r->loss + 1, 0, sizeof(double), cs));
+  adj_loss(cs, (uint32_t)n, r->fin, r->target, r->lam_s[0].f[0], r->loss + 1);
+  PlainHooks run;
+  run.inflow = r->npatch ? r->inflow : nullptr;
+  run.patch = r->patch;
+  PlainHooks tape = run;
+  tape.t1 = r->t1;
+  tape.r1 = r->r1;
+  tape.v1 = r->v1;
+  tape.a = r->a;
+  tape.b = r->b;
+  const uint32_t every = r->d.checkpoint_interval;
+  for (int seg = (int)r->nck - 1; seg >= 0; --seg) {
+    const uint32_t k0 = (uint32_t)seg * every, k1 = std::min(k0 + every, r->d.steps);
+    if (restore_state(r, r->ck + (size_t)seg * 7 * n, r->ck_host[seg]) != FX_OK) return FX_ERR_CUDA;
+    for (uint32_t k = k0; k < k1; ++k) {
+      if (save_state(r, r->seg + (size_t)(k - k0) * 7 * n, r->seg_host[k - k0]) != FX_OK) return FX_ERR_CUDA;
+      if (k + 1 < k1 && (st = rollout_step(r, k, run)) != FX_OK) return st;
+    }
+    for (int k = (int)k1 - 1; k >= (int)k0; --k) {
+      const float* state0 = r->seg + (size_t)(k - k0) * 7 * n;
+      if (restore_state(r, state0, r->seg_host[k - k0]) != FX_OK) return FX_ERR_CUDA;
+      const int cur = s->cur;
+      if ((st = rollout_step(r, (uint32_t)k, tape)) != FX_OK) return st;
+      if ((st = reverse_step(r, cur, state0, o)) != FX_OK) return st;
+      o ^= 1;
+    }
+  }
+  if (restore_state(r, r->fin, r->fin_host) != FX_OK) return FX_ERR_CUDA;
+  if (r->npatch)
+    FX_CUDA(s, cudaMemcpyAsync(grad_inflow, r->grad_inflow, r->npatch * sizeof(float), cudaMemcpyDeviceToHost, cs));
+  if (grad_velocity)
+    for (int k = 0; k < 3; ++k)
+      FX_CUDA(s, cudaMemcpyAsync(grad_velocity + k * n, r->lam_v[o].c[k], n * sizeof(float), cudaMemcpyDeviceToHost, cs));
+  FX_CUDA(s, cudaStreamSynchronize(cs));
+  return FX_OK;
 }
 
 }  // extern "C"

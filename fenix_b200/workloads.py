@@ -297,3 +297,41 @@ def batch_c3(seed: int = 1237, count: int = 64, processes: int = 0) -> List[Work
         with ProcessPoolExecutor(max_workers=processes, mp_context=multiprocessing.get_context("spawn")) as ex:
             return list(ex.map(_batch_build, params))
     return [_batch_build(p) for p in params]
+
+
+@dataclass
+class AdjointWorkload:
+    """The differentiation workload: a sparse plume, a patch of per-voxel inflow
+    velocity at y = 1 (the control), its initial values and the density target."""
+
+    workload: Workload
+    patch: Dict[str, int]  # x0, y, z0, nx, nz
+    inflow: np.ndarray  # (nz, nx) float32
+    target: np.ndarray  # (D, H, W) float32
+    steps: int = 64
+    checkpoint_interval: int = 8
+
+
+def adjoint_c4(seed: int = 1238, size: int = 128, steps: int = 64) -> AdjointWorkload:
+    """size^3 (128 by default) four-plume state with about 30 % of bricks active,
+    reference-default quality; a 16 x 16 inflow patch centred on the floor at
+    y = 1 (the y = 0 layer is zeroed by advect-velocity) with values
+    2 + N(0, 0.1^2); the target is a sum of 3 isotropic Gaussians (sigma 6-12
+    voxels, amplitude 0.5-1.0, scaled with size / 128)."""
+    wl = plume_256(seed=seed, size=size)
+    wl.options = dict(wl.options)
+    wl.options.pop("qualitySettings", None)
+    wl.name = f"adjoint_{size}"
+    rng = np.random.default_rng(seed)
+    n = min(16, size // 2)
+    patch = {"x0": (size - n) // 2, "y": 1, "z0": (size - n) // 2, "nx": n, "nz": n}
+    inflow = (2.0 + 0.1 * rng.standard_normal((n, n))).astype(np.float32)
+    s = size / 128.0
+    z, y, x = np.meshgrid(*(np.arange(size, dtype=np.float64),) * 3, indexing="ij")
+    target = np.zeros((size, size, size))
+    for _ in range(3):
+        c = (rng.uniform(0.25, 0.75) * size, rng.uniform(0.3, 0.8) * size, rng.uniform(0.25, 0.75) * size)
+        sigma = rng.uniform(6.0, 12.0) * s
+        amp = rng.uniform(0.5, 1.0)
+        target += amp * np.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / (2.0 * sigma * sigma))
+    return AdjointWorkload(wl, patch, inflow, target.astype(np.float32), steps=steps)

@@ -467,6 +467,48 @@ void fx_bloom_destroy(fx_bloom* pass);
 fx_status fx_bloom_render(fx_bloom* pass, const void* hdr, int32_t hdr_format, uint32_t width, uint32_t height,
                           const fx_bloom_params* params, void* out, int32_t out_format, void* stream);
 
+/* Differentiable rollout: an extension with no counterpart in the reference.
+ * K plain FP32 steps of a simulation (FX_KERNELS_PLAIN, f32 storage, the
+ * reference pressure schedule, MacCormack advection, pressure and vorticity
+ * intervals of 1) from its current state, with a control patch of per-voxel
+ * inflow velocity: after inject-velocity, every step sets velocity.y at
+ * (inflow_x0 + i, inflow_y, inflow_z0 + k) to inflow[i + inflow_nx * k]. The loss
+ * is sum over voxels of (density_K - target)^2 (FP64 accumulation). Step k runs
+ * at elapsed = start_elapsed + k * step_seconds with step = step_seconds.
+ *
+ * fx_rollout_forward leaves the simulation in its final state and keeps a state
+ * checkpoint every checkpoint_interval steps; fx_rollout_backward returns the
+ * gradient of the loss with respect to the inflow values and the initial
+ * velocity field by the adjoint of every pass, recomputing each segment from its
+ * checkpoint, and leaves the simulation in the forward's final state again.
+ * Brick flags, emitter sources and the step uniform are constants of the
+ * differentiation; a branch (min, max, clamp, the MacCormack limiter) passes the
+ * adjoint of the operand it selected. */
+typedef struct fx_rollout_desc {
+  uint32_t struct_size;
+  uint32_t steps;               /* K (default 64) */
+  uint32_t checkpoint_interval; /* k (default 8) */
+  uint32_t reserved0;
+  double start_elapsed;         /* elapsed seconds of step 0 */
+  double step_seconds;          /* default 1/60 */
+  uint32_t inflow_x0, inflow_y, inflow_z0;
+  uint32_t inflow_nx, inflow_nz; /* 0 x 0: no control patch */
+  uint32_t reserved1;
+} fx_rollout_desc;
+
+typedef struct fx_rollout fx_rollout;
+void fx_rollout_desc_default(fx_rollout_desc* desc);
+/* The rollout borrows `sim`: every call but fx_rollout_destroy needs it alive. */
+fx_status fx_rollout_create(fx_sim* sim, const fx_rollout_desc* desc, fx_rollout** out);
+void fx_rollout_destroy(fx_rollout* rollout);
+/* target: width * height * depth host floats (x fastest). */
+fx_status fx_rollout_set_target(fx_rollout* rollout, const float* target);
+/* inflow: inflow_nx * inflow_nz host floats; *loss receives the loss. */
+fx_status fx_rollout_forward(fx_rollout* rollout, const float* inflow, double* loss);
+/* grad_inflow: inflow_nx * inflow_nz host floats; grad_velocity: NULL or
+ * 3 * width * height * depth host floats (the x, y, z planes). */
+fx_status fx_rollout_backward(fx_rollout* rollout, float* grad_inflow, float* grad_velocity);
+
 /* Brick flags of caller-owned fields, allocating nothing. No counterpart in the
  * reference. It computes what compute-active-bricks.wgsl.ts:35-58 computes, for
  * the density, temperature and reaction fields (width*height*depth floats each,

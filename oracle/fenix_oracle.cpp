@@ -103,6 +103,75 @@ inline float pinned_sincos(float x, int quadrant_offset) {
   }
 }
 
+// Tangent numbers: a value (V = double for the FP64 restatement, V = float
+// for the f32 one) with one directional derivative in FP64. Sim<Tan> and
+// Sim<Tan32> evaluate the restatement in forward mode, which gives the exact
+// derivative of its output along a chosen input direction (the check of the
+// product's hand-written adjoint); Sim<Tan32> follows the f32 trajectory bit for
+// bit. A branch (min, max, clamp, select) follows the value and carries the
+// derivative of the branch taken; floor has derivative 0; sqrt has derivative 0
+// at 0.
+template <class V>
+struct TanT {
+  V v = 0;
+  double d = 0.0;
+  TanT() = default;
+  TanT(double x) : v((V)x), d(0.0) {}
+  TanT(V x, double dx, int) : v(x), d(dx) {}
+  explicit operator double() const { return (double)v; }
+  explicit operator float() const { return (float)v; }
+  explicit operator uint32_t() const { return (uint32_t)v; }
+  TanT operator-() const { return TanT(-v, -d, 0); }
+  TanT& operator+=(TanT b) { v += b.v; d += b.d; return *this; }
+  TanT& operator-=(TanT b) { v -= b.v; d -= b.d; return *this; }
+  TanT& operator*=(TanT b) { d = d * (double)b.v + (double)v * b.d; v *= b.v; return *this; }
+};
+template <class V> inline TanT<V> operator+(TanT<V> a, TanT<V> b) { return TanT<V>(a.v + b.v, a.d + b.d, 0); }
+template <class V> inline TanT<V> operator-(TanT<V> a, TanT<V> b) { return TanT<V>(a.v - b.v, a.d - b.d, 0); }
+template <class V> inline TanT<V> operator*(TanT<V> a, TanT<V> b) {
+  return TanT<V>(a.v * b.v, a.d * (double)b.v + (double)a.v * b.d, 0);
+}
+template <class V> inline TanT<V> operator/(TanT<V> a, TanT<V> b) {
+  const V q = a.v / b.v;
+  return TanT<V>(q, (a.d - (double)q * b.d) / (double)b.v, 0);
+}
+#define FX_TAN_MIXED(op)                                                                          \
+  template <class V> inline auto operator op(TanT<V> a, double b) { return a op TanT<V>(b); }    \
+  template <class V> inline auto operator op(double a, TanT<V> b) { return TanT<V>(a) op b; }
+FX_TAN_MIXED(+)
+FX_TAN_MIXED(-)
+FX_TAN_MIXED(*)
+FX_TAN_MIXED(/)
+#undef FX_TAN_MIXED
+template <class V> inline bool operator<(TanT<V> a, TanT<V> b) { return a.v < b.v; }
+template <class V> inline bool operator>(TanT<V> a, TanT<V> b) { return a.v > b.v; }
+template <class V> inline bool operator<=(TanT<V> a, TanT<V> b) { return a.v <= b.v; }
+template <class V> inline bool operator>=(TanT<V> a, TanT<V> b) { return a.v >= b.v; }
+template <class V> inline bool operator==(TanT<V> a, TanT<V> b) { return a.v == b.v; }
+template <class V> inline bool operator!=(TanT<V> a, TanT<V> b) { return a.v != b.v; }
+using Tan = TanT<double>;
+using Tan32 = TanT<float>;
+
+template <class R> struct is_tan : std::false_type {};
+template <class V> struct is_tan<TanT<V>> : std::true_type {};
+// Instantiations whose values are f32 (f32 literals and the pinned sin/cos).
+template <class R> struct is_f32 : std::is_same<R, float> {};
+template <> struct is_f32<Tan32> : std::true_type {};
+
+// floor, sqrt and |x| for every instantiation.
+inline float flr(float x) { return std::floor(x); }
+inline double flr(double x) { return std::floor(x); }
+template <class V> inline TanT<V> flr(TanT<V> x) { return TanT<V>(std::floor(x.v), 0.0, 0); }
+inline float sqr(float x) { return std::sqrt(x); }
+inline double sqr(double x) { return std::sqrt(x); }
+template <class V> inline TanT<V> sqr(TanT<V> x) {
+  const V r = std::sqrt(x.v);
+  return TanT<V>(r, r > 0 ? x.d / (2.0 * (double)r) : 0.0, 0);
+}
+inline float absr(float x) { return std::fabs(x); }
+inline double absr(double x) { return std::fabs(x); }
+template <class V> inline TanT<V> absr(TanT<V> x) { return x.v < 0 ? -x : x; }
+
 template <class R> struct Mth;
 template <> struct Mth<float> {
   static float sin(float x) { return pinned_sincos(x, 0); }
@@ -112,23 +181,31 @@ template <> struct Mth<double> {
   static double sin(double x) { return std::sin(x); }
   static double cos(double x) { return std::cos(x); }
 };
+template <> struct Mth<Tan> {
+  static Tan sin(Tan x) { return Tan(std::sin(x.v), std::cos(x.v) * x.d, 0); }
+  static Tan cos(Tan x) { return Tan(std::cos(x.v), -std::sin(x.v) * x.d, 0); }
+};
+template <> struct Mth<Tan32> {
+  static Tan32 sin(Tan32 x) { return Tan32(pinned_sincos(x.v, 0), (double)pinned_sincos(x.v, 1) * x.d, 0); }
+  static Tan32 cos(Tan32 x) { return Tan32(pinned_sincos(x.v, 1), -(double)pinned_sincos(x.v, 0) * x.d, 0); }
+};
 
 // A literal in the precision of the instantiation: the f32 literal for float
 // (matching WGSL's f32 constants), the f64 literal for double.
-#define K(x) (static_cast<R>(std::is_same<R, float>::value ? static_cast<double>(x##f) : static_cast<double>(x)))
+#define K(x) (static_cast<R>(is_f32<R>::value ? static_cast<double>(x##f) : static_cast<double>(x)))
 
 template <class R> inline R mn(R a, R b) { return b < a ? b : a; }
 template <class R> inline R mx(R a, R b) { return a < b ? b : a; }
 template <class R> inline R clampv(R x, R lo, R hi) { return mn(mx(x, lo), hi); }
 template <class R> inline R clamp01(R x) { return clampv(x, R(0), R(1)); }
 template <class R> inline R mixv(R a, R b, R t) { return a * (R(1) - t) + b * t; }
-template <class R> inline R fractv(R x) { return x - std::floor(x); }
+template <class R> inline R fractv(R x) { return x - flr(x); }
 template <class R> inline R stepv(R e, R x) { return x >= e ? R(1) : R(0); }
 template <class R> inline R smoothstepv(R e0, R e1, R x) {
   const R t = clampv((x - e0) / (e1 - e0), R(0), R(1));
   return t * t * (R(3) - R(2) * t);
 }
-template <class R> inline R length3(R x, R y, R z) { return std::sqrt(x * x + y * y + z * z); }
+template <class R> inline R length3(R x, R y, R z) { return sqr(x * x + y * y + z * z); }
 
 template <class R> struct V3 {
   R x, y, z;
@@ -184,7 +261,7 @@ template <class R> struct Corners {
 template <class R> inline Corners<R> corners(const Dims& dm, R px, R py, R pz) {
   const R mxp = R(dm.w - 1), myp = R(dm.h - 1), mzp = R(dm.d - 1);
   const R cx = clamp_pos(px, mxp), cy = clamp_pos(py, myp), cz = clamp_pos(pz, mzp);
-  const R flx = std::floor(cx), fly = std::floor(cy), flz = std::floor(cz);
+  const R flx = flr(cx), fly = flr(cy), flz = flr(cz);
   const uint32_t bx = (uint32_t)flx, by = (uint32_t)fly, bz = (uint32_t)flz;
   const uint32_t ux = std::min(bx + 1, dm.w - 1), uy = std::min(by + 1, dm.h - 1), uz = std::min(bz + 1, dm.d - 1);
   Corners<R> c;
@@ -274,7 +351,19 @@ template <class R> class Sim {
   // value a reference pass stores into one of those buffers is rounded to the
   // nearest binary16 (ties to even) and read back as R. Arithmetic stays in R.
   bool half_storage = false;
-  R qs(R v) const { return half_storage ? (R)(_Float16)v : v; }
+  R qs(R v) const {
+    if constexpr (is_tan<R>::value) return v;
+    else return half_storage ? (R)(_Float16)v : v;
+  }
+  // Extension with no reference counterpart: a patch of per-voxel inflow
+  // velocity. After inject-velocity, velocity.y at (x0 + i, y, z0 + k) is set to
+  // inflow[i + nx * k] (the control of the differentiable rollout).
+  uint32_t in_x0 = 0, in_y = 0, in_z0 = 0, in_nx = 0, in_nz = 0;
+  std::vector<R> inflow;
+  void apply_inflow() {
+    for (uint32_t k = 0; k < in_nz; ++k)
+      for (uint32_t i = 0; i < in_nx; ++i) vc[1][flat(dm, in_x0 + i, in_y, in_z0 + k)] = inflow[i + in_nx * k];
+  }
   // runtime params (createCombustionVolumeSimulation.ts:194-204)
   double wind[3] = {0, 0, 0}, wind_strength = 0, gravity[3] = {0, -1, 0}, gravity_strength = 0.45;
   double buoyancy = 3.6, vorticity_strength = 2.15;
@@ -396,7 +485,7 @@ template <class R> class Sim {
     return (R)fractv(pinned_sincos(d, 0) * 43758.5453123f);
   }
   static R value_noise3(R px, R py, R pz) {  // :106-117
-    const R cx = std::floor(px), cy = std::floor(py), cz = std::floor(pz);
+    const R cx = flr(px), cy = flr(py), cz = flr(pz);
     const R fx = fractv(px), fy = fractv(py), fz = fractv(pz);
     const R ux = fx * fx * (R(3) - R(2) * fx);
     const R uy = fy * fy * (R(3) - R(2) * fy);
@@ -816,7 +905,7 @@ template <class R> class Sim {
       const size_t i = flat(dm, x, y, z);
       const R dt = R(P.dt);
       const R b = R(P.buoyancy);
-      const R response = b * (R(1) + smoothstepv(K(6.0), K(24.0), std::fabs(b)) * K(0.38));
+      const R response = b * (R(1) + smoothstepv(K(6.0), K(24.0), absr(b)) * K(0.38));
       const R hot_gas = hot(x, y, z);
       const R lift = hot_gas * response;
       const R d = D[i];
@@ -853,7 +942,7 @@ template <class R> class Sim {
       R vx = vs[0][i] * keep, vy = vs[1][i] * keep, vz = vs[2][i] * keep;
       vx += windx * dt; vy += windy * dt; vz += windz * dt;
       vx += gfx * dt; vy += gfy * dt; vz += gfz * dt;
-      const R tk = K(3.2) + std::fabs(b) * K(0.08);
+      const R tk = K(3.2) + absr(b) * K(0.08);
       vx += tgx * collapse * dt * tk; vy += tgy * collapse * dt * tk; vz += tgz * collapse * dt * tk;
       vx += (-dgx) / dgl * breakup * dt * K(2.8);
       vy += (-dgy) / dgl * breakup * dt * K(2.8);
@@ -1265,6 +1354,7 @@ template <class R> class Sim {
     const int next = cur == 0 ? 1 : 0;
     inject_scalar(cur);
     inject_velocity();
+    apply_inflow();
     inject_igniter(cur);
     active_bricks(cur);
     advect_velocity();
@@ -1343,8 +1433,12 @@ struct Handle {
 
 template <class R> Sim<R>* as(Handle* h) { return static_cast<Sim<R>*>(h->sim); }
 
+// precision 32 (f32), 64 (f64), 65 (f64 tangent numbers) or 66 (f32 values
+// with FP64 tangents)
 template <class F> auto dispatch(Handle* h, F f) {
   if (h->precision == 32) return f(as<float>(h));
+  if (h->precision == 65) return f(as<Tan>(h));
+  if (h->precision == 66) return f(as<Tan32>(h));
   return f(as<double>(h));
 }
 
@@ -1354,11 +1448,16 @@ extern "C" {
 
 // Creates an oracle simulation (precision 32 or 64) of the given resolution with
 // the reference defaults (createCombustionVolumeSimulation.ts:54,194-204).
+// precisions 65 (FP64) and 66 (f32 values, the f32 trajectory) carry tangent
+// numbers: every field has a directional derivative in FP64
+// (orc_write_tangent seeds it, orc_read_tangent reads it).
 void* orc_create(int precision, uint32_t w, uint32_t h, uint32_t d) {
-  if ((precision != 32 && precision != 64) || w < 2 || h < 2 || d < 2) return nullptr;
+  if ((precision != 32 && precision != 64 && precision != 65 && precision != 66) || w < 2 || h < 2 || d < 2) return nullptr;
   Handle* hd = new Handle;
   hd->precision = precision;
   if (precision == 32) hd->sim = new Sim<float>(w, h, d);
+  else if (precision == 65) hd->sim = new Sim<Tan>(w, h, d);
+  else if (precision == 66) hd->sim = new Sim<Tan32>(w, h, d);
   else hd->sim = new Sim<double>(w, h, d);
   return hd;
 }
@@ -1367,6 +1466,8 @@ void orc_destroy(void* hv) {
   Handle* h = static_cast<Handle*>(hv);
   if (!h) return;
   if (h->precision == 32) delete as<float>(h);
+  else if (h->precision == 65) delete as<Tan>(h);
+  else if (h->precision == 66) delete as<Tan32>(h);
   else delete as<double>(h);
   delete h;
 }
@@ -1572,6 +1673,66 @@ long orc_write_field(void* hv, int id, const double* src, long count) {
     const bool scalar = id >= F_DENSITY && id <= F_PREV_REACTION;
     for (size_t i = 0; i < n; ++i) p[i] = scalar ? s->qs((R)src[i]) : (R)src[i];
     return (long)n;
+  });
+}
+
+// The inflow patch (extension): nx * nz values (row x fastest) of velocity.y at
+// (x0 .. x0+nx-1, y, z0 .. z0+nz-1), set after inject-velocity every step;
+// nx * nz == 0 turns it off. `tangents` (nullable) seeds their derivatives in a
+// precision-65 simulation. Returns 0, or -1 when the patch leaves the grid.
+int orc_set_inflow(void* hv, uint32_t x0, uint32_t y, uint32_t z0, uint32_t nx, uint32_t nz, const double* values,
+                   const double* tangents) {
+  return dispatch(static_cast<Handle*>(hv), [&](auto* s) -> int {
+    using R = typename std::remove_reference_t<decltype(s->inflow)>::value_type;
+    if ((uint64_t)x0 + nx > s->dm.w || y >= s->dm.h || (uint64_t)z0 + nz > s->dm.d) return -1;
+    s->in_x0 = x0;
+    s->in_y = y;
+    s->in_z0 = z0;
+    s->in_nx = nx;
+    s->in_nz = nz;
+    s->inflow.assign((size_t)nx * nz, R(0));
+    for (size_t k = 0; k < s->inflow.size(); ++k) {
+      if constexpr (is_tan<R>::value) s->inflow[k] = R((typename std::remove_reference_t<decltype(s->inflow[k].v)>)values[k], tangents ? tangents[k] : 0.0, 0);
+      else s->inflow[k] = (R)values[k];
+    }
+    return 0;
+  });
+}
+
+// Tangent parts of a field in a precision-65 simulation: read into dst (returns
+// the count, 0 for another precision or a bad id, -(needed) when cap is too
+// small) or overwrite them from src (values stay).
+long orc_read_tangent(void* hv, int id, double* dst, long cap) {
+  Handle* h = static_cast<Handle*>(hv);
+  if ((h->precision != 65 && h->precision != 66) || id == F_FLAGS || id == F_PREV_FLAGS) return 0;
+  return dispatch(h, [&](auto* s) -> long {
+    using R = typename std::remove_reference_t<decltype(s->inflow)>::value_type;
+    if constexpr (is_tan<R>::value) {
+      size_t n = 0;
+      R* p = s->field_ptr(id, &n);
+      if (!p) return 0;
+      if ((long)n > cap) return -(long)n;
+      for (size_t i = 0; i < n; ++i) dst[i] = p[i].d;
+      return (long)n;
+    } else {
+      return 0;
+    }
+  });
+}
+long orc_write_tangent(void* hv, int id, const double* src, long count) {
+  Handle* h = static_cast<Handle*>(hv);
+  if ((h->precision != 65 && h->precision != 66) || id == F_FLAGS || id == F_PREV_FLAGS) return 0;
+  return dispatch(h, [&](auto* s) -> long {
+    using R = typename std::remove_reference_t<decltype(s->inflow)>::value_type;
+    if constexpr (is_tan<R>::value) {
+      size_t n = 0;
+      R* p = s->field_ptr(id, &n);
+      if (!p || (long)n != count) return 0;
+      for (size_t i = 0; i < n; ++i) p[i].d = src[i];
+      return (long)n;
+    } else {
+      return 0;
+    }
   });
 }
 

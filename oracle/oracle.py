@@ -49,6 +49,12 @@ def load() -> ctypes.CDLL:
         lib.orc_bloom.argtypes = [POINTER(c_float), c_uint32, c_uint32, c_int, c_double, c_double, c_double, POINTER(c_float),
                                   POINTER(ctypes.c_uint8)]
         lib.orc_set_solver.argtypes = [c_void_p, POINTER(c_int), POINTER(c_double), c_int]
+        lib.orc_set_inflow.restype = c_int
+        lib.orc_set_inflow.argtypes = [c_void_p, c_uint32, c_uint32, c_uint32, c_uint32, c_uint32, POINTER(c_double), POINTER(c_double)]
+        lib.orc_read_tangent.restype = c_long
+        lib.orc_read_tangent.argtypes = [c_void_p, c_int, POINTER(c_double), c_long]
+        lib.orc_write_tangent.restype = c_long
+        lib.orc_write_tangent.argtypes = [c_void_p, c_int, POINTER(c_double), c_long]
         lib.orc_get_solver_stats.argtypes = [c_void_p, POINTER(c_double), POINTER(c_int)]
         lib.orc_update_sources.argtypes = [c_void_p, POINTER(c_float), c_uint32]
         lib.orc_step.argtypes = [c_void_p, c_double, c_double]
@@ -106,7 +112,11 @@ def num_threads() -> int:
 
 
 class OracleSimulation:
-    """The reference step on the CPU, in f32 (precision=32) or f64 (precision=64).
+    """The reference step on the CPU, in f32 (precision=32), f64 (precision=64)
+    or with tangent numbers: every value carries an FP64 directional derivative,
+    seeded with writeTangent / setInflow and read with readTangent, on the f64
+    trajectory (precision=65) or on the f32 trajectory, bit for bit
+    (precision=66).
 
     storage="f16" stores the scalar sets in binary16: every value a pass writes to
     density, temperature, fuel or reaction is rounded to the nearest binary16."""
@@ -237,12 +247,43 @@ class OracleSimulation:
             return buf[:n].astype(np.uint32)
         return buf[:n].astype(np.float32) if self.precision == 32 else buf[:n]
 
+
     def writeField(self, name: str, values: np.ndarray) -> None:
         fid = fxlib.FIELD_IDS[name]
         arr = np.ascontiguousarray(values, dtype=np.float64).ravel()
         n = self._lib.orc_write_field(self._h, fid, arr.ctypes.data_as(POINTER(c_double)), arr.size)
         if n != arr.size:
             raise ValueError(f"writeField({name}): size mismatch")
+
+    def setInflow(self, x0: int, y: int, z0: int, values: Optional[np.ndarray], tangents: Optional[np.ndarray] = None) -> None:
+        """The inflow patch (an extension): values[k, i] (nz x nx) is written to
+        velocity.y at (x0 + i, y, z0 + k) after inject-velocity every step; None
+        turns it off. `tangents` seeds their derivatives (precision 65)."""
+        if values is None:
+            self._lib.orc_set_inflow(self._h, 0, 0, 0, 0, 0, None, None)
+            return
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        nz, nx = v.shape
+        t = None if tangents is None else np.ascontiguousarray(tangents, dtype=np.float64).reshape(nz, nx)
+        r = self._lib.orc_set_inflow(self._h, x0, y, z0, nx, nz, v.ctypes.data_as(POINTER(c_double)),
+                                     None if t is None else t.ctypes.data_as(POINTER(c_double)))
+        if r != 0:
+            raise ValueError("the inflow patch leaves the grid")
+
+    def readTangent(self, name: str) -> np.ndarray:
+        fid = fxlib.FIELD_IDS[name]
+        cap = self._field_count(fid)
+        buf = np.empty(cap, dtype=np.float64)
+        n = self._lib.orc_read_tangent(self._h, fid, buf.ctypes.data_as(POINTER(c_double)), cap)
+        if n <= 0:
+            raise KeyError(f"readTangent({name}) needs precision 65")
+        return buf[:n]
+
+    def writeTangent(self, name: str, values: np.ndarray) -> None:
+        fid = fxlib.FIELD_IDS[name]
+        arr = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        if self._lib.orc_write_tangent(self._h, fid, arr.ctypes.data_as(POINTER(c_double)), arr.size) != arr.size:
+            raise ValueError(f"writeTangent({name}): size mismatch or precision")
 
     def _field_count(self, fid: int) -> int:
         n = self._lib.orc_read_field(self._h, fid, None, 0)

@@ -1,0 +1,156 @@
+"""The differentiable rollout on the GPU: its forward against the f32 oracle bit
+for bit, and its adjoint gradient against the oracle's tangent derivatives (the
+exact derivative of the f32 trajectory, and of the f64 one) and against central
+finite differences of the f64 oracle, on the 32^3 copy of the differentiation
+workload (64 steps, a checkpoint every 8) and, through the committed fixture,
+at its full 128^3 size."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import adjoint_refs as R
+from fenix_b200 import createCombustionVolumeSimulation, workloads
+from fenix_b200._lib import FenixError
+from fenix_b200.adjoint import Rollout, rollout_loss, start_from
+
+pytestmark = pytest.mark.gpu
+
+AW = workloads.adjoint_c4(size=32)
+PICKS = R.picks(AW)
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def rel(got: float, want: float, scale: float) -> float:
+    return abs(got - want) / max(abs(want), 1e-3 * scale)
+
+
+def run_rollout(aw, every=None):
+    sim = createCombustionVolumeSimulation(aw.workload.options, device=0, kernels="plain")
+    sim.updateSources(aw.workload.sources)
+    ro = Rollout(sim, steps=aw.steps, checkpoint_interval=every or aw.checkpoint_interval, patch=aw.patch)
+    ro.setTarget(aw.target)
+    start_from(sim, aw.workload.state)
+    loss = ro.forward(aw.inflow)
+    final = {k: sim.readField(k) for k in ("density", "temperature", "velocity_y")}
+    gi, gv = ro.backward()
+    return sim, ro, loss, final, gi, gv
+
+
+@pytest.fixture(scope="module")
+def rolled():
+    out = run_rollout(AW)
+    yield out
+    out[1].dispose()
+    out[0].dispose()
+
+
+def test_forward_matches_the_f32_oracle(rolled):
+    sim, ro, loss, final, gi, gv = rolled
+    orc = R.oracle_rollout(AW, 32)
+    for k, v in final.items():
+        np.testing.assert_array_equal(v, orc.readField(k), err_msg=k)
+    want = R.loss(AW, orc)
+    assert abs(loss - want) <= 1e-12 * want
+    # backward leaves the simulation in the forward's final state
+    for k, v in final.items():
+        np.testing.assert_array_equal(sim.readField(k), v, err_msg=k)
+
+
+def test_inflow_gradient_is_the_derivative_of_the_f32_step(rolled):
+    gi = rolled[4]
+    scale = float(np.abs(gi).max())
+    worst = max(rel(float(gi.ravel()[j]), R.tangent_loss(AW, R.oracle_rollout(AW, 66, tangent=R.unit(AW, j))), scale) for j in PICKS)
+    print(f"inflow gradient vs f32 tangent: max rel {worst:.2e}")
+    assert worst <= 1e-4
+
+
+def test_inflow_gradient_against_fp64_central_differences(rolled):
+    gi = rolled[4]
+    scale = float(np.abs(gi).max())
+    worst_fd = worst_tan = 0.0
+    for j in PICKS[:4]:
+        fd = R.central_difference(AW, j)
+        tan = R.tangent_loss(AW, R.oracle_rollout(AW, 65, tangent=R.unit(AW, j)))
+        assert rel(fd, tan, scale) <= 1e-4  # the two f64 references agree (h = 1e-3 truncation)
+        worst_fd = max(worst_fd, rel(float(gi.ravel()[j]), fd, scale))
+        worst_tan = max(worst_tan, rel(float(gi.ravel()[j]), tan, scale))
+    print(f"inflow gradient vs f64 central differences: max rel {worst_fd:.2e} (vs f64 tangent {worst_tan:.2e})")
+    assert worst_fd <= 1e-3
+
+
+def test_velocity_gradient_is_the_derivative_of_the_f32_step(rolled):
+    gv = rolled[5]
+    for seed in (7, 8):
+        dirv = R.velocity_direction(AW, seed)
+        tan = R.tangent_loss(AW, R.oracle_rollout(AW, 66, vel_tangent=dirv))
+        g = float((gv.reshape(3, -1).astype(np.float64) * dirv).sum())
+        print(f"velocity direction {seed}: adjoint {g:.6e} f32 tangent {tan:.6e}")
+        assert abs(g - tan) <= 1e-4 * abs(tan)
+
+
+def test_checkpoint_interval_does_not_change_the_gradient(rolled):
+    sim, gi = rolled[0], rolled[4]
+    for every in (1, 5, 64):
+        ro = Rollout(sim, steps=AW.steps, checkpoint_interval=every, patch=AW.patch)
+        ro.setTarget(AW.target)
+        start_from(sim, AW.workload.state)
+        ro.forward(AW.inflow)
+        g2, _ = ro.backward(velocity=False)
+        ro.dispose()
+        np.testing.assert_allclose(g2, gi, rtol=1e-4, atol=1e-6 * float(np.abs(gi).max()))
+
+
+def test_autograd_function_pair(rolled):
+    import torch
+
+    sim, ro, loss, final, gi, gv = rolled
+    u = torch.tensor(AW.inflow, requires_grad=True)
+    v0 = torch.tensor(np.stack([AW.workload.state["velocity_" + c] for c in "xyz"]), requires_grad=True)
+    out = rollout_loss(u, v0, ro, AW.workload.state)
+    assert abs(float(out) - loss) <= 1e-12 * loss
+    (2.0 * out).backward()
+    np.testing.assert_allclose(u.grad.numpy(), 2.0 * gi, rtol=1e-4, atol=1e-6 * float(np.abs(gi).max()))
+    np.testing.assert_allclose(v0.grad.numpy().reshape(3, -1), 2.0 * gv.reshape(3, -1), rtol=1e-3, atol=1e-5 * float(np.abs(gv).max()))
+
+
+def test_full_size_gradient_against_the_fixture():
+    """128^3, 16 x 16 inflow, 64 steps, a checkpoint every 8: the adjoint against
+    the committed f32-trajectory tangents and f64 central differences."""
+    with open(os.path.join(GOLDEN, "adjoint_c4_128.json")) as f:
+        ref = json.load(f)
+    aw = workloads.adjoint_c4(size=128)
+    sim, ro, loss, final, gi, gv = run_rollout(aw)
+    assert abs(loss - ref["loss32"]) <= 1e-9 * ref["loss32"]
+    scale = float(np.abs(gi).max())
+    g = [float(gi.ravel()[j]) for j in ref["picks"]]
+    worst32 = max(rel(a, b, scale) for a, b in zip(g, ref["tan32"]))
+    worst_fd = max(rel(a, b, scale) for a, b in zip(g, ref["fd64"]))
+    dirv = R.velocity_direction(aw, ref["velocity_direction_seed"])
+    gvd = float((gv.reshape(3, -1).astype(np.float64) * dirv).sum())
+    print(f"128^3: vs f32 tangent max rel {worst32:.2e}; vs f64 central differences max rel {worst_fd:.2e}; "
+          f"velocity direction {gvd:.6e} vs {ref['velocity_tan32']:.6e}")
+    ro.dispose()
+    sim.dispose()
+    assert worst32 <= 1e-4
+    assert abs(gvd - ref["velocity_tan32"]) <= 1e-4 * abs(ref["velocity_tan32"])
+    assert worst_fd <= 1e-3
+
+
+def test_rollout_rejects_unsupported_simulations():
+    opts = AW.workload.options
+    fused = createCombustionVolumeSimulation(opts, device=0)
+    with pytest.raises(FenixError, match="plain"):
+        Rollout(fused, steps=4, patch=AW.patch)
+    fused.dispose()
+    plain = createCombustionVolumeSimulation(opts, device=0, kernels="plain")
+    with pytest.raises(FenixError, match="grid"):
+        Rollout(plain, steps=4, patch={"x0": 30, "y": 1, "z0": 0, "nx": 8, "nz": 8})
+    plain.setQualitySettings({"pressureInterval": 2})
+    with pytest.raises(FenixError, match="interval"):
+        Rollout(plain, steps=4, patch=AW.patch)
+    # the simulation stays usable after those errors
+    plain.setQualitySettings({"pressureInterval": 1})
+    plain.step(0.0, 1 / 60)
+    plain.dispose()
