@@ -254,6 +254,8 @@ PROTOTYPES = [
     ("fx_sim_get_solver", c_int32, [c_void_p, POINTER(FxSolverSettings)]),
     ("fx_sim_read_solver_stats", c_int32, [c_void_p, POINTER(FxSolverStats)]),
     ("fx_sim_autotune", c_int32, [c_void_p, POINTER(FxAutotuneReport)]),
+    ("fx_sim_set_sweep_variants", c_int32, [c_void_p, POINTER(c_int32)]),
+    ("fx_sim_get_sweep_variants", c_int32, [c_void_p, POINTER(c_int32)]),
     ("fx_rollout_desc_default", None, [POINTER(FxRolloutDesc)]),
     ("fx_rollout_create", c_int32, [c_void_p, POINTER(FxRolloutDesc), POINTER(c_void_p)]),
     ("fx_rollout_destroy", None, [c_void_p]),

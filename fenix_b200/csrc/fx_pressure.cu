@@ -536,6 +536,83 @@ __global__ void __launch_bounds__(256) k_sweep_v2(Dims dm, const float* __restri
   }
 }
 
+// k_sweep with four consecutive x per thread (widths divisible by 4): a warp
+// covers 128 x, the column loads are float4, and one shuffle each way per voxel
+// row brings the outer x neighbours from the adjacent lanes. Each voxel's sum,
+// division and prolongation are those of k_sweep, in the same order, so the
+// results are the same bits.
+template <int ZB>
+__global__ void __launch_bounds__(256) k_sweep_v4(Dims dm, const float* __restrict__ div, const float* __restrict__ src, float* __restrict__ dst,
+                                                  Dims mid, const float* __restrict__ mid_p) {
+  const uint32_t lane = threadIdx.x;
+  const uint32_t x0 = blockIdx.x * 128 + 4 * lane, y = blockIdx.y * 8 + threadIdx.y, z0 = blockIdx.z * ZB;
+  if (y >= dm.h) return;  // whole warp
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  const bool xin = x0 < dm.w;  // dm.w % 4 == 0: x0 + 3 < dm.w too
+  const uint32_t base = (xin ? x0 : dm.w - 4) + dm.w * y;
+  const bool yint = y > 0 && y < dm.h - 1;
+  const int nz = min(ZB, (int)dm.d - (int)z0);
+  const float4* __restrict__ src4 = reinterpret_cast<const float4*>(src);
+  const float4* __restrict__ div4 = reinterpret_cast<const float4*>(div);
+  float4* __restrict__ dst4 = reinterpret_cast<float4*>(dst);
+  if (!yint) {
+    if (xin)
+      for (int k = 0; k < nz; ++k) dst4[(base + sz * (z0 + k)) >> 2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    return;
+  }
+  const bool int0 = x0 > 0, int3 = x0 + 3 < dm.w - 1;  // x0 + 1 and x0 + 2 are always interior
+  const bool left_end = lane == 0 && x0 > 0, right_end = lane == 31 && x0 + 4 < dm.w;
+  float4 c[ZB + 2], yp[ZB], ym[ZB], dv[ZB];
+  float xl_e[ZB], xr_e[ZB];
+  const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+  for (int k = 0; k < ZB + 2; ++k) {
+    const int z = (int)z0 + k - 1;
+    c[k] = (src && z >= 0 && z < (int)dm.d) ? __ldg(src4 + ((base + sz * (uint32_t)z) >> 2)) : zero4;
+  }
+#pragma unroll
+  for (int k = 0; k < ZB; ++k) {
+    const uint32_t z = min(z0 + k, dm.d - 1);
+    const uint32_t i = base + sz * z;
+    dv[k] = __ldg(div4 + (i >> 2));
+    yp[k] = src ? __ldg(src4 + ((i + sy) >> 2)) : zero4;
+    ym[k] = src ? __ldg(src4 + ((i - sy) >> 2)) : zero4;
+    xl_e[k] = (src && left_end) ? __ldg(src + i - 1) : 0.0f;
+    xr_e[k] = (src && right_end) ? __ldg(src + i + 4) : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < ZB; ++k) {
+    const float4 cm = c[k + 1];
+    float left = __shfl_up_sync(0xffffffffu, cm.w, 1);     // x0 - 1
+    float right = __shfl_down_sync(0xffffffffu, cm.x, 1);  // x0 + 4
+    if (left_end) left = xl_e[k];
+    if (right_end) right = xr_e[k];
+    const uint32_t z = z0 + k;
+    if (k >= nz || !xin) continue;
+    float4 v = zero4;
+    if (z > 0 && z < dm.d - 1) {
+      if (src) {
+        if (int0) v.x = div6(cm.y + left + yp[k].x + ym[k].x + c[k + 2].x + c[k].x - dv[k].x);
+        v.y = div6(cm.z + cm.x + yp[k].y + ym[k].y + c[k + 2].y + c[k].y - dv[k].y);
+        v.z = div6(cm.w + cm.y + yp[k].z + ym[k].z + c[k + 2].z + c[k].z - dv[k].z);
+        if (int3) v.w = div6(right + cm.z + yp[k].w + ym[k].w + c[k + 2].w + c[k].w - dv[k].w);
+      } else {
+        if (int0) v.x = div6(0.0f - dv[k].x);
+        v.y = div6(0.0f - dv[k].y);
+        v.z = div6(0.0f - dv[k].z);
+        if (int3) v.w = div6(0.0f - dv[k].w);
+      }
+      if (mid_p) {
+        if (int0) v.x = v.x + prolong_sample(mid, mid_p, (int)x0, (int)y, (int)z);
+        v.y = v.y + prolong_sample(mid, mid_p, (int)x0 + 1, (int)y, (int)z);
+        v.z = v.z + prolong_sample(mid, mid_p, (int)x0 + 2, (int)y, (int)z);
+        if (int3) v.w = v.w + prolong_sample(mid, mid_p, (int)x0 + 3, (int)y, (int)z);
+      }
+    }
+    dst4[(base + sz * z) >> 2] = v;
+  }
+}
+
 // The cleared buffer plus the prolongation (finePre = 0): boundary 0, interior 0 + sample.
 __global__ void __launch_bounds__(256) k_prolong_zero(Dims dm, float* __restrict__ dst, Dims mid, const float* __restrict__ mid_p) {
   const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 4 + threadIdx.y, z = blockIdx.z * 2 + threadIdx.z;
@@ -803,14 +880,19 @@ cudaError_t lean_div_first(cudaStream_t s, Dims dm, VelField v, float* div, floa
 
 bool sweep_variant_valid(int variant, Dims dm) {
   if (variant < 0 || variant >= kSweepVariants) return false;
+  if (variant >= SWEEP_VEC4_Z2) return dm.w % 4 == 0 && dm.w >= 8;
   return variant < SWEEP_VEC_Z2 || (dm.w % 2 == 0 && dm.w >= 4);
 }
 
+// The variant used when none was chosen: four x per thread at z-depth 2 where
+// the width allows (fastest on the 256^3 and 128^3 levels of plume_256), else two
+// x, else one. FENIX_SWEEP_VEC (0, 1, 2) caps the x per thread at 1, 2 or 4.
 int sweep_variant_default(Dims dm) {
   static const int zb = env_int("FENIX_SWEEP_ZB", 4, 1, 8);
-  static const int vec = env_int("FENIX_SWEEP_VEC", 1, 0, 1);
+  static const int vec = env_int("FENIX_SWEEP_VEC", 2, 0, 2);
   static const int vzb = env_int("FENIX_SWEEP_VEC_ZB", 2, 2, 4);
-  if (vec && sweep_variant_valid(SWEEP_VEC_Z2, dm)) return vzb <= 2 ? SWEEP_VEC_Z2 : SWEEP_VEC_Z4;
+  if (vec >= 2 && sweep_variant_valid(SWEEP_VEC4_Z2, dm)) return vzb <= 2 ? SWEEP_VEC4_Z2 : SWEEP_VEC4_Z4;
+  if (vec >= 1 && sweep_variant_valid(SWEEP_VEC_Z2, dm)) return vzb <= 2 ? SWEEP_VEC_Z2 : SWEEP_VEC_Z4;
   return zb <= 2 ? SWEEP_Z2 : (zb <= 4 ? SWEEP_Z4 : SWEEP_Z8);
 }
 
@@ -824,7 +906,10 @@ cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float
     case SWEEP_Z4: k_sweep<4><<<grid(32, 4), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
     case SWEEP_Z8: k_sweep<8><<<grid(32, 8), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
     case SWEEP_VEC_Z2: k_sweep_v2<2><<<grid(64, 2), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
-    default: k_sweep_v2<4><<<grid(64, 4), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
+    case SWEEP_VEC_Z4: k_sweep_v2<4><<<grid(64, 4), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
+    case SWEEP_VEC4_Z2: k_sweep_v4<2><<<grid(128, 2), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
+    case SWEEP_VEC4_Z4: k_sweep_v4<4><<<grid(128, 4), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
+    default: k_sweep_v4<1><<<grid(128, 1), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
   }
   return cudaGetLastError();
 }

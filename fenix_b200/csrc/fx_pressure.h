@@ -50,7 +50,17 @@ cudaError_t lean_sweep(cudaStream_t s, Dims dm, const float* div, const float* s
 // Sweep kernel variants (all give the same bits): one x per thread with z-depth
 // 2, 4 or 8, or two x per thread (even widths) with z-depth 2 or 4. An invalid
 // variant (-1, or a two-x variant on an odd width) takes the default.
-enum SweepVariant { SWEEP_Z2 = 0, SWEEP_Z4 = 1, SWEEP_Z8 = 2, SWEEP_VEC_Z2 = 3, SWEEP_VEC_Z4 = 4, kSweepVariants = 5 };
+enum SweepVariant {
+  SWEEP_Z2 = 0,
+  SWEEP_Z4 = 1,
+  SWEEP_Z8 = 2,
+  SWEEP_VEC_Z2 = 3,   // two x per thread (even widths)
+  SWEEP_VEC_Z4 = 4,
+  SWEEP_VEC4_Z2 = 5,  // four x per thread (widths divisible by 4)
+  SWEEP_VEC4_Z4 = 6,
+  SWEEP_VEC4_Z1 = 7,
+  kSweepVariants = 8
+};
 bool sweep_variant_valid(int variant, Dims dm);
 int sweep_variant_default(Dims dm);
 cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float* div, const float* src, float* dst, Dims mid,

@@ -1098,6 +1098,22 @@ fx_status fx_sim_get_solver(fx_sim* s, fx_solver_settings* o) {
   return FX_OK;
 }
 
+fx_status fx_sim_set_sweep_variants(fx_sim* s, const int32_t v[3]) {
+  if (!s || !v) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_sweep_variants: NULL argument");
+  for (int l = 0; l < 3; ++l)
+    if (v[l] != -1 && !sweep_variant_valid(v[l], s->lv[l].dm))
+      return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_sweep_variants: variant " + std::to_string(v[l]) +
+                                                         " does not fit level " + std::to_string(l));
+  for (int l = 0; l < 3; ++l) s->sweep_variant[l] = v[l];
+  return FX_OK;
+}
+
+fx_status fx_sim_get_sweep_variants(fx_sim* s, int32_t v[3]) {
+  if (!s || !v) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_sweep_variants: NULL argument");
+  for (int l = 0; l < 3; ++l) v[l] = s->sweep_variant[l] >= 0 ? s->sweep_variant[l] : sweep_variant_default(s->lv[l].dm);
+  return FX_OK;
+}
+
 fx_status fx_sim_autotune(fx_sim* s, fx_autotune_report* o) {
   if (!s || !o) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_autotune: NULL argument");
   if (s->kernels != FX_KERNELS_FUSED) return fail(s, FX_ERR_UNSUPPORTED, "fx_sim_autotune: the plain kernels have nothing to tune");

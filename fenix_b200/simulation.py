@@ -13,6 +13,8 @@ All arithmetic runs in libfenixcuda.so; this module only moves arguments.
 from __future__ import annotations
 
 import ctypes
+import json
+import os
 from typing import Any, Dict, Mapping, Optional, Sequence
 
 import numpy as np
@@ -292,12 +294,54 @@ class CombustionVolumeSimulation:
         check(self._lib.fx_sim_get_solver(self._h, ctypes.byref(st)), self._h)
         return solver_dict(st)
 
-    def autotune(self) -> Dict[str, Any]:
+    def autotune(self, cache: Optional[str] = None, key: Optional[str] = None) -> Dict[str, Any]:
         """Times the pressure sweep kernels on this grid's levels and keeps the
-        fastest per level (same results; waits for the stream)."""
+        fastest per level (same results; waits for the stream).
+
+        With `cache` (a JSON file path) the result is stored under `key`
+        (default: the current CUDA device's name and the grid size) and reused
+        by later calls instead of timing again."""
+        table: Dict[str, Any] = {}
+        if cache:
+            key = key or self._tune_key()
+            try:
+                with open(cache) as f:
+                    table = json.load(f)
+            except (OSError, ValueError):
+                table = {}
+            if key in table:
+                self.setSweepVariants(table[key]["sweepVariant"])
+                return {**table[key], "cached": True}
         r = _lib.FxAutotuneReport()
         check(self._lib.fx_sim_autotune(self._h, ctypes.byref(r)), self._h)
-        return {"sweepVariant": list(r.sweep_variant), "sweepUs": list(r.sweep_us), "defaultUs": list(r.default_us)}
+        rep = {"sweepVariant": list(r.sweep_variant), "sweepUs": list(r.sweep_us), "defaultUs": list(r.default_us)}
+        if cache:
+            table[key] = rep
+            tmp = f"{cache}.{os.getpid()}.tmp"
+            with open(tmp, "w") as f:
+                json.dump(table, f, indent=1)
+            os.replace(tmp, cache)
+        return rep
+
+    def _tune_key(self) -> str:
+        try:
+            import torch
+
+            name = torch.cuda.get_device_name(torch.cuda.current_device())
+        except Exception:  # pragma: no cover - no torch / no device name
+            name = "cuda"
+        r = self.resolution
+        return f"{name}|{r['width']}x{r['height']}x{r['depth']}"
+
+    def setSweepVariants(self, variants: Sequence[int]) -> None:
+        """The sweep kernel per pressure level (fine, mid, coarse); -1 keeps the default."""
+        arr = (ctypes.c_int32 * 3)(*[int(v) for v in variants])
+        check(self._lib.fx_sim_set_sweep_variants(self._h, arr), None)
+
+    def getSweepVariants(self) -> list:
+        arr = (ctypes.c_int32 * 3)()
+        check(self._lib.fx_sim_get_sweep_variants(self._h, arr), None)
+        return list(arr)
 
     def readSolverStats(self) -> Dict[str, Any]:
         """FP64 statistics of the latest solve (waits for the stream)."""

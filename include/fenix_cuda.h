@@ -344,12 +344,19 @@ fx_status fx_sim_read_solver_stats(fx_sim* sim, fx_solver_stats* out);
  * non-current fine buffer and the mid/coarse levels, which every solve
  * rewrites from zero). */
 typedef struct fx_autotune_report {
-  int32_t sweep_variant[3]; /* chosen variant per level (0..4) */
+  int32_t sweep_variant[3]; /* chosen variant per level (0..7) */
   float sweep_us[3];        /* its time per sweep */
   float default_us[3];      /* the default variant's time per sweep */
 } fx_autotune_report;
 
 fx_status fx_sim_autotune(fx_sim* sim, fx_autotune_report* out);
+/* Sets the sweep variant of each level directly (a cached autotuning result):
+ * -1 keeps the default; a variant that does not fit the level's width is
+ * FX_ERR_INVALID_ARGUMENT. Variants: 0-2 one x per thread at z-depth 2/4/8,
+ * 3-4 two x per thread (even widths) at z-depth 2/4, 5-7 four x per thread
+ * (widths divisible by 4) at z-depth 2/4/1. */
+fx_status fx_sim_set_sweep_variants(fx_sim* sim, const int32_t variants[3]);
+fx_status fx_sim_get_sweep_variants(fx_sim* sim, int32_t variants[3]);
 
 /* Batches (extension; the reference steps one simulation per device): many
  * independent simulations, each with its own options (sizes may differ), stepped
