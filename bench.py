@@ -66,7 +66,7 @@ KERNEL_BYTES = {
 # storage (profiles/fused_step_plume256_f16_launches.md), per kernel of the
 # fused path, for roofline.traffic.
 NCU_TRAFFIC = {
-    "fused_sweep": 174.7e6,
+    "fused_sweep": 170.6e6,
     "fused_advect_velocity": 360.8e6,
     "fused_advect_scalars": 109.5e6,
     "fused_combustion": 50.7e6,
