@@ -69,7 +69,29 @@ FX_DEV float clamp01(float x) { return clampv(x, 0.0f, 1.0f); }
 FX_DEV float mixv(float a, float b, float t) { return a * (1.0f - t) + b * t; }
 FX_DEV float fractv(float x) { return x - floorf(x); }
 FX_DEV float stepv(float e, float x) { return x >= e ? 1.0f : 0.0f; }
+// x / c rounded to nearest for a constant divisor c, by Markstein's correction
+// of the product with r = RN(1/c) ("IA-64 and Elementary Functions", 2000):
+// q0 = x r, q = fma(fma(-q0, c, x), r, q0). For every divisor smoothstepv meets
+// in these kernels (the difference of its two literal edges), an exhaustive
+// check over 2^-100 <= |x| <= 2^100 shows q equals the IEEE quotient
+// (tests/native/divconst_check.c, run by tests/test_exact_division.py); other x
+// take the IEEE division. With literal edges c and r fold at compile time.
+FX_DEV float div_const(float x, float c) {
+  const float r = 1.0f / c;
+  const float ax = fabsf(x);
+  if (ax >= 0x1p-100f && ax <= 0x1p100f) {
+    const float q0 = x * r;
+    return fmaf(fmaf(-q0, c, x), r, q0);
+  }
+  return x / c;
+}
+// smoothstep with literal edges (their difference is a verified divisor).
 FX_DEV float smoothstepv(float e0, float e1, float x) {
+  const float t = clampv(div_const(x - e0, e1 - e0), 0.0f, 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+// smoothstep with edges computed at run time (IEEE division).
+FX_DEV float smoothstep_dyn(float e0, float e1, float x) {
   const float t = clampv((x - e0) / (e1 - e0), 0.0f, 1.0f);
   return t * t * (3.0f - 2.0f * t);
 }
@@ -220,7 +242,7 @@ FX_DEV float eruptive_falloff(const Params& P, float px, float py, float pz, flo
   const float fine = emitter_noise(px + (-age) * 0.33f, py + age * 0.21f, pz + (-age) * 0.15f, 18.0f, seed + 41.0f);
   const float lobe = clampv(coarse * 0.72f + fine * 0.28f, 0.0f, 1.0f);
   const float reach = target * growth * mixv(0.62f, 1.0f, smoothstepv(0.2f, 0.92f, lobe));
-  const float front = 1.0f - smoothstepv(reach - feather, reach + feather, dist);
+  const float front = 1.0f - smoothstep_dyn(reach - feather, reach + feather, dist);
   const float core_radius = mx(target * (0.18f + growth * 0.38f), feather);
   const float core = sphere_falloff(dist, core_radius, falloff) * (1.0f - growth * 0.35f);
   const float body = sphere_falloff(dist, mx(reach + feather, feather), falloff) * front;
