@@ -31,7 +31,9 @@ def check(status: int, sim_handle) -> None:
 
 
 class Rollout:
-    """K steps of `sim` (plain kernels, f32 storage) from its current state."""
+    """K steps of `sim` (f32 storage) from its current state. With the fused
+    kernels the forward and the recomputed steps run fused (the same bits); the
+    adjoint differentiates the plain step either way."""
 
     def __init__(self, sim: CombustionVolumeSimulation, steps: int = 64, checkpoint_interval: int = 8, step_seconds: float = 1.0 / 60.0,
                  start_elapsed: float = 0.0, patch: Optional[Mapping[str, int]] = None):

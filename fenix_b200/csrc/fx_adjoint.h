@@ -12,12 +12,6 @@
 
 namespace fx {
 
-// The inflow patch: velocity.y at (x0 + i, y, z0 + k) is set to values[i + nx k]
-// after inject-velocity (an extension with no counterpart in the reference).
-struct InflowPatch {
-  uint32_t x0, y, z0, nx, nz;
-};
-void plain_inflow(cudaStream_t s, Dims dm, InflowPatch p, const float* values, VelField v);
 
 // loss += sum (d - target)^2 in FP64 (loss is a device double; each difference is
 // formed in FP64); lam_d = 2 (d - target) rounded to f32 (when lam_d is not NULL).

@@ -952,6 +952,9 @@ uint64_t fused_key(const FusedStep& st, uint32_t ninj) {
   mix_key((uint64_t)st.solver_mode);
   for (int l = 0; l < 3; ++l) mix_key((uint64_t)(st.sweep_variant[l] + 1));
   mix_key(st.solver_norms);
+  mix_key((uint64_t)(uintptr_t)st.inflow);
+  if (st.inflow)
+    for (uint32_t v : {st.inflow_patch.x0, st.inflow_patch.y, st.inflow_patch.z0, st.inflow_patch.nx, st.inflow_patch.nz}) mix_key(v);
   if (st.solver_mode == 1) {
     const VCycleConfig& c = st.vc;
     for (int v : {c.levels, c.pre, c.post, c.coarse, c.max_cycles, (int)c.warm, (int)c.omega_one}) mix_key((uint64_t)v);
@@ -1101,6 +1104,14 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       k_inject<S><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.sources, st.nsrc, w.list_inj, c_inj, sset<S>(st.cur), st.vcur,
                                                        w.summary_set[cur], w.nz_set[cur]);
     });
+    ++launches;
+  }
+
+  // The inflow patch after injection; its values are not bounded by the recorded
+  // max |v|, so the velocity advection clamps on read in this step.
+  if (st.inflow) {
+    plain_inflow(s, dm, st.inflow_patch, st.inflow, st.vcur);
+    FX_CK(cudaMemsetAsync(w.vmax, 0xFF, sizeof(unsigned), s));
     ++launches;
   }
 

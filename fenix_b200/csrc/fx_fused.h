@@ -75,6 +75,8 @@ struct FusedWork {
 
 struct FusedStep {
   cudaStream_t stream;
+  const float* inflow = nullptr;  // device values of the inflow patch (NULL: none)
+  InflowPatch inflow_patch{};
   Dims dm;
   uint3 bricks;
   const Params* params;

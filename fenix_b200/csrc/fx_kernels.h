@@ -44,6 +44,14 @@ void plain_prolong(cudaStream_t s, Dims coarse, Dims fine, const float* coarse_p
 void plain_project(cudaStream_t s, Dims dm, VelField vsrc, const float* p, VelField vdst);
 void plain_velocity_magnitude(cudaStream_t s, Dims dm, VelField v, float* out);
 
+// The inflow patch of the differentiable rollout (an extension with no
+// counterpart in the reference): velocity.y at (x0 + i, y, z0 + k) is set to
+// values[i + nx k] after inject-velocity (fx_adjoint.cu).
+struct InflowPatch {
+  uint32_t x0, y, z0, nx, nz;
+};
+void plain_inflow(cudaStream_t s, Dims dm, InflowPatch p, const float* values, VelField v);
+
 // Pinned sin/cos over an array (tests compare it with the oracle bit for bit).
 void pinned_sincos_array(cudaStream_t s, const float* x, float* out, uint32_t n, int cosine);
 

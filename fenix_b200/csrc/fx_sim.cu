@@ -1450,6 +1450,11 @@ struct fx_rollout {
   float* lam_div[3]{};
   bool have_target = false;
   bool forward_done = false;
+  // The untaped steps (the forward and the segment recomputation) run the fused
+  // step when the simulation has the fused kernels and every inflow value is
+  // within the speed limit (the fused velocity advection clamps on read, where
+  // the plain step leaves the inflow values as they are); both give the same bits.
+  bool fused_steps = false;
 };
 
 namespace {
@@ -1460,8 +1465,7 @@ namespace {
 fx_status rollout_check(fx_rollout* r) {
   fx_sim* s = r->s;
   if (!s->err.empty()) return fail(nullptr, FX_ERR_STATE, "fx_rollout: the simulation has an error: " + s->err);
-  if (s->kernels != FX_KERNELS_PLAIN || s->half)
-    return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_rollout: the simulation must use the plain kernels with f32 storage");
+  if (s->half) return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_rollout: the simulation must use f32 storage");
   if (s->solver.mode != FX_SOLVER_REFERENCE || s->advect_mode != FX_ADVECT_MACCORMACK)
     return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_rollout: needs the reference pressure schedule and MacCormack advection");
   if (s->qi[0] != 1 || s->qi[1] != 1)
@@ -1492,6 +1496,8 @@ fx_status save_state(fx_rollout* r, float* dst, HostState& h) {
 
 fx_status restore_state(fx_rollout* r, const float* src, const HostState& h) {
   fx_sim* s = r->s;
+  // the fused path's per-brick bookkeeping is rebuilt from the restored fields
+  if (s->kernels == FX_KERNELS_FUSED) fused_invalidate(s->fw, s->stream);
   s->cur = h.cur;
   s->step_index = h.step_index;
   s->initialized = h.initialized;
@@ -1511,7 +1517,25 @@ fx_status rollout_step(fx_rollout* r, uint32_t k, const PlainHooks& hk) {
   StepPlan sp;
   fx_status st = step_begin(s, elapsed, r->d.step_seconds, sp);
   if (st != FX_OK) return st;
-  return step_finish(s, step_plain(s, sp.vort_on, sp.pressure_on, sp.debug_on, &hk), nullptr, sp, elapsed);
+  const bool taped = hk.t1 || hk.r1 || hk.v1.c[0] || hk.a.c[0] || hk.b.c[0];
+  if (r->fused_steps && !taped) {
+    sp.fs.inflow = hk.inflow;
+    sp.fs.inflow_patch = hk.patch;
+    FusedResult fr;
+    st = fused_step(s->fw, sp.fs, fr);
+    if (st != FX_OK) fail(s, st, "fx_rollout: fused step failed: " + fr.error);
+    return step_finish(s, st, &fr, sp, elapsed);
+  }
+  st = step_finish(s, step_plain(s, sp.vort_on, sp.pressure_on, sp.debug_on, &hk), nullptr, sp, elapsed);
+  if (s->kernels == FX_KERNELS_FUSED) fused_invalidate(s->fw, s->stream);
+  return st;
+}
+
+// The speed limit of the step uniform (speed_limit in fx_math.cuh), in the same
+// f32 operations.
+float speed_limit_of(const fx_sim* s) {
+  const float dx = (float)(s->rp.world_size / (double)std::max(s->dm.w, s->dm.d));
+  return 80.0f / (dx < 0.001f ? 0.001f : dx);
 }
 
 // PressureSolvePass.smooth (:129-143) in reverse.
@@ -1715,6 +1739,10 @@ fx_status fx_rollout_forward(fx_rollout* r, const float* inflow, double* loss) {
   r->forward_done = false;
   if (r->npatch)
     FX_CUDA(s, cudaMemcpyAsync(r->inflow, inflow, r->npatch * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  r->fused_steps = s->kernels == FX_KERNELS_FUSED;
+  const float lim = speed_limit_of(s);
+  for (uint32_t k = 0; k < r->npatch; ++k)
+    if (inflow[k] < -lim || inflow[k] > lim) r->fused_steps = false;
   PlainHooks hk;
   hk.inflow = r->npatch ? r->inflow : nullptr;
   hk.patch = r->patch;

@@ -475,14 +475,17 @@ fx_status fx_bloom_render(fx_bloom* pass, const void* hdr, int32_t hdr_format, u
                           const fx_bloom_params* params, void* out, int32_t out_format, void* stream);
 
 /* Differentiable rollout: an extension with no counterpart in the reference.
- * K plain FP32 steps of a simulation (FX_KERNELS_PLAIN, f32 storage, the
- * reference pressure schedule, MacCormack advection, pressure and vorticity
- * intervals of 1) from its current state, with a control patch of per-voxel
+ * K FP32 steps of a simulation (f32 storage, the reference pressure schedule,
+ * MacCormack advection, pressure and vorticity intervals of 1) from its current
+ * state, with a control patch of per-voxel
  * inflow velocity: after inject-velocity, every step sets velocity.y at
  * (inflow_x0 + i, inflow_y, inflow_z0 + k) to inflow[i + inflow_nx * k]. The loss
  * is sum over voxels of (density_K - target)^2 (FP64 accumulation). Step k runs
  * at elapsed = start_elapsed + k * step_seconds with step = step_seconds.
  *
+ * The adjoint differentiates the plain step; with FX_KERNELS_FUSED the forward
+ * and the recomputed steps run the fused kernels, which give the same bits
+ * (unless an inflow value exceeds the speed limit, when every step is plain).
  * fx_rollout_forward leaves the simulation in its final state and keeps a state
  * checkpoint every checkpoint_interval steps; fx_rollout_backward returns the
  * gradient of the loss with respect to the inflow values and the initial

@@ -26,8 +26,8 @@ def rel(got: float, want: float, scale: float) -> float:
     return abs(got - want) / max(abs(want), 1e-3 * scale)
 
 
-def run_rollout(aw, every=None):
-    sim = createCombustionVolumeSimulation(aw.workload.options, device=0, kernels="plain")
+def run_rollout(aw, every=None, fused=False):
+    sim = createCombustionVolumeSimulation(aw.workload.options, device=0, kernels="fused" if fused else "plain")
     sim.updateSources(aw.workload.sources)
     ro = Rollout(sim, steps=aw.steps, checkpoint_interval=every or aw.checkpoint_interval, patch=aw.patch)
     ro.setTarget(aw.target)
@@ -138,12 +138,39 @@ def test_full_size_gradient_against_the_fixture():
     assert worst_fd <= 1e-3
 
 
+def test_fused_simulation_gives_the_same_rollout(rolled):
+    """The fused kernels run the forward and the recomputed steps: the final
+    state and loss are the plain rollout's bits, and the gradient is the same
+    up to the order of the adjoint's float atomics."""
+    sim, ro, loss, final, gi, gv = rolled
+    fsim, fro, floss, ffinal, fgi, fgv = run_rollout(AW, fused=True)
+    assert floss == loss
+    for k, v in final.items():
+        np.testing.assert_array_equal(ffinal[k], v, err_msg=k)
+    np.testing.assert_allclose(fgi, gi, rtol=1e-4, atol=1e-6 * float(np.abs(gi).max()))
+    np.testing.assert_allclose(fgv.reshape(3, -1), gv.reshape(3, -1), rtol=1e-3, atol=1e-5 * float(np.abs(gv).max()))
+    # an inflow value beyond the speed limit keeps every step plain, with the same result as the plain rollout
+    big = AW.inflow.copy()
+    big[0, 0] = 5000.0
+    start_from(fsim, AW.workload.state)
+    lf = fro.forward(big)
+    psim = createCombustionVolumeSimulation(AW.workload.options, device=0, kernels="plain")
+    psim.updateSources(AW.workload.sources)
+    pro = Rollout(psim, steps=AW.steps, checkpoint_interval=AW.checkpoint_interval, patch=AW.patch)
+    pro.setTarget(AW.target)
+    start_from(psim, AW.workload.state)
+    assert pro.forward(big) == lf
+    for r_, s_ in ((fro, fsim), (pro, psim)):
+        r_.dispose()
+        s_.dispose()
+
+
 def test_rollout_rejects_unsupported_simulations():
     opts = AW.workload.options
-    fused = createCombustionVolumeSimulation(opts, device=0)
-    with pytest.raises(FenixError, match="plain"):
-        Rollout(fused, steps=4, patch=AW.patch)
-    fused.dispose()
+    half = createCombustionVolumeSimulation(opts, device=0, storage="f16")
+    with pytest.raises(FenixError, match="f32"):
+        Rollout(half, steps=4, patch=AW.patch)
+    half.dispose()
     plain = createCombustionVolumeSimulation(opts, device=0, kernels="plain")
     with pytest.raises(FenixError, match="grid"):
         Rollout(plain, steps=4, patch={"x0": 30, "y": 1, "z0": 0, "nx": 8, "nz": 8})
