@@ -140,11 +140,11 @@ def test_full_size_gradient_against_the_fixture():
 
 def test_fused_simulation_gives_the_same_rollout(rolled):
     """The fused kernels run the forward and the recomputed steps: the final
-    state and loss are the plain rollout's bits, and the gradient is the same
-    up to the order of the adjoint's float atomics."""
+    state is the plain rollout's bits, the loss equals it up to the order of the
+    FP64 atomic sum, and the gradient up to the order of the float atomics."""
     sim, ro, loss, final, gi, gv = rolled
     fsim, fro, floss, ffinal, fgi, fgv = run_rollout(AW, fused=True)
-    assert floss == loss
+    assert abs(floss - loss) <= 1e-12 * loss
     for k, v in final.items():
         np.testing.assert_array_equal(ffinal[k], v, err_msg=k)
     np.testing.assert_allclose(fgi, gi, rtol=1e-4, atol=1e-6 * float(np.abs(gi).max()))
@@ -159,7 +159,8 @@ def test_fused_simulation_gives_the_same_rollout(rolled):
     pro = Rollout(psim, steps=AW.steps, checkpoint_interval=AW.checkpoint_interval, patch=AW.patch)
     pro.setTarget(AW.target)
     start_from(psim, AW.workload.state)
-    assert pro.forward(big) == lf
+    assert abs(pro.forward(big) - lf) <= 1e-12 * lf
+    np.testing.assert_array_equal(psim.readField("density"), fsim.readField("density"))
     for r_, s_ in ((fro, fsim), (pro, psim)):
         r_.dispose()
         s_.dispose()
