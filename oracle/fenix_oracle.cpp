@@ -20,6 +20,10 @@
 //                   for bit. This instantiation is also the timed CPU baseline.
 //   Real = double : the accuracy reference (libm sin/cos), used to state the f32
 //                   and f16-storage error of the CUDA path.
+//   Real = Tan, Tan32 : tangent numbers (FP64 values, or f32 values on the f32
+//                   trajectory bit for bit, each with an FP64 directional
+//                   derivative): the exact derivative of the restatement along a
+//                   seeded direction, the reference for the CUDA adjoint.
 // Either instantiation can store the scalar sets in binary16 (orc_set_half_storage):
 // each value a reference pass writes to density, temperature, fuel or reaction is
 // rounded to the nearest binary16, ties to even, as the CUDA FP16-storage path does.
