@@ -181,6 +181,18 @@ def dist_setup():
     return world, rank, local
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), for the baseline records."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def run_reference(args):
     """The reference's step on the host CPU (the f32 restatement, all threads)."""
     world, rank, _ = dist_setup()
@@ -211,7 +223,8 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"plume_{args.size} (four floor plumes, {args.size}^3, 4/4/4/4/20 sweeps, dt 1/60)",
                    "global_batch": 1, "seq_len": 0, "parallelism": "cpu"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": num_threads(), "kind": "port",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": num_threads(), "kind": "port", "cpu_model": cpu_model(),
+                         "nproc": os.cpu_count(),
                          "sample": f"{args.steps} full steps of plume_{args.size} after {args.warmup} warm-up steps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -241,18 +254,17 @@ def cpu_baseline_and_parity(args, wl, counts, kernels, storage):
     for s in set(everyone):
         s.updateSources(wl.sources)
         workloads.load_state(s, wl.state)
-    active = 0
-    el = 0.0
+    per_step = []
     parity = True
     for k in range(args.cpu_steps):
         t0 = time.perf_counter()
         orc.step(k * wl.dt, wl.dt)
-        el += time.perf_counter() - t0
+        dt_s = time.perf_counter() - t0
         for s in (orc64, sim, sim32) + (() if orc_same is orc else (orc_same,)):
             if s is not None:
                 s.step(k * wl.dt, wl.dt)
         flags = orc.readField("brick_flags")
-        active += int(counts[flags != 0].sum())
+        per_step.append(int(counts[flags != 0].sum()) / dt_s)
         for name in PARITY_FIELDS:
             a, b = sim.readField(name), orc_same.readField(name)
             if not np.array_equal(a.view(np.uint32), b.view(np.uint32)):
@@ -271,8 +283,10 @@ def cpu_baseline_and_parity(args, wl, counts, kernels, storage):
     for s in set(everyone):
         s.dispose()
     return {
-        "value": active / el, "unit": UNIT, "cores": num_threads(), "kind": "port",
-        "sample": f"{args.cpu_steps} full steps of the same workload from the same start state (f32 restatement, OpenMP)",
+        "value": float(np.median(per_step)), "unit": UNIT, "cores": num_threads(), "kind": "port", "cpu_model": cpu_model(),
+        "nproc": os.cpu_count(), "per_step": [round(v) for v in per_step],
+        "sample": f"{args.cpu_steps} full steps of the same workload from the same start state (f32 restatement, OpenMP); "
+                  "value = median of the per-step rates",
     }, {"steps": args.cpu_steps, "bit_exact_vs_oracle": parity, "oracle": f"f32 arithmetic, {storage} storage"}, {
         "steps": args.cpu_steps, "against": "f64 oracle (same start state and steps)", "fields": err}
 
