@@ -19,6 +19,7 @@
 //    neighbour read sees the state before the pass.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -312,17 +313,19 @@ FX_DEV float tri_interp_clamped(const float* __restrict__ f, const Tri& c, float
 // the trilinear mix is 0, so the mix equals the voxel's own (clamped) value up to
 // the sign of a zero, and c - v*dt comes out the same (c >= 0.5). For fields
 // without NaN this reads one value instead of eight.
-constexpr int kAdvZ = 4;
+// Voxels per thread along z (one: measured fastest on the 256^3 plume, 170 against
+// 179 us for four; FENIX_ADV_Z = 2, 4 or 8 selects the others, with the same bits).
+constexpr int kAdvZ = 1;
 
 // The clamp is the identity on every value when the largest |v| of the field is
 // within the limit: `vmax` holds that bound (float bits, written by the
 // projection that produced the field; all ones when unknown), and the kernel
 // then reads the values as they are, with the same results.
-template <bool CLAMP>
+template <bool CLAMP, int ZB>
 FX_DEV void advect_velocity_column(Dims dm, uint32_t x, uint32_t y, uint32_t z0, float dt, float lim, float damp, bool xyint,
                                    const VelField& src, const VelField& dst) {
 #pragma unroll
-  for (int k = 0; k < kAdvZ; ++k) {
+  for (int k = 0; k < ZB; ++k) {
     const uint32_t z = z0 + k;
     if (z >= dm.d) break;
     const uint32_t i = flat(dm, x, y, z);
@@ -353,16 +356,17 @@ FX_DEV void advect_velocity_column(Dims dm, uint32_t x, uint32_t y, uint32_t z0,
   }
 }
 
+template <int ZB>
 __global__ void __launch_bounds__(256) k_advect_velocity(Dims dm, const Params* __restrict__ Pp, VelField src, VelField dst,
                                                          const unsigned* __restrict__ vmax) {
-  const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z0 = blockIdx.z * kAdvZ;
+  const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z0 = blockIdx.z * ZB;
   if (x >= dm.w || y >= dm.h) return;
   const float dt = Pp->dt;
   const float lim = speed_limit(*Pp);
   const float damp = 1.0f - dt * 0.025f;
   const bool xyint = x > 0 && y > 0 && x < dm.w - 1 && y < dm.h - 1;
-  if (__uint_as_float(__ldg(vmax)) <= lim) advect_velocity_column<false>(dm, x, y, z0, dt, lim, damp, xyint, src, dst);
-  else advect_velocity_column<true>(dm, x, y, z0, dt, lim, damp, xyint, src, dst);
+  if (__uint_as_float(__ldg(vmax)) <= lim) advect_velocity_column<false, ZB>(dm, x, y, z0, dt, lim, damp, xyint, src, dst);
+  else advect_velocity_column<true, ZB>(dm, x, y, z0, dt, lim, damp, xyint, src, dst);
 }
 
 // -------------------------------------------------------------- scalar advection
@@ -1125,8 +1129,18 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   // 3. velocity advection (dense)
   {
     Timed tm(w, s, "fused_advect_velocity");
-    k_advect_velocity<<<dim3((dm.w + 31) / 32, (dm.h + 7) / 8, (dm.d + kAdvZ - 1) / kAdvZ), dim3(32, 8, 1), 0, s>>>(dm, st.params, st.vcur, st.vscr,
-                                                                                                                 w.vmax);
+    static const int zb = [] {
+      const char* v = std::getenv("FENIX_ADV_Z");
+      return v && *v ? std::atoi(v) : kAdvZ;
+    }();
+    const dim3 blk(32, 8, 1);
+    auto grid = [&](int z) { return dim3((dm.w + 31) / 32, (dm.h + 7) / 8, (dm.d + z - 1) / z); };
+    switch (zb) {
+      case 2: k_advect_velocity<2><<<grid(2), blk, 0, s>>>(dm, st.params, st.vcur, st.vscr, w.vmax); break;
+      case 8: k_advect_velocity<8><<<grid(8), blk, 0, s>>>(dm, st.params, st.vcur, st.vscr, w.vmax); break;
+      case 4: k_advect_velocity<4><<<grid(4), blk, 0, s>>>(dm, st.params, st.vcur, st.vscr, w.vmax); break;
+      default: k_advect_velocity<kAdvZ><<<grid(kAdvZ), blk, 0, s>>>(dm, st.params, st.vcur, st.vscr, w.vmax); break;
+    }
     ++launches;
   }
   // 4. scalar advection over the list
