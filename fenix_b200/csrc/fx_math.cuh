@@ -106,20 +106,27 @@ struct Dims {
 FX_DEV uint32_t flat(const Dims& dm, uint32_t x, uint32_t y, uint32_t z) { return x + dm.w * (y + dm.h * z); }
 FX_DEV uint32_t dec(uint32_t v) { return v == 0u ? 0u : v - 1u; }
 FX_DEV uint32_t inc(uint32_t v, uint32_t m) { return min(v + 1u, m); }
-// x / 6 rounded to nearest, for every float x. For |x| in [2^-125, FLT_MAX] the
-// quotient is q0 = x * RN(1/6) corrected once by its exact residual (Markstein,
-// "IA-64 and Elementary Functions", 2000): r = fma(-q0, 6, x), q = fma(r, RN(1/6), q0).
-// An exhaustive check over all 2^32 inputs shows this equals the IEEE quotient on
-// that range; tiny, infinite and NaN inputs take the IEEE division.
+// x / 6 rounded to nearest, for every float x, without a division. For |x| in
+// [2^-125, FLT_MAX] the quotient is q0 = x * RN(1/6) corrected once by its exact
+// residual (Markstein, "IA-64 and Elementary Functions", 2000):
+// e = fma(-q0, 6, x), q = fma(e, RN(1/6), q0). Nonzero |x| below 2^-125 runs the
+// same correction in f64, where x is far from the subnormal range, and rounds the
+// f64 quotient to float once; rounding twice, first to 53 bits, gives the same
+// float because 53 >= 2 * 24 + 2 (Figueroa, "When is double rounding
+// innocuous?", 1995). For +-0, +-inf and NaN, q0 itself is the quotient. An
+// exhaustive check over all 2^32 inputs compares the result with the IEEE
+// quotient. Having no division keeps a slow path and its call out of the sweep
+// kernels, whose pressure tails reach the subnormal range.
 FX_DEV float div6(float x) {
   const float ax = fabsf(x);
-  if (ax >= 0x1p-125f && ax <= 0x1.fffffep127f) {
-    const float r6 = 0x1.555556p-3f;  // RN(1/6)
-    const float q0 = x * r6;
-    const float e = fmaf(-q0, 6.0f, x);
-    return fmaf(e, r6, q0);
-  }
-  return x / 6.0f;
+  const float r6 = 0x1.555556p-3f;  // RN(1/6)
+  const float q0 = x * r6;
+  if (ax >= 0x1p-125f && ax <= 0x1.fffffep127f) return fmaf(fmaf(-q0, 6.0f, x), r6, q0);
+  if (!(ax > 0.0f && ax < 0x1p-125f)) return q0;  // +-0, +-inf, NaN
+  const double r = 0x1.5555555555555p-3;  // RN(1/6) in f64
+  const double xd = (double)x;
+  const double p0 = xd * r;
+  return (float)fma(fma(-p0, 6.0, xd), r, p0);
 }
 
 FX_DEV bool is_boundary(const Dims& dm, uint32_t x, uint32_t y, uint32_t z) {

@@ -398,6 +398,135 @@ __global__ void __launch_bounds__(256) k_div_first(Dims dm, VelField v, float* _
   }
 }
 
+// k_div_first with four x per thread marching runs of planes (widths divisible
+// by 4, even heights and depths; runs of even length starting on even planes).
+// Per plane a thread loads one float4 of vx (the x neighbours by warp shuffle,
+// the row ends load theirs), two of vy (rows y - 1 and y + 1) and one of vz
+// (plane z + 1; planes z - 1 and z are held from the earlier planes), issuing
+// the next plane's loads before it computes the current one. The restriction
+// adds each 2x2x2 group in k_div_first's order: the even row's warp sums plane
+// 2m (its row, then the odd row's from shared memory) and carries the partial
+// sum to plane 2m + 1. Every value is computed with the same operations in the
+// same order, so the results are the same bits.
+__global__ void __launch_bounds__(256, 4) k_div_march(Dims dm, VelField v, float* __restrict__ div, float* __restrict__ p1, Dims mid,
+                                                      float* __restrict__ mid_div, int restrict_mid, int run) {
+  __shared__ float4 srow[2][8][32];  // this plane's divergence rows of the block, double-buffered by plane parity
+  const uint32_t lane = threadIdx.x, ty = threadIdx.y;
+  const uint32_t x0 = blockIdx.x * 128 + 4 * lane, y = blockIdx.y * 8 + ty;
+  const int zb = (int)blockIdx.z * run, ze = min(zb + run, (int)dm.d);
+  if (zb >= ze) return;  // whole block
+  const int D = (int)dm.d;
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  const bool yin = y < dm.h;
+  const bool xin = x0 < dm.w;  // dm.w % 4 == 0: x0 + 3 < dm.w too
+  const uint32_t base = (xin ? x0 : dm.w - 4) + dm.w * (yin ? y : dm.h - 1);
+  const bool yint = yin && y > 0 && y < dm.h - 1;
+  const bool int0 = x0 > 0, int3 = x0 + 3 < dm.w - 1;  // x0 + 1 and x0 + 2 are interior in x
+  const bool left_end = lane == 0 && x0 > 0, right_end = lane == 31 && x0 + 4 < dm.w;
+  const float4* __restrict__ vx4 = reinterpret_cast<const float4*>(v.c[0]);
+  const float4* __restrict__ vy4 = reinterpret_cast<const float4*>(v.c[1]);
+  const float4* __restrict__ vz4 = reinterpret_cast<const float4*>(v.c[2]);
+  const float* __restrict__ vx = v.c[0];
+  float4* __restrict__ div4 = reinterpret_cast<float4*>(div);
+  float4* __restrict__ p14 = reinterpret_cast<float4*>(p1);
+  const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  // vz row at a plane (zero outside the grid and on boundary rows, which never use it)
+  auto vzrow = [&](int z) { return (yint && z >= 0 && z < D) ? __ldg(vz4 + ((base + sz * (uint32_t)z) >> 2)) : zero4; };
+  float4 vzm = vzrow(zb - 1), vzc = vzrow(zb), vzp = vzrow(zb + 1);
+  float4 X = zero4, YP = zero4, YM = zero4;
+  float XL = 0.0f, XR = 0.0f;
+  {
+    const uint32_t i = base + sz * (uint32_t)zb;
+    if (yint) {
+      X = __ldg(vx4 + (i >> 2));
+      YP = __ldg(vy4 + ((i + sy) >> 2));
+      YM = __ldg(vy4 + ((i - sy) >> 2));
+      if (left_end) XL = __ldg(vx + i - 1);
+      if (right_end) XR = __ldg(vx + i + 4);
+    }
+  }
+  float part0 = 0.0f, part1 = 0.0f;  // restriction sums of mid x = x0/2 and x0/2 + 1 (even rows)
+  for (int z = zb; z < ze; ++z) {
+    // next plane's loads (clamped in range on the last plane, values then unused)
+    const int zn = min(z + 1, D - 1);
+    const uint32_t in = base + sz * (uint32_t)zn;
+    float4 nX = zero4, nYP = zero4, nYM = zero4;
+    float nXL = 0.0f, nXR = 0.0f;
+    if (yint) {
+      nX = __ldg(vx4 + (in >> 2));
+      nYP = __ldg(vy4 + ((in + sy) >> 2));
+      nYM = __ldg(vy4 + ((in - sy) >> 2));
+      if (left_end) nXL = __ldg(vx + in - 1);
+      if (right_end) nXR = __ldg(vx + in + 4);
+    }
+    const float4 nvz = vzrow(z + 2);
+    float left = __shfl_up_sync(0xffffffffu, X.w, 1);     // vx at x0 - 1
+    float right = __shfl_down_sync(0xffffffffu, X.x, 1);  // vx at x0 + 4
+    if (left_end) left = XL;
+    if (right_end) right = XR;
+    float4 d = zero4;
+    const bool plane_int = yint && z > 0 && z < D - 1;
+    if (plane_int) {
+      if (int0) d.x = ((X.y - left) + (YP.x - YM.x) + (vzp.x - vzm.x)) * 0.5f;
+      d.y = ((X.z - X.x) + (YP.y - YM.y) + (vzp.y - vzm.y)) * 0.5f;
+      d.z = ((X.w - X.y) + (YP.z - YM.z) + (vzp.z - vzm.z)) * 0.5f;
+      if (int3) d.w = ((right - X.z) + (YP.w - YM.w) + (vzp.w - vzm.w)) * 0.5f;
+    }
+    const uint32_t i = base + sz * (uint32_t)z;
+    if (yin && xin) {
+      div4[i >> 2] = d;
+      if (p1) {
+        float4 q = zero4;
+        if (plane_int) {
+          if (int0) q.x = div6(0.0f - d.x);
+          q.y = div6(0.0f - d.y);
+          q.z = div6(0.0f - d.z);
+          if (int3) q.w = div6(0.0f - d.w);
+        }
+        p14[i >> 2] = q;
+      }
+    }
+    if (restrict_mid) {
+      const int b = z & 1;
+      srow[b][ty][lane] = d;
+      __syncthreads();
+      if ((ty & 1) == 0) {
+        const float4 o = srow[b][ty + 1][lane];  // row y + 1 (zero beyond the grid)
+        if (b == 0) {
+          part0 = 0.0f;
+          part1 = 0.0f;
+        }
+        part0 += d.x;
+        part0 += d.y;
+        part0 += o.x;
+        part0 += o.y;
+        part1 += d.z;
+        part1 += d.w;
+        part1 += o.z;
+        part1 += o.w;
+        if (b == 1 && xin && yin) {
+          const uint32_t my_ = y >> 1, mz_ = (uint32_t)z >> 1;
+          for (int h = 0; h < 2; ++h) {
+            const uint32_t mx_ = (x0 >> 1) + (uint32_t)h;
+            if (mx_ < mid.w && my_ < mid.h && mz_ < mid.d) {
+              const bool mb = mx_ == 0 || my_ == 0 || mz_ == 0 || mx_ == mid.w - 1 || my_ == mid.h - 1 || mz_ == mid.d - 1;
+              mid_div[flat(mid, mx_, my_, mz_)] = mb ? 0.0f : (h ? part1 : part0) * 0.125f;
+            }
+          }
+        }
+      }
+    }
+    vzm = vzc;
+    vzc = vzp;
+    vzp = nvz;
+    X = nX;
+    YP = nYP;
+    YM = nYM;
+    XL = nXL;
+    XR = nXR;
+  }
+}
+
 // One Jacobi sweep (pressure-jacobi.wgsl.ts:15-36). With `mid_p`, the result
 // then gets the prolongation added (pressure-prolongation.wgsl.ts:36-43: the
 // boundary stays 0, the interior becomes p + sample), as when the reference
@@ -610,6 +739,90 @@ __global__ void __launch_bounds__(256) k_sweep_v4(Dims dm, const float* __restri
       }
     }
     dst4[(base + sz * z) >> 2] = v;
+  }
+}
+
+// k_sweep_v4 marching in z: a thread owns four x of one row and walks a run of
+// `run` planes, holding the rows at z - 1, z and z + 1 in registers and issuing
+// the loads of plane z + 1 before it computes plane z, so a warp always has one
+// plane of loads in flight. The host sizes the runs so the grid is one wave of
+// resident blocks. Each voxel's sum and division are those of k_sweep, in the
+// same order, so the results are the same bits. (The sweep with the fused
+// prolongation stays on k_sweep_v4<2>: marching it measured 88 against 86 us
+// at 256^3, its trilinear samples being issue-bound.)
+__global__ void __launch_bounds__(256, 4) k_sweep_march(Dims dm, const float* __restrict__ div, const float* __restrict__ src,
+                                                        float* __restrict__ dst, int run) {
+  const uint32_t lane = threadIdx.x;
+  const uint32_t x0 = blockIdx.x * 128 + 4 * lane, y = blockIdx.y * 8 + threadIdx.y;
+  const int zb = (int)blockIdx.z * run, ze = min(zb + run, (int)dm.d);
+  if (y >= dm.h || zb >= ze) return;  // whole warp
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  const bool xin = x0 < dm.w;  // dm.w % 4 == 0: x0 + 3 < dm.w too
+  const uint32_t base = (xin ? x0 : dm.w - 4) + dm.w * y;
+  const bool yint = y > 0 && y < dm.h - 1;
+  const float4* __restrict__ src4 = reinterpret_cast<const float4*>(src);
+  const float4* __restrict__ div4 = reinterpret_cast<const float4*>(div);
+  float4* __restrict__ dst4 = reinterpret_cast<float4*>(dst);
+  const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (!yint) {
+    if (xin)
+      for (int z = zb; z < ze; ++z) dst4[(base + sz * (uint32_t)z) >> 2] = zero4;
+    return;
+  }
+  const bool int0 = x0 > 0, int3 = x0 + 3 < dm.w - 1;  // x0 + 1 and x0 + 2 are always interior
+  const bool left_end = lane == 0 && x0 > 0, right_end = lane == 31 && x0 + 4 < dm.w;
+  const int D = (int)dm.d;
+  // Rows of the source at a plane, zero outside the grid (only the interior
+  // planes 1..D-2 read them, and those reach 0..D-1).
+  auto crow = [&](int z) { return (src && z >= 0 && z < D) ? __ldg(src4 + ((base + sz * (uint32_t)z) >> 2)) : zero4; };
+  float4 cm = crow(zb - 1), c0 = crow(zb), cp = crow(zb + 1);
+  // Plane zb's own rows; every later plane's are loaded one iteration ahead.
+  uint32_t i = base + sz * (uint32_t)zb;
+  float4 dv = __ldg(div4 + (i >> 2));
+  float4 yp = src ? __ldg(src4 + ((i + sy) >> 2)) : zero4;
+  float4 ym = src ? __ldg(src4 + ((i - sy) >> 2)) : zero4;
+  float xle = (src && left_end) ? __ldg(src + i - 1) : 0.0f;
+  float xre = (src && right_end) ? __ldg(src + i + 4) : 0.0f;
+  for (int z = zb; z < ze; ++z) {
+    // Loads for plane z + 1 (its z + 1 row is plane z + 2), clamped in range on
+    // the last plane, whose values are then never used.
+    const int zn = min(z + 1, D - 1);
+    const uint32_t in = base + sz * (uint32_t)zn;
+    const float4 n_c = crow(z + 2);
+    const float4 n_dv = __ldg(div4 + (in >> 2));
+    const float4 n_yp = src ? __ldg(src4 + ((in + sy) >> 2)) : zero4;
+    const float4 n_ym = src ? __ldg(src4 + ((in - sy) >> 2)) : zero4;
+    const float n_xle = (src && left_end) ? __ldg(src + in - 1) : 0.0f;
+    const float n_xre = (src && right_end) ? __ldg(src + in + 4) : 0.0f;
+    float left = __shfl_up_sync(0xffffffffu, c0.w, 1);     // x0 - 1
+    float right = __shfl_down_sync(0xffffffffu, c0.x, 1);  // x0 + 4
+    if (left_end) left = xle;
+    if (right_end) right = xre;
+    if (xin) {
+      float4 v = zero4;
+      if (z > 0 && z < D - 1) {
+        if (src) {
+          if (int0) v.x = div6(c0.y + left + yp.x + ym.x + cp.x + cm.x - dv.x);
+          v.y = div6(c0.z + c0.x + yp.y + ym.y + cp.y + cm.y - dv.y);
+          v.z = div6(c0.w + c0.y + yp.z + ym.z + cp.z + cm.z - dv.z);
+          if (int3) v.w = div6(right + c0.z + yp.w + ym.w + cp.w + cm.w - dv.w);
+        } else {
+          if (int0) v.x = div6(0.0f - dv.x);
+          v.y = div6(0.0f - dv.y);
+          v.z = div6(0.0f - dv.z);
+          if (int3) v.w = div6(0.0f - dv.w);
+        }
+      }
+      dst4[(base + sz * (uint32_t)z) >> 2] = v;
+    }
+    cm = c0;
+    c0 = cp;
+    cp = n_c;
+    dv = n_dv;
+    yp = n_yp;
+    ym = n_ym;
+    xle = n_xle;
+    xre = n_xre;
   }
 }
 
@@ -873,7 +1086,34 @@ int zpass_zchunk() {
   return z;
 }
 
+// k_div_march where the grid allows it (FENIX_DIV_MARCH=0 keeps k_div_first):
+// widths divisible by 4, even heights and depths. Runs of an even number of
+// planes such that the row tiles times the runs fill the resident blocks once.
 cudaError_t lean_div_first(cudaStream_t s, Dims dm, VelField v, float* div, float* p1, Dims mid, float* mid_div, bool restrict_mid) {
+  static const int march = env_int("FENIX_DIV_MARCH", 1, 0, 1);
+  if (march && dm.w % 4 == 0 && dm.w >= 8 && dm.h % 2 == 0 && dm.d % 2 == 0) {
+    static int slots[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    int n = (dev >= 0 && dev < 64) ? slots[dev] : 0;
+    if (n <= 0) {
+      int per_sm = 0, sms = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_div_march, 256, 0);
+      if (e != cudaSuccess) return e;
+      e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return e;
+      n = std::max(1, per_sm) * std::max(1, sms);
+      if (dev >= 0 && dev < 64) slots[dev] = n;
+    }
+    const int tiles = (int)(((dm.w + 127) / 128) * ((dm.h + 7) / 8));
+    const int pairs = (int)dm.d / 2;
+    const int runs = std::max(1, std::min(pairs, n / std::max(tiles, 1)));
+    const int run = 2 * ((pairs + runs - 1) / runs);
+    const dim3 g((dm.w + 127) / 128, (dm.h + 7) / 8, (dm.d + run - 1) / run);
+    k_div_march<<<g, dim3(32, 8, 1), 0, s>>>(dm, v, div, p1, mid, mid_div, restrict_mid ? 1 : 0, run);
+    return cudaGetLastError();
+  }
   k_div_first<<<lean_grid(dm), dim3(32, 4, 2), 0, s>>>(dm, v, div, p1, mid, mid_div, restrict_mid ? 1 : 0);
   return cudaGetLastError();
 }
@@ -884,16 +1124,57 @@ bool sweep_variant_valid(int variant, Dims dm) {
   return variant < SWEEP_VEC_Z2 || (dm.w % 2 == 0 && dm.w >= 4);
 }
 
-// The variant used when none was chosen: four x per thread at z-depth 2 where
-// the width allows (fastest on the 256^3 and 128^3 levels of plume_256), else two
-// x, else one. FENIX_SWEEP_VEC (0, 1, 2) caps the x per thread at 1, 2 or 4.
+static cudaError_t march_run(Dims dm, int* run);
+
+// The variant used when none was chosen: four x per thread marching in z where
+// the width allows and a thread marches at least 8 planes (the 256^3 level of
+// plume_256, 39.8 against 49.8 us per sweep), else four x per thread at z-depth
+// 2 where the width allows (on the 128^3 and 64^3 levels the marching kernel
+// gets 4 and 1 planes per thread and ties with it), else two x, else one.
+// FENIX_SWEEP_VEC (0, 1, 2) caps the x per thread at 1, 2 or 4, and 2 also
+// leaves out the marching kernel.
 int sweep_variant_default(Dims dm) {
   static const int zb = env_int("FENIX_SWEEP_ZB", 4, 1, 8);
-  static const int vec = env_int("FENIX_SWEEP_VEC", 2, 0, 2);
+  static const int vec = env_int("FENIX_SWEEP_VEC", 3, 0, 3);
   static const int vzb = env_int("FENIX_SWEEP_VEC_ZB", 2, 2, 4);
+  int run = 0;
+  if (vec >= 3 && sweep_variant_valid(SWEEP_VEC4_MARCH, dm) && march_run(dm, &run) == cudaSuccess && run >= 8) return SWEEP_VEC4_MARCH;
   if (vec >= 2 && sweep_variant_valid(SWEEP_VEC4_Z2, dm)) return vzb <= 2 ? SWEEP_VEC4_Z2 : SWEEP_VEC4_Z4;
   if (vec >= 1 && sweep_variant_valid(SWEEP_VEC_Z2, dm)) return vzb <= 2 ? SWEEP_VEC_Z2 : SWEEP_VEC_Z4;
   return zb <= 2 ? SWEEP_Z2 : (zb <= 4 ? SWEEP_Z4 : SWEEP_Z8);
+}
+
+// Resident blocks of k_sweep_march on the current device (SMs x blocks per SM),
+// looked up once per device.
+static cudaError_t march_slots(int* slots) {
+  static int cached[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < 64 && cached[dev] > 0) {
+    *slots = cached[dev];
+    return cudaSuccess;
+  }
+  int per_sm = 0, sms = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_march, 256, 0);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  *slots = std::max(1, per_sm) * std::max(1, sms);
+  if (dev >= 0 && dev < 64) cached[dev] = *slots;
+  return cudaSuccess;
+}
+
+// Planes per thread of k_sweep_march on a level: runs of planes such that the
+// row tiles times the runs fill the resident slots once.
+static cudaError_t march_run(Dims dm, int* run) {
+  int slots = 0;
+  const cudaError_t e = march_slots(&slots);
+  if (e != cudaSuccess) return e;
+  const int tiles = (int)(((dm.w + 127) / 128) * ((dm.h + 7) / 8));
+  const int runs = std::max(1, std::min((int)dm.d, slots / std::max(tiles, 1)));
+  *run = ((int)dm.d + runs - 1) / runs;
+  return cudaSuccess;
 }
 
 cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float* div, const float* src, float* dst, Dims mid,
@@ -909,7 +1190,19 @@ cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float
     case SWEEP_VEC_Z4: k_sweep_v2<4><<<grid(64, 4), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
     case SWEEP_VEC4_Z2: k_sweep_v4<2><<<grid(128, 2), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
     case SWEEP_VEC4_Z4: k_sweep_v4<4><<<grid(128, 4), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
-    default: k_sweep_v4<1><<<grid(128, 1), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
+    case SWEEP_VEC4_Z1: k_sweep_v4<1><<<grid(128, 1), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
+    default: {
+      int run = 0;
+      const cudaError_t e = march_run(dm, &run);
+      if (e != cudaSuccess) return e;
+      if (mid_p) {
+        k_sweep_v4<2><<<grid(128, 2), block, 0, s>>>(dm, div, src, dst, mid, mid_p);
+      } else {
+        const dim3 g((dm.w + 127) / 128, (dm.h + 7) / 8, (dm.d + run - 1) / run);
+        k_sweep_march<<<g, block, 0, s>>>(dm, div, src, dst, run);
+      }
+      break;
+    }
   }
   return cudaGetLastError();
 }

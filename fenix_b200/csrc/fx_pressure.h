@@ -48,8 +48,11 @@ cudaError_t lean_div_first(cudaStream_t s, Dims dm, VelField v, float* div, floa
 cudaError_t lean_sweep(cudaStream_t s, Dims dm, const float* div, const float* src, float* dst, Dims mid, const float* mid_p);
 
 // Sweep kernel variants (all give the same bits): one x per thread with z-depth
-// 2, 4 or 8, or two x per thread (even widths) with z-depth 2 or 4. An invalid
-// variant (-1, or a two-x variant on an odd width) takes the default.
+// 2, 4 or 8, two x per thread (even widths) with z-depth 2 or 4, four x per
+// thread (widths divisible by 4) with z-depth 2, 4 or 1, or four x per thread
+// marching runs of planes with the next plane's loads in flight. An invalid
+// variant (-1, or a vector variant on a width it does not divide) takes the
+// default.
 enum SweepVariant {
   SWEEP_Z2 = 0,
   SWEEP_Z4 = 1,
@@ -59,7 +62,8 @@ enum SweepVariant {
   SWEEP_VEC4_Z2 = 5,  // four x per thread (widths divisible by 4)
   SWEEP_VEC4_Z4 = 6,
   SWEEP_VEC4_Z1 = 7,
-  kSweepVariants = 8
+  SWEEP_VEC4_MARCH = 8,  // four x per thread, one wave of blocks marching in z
+  kSweepVariants = 9
 };
 bool sweep_variant_valid(int variant, Dims dm);
 int sweep_variant_default(Dims dm);

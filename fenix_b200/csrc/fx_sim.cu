@@ -1155,6 +1155,13 @@ fx_status fx_sim_autotune(fx_sim* s, fx_autotune_report* o) {
         best = v;
       }
     }
+    // A variant replaces the default only when it is at least 3 % faster:
+    // closer timings of 20 sweeps are within the run-to-run noise, and on the
+    // small levels such ties measured slower inside the step's graph.
+    if (best != dflt && o->default_us[l] > 0.0f && best_us > 0.97f * o->default_us[l]) {
+      best = dflt;
+      best_us = o->default_us[l];
+    }
     s->sweep_variant[l] = best;
     o->sweep_variant[l] = best;
     o->sweep_us[l] = best_us;

@@ -339,12 +339,13 @@ fx_status fx_sim_read_solver_stats(fx_sim* sim, fx_solver_stats* out);
 
 /* Autotuning (extension): times every sweep kernel variant of the pressure
  * solve on each level (fine, mid, coarse) of this simulation's grid and keeps
- * the fastest for its later steps. All variants give the same bits. Waits for
+ * the fastest for its later steps, where it beats the level's default by at
+ * least 3 % (else the default). All variants give the same bits. Waits for
  * the stream; overwrites the pressure buffers that are not current (the
  * non-current fine buffer and the mid/coarse levels, which every solve
  * rewrites from zero). */
 typedef struct fx_autotune_report {
-  int32_t sweep_variant[3]; /* chosen variant per level (0..7) */
+  int32_t sweep_variant[3]; /* chosen variant per level (0..8) */
   float sweep_us[3];        /* its time per sweep */
   float default_us[3];      /* the default variant's time per sweep */
 } fx_autotune_report;
@@ -354,7 +355,8 @@ fx_status fx_sim_autotune(fx_sim* sim, fx_autotune_report* out);
  * -1 keeps the default; a variant that does not fit the level's width is
  * FX_ERR_INVALID_ARGUMENT. Variants: 0-2 one x per thread at z-depth 2/4/8,
  * 3-4 two x per thread (even widths) at z-depth 2/4, 5-7 four x per thread
- * (widths divisible by 4) at z-depth 2/4/1. */
+ * (widths divisible by 4) at z-depth 2/4/1, 8 four x per thread marching runs
+ * of planes with the next plane's loads in flight (widths divisible by 4). */
 fx_status fx_sim_set_sweep_variants(fx_sim* sim, const int32_t variants[3]);
 fx_status fx_sim_get_sweep_variants(fx_sim* sim, int32_t variants[3]);
 

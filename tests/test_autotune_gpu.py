@@ -11,7 +11,7 @@ from parity_util import EXPOSED_FIELDS, all_kind_sources, compare
 
 pytestmark = pytest.mark.gpu
 
-VECTOR_VARIANTS = (3, 4, 5, 6, 7)
+VECTOR_VARIANTS = (3, 4, 5, 6, 7, 8)
 
 
 @pytest.mark.parametrize("opts,sources", [
@@ -32,7 +32,7 @@ def test_autotuned_steps_equal_the_oracle(opts, sources):
         sim.step(k / 60, 1 / 60)
         orc.step(k / 60, 1 / 60)
     rep = sim.autotune()
-    assert all(0 <= v <= 7 for v in rep["sweepVariant"]) and all(t > 0 for t in rep["sweepUs"])
+    assert all(0 <= v <= 8 for v in rep["sweepVariant"]) and all(t > 0 for t in rep["sweepUs"])
     assert all(rep["sweepUs"][l] <= rep["defaultUs"][l] * 1.0001 for l in range(3))
     if opts["resolution"][0] % 2:
         assert rep["sweepVariant"][0] not in VECTOR_VARIANTS
@@ -44,7 +44,7 @@ def test_autotuned_steps_equal_the_oracle(opts, sources):
         compare(sim, orc, EXPOSED_FIELDS, f"tuned step {k + 1}")
 
 
-@pytest.mark.parametrize("variant", range(8))
+@pytest.mark.parametrize("variant", range(9))
 def test_every_sweep_variant_equals_the_oracle(variant):
     """Each sweep kernel forced on every level that it fits (widths 64/32/16 fit
     all of them) gives the oracle's bits, with the first post-sweep's fused
