@@ -63,17 +63,17 @@ KERNEL_BYTES = {
 
 
 # DRAM bytes (read + written) per launch measured by ncu on plume_256 with FP16
-# storage (profiles/fused_step_plume256_f16_launches.md), per kernel of the
-# fused path, for roofline.traffic.
+# storage (the launch-list summary under profiles/), per kernel of the fused
+# path, for roofline.traffic. fused_sweep is the marching fine sweep.
 NCU_TRAFFIC = {
-    "fused_sweep": 170.6e6,
+    "fused_sweep": 176.3e6,
     "fused_advect_velocity": 360.8e6,
     "fused_advect_scalars": 109.5e6,
     "fused_combustion": 50.7e6,
     "fused_buoyancy": 84.8e6,
     "fused_vorticity": 248.1e6,
     "fused_confinement": 456.4e6,
-    "fused_div_first_sweep": 306.2e6,
+    "fused_div_first_sweep": 312.9e6,
     "fused_project": 426.7e6,
 }
 
