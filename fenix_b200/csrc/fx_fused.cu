@@ -677,6 +677,158 @@ __global__ void __launch_bounds__(256) k_project(Dims dm, VelField vs, const flo
 
 inline dim3 proj_grid(Dims d) { return dim3((d.w + 31) / 32, (d.h + 7) / 8, (d.d + kProjZ - 1) / kProjZ); }
 
+// k_project with four x per thread marching runs of planes (widths divisible by
+// 4). A thread holds the pressure rows at z - 1, z and z + 1, takes the x
+// neighbours of its row by warp shuffle (the row ends load theirs) and reads the
+// rows y -+ 1, which its neighbour warps loaded a plane earlier, from cache. The
+// loads only it makes from DRAM (the three velocity rows of plane z + 1 and the
+// pressure row of plane z + 2) are issued before it computes plane z. Each
+// component, |v| and the running maximum are computed with project_column's
+// operations in its order, so the results are the same bits.
+template <bool VMAG>
+__global__ void __launch_bounds__(256, 4) k_project_march(Dims dm, VelField vs, const float* __restrict__ p, VelField vd,
+                                                          float* __restrict__ vmag, unsigned* __restrict__ vmax, int run) {
+  const uint32_t lane = threadIdx.x;
+  const uint32_t x0 = blockIdx.x * 128 + 4 * lane, y = blockIdx.y * 8 + threadIdx.y;
+  const int zb = (int)blockIdx.z * run, ze = min(zb + run, (int)dm.d);
+  if (zb >= ze) return;  // whole block
+  const int D = (int)dm.d;
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  const bool yin = y < dm.h;
+  const bool xin = x0 < dm.w;  // dm.w % 4 == 0: x0 + 3 < dm.w too
+  const uint32_t base = (xin ? x0 : dm.w - 4) + dm.w * (yin ? y : dm.h - 1);
+  const bool yint = yin && y > 0 && y < dm.h - 1;
+  const bool int0 = x0 > 0, int3 = x0 + 3 < dm.w - 1;  // x0 + 1 and x0 + 2 are interior in x
+  const bool left_end = lane == 0 && x0 > 0, right_end = lane == 31 && x0 + 4 < dm.w;
+  const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  auto ld4 = [&](const float* f, uint32_t i) { return __ldg(reinterpret_cast<const float4*>(f) + (i >> 2)); };
+  auto st4 = [&](float* f, uint32_t i, float4 v) { reinterpret_cast<float4*>(f)[i >> 2] = v; };
+  auto prow = [&](int z) { return (yint && z >= 0 && z < D) ? ld4(p, base + sz * (uint32_t)z) : zero4; };
+  float4 pm = prow(zb - 1), pc = prow(zb), pp = prow(zb + 1);
+  float4 VX = zero4, VY = zero4, VZ = zero4;
+  {
+    const uint32_t i = base + sz * (uint32_t)zb;
+    if (yint) {
+      VX = ld4(vs.c[0], i);
+      VY = ld4(vs.c[1], i);
+      VZ = ld4(vs.c[2], i);
+    }
+  }
+  float m = 0.0f;
+  for (int z = zb; z < ze; ++z) {
+    const uint32_t i = base + sz * (uint32_t)z;
+    const uint32_t in = base + sz * (uint32_t)min(z + 1, D - 1);
+    float4 nVX = zero4, nVY = zero4, nVZ = zero4;
+    if (yint) {
+      nVX = ld4(vs.c[0], in);
+      nVY = ld4(vs.c[1], in);
+      nVZ = ld4(vs.c[2], in);
+    }
+    const float4 npp = prow(z + 2);
+    const bool zint = yint && z > 0 && z < D - 1;
+    float4 PU = zero4, PD = zero4;
+    float pl = 0.0f, pr = 0.0f;
+    if (zint) {
+      PU = ld4(p, i + sy);
+      PD = ld4(p, i - sy);
+      if (left_end) pl = __ldg(p + i - 1);
+      if (right_end) pr = __ldg(p + i + 4);
+    }
+    float left = __shfl_up_sync(0xffffffffu, pc.w, 1);     // p at x0 - 1
+    float right = __shfl_down_sync(0xffffffffu, pc.x, 1);  // p at x0 + 4
+    if (left_end) left = pl;
+    if (right_end) right = pr;
+    if (yin && xin) {
+      // each component is stored as soon as it is formed (fewer live registers);
+      // the running maximum is exact in any order
+      float4 ox = zero4;
+      if (zint) {
+        if (int0) ox.x = VX.x - (pc.y - left) * 0.5f;
+        ox.y = VX.y - (pc.z - pc.x) * 0.5f;
+        ox.z = VX.z - (pc.w - pc.y) * 0.5f;
+        if (int3) ox.w = VX.w - (right - pc.z) * 0.5f;
+      }
+      st4(vd.c[0], i, ox);
+      float4 oy = zero4;
+      if (zint) {
+        if (int0) oy.x = VY.x - (PU.x - PD.x) * 0.5f;
+        oy.y = VY.y - (PU.y - PD.y) * 0.5f;
+        oy.z = VY.z - (PU.z - PD.z) * 0.5f;
+        if (int3) oy.w = VY.w - (PU.w - PD.w) * 0.5f;
+      }
+      st4(vd.c[1], i, oy);
+      float4 oz = zero4;
+      if (zint) {
+        if (int0) oz.x = VZ.x - (pp.x - pm.x) * 0.5f;
+        oz.y = VZ.y - (pp.y - pm.y) * 0.5f;
+        oz.z = VZ.z - (pp.z - pm.z) * 0.5f;
+        if (int3) oz.w = VZ.w - (pp.w - pm.w) * 0.5f;
+      }
+      st4(vd.c[2], i, oz);
+      if (VMAG)
+        st4(vmag, i, make_float4(length3(ox.x, oy.x, oz.x), length3(ox.y, oy.y, oz.y), length3(ox.z, oy.z, oz.z), length3(ox.w, oy.w, oz.w)));
+      m = fmaxf(m, fmaxf(fabsf(ox.x), fmaxf(fabsf(oy.x), fabsf(oz.x))));
+      m = fmaxf(m, fmaxf(fabsf(ox.y), fmaxf(fabsf(oy.y), fabsf(oz.y))));
+      m = fmaxf(m, fmaxf(fabsf(ox.z), fmaxf(fabsf(oy.z), fabsf(oz.z))));
+      m = fmaxf(m, fmaxf(fabsf(ox.w), fmaxf(fabsf(oy.w), fabsf(oz.w))));
+    }
+    pm = pc;
+    pc = pp;
+    pp = npp;
+    VX = nVX;
+    VY = nVY;
+    VZ = nVZ;
+  }
+  // block maximum, then one atomic per block when it raises the bound
+  unsigned bits = __reduce_max_sync(0xffffffffu, __float_as_uint(m));
+  __shared__ unsigned part[8];
+  const int warp = threadIdx.y;
+  if (threadIdx.x == 0) part[warp] = bits;
+  __syncthreads();
+  if (threadIdx.x == 0 && warp == 0) {
+    for (int k = 1; k < 8; ++k) bits = max(bits, part[k]);
+    if (bits > __ldcg(vmax)) atomicMax(vmax, bits);
+  }
+}
+
+// The projection launch: k_project_march where the width allows it
+// (FENIX_PROJ_MARCH=0 keeps k_project), with runs of planes such that the
+// 128 x 8 row tiles times the runs fill the resident blocks once.
+cudaError_t launch_project(cudaStream_t s, Dims dm, const VelField& vs, const float* p, const VelField& vd, float* vmag, int write_vmag,
+                           unsigned* vmax) {
+  static const bool march = [] {
+    const char* v = std::getenv("FENIX_PROJ_MARCH");
+    return !(v && *v == '0');
+  }();
+  if (march && dm.w % 4 == 0 && dm.w >= 8) {
+    static int slots[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    int n = (dev >= 0 && dev < 64) ? slots[dev] : 0;
+    if (n <= 0) {
+      int per_sm = 0, sms = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_project_march<true>, 256, 0);
+      if (e != cudaSuccess) return e;
+      e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return e;
+      n = std::max(1, per_sm) * std::max(1, sms);
+      if (dev >= 0 && dev < 64) slots[dev] = n;
+    }
+    const int tiles = (int)(((dm.w + 127) / 128) * ((dm.h + 7) / 8));
+    const int runs = std::max(1, std::min((int)dm.d, n / std::max(tiles, 1)));
+    const int run = ((int)dm.d + runs - 1) / runs;
+    const dim3 g((dm.w + 127) / 128, (dm.h + 7) / 8, (dm.d + run - 1) / run);
+    if (write_vmag)
+      k_project_march<true><<<g, dim3(32, 8, 1), 0, s>>>(dm, vs, p, vd, vmag, vmax, run);
+    else
+      k_project_march<false><<<g, dim3(32, 8, 1), 0, s>>>(dm, vs, p, vd, vmag, vmax, run);
+  } else {
+    k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, vs, p, vd, vmag, write_vmag, vmax);
+  }
+  return cudaGetLastError();
+}
+
 // Rebuilds the per-brick bookkeeping after the fields were written from the host:
 // the non-zero bits of the three scalar buffers and the summary of the current set.
 template <typename S>
@@ -1205,7 +1357,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     if (vs != FX_OK) return vs;
     Timed tm(w, s, "fused_project");
     FX_CK(cudaMemsetAsync(w.vmax, 0, sizeof(unsigned), s));
-    k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax);
+    FX_CK(launch_project(s, dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax));
     ++launches;
   } else if (st.pressure_on) {
     const int m = st.q[2], n = st.q[3];
@@ -1318,7 +1470,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       {
         Timed tm(w, s, "fused_project");
         FX_CK(cudaMemsetAsync(w.vmax, 0, sizeof(unsigned), s));
-        k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, F.p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax);
+        FX_CK(launch_project(s, dm, *vfinal, F.p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax));
         ++launches;
       }
     } else {
@@ -1441,7 +1593,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     // 10. projection with the pressure of the last solve (+ |v|)
     Timed tm(w, s, "fused_project");
     FX_CK(cudaMemsetAsync(w.vmax, 0, sizeof(unsigned), s));
-    k_project<<<proj_grid(dm), dim3(32, 8, 1), 0, s>>>(dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax);
+    FX_CK(launch_project(s, dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax));
     ++launches;
   }
   // FP64 statistics of the solve: ||div||, ||div - A p|| (the V-cycle has them
