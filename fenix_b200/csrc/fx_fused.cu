@@ -299,6 +299,43 @@ __global__ void k_dilate(uint3 bc, const uint8_t* __restrict__ summary, uint32_t
 
 FX_DEV bool flag_at(const uint32_t* __restrict__ flags, uint3 bc, uint32_t b) { return __ldg(flags + b) != 0u; }
 
+// Planes per thread for a kernel of 256-thread blocks marching runs of z over
+// tx x ty row tiles: the number of runs (at most one per 8 planes) that fills
+// whole waves of the kernel's resident blocks best, the fewest runs among equals.
+template <typename K>
+cudaError_t march_runs(K kernel, Dims dm, int tx, int ty, int* run) {
+  static int slots[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int n = (dev >= 0 && dev < 64) ? slots[dev] : 0;
+  if (n <= 0) {
+    int per_sm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    n = std::max(1, per_sm) * std::max(1, sms);
+    if (dev >= 0 && dev < 64) slots[dev] = n;
+  }
+  const long tiles = (long)((dm.w + tx - 1) / tx) * (long)((dm.h + ty - 1) / ty);
+  int best = 1;
+  double best_eff = -1.0;
+  for (int r = 1; r <= std::max(1, (int)dm.d / 8); ++r) {
+    const int len = ((int)dm.d + r - 1) / r;
+    const int runs = ((int)dm.d + len - 1) / len;
+    const long blocks = tiles * runs;
+    const long waves = (blocks + n - 1) / n;
+    const double eff = (double)blocks / (double)(waves * n);
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = len;
+    }
+  }
+  *run = best;
+  return cudaSuccess;
+}
+
 // ------------------------------------------------------------ velocity advection
 // advect-velocity-semilagrangian.wgsl.ts:23-41 over vCurrent clamped to +-lim on read.
 FX_DEV float tri_interp_clamped(const float* __restrict__ f, const Tri& c, float lim) {
@@ -367,6 +404,75 @@ __global__ void __launch_bounds__(256) k_advect_velocity(Dims dm, const Params* 
   const bool xyint = x > 0 && y > 0 && x < dm.w - 1 && y < dm.h - 1;
   if (__uint_as_float(__ldg(vmax)) <= lim) advect_velocity_column<false, ZB>(dm, x, y, z0, dt, lim, damp, xyint, src, dst);
   else advect_velocity_column<true, ZB>(dm, x, y, z0, dt, lim, damp, xyint, src, dst);
+}
+
+// k_advect_velocity with each thread marching a run of z planes of one (x, y)
+// column: the velocity at plane z + 1 (the start of its back-trace) is loaded
+// before the 24 gathers of plane z are issued, so a voxel waits for one memory
+// latency instead of two. Each voxel's back-trace, samples and damping are
+// advect_velocity_column's, in the same order, so the results are the same bits.
+template <bool CLAMP>
+FX_DEV void advect_velocity_march(Dims dm, uint32_t x, uint32_t y, int zb, int ze, float dt, float lim, float damp, const VelField& src,
+                                  const VelField& dst) {
+  const uint32_t sz = dm.w * dm.h;
+  const uint32_t base = x + dm.w * y;
+  const int D = (int)dm.d;
+  uint32_t i = base + sz * (uint32_t)zb;
+  float v0x = __ldg(src.c[0] + i), v0y = __ldg(src.c[1] + i), v0z = __ldg(src.c[2] + i);
+  for (int z = zb; z < ze; ++z) {
+    const uint32_t in = base + sz * (uint32_t)min(z + 1, D - 1);
+    const float nx = __ldg(src.c[0] + in), ny = __ldg(src.c[1] + in), nz = __ldg(src.c[2] + in);
+    if (z == 0 || z == D - 1) {
+      dst.c[0][i] = 0.0f;
+      dst.c[1][i] = 0.0f;
+      dst.c[2][i] = 0.0f;
+    } else {
+      const float cx = (float)x + 0.5f, cy = (float)y + 0.5f, cz = (float)z + 0.5f;
+      float ax = v0x, ay = v0y, az = v0z;
+      if (CLAMP) {
+        ax = clampv(ax, -lim, lim);
+        ay = clampv(ay, -lim, lim);
+        az = clampv(az, -lim, lim);
+      }
+      const float bx = cx - ax * dt, by = cy - ay * dt, bz = cz - az * dt;
+      const Tri c1 = tri_corners(dm, bx - 0.5f, by - 0.5f, bz - 0.5f);
+      if (CLAMP) {
+        dst.c[0][i] = tri_interp_clamped(src.c[0], c1, lim) * damp;
+        dst.c[1][i] = tri_interp_clamped(src.c[1], c1, lim) * damp;
+        dst.c[2][i] = tri_interp_clamped(src.c[2], c1, lim) * damp;
+      } else {
+        dst.c[0][i] = tri_interp(src.c[0], c1) * damp;
+        dst.c[1][i] = tri_interp(src.c[1], c1) * damp;
+        dst.c[2][i] = tri_interp(src.c[2], c1) * damp;
+      }
+    }
+    v0x = nx;
+    v0y = ny;
+    v0z = nz;
+    i = in;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_advect_velocity_march(Dims dm, const Params* __restrict__ Pp, VelField src, VelField dst,
+                                                               const unsigned* __restrict__ vmax, int run) {
+  const uint32_t x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y;
+  const int zb = (int)blockIdx.z * run, ze = min(zb + run, (int)dm.d);
+  if (x >= dm.w || y >= dm.h || zb >= ze) return;
+  const float dt = Pp->dt;
+  const float lim = speed_limit(*Pp);
+  const float damp = 1.0f - dt * 0.025f;
+  const bool xyint = x > 0 && y > 0 && x < dm.w - 1 && y < dm.h - 1;
+  if (!xyint) {
+    for (int z = zb; z < ze; ++z) {
+      const uint32_t i = flat(dm, x, y, (uint32_t)z);
+      dst.c[0][i] = 0.0f;
+      dst.c[1][i] = 0.0f;
+      dst.c[2][i] = 0.0f;
+    }
+    return;
+  }
+  if (__uint_as_float(__ldg(vmax)) <= lim) advect_velocity_march<false>(dm, x, y, zb, ze, dt, lim, damp, src, dst);
+  else advect_velocity_march<true>(dm, x, y, zb, ze, dt, lim, damp, src, dst);
 }
 
 // -------------------------------------------------------------- scalar advection
@@ -1287,7 +1393,14 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     }();
     const dim3 blk(32, 8, 1);
     auto grid = [&](int z) { return dim3((dm.w + 31) / 32, (dm.h + 7) / 8, (dm.d + z - 1) / z); };
-    switch (zb) {
+    static const bool march = [] {
+      const char* v = std::getenv("FENIX_ADV_MARCH");
+      return !(v && *v == '0');
+    }();
+    int run = 0;
+    if (march && std::getenv("FENIX_ADV_Z") == nullptr && march_runs(k_advect_velocity_march, dm, 32, 8, &run) == cudaSuccess) {
+      k_advect_velocity_march<<<grid(run), blk, 0, s>>>(dm, st.params, st.vcur, st.vscr, w.vmax, run);
+    } else switch (zb) {
       case 2: k_advect_velocity<2><<<grid(2), blk, 0, s>>>(dm, st.params, st.vcur, st.vscr, w.vmax); break;
       case 8: k_advect_velocity<8><<<grid(8), blk, 0, s>>>(dm, st.params, st.vcur, st.vscr, w.vmax); break;
       case 4: k_advect_velocity<4><<<grid(4), blk, 0, s>>>(dm, st.params, st.vcur, st.vscr, w.vmax); break;
