@@ -747,9 +747,9 @@ __global__ void __launch_bounds__(256) k_sweep_v4(Dims dm, const float* __restri
 // the loads of plane z + 1 before it computes plane z, so a warp always has one
 // plane of loads in flight. The host sizes the runs so the grid is one wave of
 // resident blocks. Each voxel's sum and division are those of k_sweep, in the
-// same order, so the results are the same bits. (The sweep with the fused
-// prolongation stays on k_sweep_v4<2>: marching it measured 88 against 86 us
-// at 256^3, its trilinear samples being issue-bound.)
+// same order, so the results are the same bits. The sweep with the fused
+// prolongation has its own marching kernel, k_sweep_march_prolong, which also
+// shares the prolongation's mid-level corners between voxels.
 __global__ void __launch_bounds__(256, 4) k_sweep_march(Dims dm, const float* __restrict__ div, const float* __restrict__ src,
                                                         float* __restrict__ dst, int run) {
   const uint32_t lane = threadIdx.x;
@@ -823,6 +823,161 @@ __global__ void __launch_bounds__(256, 4) k_sweep_march(Dims dm, const float* __
     ym = n_ym;
     xle = n_xle;
     xre = n_xre;
+  }
+}
+
+// k_sweep_march with the prolongation of mid_p added (the first fine post-sweep),
+// for even fine grids with widths divisible by 4 whose mid level is exactly half
+// their size. There, at an interior fine voxel, prolong_sample's position
+// ((c + 0.5) * 0.5 - 0.5 per axis) needs no clamp, its corners are mid cells
+// (c - 1) >> 1 and one more, and its weights are exactly 0.75 for even c and
+// 0.25 for odd c. A thread's four x then read mid columns x0/2 - 1 .. x0/2 + 2 of
+// two mid rows, and consecutive fine planes share mid planes: the kernel holds
+// the two mid planes of the current fine plane (8 values each: a float2 load
+// per row, the outer columns by warp shuffle) and loads the next one, from L2,
+// when fine z reaches it. Each sample is tri_interp's mix of the same corner values with the
+// same weights in the same order, so the results are the same bits.
+__global__ void __launch_bounds__(256, 3) k_sweep_march_prolong(Dims dm, const float* __restrict__ div, const float* __restrict__ src,
+                                                                float* __restrict__ dst, Dims mid, const float* __restrict__ mid_p, int run) {
+  const uint32_t lane = threadIdx.x;
+  const uint32_t x0 = blockIdx.x * 128 + 4 * lane, y = blockIdx.y * 8 + threadIdx.y;
+  const int zb = (int)blockIdx.z * run, ze = min(zb + run, (int)dm.d);
+  if (y >= dm.h || zb >= ze) return;  // whole warp
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  const bool xin = x0 < dm.w;  // dm.w % 4 == 0: x0 + 3 < dm.w too
+  const uint32_t xb = xin ? x0 : dm.w - 4;
+  const uint32_t base = xb + dm.w * y;
+  const bool yint = y > 0 && y < dm.h - 1;
+  const float4* __restrict__ src4 = reinterpret_cast<const float4*>(src);
+  const float4* __restrict__ div4 = reinterpret_cast<const float4*>(div);
+  float4* __restrict__ dst4 = reinterpret_cast<float4*>(dst);
+  const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (!yint) {
+    if (xin)
+      for (int z = zb; z < ze; ++z) dst4[(base + sz * (uint32_t)z) >> 2] = zero4;
+    return;
+  }
+  const bool int0 = x0 > 0, int3 = x0 + 3 < dm.w - 1;  // x0 + 1 and x0 + 2 are always interior
+  const bool left_end = lane == 0 && x0 > 0, right_end = lane == 31 && x0 + 4 < dm.w;
+  const int D = (int)dm.d;
+  // mid rows and row weight of this fine row (interior, so unclamped)
+  const uint32_t mc = xb >> 1;  // even; the thread's mid columns are mc - 1 .. mc + 2
+  const uint32_t mby = (y - 1u) >> 1, muy = mby + 1u;
+  const float fy = (y & 1u) ? 0.25f : 0.75f;
+  const float2* __restrict__ mid2 = reinterpret_cast<const float2*>(mid_p);
+  // Raw loads of one mid plane: the float2 (mc, mc + 1) of each row, and at the
+  // row ends of the warp the outer column the shuffle cannot bring.
+  struct Raw {
+    float2 r0, r1;
+    float l0, l1, q0, q1;
+  };
+  auto mid_raw = [&](int pz) {
+    Raw o;
+    const uint32_t pc = (uint32_t)max(0, min(pz, (int)mid.d - 1));
+    const uint32_t i0 = mc + mid.w * (mby + mid.h * pc), i1 = mc + mid.w * (muy + mid.h * pc);
+    o.r0 = __ldg(mid2 + (i0 >> 1));
+    o.r1 = __ldg(mid2 + (i1 >> 1));
+    o.l0 = left_end ? __ldg(mid_p + i0 - 1) : 0.0f;
+    o.l1 = left_end ? __ldg(mid_p + i1 - 1) : 0.0f;
+    o.q0 = right_end ? __ldg(mid_p + i0 + 2) : 0.0f;
+    o.q1 = right_end ? __ldg(mid_p + i1 + 2) : 0.0f;
+    return o;
+  };
+  // The 8 values of a mid plane: [row][column mc - 1 + k]
+  struct Plane {
+    float v[2][4];
+  };
+  auto expand = [&](const Raw& r) {
+    Plane p;
+    float a = __shfl_up_sync(0xffffffffu, r.r0.y, 1), b = __shfl_down_sync(0xffffffffu, r.r0.x, 1);
+    float c = __shfl_up_sync(0xffffffffu, r.r1.y, 1), d = __shfl_down_sync(0xffffffffu, r.r1.x, 1);
+    if (left_end) {
+      a = r.l0;
+      c = r.l1;
+    }
+    if (right_end) {
+      b = r.q0;
+      d = r.q1;
+    }
+    p.v[0][0] = a;
+    p.v[0][1] = r.r0.x;
+    p.v[0][2] = r.r0.y;
+    p.v[0][3] = b;
+    p.v[1][0] = c;
+    p.v[1][1] = r.r1.x;
+    p.v[1][2] = r.r1.y;
+    p.v[1][3] = d;
+    return p;
+  };
+  // tri_interp over mid columns (k, k + 1) of planes A (z corner b) and B (u)
+  auto sample = [&](const Plane& A, const Plane& B, int k, float fx, float fz) {
+    const float x00 = mixv(A.v[0][k], A.v[0][k + 1], fx);
+    const float x10 = mixv(A.v[1][k], A.v[1][k + 1], fx);
+    const float x01 = mixv(B.v[0][k], B.v[0][k + 1], fx);
+    const float x11 = mixv(B.v[1][k], B.v[1][k + 1], fx);
+    return mixv(mixv(x00, x10, fy), mixv(x01, x11, fy), fz);
+  };
+  int cbz = (zb - 1) >> 1;  // the mid plane held in A (B holds cbz + 1)
+  Plane A = expand(mid_raw(cbz)), B = expand(mid_raw(cbz + 1));
+
+  auto crow = [&](int z) { return (src && z >= 0 && z < D) ? __ldg(src4 + ((base + sz * (uint32_t)z) >> 2)) : zero4; };
+  float4 cm = crow(zb - 1), c0 = crow(zb), cp = crow(zb + 1);
+  uint32_t i = base + sz * (uint32_t)zb;
+  float4 dv = __ldg(div4 + (i >> 2));
+  float4 yp = src ? __ldg(src4 + ((i + sy) >> 2)) : zero4;
+  float4 ym = src ? __ldg(src4 + ((i - sy) >> 2)) : zero4;
+  float xle = (src && left_end) ? __ldg(src + i - 1) : 0.0f;
+  float xre = (src && right_end) ? __ldg(src + i + 4) : 0.0f;
+  for (int z = zb; z < ze; ++z) {
+    const int bz = (z - 1) >> 1;
+    if (bz != cbz) {  // warp-uniform: fine z moved on to the next mid plane pair (an L2 hit)
+      A = B;
+      cbz = bz;
+      B = expand(mid_raw(cbz + 1));
+    }
+    const int zn = min(z + 1, D - 1);
+    const uint32_t in = base + sz * (uint32_t)zn;
+    const float4 n_c = crow(z + 2);
+    const float4 n_dv = __ldg(div4 + (in >> 2));
+    const float4 n_yp = src ? __ldg(src4 + ((in + sy) >> 2)) : zero4;
+    const float4 n_ym = src ? __ldg(src4 + ((in - sy) >> 2)) : zero4;
+    const float n_xle = (src && left_end) ? __ldg(src + in - 1) : 0.0f;
+    const float n_xre = (src && right_end) ? __ldg(src + in + 4) : 0.0f;
+    float left = __shfl_up_sync(0xffffffffu, c0.w, 1);     // x0 - 1
+    float right = __shfl_down_sync(0xffffffffu, c0.x, 1);  // x0 + 4
+    if (left_end) left = xle;
+    if (right_end) right = xre;
+    if (xin) {
+      float4 v = zero4;
+      if (z > 0 && z < D - 1) {
+        if (src) {
+          if (int0) v.x = div6(c0.y + left + yp.x + ym.x + cp.x + cm.x - dv.x);
+          v.y = div6(c0.z + c0.x + yp.y + ym.y + cp.y + cm.y - dv.y);
+          v.z = div6(c0.w + c0.y + yp.z + ym.z + cp.z + cm.z - dv.z);
+          if (int3) v.w = div6(right + c0.z + yp.w + ym.w + cp.w + cm.w - dv.w);
+        } else {
+          if (int0) v.x = div6(0.0f - dv.x);
+          v.y = div6(0.0f - dv.y);
+          v.z = div6(0.0f - dv.z);
+          if (int3) v.w = div6(0.0f - dv.w);
+        }
+        const float fz = (z & 1) ? 0.25f : 0.75f;
+        if (int0) v.x = v.x + sample(A, B, 0, 0.75f, fz);
+        v.y = v.y + sample(A, B, 1, 0.25f, fz);
+        v.z = v.z + sample(A, B, 1, 0.75f, fz);
+        if (int3) v.w = v.w + sample(A, B, 2, 0.25f, fz);
+      }
+      dst4[(base + sz * (uint32_t)z) >> 2] = v;
+    }
+    cm = c0;
+    c0 = cp;
+    cp = n_c;
+    dv = n_dv;
+    yp = n_yp;
+    ym = n_ym;
+    xle = n_xle;
+    xre = n_xre;
+    i = in;
   }
 }
 
@@ -1177,6 +1332,30 @@ static cudaError_t march_run(Dims dm, int* run) {
   return cudaSuccess;
 }
 
+// march_run for another marching kernel of 256-thread blocks over 128 x 8 row
+// tiles (its own resident blocks, looked up once per device).
+template <typename K>
+static cudaError_t march_run_of(K kernel, Dims dm, int* run) {
+  static int cached[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int slots = (dev >= 0 && dev < 64) ? cached[dev] : 0;
+  if (slots <= 0) {
+    int per_sm = 0, sms = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    slots = std::max(1, per_sm) * std::max(1, sms);
+    if (dev >= 0 && dev < 64) cached[dev] = slots;
+  }
+  const int tiles = (int)(((dm.w + 127) / 128) * ((dm.h + 7) / 8));
+  const int runs = std::max(1, std::min((int)dm.d, slots / std::max(tiles, 1)));
+  *run = ((int)dm.d + runs - 1) / runs;
+  return cudaSuccess;
+}
+
 cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float* div, const float* src, float* dst, Dims mid,
                                const float* mid_p) {
   if (!sweep_variant_valid(variant, dm)) variant = sweep_variant_default(dm);
@@ -1195,7 +1374,14 @@ cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float
       int run = 0;
       const cudaError_t e = march_run(dm, &run);
       if (e != cudaSuccess) return e;
-      if (mid_p) {
+      // FENIX_PROLONG_MARCH=0 keeps k_sweep_v4<2> for the sweep with the prolongation
+      static const bool prolong_march = env_int("FENIX_PROLONG_MARCH", 1, 0, 1) == 1;
+      int prun = 0;
+      const bool pm_ok = mid_p && dm.h % 2 == 0 && dm.d % 2 == 0 && mid.w * 2 == dm.w && mid.h * 2 == dm.h && mid.d * 2 == dm.d;
+      if (pm_ok && prolong_march && march_run_of(k_sweep_march_prolong, dm, &prun) == cudaSuccess) {
+        const dim3 g((dm.w + 127) / 128, (dm.h + 7) / 8, (dm.d + prun - 1) / prun);
+        k_sweep_march_prolong<<<g, block, 0, s>>>(dm, div, src, dst, mid, mid_p, prun);
+      } else if (mid_p) {
         k_sweep_v4<2><<<grid(128, 2), block, 0, s>>>(dm, div, src, dst, mid, mid_p);
       } else {
         const dim3 g((dm.w + 127) / 128, (dm.h + 7) / 8, (dm.d + run - 1) / run);
