@@ -81,6 +81,67 @@ FX_DEV float tri_interp_s(const S* __restrict__ f, const Tri& c) {
   return mixv(mixv(x00, x10, c.fy), mixv(x01, x11, c.fy), c.fz);
 }
 
+// The interleaved copy of a scalar set: per voxel (d, t, f, r) as a float4, or
+// as four binary16 values in a uint2 (d and t in .x, f and r in .y, low half
+// first).
+template <typename S>
+struct Aos;
+template <>
+struct Aos<float> {
+  using T = float4;
+  static FX_DEV T pack(const SSet<float>& s, uint32_t i) {
+    return make_float4(__ldg(s.f[0] + i), __ldg(s.f[1] + i), __ldg(s.f[2] + i), __ldg(s.f[3] + i));
+  }
+  static FX_DEV T zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+  static FX_DEV void unpack(const T* __restrict__ a, uint32_t i, float (&o)[4]) {
+    const float4 v = __ldg(a + i);
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+    o[3] = v.w;
+  }
+};
+template <>
+struct Aos<__half> {
+  using T = uint2;
+  static FX_DEV T pack(const SSet<__half>& s, uint32_t i) {
+    const uint32_t d = __half_as_ushort(__ldg(s.f[0] + i)), t = __half_as_ushort(__ldg(s.f[1] + i));
+    const uint32_t f = __half_as_ushort(__ldg(s.f[2] + i)), r = __half_as_ushort(__ldg(s.f[3] + i));
+    return make_uint2(d | (t << 16), f | (r << 16));
+  }
+  static FX_DEV T zero() { return make_uint2(0u, 0u); }
+  static FX_DEV void unpack(const T* __restrict__ a, uint32_t i, float (&o)[4]) {
+    const uint2 v = __ldg(a + i);
+    o[0] = __half2float(__ushort_as_half((unsigned short)(v.x & 0xFFFFu)));
+    o[1] = __half2float(__ushort_as_half((unsigned short)(v.x >> 16)));
+    o[2] = __half2float(__ushort_as_half((unsigned short)(v.y & 0xFFFFu)));
+    o[3] = __half2float(__ushort_as_half((unsigned short)(v.y >> 16)));
+  }
+};
+
+// tri_interp_s of all four fields at once from the interleaved copy: the same
+// corner values, mixed per field in tri_interp's order.
+template <typename S>
+FX_DEV void tri_interp_aos(const typename Aos<S>::T* __restrict__ a, const Tri& c, float (&out)[4]) {
+  float v000[4], v100[4], v010[4], v110[4], v001[4], v101[4], v011[4], v111[4];
+  Aos<S>::unpack(a, c.i000, v000);
+  Aos<S>::unpack(a, c.i100, v100);
+  Aos<S>::unpack(a, c.i010, v010);
+  Aos<S>::unpack(a, c.i110, v110);
+  Aos<S>::unpack(a, c.i001, v001);
+  Aos<S>::unpack(a, c.i101, v101);
+  Aos<S>::unpack(a, c.i011, v011);
+  Aos<S>::unpack(a, c.i111, v111);
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    const float x00 = mixv(v000[f], v100[f], c.fx);
+    const float x10 = mixv(v010[f], v110[f], c.fx);
+    const float x01 = mixv(v001[f], v101[f], c.fx);
+    const float x11 = mixv(v011[f], v111[f], c.fx);
+    out[f] = mixv(mixv(x00, x10, c.fy), mixv(x01, x11, c.fy), c.fz);
+  }
+}
+
 // Calls f(tag) where decltype(tag)::type is the storage type (float or __half).
 template <typename S>
 struct StorageTag {
@@ -475,13 +536,101 @@ __global__ void __launch_bounds__(256) k_advect_velocity_march(Dims dm, const Pa
   else advect_velocity_march<true>(dm, x, y, zb, ze, dt, lim, damp, src, dst);
 }
 
+// ------------------------------------------------------------ interleaved copy
+// Mirrors the current scalar set into the interleaved copy the scalar advection
+// gathers from: every brick that may be non-zero in the set is packed, and every
+// brick whose copy may still hold values of an earlier step is cleared; nz_aos
+// then marks the bricks where the copy may be non-zero. Elsewhere the copy and
+// the set are both zero, so the copy equals the set everywhere.
+//
+// One warp per brick; a lane packs two 8-voxel x rows. Where the width is a
+// multiple of 8, a row of a field is one 16-byte load (binary16) or two (f32),
+// and the row's interleaved values are 64 or 128 contiguous bytes.
+template <typename S>
+FX_DEV void pack_row(const SSet<S>& set, uint32_t i, uint32_t nx, bool live, bool vec, typename Aos<S>::T* __restrict__ aos) {
+  using A = Aos<S>;
+  if (vec) {
+    if constexpr (sizeof(S) == 2) {
+      uint4 out[4] = {};  // 8 voxels x 8 bytes
+      if (live) {
+        uint4 f[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) f[k] = __ldg(reinterpret_cast<const uint4*>(set.f[k] + i));
+        const uint32_t* d = reinterpret_cast<const uint32_t*>(&f[0]);
+        const uint32_t* t = reinterpret_cast<const uint32_t*>(&f[1]);
+        const uint32_t* fu = reinterpret_cast<const uint32_t*>(&f[2]);
+        const uint32_t* r = reinterpret_cast<const uint32_t*>(&f[3]);
+        uint32_t* o = reinterpret_cast<uint32_t*>(out);
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+          const int w = v >> 1, sh = (v & 1) * 16;
+          const uint32_t dv = (d[w] >> sh) & 0xFFFFu, tv = (t[w] >> sh) & 0xFFFFu;
+          const uint32_t fv = (fu[w] >> sh) & 0xFFFFu, rv = (r[w] >> sh) & 0xFFFFu;
+          o[2 * v] = dv | (tv << 16);
+          o[2 * v + 1] = fv | (rv << 16);
+        }
+      }
+      uint4* dst = reinterpret_cast<uint4*>(aos + i);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) dst[k] = out[k];
+    } else {
+      float4 out[8];
+      if (live) {
+        float4 f[4][2];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          f[k][0] = __ldg(reinterpret_cast<const float4*>(set.f[k] + i));
+          f[k][1] = __ldg(reinterpret_cast<const float4*>(set.f[k] + i) + 1);
+        }
+        auto at = [&](int k, int v) {
+          const float4 q = f[k][v >> 2];
+          const int c = v & 3;
+          return c == 0 ? q.x : c == 1 ? q.y : c == 2 ? q.z : q.w;
+        };
+#pragma unroll
+        for (int v = 0; v < 8; ++v) out[v] = make_float4(at(0, v), at(1, v), at(2, v), at(3, v));
+      } else {
+#pragma unroll
+        for (int v = 0; v < 8; ++v) out[v] = A::zero();
+      }
+      float4* dst = reinterpret_cast<float4*>(aos + i);
+#pragma unroll
+      for (int v = 0; v < 8; ++v) dst[v] = out[v];
+    }
+  } else {
+    for (uint32_t v = 0; v < nx; ++v) aos[i + v] = live ? A::pack(set, i + v) : A::zero();
+  }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) k_pack_aos(Dims dm, uint3 bc, SSet<S> set, const uint8_t* __restrict__ nz_set,
+                                                  uint8_t* __restrict__ nz_aos, typename Aos<S>::T* __restrict__ aos) {
+  const uint32_t nb = bc.x * bc.y * bc.z;
+  const uint32_t b = blockIdx.x * 8 + threadIdx.y;  // one warp per brick
+  if (b >= nb) return;
+  const bool live = __ldg(nz_set + b) != 0, stale = nz_aos[b] != 0;
+  if (!live && !stale) return;  // the same for the whole warp
+  const BrickCtx c = brick_ctx(dm, bc, b);
+  const uint32_t nx = min(8u, dm.w - c.x0);
+  const bool vec = nx == 8u && dm.w % 8u == 0u;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const uint32_t row = threadIdx.x + 32u * j;  // 64 rows: y = row & 7, z = row >> 3
+    const uint32_t y = c.y0 + (row & 7u), z = c.z0 + (row >> 3);
+    if (y < dm.h && z < dm.d) pack_row<S>(set, flat(dm, c.x0, y, z), nx, live, vec, aos);
+  }
+  __syncwarp();  // every lane has read nz_aos[b] before it changes
+  if (threadIdx.x == 0) nz_aos[b] = live ? 1 : 0;
+}
+
 // -------------------------------------------------------------- scalar advection
 // advect-scalar-maccormack.wgsl.ts:33-101 / advect-scalar-semilagrangian.wgsl.ts
 // over the bricks of list_adv: flagged bricks are advected into T, the others
 // (T may hold old values there) are zeroed. Emits T's brick summary and non-zero bit.
 template <typename S>
-__global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3 bc, const Params* __restrict__ Pp, int mode, SSet<S> src,
-                                                                  VelField vel, const uint32_t* __restrict__ flags,
+__global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3 bc, const Params* __restrict__ Pp, int mode,
+                                                                  const typename Aos<S>::T* __restrict__ src, VelField vel,
+                                                                  const uint32_t* __restrict__ flags,
                                                                   const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
                                                                   SSet<S> dst, uint8_t* __restrict__ summary, uint8_t* __restrict__ nz) {
   const Params P = *Pp;
@@ -514,18 +663,18 @@ __global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3
           const float fvx = tri_interp(vel.c[0], cs), fvy = tri_interp(vel.c[1], cs), fvz = tri_interp(vel.c[2], cs);
           const float rx = bxp + fvx * dt, ry = byp + fvy * dt, rz = bzp + fvz * dt;
           const Tri cr = tri_corners(dm, rx - 0.5f, ry - 0.5f, rz - 0.5f);
+          float predicted[4], recovered[4], original[4];
+          tri_interp_aos<S>(src, cs, predicted);
+          tri_interp_aos<S>(src, cr, recovered);
+          Aos<S>::unpack(src, ic, original);
 #pragma unroll
           for (int f = 0; f < 4; ++f) {
-            const float predicted = tri_interp_s(src.f[f], cs);
-            const float recovered = tri_interp_s(src.f[f], cr);
-            const float original = ldS(src.f[f], ic);
-            const float corrected = predicted + 0.5f * (original - recovered);
-            out[f] = clampv(corrected, mn(original, predicted), mx(original, predicted));
+            const float corrected = predicted[f] + 0.5f * (original[f] - recovered[f]);
+            out[f] = clampv(corrected, mn(original[f], predicted[f]), mx(original[f], predicted[f]));
           }
           noise = thermal_noise(P, cx, cy, cz);
         } else {
-#pragma unroll
-          for (int f = 0; f < 4; ++f) out[f] = tri_interp_s(src.f[f], cs);
+          tri_interp_aos<S>(src, cs, out);
           noise = thermal_noise(P, spx, spy, spz);
         }
         const float ny = ((float)y + 0.5f) / (float)dm.h;
@@ -1032,12 +1181,14 @@ void injection_bricks(const FusedStep& st, std::vector<uint8_t>& mark, std::vect
 
 }  // namespace
 
-size_t fused_work_bytes(Dims, uint3 bricks) {
+size_t fused_work_bytes(Dims dm, uint3 bricks, size_t aos_voxel_bytes) {
   const size_t nb = (size_t)bricks.x * bricks.y * bricks.z;
-  return 8 * align256(nb) + 3 * align256(nb * 4) + align256(16 * 4) + align256(96 * 4) + align256(sizeof(SolverDev)) + align256(4);
+  const size_t n = (size_t)dm.w * dm.h * dm.d;
+  return 8 * align256(nb) + 3 * align256(nb * 4) + align256(16 * 4) + align256(96 * 4) + align256(sizeof(SolverDev)) + align256(4) +
+         align256(n * aos_voxel_bytes);
 }
 
-void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks) {
+void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks, size_t aos_voxel_bytes) {
   w.dm = dm;
   w.bricks = bricks;
   w.nb = bricks.x * bricks.y * bricks.z;
@@ -1053,7 +1204,7 @@ void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks) {
   w.nz_set[0] = (uint8_t*)take(w.nb);
   w.nz_set[1] = (uint8_t*)take(w.nb);
   w.nz_t = (uint8_t*)take(w.nb);
-  take(w.nb);
+  w.nz_aos = (uint8_t*)take(w.nb);
   take(w.nb);
   w.list_adv = (uint32_t*)take((size_t)w.nb * 4);
   w.list_next = (uint32_t*)take((size_t)w.nb * 4);
@@ -1062,6 +1213,7 @@ void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks) {
   w.mg_bar = (unsigned*)take(96 * 4);
   w.solver = (SolverDev*)take(sizeof(SolverDev));
   w.vmax = (unsigned*)take(4);
+  w.aos = take((size_t)dm.w * dm.h * dm.d * aos_voxel_bytes);
 }
 
 fx_status fused_init(FusedWork& w, cudaStream_t) {
@@ -1377,6 +1529,17 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     ++launches;
   }
 
+  // the interleaved copy of the current set for the scalar advection
+  {
+    Timed tm(w, s, "fused_pack_aos");
+    by_storage(st.half_storage, [&](auto tag) {
+      using S = typename decltype(tag)::type;
+      k_pack_aos<S><<<(nb + 7) / 8, dim3(32, 8), 0, s>>>(dm, bc, sset<S>(st.cur), w.nz_set[cur], w.nz_aos,
+                                                         static_cast<typename Aos<S>::T*>(w.aos));
+    });
+    ++launches;
+  }
+
   // 2. flags of the current set, list of bricks for scalar advection
   FX_CK(cudaMemsetAsync(w.counters, 0, 3 * sizeof(uint32_t), s));
   {
@@ -1414,7 +1577,8 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     Timed tm(w, s, "fused_advect_scalars");
     by_storage(st.half_storage, [&](auto tag) {
       using S = typename decltype(tag)::type;
-      k_advect_scalars<S><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.advect_mode, sset<S>(st.cur), st.vscr, st.flags_cur,
+      k_advect_scalars<S><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.advect_mode,
+                                                               static_cast<const typename Aos<S>::T*>(w.aos), st.vscr, st.flags_cur,
                                                                w.list_adv, c_adv, sset<S>(st.scratch), w.summary_t, w.nz_t);
     });
     ++launches;

@@ -37,6 +37,11 @@ struct FusedWork {
   // Bricks whose voxels may be non-zero, per scalar buffer.
   uint8_t* nz_set[2] = {nullptr, nullptr};
   uint8_t* nz_t = nullptr;
+  // The current scalar set interleaved per voxel (d, t, f, r; 16 B in f32, 8 B in
+  // binary16), rebuilt each step after the injection for the scalar advection's
+  // gathers, and the bricks where that copy may be non-zero.
+  void* aos = nullptr;
+  uint8_t* nz_aos = nullptr;
   // Compacted brick lists.
   uint32_t* list_adv = nullptr;   // bricks the scalar advection kernel visits
   uint32_t* list_next = nullptr;  // bricks the combustion/buoyancy kernels visit
@@ -104,8 +109,10 @@ struct FusedStep {
 };
 
 
-size_t fused_work_bytes(Dims dm, uint3 bricks);
-void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks);
+// aos_voxel_bytes: bytes per voxel of the interleaved scalar copy (16 for f32
+// storage, 8 for binary16).
+size_t fused_work_bytes(Dims dm, uint3 bricks, size_t aos_voxel_bytes);
+void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks, size_t aos_voxel_bytes);
 fx_status fused_init(FusedWork& w, cudaStream_t s);
 fx_status fused_reset(FusedWork& w, cudaStream_t s);
 fx_status fused_invalidate(FusedWork& w, cudaStream_t s);

@@ -692,7 +692,7 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
   o_params = carve(sizeof(Params));
   const size_t o_acc = carve(2 * sizeof(unsigned long long));
   const size_t o_fused = off;
-  off += fused_work_bytes(s->dm, s->bricks);
+  off += fused_work_bytes(s->dm, s->bricks, s->half ? 8 : 16);
   s->arena_bytes = off;
   {
     cudaError_t e = cudaMalloc(&s->arena, s->arena_bytes);
@@ -725,7 +725,7 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
   }
   s->d_params = (Params*)(base + o_params);
   s->d_active_acc = (unsigned long long*)(base + o_acc);
-  fused_work_carve(s->fw, base + o_fused, s->dm, s->bricks);
+  fused_work_carve(s->fw, base + o_fused, s->dm, s->bricks, s->half ? 8 : 16);
   s->fw.use_graphs = (s->opt_flags & FX_OPT_NO_GRAPHS) == 0;
   s->final_vscr = &s->vscr;
 
