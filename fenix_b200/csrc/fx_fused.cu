@@ -641,10 +641,17 @@ __global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3
     const bool active = flag_at(flags, bc, b);
     Energy e{false, false, false};
     bool any = false;
+    // the thread's two voxels share x and y (z and z + 4), hence the row weight
+    // and the y-only sine of the thermal noise at the voxel centre
+    const uint32_t x = c.x0 + (threadIdx.x & 7u), y = c.y0 + ((threadIdx.x >> 3) & 7u);
+    float ny = 0.0f, ysin = 0.0f;
+    if (active) {
+      ny = ((float)y + 0.5f) / (float)dm.h;
+      if (mode == 1) ysin = thermal_noise_ysin(P, (float)y + 0.5f);
+    }
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-      const uint32_t lv = threadIdx.x + kBrickThreads * j;
-      const uint32_t x = c.x0 + (lv & 7u), y = c.y0 + ((lv >> 3) & 7u), z = c.z0 + (lv >> 6);
+      const uint32_t z = c.z0 + ((threadIdx.x + kBrickThreads * j) >> 6);
       const bool inside = x < dm.w && y < dm.h && z < dm.d;
       float out[4] = {0.f, 0.f, 0.f, 0.f};
       if (inside && active) {
@@ -672,12 +679,11 @@ __global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3
             const float corrected = predicted[f] + 0.5f * (original[f] - recovered[f]);
             out[f] = clampv(corrected, mn(original[f], predicted[f]), mx(original[f], predicted[f]));
           }
-          noise = thermal_noise(P, cx, cy, cz);
+          noise = thermal_noise_ys(P, cx, cy, cz, ysin);
         } else {
           tri_interp_aos<S>(src, cs, out);
           noise = thermal_noise(P, spx, spy, spz);
         }
-        const float ny = ((float)y + 0.5f) / (float)dm.h;
         decay_scalars(P, ny, noise, out[0], out[1], out[2], out[3]);
 #pragma unroll
         for (int f = 0; f < 4; ++f) out[f] = qS<S>(out[f]);
@@ -721,10 +727,17 @@ __global__ void __launch_bounds__(kBrickThreads) k_combustion(Dims dm, uint3 bc,
     const bool t_nonzero = nz_t[b] != 0;
     Energy e{false, false, false};
     bool any = false;
+    // the thread's two voxels share x and y (z and z + 4), hence the row weight
+    // and the y-only sine of the thermal cluster
+    const uint32_t x = c.x0 + (threadIdx.x & 7u), y = c.y0 + ((threadIdx.x >> 3) & 7u);
+    float ny = 0.0f, ysin = 0.0f;
+    if (active) {
+      ny = ((float)y + 0.5f) / (float)dm.h;
+      ysin = thermal_cluster_ysin(P, (float)y);
+    }
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-      const uint32_t lv = threadIdx.x + kBrickThreads * j;
-      const uint32_t x = c.x0 + (lv & 7u), y = c.y0 + ((lv >> 3) & 7u), z = c.z0 + (lv >> 6);
+      const uint32_t z = c.z0 + ((threadIdx.x + kBrickThreads * j) >> 6);
       const bool inside = x < dm.w && y < dm.h && z < dm.d;
       if (!inside) continue;
       const uint32_t i = flat(dm, x, y, z);
@@ -739,8 +752,7 @@ __global__ void __launch_bounds__(kBrickThreads) k_combustion(Dims dm, uint3 bc,
         auto hot = [&](uint32_t k) { return comb_hot(ldS(tset.f[1], k), ldS(tset.f[2], k), ldS(tset.f[3], k)); };
         const Nbr n = neighbours(dm, x, y, z, i);
         const float nsum = hot(n.xp) + hot(n.xm) + hot(n.yp) + hot(n.ym) + hot(n.zp) + hot(n.zm);
-        const float ny = ((float)y + 0.5f) / (float)dm.h;
-        combustion_voxel(P, x, y, z, ny, nsum, d, t, f, r);
+        combustion_voxel_c(P, thermal_cluster_ys(P, (float)x, (float)y, (float)z, ysin), ny, nsum, d, t, f, r);
         d = qS<S>(d);
         t = qS<S>(t);
         f = qS<S>(f);
@@ -775,10 +787,12 @@ __global__ void __launch_bounds__(kBrickThreads) k_buoyancy(Dims dm, uint3 bc, c
     const uint32_t b = list[li];
     if (!flag_at(flags, bc, b)) continue;
     const BrickCtx c = brick_ctx(dm, bc, b);
+    // the thread's two voxels share x and y (z and z + 4)
+    const uint32_t x = c.x0 + (threadIdx.x & 7u), y = c.y0 + ((threadIdx.x >> 3) & 7u);
+    const BuoyXY q = buoy_xy(P, dm, x, y);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
-      const uint32_t lv = threadIdx.x + kBrickThreads * j;
-      const uint32_t x = c.x0 + (lv & 7u), y = c.y0 + ((lv >> 3) & 7u), z = c.z0 + (lv >> 6);
+      const uint32_t z = c.z0 + ((threadIdx.x + kBrickThreads * j) >> 6);
       if (x >= dm.w || y >= dm.h || z >= dm.d) continue;
       const uint32_t i = flat(dm, x, y, z);
       const S* D = set.f[0];
@@ -792,7 +806,7 @@ __global__ void __launch_bounds__(kBrickThreads) k_buoyancy(Dims dm, uint3 bc, c
       const float dgy = (ldS(D, n.yp) - ldS(D, n.ym)) * 0.5f;
       const float dgz = (ldS(D, n.zp) - ldS(D, n.zm)) * 0.5f;
       float vx = v.c[0][i], vy = v.c[1][i], vz = v.c[2][i];
-      buoyancy_voxel(P, dm, x, y, z, ldS(D, i), hot_gas, tgx, tgy, tgz, dgx, dgy, dgz, vx, vy, vz);
+      buoyancy_voxel_xy(P, dm, q, x, y, z, ldS(D, i), hot_gas, tgx, tgy, tgz, dgx, dgy, dgz, vx, vy, vz);
       v.c[0][i] = vx;
       v.c[1][i] = vy;
       v.c[2][i] = vz;

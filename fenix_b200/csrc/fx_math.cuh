@@ -386,6 +386,19 @@ FX_DEV void inject_igniter_voxel(const Params& P, const float* __restrict__ src,
 // ---------------------------------------------------------------------------
 
 // scalarThermalNoise, advect-scalar-maccormack.wgsl.ts:52-57.
+// thermal_noise's inner sine, which depends on y only.
+FX_DEV float thermal_noise_ysin(const Params& P, float py) {
+  const float y = py + (-P.time) * 3.1f;
+  return psin(y * 0.079f);
+}
+// thermal_noise given its inner sine (thermal_noise_ysin(P, py)).
+FX_DEV float thermal_noise_ys(const Params& P, float px, float py, float pz, float ysin) {
+  const float t = P.time;
+  const float x = px + t * 1.7f, y = py + (-t) * 3.1f, z = pz + t * 1.1f;
+  const float a = 0.5f + 0.5f * psin(x * 0.097f + y * 0.061f + z * -0.083f);
+  const float b = 0.5f + 0.5f * psin(x * -0.043f + y * 0.137f + z * 0.071f + ysin * 1.6f);
+  return clampv(a * 0.58f + b * 0.42f, 0.0f, 1.0f);
+}
 FX_DEV float thermal_noise(const Params& P, float px, float py, float pz) {
   const float t = P.time;
   const float x = px + t * 1.7f, y = py + (-t) * 3.1f, z = pz + t * 1.1f;
@@ -416,6 +429,20 @@ FX_DEV void decay_scalars(const Params& P, float ny, float noise, T& density, T&
 }
 
 // thermalCluster, combustion-update.wgsl.ts:27-34.
+// thermal_cluster's inner sine, which depends on y only.
+FX_DEV float thermal_cluster_ysin(const Params& P, float py) {
+  const float y = py + P.time * 5.2f;
+  return psin(y * 0.057f);
+}
+// thermal_cluster given its inner sine (thermal_cluster_ysin(P, py)).
+FX_DEV float thermal_cluster_ys(const Params& P, float px, float py, float pz, float ysin) {
+  const float t = P.time;
+  const float x = px + t * 2.2f, y = py + t * 5.2f, z = pz + (-t) * 1.7f;
+  const float body = 0.5f + 0.5f * psin(x * 0.071f + y * 0.093f + z * -0.064f + ysin * 1.8f);
+  const float pocket = 0.5f + 0.5f * psin(x * 0.143f + y * -0.081f + z * 0.119f + psin(x * 0.11f + z * 0.07f) * 1.2f);
+  const float rising = 0.5f + 0.5f * psin(x * 0.18f + y * 0.13f - z * 0.16f + t * 1.4f);
+  return clampv(body * 0.46f + pocket * 0.34f + rising * 0.2f, 0.0f, 1.0f);
+}
 FX_DEV float thermal_cluster(const Params& P, float px, float py, float pz) {
   const float t = P.time;
   const float x = px + t * 2.2f, y = py + t * 5.2f, z = pz + (-t) * 1.7f;
@@ -434,9 +461,17 @@ FX_DEV T comb_hot(T t, T f, T r) {
 // combustion-update.wgsl.ts:52-92, given the six neighbour hot-gas values summed
 // in the reference order (+x, -x, +y, -y, +z, -z).
 template <class T>
+FX_DEV void combustion_voxel_c(const Params& P, float cluster, float ny, T neighbor_sum, T& d, T& t, T& f, T& r);
+
+template <class T>
 FX_DEV void combustion_voxel(const Params& P, uint32_t x, uint32_t y, uint32_t z, float ny, T neighbor_sum, T& d, T& t, T& f, T& r) {
+  combustion_voxel_c(P, thermal_cluster(P, (float)x, (float)y, (float)z), ny, neighbor_sum, d, t, f, r);
+}
+
+// combustion_voxel given the voxel's thermal cluster value.
+template <class T>
+FX_DEV void combustion_voxel_c(const Params& P, float cluster, float ny, T neighbor_sum, T& d, T& t, T& f, T& r) {
   const float dt = P.dt;
-  const float cluster = thermal_cluster(P, (float)x, (float)y, (float)z);
   const T neighbor = neighbor_sum * 0.16666667f;
   const T local_before = comb_hot(t, f, r);
   const T radiative =
@@ -472,9 +507,36 @@ FX_DEV T buoy_hot(T t, T r) {
 
 // apply-buoyancy.wgsl.ts:47-109 given the voxel's own density/hot gas, the
 // central differences of hot gas (tg*) and density (dg*), and its velocity.
+// The terms of buoyancy_voxel that depend on x and y only (a brick thread's two
+// voxels share them).
+struct BuoyXY {
+  float ny, shear_y, s1, s3;
+};
+FX_DEV BuoyXY buoy_xy(const Params& P, const Dims& dm, uint32_t x, uint32_t y) {
+  const float t = P.time;
+  const float fxv = (float)x, fyv = (float)y;
+  BuoyXY o;
+  o.ny = ((float)y + 0.5f) / (float)dm.h;
+  o.shear_y = psin(fyv * 0.073f + t * 0.9f);
+  o.s1 = psin(fyv * 0.117f + t * 1.9f);
+  o.s3 = pcos(fxv * 0.061f + fyv * 0.049f - t * 1.6f);
+  return o;
+}
+
+template <class T>
+FX_DEV void buoyancy_voxel_xy(const Params& P, const Dims& dm, const BuoyXY& q, uint32_t x, uint32_t y, uint32_t z, T d, T hot_gas, T tgx,
+                              T tgy, T tgz, T dgx, T dgy, T dgz, T& vx, T& vy, T& vz);
+
 template <class T>
 FX_DEV void buoyancy_voxel(const Params& P, const Dims& dm, uint32_t x, uint32_t y, uint32_t z, T d, T hot_gas, T tgx, T tgy, T tgz,
                            T dgx, T dgy, T dgz, T& vx, T& vy, T& vz) {
+  buoyancy_voxel_xy(P, dm, buoy_xy(P, dm, x, y), x, y, z, d, hot_gas, tgx, tgy, tgz, dgx, dgy, dgz, vx, vy, vz);
+}
+
+// apply-buoyancy.wgsl.ts:37-110 given the voxel's (x, y) terms.
+template <class T>
+FX_DEV void buoyancy_voxel_xy(const Params& P, const Dims& dm, const BuoyXY& q, uint32_t x, uint32_t y, uint32_t z, T d, T hot_gas, T tgx,
+                              T tgy, T tgz, T dgx, T dgy, T dgz, T& vx, T& vy, T& vz) {
   const float dt = P.dt;
   const float b = P.buoyancy;
   const float response = b * (1.0f + smoothstepv(6.0f, 24.0f, fabsf(b)) * 0.38f);
@@ -482,10 +544,10 @@ FX_DEV void buoyancy_voxel(const Params& P, const Dims& dm, uint32_t x, uint32_t
   const float gw = P.gravity[3];
   const T gfx = P.gravity[0] * d * gw, gfy = P.gravity[1] * d * gw, gfz = P.gravity[2] * d * gw;
   const T entrain = d * smoothstepv(0.04f, 0.3f, hot_gas);
-  const float ny = ((float)y + 0.5f) / (float)dm.h;
+  const float ny = q.ny;
   const float t = P.time;
-  const float fxv = (float)x, fyv = (float)y, fzv = (float)z;
-  const float shear = psin(fyv * 0.073f + t * 0.9f) * 0.35f + psin(fxv * 0.041f - fzv * 0.052f + t * 0.43f) * 0.22f;
+  const float fxv = (float)x, fzv = (float)z;
+  const float shear = q.shear_y * 0.35f + psin(fxv * 0.041f - fzv * 0.052f + t * 0.43f) * 0.22f;
   const float ww = P.wind[3];
   const float wx = P.wind[0], wy = P.wind[1], wz = P.wind[2];
   const T amount = ww * (0.18f + d * 0.55f + ny * 0.45f);
@@ -495,9 +557,9 @@ FX_DEV void buoyancy_voxel(const Params& P, const Dims& dm, uint32_t x, uint32_t
   const T dgl = mx(length3(dgx, dgy, dgz), 0.0001f);
   const T cold = d * (1.0f - smoothstepv(0.12f, 0.72f, hot_gas));
   const T breakup = smoothstepv(0.008f, 0.06f, dgl) * cold;
-  const float s1 = psin(fyv * 0.117f + t * 1.9f);
+  const float s1 = q.s1;
   const float s2 = psin(fxv * 0.071f - fzv * 0.083f + t * 1.35f) * 0.35f;
-  const float s3 = pcos(fxv * 0.061f + fyv * 0.049f - t * 1.6f);
+  const float s3 = q.s3;
   const float sl = length3(s1, s2, s3);
   const float shx = s1 / sl, shy = s2 / sl, shz = s3 / sl;
   const T collapse = d * (1.0f - smoothstepv(0.16f, 0.64f, hot_gas));
