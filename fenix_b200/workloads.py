@@ -152,6 +152,31 @@ def plume_256(seed: int = 1235, size: int = 256) -> Workload:
     return Workload(f"plume_{size}", options, _plume_sources(res, centers, radii, rng), _plume_state(res, centers, radii, heights, seed))
 
 
+def plume_box(res, seed: int = 1239, plumes: int = 3) -> Workload:
+    """Developed plumes on a box-shaped grid res = (w, h, d): `plumes` floor
+    sources at seeded positions, with the plume_256 start state's shape."""
+    rng = Pcg32(seed)
+    w, h, d = res
+    centers, radii, heights = [], [], []
+    for _ in range(plumes):
+        cx = rng.uniform(0.2, 0.8) * w
+        cz = rng.uniform(0.2, 0.8) * d
+        r = rng.uniform(0.04, 0.06) * min(w, d)
+        centers.append((cx, 0.03 * h, cz))
+        radii.append(r)
+        heights.append(rng.uniform(0.6, 0.9) * h)
+    options = {
+        "resolution": tuple(res),
+        "worldSize": 10.0,
+        "gravityStrength": 0.1,
+        "buoyancy": 1.0,
+        "vorticityStrength": 0.3,
+        "qualitySettings": dict(QUALITY_C0),
+    }
+    name = "plume_box_%dx%dx%d" % (w, h, d)
+    return Workload(name, options, _plume_sources(res, centers, radii, rng), _plume_state(res, centers, radii, heights, seed))
+
+
 def plume_64(seed: int = 1234) -> Workload:
     """One emitter at (32, 6, 32) voxels of a 64^3 grid with radius 6 voxels, voxel size 1/64."""
     res = (64, 64, 64)
