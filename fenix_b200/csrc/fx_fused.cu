@@ -846,10 +846,9 @@ __global__ void __launch_bounds__(256) k_vorticity(Dims dm, VelField v, float* _
 // apply-vorticity-confinement.wgsl.ts:30-66 from vScratch into vScratch2, with w
 // recomputed at the voxel and the scalars read only from bricks that may be
 // non-zero.
-template <typename S>
+template <typename S, bool FMAG>
 __global__ void __launch_bounds__(256) k_confinement(Dims dm, uint3 bc, const Params* __restrict__ Pp, VelField v, const float* __restrict__ wmag,
-                                                     SSet<S> set, const uint8_t* __restrict__ nz, VelField out, float* __restrict__ fmag,
-                                                     int write_fmag) {
+                                                     SSet<S> set, const uint8_t* __restrict__ nz, VelField out, float* __restrict__ fmag) {
   const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
   const uint32_t z = blockIdx.z * blockDim.z + threadIdx.z;
@@ -860,7 +859,7 @@ __global__ void __launch_bounds__(256) k_confinement(Dims dm, uint3 bc, const Pa
     out.c[0][i] = vx;
     out.c[1][i] = vy;
     out.c[2][i] = vz;
-    if (write_fmag) fmag[i] = 0.0f;
+    if (FMAG) fmag[i] = 0.0f;
     return;
   }
   const Params P = *Pp;
@@ -877,11 +876,15 @@ __global__ void __launch_bounds__(256) k_confinement(Dims dm, uint3 bc, const Pa
     t = ldS(set.f[1], i);
     r = ldS(set.f[3], i);
   }
-  const float fm = confinement_voxel(P, gx, gy, gz, wx, wy, wz, __ldg(wmag + i), d, t, r, vx, vy, vz);
+  // |F| (a length and a square root) only when the debug fields want it
+  if (FMAG) {
+    fmag[i] = confinement_voxel(P, gx, gy, gz, wx, wy, wz, __ldg(wmag + i), d, t, r, vx, vy, vz);
+  } else {
+    confinement_voxel_v(P, gx, gy, gz, wx, wy, wz, __ldg(wmag + i), d, t, r, vx, vy, vz);
+  }
   out.c[0][i] = vx;
   out.c[1][i] = vy;
   out.c[2][i] = vz;
-  if (write_fmag) fmag[i] = fm;
 }
 
 // Projection (project-velocity.wgsl.ts:21-43) with |v|
@@ -1634,8 +1637,12 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       Timed tm(w, s, "fused_confinement");
       by_storage(st.half_storage, [&](auto tag) {
         using S = typename decltype(tag)::type;
-        k_confinement<S><<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, bc, st.params, st.vscr, st.vort_mag, sset<S>(st.next), w.nz_set[next],
-                                                                st.vscr2, st.conf_mag, st.debug_fields ? 1 : 0);
+        if (st.debug_fields)
+          k_confinement<S, true><<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, bc, st.params, st.vscr, st.vort_mag, sset<S>(st.next),
+                                                                        w.nz_set[next], st.vscr2, st.conf_mag);
+        else
+          k_confinement<S, false><<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, bc, st.params, st.vscr, st.vort_mag, sset<S>(st.next),
+                                                                         w.nz_set[next], st.vscr2, st.conf_mag);
       });
       ++launches;
     }

@@ -589,9 +589,10 @@ FX_DEV void buoyancy_voxel_xy(const Params& P, const Dims& dm, const BuoyXY& q, 
 }
 
 // apply-vorticity-confinement.wgsl.ts:42-65 given the |w| central differences,
-// the voxel's w, |w| and scalars. Returns |F|.
+// the voxel's w, |w| and scalars: applies the force to v and returns it in f.
 template <class T>
-FX_DEV T confinement_voxel(const Params& P, T gx, T gy, T gz, T wx, T wy, T wz, T wmag, T d, T t, T r, T& vx, T& vy, T& vz) {
+FX_DEV void confinement_force(const Params& P, T gx, T gy, T gz, T wx, T wy, T wz, T wmag, T d, T t, T r, T& vx, T& vy, T& vz, T& fx, T& fy,
+                              T& fz) {
   const T gl = mx(length3(gx, gy, gz), 0.0001f);
   const T nx = gx / gl, ny = gy / gl, nz = gz / gl;
   const T hot_gas = clampv(t + r * 0.85f, 0.0f, 1.0f);
@@ -599,14 +600,28 @@ FX_DEV T confinement_voxel(const Params& P, T gx, T gy, T gz, T wx, T wy, T wz, 
                             smoothstepv(0.04f, 0.65f, d) * P.vmask[3],
                         0.0f, 4.0f);
   const float k = P.vorticity_strength;
-  const T fx = (ny * wz - nz * wy) * k * mask * 1.45f;
-  const T fy = (nz * wx - nx * wz) * k * mask * 1.45f;
-  const T fz = (nx * wy - ny * wx) * k * mask * 1.45f;
+  fx = (ny * wz - nz * wy) * k * mask * 1.45f;
+  fy = (nz * wx - nx * wz) * k * mask * 1.45f;
+  fz = (nx * wy - ny * wx) * k * mask * 1.45f;
   const float lim = speed_limit(P);
   vx = clampv(vx + fx * P.dt, -lim, lim);
   vy = clampv(vy + fy * P.dt, -lim, lim);
   vz = clampv(vz + fz * P.dt, -lim, lim);
+}
+
+// The same, returning |F|.
+template <class T>
+FX_DEV T confinement_voxel(const Params& P, T gx, T gy, T gz, T wx, T wy, T wz, T wmag, T d, T t, T r, T& vx, T& vy, T& vz) {
+  T fx, fy, fz;
+  confinement_force(P, gx, gy, gz, wx, wy, wz, wmag, d, t, r, vx, vy, vz, fx, fy, fz);
   return length3(fx, fy, fz);
+}
+
+// The same, without |F|.
+template <class T>
+FX_DEV void confinement_voxel_v(const Params& P, T gx, T gy, T gz, T wx, T wy, T wz, T wmag, T d, T t, T r, T& vx, T& vy, T& vz) {
+  T fx, fy, fz;
+  confinement_force(P, gx, gy, gz, wx, wy, wz, wmag, d, t, r, vx, vy, vz, fx, fy, fz);
 }
 
 }  // namespace fx
