@@ -843,6 +843,79 @@ __global__ void __launch_bounds__(256) k_vorticity(Dims dm, VelField v, float* _
   }
 }
 
+// k_vorticity with four x per thread (widths divisible by 4), one plane per
+// thread: the rows it needs are float4 loads (vx at y -+ 1 and z -+ 1, vy at its
+// row and z -+ 1, vz at its row and y -+ 1), the x neighbours of vy and vz come
+// by warp shuffle (the row ends load theirs), and all of them are issued before
+// the arithmetic. Each component and |w| are curl_at's operations in its order,
+// so the results are the same bits.
+__global__ void __launch_bounds__(256) k_vorticity_v4(Dims dm, VelField v, float* __restrict__ wmag, VelField w, int write_w) {
+  const uint32_t lane = threadIdx.x;
+  const uint32_t x0 = blockIdx.x * 128 + 4 * lane, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+  if (y >= dm.h) return;  // whole warp
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  const bool xin = x0 < dm.w;  // dm.w % 4 == 0: x0 + 3 < dm.w too
+  const uint32_t i = (xin ? x0 : dm.w - 4) + dm.w * (y + dm.h * z);
+  const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  auto ld4 = [&](const float* f, uint32_t k) { return __ldg(reinterpret_cast<const float4*>(f) + (k >> 2)); };
+  auto st4 = [&](float* f, float4 val) { reinterpret_cast<float4*>(f)[i >> 2] = val; };
+  const bool inner = y > 0 && y < dm.h - 1 && z > 0 && z < dm.d - 1;
+  if (!inner) {
+    if (xin) {
+      st4(wmag, zero4);
+      if (write_w) {
+        st4(w.c[0], zero4);
+        st4(w.c[1], zero4);
+        st4(w.c[2], zero4);
+      }
+    }
+    return;  // the whole warp shares y and z
+  }
+  const bool int0 = x0 > 0, int3 = x0 + 3 < dm.w - 1;
+  const bool left_end = lane == 0 && x0 > 0, right_end = lane == 31 && x0 + 4 < dm.w;
+  const float4 XU = ld4(v.c[0], i + sy), XD = ld4(v.c[0], i - sy), XP = ld4(v.c[0], i + sz), XM = ld4(v.c[0], i - sz);
+  const float4 Y = ld4(v.c[1], i), YP = ld4(v.c[1], i + sz), YM = ld4(v.c[1], i - sz);
+  const float4 Z = ld4(v.c[2], i), ZU = ld4(v.c[2], i + sy), ZD = ld4(v.c[2], i - sy);
+  float yl = __shfl_up_sync(0xffffffffu, Y.w, 1), yr = __shfl_down_sync(0xffffffffu, Y.x, 1);
+  float zl = __shfl_up_sync(0xffffffffu, Z.w, 1), zr = __shfl_down_sync(0xffffffffu, Z.x, 1);
+  if (left_end) {
+    yl = __ldg(v.c[1] + i - 1);
+    zl = __ldg(v.c[2] + i - 1);
+  }
+  if (right_end) {
+    yr = __ldg(v.c[1] + i + 4);
+    zr = __ldg(v.c[2] + i + 4);
+  }
+  if (!xin) return;
+  float4 cx = zero4, cy = zero4, cz = zero4, m = zero4;
+  if (int0) {
+    cx.x = ((ZU.x - ZD.x) - (YP.x - YM.x)) * 0.5f;
+    cy.x = ((XP.x - XM.x) - (Z.y - zl)) * 0.5f;
+    cz.x = ((Y.y - yl) - (XU.x - XD.x)) * 0.5f;
+    m.x = length3(cx.x, cy.x, cz.x);
+  }
+  cx.y = ((ZU.y - ZD.y) - (YP.y - YM.y)) * 0.5f;
+  cy.y = ((XP.y - XM.y) - (Z.z - Z.x)) * 0.5f;
+  cz.y = ((Y.z - Y.x) - (XU.y - XD.y)) * 0.5f;
+  m.y = length3(cx.y, cy.y, cz.y);
+  cx.z = ((ZU.z - ZD.z) - (YP.z - YM.z)) * 0.5f;
+  cy.z = ((XP.z - XM.z) - (Z.w - Z.y)) * 0.5f;
+  cz.z = ((Y.w - Y.y) - (XU.z - XD.z)) * 0.5f;
+  m.z = length3(cx.z, cy.z, cz.z);
+  if (int3) {
+    cx.w = ((ZU.w - ZD.w) - (YP.w - YM.w)) * 0.5f;
+    cy.w = ((XP.w - XM.w) - (zr - Z.z)) * 0.5f;
+    cz.w = ((yr - Y.z) - (XU.w - XD.w)) * 0.5f;
+    m.w = length3(cx.w, cy.w, cz.w);
+  }
+  st4(wmag, m);
+  if (write_w) {
+    st4(w.c[0], cx);
+    st4(w.c[1], cy);
+    st4(w.c[2], cz);
+  }
+}
+
 // apply-vorticity-confinement.wgsl.ts:30-66 from vScratch into vScratch2, with w
 // recomputed at the voxel and the scalars read only from bricks that may be
 // non-zero.
@@ -1630,7 +1703,15 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   if (st.vort_on) {
     {
       Timed tm(w, s, "fused_vorticity");
-      k_vorticity<<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, st.vscr, st.vort_mag, st.vort, st.debug_fields ? 1 : 0);
+      static const bool v4 = [] {
+        const char* e = std::getenv("FENIX_VORT_V4");
+        return !(e && *e == '0');
+      }();
+      if (v4 && dm.w % 4 == 0 && dm.w >= 8)
+        k_vorticity_v4<<<dim3((dm.w + 127) / 128, (dm.h + 7) / 8, dm.d), dim3(32, 8, 1), 0, s>>>(dm, st.vscr, st.vort_mag, st.vort,
+                                                                                               st.debug_fields ? 1 : 0);
+      else
+        k_vorticity<<<dense_grid(dm), kDenseBlock, 0, s>>>(dm, st.vscr, st.vort_mag, st.vort, st.debug_fields ? 1 : 0);
       ++launches;
     }
     {
