@@ -87,3 +87,19 @@ def test_sharded_run_on_two_gloo_ranks_equals_one_process(tmp_path):
     np.testing.assert_array_equal(got[0], np.arange(len(wls)))
     np.testing.assert_array_equal(got[1], np.array(ref["checksums"]))
     assert all(c > 0 for c in ref["checksums"])
+
+
+def test_plume_box_workload_is_seeded_and_inside_its_grid():
+    """plume_box: the box-shaped developed plume the long-march parity test steps."""
+    res = (32, 64, 24)
+    a = workloads.plume_box(res, seed=5)
+    b = workloads.plume_box(res, seed=5)
+    assert a.options["resolution"] == res
+    for name, arr in a.state.items():
+        assert arr.shape == (res[2], res[1], res[0]) and arr.dtype == np.float32
+        assert np.array_equal(arr, b.state[name])
+    assert a.state["density"].max() > 0.1 and a.state["velocity_y"].max() > 1.0
+    for src in a.sources:
+        assert all(0.0 < p < 1.0 for p in src.position)
+    c = workloads.plume_box(res, seed=6)
+    assert not np.array_equal(a.state["density"], c.state["density"])
