@@ -379,21 +379,7 @@ cudaError_t march_runs(K kernel, Dims dm, int tx, int ty, int* run) {
     n = std::max(1, per_sm) * std::max(1, sms);
     if (dev >= 0 && dev < 64) slots[dev] = n;
   }
-  const long tiles = (long)((dm.w + tx - 1) / tx) * (long)((dm.h + ty - 1) / ty);
-  int best = 1;
-  double best_eff = -1.0;
-  for (int r = 1; r <= std::max(1, (int)dm.d / 8); ++r) {
-    const int len = ((int)dm.d + r - 1) / r;
-    const int runs = ((int)dm.d + len - 1) / len;
-    const long blocks = tiles * runs;
-    const long waves = (blocks + n - 1) / n;
-    const double eff = (double)blocks / (double)(waves * n);
-    if (eff > best_eff + 1e-9) {
-      best_eff = eff;
-      best = len;
-    }
-  }
-  *run = best;
+  *run = march_plan_waves(dm, tx, ty, n);
   return cudaSuccess;
 }
 
@@ -1160,9 +1146,7 @@ cudaError_t launch_project(cudaStream_t s, Dims dm, const VelField& vs, const fl
       n = std::max(1, per_sm) * std::max(1, sms);
       if (dev >= 0 && dev < 64) slots[dev] = n;
     }
-    const int tiles = (int)(((dm.w + 127) / 128) * ((dm.h + 7) / 8));
-    const int runs = std::max(1, std::min((int)dm.d, n / std::max(tiles, 1)));
-    const int run = ((int)dm.d + runs - 1) / runs;
+    const int run = march_plan_one_wave(dm, n);
     const dim3 g((dm.w + 127) / 128, (dm.h + 7) / 8, (dm.d + run - 1) / run);
     if (write_vmag)
       k_project_march<true><<<g, dim3(32, 8, 1), 0, s>>>(dm, vs, p, vd, vmag, vmax, run);

@@ -1261,10 +1261,7 @@ cudaError_t lean_div_first(cudaStream_t s, Dims dm, VelField v, float* div, floa
       n = std::max(1, per_sm) * std::max(1, sms);
       if (dev >= 0 && dev < 64) slots[dev] = n;
     }
-    const int tiles = (int)(((dm.w + 127) / 128) * ((dm.h + 7) / 8));
-    const int pairs = (int)dm.d / 2;
-    const int runs = std::max(1, std::min(pairs, n / std::max(tiles, 1)));
-    const int run = 2 * ((pairs + runs - 1) / runs);
+    const int run = march_plan_pairs(dm, n);
     const dim3 g((dm.w + 127) / 128, (dm.h + 7) / 8, (dm.d + run - 1) / run);
     k_div_march<<<g, dim3(32, 8, 1), 0, s>>>(dm, v, div, p1, mid, mid_div, restrict_mid ? 1 : 0, run);
     return cudaGetLastError();
@@ -1277,6 +1274,38 @@ bool sweep_variant_valid(int variant, Dims dm) {
   if (variant < 0 || variant >= kSweepVariants) return false;
   if (variant >= SWEEP_VEC4_Z2) return dm.w % 4 == 0 && dm.w >= 8;
   return variant < SWEEP_VEC_Z2 || (dm.w % 2 == 0 && dm.w >= 4);
+}
+
+int march_plan_one_wave(Dims dm, int slots) {
+  const int tiles = (int)(((dm.w + 127) / 128) * ((dm.h + 7) / 8));
+  const int runs = std::max(1, std::min((int)dm.d, std::max(slots, 1) / std::max(tiles, 1)));
+  return ((int)dm.d + runs - 1) / runs;
+}
+
+int march_plan_pairs(Dims dm, int slots) {
+  const int tiles = (int)(((dm.w + 127) / 128) * ((dm.h + 7) / 8));
+  const int pairs = std::max(1, (int)dm.d / 2);
+  const int runs = std::max(1, std::min(pairs, std::max(slots, 1) / std::max(tiles, 1)));
+  return 2 * ((pairs + runs - 1) / runs);
+}
+
+int march_plan_waves(Dims dm, int tx, int ty, int slots) {
+  const long n = std::max(slots, 1);
+  const long tiles = (long)((dm.w + tx - 1) / tx) * (long)((dm.h + ty - 1) / ty);
+  int best = 1;
+  double best_eff = -1.0;
+  for (int r = 1; r <= std::max(1, (int)dm.d / 8); ++r) {
+    const int len = ((int)dm.d + r - 1) / r;
+    const int runs = ((int)dm.d + len - 1) / len;
+    const long blocks = tiles * runs;
+    const long waves = (blocks + n - 1) / n;
+    const double eff = (double)blocks / (double)(waves * n);
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = len;
+    }
+  }
+  return best;
 }
 
 static cudaError_t march_run(Dims dm, int* run);
@@ -1326,9 +1355,7 @@ static cudaError_t march_run(Dims dm, int* run) {
   int slots = 0;
   const cudaError_t e = march_slots(&slots);
   if (e != cudaSuccess) return e;
-  const int tiles = (int)(((dm.w + 127) / 128) * ((dm.h + 7) / 8));
-  const int runs = std::max(1, std::min((int)dm.d, slots / std::max(tiles, 1)));
-  *run = ((int)dm.d + runs - 1) / runs;
+  *run = march_plan_one_wave(dm, slots);
   return cudaSuccess;
 }
 
@@ -1350,9 +1377,7 @@ static cudaError_t march_run_of(K kernel, Dims dm, int* run) {
     slots = std::max(1, per_sm) * std::max(1, sms);
     if (dev >= 0 && dev < 64) cached[dev] = slots;
   }
-  const int tiles = (int)(((dm.w + 127) / 128) * ((dm.h + 7) / 8));
-  const int runs = std::max(1, std::min((int)dm.d, slots / std::max(tiles, 1)));
-  *run = ((int)dm.d + runs - 1) / runs;
+  *run = march_plan_one_wave(dm, slots);
   return cudaSuccess;
 }
 

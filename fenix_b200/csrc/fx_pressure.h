@@ -65,6 +65,17 @@ enum SweepVariant {
   SWEEP_VEC4_MARCH = 8,  // four x per thread, one wave of blocks marching in z
   kSweepVariants = 9
 };
+// Planes per block of a marching kernel (host arithmetic; `slots` = resident
+// blocks of the kernel on the device). One wave over 128 x 8 row tiles: the
+// tiles times the runs fill the slots once (at most one run per plane).
+int march_plan_one_wave(Dims dm, int slots);
+// The same with runs of an even number of planes (dm.d even), for kernels that
+// pair planes.
+int march_plan_pairs(Dims dm, int slots);
+// Over tx x ty tiles: the run count (at most one per 8 planes) whose blocks fill
+// whole waves of the slots best, the fewest runs among equals.
+int march_plan_waves(Dims dm, int tx, int ty, int slots);
+
 bool sweep_variant_valid(int variant, Dims dm);
 int sweep_variant_default(Dims dm);
 cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float* div, const float* src, float* dst, Dims mid,

@@ -1398,6 +1398,19 @@ const char* fx_batch_last_error(fx_batch* b) { return b ? b->err.c_str() : g_las
 
 // Test hook: exhaustive comparison of the pressure kernels' division by 6 with
 // the IEEE division on the device. Returns the mismatch count in *bad.
+// Test entry (host arithmetic only): the planes per block a marching kernel
+// launch uses for a w x h x d level with `slots` resident blocks. kind 0: one
+// wave over 128 x 8 tiles (the fine sweeps, the projection); 1: the same in
+// runs of an even number of planes (the divergence; d must be even); 2: whole
+// waves over 32 x 8 tiles (the velocity advection).
+fx_status fx_test_march_plan(int32_t kind, uint32_t w, uint32_t h, uint32_t d, int32_t slots, int32_t* run) {
+  if (!run || w == 0 || h == 0 || d == 0 || slots < 1 || kind < 0 || kind > 2 || (kind == 1 && d % 2 != 0))
+    return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_test_march_plan: invalid argument");
+  const Dims dm{w, h, d};
+  *run = kind == 0 ? march_plan_one_wave(dm, slots) : kind == 1 ? march_plan_pairs(dm, slots) : march_plan_waves(dm, 32, 8, slots);
+  return FX_OK;
+}
+
 fx_status fx_test_div6_exhaustive(unsigned long long* bad) {
   if (!bad) return FX_ERR_INVALID_ARGUMENT;
   return div6_exhaustive_check(bad) == cudaSuccess ? FX_OK : FX_ERR_CUDA;
