@@ -35,3 +35,21 @@ def test_long_marches_equal_the_oracle(storage):
         sim.step(k * DT, DT)
         orc.step(k * DT, DT)
         compare(sim, orc, EXPOSED_FIELDS, f"plume_box {storage} step {k + 1}")
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("res", [(52, 30, 11), (48, 32, 24)])
+def test_four_x_kernels_with_debug_fields(storage, res):
+    """Widths divisible by 4 with the debug fields on: the four-x |w| kernel also
+    writes w, the projection writes |v|, and the ragged heights and depths
+    (30 rows, 11 planes) leave partial row tiles, an odd depth (the divergence
+    falls back to k_div_first) and a width that is not a multiple of 8 (the
+    interleaved copy's row-by-row path)."""
+    from parity_util import DEBUG_FIELDS, all_kind_sources, run_lockstep
+
+    opts = {"resolution": res, "worldSize": 1.5}
+    sim = createCombustionVolumeSimulation(opts, device=0, kernels="fused", debug_fields=True, storage=storage)
+    orc = OracleSimulation(opts, precision=32, storage=storage)
+    for s in (sim, orc):
+        s.updateSources(all_kind_sources(seed=404.0))
+    run_lockstep(sim, orc, 8, DT, EXPOSED_FIELDS + DEBUG_FIELDS, f"four-x debug {res} {storage}")
