@@ -705,7 +705,6 @@ __global__ void __launch_bounds__(kBrickThreads) k_combustion(Dims dm, uint3 bc,
                                                               uint8_t* __restrict__ summary, uint8_t* __restrict__ nz) {
   const Params P = *Pp;
   const uint32_t n = *count;
-  const uint32_t W1 = dm.w - 1u, H1 = dm.h - 1u, D1 = dm.d - 1u;
   for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
     const uint32_t b = list[li];
     const BrickCtx c = brick_ctx(dm, bc, b);
@@ -768,7 +767,6 @@ __global__ void __launch_bounds__(kBrickThreads) k_buoyancy(Dims dm, uint3 bc, c
                                                             const uint32_t* __restrict__ count, VelField v) {
   const Params P = *Pp;
   const uint32_t n = *count;
-  const uint32_t W1 = dm.w - 1u, H1 = dm.h - 1u, D1 = dm.d - 1u;
   for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
     const uint32_t b = list[li];
     if (!flag_at(flags, bc, b)) continue;

@@ -777,7 +777,7 @@ __global__ void __launch_bounds__(256, 4) k_sweep_march(Dims dm, const float* __
   auto crow = [&](int z) { return (src && z >= 0 && z < D) ? __ldg(src4 + ((base + sz * (uint32_t)z) >> 2)) : zero4; };
   float4 cm = crow(zb - 1), c0 = crow(zb), cp = crow(zb + 1);
   // Plane zb's own rows; every later plane's are loaded one iteration ahead.
-  uint32_t i = base + sz * (uint32_t)zb;
+  const uint32_t i = base + sz * (uint32_t)zb;
   float4 dv = __ldg(div4 + (i >> 2));
   float4 yp = src ? __ldg(src4 + ((i + sy) >> 2)) : zero4;
   float4 ym = src ? __ldg(src4 + ((i - sy) >> 2)) : zero4;
@@ -922,7 +922,7 @@ __global__ void __launch_bounds__(256, 3) k_sweep_march_prolong(Dims dm, const f
 
   auto crow = [&](int z) { return (src && z >= 0 && z < D) ? __ldg(src4 + ((base + sz * (uint32_t)z) >> 2)) : zero4; };
   float4 cm = crow(zb - 1), c0 = crow(zb), cp = crow(zb + 1);
-  uint32_t i = base + sz * (uint32_t)zb;
+  const uint32_t i = base + sz * (uint32_t)zb;
   float4 dv = __ldg(div4 + (i >> 2));
   float4 yp = src ? __ldg(src4 + ((i + sy) >> 2)) : zero4;
   float4 ym = src ? __ldg(src4 + ((i - sy) >> 2)) : zero4;
@@ -977,7 +977,6 @@ __global__ void __launch_bounds__(256, 3) k_sweep_march_prolong(Dims dm, const f
     ym = n_ym;
     xle = n_xle;
     xre = n_xre;
-    i = in;
   }
 }
 
