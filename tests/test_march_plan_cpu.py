@@ -45,8 +45,6 @@ def test_runs_cover_every_plane_once(kind):
         assert (blocks - 1) * run < d <= blocks * run  # no empty block, every plane covered
         if kind == 1:
             assert run % 2 == 0  # runs start on even planes and hold whole pairs
-        if kind == 2:
-            assert run == d or d // 8 >= 1
 
 
 def test_one_wave_plan_fits_the_resident_blocks():
@@ -73,3 +71,20 @@ def test_invalid_arguments_are_rejected():
     assert lib.fx_test_march_plan(3, 64, 64, 64, 592, ctypes.byref(run)) != 0
     assert lib.fx_test_march_plan(0, 0, 64, 64, 592, ctypes.byref(run)) != 0
     assert lib.fx_test_march_plan(0, 64, 64, 64, 0, ctypes.byref(run)) != 0
+
+
+def wave_efficiency(tiles_n, d, run, slots):
+    blocks = tiles_n * -(-d // run)
+    waves = -(-blocks // slots)
+    return blocks / (waves * slots)
+
+
+def test_wave_plan_fills_whole_waves_best():
+    """kind 2 (the velocity advection, 32 x 8 tiles): no run length reachable
+    with at most one run per 8 planes fills whole waves better."""
+    for (w, h, d), slots in itertools.product(SHAPES, SLOTS):
+        t = tiles(w, h, 32, 8)
+        run = plan(2, w, h, d, slots)
+        best = max(wave_efficiency(t, d, -(-d // r), slots) for r in range(1, max(1, d // 8) + 1))
+        assert wave_efficiency(t, d, run, slots) >= best - 1e-9, (w, h, d, slots, run)
+
