@@ -45,3 +45,19 @@ def test_constant_divisions_equal_ieee_division(tmp_path):
     assert len(rows) == len(divisors)
     failures = [r for r in rows if int(r[1]) != 0]
     assert not failures, f"divisors whose short sequence differs from IEEE division: {failures}"
+
+
+def test_shared_reciprocal_division_in_the_normal_range(tmp_path):
+    """A division by a shared reciprocal, RN32(RN64(x * r)) with r within one f64
+    ulp of 1/y, equals the IEEE quotient wherever |x / y| >= 2^-126; below that an
+    exact quotient can be a midpoint of the subnormal grid (the check finds such
+    pairs), so a kernel using it must keep the IEEE division there
+    (tests/native/recip_division_check.c)."""
+    exe = str(tmp_path / "recip_division_check")
+    subprocess.run(["gcc", "-O2", "-fopenmp", "-ffp-contract=off", os.path.join(ROOT, "tests", "native", "recip_division_check.c"),
+                    "-o", exe, "-lm"], check=True)
+    out = subprocess.run([exe, str(1 << 24)], capture_output=True, text=True, check=True).stdout.split()
+    checked, bad, bad_normal = int(out[0]), int(out[1]), int(out[2])
+    assert checked > (1 << 24)
+    assert bad_normal == 0, out
+    assert bad > 0  # the subnormal-grid ties exist, which is why the range limit is needed
