@@ -1256,7 +1256,7 @@ void injection_bricks(const FusedStep& st, std::vector<uint8_t>& mark, std::vect
 size_t fused_work_bytes(Dims dm, uint3 bricks, size_t aos_voxel_bytes) {
   const size_t nb = (size_t)bricks.x * bricks.y * bricks.z;
   const size_t n = (size_t)dm.w * dm.h * dm.d;
-  return 8 * align256(nb) + 3 * align256(nb * 4) + align256(16 * 4) + align256(96 * 4) + align256(sizeof(SolverDev)) + align256(4) +
+  return 8 * align256(nb) + 3 * align256(nb * 4) + align256(16 * 4) + align256(sizeof(SolverDev)) + align256(4) +
          align256(n * aos_voxel_bytes);
 }
 
@@ -1282,7 +1282,6 @@ void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks, size_t ao
   w.list_next = (uint32_t*)take((size_t)w.nb * 4);
   w.list_inj = (uint32_t*)take((size_t)w.nb * 4);
   w.counters = (uint32_t*)take(16 * 4);
-  w.mg_bar = (unsigned*)take(96 * 4);
   w.solver = (SolverDev*)take(sizeof(SolverDev));
   w.vmax = (unsigned*)take(4);
   w.aos = take((size_t)dm.w * dm.h * dm.d * aos_voxel_bytes);
@@ -1290,8 +1289,8 @@ void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks, size_t ao
 
 fx_status fused_init(FusedWork& w, cudaStream_t) {
   if (cudaEventCreateWithFlags(&w.inj_event, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
-  if (cudaMallocHost(&w.host_list_inj, ((size_t)w.nb + 1) * 4) != cudaSuccess) return FX_ERR_OUT_OF_MEMORY;
-  if (cudaMallocHost(&w.host_cont, sizeof(int)) != cudaSuccess) return FX_ERR_OUT_OF_MEMORY;
+  if (host_alloc((void**)&w.host_list_inj, ((size_t)w.nb + 1) * 4) != cudaSuccess) return FX_ERR_OUT_OF_MEMORY;
+  if (host_alloc((void**)&w.host_cont, sizeof(int)) != cudaSuccess) return FX_ERR_OUT_OF_MEMORY;
   if (cudaStreamCreateWithFlags(&w.aux, cudaStreamNonBlocking) != cudaSuccess) return FX_ERR_CUDA;
   w.valid = true;  // the arena starts cleared: every brick is zero
   return FX_OK;
@@ -1386,7 +1385,7 @@ fx_status fused_prepare(FusedWork& w, const FusedStep& st, uint32_t* ninj_out, F
   const uint32_t nb = w.nb;
   const int cur = st.cur_index, next = cur ^ 1;
   uint32_t launches = 0;
-  const uint32_t brick_grid = std::max<uint32_t>(1, std::min<uint32_t>(nb, 148u * 8u));
+  const uint32_t brick_grid = std::max<uint32_t>(1, std::min<uint32_t>(nb, (uint32_t)device_sm_count() * 8u));
   uint32_t* c_inj = w.counters + 3;
 
   if (!w.valid) {
@@ -1579,7 +1578,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   const uint32_t nb = w.nb;
   const int cur = st.cur_index, next = cur ^ 1;
   uint32_t launches = 0;
-  const uint32_t brick_grid = std::max<uint32_t>(1, std::min<uint32_t>(nb, 148u * 8u));
+  const uint32_t brick_grid = std::max<uint32_t>(1, std::min<uint32_t>(nb, (uint32_t)device_sm_count() * 8u));
   uint32_t* c_adv = w.counters + 0;
   uint32_t* c_next = w.counters + 1;
   uint32_t* c_inj = w.counters + 3;
@@ -1735,220 +1734,99 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     FX_CK(cudaMemsetAsync(M.p[0], 0, (size_t)M.dm.w * M.dm.h * M.dm.d * sizeof(float), s));
     FX_CK(cudaMemsetAsync(C.p[0], 0, (size_t)C.dm.w * C.dm.h * C.dm.d * sizeof(float), s));
 
-    if (pressure_plan() == 0) {
-      // Per-voxel plan. Fine writes in order: the first sweep (fused into the
-      // divergence kernel), the remaining pre sweeps (the last one adds the
-      // prolongation when the reference prolongs into it), the prolongation alone
-      // when there is no pre sweep, then the post sweeps. The last write lands in
-      // p[last]; going backwards the writes alternate with the other buffer, so no
-      // sweep reads the buffer it writes.
-      const bool prolong_live = (m & 1) == 0;  // odd m: the correction lands in a buffer never read
-      const int nwrites = std::max(m, 0) + (m == 0 ? 1 : 0) + n;
-      std::vector<float*> outs(nwrites);
-      for (int i = nwrites; i-- > 0;)
-        outs[i] = (i + 1 == nwrites) ? F.p[last_p] : (outs[i + 1] == F.p[last_p] ? F.p[last_p ^ 1] : F.p[last_p]);
-      int wi = 0;
-      const float* chain = nullptr;
+    // Per-voxel plan. Fine writes in order: the first sweep (fused into the
+    // divergence kernel), the remaining pre sweeps (the last one adds the
+    // prolongation when the reference prolongs into it), the prolongation alone
+    // when there is no pre sweep, then the post sweeps. The last write lands in
+    // p[last]; going backwards the writes alternate with the other buffer, so no
+    // sweep reads the buffer it writes.
+    const bool prolong_live = (m & 1) == 0;  // odd m: the correction lands in a buffer never read
+    const int nwrites = std::max(m, 0) + (m == 0 ? 1 : 0) + n;
+    std::vector<float*> outs(nwrites);
+    for (int i = nwrites; i-- > 0;)
+      outs[i] = (i + 1 == nwrites) ? F.p[last_p] : (outs[i + 1] == F.p[last_p] ? F.p[last_p ^ 1] : F.p[last_p]);
+    int wi = 0;
+    const float* chain = nullptr;
+    {
+      Timed tm(w, s, "fused_div_first_sweep");
+      FX_CK(lean_div_first(s, dm, *vfinal, F.div, m >= 1 ? outs[0] : nullptr, M.dm, M.div, fuse_restrict));
+      ++launches;
+    }
+    if (m >= 1) chain = outs[wi++];
+    if (!fuse_restrict) {
+      Timed tm(w, s, "fused_restrict");
+      plain_restrict(s, F.dm, M.dm, F.div, M.div);
+      ++launches;
+    }
+    int mid = 0;
+    if (prolong_live) {
+      // Mid and coarse levels sweep by sweep (inside the step's CUDA graph the
+      // launch gaps are short). The first sweep of a level reads the cleared
+      // buffer, so it is computed from the divergence alone.
+      int mid_pre = 0;
       {
-        Timed tm(w, s, "fused_div_first_sweep");
-        FX_CK(lean_div_first(s, dm, *vfinal, F.div, m >= 1 ? outs[0] : nullptr, M.dm, M.div, fuse_restrict));
-        ++launches;
-      }
-      if (m >= 1) chain = outs[wi++];
-      if (!fuse_restrict) {
-        Timed tm(w, s, "fused_restrict");
-        plain_restrict(s, F.dm, M.dm, F.div, M.div);
-        ++launches;
-      }
-      int mid = 0;
-      if (prolong_live && multigrid_plan() == 1) {
-        Timed tm(w, s, "fused_multigrid_lower");
-        FX_CK(mg_lower_launch(s, M, C, st.q[4], st.q[6], st.q[5], w.mg_bar, &mid));
-        ++launches;
-      } else if (prolong_live) {
-        // Mid and coarse levels sweep by sweep (inside the step's CUDA graph the
-        // launch gaps are short). The first sweep of a level reads the cleared
-        // buffer, so it is computed from the divergence alone.
-        int mid_pre = 0;
-        {
-          int a = 0;
-          for (int k = 0; k < st.q[4]; ++k) {
-            Timed tm(w, s, "fused_sweep_mid");
-            FX_CK(lean_sweep_variant(s, st.sweep_variant[1], M.dm, M.div, k == 0 ? nullptr : M.p[a], M.p[a ^ 1], M.dm, nullptr));
-            a ^= 1;
-            ++launches;
-          }
-          mid_pre = a;
-        }
-        {
-          Timed tm(w, s, "fused_restrict");
-          plain_restrict(s, M.dm, C.dm, M.div, C.div);
-          ++launches;
-        }
-        int coarse = 0;
-        {
-          int a = 0;
-          for (int k = 0; k < st.q[6]; ++k) {
-            Timed tm(w, s, "fused_sweep_coarse");
-            FX_CK(lean_sweep_variant(s, st.sweep_variant[2], C.dm, C.div, k == 0 ? nullptr : C.p[a], C.p[a ^ 1], C.dm, nullptr));
-            a ^= 1;
-            ++launches;
-          }
-          coarse = a;
-        }
-        {
-          Timed tm(w, s, "fused_prolong");
-          plain_prolong(s, C.dm, M.dm, C.p[coarse], M.p[0]);
-          ++launches;
-        }
-        mid = mid_pre;
-        for (int k = 0; k < st.q[5]; ++k) {
+        int a = 0;
+        for (int k = 0; k < st.q[4]; ++k) {
           Timed tm(w, s, "fused_sweep_mid");
-          FX_CK(lean_sweep_variant(s, st.sweep_variant[1], M.dm, M.div, M.p[mid], M.p[mid ^ 1], M.dm, nullptr));
-          mid ^= 1;
-          ++launches;
-        }
-      }
-      for (int k = 2; k <= m; ++k) {
-        const bool add = prolong_live && k == m;
-        Timed tm(w, s, add ? "fused_sweep_prolong" : "fused_sweep");
-        FX_CK(lean_sweep_variant(s, st.sweep_variant[0], dm, F.div, chain, outs[wi], M.dm, add ? M.p[mid] : nullptr));
-        chain = outs[wi++];
-        ++launches;
-      }
-      if (m == 0) {
-        Timed tm(w, s, "fused_prolong_fine");
-        FX_CK(lean_prolong_zero(s, dm, outs[wi], M.dm, M.p[mid]));
-        chain = outs[wi++];
-        ++launches;
-      }
-      for (int k = 1; k <= n; ++k) {
-        Timed tm(w, s, "fused_sweep");
-        FX_CK(lean_sweep_variant(s, st.sweep_variant[0], dm, F.div, chain, outs[wi], M.dm, nullptr));
-        chain = outs[wi++];
-        ++launches;
-      }
-      {
-        Timed tm(w, s, "fused_project");
-        FX_CK(cudaMemsetAsync(w.vmax, 0, sizeof(unsigned), s));
-        FX_CK(launch_project(s, dm, *vfinal, F.p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax));
-        ++launches;
-      }
-    } else {
-      // The projection of these passes does not record max |v|: mark it unknown.
-      FX_CK(cudaMemsetAsync(w.vmax, 0xFF, sizeof(unsigned), s));
-      // Plan the fine passes: pre-smoothing in groups of <= 4 sweeps (the first one
-      // also computes the divergence), post-smoothing in groups of <= 4 sweeps (the
-      // first adds the prolongation, the last finishes with the projection).
-      struct Plan {
-        int sweeps;
-        ZInput input;
-        bool divv, proj;
-      };
-      std::vector<Plan> pre, post;
-      const int kmax = zpass_max_sweeps();
-      for (int left = m; left > 0;) {
-        const int k = std::min(left, kmax);
-        pre.push_back({k, pre.empty() ? ZIN_ZERO : ZIN_BUF, pre.empty(), false});
-        left -= k;
-      }
-      {
-        const ZInput first_in = (m & 1) ? ZIN_BUF : (m == 0 ? ZIN_ZERO_PROLONG : ZIN_BUF_PROLONG);
-        if (n == 0) {
-          post.push_back({0, first_in, false, true});
-        } else {
-          for (int left = n; left > 0;) {
-            const int k = std::min(left, kmax);
-            post.push_back({k, post.empty() ? first_in : ZIN_BUF, false, left - k == 0});
-            left -= k;
-          }
-        }
-      }
-      // Output buffers: the last pass writes p[last]; going backwards the passes
-      // alternate with the other buffer, so no pass reads the buffer it writes.
-      const size_t npass = pre.size() + post.size();
-      std::vector<float*> outs(npass);
-      for (size_t i = npass; i-- > 0;)
-        outs[i] = (i + 1 == npass) ? F.p[last_p] : (outs[i + 1] == F.p[last_p] ? F.p[last_p ^ 1] : F.p[last_p]);
-      size_t pi = 0;
-      const float* chain = nullptr;  // the latest fine pressure (nullptr: the cleared buffer)
-      if (m == 0) {
-        Timed tm(w, s, "fused_divergence");
-        plain_divergence(s, dm, *vfinal, F.div);
-        ++launches;
-      }
-      for (const Plan& pl : pre) {
-        ZPass zp{};
-        zp.dm = dm;
-        zp.mid = M.dm;
-        zp.sweeps = pl.sweeps;
-        zp.zchunk = zpass_zchunk();
-        zp.input = pl.input;
-        zp.div_from_velocity = pl.divv;
-        zp.project = false;
-        zp.restrict_mid = (pl.divv && fuse_restrict) ? 1 : 0;
-        zp.p_in = chain;
-        zp.div_in = F.div;
-        zp.div_out = F.div;
-        zp.mid_div = M.div;
-        zp.p_out = outs[pi];
-        zp.vfin = *vfinal;
-        Timed tm(w, s, pl.divv ? "fused_zpass_div_pre" : "fused_zpass_pre");
-        FX_CK(zpass_launch(s, zp));
-        ++launches;
-        chain = outs[pi++];
-      }
-      if (m == 0 || !fuse_restrict) {
-        Timed tm(w, s, "fused_restrict");
-        plain_restrict(s, F.dm, M.dm, F.div, M.div);
-        ++launches;
-      }
-      // mid and coarse levels (sweep by sweep)
-      auto smooth = [&](const LevelBuf& L, int iters, int start, const char* name) {
-        int a = start;
-        for (int k = 0; k < iters; ++k) {
-          Timed tm(w, s, name);
-          plain_jacobi(s, L.dm, L.div, L.p[a], L.p[a ^ 1]);
+          FX_CK(lean_sweep_variant(s, st.sweep_variant[1], M.dm, M.div, k == 0 ? nullptr : M.p[a], M.p[a ^ 1], M.dm, nullptr));
           a ^= 1;
           ++launches;
         }
-        return a;
-      };
-      const int mid_pre = smooth(M, st.q[4], 0, "fused_jacobi_mid");
+        mid_pre = a;
+      }
       {
         Timed tm(w, s, "fused_restrict");
         plain_restrict(s, M.dm, C.dm, M.div, C.div);
         ++launches;
       }
-      const int coarse = smooth(C, st.q[6], 0, "fused_jacobi_coarse");
+      int coarse = 0;
+      {
+        int a = 0;
+        for (int k = 0; k < st.q[6]; ++k) {
+          Timed tm(w, s, "fused_sweep_coarse");
+          FX_CK(lean_sweep_variant(s, st.sweep_variant[2], C.dm, C.div, k == 0 ? nullptr : C.p[a], C.p[a ^ 1], C.dm, nullptr));
+          a ^= 1;
+          ++launches;
+        }
+        coarse = a;
+      }
       {
         Timed tm(w, s, "fused_prolong");
         plain_prolong(s, C.dm, M.dm, C.p[coarse], M.p[0]);
         ++launches;
       }
-      const int mid = smooth(M, st.q[5], mid_pre, "fused_jacobi_mid");
-      for (const Plan& pl : post) {
-        ZPass zp{};
-        zp.dm = dm;
-        zp.mid = M.dm;
-        zp.sweeps = pl.sweeps;
-        zp.zchunk = zpass_zchunk();
-        zp.input = pl.input;
-        zp.div_from_velocity = false;
-        zp.project = pl.proj;
-        zp.p_in = chain;
-        zp.div_in = F.div;
-        zp.mid_p = M.p[mid];
-        zp.p_out = outs[pi];
-        zp.vfin = *vfinal;
-        zp.vcur = st.vcur;
-        zp.vmag = st.vel_mag;
-        zp.write_vmag = st.debug_on ? 1 : 0;
-        Timed tm(w, s, pl.proj ? "fused_zpass_post_project" : "fused_zpass_post");
-        FX_CK(zpass_launch(s, zp));
+      mid = mid_pre;
+      for (int k = 0; k < st.q[5]; ++k) {
+        Timed tm(w, s, "fused_sweep_mid");
+        FX_CK(lean_sweep_variant(s, st.sweep_variant[1], M.dm, M.div, M.p[mid], M.p[mid ^ 1], M.dm, nullptr));
+        mid ^= 1;
         ++launches;
-        chain = outs[pi++];
       }
+    }
+    for (int k = 2; k <= m; ++k) {
+      const bool add = prolong_live && k == m;
+      Timed tm(w, s, add ? "fused_sweep_prolong" : "fused_sweep");
+      FX_CK(lean_sweep_variant(s, st.sweep_variant[0], dm, F.div, chain, outs[wi], M.dm, add ? M.p[mid] : nullptr));
+      chain = outs[wi++];
+      ++launches;
+    }
+    if (m == 0) {
+      Timed tm(w, s, "fused_prolong_fine");
+      FX_CK(lean_prolong_zero(s, dm, outs[wi], M.dm, M.p[mid]));
+      chain = outs[wi++];
+      ++launches;
+    }
+    for (int k = 1; k <= n; ++k) {
+      Timed tm(w, s, "fused_sweep");
+      FX_CK(lean_sweep_variant(s, st.sweep_variant[0], dm, F.div, chain, outs[wi], M.dm, nullptr));
+      chain = outs[wi++];
+      ++launches;
+    }
+    {
+      Timed tm(w, s, "fused_project");
+      FX_CK(cudaMemsetAsync(w.vmax, 0, sizeof(unsigned), s));
+      FX_CK(launch_project(s, dm, *vfinal, F.p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax));
+      ++launches;
     }
   } else {
     // 10. projection with the pressure of the last solve (+ |v|)
@@ -1975,17 +1853,10 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   return FX_OK;
 }
 
-fx_status fused_check_device_error(FusedWork& w, cudaStream_t s) {
-  unsigned h = 0;
-  if (cudaMemcpyAsync(&h, w.mg_bar + 64, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess) return FX_ERR_CUDA;
-  if (cudaStreamSynchronize(s) != cudaSuccess) return FX_ERR_CUDA;
-  return h ? FX_ERR_TIMEOUT : FX_OK;
-}
-
 fx_status fused_count_active(FusedWork& w, cudaStream_t s, const uint32_t* flags, uint32_t nb, uint32_t* out) {
   uint32_t* c = w.counters + 2;
   if (cudaMemsetAsync(c, 0, 4, s) != cudaSuccess) return FX_ERR_CUDA;
-  k_count_flags<<<148, 256, 0, s>>>(flags, nb, c);
+  k_count_flags<<<device_sm_count(), 256, 0, s>>>(flags, nb, c);
   uint32_t h = 0;
   if (cudaMemcpyAsync(&h, c, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return FX_ERR_CUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return FX_ERR_CUDA;
@@ -1995,7 +1866,7 @@ fx_status fused_count_active(FusedWork& w, cudaStream_t s, const uint32_t* flags
 
 cudaError_t fused_accumulate_active(cudaStream_t s, Dims dm, uint3 bricks, const uint32_t* flags, unsigned long long* acc) {
   const uint32_t nb = bricks.x * bricks.y * bricks.z;
-  const uint32_t blocks = std::min<uint32_t>((nb + 255) / 256, 148);
+  const uint32_t blocks = std::min<uint32_t>((nb + 255) / 256, (uint32_t)device_sm_count());
   k_accumulate_active<<<blocks, 256, 0, s>>>(dm, bricks, flags, acc);
   return cudaGetLastError();
 }

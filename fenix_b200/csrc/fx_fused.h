@@ -47,7 +47,6 @@ struct FusedWork {
   uint32_t* list_next = nullptr;  // bricks the combustion/buoyancy kernels visit
   uint32_t* list_inj = nullptr;   // bricks the injection kernel visits (host-filled)
   uint32_t* counters = nullptr;   // [0] adv count, [1] next count, [2] scratch, [3] inject count
-  unsigned* mg_bar = nullptr;      // grid barrier of the lower multigrid kernel: arrivals, generation, error flag
   SolverDev* solver = nullptr;     // FP64 solver statistics and the V-cycle loop state
   unsigned* vmax = nullptr;        // max |v| of the current velocity (float bits; all ones = unknown)
   cudaStream_t aux = nullptr;      // captures the V-cycle body graph
@@ -127,10 +126,6 @@ fx_status fused_prepare(FusedWork& w, const FusedStep& st, uint32_t* ninj, Fused
 uint64_t fused_key(const FusedStep& st, uint32_t ninj);
 fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, FusedResult& out);
 fx_status fused_count_active(FusedWork& w, cudaStream_t s, const uint32_t* flags, uint32_t nb, uint32_t* out);
-
-// FX_ERR_TIMEOUT when a grid barrier of the fused path gave up waiting
-// (waits for the stream), FX_OK otherwise.
-fx_status fused_check_device_error(FusedWork& w, cudaStream_t s);
 
 // Adds the active bricks of `flags` and their voxel count to acc[0] and acc[1].
 cudaError_t fused_accumulate_active(cudaStream_t s, Dims dm, uint3 bricks, const uint32_t* flags, unsigned long long* acc);

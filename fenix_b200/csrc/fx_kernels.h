@@ -52,6 +52,16 @@ struct InflowPatch {
 };
 void plain_inflow(cudaStream_t s, Dims dm, InflowPatch p, const float* values, VelField v);
 
+// Streaming multiprocessors of the current device (queried once per device).
+int device_sm_count();
+
+// The library's device and pinned-host allocations go through these two, so a
+// test can make the n-th of them fail as an exhausted memory would
+// (fx_test_fail_allocations): the call then returns cudaErrorMemoryAllocation
+// without reaching CUDA.
+cudaError_t device_alloc(void** ptr, size_t bytes);
+cudaError_t host_alloc(void** ptr, size_t bytes);
+
 // Pinned sin/cos over an array (tests compare it with the oracle bit for bit).
 void pinned_sincos_array(cudaStream_t s, const float* x, float* out, uint32_t n, int cosine);
 

@@ -15,15 +15,27 @@
 // an allocation there fails or evicts. So the call allocates nothing. It makes no
 // cudaMalloc, cudaFree or cudaMallocAsync call and uses no library routine that
 // allocates, torch's included. The one scratch buffer it needs (a summary byte
-// per brick between the two kernels) is the static device array below. The
-// driver reserves it when the module loads.
+// per brick between the two kernels) is the static device array below, which
+// the driver places when it loads this library's module on a device.
 //
 // Limits and ordering:
 //  - at most kNoAllocMaxBricks bricks (8^3 voxels each, ragged edges count as
 //    bricks), i.e. 1 MiB of scratch; larger grids are rejected before any CUDA call;
-//  - the first call on a device looks up the scratch address with
-//    cudaGetSymbolAddress, once per device, with that device current. When the
-//    first call does this setup, it should come before any stream capture;
+//  - the first call on a device is its set-up: with that device current it looks
+//    up the scratch address with cudaGetSymbolAddress, once per device. CUDA 12
+//    loads modules lazily by default, so that first call is also when the module
+//    (its code and the 1 MiB array) is loaded onto the device, and its first
+//    launches load the two kernels. A caller that reserves the rest of the
+//    device's memory up front makes one call (on any small grid) before it
+//    reserves, or runs with CUDA_MODULE_LOADING=EAGER; later calls then take no
+//    device memory at all. The first call should also come before any stream
+//    capture;
+//  - the scratch address is cached per device ordinal for the life of the
+//    process. A cudaDeviceReset destroys the context that holds the array, so a
+//    process that resets a device must not call this entry point on it again;
+//  - launch errors are taken from the launches themselves (cudaLaunchKernel's
+//    return value), so an error left pending by unrelated earlier work is neither
+//    reported as this call's nor cleared;
 //  - nothing has to start at zero: the summary kernel writes every scratch byte
 //    that the dilation kernel reads, and the dilation kernel writes every flag;
 //  - the scratch is one per device, so two calls in flight at once on one
@@ -138,9 +150,13 @@ extern "C" fx_status fx_brick_flags_noalloc(const float* density, const float* t
   const uint3 bc = make_uint3((uint32_t)bcx, (uint32_t)bcy, (uint32_t)bcz);
   const cudaStream_t s = static_cast<cudaStream_t>(stream);
   const uint32_t n = (uint32_t)nb;
-  k_noalloc_summary<<<(n + 7u) / 8u, 256, 0, s>>>(dm, bc, density, temperature, reaction, static_cast<uint8_t*>(scratch));
-  k_noalloc_dilate<<<(n + 255u) / 256u, 256, 0, s>>>(bc, static_cast<const uint8_t*>(scratch), flags);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return noalloc_fail(FX_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+  uint8_t* summary = static_cast<uint8_t*>(scratch);
+  const uint8_t* summary_in = summary;
+  void* sum_args[] = {(void*)&dm, (void*)&bc, (void*)&density, (void*)&temperature, (void*)&reaction, (void*)&summary};
+  e = cudaLaunchKernel((const void*)k_noalloc_summary, dim3((n + 7u) / 8u), dim3(256), sum_args, 0, s);
+  if (e != cudaSuccess) return noalloc_fail(FX_ERR_CUDA, std::string("summary launch: ") + cudaGetErrorString(e));
+  void* dil_args[] = {(void*)&bc, (void*)&summary_in, (void*)&flags};
+  e = cudaLaunchKernel((const void*)k_noalloc_dilate, dim3((n + 255u) / 256u), dim3(256), dil_args, 0, s);
+  if (e != cudaSuccess) return noalloc_fail(FX_ERR_CUDA, std::string("dilation launch: ") + cudaGetErrorString(e));
   return FX_OK;
 }

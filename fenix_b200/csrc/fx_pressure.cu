@@ -1,26 +1,13 @@
-// Fine-level pressure passes of the fused path: up to four Jacobi sweeps
-// (pressure-jacobi.wgsl.ts:15-36) temporally blocked on chip, with the
-// divergence (compute-divergence.wgsl.ts:22-42), the fine->mid restriction
-// (pressure-restriction.wgsl.ts:27-50), the mid->fine prolongation
-// (pressure-prolongation.wgsl.ts:29-44) and the projection
-// (project-velocity.wgsl.ts:21-43) fused where the reference runs them next to
-// the sweeps.
-//
-// A block owns a TX x TY column of the grid and marches along z through a chunk
-// of planes. Stage 0 is the pass input and stage j the j-th sweep; stage j at
-// plane z needs stage j-1 at planes z-1..z+1, so stage j runs j planes behind
-// the input (one more when the divergence is computed in the block). Each thread
-// owns fixed (x, y) positions of a frame = the column widened by H voxels (H =
-// number of stencil stages after stage 0). For its positions it keeps every
-// stage's last three planes in registers (the z neighbours) and publishes the
-// newest plane to a double-buffered shared plane (the x and y neighbours).
-// Stage j is valid on the frame shrunk by j, which is all the next stage needs.
-// A stage at clock t reads only planes published at clock t-1, so one barrier
-// per plane suffices.
+// Fine-level pressure passes of the fused path: the Jacobi sweep
+// (pressure-jacobi.wgsl.ts:15-36) in several bit-identical thread layouts, the
+// divergence (compute-divergence.wgsl.ts:22-42) fused with the first sweep and
+// the fine->mid restriction (pressure-restriction.wgsl.ts:27-50), and the
+// mid->fine prolongation (pressure-prolongation.wgsl.ts:29-44) fused with the
+// first post-sweep.
 //
 // Every value is computed with the reference's operations in its order: the
-// result equals the sweep-by-sweep evaluation bit for bit. The division by 6 is
-// the exact IEEE quotient (div6, fx_math.cuh).
+// result equals the sweep-by-sweep evaluation of the reference bit for bit. The
+// division by 6 is the exact IEEE quotient (div6, fx_math.cuh).
 #include <algorithm>
 #include <cstdlib>
 
@@ -30,8 +17,6 @@
 namespace fx {
 namespace {
 
-constexpr int TX = 32, TY = 16, NT = TX * TY;
-
 // Integer tuning knob from the environment (defaults come from measurement).
 int env_int(const char* name, int dflt, int lo, int hi) {
   const char* v = std::getenv(name);
@@ -40,309 +25,12 @@ int env_int(const char* name, int dflt, int lo, int hi) {
   return (x >= lo && x <= hi) ? x : dflt;
 }
 
-enum { IN_ZERO = 0, IN_BUF = 1, IN_BUF_PROLONG = 2, IN_ZERO_PROLONG = 3 };
-
-struct ZArgs {
-  Dims dm;
-  Dims mid;
-  int zchunk;
-  const float* p_in;
-  const float* div_in;
-  float* div_out;
-  float* mid_div;
-  const float* mid_p;
-  float* p_out;
-  VelField vfin;
-  VelField vcur;
-  float* vmag;
-  int write_vmag;
-  int restrict_mid;
-};
-
 // Prolongation term of pressure-prolongation.wgsl.ts:42-43 at fine voxel (x,y,z).
 FX_DEV float prolong_sample(const Dims& mid, const float* __restrict__ mp, int x, int y, int z) {
   const float px = ((float)x + 0.5f) * 0.5f - 0.5f;
   const float py = ((float)y + 0.5f) * 0.5f - 0.5f;
   const float pz = ((float)z + 0.5f) * 0.5f - 0.5f;
   return tri_interp(mp, tri_corners(mid, px, py, pz));
-}
-
-template <int S, int IN, bool DIVV, bool PROJ>
-struct Frame {
-  static constexpr int H = S + (PROJ ? 1 : 0);
-  static constexpr int EX = TX + 2 * H;
-  static constexpr int EY = TY + 2 * H;
-  static constexpr int P = EX * EY;
-  static constexpr int RP = (P + NT - 1) / NT;
-  static constexpr bool stage0 = IN != IN_ZERO;
-  static constexpr int first = stage0 ? 0 : 1;  // first stage held in registers
-  // Shared planes (P floats each): 2 per published stage (stages first..S-1, and
-  // S when projecting), 2 each for vx and vy and 3 for the divergence when it is
-  // computed in the block.
-  static constexpr int pub_last = PROJ ? S : S - 1;
-  static constexpr int npub = pub_last >= first ? pub_last - first + 1 : 0;
-  static constexpr int floats = P * (2 * npub + (DIVV ? 7 : 0));
-};
-
-template <int S, int IN, bool DIVV, bool PROJ>
-__global__ void __launch_bounds__(NT, 1) k_zjacobi(ZArgs a) {
-  using Fr = Frame<S, IN, DIVV, PROJ>;
-  constexpr int H = Fr::H, EX = Fr::EX, EY = Fr::EY, P = Fr::P, RP = Fr::RP;
-  constexpr int dl = DIVV ? 1 : 0;
-  constexpr int L = S + (PROJ ? 1 : 0);
-  extern __shared__ float sm[];
-  const Dims dm = a.dm;
-  const int W = (int)dm.w, Hh = (int)dm.h, D = (int)dm.d;
-  const int tid = threadIdx.x + TX * threadIdx.y;
-  const int gx0 = (int)blockIdx.x * TX - H, gy0 = (int)blockIdx.y * TY - H;
-  const int za = (int)blockIdx.z * a.zchunk;
-  const int zb = min(za + a.zchunk, D);
-  const size_t plane = (size_t)W * (size_t)Hh;
-
-  // shared planes
-  auto pub = [&](int j, int buf) -> float* { return sm + ((j - Fr::first) * 2 + buf) * P; };
-  float* vxs = sm + 2 * Fr::npub * P;  // [2][P]
-  float* vys = vxs + 2 * P;            // [2][P]
-  float* dvs = vys + 2 * P;            // [3][P]
-
-  // per-position constants
-  int pidx[RP], dist[RP], gxr[RP], gyr[RP], gxy[RP];
-  bool valid[RP], indom[RP], xyint[RP];
-#pragma unroll
-  for (int r = 0; r < RP; ++r) {
-    const int p = tid + NT * r;
-    valid[r] = p < P;
-    const int lx = p % EX, ly = p / EX;
-    pidx[r] = p;
-    dist[r] = min(min(lx, EX - 1 - lx), min(ly, EY - 1 - ly));
-    const int gx = gx0 + lx, gy = gy0 + ly;
-    indom[r] = valid[r] && gx >= 0 && gy >= 0 && gx < W && gy < Hh;
-    xyint[r] = valid[r] && gx > 0 && gy > 0 && gx < W - 1 && gy < Hh - 1;
-    gxy[r] = indom[r] ? gx + W * gy : 0;
-    gxr[r] = gx;
-    gyr[r] = gy;
-  }
-  for (int k = tid; k < Fr::floats; k += NT) sm[k] = 0.0f;
-
-  // register rings: ring[j][r][0..2] = stage j at planes q_j-2, q_j-1, q_j
-  float ring[S + 1][RP][3];
-  float divr[RP][S + 1];  // divr[r][k] = divergence at plane (t - dl - k)
-  float vzr[RP][3];       // vz at planes t-2, t-1, t (divergence in block)
-#pragma unroll
-  for (int j = 0; j <= S; ++j)
-#pragma unroll
-    for (int r = 0; r < RP; ++r) ring[j][r][0] = ring[j][r][1] = ring[j][r][2] = 0.0f;
-#pragma unroll
-  for (int r = 0; r < RP; ++r) {
-#pragma unroll
-    for (int k = 0; k <= S; ++k) divr[r][k] = 0.0f;
-    vzr[r][0] = vzr[r][1] = vzr[r][2] = 0.0f;
-  }
-  __syncthreads();
-
-  const int t_begin = za - L;
-  const int t_end = zb - 1 + L + dl;
-
-  // Raw inputs of plane tt for this thread's positions, loaded one clock ahead.
-  float pre_v[RP], pre_a[RP], pre_b[RP], pre_c[RP];
-  auto fetch = [&](int tt) {
-    const bool t_in = tt >= 0 && tt < D;
-    const bool zint = tt > 0 && tt < D - 1;
-#pragma unroll
-    for (int r = 0; r < RP; ++r) {
-      pre_a[r] = pre_b[r] = pre_c[r] = pre_v[r] = 0.0f;
-      if (!(t_in && indom[r])) continue;
-      const size_t i = (size_t)gxy[r] + plane * (size_t)tt;
-      if (DIVV) {
-        pre_a[r] = __ldg(a.vfin.c[0] + i);
-        pre_b[r] = __ldg(a.vfin.c[1] + i);
-        pre_c[r] = __ldg(a.vfin.c[2] + i);
-      } else if (S >= 1) {
-        pre_a[r] = __ldg(a.div_in + i);
-      }
-      if (Fr::stage0) {
-        if (IN == IN_BUF) {
-          pre_v[r] = __ldg(a.p_in + i);
-        } else if (zint && xyint[r]) {
-          const float ps = prolong_sample(a.mid, a.mid_p, gxr[r], gyr[r], tt);
-          pre_v[r] = (IN == IN_BUF_PROLONG) ? __ldg(a.p_in + i) + ps : 0.0f + ps;
-        }
-      }
-    }
-  };
-  fetch(t_begin);
-
-  for (int t = t_begin; t <= t_end; ++t) {
-    const int b = t & 1;
-
-    // ---- consume the prefetched plane t
-    if (DIVV) {
-#pragma unroll
-      for (int r = 0; r < RP; ++r) {
-        if (valid[r]) {
-          vxs[b * P + pidx[r]] = pre_a[r];
-          vys[b * P + pidx[r]] = pre_b[r];
-        }
-        vzr[r][0] = vzr[r][1];
-        vzr[r][1] = vzr[r][2];
-        vzr[r][2] = pre_c[r];
-      }
-    } else {
-#pragma unroll
-      for (int r = 0; r < RP; ++r) {
-#pragma unroll
-        for (int k = S; k > 0; --k) divr[r][k] = divr[r][k - 1];
-        divr[r][0] = pre_a[r];
-      }
-    }
-    if (Fr::stage0) {
-#pragma unroll
-      for (int r = 0; r < RP; ++r) {
-        ring[0][r][0] = ring[0][r][1];
-        ring[0][r][1] = ring[0][r][2];
-        ring[0][r][2] = pre_v[r];
-        if (valid[r] && Fr::pub_last >= 0) pub(0, b)[pidx[r]] = pre_v[r];
-      }
-    }
-    // ---- issue the loads of plane t + 1; they complete while this clock computes
-    if (t < t_end) fetch(t + 1);
-
-    // ---- divergence at plane t - 1 (in block)
-    if (DIVV) {
-      const int q = t - 1;
-      const int qb = q & 1;
-      const bool qint = q > 0 && q < D - 1;
-      const int slot = ((q % 3) + 3) % 3;
-#pragma unroll
-      for (int r = 0; r < RP; ++r) {
-        float d = 0.0f;
-        if (qint && xyint[r] && dist[r] >= 1) {
-          const int c = pidx[r];
-          const float* vx = vxs + qb * P;
-          const float* vy = vys + qb * P;
-          const float ddx = vx[c + 1] - vx[c - 1];
-          const float ddy = vy[c + EX] - vy[c - EX];
-          const float ddz = vzr[r][2] - vzr[r][0];
-          d = (ddx + ddy + ddz) * 0.5f;
-        }
-#pragma unroll
-        for (int k = S; k > 0; --k) divr[r][k] = divr[r][k - 1];
-        divr[r][0] = d;
-        if (valid[r]) dvs[slot * P + pidx[r]] = d;
-        if (q >= za && q < zb && dist[r] >= H && indom[r]) a.div_out[(size_t)gxy[r] + plane * (size_t)q] = d;
-      }
-      // restriction of fine planes q-2, q-1 (published at clocks t-2, t-1)
-      const int q1 = q - 1;
-      if (a.restrict_mid && q1 >= za && q1 < zb && (q1 & 1) == 1 && tid < (TX / 2) * (TY / 2)) {
-        const int mx_ = (gx0 + H) / 2 + (tid % (TX / 2)), my_ = (gy0 + H) / 2 + (tid / (TX / 2)), mz_ = q1 / 2;
-        if (mx_ < (int)a.mid.w && my_ < (int)a.mid.h && mz_ < (int)a.mid.d) {
-          float out = 0.0f;
-          if (!(mx_ == 0 || my_ == 0 || mz_ == 0 || mx_ == (int)a.mid.w - 1 || my_ == (int)a.mid.h - 1 || mz_ == (int)a.mid.d - 1)) {
-            const float* d0 = dvs + (((q1 - 1) % 3 + 3) % 3) * P;
-            const float* d1 = dvs + ((q1 % 3 + 3) % 3) * P;
-            const int c = (2 * mx_ - gx0) + (2 * my_ - gy0) * EX;
-            float sum = 0.0f;
-            sum += d0[c];
-            sum += d0[c + 1];
-            sum += d0[c + EX];
-            sum += d0[c + EX + 1];
-            sum += d1[c];
-            sum += d1[c + 1];
-            sum += d1[c + EX];
-            sum += d1[c + EX + 1];
-            out = sum * 0.125f;
-          }
-          a.mid_div[flat(a.mid, (uint32_t)mx_, (uint32_t)my_, (uint32_t)mz_)] = out;
-        }
-      }
-    }
-
-    // ---- sweeps: stage j at plane q_j = t - dl - j
-#pragma unroll
-    for (int j = 1; j <= S; ++j) {
-      const int q = t - dl - j;
-      const bool qint = q > 0 && q < D - 1;
-      const float* xy = (j - 1 >= Fr::first) ? pub(j - 1, (q & 1)) : nullptr;
-#pragma unroll
-      for (int r = 0; r < RP; ++r) {
-        float v = 0.0f;
-        if (qint && xyint[r] && dist[r] >= j) {
-          const float dd = divr[r][j];
-          if (j == 1 && !Fr::stage0) {
-            v = div6(0.0f - dd);
-          } else {
-            const int c = pidx[r];
-            const float s = xy[c + 1] + xy[c - 1] + xy[c + EX] + xy[c - EX] + ring[j - 1][r][2] + ring[j - 1][r][0];
-            v = div6(s - dd);
-          }
-        }
-        ring[j][r][0] = ring[j][r][1];
-        ring[j][r][1] = ring[j][r][2];
-        ring[j][r][2] = v;
-        if (j <= Fr::pub_last && valid[r]) pub(j, q & 1)[pidx[r]] = v;
-      }
-    }
-
-    // ---- last stage to global, projection
-    {
-      const int q = t - dl - S;
-      if (q >= za && q < zb) {
-#pragma unroll
-        for (int r = 0; r < RP; ++r)
-          if (dist[r] >= H && indom[r]) a.p_out[(size_t)gxy[r] + plane * (size_t)q] = ring[S][r][2];
-      }
-    }
-    if (PROJ) {
-      const int q = t - dl - S - 1;
-      if (q >= za && q < zb) {
-        const bool qint = q > 0 && q < D - 1;
-        const float* xy = pub(S, q & 1);
-#pragma unroll
-        for (int r = 0; r < RP; ++r) {
-          if (dist[r] >= H && indom[r]) {
-            const size_t i = (size_t)gxy[r] + plane * (size_t)q;
-            float ox = 0.f, oy = 0.f, oz = 0.f;
-            if (qint && xyint[r]) {
-              const int c = pidx[r];
-              const float gx = (xy[c + 1] - xy[c - 1]) * 0.5f;
-              const float gy = (xy[c + EX] - xy[c - EX]) * 0.5f;
-              const float gz = (ring[S][r][2] - ring[S][r][0]) * 0.5f;
-              ox = __ldg(a.vfin.c[0] + i) - gx;
-              oy = __ldg(a.vfin.c[1] + i) - gy;
-              oz = __ldg(a.vfin.c[2] + i) - gz;
-            }
-            a.vcur.c[0][i] = ox;
-            a.vcur.c[1][i] = oy;
-            a.vcur.c[2][i] = oz;
-            if (a.write_vmag) a.vmag[i] = length3(ox, oy, oz);
-          }
-        }
-      }
-    }
-    __syncthreads();
-  }
-}
-
-template <int S, int IN, bool DIVV, bool PROJ>
-cudaError_t launch_z(cudaStream_t s, const ZArgs& a) {
-  using Fr = Frame<S, IN, DIVV, PROJ>;
-  const size_t smem = (size_t)Fr::floats * sizeof(float);
-  cudaError_t e = cudaFuncSetAttribute(k_zjacobi<S, IN, DIVV, PROJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  const dim3 grid((a.dm.w + TX - 1) / TX, (a.dm.h + TY - 1) / TY, (a.dm.d + a.zchunk - 1) / a.zchunk);
-  k_zjacobi<S, IN, DIVV, PROJ><<<grid, dim3(TX, TY), smem, s>>>(a);
-  return cudaGetLastError();
-}
-
-template <int IN, bool DIVV, bool PROJ>
-cudaError_t launch_s(cudaStream_t s, int sweeps, const ZArgs& a) {
-  switch (sweeps) {
-    case 0: return launch_z<0, IN, DIVV, PROJ>(s, a);
-    case 1: return launch_z<1, IN, DIVV, PROJ>(s, a);
-    case 2: return launch_z<2, IN, DIVV, PROJ>(s, a);
-    case 3: return launch_z<3, IN, DIVV, PROJ>(s, a);
-    default: return launch_z<4, IN, DIVV, PROJ>(s, a);
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -990,202 +678,6 @@ __global__ void __launch_bounds__(256) k_prolong_zero(Dims dm, float* __restrict
 
 inline dim3 lean_grid(Dims d) { return dim3((d.w + 31) / 32, (d.h + 3) / 4, (d.d + 1) / 2); }
 
-// ---------------------------------------------------------------------------
-// The mid and coarse levels of PressureSolvePass.solve (:73-82) in one
-// cooperative launch: mid pre-smoothing, restriction to coarse, coarse
-// smoothing, prolongation into mid pressureA and mid post-smoothing, separated
-// by grid-wide barriers. The levels are small enough to stay in L2, so the
-// launch-per-sweep cost of the reference schedule dominates without this.
-// ---------------------------------------------------------------------------
-struct MgArgs {
-  Dims mid, coarse;
-  float* mdiv;
-  float* mp[2];
-  float* cdiv;
-  float* cp[2];
-  int mid_pre, coarse_n, mid_post;
-  unsigned* bar;  // [0] arrivals, [1] generation, [2] error flag
-};
-
-// Grid barrier with a bounded wait: after 2^24 polls of at least 64 ns (about a
-// second; a correct barrier takes microseconds) the waiting block records an
-// error and every block leaves the kernel.
-FX_DEV bool grid_sync(unsigned* bar) {
-  // bar[0]: arrivals, bar[32]: generation, bar[64]: error flag (separate 128-byte lines)
-  __syncthreads();
-  __shared__ int failed;
-  if (threadIdx.x == 0) {
-    failed = 0;
-    volatile unsigned* vgen = bar + 32;
-    volatile unsigned* verr = bar + 64;
-    const unsigned gen = *vgen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(bar, 1u);
-    if (arrived == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 32, 1u);
-    } else {
-      unsigned polls = 0;
-      while (*vgen == gen) {
-        __nanosleep(64);
-        if (++polls > (1u << 24) || *verr) {
-          atomicExch(bar + 64, 1u);
-          failed = 1;
-          break;
-        }
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return failed == 0 && *((volatile unsigned*)bar + 64) == 0;
-}
-
-// Grid-stride walk over a level's voxels keeping (x, y, z) by carry instead of
-// dividing each linear index by the dimensions.
-struct Walk {
-  uint32_t i, x, y, z, step, sx, sy, sz;
-  FX_DEV Walk(const Dims& d) {
-    i = blockIdx.x * blockDim.x + threadIdx.x;
-    step = gridDim.x * blockDim.x;
-    x = i % d.w;
-    y = (i / d.w) % d.h;
-    z = i / (d.w * d.h);
-    sx = step % d.w;
-    sy = (step / d.w) % d.h;
-    sz = step / (d.w * d.h);
-  }
-  FX_DEV void next(const Dims& d) {
-    i += step;
-    x += sx;
-    uint32_t cy = 0;
-    if (x >= d.w) {
-      x -= d.w;
-      cy = 1;
-    }
-    y += sy + cy;
-    uint32_t cz = 0;
-    if (y >= d.h) {
-      y -= d.h;
-      cz = 1;
-    }
-    z += sz + cz;
-  }
-};
-
-// A warp owns chunks of 32*MG_RUN consecutive voxels, lane-interleaved (so the
-// accesses stay coalesced); each lane loads its MG_RUN voxels' operands before
-// computing, which keeps MG_RUN independent loads in flight per thread.
-constexpr int MG_RUN = 8;
-
-FX_DEV void mg_sweep(const Dims& d, const float* __restrict__ div, const float* __restrict__ src, float* __restrict__ dst) {
-  const uint32_t n = d.w * d.h * d.d;
-  const uint32_t sy = d.w, sz = d.w * d.h;
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  const uint32_t chunk = 32u * MG_RUN;
-  for (uint32_t c0 = warp * chunk; c0 < n; c0 += nwarps * chunk) {
-    uint32_t i0 = c0 + lane;
-    uint32_t x = i0 % d.w, y = (i0 / d.w) % d.h, z = i0 / sz;
-    float nb[MG_RUN][6], dv[MG_RUN];
-    bool live[MG_RUN], interior[MG_RUN];
-    uint32_t idx[MG_RUN];
-#pragma unroll
-    for (int k = 0; k < MG_RUN; ++k) {
-      const uint32_t i = i0 + 32u * k;
-      idx[k] = i;
-      live[k] = i < n;
-      interior[k] = live[k] && !is_boundary(d, x, y, z);
-      if (interior[k]) {
-        nb[k][0] = src[i + 1];
-        nb[k][1] = src[i - 1];
-        nb[k][2] = src[i + sy];
-        nb[k][3] = src[i - sy];
-        nb[k][4] = src[i + sz];
-        nb[k][5] = src[i - sz];
-        dv[k] = div[i];
-      }
-      // advance (x, y, z) by 32 voxels
-      x += 32u;
-      while (x >= d.w) {
-        x -= d.w;
-        if (++y >= d.h) {
-          y = 0;
-          ++z;
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < MG_RUN; ++k) {
-      if (!live[k]) continue;
-      float v = 0.0f;
-      if (interior[k]) {
-        const float s = nb[k][0] + nb[k][1] + nb[k][2] + nb[k][3] + nb[k][4] + nb[k][5];
-        v = div6(s - dv[k]);
-      }
-      dst[idx[k]] = v;
-    }
-  }
-}
-
-__global__ void __launch_bounds__(512) k_mg_lower(MgArgs a) {
-  int m = 0;
-  for (int k = 0; k < a.mid_pre; ++k, m ^= 1) {
-    mg_sweep(a.mid, a.mdiv, a.mp[m], a.mp[m ^ 1]);
-    if (!grid_sync(a.bar)) return;
-  }
-  const int mid_pre = m;
-  {  // restriction mid -> coarse (pressure-restriction.wgsl.ts:27-50)
-    const Dims& t = a.coarse;
-    const Dims& sdm = a.mid;
-    const uint32_t n = t.w * t.h * t.d;
-    for (Walk w(t); w.i < n; w.next(t)) {
-      const uint32_t i = w.i, x = w.x, y = w.y, z = w.z;
-      if (x == 0u || y == 0u || z == 0u || x == t.w - 1u || y == t.h - 1u || z == t.d - 1u) {
-        a.cdiv[i] = 0.0f;
-        continue;
-      }
-      float sum = 0.0f;
-      for (uint32_t dz = 0; dz < 2u; ++dz)
-        for (uint32_t dy = 0; dy < 2u; ++dy)
-          for (uint32_t dx = 0; dx < 2u; ++dx) {
-            const uint32_t sx = min(2u * x + dx, sdm.w - 1u), sy = min(2u * y + dy, sdm.h - 1u), sz = min(2u * z + dz, sdm.d - 1u);
-            sum += a.mdiv[flat(sdm, sx, sy, sz)];
-          }
-      a.cdiv[i] = sum * 0.125f;
-    }
-    if (!grid_sync(a.bar)) return;
-  }
-  int c = 0;
-  for (int k = 0; k < a.coarse_n; ++k, c ^= 1) {
-    mg_sweep(a.coarse, a.cdiv, a.cp[c], a.cp[c ^ 1]);
-    if (!grid_sync(a.bar)) return;
-  }
-  {  // prolongation coarse -> mid pressureA (pressure-prolongation.wgsl.ts:29-44)
-    const Dims& t = a.mid;
-    const uint32_t n = t.w * t.h * t.d;
-    for (Walk w(t); w.i < n; w.next(t)) {
-      const uint32_t i = w.i, x = w.x, y = w.y, z = w.z;
-      if (x == 0u || y == 0u || z == 0u || x == t.w - 1u || y == t.h - 1u || z == t.d - 1u) {
-        a.mp[0][i] = 0.0f;
-        continue;
-      }
-      const float px = ((float)x + 0.5f) * 0.5f - 0.5f;
-      const float py = ((float)y + 0.5f) * 0.5f - 0.5f;
-      const float pz = ((float)z + 0.5f) * 0.5f - 0.5f;
-      a.mp[0][i] += tri_interp(a.cp[c], tri_corners(a.coarse, px, py, pz));
-    }
-    if (!grid_sync(a.bar)) return;
-  }
-  m = mid_pre;
-  for (int k = 0; k < a.mid_post; ++k, m ^= 1) {
-    mg_sweep(a.mid, a.mdiv, a.mp[m], a.mp[m ^ 1]);
-    if (k + 1 < a.mid_post && !grid_sync(a.bar)) return;
-  }
-}
-
 __global__ void k_div6_check(uint32_t hi_base, unsigned long long* bad) {
   const uint32_t u = hi_base + blockIdx.x * blockDim.x + threadIdx.x;
   const float x = __uint_as_float(u);
@@ -1195,50 +687,6 @@ __global__ void k_div6_check(uint32_t hi_base, unsigned long long* bad) {
 }
 
 }  // namespace
-
-cudaError_t zpass_launch(cudaStream_t s, const ZPass& p) {
-  ZArgs a{};
-  a.dm = p.dm;
-  a.mid = p.mid;
-  a.zchunk = p.zchunk > 0 ? p.zchunk : 64;
-  a.p_in = p.p_in;
-  a.div_in = p.div_in;
-  a.div_out = p.div_out;
-  a.mid_div = p.mid_div;
-  a.mid_p = p.mid_p;
-  a.p_out = p.p_out;
-  a.vfin = p.vfin;
-  a.vcur = p.vcur;
-  a.vmag = p.vmag;
-  a.write_vmag = p.write_vmag;
-  a.restrict_mid = p.restrict_mid;
-  const int S = std::min(p.sweeps, 4);
-  if (p.div_from_velocity) {
-    if (p.input != ZIN_ZERO || p.project || S < 1) return cudaErrorInvalidValue;
-    return launch_s<IN_ZERO, true, false>(s, S, a);
-  }
-  switch (p.input) {
-    case ZIN_BUF:
-      return p.project ? launch_s<IN_BUF, false, true>(s, S, a) : launch_s<IN_BUF, false, false>(s, S, a);
-    case ZIN_BUF_PROLONG:
-      return p.project ? launch_s<IN_BUF_PROLONG, false, true>(s, S, a) : launch_s<IN_BUF_PROLONG, false, false>(s, S, a);
-    case ZIN_ZERO_PROLONG:
-      return p.project ? launch_s<IN_ZERO_PROLONG, false, true>(s, S, a) : launch_s<IN_ZERO_PROLONG, false, false>(s, S, a);
-    default:
-      return cudaErrorInvalidValue;
-  }
-}
-
-
-int zpass_max_sweeps() {
-  static const int k = env_int("FENIX_ZPASS_SWEEPS", 4, 1, 4);
-  return k;
-}
-
-int zpass_zchunk() {
-  static const int z = env_int("FENIX_ZPASS_ZCHUNK", 64, 8, 4096) & ~1;
-  return z;
-}
 
 // k_div_march where the grid allows it (FENIX_DIV_MARCH=0 keeps k_div_first):
 // widths divisible by 4, even heights and depths. Runs of an even number of
@@ -1424,61 +872,6 @@ cudaError_t lean_sweep(cudaStream_t s, Dims dm, const float* div, const float* s
 cudaError_t lean_prolong_zero(cudaStream_t s, Dims dm, float* dst, Dims mid, const float* mid_p) {
   k_prolong_zero<<<lean_grid(dm), dim3(32, 4, 2), 0, s>>>(dm, dst, mid, mid_p);
   return cudaGetLastError();
-}
-
-cudaError_t mg_lower_launch(cudaStream_t s, const LevelBuf& mid, const LevelBuf& coarse, int mid_pre, int coarse_n, int mid_post,
-                            unsigned* bar, int* mid_result) {
-  static int grid = 0;
-  static int grid_dev = -1;
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (grid == 0 || grid_dev != dev) {
-    int per_sm = 0, sms = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mg_lower, 512, 0);
-    if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return e;
-    grid = std::max(1, std::min(per_sm, 2) * sms);
-    grid_dev = dev;
-  }
-  MgArgs a;
-  a.mid = mid.dm;
-  a.coarse = coarse.dm;
-  a.mdiv = mid.div;
-  a.mp[0] = mid.p[0];
-  a.mp[1] = mid.p[1];
-  a.cdiv = coarse.div;
-  a.cp[0] = coarse.p[0];
-  a.cp[1] = coarse.p[1];
-  a.mid_pre = mid_pre;
-  a.coarse_n = coarse_n;
-  a.mid_post = mid_post;
-  a.bar = bar;
-  *mid_result = (mid_pre & 1) ^ (mid_post & 1);
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(512);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  e = cudaLaunchKernelEx(&cfg, k_mg_lower, a);
-  if (e != cudaSuccess) return e;
-  return cudaGetLastError();
-}
-
-int multigrid_plan() {
-  static const int p = env_int("FENIX_MG_PLAN", 0, 0, 1);
-  return p;
-}
-
-int pressure_plan() {
-  static const int p = env_int("FENIX_PRESSURE_PLAN", 0, 0, 1);
-  return p;
 }
 
 cudaError_t div6_exhaustive_check(unsigned long long* host_bad) {

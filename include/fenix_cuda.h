@@ -534,11 +534,18 @@ fx_status fx_rollout_backward(fx_rollout* rollout, float* grad_inflow, float* gr
  * cudaMalloc or cudaFree and no allocating library routine. Its scratch is a
  * 1 MiB static device array, one summary byte per brick, so grids above
  * 1,048,576 bricks are rejected with FX_ERR_INVALID_ARGUMENT before any CUDA
- * call. The first call on a device looks up that array's address
- * (cudaGetSymbolAddress), with the device current, and should come before any
- * stream capture. Nothing has to start at zero. There is one scratch array per
- * device, so two calls in flight at once on one device race; calls on one
- * stream are ordered. Errors go to fx_last_error(). */
+ * call. The first call on a device is its set-up: it looks up that array's
+ * address (cudaGetSymbolAddress) with the device current, and, as CUDA 12
+ * loads modules lazily by default, that is when the driver loads the module
+ * holding the array and the kernels onto the device. So make one call (any
+ * small grid) before an arena reserves the rest of device memory, or set
+ * CUDA_MODULE_LOADING=EAGER; later calls take no device memory. The first call
+ * should also come before any stream capture. The address is cached per device
+ * ordinal and does not survive cudaDeviceReset. Nothing has to start at zero.
+ * There is one scratch array per device, so two calls in flight at once on one
+ * device race; calls on one stream are ordered. Launch errors come from the
+ * launches themselves, so an error pending from earlier unrelated work is left
+ * alone. Errors go to fx_last_error(). */
 fx_status fx_brick_flags_noalloc(const float* density, const float* temperature, const float* reaction, uint32_t width,
                                  uint32_t height, uint32_t depth, uint32_t* flags, void* stream);
 

@@ -1,12 +1,25 @@
 """Precision study of the FP16 scalar storage (test infrastructure).
 
-The 256^3 plume (plume_256) is stepped from one start state three ways: the
-fused CUDA step with FP16 scalar storage, the fused CUDA step in f32, and the
-f64 oracle on the host cores. At the requested steps it prints, per state field,
-the relative L2 and max-abs error of both CUDA runs against f64, as one JSON
-object and as a markdown table.
+The 256^3 plume (plume_256) is stepped from one start state by several CUDA
+runs (legs) and by the f64 oracle on the host cores. At the requested steps it
+prints, per state field, the relative L2 and max-abs error of every leg against
+f64, as one JSON object and as markdown tables.
 
-    python tests/precision_study.py [--steps 1,50,200] [--size 256] [--threads N]
+Legs:
+  f16                 fused step, FP16 scalar storage (every stored scalar rounded to binary16)
+  f32                 fused step, f32 storage
+  f32_once_f16        f32 storage, the start state's scalars rounded to binary16 once
+  f32_perturbed       f32 storage, the start state's scalars multiplied once by
+                      (1 + 2^-12 u), u uniform in [-1, 1] (seeded)
+The last two separate the amplification of one storage-sized perturbation by
+the flow from the rounding that FP16 storage adds at every step.
+
+--solver vcycle runs every leg and the oracle with the FP64-norm V-cycle
+(5 levels, V(4,4), 20 coarse sweeps, warm start, stop at relative residual
+1e-5); the default is the reference's fixed schedule.
+
+    python tests/precision_study.py [--steps 1,50,200] [--size 256] [--solver reference|vcycle]
+                                    [--legs f16,f32,f32_once_f16,f32_perturbed] [--threads N]
 """
 from __future__ import annotations
 
@@ -22,6 +35,10 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 FIELDS = ("density", "temperature", "fuel", "reaction", "velocity_x", "velocity_y", "velocity_z")
+SCALARS = ("density", "temperature", "fuel", "reaction")
+VCYCLE = {"mode": "vcycle", "levels": 5, "preSweeps": 4, "postSweeps": 4, "coarseSweeps": 20, "maxCycles": 30,
+          "warmStart": True, "omega": 2.0 / 3.0, "tolerance": 1e-5}
+LEGS = ("f16", "f32", "f32_once_f16", "f32_perturbed")
 
 
 def errors(got: np.ndarray, ref: np.ndarray) -> dict:
@@ -30,13 +47,32 @@ def errors(got: np.ndarray, ref: np.ndarray) -> dict:
     return {"rel_l2": float(np.linalg.norm(g - ref)) / max(nrm, 1e-300), "max_abs": float(np.max(np.abs(g - ref)))}
 
 
+def leg_state(leg: str, state: dict, seed: int = 4242) -> dict:
+    out = dict(state)
+    if leg == "f32_once_f16":
+        for f in SCALARS:
+            out[f] = state[f].astype(np.float16).astype(np.float32)
+    elif leg == "f32_perturbed":
+        rng = np.random.default_rng(seed)
+        for f in SCALARS:
+            u = rng.uniform(-1.0, 1.0, size=state[f].shape)
+            out[f] = (state[f].astype(np.float64) * (1.0 + 2.0 ** -12 * u)).astype(np.float32)
+    return out
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", default="1,50,200")
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--threads", type=int, default=os.cpu_count() or 1)
+    ap.add_argument("--solver", choices=("reference", "vcycle"), default="reference")
+    ap.add_argument("--legs", default="f16,f32")
     args = ap.parse_args()
     marks = sorted({int(s) for s in args.steps.split(",")})
+    legs = [l for l in args.legs.split(",") if l]
+    for l in legs:
+        if l not in LEGS:
+            raise SystemExit(f"unknown leg {l!r}; expected some of {LEGS}")
 
     from fenix_b200 import createCombustionVolumeSimulation, workloads
     from oracle import oracle as orc_mod
@@ -45,37 +81,53 @@ def main() -> int:
     orc_mod.set_threads(args.threads)
     wl = workloads.plume_256(size=args.size)
     sims = {}
-    for storage in ("f16", "f32"):
-        s = createCombustionVolumeSimulation(wl.options, device=0, storage=storage)
+    for leg in legs:
+        s = createCombustionVolumeSimulation(wl.options, device=0, storage="f16" if leg == "f16" else "f32")
         s.updateSources(wl.sources)
-        workloads.load_state(s, wl.state)
-        sims[storage] = s
+        if args.solver == "vcycle":
+            s.setSolver(VCYCLE)
+        workloads.load_state(s, leg_state(leg, wl.state))
+        sims[leg] = s
     ref = OracleSimulation(wl.options, precision=64)
     ref.updateSources(wl.sources)
+    if args.solver == "vcycle":
+        ref.setSolver(VCYCLE, norms=True)
     workloads.load_state(ref, wl.state)
-    out = {"workload": f"plume_{args.size}", "steps": marks, "dt": wl.dt, "against": "f64 oracle, same start state and steps",
-           "threads": args.threads, "at": {}}
+    out = {"workload": f"plume_{args.size}", "solver": VCYCLE if args.solver == "vcycle" else "reference schedule",
+           "steps": marks, "dt": wl.dt, "against": "f64 oracle, same start state and steps", "threads": args.threads,
+           "legs": legs, "at": {}, "cycles": {}}
     t0 = time.time()
     step = 0
+    cycles = {leg: 0 for leg in legs}
+    cycles["f64"] = 0
     for mark in marks:
         while step < mark:
             t = step * wl.dt
-            for s in sims.values():
+            for leg, s in sims.items():
                 s.step(t, wl.dt)
+                if args.solver == "vcycle":
+                    cycles[leg] += s.readSolverStats()["cycles"]
             ref.step(t, wl.dt)
+            if args.solver == "vcycle":
+                cycles["f64"] += ref.readSolverStats()["cycles"]
             step += 1
         row = {}
         refs = {f: ref.readField(f) for f in FIELDS}
-        for storage, s in sims.items():
-            row[f"{storage}_fused"] = {f: errors(s.readField(f), refs[f]) for f in FIELDS}
+        for leg, s in sims.items():
+            row[leg] = {f: errors(s.readField(f), refs[f]) for f in FIELDS}
         out["at"][str(mark)] = row
+        out["cycles"][str(mark)] = dict(cycles)
         print(f"step {mark} done ({time.time() - t0:.0f} s)", file=sys.stderr, flush=True)
+    out["seconds"] = time.time() - t0
     print(json.dumps(out))
-    print("\n| step | storage | " + " | ".join(f"{f} rel-L2" for f in FIELDS) + " |")
-    print("|---:|---|" + "---:|" * len(FIELDS))
-    for mark in marks:
-        for key, errs in out["at"][str(mark)].items():
-            print(f"| {mark} | {key} | " + " | ".join(f"{errs[f]['rel_l2']:.2e}" for f in FIELDS) + " |")
+    for key, name in (("rel_l2", "rel-L2"), ("max_abs", "max-abs")):
+        print(f"\n| step | leg | " + " | ".join(f"{f} {name}" for f in FIELDS) + " |")
+        print("|---:|---|" + "---:|" * len(FIELDS))
+        for mark in marks:
+            for leg, errs in out["at"][str(mark)].items():
+                print(f"| {mark} | {leg} | " + " | ".join(f"{errs[f][key]:.2e}" for f in FIELDS) + " |")
+    if args.solver == "vcycle":
+        print("\nV-cycles summed over the steps so far: " + json.dumps(out["cycles"]))
     return 0
 
 

@@ -1,10 +1,10 @@
 """fx_brick_flags_noalloc, the brick-flags entry point that allocates nothing.
 
 It is compared with the brick flags that the simulation itself computes at the
-start of a step (compute-active-bricks.wgsl.ts:35-58). A simulation with no
-sources leaves the scalar set unchanged through injection, so the flags of the
-set written with writeField come back as "prev_brick_flags" after one step.
-Flags are integers: the comparison is exact.
+start of a step (compute-active-bricks.wgsl.ts:35-58), and with the oracle's.
+A simulation with no sources leaves the scalar set unchanged through injection,
+so the flags of the set written with writeField come back as
+"prev_brick_flags" after one step. Flags are integers: the comparison is exact.
 """
 import ctypes
 import os
@@ -52,6 +52,20 @@ def simulation_flags(shape, fields):
         sim.dispose()
 
 
+def oracle_flags(shape, fields):
+    from oracle.oracle import OracleSimulation
+
+    d, h, w = shape
+    orc = OracleSimulation({"resolution": (w, h, d)}, precision=32)
+    try:
+        for name, values in fields.items():
+            orc.writeField(name, values.ravel())
+        orc.step(0.0, DT)
+        return orc.readField("prev_brick_flags")
+    finally:
+        orc.dispose()
+
+
 def call_noalloc(lib, dens, temp, reac, shape, flags, stream):
     d, h, w = shape
     st = lib.fx_brick_flags_noalloc(dens.data_ptr(), temp.data_ptr(), reac.data_ptr(), w, h, d, flags.data_ptr(), stream)
@@ -67,6 +81,8 @@ def test_noalloc_matches_simulation_flags_on_two_calls_in_a_row():
     fa, fb = scalar_fields(shape, 11), scalar_fields(shape, 12)
     want_a, want_b = simulation_flags(shape, fa), simulation_flags(shape, fb)
     assert want_a.any() and not want_a.all() and not np.array_equal(want_a, want_b)
+    np.testing.assert_array_equal(oracle_flags(shape, fa), want_a)
+    np.testing.assert_array_equal(oracle_flags(shape, fb), want_b)
 
     dev = torch.device("cuda", 0)
     ta = [torch.from_numpy(fa[n]).to(dev) for n in ("density", "temperature", "reaction")]
@@ -84,6 +100,33 @@ def test_noalloc_matches_simulation_flags_on_two_calls_in_a_row():
     got_b = out_b.cpu().numpy().view(np.uint32)
     np.testing.assert_array_equal(got_a, want_a)
     np.testing.assert_array_equal(got_b, want_b)
+
+
+@pytest.mark.gpu
+def test_noalloc_calls_after_the_first_take_no_device_memory():
+    """The first call on a device loads the module (lazy loading); every later
+    call leaves the device's free memory and torch's allocations unchanged."""
+    import torch
+
+    lib = _lib.load()
+    shape = (40, 48, 56)
+    fields = scalar_fields(shape, 21)
+    dev = torch.device("cuda", 0)
+    t = [torch.from_numpy(fields[n]).to(dev) for n in ("density", "temperature", "reaction")]
+    nb = int(np.prod(bricks(shape[2], shape[1], shape[0])))
+    out = torch.zeros((nb,), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    call_noalloc(lib, *t, shape, out, stream)  # set-up call
+    torch.cuda.synchronize(dev)
+    free0, _ = torch.cuda.mem_get_info(dev)
+    held0 = torch.cuda.memory_allocated(dev)
+    for _ in range(8):
+        call_noalloc(lib, *t, shape, out, stream)
+    torch.cuda.synchronize(dev)
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0, f"free device memory changed by {free0 - free1} bytes"
+    assert torch.cuda.memory_allocated(dev) == held0
+    np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), oracle_flags(shape, fields))
 
 
 @pytest.mark.gpu
