@@ -438,8 +438,13 @@ __global__ void __launch_bounds__(256) k_sweep_v4(Dims dm, const float* __restri
 // same order, so the results are the same bits. The sweep with the fused
 // prolongation has its own marching kernel, k_sweep_march_prolong, which also
 // shares the prolongation's mid-level corners between voxels.
+//
+// WEIGHTED is the V-cycle's weighted sweep (an extension, fx_vcycle.cu): each
+// interior value becomes c + w (j - c), with j the Jacobi value above and c the
+// source value, in that operation order; the boundary stays 0.
+template <bool WEIGHTED>
 __global__ void __launch_bounds__(256, 4) k_sweep_march(Dims dm, const float* __restrict__ div, const float* __restrict__ src,
-                                                        float* __restrict__ dst, int run) {
+                                                        float* __restrict__ dst, int run, float w) {
   const uint32_t lane = threadIdx.x;
   const uint32_t x0 = blockIdx.x * 128 + 4 * lane, y = blockIdx.y * 8 + threadIdx.y;
   const int zb = (int)blockIdx.z * run, ze = min(zb + run, (int)dm.d);
@@ -499,6 +504,12 @@ __global__ void __launch_bounds__(256, 4) k_sweep_march(Dims dm, const float* __
           v.y = div6(0.0f - dv.y);
           v.z = div6(0.0f - dv.z);
           if (int3) v.w = div6(0.0f - dv.w);
+        }
+        if (WEIGHTED) {
+          if (int0) v.x = c0.x + w * (v.x - c0.x);
+          v.y = c0.y + w * (v.y - c0.y);
+          v.z = c0.z + w * (v.z - c0.z);
+          if (int3) v.w = c0.w + w * (v.w - c0.w);
         }
       }
       dst4[(base + sz * (uint32_t)z) >> 2] = v;
@@ -787,7 +798,7 @@ static cudaError_t march_slots(int* slots) {
     return cudaSuccess;
   }
   int per_sm = 0, sms = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_march, 256, 0);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_march<false>, 256, 0);
   if (e != cudaSuccess) return e;
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
@@ -857,11 +868,34 @@ cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float
         k_sweep_v4<2><<<grid(128, 2), block, 0, s>>>(dm, div, src, dst, mid, mid_p);
       } else {
         const dim3 g((dm.w + 127) / 128, (dm.h + 7) / 8, (dm.d + run - 1) / run);
-        k_sweep_march<<<g, block, 0, s>>>(dm, div, src, dst, run);
+        k_sweep_march<false><<<g, block, 0, s>>>(dm, div, src, dst, run, 1.0f);
       }
       break;
     }
   }
+  return cudaGetLastError();
+}
+
+cudaError_t march_wsweep(cudaStream_t s, Dims dm, const float* rhs, const float* src, float* dst, float w, bool one) {
+  if (dm.w % 4 != 0 || dm.w < 8 || !src) return cudaErrorNotSupported;
+  static int slots[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int n = (dev >= 0 && dev < 64) ? slots[dev] : 0;
+  if (n <= 0) {
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_march<true>, 256, 0);
+    if (e != cudaSuccess) return e;
+    n = std::max(1, per_sm) * device_sm_count();
+    if (dev >= 0 && dev < 64) slots[dev] = n;
+  }
+  const int run = march_plan_one_wave(dm, n);
+  const dim3 g((dm.w + 127) / 128, (dm.h + 7) / 8, (dm.d + run - 1) / run);
+  if (one)
+    k_sweep_march<false><<<g, dim3(32, 8, 1), 0, s>>>(dm, rhs, src, dst, run, 1.0f);
+  else
+    k_sweep_march<true><<<g, dim3(32, 8, 1), 0, s>>>(dm, rhs, src, dst, run, w);
   return cudaGetLastError();
 }
 

@@ -40,6 +40,11 @@ int march_plan_pairs(Dims dm, int slots);
 // whole waves of the slots best, the fewest runs among equals.
 int march_plan_waves(Dims dm, int tx, int ty, int slots);
 
+// The V-cycle's weighted sweep (dst = src + w (J(src) - src); J(src) itself
+// when `one`) as the marching four-x kernel: same bits as the V-cycle's
+// one-x kernel. cudaErrorNotSupported where the width is not a multiple of 4.
+cudaError_t march_wsweep(cudaStream_t s, Dims dm, const float* rhs, const float* src, float* dst, float w, bool one);
+
 bool sweep_variant_valid(int variant, Dims dm);
 int sweep_variant_default(Dims dm);
 cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float* div, const float* src, float* dst, Dims mid,

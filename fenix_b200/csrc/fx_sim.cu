@@ -356,6 +356,21 @@ int plain_smooth(fx_sim* s, LevelBuf& L, int iters, int start, uint32_t& launche
 // Additions to a plain step used by the differentiable rollout: the inflow
 // patch (applied after inject-velocity), and copies of the intermediate fields
 // its adjoint reads (a null pointer skips a copy).
+VCycleConfig vcycle_config(const fx_sim* s, bool plain) {
+  VCycleConfig c{};
+  c.levels = s->solver.levels;
+  c.pre = s->solver.pre_sweeps;
+  c.post = s->solver.post_sweeps;
+  c.coarse = s->solver.coarse_sweeps;
+  c.max_cycles = s->solver.max_cycles;
+  c.omega = (float)s->solver.omega;
+  c.omega_one = s->solver.omega == 1.0;
+  c.tol = s->solver.tolerance;
+  c.warm = s->solver.warm_start != 0;
+  c.plain = plain;
+  return c;
+}
+
 struct PlainHooks {
   const float* inflow = nullptr;
   InflowPatch patch{};
@@ -409,7 +424,32 @@ fx_status step_plain(fx_sim* s, bool vort_on, bool pressure_on, bool debug_on, c
     FX_TIMED(s, "plain_confinement", plain_confinement(st, s->dm, s->d_params, s->vort, s->vort_mag, s->sets[next], s->vscr, s->conf_mag));
     launches += 2;
   }
-  if (pressure_on) {
+  const bool vcycle = pressure_on && s->solver.mode == FX_SOLVER_VCYCLE;
+  if (vcycle) {
+    // The V-cycle extension with its one-voxel kernels, from the previous
+    // step's pressure; the host reads the continue flag after every cycle.
+    FX_TIMED(s, "plain_divergence", plain_divergence(st, s->dm, s->vscr, s->lv[0].div));
+    ++launches;
+    VCycleLevels L;
+    for (int k = 0; k < 3; ++k) {
+      L.lv[k] = s->lv[k];
+      L.lv[3 + k] = s->xlv[k];
+    }
+    const VCycleConfig c = vcycle_config(s, true);
+    const int start = s->last_p;
+    FX_CUDA(s, vcycle_prologue(st, L, c, start, s->fw.solver, 0));
+    launches += 3;
+    for (int k = 0; k < c.max_cycles; ++k) {
+      FX_CUDA(s, cudaMemcpyAsync(s->fw.host_cont, &s->fw.solver->cont, sizeof(int), cudaMemcpyDeviceToHost, st));
+      FX_CUDA(s, cudaStreamSynchronize(st));
+      if (!*s->fw.host_cont) break;
+      uint32_t body = 0;
+      s->timer.begin(st, "plain_vcycle");
+      FX_CUDA(s, vcycle_body(st, L, c, start, s->fw.solver, 0, &body));
+      s->timer.end(st);
+      launches += body;
+    }
+  } else if (pressure_on) {
     for (auto& L : s->lv) FX_CUDA(s, cudaMemsetAsync(L.p[0], 0, count_of(L.dm) * sizeof(float), st));
     FX_TIMED(s, "plain_divergence", plain_divergence(st, s->dm, s->vscr, s->lv[0].div));
     ++launches;
@@ -427,6 +467,10 @@ fx_status step_plain(fx_sim* s, bool vort_on, bool pressure_on, bool debug_on, c
   }
   FX_TIMED(s, "plain_project", plain_project(st, s->dm, s->vscr, s->lv[0].p[s->last_p], s->vcur));
   ++launches;
+  if (vcycle) {
+    FX_CUDA(s, max_divergence(st, s->dm, s->vcur, s->fw.solver));
+    ++launches;
+  }
   if (debug_on) {
     FX_TIMED(s, "plain_velocity_magnitude", plain_velocity_magnitude(st, s->dm, s->vcur, s->vel_mag));
     ++launches;
@@ -529,15 +573,7 @@ fx_status step_begin(fx_sim* s, double elapsed, double step_s, StepPlan& sp) {
   for (int k = 0; k < 7; ++k) fs.q[k] = s->qi[k];
   for (int l = 0; l < 3; ++l) fs.sweep_variant[l] = s->sweep_variant[l];
   fs.solver_mode = s->solver.mode;
-  fs.vc.levels = s->solver.levels;
-  fs.vc.pre = s->solver.pre_sweeps;
-  fs.vc.post = s->solver.post_sweeps;
-  fs.vc.coarse = s->solver.coarse_sweeps;
-  fs.vc.max_cycles = s->solver.max_cycles;
-  fs.vc.omega = (float)s->solver.omega;
-  fs.vc.omega_one = s->solver.omega == 1.0;
-  fs.vc.tol = s->solver.tolerance;
-  fs.vc.warm = s->solver.warm_start != 0;
+  fs.vc = vcycle_config(s, false);
   fs.solver_norms = (s->instr & FX_INSTR_SOLVER_NORMS) != 0;
   fs.vort_on = sp.vort_on;
   fs.pressure_on = sp.pressure_on;
@@ -1126,8 +1162,6 @@ fx_status fx_sim_set_solver(fx_sim* s, const fx_solver_settings* v) {
     return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_solver: a count is out of range");
   if (!(v->omega > 0.0 && v->omega <= 1.0) || !(v->tolerance >= 0.0) || !std::isfinite(v->tolerance))
     return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_solver: omega must be in (0, 1] and tolerance finite and >= 0");
-  if (v->mode == FX_SOLVER_VCYCLE && s->kernels != FX_KERNELS_FUSED)
-    return fail(s, FX_ERR_UNSUPPORTED, "fx_sim_set_solver: the V-cycle needs the fused kernels");
   s->solver = *v;
   s->solver.reserved = 0;
   return FX_OK;
@@ -1217,7 +1251,6 @@ fx_status fx_sim_autotune(fx_sim* s, fx_autotune_report* o) {
 fx_status fx_sim_read_solver_stats(fx_sim* s, fx_solver_stats* o) {
   if (!s || !o) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_read_solver_stats: NULL argument");
   std::memset(o, 0, sizeof *o);
-  if (s->kernels != FX_KERNELS_FUSED) return FX_OK;
   FX_CUDA(s, cudaSetDevice(s->device));
   SolverDev d{};
   FX_CUDA(s, cudaMemcpyAsync(&d, s->fw.solver, sizeof d, cudaMemcpyDeviceToHost, s->stream));

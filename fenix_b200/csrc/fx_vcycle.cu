@@ -14,9 +14,18 @@
 // The loop runs as a WHILE conditional node of the step's CUDA graph: the
 // finalize kernel sets the condition from the FP64 residual, and it is 0 once
 // max_cycles cycles have run, so the loop always ends.
+//
+// On levels whose width is a multiple of 4 the sweeps, the residual restriction
+// and the prolongation run as marching kernels (four x per thread, a run of z
+// planes per thread, the next plane's loads in flight), with the same
+// operations in the same order as the one-voxel kernels, so the iterates are the
+// same bits. The FP64 norms are reduced deterministically: every block writes one
+// partial sum and the finalize kernel adds the partials in a fixed order, so the
+// cycle count and the statistics repeat from run to run.
 #include <algorithm>
 #include <cmath>
 
+#include "fx_pressure.h"
 #include "fx_vcycle.h"
 
 namespace fx {
@@ -130,37 +139,305 @@ __global__ void __launch_bounds__(256) k_prolong_add(Dims c, const float* __rest
   dst[i] = v + tri_interp(ec, tri_corners(c, px, py, pz));
 }
 
+// Block sum of one double per thread (fixed tree order) written to part[block].
+FX_DEV void block_sum_to(double v, double* part) {
+  __shared__ double wsum[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int nthreads = blockDim.x * blockDim.y;
+  const int t = threadIdx.x + blockDim.x * threadIdx.y;
+  const int warp = t >> 5, lane = t & 31;
+  if (lane == 0) wsum[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = nthreads >> 5;
+    v = lane < nw ? wsum[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = v;
+  }
+}
+
+// Sum of part[0..n) by one block of 256 threads in a fixed order.
+FX_DEV double sum_parts(const double* part, int n) {
+  __shared__ double wsum[8];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) v += part[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < 8; ++w) t += wsum[w];
+  __syncthreads();
+  return t;
+}
+
+// k_resid_restrict for a fine level that is exactly twice its coarse level
+// (widths divisible by 4), marching runs of an even number of planes with four
+// fine x per thread: the residual of each fine voxel is resid_at's (same
+// operations, same order), and the 2x2x2 sums follow k_resid_restrict's
+// dz, dy, dx order. The even row's warp adds plane 2m (its row, then the odd
+// row's from shared memory) and carries the partial sum to plane 2m + 1. The
+// children of every interior coarse cell are interior fine voxels, so no
+// neighbour is clamped.
+__global__ void __launch_bounds__(256, 4) k_resid_restrict_march(Dims f, const float* __restrict__ rhs, const float* __restrict__ e, Dims c,
+                                                                 float* __restrict__ rhs_c, int run) {
+  __shared__ float4 srow[2][8][32];  // this plane's residual rows of the block, double-buffered by plane parity
+  const uint32_t lane = threadIdx.x, ty = threadIdx.y;
+  const uint32_t x0 = blockIdx.x * 128 + 4 * lane, y = blockIdx.y * 8 + ty;
+  const int zb = (int)blockIdx.z * run, ze = min(zb + run, (int)f.d);
+  if (zb >= ze) return;  // whole block
+  const int D = (int)f.d;
+  const uint32_t sy = f.w, sz = f.w * f.h;
+  const bool yin = y < f.h;
+  const bool xin = x0 < f.w;  // f.w % 4 == 0: x0 + 3 < f.w too
+  const uint32_t base = (xin ? x0 : f.w - 4) + f.w * (yin ? y : f.h - 1);
+  const bool yint = yin && y > 0 && y < f.h - 1;
+  const bool int0 = x0 > 0, int3 = x0 + 3 < f.w - 1;
+  const bool left_end = lane == 0 && x0 > 0, right_end = lane == 31 && x0 + 4 < f.w;
+  const float4* __restrict__ e4 = reinterpret_cast<const float4*>(e);
+  const float4* __restrict__ rhs4 = reinterpret_cast<const float4*>(rhs);
+  const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  auto erow = [&](int z) { return (yint && z >= 0 && z < D) ? __ldg(e4 + ((base + sz * (uint32_t)z) >> 2)) : zero4; };
+  float4 cm = erow(zb - 1), c0 = erow(zb), cp = erow(zb + 1);
+  float4 dv = zero4, yp = zero4, ym = zero4;
+  float xle = 0.0f, xre = 0.0f;
+  if (yint) {
+    const uint32_t i = base + sz * (uint32_t)zb;
+    dv = __ldg(rhs4 + (i >> 2));
+    yp = __ldg(e4 + ((i + sy) >> 2));
+    ym = __ldg(e4 + ((i - sy) >> 2));
+    if (left_end) xle = __ldg(e + i - 1);
+    if (right_end) xre = __ldg(e + i + 4);
+  }
+  float part0 = 0.0f, part1 = 0.0f;  // sums of coarse x = x0/2 and x0/2 + 1 (even rows)
+  for (int z = zb; z < ze; ++z) {
+    const int zn = min(z + 1, D - 1);
+    const uint32_t in = base + sz * (uint32_t)zn;
+    const float4 n_c = erow(z + 2);
+    float4 n_dv = zero4, n_yp = zero4, n_ym = zero4;
+    float n_xle = 0.0f, n_xre = 0.0f;
+    if (yint) {
+      n_dv = __ldg(rhs4 + (in >> 2));
+      n_yp = __ldg(e4 + ((in + sy) >> 2));
+      n_ym = __ldg(e4 + ((in - sy) >> 2));
+      if (left_end) n_xle = __ldg(e + in - 1);
+      if (right_end) n_xre = __ldg(e + in + 4);
+    }
+    float left = __shfl_up_sync(0xffffffffu, c0.w, 1);     // x0 - 1
+    float right = __shfl_down_sync(0xffffffffu, c0.x, 1);  // x0 + 4
+    if (left_end) left = xle;
+    if (right_end) right = xre;
+    float4 r = zero4;
+    if (yint && z > 0 && z < D - 1) {
+      if (int0) r.x = dv.x - ((c0.y + left + yp.x + ym.x + cp.x + cm.x) - c0.x * 6.0f);
+      r.y = dv.y - ((c0.z + c0.x + yp.y + ym.y + cp.y + cm.y) - c0.y * 6.0f);
+      r.z = dv.z - ((c0.w + c0.y + yp.z + ym.z + cp.z + cm.z) - c0.z * 6.0f);
+      if (int3) r.w = dv.w - ((right + c0.z + yp.w + ym.w + cp.w + cm.w) - c0.w * 6.0f);
+    }
+    const int b = z & 1;
+    srow[b][ty][lane] = r;
+    __syncthreads();
+    if ((ty & 1) == 0) {
+      const float4 o = srow[b][ty + 1][lane];  // row y + 1
+      if (b == 0) {
+        part0 = 0.0f;
+        part1 = 0.0f;
+      }
+      part0 += r.x;
+      part0 += r.y;
+      part0 += o.x;
+      part0 += o.y;
+      part1 += r.z;
+      part1 += r.w;
+      part1 += o.z;
+      part1 += o.w;
+      if (b == 1 && xin && yin) {
+        const uint32_t cy = y >> 1, cz = (uint32_t)z >> 1;
+        for (int h = 0; h < 2; ++h) {
+          const uint32_t cx = (x0 >> 1) + (uint32_t)h;
+          const bool cb = cx == 0u || cy == 0u || cz == 0u || cx == c.w - 1u || cy == c.h - 1u || cz == c.d - 1u;
+          rhs_c[flat(c, cx, cy, cz)] = cb ? 0.0f : ((h ? part1 : part0) * 0.125f) * 4.0f;
+        }
+      }
+    }
+    cm = c0;
+    c0 = cp;
+    cp = n_c;
+    dv = n_dv;
+    yp = n_yp;
+    ym = n_ym;
+    xle = n_xle;
+    xre = n_xre;
+  }
+}
+
+// k_prolong_add for a fine level that is exactly twice its coarse level
+// (widths divisible by 4), marching runs of planes with four fine x per thread.
+// At an interior fine voxel the sample position needs no clamp, its corners are
+// coarse cells (c - 1) >> 1 and one more per axis, and its weights are exactly
+// 0.75 (even c) or 0.25 (odd c); consecutive fine planes share coarse planes, so
+// the thread keeps the two coarse planes of the current fine plane (a float2
+// per row, the outer columns by warp shuffle). The mixes are tri_interp's in
+// its order, so the values are the same bits. src and dst may be one buffer.
+__global__ void __launch_bounds__(256, 4) k_prolong_add_march(Dims c, const float* __restrict__ ec, Dims f, const float* src, float* dst,
+                                                              int run) {
+  const uint32_t lane = threadIdx.x;
+  const uint32_t x0 = blockIdx.x * 128 + 4 * lane, y = blockIdx.y * 8 + threadIdx.y;
+  const int zb = (int)blockIdx.z * run, ze = min(zb + run, (int)f.d);
+  if (y >= f.h || zb >= ze) return;  // whole warp
+  const uint32_t sz = f.w * f.h;
+  const bool xin = x0 < f.w;
+  const uint32_t xb = xin ? x0 : f.w - 4;
+  const uint32_t base = xb + f.w * y;
+  const float4* src4 = reinterpret_cast<const float4*>(src);
+  float4* dst4 = reinterpret_cast<float4*>(dst);
+  const bool yint = y > 0 && y < f.h - 1;
+  if (!yint) {  // boundary row: dst = src
+    if (xin)
+      for (int z = zb; z < ze; ++z) {
+        const uint32_t q = (base + sz * (uint32_t)z) >> 2;
+        dst4[q] = src4[q];
+      }
+    return;
+  }
+  const bool int0 = x0 > 0, int3 = x0 + 3 < f.w - 1;
+  const bool left_end = lane == 0 && x0 > 0, right_end = lane == 31 && x0 + 4 < f.w;
+  const int D = (int)f.d;
+  const uint32_t mc = xb >> 1;
+  const uint32_t mby = (y - 1u) >> 1, muy = mby + 1u;
+  const float fy = (y & 1u) ? 0.25f : 0.75f;
+  const float2* __restrict__ c2 = reinterpret_cast<const float2*>(ec);
+  struct Plane {
+    float v[2][4];
+  };
+  auto load_plane = [&](int pz) {
+    const uint32_t pc = (uint32_t)max(0, min(pz, (int)c.d - 1));
+    const uint32_t i0 = mc + c.w * (mby + c.h * pc), i1 = mc + c.w * (muy + c.h * pc);
+    const float2 r0 = __ldg(c2 + (i0 >> 1)), r1 = __ldg(c2 + (i1 >> 1));
+    float a = __shfl_up_sync(0xffffffffu, r0.y, 1), b = __shfl_down_sync(0xffffffffu, r0.x, 1);
+    float d0 = __shfl_up_sync(0xffffffffu, r1.y, 1), d1 = __shfl_down_sync(0xffffffffu, r1.x, 1);
+    if (left_end) {
+      a = __ldg(ec + i0 - 1);
+      d0 = __ldg(ec + i1 - 1);
+    }
+    if (right_end) {
+      b = __ldg(ec + i0 + 2);
+      d1 = __ldg(ec + i1 + 2);
+    }
+    Plane p;
+    p.v[0][0] = a;
+    p.v[0][1] = r0.x;
+    p.v[0][2] = r0.y;
+    p.v[0][3] = b;
+    p.v[1][0] = d0;
+    p.v[1][1] = r1.x;
+    p.v[1][2] = r1.y;
+    p.v[1][3] = d1;
+    return p;
+  };
+  auto sample = [&](const Plane& A, const Plane& B, int k, float fx, float fz) {
+    const float x00 = mixv(A.v[0][k], A.v[0][k + 1], fx);
+    const float x10 = mixv(A.v[1][k], A.v[1][k + 1], fx);
+    const float x01 = mixv(B.v[0][k], B.v[0][k + 1], fx);
+    const float x11 = mixv(B.v[1][k], B.v[1][k + 1], fx);
+    return mixv(mixv(x00, x10, fy), mixv(x01, x11, fy), fz);
+  };
+  int cbz = (zb - 1) >> 1;
+  Plane A = load_plane(cbz), B = load_plane(cbz + 1);
+  for (int z = zb; z < ze; ++z) {
+    const int bz = (z - 1) >> 1;
+    if (bz != cbz) {  // warp-uniform
+      A = B;
+      cbz = bz;
+      B = load_plane(cbz + 1);
+    }
+    if (!xin) continue;
+    const uint32_t q = (base + sz * (uint32_t)z) >> 2;
+    float4 v = src4[q];
+    if (z > 0 && z < D - 1) {
+      const float fz = (z & 1) ? 0.25f : 0.75f;
+      if (int0) v.x = v.x + sample(A, B, 0, 0.75f, fz);
+      v.y = v.y + sample(A, B, 1, 0.25f, fz);
+      v.z = v.z + sample(A, B, 1, 0.75f, fz);
+      if (int3) v.w = v.w + sample(A, B, 2, 0.25f, fz);
+    }
+    dst4[q] = v;
+  }
+}
+
+// k_resid_norm with four x per thread marching runs of planes (widths divisible
+// by 4): each residual term is computed as there, in double from the stored f32
+// values; one partial sum per block.
+__global__ void __launch_bounds__(256, 4) k_resid_norm_march(Dims f, const float* __restrict__ rhs, const float* __restrict__ p,
+                                                             double* part, int run) {
+  const uint32_t lane = threadIdx.x;
+  const uint32_t x0 = blockIdx.x * 128 + 4 * lane, y = blockIdx.y * 8 + threadIdx.y;
+  const int zb = (int)blockIdx.z * run, ze = min(zb + run, (int)f.d);
+  const int D = (int)f.d;
+  const uint32_t sy = f.w, sz = f.w * f.h;
+  const bool yin = y < f.h;
+  const bool xin = x0 < f.w;
+  const uint32_t base = (xin ? x0 : f.w - 4) + f.w * (yin ? y : f.h - 1);
+  const bool act = yin && xin && y > 0 && y < f.h - 1;
+  const bool int0 = x0 > 0, int3 = x0 + 3 < f.w - 1;
+  const bool left_end = lane == 0 && x0 > 0, right_end = lane == 31 && x0 + 4 < f.w;
+  const float4* __restrict__ p4 = reinterpret_cast<const float4*>(p);
+  const float4* __restrict__ rhs4 = reinterpret_cast<const float4*>(rhs);
+  const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  auto prow = [&](int z) { return (act && z >= 0 && z < D) ? __ldg(p4 + ((base + sz * (uint32_t)z) >> 2)) : zero4; };
+  double s2 = 0.0;
+  if (zb < ze) {
+    float4 cm = prow(zb - 1), c0 = prow(zb), cp = prow(zb + 1);
+    for (int z = zb; z < ze; ++z) {
+      const uint32_t i = base + sz * (uint32_t)z;
+      float4 dv = zero4, yp = zero4, ym = zero4;
+      float xle = 0.0f, xre = 0.0f;
+      if (act) {
+        dv = __ldg(rhs4 + (i >> 2));
+        yp = __ldg(p4 + ((i + sy) >> 2));
+        ym = __ldg(p4 + ((i - sy) >> 2));
+        if (left_end) xle = __ldg(p + i - 1);
+        if (right_end) xre = __ldg(p + i + 4);
+      }
+      const float4 n_c = prow(z + 2);
+      float left = __shfl_up_sync(0xffffffffu, c0.w, 1);
+      float right = __shfl_down_sync(0xffffffffu, c0.x, 1);
+      if (left_end) left = xle;
+      if (right_end) right = xre;
+      if (act && z > 0 && z < D - 1) {
+        auto term = [&](float xp, float xm, float ypv, float ymv, float zp, float zm, float c, float rh) {
+          const double s = (double)xp + (double)xm + (double)ypv + (double)ymv + (double)zp + (double)zm;
+          const double r = (double)rh - (s - 6.0 * (double)c);
+          return r * r;
+        };
+        if (int0) s2 += term(c0.y, left, yp.x, ym.x, cp.x, cm.x, c0.x, dv.x);
+        s2 += term(c0.z, c0.x, yp.y, ym.y, cp.y, cm.y, c0.y, dv.y);
+        s2 += term(c0.w, c0.y, yp.z, ym.z, cp.z, cm.z, c0.z, dv.z);
+        if (int3) s2 += term(right, c0.z, yp.w, ym.w, cp.w, cm.w, c0.w, dv.w);
+      }
+      cm = c0;
+      c0 = cp;
+      cp = n_c;
+    }
+  }
+  block_sum_to(s2, part);
+}
+
 __global__ void __launch_bounds__(256) k_fill0(float* __restrict__ p, uint32_t n) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0.0f;
 }
 
-// Block sum of one double per thread into *acc (one atomic per block).
-FX_DEV void block_sum_to(double v, double* acc) {
-  __shared__ double part[32];
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) part[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    const int nw = blockDim.x >> 5;
-    v = lane < nw ? part[lane] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) atomicAdd(acc, v);
-  }
-}
-
-__global__ void __launch_bounds__(256) k_sumsq(const float* __restrict__ a, uint32_t n, double* acc) {
+__global__ void __launch_bounds__(256) k_sumsq(const float* __restrict__ a, uint32_t n, double* part) {
   double s = 0.0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double v = (double)__ldg(a + i);
     s += v * v;
   }
-  block_sum_to(s, acc);
+  block_sum_to(s, part);
 }
 
 // Sum over interior voxels of (rhs - (sum of the 6 neighbours - 6 p))^2, each
 // term in double from the stored f32 values.
-__global__ void __launch_bounds__(256) k_resid_norm(Dims f, const float* __restrict__ rhs, const float* __restrict__ p, double* acc) {
+__global__ void __launch_bounds__(256) k_resid_norm(Dims f, const float* __restrict__ rhs, const float* __restrict__ p, double* part) {
   const uint32_t iw = f.w - 2u, ih = f.h - 2u, id = f.d - 2u;
   const uint32_t n = iw * ih * id;
   const uint32_t sy = f.w, sz = f.w * f.h;
@@ -173,16 +450,20 @@ __global__ void __launch_bounds__(256) k_resid_norm(Dims f, const float* __restr
     const double r = (double)__ldg(rhs + i) - (s - 6.0 * (double)__ldg(p + i));
     s2 += r * r;
   }
-  block_sum_to(s2, acc);
+  block_sum_to(s2, part);
 }
 
-// Takes the accumulated residual, counts the cycle, decides whether another
-// cycle is due and hands the decision to the graph's WHILE node.
-__global__ void k_finalize(SolverDev* st, double tol, int max_cycles, int count, cudaGraphConditionalHandle cond) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// Adds the residual partials (and, with nrhs > 0, the right-hand side's),
+// counts the cycle, decides whether another cycle is due and hands the decision
+// to the graph's WHILE node. One block of 256 threads.
+__global__ void __launch_bounds__(256) k_finalize(SolverDev* st, double tol, int max_cycles, int count, int nres, int nrhs,
+                                                  cudaGraphConditionalHandle cond) {
+  const double res2 = sum_parts(st->part_res, nres);
+  const double rhs2 = nrhs > 0 ? sum_parts(st->part_rhs, nrhs) : 0.0;
+  if (threadIdx.x != 0) return;
+  if (nrhs > 0) st->rhs2 = rhs2;
   if (count) st->cycles += 1;
-  st->res2 = st->res2_acc;
-  st->res2_acc = 0.0;
+  st->res2 = res2;
   const bool done = sqrt(st->res2) <= tol * sqrt(st->rhs2);
   st->converged = done ? 1 : 0;
   const int cont = (!done && st->cycles < max_cycles) ? 1 : 0;
@@ -208,13 +489,32 @@ __global__ void __launch_bounds__(256) k_maxdiv(Dims dm, VelField v, unsigned lo
   if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(bits, (unsigned long long)__double_as_longlong(m));
 }
 
-inline uint32_t reduce_blocks() { return (uint32_t)device_sm_count() * 4u; }
+inline uint32_t reduce_blocks() { return std::min<uint32_t>((uint32_t)device_sm_count() * 4u, (uint32_t)kNormParts); }
 
 inline dim3 vz_grid(Dims d) { return dim3((d.w + 31) / 32, (d.h + 7) / 8, (d.d + kVZ - 1) / kVZ); }
 inline dim3 pt_grid(Dims d) { return dim3((d.w + 31) / 32, (d.h + 3) / 4, (d.d + 1) / 2); }
 const dim3 kPtBlock(32, 4, 2);
+const dim3 kMarchBlock(32, 8, 1);
 
 inline uint32_t count_of(Dims d) { return d.w * d.h * d.d; }
+
+// Resident 256-thread blocks of `kernel` on the current device, cached per device.
+int resident_slots(const void* kernel, int* cache) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return device_sm_count();
+  if (cache[dev] <= 0) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0) != cudaSuccess) per_sm = 1;
+    cache[dev] = std::max(1, per_sm) * device_sm_count();
+  }
+  return cache[dev];
+}
+
+// Four-x marching kernels need widths divisible by 4 (and at least 8).
+inline bool marchable(Dims d) { return d.w % 4 == 0 && d.w >= 8; }
+// The fine level is exactly twice the coarse one on every axis.
+inline bool halves(Dims f, Dims c) { return marchable(f) && f.w == 2 * c.w && f.h == 2 * c.h && f.d == 2 * c.d; }
+inline dim3 march_grid(Dims d, int run) { return dim3((d.w + 127) / 128, (d.h + 7) / 8, (d.d + run - 1) / run); }
 
 void fill0(cudaStream_t s, float* p, Dims d) {
   const uint32_t n = count_of(d);
@@ -224,11 +524,50 @@ void fill0(cudaStream_t s, float* p, Dims d) {
 int smooth(cudaStream_t s, const LevelBuf& B, int sweeps, int start, const VCycleConfig& c, uint32_t* launches) {
   int a = start;
   for (int k = 0; k < sweeps; ++k) {
-    k_wjacobi<<<vz_grid(B.dm), dim3(32, 8, 1), 0, s>>>(B.dm, B.div, B.p[a], B.p[a ^ 1], c.omega, c.omega_one ? 1 : 0);
+    if (c.plain || march_wsweep(s, B.dm, B.div, B.p[a], B.p[a ^ 1], c.omega, c.omega_one) != cudaSuccess) {
+      (void)cudaGetLastError();  // cudaErrorNotSupported is a host-side refusal, nothing was launched
+      k_wjacobi<<<vz_grid(B.dm), dim3(32, 8, 1), 0, s>>>(B.dm, B.div, B.p[a], B.p[a ^ 1], c.omega, c.omega_one ? 1 : 0);
+    }
     a ^= 1;
     ++*launches;
   }
   return a;
+}
+
+void resid_restrict(cudaStream_t s, const LevelBuf& B, const float* e, const LevelBuf& C, bool plain) {
+  if (!plain && halves(B.dm, C.dm)) {
+    static int cache[64];
+    const int run = march_plan_pairs(B.dm, resident_slots((const void*)k_resid_restrict_march, cache));
+    k_resid_restrict_march<<<march_grid(B.dm, run), kMarchBlock, 0, s>>>(B.dm, B.div, e, C.dm, C.div, run);
+  } else {
+    k_resid_restrict<<<pt_grid(C.dm), kPtBlock, 0, s>>>(B.dm, B.div, e, C.dm, C.div);
+  }
+}
+
+void prolong_add(cudaStream_t s, const LevelBuf& C, const float* ec, const LevelBuf& B, const float* src, float* dst, bool plain) {
+  if (!plain && halves(B.dm, C.dm)) {
+    static int cache[64];
+    const int run = march_plan_one_wave(B.dm, resident_slots((const void*)k_prolong_add_march, cache));
+    k_prolong_add_march<<<march_grid(B.dm, run), kMarchBlock, 0, s>>>(C.dm, ec, B.dm, src, dst, run);
+  } else {
+    k_prolong_add<<<pt_grid(B.dm), kPtBlock, 0, s>>>(C.dm, ec, B.dm, src, dst);
+  }
+}
+
+// The FP64 residual norm's partials into part; returns how many.
+int resid_norm(cudaStream_t s, Dims dm, const float* rhs, const float* p, double* part, bool plain) {
+  if (!plain && marchable(dm)) {
+    static int cache[64];
+    const int run = march_plan_one_wave(dm, resident_slots((const void*)k_resid_norm_march, cache));
+    const dim3 g = march_grid(dm, run);
+    const uint32_t blocks = g.x * g.y * g.z;
+    if (blocks <= (uint32_t)kNormParts) {
+      k_resid_norm_march<<<g, kMarchBlock, 0, s>>>(dm, rhs, p, part, run);
+      return (int)blocks;
+    }
+  }
+  k_resid_norm<<<reduce_blocks(), 256, 0, s>>>(dm, rhs, p, part);
+  return (int)reduce_blocks();
 }
 
 int level_cycle(cudaStream_t s, const VCycleLevels& L, const VCycleConfig& c, int k, int start, uint32_t* launches) {
@@ -236,12 +575,12 @@ int level_cycle(cudaStream_t s, const VCycleLevels& L, const VCycleConfig& c, in
   if (k == c.levels - 1) return smooth(s, B, c.coarse, start, c, launches);
   const int a = smooth(s, B, c.pre, start, c, launches);
   const LevelBuf& C = L.lv[k + 1];
-  k_resid_restrict<<<pt_grid(C.dm), kPtBlock, 0, s>>>(B.dm, B.div, B.p[a], C.dm, C.div);
+  resid_restrict(s, B, B.p[a], C, c.plain);
   fill0(s, C.p[0], C.dm);
   *launches += 2;
   const int ce = level_cycle(s, L, c, k + 1, 0, launches);
   const int b = ((c.pre + c.post) & 1) ? a ^ 1 : a;
-  k_prolong_add<<<pt_grid(B.dm), kPtBlock, 0, s>>>(C.dm, C.p[ce], B.dm, B.p[a], B.p[b]);
+  prolong_add(s, C, C.p[ce], B, B.p[a], B.p[b], c.plain);
   ++*launches;
   return smooth(s, B, c.post, b, c, launches);
 }
@@ -254,9 +593,9 @@ cudaError_t vcycle_prologue(cudaStream_t s, const VCycleLevels& L, const VCycleC
   cudaError_t e = cudaMemsetAsync(st, 0, sizeof(SolverDev), s);
   if (e != cudaSuccess) return e;
   if (!c.warm) fill0(s, F.p[start], F.dm);
-  k_sumsq<<<reduce_blocks(), 256, 0, s>>>(F.div, count_of(F.dm), &st->rhs2);
-  k_resid_norm<<<reduce_blocks(), 256, 0, s>>>(F.dm, F.div, F.p[start], &st->res2_acc);
-  k_finalize<<<1, 32, 0, s>>>(st, c.tol, c.max_cycles, 0, cond);
+  k_sumsq<<<reduce_blocks(), 256, 0, s>>>(F.div, count_of(F.dm), st->part_rhs);
+  const int nres = resid_norm(s, F.dm, F.div, F.p[start], st->part_res, c.plain);
+  k_finalize<<<1, 256, 0, s>>>(st, c.tol, c.max_cycles, 0, nres, (int)reduce_blocks(), cond);
   return cudaGetLastError();
 }
 
@@ -265,8 +604,8 @@ cudaError_t vcycle_body(cudaStream_t s, const VCycleLevels& L, const VCycleConfi
   const LevelBuf& F = L.lv[0];
   const int fin = level_cycle(s, L, c, 0, start, launches);
   (void)fin;  // == start: the fine level ends in the buffer it started from
-  k_resid_norm<<<reduce_blocks(), 256, 0, s>>>(F.dm, F.div, F.p[start], &st->res2_acc);
-  k_finalize<<<1, 32, 0, s>>>(st, c.tol, c.max_cycles, 1, cond);
+  const int nres = resid_norm(s, F.dm, F.div, F.p[start], st->part_res, c.plain);
+  k_finalize<<<1, 256, 0, s>>>(st, c.tol, c.max_cycles, 1, nres, 0, cond);
   *launches += 2;
   return cudaGetLastError();
 }
@@ -274,9 +613,9 @@ cudaError_t vcycle_body(cudaStream_t s, const VCycleLevels& L, const VCycleConfi
 cudaError_t solver_norms(cudaStream_t s, Dims dm, const float* div, const float* p, double tol, SolverDev* st) {
   cudaError_t e = cudaMemsetAsync(st, 0, sizeof(SolverDev), s);
   if (e != cudaSuccess) return e;
-  k_sumsq<<<reduce_blocks(), 256, 0, s>>>(div, count_of(dm), &st->rhs2);
-  k_resid_norm<<<reduce_blocks(), 256, 0, s>>>(dm, div, p, &st->res2_acc);
-  k_finalize<<<1, 32, 0, s>>>(st, tol, 0, 0, 0);
+  k_sumsq<<<reduce_blocks(), 256, 0, s>>>(div, count_of(dm), st->part_rhs);
+  const int nres = resid_norm(s, dm, div, p, st->part_res, false);
+  k_finalize<<<1, 256, 0, s>>>(st, tol, 0, 0, nres, (int)reduce_blocks(), 0);
   return cudaGetLastError();
 }
 

@@ -15,17 +15,20 @@
 namespace fx {
 
 constexpr int kMaxVLevels = 6;
+// Blocks of a norm kernel: one FP64 partial sum each.
+constexpr int kNormParts = 2048;
 
 // Device-side solver state and statistics (FP64).
 struct SolverDev {
   double rhs2;                     // sum of div^2
   double res2;                     // sum of residual^2 of the latest iterate
-  double res2_acc;                 // accumulator of the residual norm kernel
   unsigned long long maxdiv_bits;  // max |div u| after projection (bits of a non-negative double)
   int cycles;
   int converged;
   int cont;  // 1 while another V-cycle is due
   int pad;
+  double part_rhs[kNormParts];  // per-block partial sums of the norm kernels,
+  double part_res[kNormParts];  // added in a fixed order by the finalize kernel
 };
 
 struct VCycleConfig {
@@ -35,6 +38,7 @@ struct VCycleConfig {
   bool omega_one;
   double tol;
   bool warm;
+  bool plain;  // one-voxel kernels only (the plain path's V-cycle), never the marching ones
 };
 
 // Level k: rhs in `div`, iterate in p[0]/p[1]; level 0 is the fine pressure.

@@ -19,8 +19,8 @@ pytestmark = pytest.mark.gpu
 DT = 1.0 / 60.0
 
 
-def make_pair(options, solver, graphs=True, storage="f32", norms=False):
-    sim = createCombustionVolumeSimulation(options, device=0, kernels="fused", use_graphs=graphs, storage=storage)
+def make_pair(options, solver, graphs=True, storage="f32", norms=False, kernels="fused"):
+    sim = createCombustionVolumeSimulation(options, device=0, kernels=kernels, use_graphs=graphs, storage=storage)
     orc = OracleSimulation(options, precision=32, storage=storage)
     sim.setSolver(solver)
     orc.setSolver(solver, norms=norms)
@@ -60,6 +60,33 @@ def test_vcycle_matches_oracle_ragged(solver, graphs):
     for s in (sim, orc):
         s.updateSources(all_kind_sources(seed=41.0))
     lockstep(sim, orc, 6, f"vcycle{solver}[graphs={graphs}]")
+    assert sim.readSolverStats()["cycles"] >= 1
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+@pytest.mark.parametrize("res", [(128, 96, 64), (48, 30, 22)])
+def test_vcycle_marching_kernels_match_oracle(res, graphs):
+    """Grids where the four-x marching sweep, residual restriction, prolongation
+    and norm kernels run: every level of 128x96x64 halves exactly; 48x30x22 halves
+    once (odd mid-level height and depth), after which the one-voxel kernels run."""
+    wl = workloads.plume_box(res)
+    sim, orc = make_pair(wl.options, {"mode": "vcycle", "levels": 5, "warmStart": True}, graphs=graphs)
+    for s in (sim, orc):
+        s.updateSources(wl.sources)
+        workloads.load_state(s, wl.state)
+    lockstep(sim, orc, 3, f"vcycle march {res} [graphs={graphs}]")
+    st = sim.readSolverStats()
+    assert st["converged"] and st["relativeResidual"] <= 1e-5
+
+
+@pytest.mark.parametrize("res", [(37, 45, 29), (64, 48, 32)])
+def test_plain_path_vcycle_matches_oracle(res):
+    """The plain path's V-cycle (one-voxel kernels, host loop) against the oracle."""
+    opts = {"resolution": res, "worldSize": 1.3}
+    sim, orc = make_pair(opts, {"mode": "vcycle", "levels": 4}, kernels="plain")
+    for s in (sim, orc):
+        s.updateSources(all_kind_sources(seed=43.0))
+    lockstep(sim, orc, 4, f"plain vcycle {res}")
     assert sim.readSolverStats()["cycles"] >= 1
 
 
