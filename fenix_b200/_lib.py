@@ -29,6 +29,7 @@ FX_KERNELS_PLAIN = 1
 FX_OPT_DEBUG_FIELDS = 1 << 0
 FX_OPT_NO_GRAPHS = 1 << 1
 FX_OPT_SCALARS_F16 = 1 << 2
+FX_OPT_SPARSE = 1 << 3
 
 FX_DTYPE_F32 = 0
 FX_DTYPE_F16 = 1
@@ -253,6 +254,8 @@ PROTOTYPES = [
     ("fx_sim_set_solver", c_int32, [c_void_p, POINTER(FxSolverSettings)]),
     ("fx_sim_get_solver", c_int32, [c_void_p, POINTER(FxSolverSettings)]),
     ("fx_sim_read_solver_stats", c_int32, [c_void_p, POINTER(FxSolverStats)]),
+    ("fx_sim_set_sparse", c_int32, [c_void_p, c_int32]),
+    ("fx_sim_get_sparse", c_int32, [c_void_p, POINTER(c_int32)]),
     ("fx_sim_autotune", c_int32, [c_void_p, POINTER(FxAutotuneReport)]),
     ("fx_sim_set_sweep_variants", c_int32, [c_void_p, POINTER(c_int32)]),
     ("fx_sim_get_sweep_variants", c_int32, [c_void_p, POINTER(c_int32)]),

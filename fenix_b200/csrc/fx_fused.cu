@@ -1200,6 +1200,8 @@ __global__ void __launch_bounds__(kBrickThreads) k_rebuild(Dims dm, uint3 bc, SS
 inline dim3 dense_grid(Dims d) { return dim3((d.w + 31) / 32, (d.h + 3) / 4, (d.d + 1) / 2); }
 const dim3 kDenseBlock(32, 4, 2);
 
+#include "fx_fused_sparse.cuh"
+
 // Host: bricks whose voxels an emitter can reach this step (conservative).
 void injection_bricks(const FusedStep& st, std::vector<uint8_t>& mark, std::vector<uint32_t>& out) {
   out.clear();
@@ -1256,7 +1258,7 @@ void injection_bricks(const FusedStep& st, std::vector<uint8_t>& mark, std::vect
 size_t fused_work_bytes(Dims dm, uint3 bricks, size_t aos_voxel_bytes) {
   const size_t nb = (size_t)bricks.x * bricks.y * bricks.z;
   const size_t n = (size_t)dm.w * dm.h * dm.d;
-  return 8 * align256(nb) + 3 * align256(nb * 4) + align256(16 * 4) + align256(sizeof(SolverDev)) + align256(4) +
+  return 12 * align256(nb) + 7 * align256(nb * 4) + align256(16 * 4) + align256(sizeof(SolverDev)) + align256(4) +
          align256(n * aos_voxel_bytes);
 }
 
@@ -1281,6 +1283,8 @@ void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks, size_t ao
   w.list_adv = (uint32_t*)take((size_t)w.nb * 4);
   w.list_next = (uint32_t*)take((size_t)w.nb * 4);
   w.list_inj = (uint32_t*)take((size_t)w.nb * 4);
+  for (auto& b : w.nz_sp) b = (uint8_t*)take(w.nb);
+  for (auto& l : w.list_sp) l = (uint32_t*)take((size_t)w.nb * 4);
   w.counters = (uint32_t*)take(16 * 4);
   w.solver = (SolverDev*)take(sizeof(SolverDev));
   w.vmax = (unsigned*)take(4);
@@ -1300,12 +1304,14 @@ fx_status fused_reset(FusedWork& w, cudaStream_t) {
   // The arena was cleared: every brick is zero, and the device copy of the
   // injection list is gone.
   w.valid = true;
+  w.sp_known = true;
   w.uploaded_list.clear();
   return FX_OK;
 }
 
 fx_status fused_invalidate(FusedWork& w, cudaStream_t) {
   w.valid = false;
+  w.sp_known = false;
   return FX_OK;
 }
 
@@ -1401,6 +1407,14 @@ fx_status fused_prepare(FusedWork& w, const FusedStep& st, uint32_t* ninj_out, F
     w.valid = true;
   }
 
+  // Sparse mode keeps per-brick non-zero bits of the velocity buffers; after a
+  // dense step or a host write every brick may be non-zero.
+  if (st.sparse && !w.sp_known) {
+    for (auto* b : w.nz_sp) FX_CK(cudaMemsetAsync(b, 1, nb, s));
+    w.sp_known = true;
+  }
+  if (!st.sparse) w.sp_known = false;
+
   // 1. injection over the reachable bricks: the list is built on the host and
   // uploaded only when it changes.
   injection_bricks(st, w.host_mark, w.host_list);
@@ -1437,6 +1451,7 @@ uint64_t fused_key(const FusedStep& st, uint32_t ninj) {
   mix_key((uint64_t)st.solver_mode);
   for (int l = 0; l < 3; ++l) mix_key((uint64_t)(st.sweep_variant[l] + 1));
   mix_key(st.solver_norms);
+  mix_key(st.sparse);
   mix_key((uint64_t)(uintptr_t)st.inflow);
   if (st.inflow)
     for (uint32_t v : {st.inflow_patch.x0, st.inflow_patch.y, st.inflow_patch.z0, st.inflow_patch.nx, st.inflow_patch.nz}) mix_key(v);
@@ -1592,6 +1607,12 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     ++launches;
   }
 
+  // Sparse mode: the injected velocity may be non-zero in the injected bricks.
+  if (st.sparse && ninj) {
+    k_sp_mark<<<std::max<uint32_t>(1, std::min<uint32_t>((ninj + 255) / 256, 256)), 256, 0, s>>>(w.list_inj, c_inj, w.nz_sp[SP_VCUR]);
+    ++launches;
+  }
+
   // The inflow patch after injection; its values are not bounded by the recorded
   // max |v|, so the velocity advection clamps on read in this step.
   if (st.inflow) {
@@ -1613,13 +1634,28 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
 
   // 2. flags of the current set, list of bricks for scalar advection
   FX_CK(cudaMemsetAsync(w.counters, 0, 3 * sizeof(uint32_t), s));
+  if (st.sparse) FX_CK(cudaMemsetAsync(w.counters + 4, 0, 4 * sizeof(uint32_t), s));
   {
     Timed tm(w, s, "fused_dilate");
     k_dilate<<<(nb + 255) / 256, 256, 0, s>>>(bc, w.summary_set[cur], st.flags_cur, w.nz_t, nullptr, w.list_adv, c_adv);
     ++launches;
   }
-  // 3. velocity advection (dense)
-  {
+  // 3. velocity advection (dense; sparse mode: over the current flags)
+  if (st.sparse) {
+    if (st.solver_mode != 0) return FX_ERR_UNSUPPORTED;
+    SpLists L{};
+    L.list[0] = w.list_sp[SP_VSCR];
+    L.count[0] = w.counters + 4 + SP_VSCR;
+    L.nz[0] = w.nz_sp[SP_VSCR];
+    {
+      Timed tm(w, s, "sparse_lists");
+      k_sp_lists<<<(nb + 255) / 256, 256, 0, s>>>(nb, st.flags_cur, nullptr, L, nullptr);
+      ++launches;
+    }
+    Timed tm(w, s, "sparse_advect_velocity");
+    k_sp_advect_velocity<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.vcur, st.vscr, L.list[0], L.count[0]);
+    ++launches;
+  } else {
     Timed tm(w, s, "fused_advect_velocity");
     static const int zb = [] {
       const char* v = std::getenv("FENIX_ADV_Z");
@@ -1660,6 +1696,25 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     k_dilate<<<(nb + 255) / 256, 256, 0, s>>>(bc, w.summary_t, st.flags_next, w.nz_t, w.nz_set[next], w.list_next, c_next);
     ++launches;
   }
+  // Sparse mode: U = current | next flags; the lists of the curl, pressure and
+  // velocity buffers (U plus the bricks where they may hold earlier values), and
+  // the velocity scratch is non-zero in U only once buoyancy has run.
+  auto sp_list = [&](int f) { return w.list_sp[f]; };
+  auto sp_count = [&](int f) { return w.counters + 4 + f; };
+  if (st.sparse) {
+    SpLists L{};
+    const int fams[3] = {SP_CURL, SP_PRESSURE, SP_VCUR};
+    const bool due[3] = {st.vort_on, st.pressure_on, true};
+    for (int k = 0; k < 3; ++k) {
+      if (!due[k]) continue;
+      L.list[k] = sp_list(fams[k]);
+      L.count[k] = sp_count(fams[k]);
+      L.nz[k] = w.nz_sp[fams[k]];
+    }
+    Timed tm(w, s, "sparse_lists");
+    k_sp_lists<<<(nb + 255) / 256, 256, 0, s>>>(nb, st.flags_cur, st.flags_next, L, w.nz_sp[SP_VSCR]);
+    ++launches;
+  }
   // 6. combustion T -> next set, 7. buoyancy
   FX_CK(cudaMemsetAsync(w.summary_set[next], 0, nb, s));
   {
@@ -1681,7 +1736,29 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   }
   // 8. vorticity confinement
   const VelField* vfinal = &st.vscr;
-  if (st.vort_on) {
+  if (st.vort_on && st.sparse) {
+    {
+      Timed tm(w, s, "sparse_vorticity");
+      k_sp_vorticity<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.vscr, st.vort_mag, st.vort, st.debug_fields ? 1 : 0, sp_list(SP_CURL),
+                                                          sp_count(SP_CURL));
+      ++launches;
+    }
+    {
+      Timed tm(w, s, "sparse_confinement");
+      by_storage(st.half_storage, [&](auto tag) {
+        using S = typename decltype(tag)::type;
+        if (st.debug_fields)
+          k_sp_confinement<S, true><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.vscr, st.vort_mag, sset<S>(st.next), w.nz_set[next],
+                                                                         st.vscr2, st.conf_mag, sp_list(SP_CURL), sp_count(SP_CURL));
+        else
+          k_sp_confinement<S, false><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.vscr, st.vort_mag, sset<S>(st.next),
+                                                                          w.nz_set[next], st.vscr2, st.conf_mag, sp_list(SP_CURL),
+                                                                          sp_count(SP_CURL));
+      });
+      ++launches;
+    }
+    vfinal = &st.vscr2;
+  } else if (st.vort_on) {
     {
       Timed tm(w, s, "fused_vorticity");
       static const bool v4 = [] {
@@ -1719,6 +1796,91 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     FX_CK(cudaMemsetAsync(w.vmax, 0, sizeof(unsigned), s));
     FX_CK(launch_project(s, dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax));
     ++launches;
+  } else if (st.pressure_on && st.sparse) {
+    // The reference schedule with the fine passes over the sparse lists (the
+    // dense path's buffer ids and fusions; the restriction rides on the
+    // divergence kernel).
+    const int m = st.q[2], n = st.q[3];
+    const LevelBuf& F = st.lv[0];
+    const LevelBuf& M = st.lv[1];
+    const LevelBuf& C = st.lv[2];
+    last_p = (m & 1) ^ (n & 1);
+    FX_CK(cudaMemsetAsync(M.p[0], 0, (size_t)M.dm.w * M.dm.h * M.dm.d * sizeof(float), s));
+    FX_CK(cudaMemsetAsync(C.p[0], 0, (size_t)C.dm.w * C.dm.h * C.dm.d * sizeof(float), s));
+    const bool prolong_live = (m & 1) == 0;
+    const int nwrites = std::max(m, 0) + (m == 0 ? 1 : 0) + n;
+    std::vector<float*> outs(nwrites);
+    for (int i = nwrites; i-- > 0;)
+      outs[i] = (i + 1 == nwrites) ? F.p[last_p] : (outs[i + 1] == F.p[last_p] ? F.p[last_p ^ 1] : F.p[last_p]);
+    int wi = 0;
+    const float* chain = nullptr;
+    const uint32_t* pl = sp_list(SP_PRESSURE);
+    const uint32_t* pc = sp_count(SP_PRESSURE);
+    {
+      Timed tm(w, s, "sparse_div_first_sweep");
+      k_sp_div_first<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, *vfinal, F.div, m >= 1 ? outs[0] : nullptr, M.dm, M.div, pl, pc);
+      ++launches;
+    }
+    if (m >= 1) chain = outs[wi++];
+    int mid = 0;
+    if (prolong_live) {
+      int a = 0;
+      for (int k = 0; k < st.q[4]; ++k) {
+        Timed tm(w, s, "fused_sweep_mid");
+        FX_CK(lean_sweep_variant(s, st.sweep_variant[1], M.dm, M.div, k == 0 ? nullptr : M.p[a], M.p[a ^ 1], M.dm, nullptr));
+        a ^= 1;
+        ++launches;
+      }
+      const int mid_pre = a;
+      {
+        Timed tm(w, s, "fused_restrict");
+        plain_restrict(s, M.dm, C.dm, M.div, C.div);
+        ++launches;
+      }
+      int coarse = 0;
+      for (int k = 0; k < st.q[6]; ++k) {
+        Timed tm(w, s, "fused_sweep_coarse");
+        FX_CK(lean_sweep_variant(s, st.sweep_variant[2], C.dm, C.div, k == 0 ? nullptr : C.p[coarse], C.p[coarse ^ 1], C.dm, nullptr));
+        coarse ^= 1;
+        ++launches;
+      }
+      {
+        Timed tm(w, s, "fused_prolong");
+        plain_prolong(s, C.dm, M.dm, C.p[coarse], M.p[0]);
+        ++launches;
+      }
+      mid = mid_pre;
+      for (int k = 0; k < st.q[5]; ++k) {
+        Timed tm(w, s, "fused_sweep_mid");
+        FX_CK(lean_sweep_variant(s, st.sweep_variant[1], M.dm, M.div, M.p[mid], M.p[mid ^ 1], M.dm, nullptr));
+        mid ^= 1;
+        ++launches;
+      }
+    }
+    for (int k = 2; k <= m; ++k) {
+      const bool add = prolong_live && k == m;
+      Timed tm(w, s, add ? "sparse_sweep_prolong" : "sparse_sweep");
+      k_sp_sweep<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, F.div, chain, outs[wi], M.dm, add ? M.p[mid] : nullptr, 0, pl, pc);
+      chain = outs[wi++];
+      ++launches;
+    }
+    if (m == 0) {
+      Timed tm(w, s, "sparse_prolong_fine");
+      k_sp_sweep<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, F.div, nullptr, outs[wi], M.dm, M.p[mid], 1, pl, pc);
+      chain = outs[wi++];
+      ++launches;
+    }
+    for (int k = 1; k <= n; ++k) {
+      Timed tm(w, s, "sparse_sweep");
+      k_sp_sweep<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, F.div, chain, outs[wi], M.dm, nullptr, 0, pl, pc);
+      chain = outs[wi++];
+      ++launches;
+    }
+    {
+      Timed tm(w, s, "sparse_project");
+      k_sp_project<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, *vfinal, F.p[last_p], st.vcur, sp_list(SP_VCUR), sp_count(SP_VCUR));
+      ++launches;
+    }
   } else if (st.pressure_on) {
     const int m = st.q[2], n = st.q[3];
     const LevelBuf& F = st.lv[0];
@@ -1828,12 +1990,25 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       FX_CK(launch_project(s, dm, *vfinal, F.p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax));
       ++launches;
     }
+  } else if (st.sparse) {
+    Timed tm(w, s, "sparse_project");
+    k_sp_project<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, *vfinal, st.lv[0].p[last_p], st.vcur, sp_list(SP_VCUR), sp_count(SP_VCUR));
+    ++launches;
   } else {
     // 10. projection with the pressure of the last solve (+ |v|)
     Timed tm(w, s, "fused_project");
     FX_CK(cudaMemsetAsync(w.vmax, 0, sizeof(unsigned), s));
     FX_CK(launch_project(s, dm, *vfinal, st.lv[0].p[last_p], st.vcur, st.vel_mag, st.debug_on ? 1 : 0, w.vmax));
     ++launches;
+  }
+  if (st.sparse) {
+    // the sparse projection records no max |v|; |v| for the debug fields over the grid
+    FX_CK(cudaMemsetAsync(w.vmax, 0xFF, sizeof(unsigned), s));
+    if (st.debug_on) {
+      Timed tm(w, s, "sparse_velocity_magnitude");
+      k_sp_velocity_magnitude<<<(uint32_t)device_sm_count() * 8u, 256, 0, s>>>(dm, st.vcur, st.vel_mag);
+      ++launches;
+    }
   }
   // FP64 statistics of the solve: ||div||, ||div - A p|| (the V-cycle has them
   // already) and max |div u| of the projected velocity.

@@ -46,7 +46,15 @@ struct FusedWork {
   uint32_t* list_adv = nullptr;   // bricks the scalar advection kernel visits
   uint32_t* list_next = nullptr;  // bricks the combustion/buoyancy kernels visit
   uint32_t* list_inj = nullptr;   // bricks the injection kernel visits (host-filled)
-  uint32_t* counters = nullptr;   // [0] adv count, [1] next count, [2] scratch, [3] inject count
+  uint32_t* counters = nullptr;   // [0] adv count, [1] next count, [2] scratch, [3] inject count, [4..7] sparse lists
+  // Sparse mode: per-brick "may be non-zero" bits of the velocity-side buffer
+  // families (velocity scratch; curl, |curl| and the confined velocity; the fine
+  // divergence and pressure; the velocity), the brick lists of the sparse
+  // kernels, one per family, and whether the bits track the buffers (false
+  // after a dense step or a host write: then every brick may be non-zero).
+  uint8_t* nz_sp[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint32_t* list_sp[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool sp_known = true;
   SolverDev* solver = nullptr;     // FP64 solver statistics and the V-cycle loop state
   unsigned* vmax = nullptr;        // max |v| of the current velocity (float bits; all ones = unknown)
   cudaStream_t aux = nullptr;      // captures the V-cycle body graph
@@ -104,6 +112,7 @@ struct FusedStep {
   VCycleConfig vc;
   bool solver_norms;  // FP64 statistics after the reference schedule too
   bool vort_on, pressure_on, debug_on, debug_fields;
+  bool sparse = false;  // sparse mode (extension): velocity passes on the active bricks only
   int last_p;
 };
 

@@ -1,0 +1,344 @@
+// Sparse mode of the fused path (an extension; part of fx_fused.cu, included
+// inside its anonymous namespace).
+//
+// The reference runs velocity advection, curl, confinement, divergence, the
+// fine pressure sweeps and the projection over the whole grid
+// (runtime/createCombustionVolumeSimulation.ts:270-296) while only a sixth of
+// its bricks hold smoke. Sparse mode runs them on a set of bricks and keeps them
+// zero outside it:
+//  - velocity advection computes in the bricks flagged in the current set
+//    (compute-active-bricks.wgsl.ts), 0 elsewhere;
+//  - once the next set's flags exist, U = current | next flags; curl, |curl|,
+//    confinement, divergence, every fine sweep, the fine prolongation and the
+//    projection compute as the reference inside U and give 0 outside it.
+// Scalar passes, injection, the mid and coarse levels and the restriction are
+// the reference's. The oracle has the same mode (Sim::sparse), and each voxel
+// computed here is the parity kernels' arithmetic in their order, so the two
+// agree bit for bit.
+//
+// Fields keep their dense layout: a gather or stencil that leaves the set reads
+// the zeros stored there, with no indirection. Per-brick "may be non-zero" bits
+// of each buffer family tell which bricks outside the set still hold values of
+// an earlier step; the lists the kernels walk are the set plus those bricks,
+// each entry the brick index with bit 31 set where the brick is computed and
+// clear where it is only zeroed.
+constexpr uint32_t kSpCompute = 0x80000000u;
+constexpr uint32_t kSpIndex = 0x7FFFFFFFu;
+
+// Buffer families with their own non-zero bits (FusedWork::nz_sp).
+enum SpFamily { SP_VSCR = 0, SP_CURL = 1, SP_PRESSURE = 2, SP_VCUR = 3, kSpFamilies = 4 };
+
+// Builds up to three lists over the bricks. For list k: a brick is computed when
+// flags_a or flags_b (nullable) flags it, and listed when computed or when
+// nz[k] marks it; nz[k] then marks exactly the computed bricks. extra (nullable)
+// also receives the computed marks. Lists of families that are not due (null)
+// are skipped, and their bits are left alone.
+struct SpLists {
+  uint32_t* list[3];
+  uint32_t* count[3];
+  uint8_t* nz[3];
+};
+
+__global__ void __launch_bounds__(256) k_sp_lists(uint32_t nb, const uint32_t* __restrict__ flags_a, const uint32_t* __restrict__ flags_b,
+                                                  SpLists L, uint8_t* __restrict__ extra) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31u;
+  const bool live = b < nb;
+  const bool comp = live && (__ldg(flags_a + b) != 0u || (flags_b && __ldg(flags_b + b) != 0u));
+  if (live && extra) extra[b] = comp ? 1 : 0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (!L.list[k]) continue;  // uniform
+    const bool take = comp || (live && L.nz[k][b] != 0);
+    const unsigned ballot = __ballot_sync(0xffffffffu, take);
+    uint32_t base = 0;
+    if (lane == 0 && ballot) base = atomicAdd(L.count[k], (uint32_t)__popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (take) L.list[k][base + __popc(ballot & ((1u << lane) - 1u))] = b | (comp ? kSpCompute : 0u);
+    if (live) L.nz[k][b] = comp ? 1 : 0;
+  }
+}
+
+// Marks the bricks of a host-built list (the injection list) in nz.
+__global__ void k_sp_mark(const uint32_t* __restrict__ list, const uint32_t* __restrict__ count, uint8_t* __restrict__ nz) {
+  const uint32_t n = *count;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) nz[list[i]] = 1;
+}
+
+// The prolongation term of pressure-prolongation.wgsl.ts:42-43 at fine voxel (x, y, z).
+FX_DEV float prolong_sample_at(const Dims& mid, const float* __restrict__ mp, int x, int y, int z) {
+  const float px = ((float)x + 0.5f) * 0.5f - 0.5f;
+  const float py = ((float)y + 0.5f) * 0.5f - 0.5f;
+  const float pz = ((float)z + 0.5f) * 0.5f - 0.5f;
+  return tri_interp(mp, tri_corners(mid, px, py, pz));
+}
+
+// Thread -> voxel of a 256-thread brick block: x = t & 7, y = (t >> 3) & 7 and
+// z = t >> 6, plus 4 for the second voxel.
+struct SpVoxel {
+  uint32_t x, y, z, i;
+  bool inside;
+};
+FX_DEV SpVoxel sp_voxel(const Dims& dm, const BrickCtx& c, int j) {
+  SpVoxel v;
+  v.x = c.x0 + (threadIdx.x & 7u);
+  v.y = c.y0 + ((threadIdx.x >> 3) & 7u);
+  v.z = c.z0 + ((threadIdx.x + kBrickThreads * j) >> 6);
+  v.inside = v.x < dm.w && v.y < dm.h && v.z < dm.d;
+  v.i = v.inside ? flat(dm, v.x, v.y, v.z) : 0u;
+  return v;
+}
+
+// advect-velocity-semilagrangian.wgsl.ts:23-41 in computed bricks, over
+// vCurrent clamped to +-80/dx on read (advect_velocity_column<true>'s
+// arithmetic); 0 in zeroed bricks.
+__global__ void __launch_bounds__(kBrickThreads) k_sp_advect_velocity(Dims dm, uint3 bc, const Params* __restrict__ Pp, VelField src,
+                                                                      VelField dst, const uint32_t* __restrict__ list,
+                                                                      const uint32_t* __restrict__ count) {
+  const float dt = Pp->dt;
+  const float lim = speed_limit(*Pp);
+  const float damp = 1.0f - dt * 0.025f;
+  const uint32_t n = *count;
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t e = list[li];
+    const bool comp = (e & kSpCompute) != 0u;
+    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const SpVoxel v = sp_voxel(dm, c, j);
+      if (!v.inside) continue;
+      float ox = 0.f, oy = 0.f, oz = 0.f;
+      if (comp && !is_boundary(dm, v.x, v.y, v.z)) {
+        const float cx = (float)v.x + 0.5f, cy = (float)v.y + 0.5f, cz = (float)v.z + 0.5f;
+        const float v0x = clampv(__ldg(src.c[0] + v.i), -lim, lim);
+        const float v0y = clampv(__ldg(src.c[1] + v.i), -lim, lim);
+        const float v0z = clampv(__ldg(src.c[2] + v.i), -lim, lim);
+        const float bx = cx - v0x * dt, by = cy - v0y * dt, bz = cz - v0z * dt;
+        const Tri c1 = tri_corners(dm, bx - 0.5f, by - 0.5f, bz - 0.5f);
+        ox = tri_interp_clamped(src.c[0], c1, lim) * damp;
+        oy = tri_interp_clamped(src.c[1], c1, lim) * damp;
+        oz = tri_interp_clamped(src.c[2], c1, lim) * damp;
+      }
+      dst.c[0][v.i] = ox;
+      dst.c[1][v.i] = oy;
+      dst.c[2][v.i] = oz;
+    }
+  }
+}
+
+// compute-vorticity.wgsl.ts:23-50: |w| (w itself with debug fields) in computed
+// bricks, 0 in zeroed bricks and on the boundary.
+__global__ void __launch_bounds__(kBrickThreads) k_sp_vorticity(Dims dm, uint3 bc, VelField v, float* __restrict__ wmag, VelField w,
+                                                                int write_w, const uint32_t* __restrict__ list,
+                                                                const uint32_t* __restrict__ count) {
+  const uint32_t n = *count;
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t e = list[li];
+    const bool comp = (e & kSpCompute) != 0u;
+    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const SpVoxel q = sp_voxel(dm, c, j);
+      if (!q.inside) continue;
+      float cx = 0.f, cy = 0.f, cz = 0.f;
+      const bool live = comp && !is_boundary(dm, q.x, q.y, q.z);
+      if (live) curl_at(v, q.i, sy, sz, cx, cy, cz);
+      wmag[q.i] = live ? length3(cx, cy, cz) : 0.0f;
+      if (write_w) {
+        w.c[0][q.i] = cx;
+        w.c[1][q.i] = cy;
+        w.c[2][q.i] = cz;
+      }
+    }
+  }
+}
+
+// apply-vorticity-confinement.wgsl.ts:30-66 in computed bricks (k_confinement's
+// arithmetic, out = vScratch + F dt clamped); the boundary passes vScratch
+// through, and zeroed bricks get 0 (vScratch is 0 there).
+template <typename S, bool FMAG>
+__global__ void __launch_bounds__(kBrickThreads) k_sp_confinement(Dims dm, uint3 bc, const Params* __restrict__ Pp, VelField v,
+                                                                  const float* __restrict__ wmag, SSet<S> set, const uint8_t* __restrict__ nz,
+                                                                  VelField out, float* __restrict__ fmag, const uint32_t* __restrict__ list,
+                                                                  const uint32_t* __restrict__ count) {
+  const Params P = *Pp;
+  const uint32_t n = *count;
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t e = list[li];
+    const bool comp = (e & kSpCompute) != 0u;
+    const uint32_t b = e & kSpIndex;
+    const BrickCtx c = brick_ctx(dm, bc, b);
+    const bool scal = __ldg(nz + b) != 0;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const SpVoxel q = sp_voxel(dm, c, j);
+      if (!q.inside) continue;
+      if (!comp) {
+        out.c[0][q.i] = 0.0f;
+        out.c[1][q.i] = 0.0f;
+        out.c[2][q.i] = 0.0f;
+        if (FMAG) fmag[q.i] = 0.0f;
+        continue;
+      }
+      float vx = __ldg(v.c[0] + q.i), vy = __ldg(v.c[1] + q.i), vz = __ldg(v.c[2] + q.i);
+      if (is_boundary(dm, q.x, q.y, q.z)) {
+        out.c[0][q.i] = vx;
+        out.c[1][q.i] = vy;
+        out.c[2][q.i] = vz;
+        if (FMAG) fmag[q.i] = 0.0f;
+        continue;
+      }
+      const uint32_t i = q.i;
+      const float gx = (__ldg(wmag + i + 1u) - __ldg(wmag + i - 1u)) * 0.5f;
+      const float gy = (__ldg(wmag + i + sy) - __ldg(wmag + i - sy)) * 0.5f;
+      const float gz = (__ldg(wmag + i + sz) - __ldg(wmag + i - sz)) * 0.5f;
+      float wx, wy, wz;
+      curl_at(v, i, sy, sz, wx, wy, wz);
+      float d = 0.f, t = 0.f, r = 0.f;
+      if (scal) {
+        d = ldS(set.f[0], i);
+        t = ldS(set.f[1], i);
+        r = ldS(set.f[3], i);
+      }
+      if (FMAG) {
+        fmag[i] = confinement_voxel(P, gx, gy, gz, wx, wy, wz, __ldg(wmag + i), d, t, r, vx, vy, vz);
+      } else {
+        confinement_voxel_v(P, gx, gy, gz, wx, wy, wz, __ldg(wmag + i), d, t, r, vx, vy, vz);
+      }
+      out.c[0][i] = vx;
+      out.c[1][i] = vy;
+      out.c[2][i] = vz;
+    }
+  }
+}
+
+// compute-divergence.wgsl.ts:22-42 in computed bricks (0 in zeroed bricks and on
+// the boundary), with the first Jacobi sweep from the cleared buffer,
+// (0 - div) / 6, when p1 is given, and the restriction of the brick's
+// divergence into the mid cells it covers (pressure-restriction.wgsl.ts:27-50:
+// the mean of the clamped 2x2x2 children, 0 on the mid boundary). Every mid cell
+// m lies in fine brick m >> 2 (the mid level is at most half the fine one, or 4
+// cells on a grid under 8), and so do its clamped children.
+__global__ void __launch_bounds__(kBrickThreads) k_sp_div_first(Dims dm, uint3 bc, VelField v, float* __restrict__ div, float* __restrict__ p1,
+                                                                Dims mid, float* __restrict__ mid_div, const uint32_t* __restrict__ list,
+                                                                const uint32_t* __restrict__ count) {
+  __shared__ float sd[512];
+  const uint32_t n = *count;
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t e = list[li];
+    const bool comp = (e & kSpCompute) != 0u;
+    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const SpVoxel q = sp_voxel(dm, c, j);
+      float dv = 0.0f;
+      if (q.inside) {
+        const bool live = comp && !is_boundary(dm, q.x, q.y, q.z);
+        if (live) {
+          const Nbr nb = neighbours(dm, q.x, q.y, q.z, q.i);
+          const float ddx = __ldg(v.c[0] + nb.xp) - __ldg(v.c[0] + nb.xm);
+          const float ddy = __ldg(v.c[1] + nb.yp) - __ldg(v.c[1] + nb.ym);
+          const float ddz = __ldg(v.c[2] + nb.zp) - __ldg(v.c[2] + nb.zm);
+          dv = (ddx + ddy + ddz) * 0.5f;
+        }
+        div[q.i] = dv;
+        if (p1) p1[q.i] = live ? div6(0.0f - dv) : 0.0f;
+      }
+      sd[threadIdx.x + kBrickThreads * j] = dv;
+    }
+    __syncthreads();
+    if (threadIdx.x < 64u) {
+      const uint32_t mx = c.bx * 4u + (threadIdx.x & 3u), my = c.by * 4u + ((threadIdx.x >> 2) & 3u), mz = c.bz * 4u + (threadIdx.x >> 4);
+      if (mx < mid.w && my < mid.h && mz < mid.d) {
+        float out = 0.0f;
+        if (mx != 0u && my != 0u && mz != 0u && mx != mid.w - 1u && my != mid.h - 1u && mz != mid.d - 1u) {
+          float sum = 0.0f;
+          for (uint32_t dz = 0; dz < 2u; ++dz)
+            for (uint32_t dy = 0; dy < 2u; ++dy)
+              for (uint32_t dx = 0; dx < 2u; ++dx) {
+                const uint32_t fx = min(2u * mx + dx, dm.w - 1u) - c.x0, fy = min(2u * my + dy, dm.h - 1u) - c.y0,
+                               fz = min(2u * mz + dz, dm.d - 1u) - c.z0;
+                sum += sd[fx + 8u * (fy + 8u * fz)];
+              }
+          out = sum * 0.125f;
+        }
+        mid_div[flat(mid, mx, my, mz)] = out;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// One fine Jacobi sweep (pressure-jacobi.wgsl.ts:15-36) in computed bricks, 0 in
+// zeroed bricks and on the boundary. src NULL is the cleared buffer. With mid_p,
+// the prolongation of the mid level is added to each interior result
+// (pressure-prolongation.wgsl.ts:36-43, as k_sweep does); with `only_prolong`,
+// the result is 0 + the prolongation (the cleared buffer prolonged into).
+__global__ void __launch_bounds__(kBrickThreads) k_sp_sweep(Dims dm, uint3 bc, const float* __restrict__ div, const float* __restrict__ src,
+                                                            float* __restrict__ dst, Dims mid, const float* __restrict__ mid_p, int only_prolong,
+                                                            const uint32_t* __restrict__ list, const uint32_t* __restrict__ count) {
+  const uint32_t n = *count;
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t e = list[li];
+    const bool comp = (e & kSpCompute) != 0u;
+    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const SpVoxel q = sp_voxel(dm, c, j);
+      if (!q.inside) continue;
+      float out = 0.0f;
+      if (comp && !is_boundary(dm, q.x, q.y, q.z)) {
+        if (only_prolong) {
+          out = 0.0f + prolong_sample_at(mid, mid_p, (int)q.x, (int)q.y, (int)q.z);
+        } else {
+          const uint32_t sy = dm.w, sz = dm.w * dm.h, i = q.i;
+          float s = 0.0f;
+          if (src) s = __ldg(src + i + 1u) + __ldg(src + i - 1u) + __ldg(src + i + sy) + __ldg(src + i - sy) + __ldg(src + i + sz) + __ldg(src + i - sz);
+          out = div6((src ? s : 0.0f) - __ldg(div + i));
+          if (mid_p) out = out + prolong_sample_at(mid, mid_p, (int)q.x, (int)q.y, (int)q.z);
+        }
+      }
+      dst[q.i] = out;
+    }
+  }
+}
+
+// project-velocity.wgsl.ts:21-43 in computed bricks (vCurrent = vScratch - the
+// central pressure gradient), 0 in zeroed bricks and on the boundary.
+__global__ void __launch_bounds__(kBrickThreads) k_sp_project(Dims dm, uint3 bc, VelField vs, const float* __restrict__ p, VelField vd,
+                                                              const uint32_t* __restrict__ list, const uint32_t* __restrict__ count) {
+  const uint32_t n = *count;
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t e = list[li];
+    const bool comp = (e & kSpCompute) != 0u;
+    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const SpVoxel q = sp_voxel(dm, c, j);
+      if (!q.inside) continue;
+      float ox = 0.f, oy = 0.f, oz = 0.f;
+      if (comp && !is_boundary(dm, q.x, q.y, q.z)) {
+        const uint32_t i = q.i;
+        const float gx = (__ldg(p + i + 1u) - __ldg(p + i - 1u)) * 0.5f;
+        const float gy = (__ldg(p + i + sy) - __ldg(p + i - sy)) * 0.5f;
+        const float gz = (__ldg(p + i + sz) - __ldg(p + i - sz)) * 0.5f;
+        ox = __ldg(vs.c[0] + i) - gx;
+        oy = __ldg(vs.c[1] + i) - gy;
+        oz = __ldg(vs.c[2] + i) - gz;
+      }
+      vd.c[0][q.i] = ox;
+      vd.c[1][q.i] = oy;
+      vd.c[2][q.i] = oz;
+    }
+  }
+}
+
+// |v| (compute-debug-fields.wgsl.ts:18-25) over the whole grid.
+__global__ void __launch_bounds__(256) k_sp_velocity_magnitude(Dims dm, VelField v, float* __restrict__ out) {
+  const uint32_t n = dm.w * dm.h * dm.d;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = length3(__ldg(v.c[0] + i), __ldg(v.c[1] + i), __ldg(v.c[2] + i));
+}

@@ -97,6 +97,7 @@ struct fx_sim {
   int kernels = FX_KERNELS_FUSED;
   uint32_t opt_flags = 0;
   bool half = false;  // FX_OPT_SCALARS_F16: the scalar sets are binary16 buffers
+  bool sparse = false;  // FX_OPT_SPARSE / fx_sim_set_sparse
   fx_solver_settings solver{};
   uint32_t last_cycle_launches = 0;  // kernels per V-cycle in the latest step
   int sweep_variant[3] = {-1, -1, -1};  // sweep kernel per pressure level, chosen by fx_sim_autotune
@@ -579,6 +580,7 @@ fx_status step_begin(fx_sim* s, double elapsed, double step_s, StepPlan& sp) {
   fs.pressure_on = sp.pressure_on;
   fs.debug_on = sp.debug_on;
   fs.debug_fields = (s->opt_flags & FX_OPT_DEBUG_FIELDS) != 0;
+  fs.sparse = s->sparse;
   fs.last_p = s->last_p;
   return FX_OK;
 }
@@ -694,6 +696,8 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
     return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_create: unknown kernels path");
   if ((opt.flags & FX_OPT_SCALARS_F16) && opt.kernels != FX_KERNELS_FUSED)
     return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_sim_create: FP16 scalar storage needs the fused kernels");
+  if ((opt.flags & FX_OPT_SPARSE) && opt.kernels != FX_KERNELS_FUSED)
+    return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_sim_create: sparse mode needs the fused kernels");
 
   fx_sim* s = new (std::nothrow) fx_sim;
   if (!s) return fail(nullptr, FX_ERR_OUT_OF_MEMORY, "fx_sim_create: host allocation failed");
@@ -706,6 +710,7 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
   s->kernels = opt.kernels;
   s->opt_flags = opt.flags;
   s->half = (opt.flags & FX_OPT_SCALARS_F16) != 0;
+  s->sparse = (opt.flags & FX_OPT_SPARSE) != 0;
   s->dm = Dims{w, h, d};
   s->n = w * h * d;
   s->bricks = make_uint3((w + 7) / 8, (h + 7) / 8, (d + 7) / 8);
@@ -1162,6 +1167,8 @@ fx_status fx_sim_set_solver(fx_sim* s, const fx_solver_settings* v) {
     return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_solver: a count is out of range");
   if (!(v->omega > 0.0 && v->omega <= 1.0) || !(v->tolerance >= 0.0) || !std::isfinite(v->tolerance))
     return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_solver: omega must be in (0, 1] and tolerance finite and >= 0");
+  if (v->mode == FX_SOLVER_VCYCLE && s->sparse)
+    return fail(s, FX_ERR_UNSUPPORTED, "fx_sim_set_solver: sparse mode has no V-cycle form");
   s->solver = *v;
   s->solver.reserved = 0;
   return FX_OK;
@@ -1245,6 +1252,20 @@ fx_status fx_sim_autotune(fx_sim* s, fx_autotune_report* o) {
   cudaEventDestroy(ev[1]);
   if (st != FX_OK) return st;
   FX_CUDA(s, cudaGetLastError());
+  return FX_OK;
+}
+
+fx_status fx_sim_set_sparse(fx_sim* s, int32_t on) {
+  if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_sparse: NULL handle");
+  if (on && s->kernels != FX_KERNELS_FUSED) return fail(s, FX_ERR_UNSUPPORTED, "fx_sim_set_sparse: sparse mode needs the fused kernels");
+  if (on && s->solver.mode == FX_SOLVER_VCYCLE) return fail(s, FX_ERR_UNSUPPORTED, "fx_sim_set_sparse: sparse mode has no V-cycle form");
+  s->sparse = on != 0;
+  return FX_OK;
+}
+
+fx_status fx_sim_get_sparse(fx_sim* s, int32_t* on) {
+  if (!s || !on) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_sparse: NULL argument");
+  *on = s->sparse ? 1 : 0;
   return FX_OK;
 }
 
@@ -1569,6 +1590,7 @@ fx_status rollout_check(fx_rollout* r) {
   fx_sim* s = r->s;
   if (!s->err.empty()) return fail(nullptr, FX_ERR_STATE, "fx_rollout: the simulation has an error: " + s->err);
   if (s->half) return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_rollout: the simulation must use f32 storage");
+  if (s->sparse) return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_rollout: the adjoint differentiates the dense step, not sparse mode");
   if (s->solver.mode != FX_SOLVER_REFERENCE || s->advect_mode != FX_ADVECT_MACCORMACK)
     return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_rollout: needs the reference pressure schedule and MacCormack advection");
   if (s->qi[0] != 1 || s->qi[1] != 1)

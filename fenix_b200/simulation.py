@@ -343,6 +343,17 @@ class CombustionVolumeSimulation:
         check(self._lib.fx_sim_get_sweep_variants(self._h, arr), None)
         return list(arr)
 
+    # -- sparse mode (extension) ---------------------------------------------------
+    def setSparse(self, on: bool) -> None:
+        """Velocity passes on the active bricks only, zero elsewhere (FX_OPT_SPARSE),
+        from the next step."""
+        check(self._lib.fx_sim_set_sparse(self._h, 1 if on else 0), self._h)
+
+    def getSparse(self) -> bool:
+        v = ctypes.c_int32()
+        check(self._lib.fx_sim_get_sparse(self._h, ctypes.byref(v)), self._h)
+        return bool(v.value)
+
     def readSolverStats(self) -> Dict[str, Any]:
         """FP64 statistics of the latest solve (waits for the stream)."""
         st = _lib.FxSolverStats()
@@ -423,9 +434,11 @@ def solver_dict(st: "_lib.FxSolverSettings") -> Dict[str, Any]:
 
 
 def build_options(options: Optional[Mapping[str, Any]] = None, *, device: int = 0, kernels: str = "fused",
-                  debug_fields: bool = False, use_graphs: bool = True, storage: str = "f32", stream: int = 0) -> FxSimOptions:
+                  debug_fields: bool = False, use_graphs: bool = True, storage: str = "f32", stream: int = 0,
+                  sparse: bool = False) -> FxSimOptions:
     """CombustionVolumeSimulationOptions -> fx_sim_options. storage="f16" stores the
-    scalar sets in binary16 (fused kernels only)."""
+    scalar sets in binary16 and sparse=True runs the velocity passes on the active
+    bricks only (both fused kernels only)."""
     if storage not in STORAGE:
         raise ValueError(f"unknown storage {storage!r}; expected one of {sorted(STORAGE)}")
     lib = _lib.load()
@@ -453,19 +466,20 @@ def build_options(options: Optional[Mapping[str, Any]] = None, *, device: int = 
         opt.runtime_mask = rmask
     opt.device = device
     opt.kernels = KERNEL_PATHS[kernels]
-    opt.flags = (_lib.FX_OPT_DEBUG_FIELDS if debug_fields else 0) | (0 if use_graphs else _lib.FX_OPT_NO_GRAPHS) | STORAGE[storage]
+    opt.flags = ((_lib.FX_OPT_DEBUG_FIELDS if debug_fields else 0) | (0 if use_graphs else _lib.FX_OPT_NO_GRAPHS) | STORAGE[storage]
+                 | (_lib.FX_OPT_SPARSE if sparse else 0))
     opt.stream = stream or None
     return opt
 
 
 def createCombustionVolumeSimulation(options: Optional[Mapping[str, Any]] = None, *, device: int = 0, kernels: str = "fused",
                                      debug_fields: bool = False, use_graphs: bool = True, storage: str = "f32",
-                                     stream: int = 0) -> CombustionVolumeSimulation:
+                                     stream: int = 0, sparse: bool = False) -> CombustionVolumeSimulation:
     """createCombustionVolumeSimulation.ts:50-401 on CUDA device `device`. `stream`
     (a cudaStream_t as an integer, 0 = the simulation's own) is where it enqueues."""
     lib = _lib.load()
     opt = build_options(options, device=device, kernels=kernels, debug_fields=debug_fields, use_graphs=use_graphs, storage=storage,
-                        stream=stream)
+                        stream=stream, sparse=sparse)
     handle = ctypes.c_void_p()
     check(lib.fx_sim_create(ctypes.byref(opt), ctypes.byref(handle)))
     return CombustionVolumeSimulation(handle, lib)

@@ -115,6 +115,17 @@ typedef struct fx_runtime_params {
  * and writes still exchange f32 (writes are rounded), and the render buffers
  * report FX_DTYPE_F16. */
 #define FX_OPT_SCALARS_F16 (1u << 2)
+/* Sparse mode (extension; fused kernels and the reference pressure schedule
+ * only). The reference computes velocity advection, curl, confinement,
+ * divergence, the fine pressure sweeps and the projection over the whole grid
+ * (runtime/createCombustionVolumeSimulation.ts:270-296). In sparse mode velocity
+ * advection runs in the bricks flagged in the current scalar set, and the
+ * others in U = the bricks flagged in the current or the next set; velocity and
+ * the fine pressure and divergence are 0 outside those bricks. Scalar passes,
+ * injection and the mid and coarse pressure levels are unchanged. Results
+ * differ from the reference where the velocity outside the active bricks
+ * matters; fx_sim_set_sparse switches it at run time. */
+#define FX_OPT_SPARSE (1u << 3)
 
 /* CombustionVolumeSimulationOptions (createCombustionVolumeSimulation.ts:39-48).
  * Fill with fx_sim_options_default() and then override fields. */
@@ -336,6 +347,12 @@ typedef struct fx_solver_stats {
 } fx_solver_stats;
 
 fx_status fx_sim_read_solver_stats(fx_sim* sim, fx_solver_stats* out);
+
+/* Sparse mode on (1) or off (0) from the next step (see FX_OPT_SPARSE). No
+ * counterpart in the reference. FX_ERR_UNSUPPORTED with the plain kernels or
+ * the V-cycle solver. */
+fx_status fx_sim_set_sparse(fx_sim* sim, int32_t on);
+fx_status fx_sim_get_sparse(fx_sim* sim, int32_t* on);
 
 /* Autotuning (extension): times every sweep kernel variant of the pressure
  * solve on each level (fine, mid, coarse) of this simulation's grid and keeps

@@ -355,6 +355,26 @@ template <class R> class Sim {
   // value a reference pass stores into one of those buffers is rounded to the
   // nearest binary16 (ties to even) and read back as R. Arithmetic stays in R.
   bool half_storage = false;
+  // Sparse mode (extension; orc_set_sparse). The velocity passes run on a set of
+  // bricks and are zero outside it, where the reference runs them on the whole
+  // grid (createCombustionVolumeSimulation.ts:270-296):
+  //  - velocity advection computes vScratch in the bricks flagged in the current
+  //    set (the reference's flags, compute-active-bricks.wgsl.ts) and writes 0
+  //    elsewhere;
+  //  - after the flags of the next set, U = current flags | next flags; curl,
+  //    |curl|, confinement, divergence, every fine Jacobi sweep and the fine
+  //    prolongation compute as the reference inside U and write 0 outside it,
+  //    and the projection writes the new velocity inside U and 0 outside it.
+  // Scalar passes, injection, the mid and coarse pressure levels and the
+  // restriction are the reference's. So velocity and the fine pressure are zero
+  // outside U, and stencils at U's edge read those zeros.
+  bool sparse = false;
+  std::vector<uint8_t> uset;  // per brick: in U this step
+  bool in_set(const std::vector<uint8_t>& m, uint32_t x, uint32_t y, uint32_t z) const {
+    const uint32_t bx = std::min(x / kBrick, bcx - 1), by = std::min(y / kBrick, bcy - 1), bz = std::min(z / kBrick, bcz - 1);
+    return m[bx + bcx * (by + bcy * bz)] != 0;
+  }
+  bool outside_u(uint32_t x, uint32_t y, uint32_t z) const { return sparse && !in_set(uset, x, y, z); }
   R qs(R v) const {
     if constexpr (is_tan<R>::value) return v;
     else return half_storage ? (R)(_Float16)v : v;
@@ -417,6 +437,7 @@ template <class R> class Sim {
       l.pb.assign(l.dm.n, R(0));
     }
     sources.assign(32, 0.0f);
+    uset.assign(nb, 0);
   }
 
   // createCombustionVolumeSimulation.ts:206-226
@@ -444,6 +465,7 @@ template <class R> class Sim {
     std::fill(vel_mag.begin(), vel_mag.end(), R(0));
     std::fill(flags[0].begin(), flags[0].end(), 0u);
     std::fill(flags[1].begin(), flags[1].end(), 0u);
+    std::fill(uset.begin(), uset.end(), 0);
     for (auto& l : lv) std::fill(l.pa.begin(), l.pa.end(), R(0));
   }
 
@@ -740,7 +762,7 @@ template <class R> class Sim {
   void advect_velocity() {
     for_voxels(dm, [&](uint32_t x, uint32_t y, uint32_t z) {
       const size_t i = flat(dm, x, y, z);
-      if (is_boundary(dm, x, y, z)) {
+      if (is_boundary(dm, x, y, z) || (sparse && !is_active_coord(flags[cur], x, y, z))) {
         vs[0][i] = vs[1][i] = vs[2][i] = R(0);
         return;
       }
@@ -973,7 +995,7 @@ template <class R> class Sim {
     const uint32_t W1 = dm.w - 1, H1 = dm.h - 1, D1 = dm.d - 1;
     for_voxels(dm, [&](uint32_t x, uint32_t y, uint32_t z) {
       const size_t i = flat(dm, x, y, z);
-      if (is_boundary(dm, x, y, z)) {
+      if (is_boundary(dm, x, y, z) || outside_u(x, y, z)) {
         vort[0][i] = vort[1][i] = vort[2][i] = R(0);
         vort_mag[i] = R(0);
         return;
@@ -999,7 +1021,7 @@ template <class R> class Sim {
     const uint32_t W1 = dm.w - 1, H1 = dm.h - 1, D1 = dm.d - 1;
     for_voxels(dm, [&](uint32_t x, uint32_t y, uint32_t z) {
       const size_t i = flat(dm, x, y, z);
-      if (is_boundary(dm, x, y, z)) {
+      if (is_boundary(dm, x, y, z) || outside_u(x, y, z)) {  // vScratch is 0 outside U already
         conf_mag[i] = R(0);
         return;
       }
@@ -1033,7 +1055,7 @@ template <class R> class Sim {
     const uint32_t W1 = dm.w - 1, H1 = dm.h - 1, D1 = dm.d - 1;
     for_voxels(dm, [&](uint32_t x, uint32_t y, uint32_t z) {
       const size_t i = flat(dm, x, y, z);
-      if (is_boundary(dm, x, y, z)) {
+      if (is_boundary(dm, x, y, z) || outside_u(x, y, z)) {
         div[i] = R(0);
         return;
       }
@@ -1048,9 +1070,10 @@ template <class R> class Sim {
   void jacobi(Level<R>& L, const std::vector<R>& src, std::vector<R>& dst) {
     const Dims& d = L.dm;
     const uint32_t W1 = d.w - 1, H1 = d.h - 1, D1 = d.d - 1;
+    const bool fine = &L == &lv[0];
     for_voxels(d, [&](uint32_t x, uint32_t y, uint32_t z) {
       const size_t i = flat(d, x, y, z);
-      if (is_boundary(d, x, y, z)) {
+      if (is_boundary(d, x, y, z) || (fine && outside_u(x, y, z))) {
         dst[i] = R(0);
         return;
       }
@@ -1102,9 +1125,10 @@ template <class R> class Sim {
   // shaders/passes/pressure-prolongation.wgsl.ts:29-44 (fine.pressureA += coarse)
   void prolong(const Level<R>& C, const std::vector<R>& coarse_p, Level<R>& F) {
     const Dims& t = F.dm;
+    const bool fine = &F == &lv[0];
     for_voxels(t, [&](uint32_t x, uint32_t y, uint32_t z) {
       const size_t i = flat(t, x, y, z);
-      if (x == 0 || y == 0 || z == 0 || x == t.w - 1 || y == t.h - 1 || z == t.d - 1) {
+      if (x == 0 || y == 0 || z == 0 || x == t.w - 1 || y == t.h - 1 || z == t.d - 1 || (fine && outside_u(x, y, z))) {
         F.pa[i] = R(0);
         return;
       }
@@ -1305,7 +1329,7 @@ template <class R> class Sim {
     const uint32_t W1 = dm.w - 1, H1 = dm.h - 1, D1 = dm.d - 1;
     for_voxels(dm, [&](uint32_t x, uint32_t y, uint32_t z) {
       const size_t i = flat(dm, x, y, z);
-      if (is_boundary(dm, x, y, z)) {
+      if (is_boundary(dm, x, y, z) || outside_u(x, y, z)) {
         vc[0][i] = vc[1][i] = vc[2][i] = R(0);
         return;
       }
@@ -1365,6 +1389,8 @@ template <class R> class Sim {
     if (advect_mode == 0) advect_scalars_semilagrangian(cur, next);
     else advect_scalars_maccormack(cur, next);
     active_bricks(next);
+    if (sparse)
+      for (uint32_t b = 0; b < nb; ++b) uset[b] = (flags[cur][b] | flags[next][b]) != 0u ? 1 : 0;
     combustion(next);
     buoyancy_pass(next);
     if (step_index % q.vorticity_interval == 0) {
@@ -1647,6 +1673,16 @@ void orc_get_solver_stats(void* hv, double* out, int* iout) {
     out[3] = s->stats.maxdiv;
     iout[0] = s->stats.cycles;
     iout[1] = s->stats.converged;
+    return 0;
+  });
+}
+
+// Switches sparse mode (see Sim::sparse) on (1) or off (0); it takes effect at
+// the next step. Returns -1 with the V-cycle solver, which has no sparse form.
+int orc_set_sparse(void* hv, int on) {
+  return dispatch(static_cast<Handle*>(hv), [&](auto* s) -> int {
+    if (on && s->sv.mode == 1) return -1;
+    s->sparse = on != 0;
     return 0;
   });
 }

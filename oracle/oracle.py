@@ -42,6 +42,8 @@ def load() -> ctypes.CDLL:
         lib.orc_set_advection_mode.argtypes = [c_void_p, c_int]
         lib.orc_set_emit_dead_residual.argtypes = [c_void_p, c_int]
         lib.orc_set_half_storage.argtypes = [c_void_p, c_int]
+        lib.orc_set_sparse.restype = c_int
+        lib.orc_set_sparse.argtypes = [c_void_p, c_int]
         lib.orc_raymarch.argtypes = [POINTER(c_float)] * 4 + [POINTER(c_uint32), c_uint32, c_uint32, c_uint32, POINTER(c_double), c_int,
                                                              c_uint32, c_uint32, c_double, POINTER(c_double), c_int, POINTER(c_double),
                                                              POINTER(c_float)]
@@ -156,6 +158,12 @@ class OracleSimulation:
                          int(full["coarseSweeps"]), int(full["maxCycles"]), 1 if full["warmStart"] else 0)
         dv = (c_double * 2)(float(full["omega"]), float(full["tolerance"]))
         self._lib.orc_set_solver(self._h, iv, dv, 1 if norms else 0)
+
+    def setSparse(self, on: bool) -> None:
+        """Sparse mode (extension): velocity and the fine pressure computed on the
+        step's active bricks only, zero elsewhere (see Sim::sparse)."""
+        if self._lib.orc_set_sparse(self._h, 1 if on else 0) != 0:
+            raise ValueError("sparse mode has no V-cycle form")
 
     def readSolverStats(self) -> dict:
         out = (c_double * 4)()
