@@ -291,14 +291,14 @@ def cpu_baseline_and_parity(args, wl, counts, kernels, storage):
         "steps": args.cpu_steps, "against": "f64 oracle (same start state and steps)", "fields": err}
 
 
-def time_steps(args, wl, local, kernels, storage, pg, solver=None):
-    """K steps of (kernels, storage[, solver]) on a fresh simulation, device time
-    on its stream (max over ranks), after the warm-up steps."""
+def time_steps(args, wl, local, kernels, storage, pg, solver=None, sparse=False):
+    """K steps of (kernels, storage[, solver][, sparse mode]) on a fresh simulation,
+    device time on its stream (max over ranks), after the warm-up steps."""
     import torch
 
     from fenix_b200 import createCombustionVolumeSimulation, workloads
 
-    sim = createCombustionVolumeSimulation(wl.options, device=local, kernels=kernels, storage=storage)
+    sim = createCombustionVolumeSimulation(wl.options, device=local, kernels=kernels, storage=storage, sparse=sparse)
     sim.updateSources(wl.sources)
     workloads.load_state(sim, wl.state)
     sim.setInstrumentation(count_active=True)
@@ -334,6 +334,8 @@ def time_steps(args, wl, local, kernels, storage, pg, solver=None):
         pg.all_reduce(vv, op=pg.ReduceOp.SUM)
         voxel_steps = int(vv.item())
     out = {"value": voxel_steps / (ms / 1e3), "ms_per_step": ms / args.steps, "kernels": kernels, "storage": storage}
+    if sparse:
+        out["sparse"] = True
     if solver:
         out["solver"] = dict(solver)
         out["last_step_solver_stats"] = solver_stats
@@ -690,6 +692,11 @@ def main():
             r["ratio"] = value / r["value"]
             compare[f"{storage}_{kernels}_vcycle"] = r
         compare["c2_mixed_over_plain_f32"] = compare["f16_fused_vcycle"]["value"] / compare["f32_plain_vcycle"]["value"]
+        # sparse mode (extension): the velocity passes on the active bricks only
+        for storage in ("f16", "f32"):
+            r = time_steps(args, wl, local, "fused", storage, pg, sparse=True)
+            r["ratio"] = value / r["value"]
+            compare[f"{storage}_fused_sparse"] = r
 
     batch_c3 = None if args.no_c3 else run_batch_c3(args, local, rank, world, pg)
     adjoint = None if args.no_adjoint else run_adjoint_c4(args, local, pg)

@@ -1286,6 +1286,7 @@ void fused_work_carve(FusedWork& w, char* base, Dims dm, uint3 bricks, size_t ao
   for (auto& b : w.nz_sp) b = (uint8_t*)take(w.nb);
   for (auto& l : w.list_sp) l = (uint32_t*)take((size_t)w.nb * 4);
   w.counters = (uint32_t*)take(16 * 4);
+  w.dev_err = w.counters + 8;
   w.solver = (SolverDev*)take(sizeof(SolverDev));
   w.vmax = (unsigned*)take(4);
   w.aos = take((size_t)dm.w * dm.h * dm.d * aos_voxel_bytes);
@@ -1857,12 +1858,33 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
         ++launches;
       }
     }
+    // The fine sweeps: TMA-staged where tensor maps of the buffers exist.
+    static const bool use_tma = [] {
+      const char* v = std::getenv("FENIX_SPARSE_TMA");
+      return !(v && *v == '0');
+    }();
+    if (use_tma && (w.tmap_base[0] != F.p[0] || w.tmap_base[1] != F.p[1] || w.tmap_base[2] != F.div)) {
+      w.tmaps_ok = field_tensor_map(&w.tmap_p[0], F.p[0], dm, 16, 10, 10) && field_tensor_map(&w.tmap_p[1], F.p[1], dm, 16, 10, 10) &&
+                   field_tensor_map(&w.tmap_div, F.div, dm, 8, 8, 8);
+      w.tmap_base[0] = F.p[0];
+      w.tmap_base[1] = F.p[1];
+      w.tmap_base[2] = F.div;
+    }
+    auto sweep = [&](const float* src, float* dst, const float* mid_p, const char* name) {
+      Timed tm(w, s, name);
+      if (use_tma && w.tmaps_ok && src) {
+        const CUtensorMap& sm = src == F.p[0] ? w.tmap_p[0] : w.tmap_p[1];
+        k_sp_sweep_tma<<<brick_grid, kBrickThreads, 0, s>>>(sm, w.tmap_div, dm, bc, dst, M.dm, mid_p, pl, pc, w.dev_err, w.tma_wait_ns,
+                                                            w.tma_extra_tx);
+      } else {
+        k_sp_sweep<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, F.div, src, dst, M.dm, mid_p, 0, pl, pc);
+      }
+      ++launches;
+    };
     for (int k = 2; k <= m; ++k) {
       const bool add = prolong_live && k == m;
-      Timed tm(w, s, add ? "sparse_sweep_prolong" : "sparse_sweep");
-      k_sp_sweep<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, F.div, chain, outs[wi], M.dm, add ? M.p[mid] : nullptr, 0, pl, pc);
+      sweep(chain, outs[wi], add ? M.p[mid] : nullptr, add ? "sparse_sweep_prolong" : "sparse_sweep");
       chain = outs[wi++];
-      ++launches;
     }
     if (m == 0) {
       Timed tm(w, s, "sparse_prolong_fine");
@@ -1871,10 +1893,8 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       ++launches;
     }
     for (int k = 1; k <= n; ++k) {
-      Timed tm(w, s, "sparse_sweep");
-      k_sp_sweep<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, F.div, chain, outs[wi], M.dm, nullptr, 0, pl, pc);
+      sweep(chain, outs[wi], nullptr, "sparse_sweep");
       chain = outs[wi++];
-      ++launches;
     }
     {
       Timed tm(w, s, "sparse_project");
@@ -2026,6 +2046,19 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   out.final_vscr_is_2 = st.vort_on;
   out.launches = launches;
   return FX_OK;
+}
+
+fx_status fused_check_device_error(FusedWork& w, cudaStream_t s) {
+  uint32_t h = 0;
+  if (cudaMemcpyAsync(&h, w.dev_err, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess) return FX_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return FX_ERR_CUDA;
+  return h ? FX_ERR_TIMEOUT : FX_OK;
+}
+
+void fused_set_tma_test(FusedWork& w, uint64_t wait_ns, uint32_t extra_tx) {
+  w.tma_wait_ns = wait_ns;
+  w.tma_extra_tx = extra_tx;
+  w.graphs.clear();  // the values are captured in the graphs
 }
 
 fx_status fused_count_active(FusedWork& w, cudaStream_t s, const uint32_t* flags, uint32_t nb, uint32_t* out) {

@@ -7,6 +7,7 @@
 #include <map>
 #include <string>
 #include <vector>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "../../include/fenix_cuda.h"
@@ -55,6 +56,14 @@ struct FusedWork {
   uint8_t* nz_sp[4] = {nullptr, nullptr, nullptr, nullptr};
   uint32_t* list_sp[4] = {nullptr, nullptr, nullptr, nullptr};
   bool sp_known = true;
+  // Tensor maps of the fine pressure buffers (16 x 10 x 10 boxes) and of the fine
+  // divergence (8 x 8 x 8) for the TMA-staged sparse sweep; built on first use.
+  CUtensorMap tmap_p[2]{};
+  CUtensorMap tmap_div{};
+  const float* tmap_base[3] = {nullptr, nullptr, nullptr};
+  bool tmaps_ok = false;
+  // Device error word: bit 0 is set when a bounded wait of a kernel ran out.
+  uint32_t* dev_err = nullptr;
   SolverDev* solver = nullptr;     // FP64 solver statistics and the V-cycle loop state
   unsigned* vmax = nullptr;        // max |v| of the current velocity (float bits; all ones = unknown)
   cudaStream_t aux = nullptr;      // captures the V-cycle body graph
@@ -64,6 +73,8 @@ struct FusedWork {
   std::vector<uint8_t> host_mark;
   std::vector<uint32_t> host_list;
   bool valid = false;  // false: the per-brick bookkeeping must be rebuilt from the fields
+  uint64_t tma_wait_ns = 1000000000ull;  // bound of a TMA tile wait (1 s; a tile takes microseconds)
+  uint32_t tma_extra_tx = 0;
   std::vector<uint32_t> uploaded_list;  // injection list currently on the device
   // CUDA graphs of the device part of the step, keyed by its configuration.
   struct GraphEntry {
@@ -135,6 +146,12 @@ fx_status fused_prepare(FusedWork& w, const FusedStep& st, uint32_t* ninj, Fused
 uint64_t fused_key(const FusedStep& st, uint32_t ninj);
 fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, FusedResult& out);
 fx_status fused_count_active(FusedWork& w, cudaStream_t s, const uint32_t* flags, uint32_t nb, uint32_t* out);
+// FX_ERR_TIMEOUT when a bounded wait of a kernel ran out since the simulation
+// was created (waits for the stream), FX_OK otherwise.
+fx_status fused_check_device_error(FusedWork& w, cudaStream_t s);
+// Test hook: the TMA-staged sweep's wait limit (ns) and the extra bytes its
+// stages expect (0 in normal use; a non-zero value makes every wait run out).
+void fused_set_tma_test(FusedWork& w, uint64_t wait_ns, uint32_t extra_tx);
 
 // Adds the active bricks of `flags` and their voxel count to acc[0] and acc[1].
 cudaError_t fused_accumulate_active(cudaStream_t s, Dims dm, uint3 bricks, const uint32_t* flags, unsigned long long* acc);

@@ -342,3 +342,165 @@ __global__ void __launch_bounds__(256) k_sp_velocity_magnitude(Dims dm, VelField
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     out[i] = length3(__ldg(v.c[0] + i), __ldg(v.c[1] + i), __ldg(v.c[2] + i));
 }
+
+// ------------------------------------------------------------------ TMA staging
+// The sparse fine sweep with each brick's source tile staged in shared memory by
+// the tensor-memory accelerator: one 3-D tile load of 16 x 10 x 10 floats (the
+// brick, its one-voxel halo in y and z, and x from x0 - 4 so the tile starts on
+// a 16-byte boundary) and one of the brick's 8 x 8 x 8 divergence, completing on
+// an mbarrier. A block walks its list entries with two stages: the loads of the
+// next entry are in flight while the current one is computed. Loads outside the
+// grid read 0 (they only reach the halo of boundary voxels, which are not
+// computed). The tensor maps cover this GPU's own buffers; no multicast.
+constexpr int kSpTileFloats = 16 * 10 * 10;
+constexpr int kSpDivFloats = 8 * 8 * 8;
+constexpr uint32_t kSpStageBytes = (kSpTileFloats + kSpDivFloats) * 4;
+
+FX_DEV uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+FX_DEV void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+FX_DEV void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+FX_DEV bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+FX_DEV uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Waits for the phase `parity` of *bar for at most limit_ns; false on timeout.
+FX_DEV bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+  if (mbar_test(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_test(bar, parity))
+    if (global_ns() - t0 > limit_ns) return false;
+  return true;
+}
+
+FX_DEV void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// k_sp_sweep (src given) from TMA-staged tiles; the same operations in the same
+// order, so the same bits. `wait_ns` bounds every wait on a tile: when one runs
+// out the block sets *err, waits (bounded again) for its loads in flight and
+// returns. `extra_tx` adds to the bytes a stage expects and is 0 except in the
+// test of that timeout path, where the stage then never completes.
+__global__ void __launch_bounds__(kBrickThreads) k_sp_sweep_tma(const __grid_constant__ CUtensorMap src_map,
+                                                                const __grid_constant__ CUtensorMap div_map, Dims dm, uint3 bc,
+                                                                float* __restrict__ dst, Dims mid, const float* __restrict__ mid_p,
+                                                                const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
+                                                                uint32_t* __restrict__ err, uint64_t wait_ns, uint32_t extra_tx) {
+  __shared__ __align__(128) float tile[2][kSpTileFloats + kSpDivFloats];
+  __shared__ __align__(8) uint64_t bar[2];
+  const uint32_t n = *count;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // Thread 0 starts the loads of list entry li into `stage` (computed entries only).
+  auto issue = [&](uint32_t li, int stage) {
+    const uint32_t e = list[li];
+    if (!(e & kSpCompute)) return false;
+    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+    mbar_arrive_expect_tx(&bar[stage], kSpStageBytes + extra_tx);
+    tma_load_3d(&tile[stage][0], &src_map, (int)c.x0 - 4, (int)c.y0 - 1, (int)c.z0 - 1, &bar[stage]);
+    tma_load_3d(&tile[stage][kSpTileFloats], &div_map, (int)c.x0, (int)c.y0, (int)c.z0, &bar[stage]);
+    return true;
+  };
+  uint32_t parity = 0u;  // bit k: the phase stage k waits for next
+  int stage = 0;
+  if (threadIdx.x == 0 && blockIdx.x < n) issue(blockIdx.x, 0);
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t nli = li + gridDim.x;
+    bool next_issued = false;
+    if (threadIdx.x == 0 && nli < n) next_issued = issue(nli, stage ^ 1);
+    const uint32_t e = list[li];
+    const bool comp = (e & kSpCompute) != 0u;
+    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+    if (comp) {
+      const uint32_t ph = (parity >> stage) & 1u;
+      const bool ok = mbar_wait_bounded(&bar[stage], ph, wait_ns);
+      if (__syncthreads_or(ok ? 0 : 1)) {
+        // A tile never arrived: record it, let the loads in flight land, leave.
+        if (threadIdx.x == 0) {
+          atomicOr(err, 1u);
+          mbar_wait_bounded(&bar[stage], ph, wait_ns);
+          if (next_issued) mbar_wait_bounded(&bar[stage ^ 1], (parity >> (stage ^ 1)) & 1u, wait_ns);
+        }
+        __syncthreads();
+        return;
+      }
+      parity ^= 1u << stage;
+    }
+    const float* T = tile[stage];
+    const float* Dv = tile[stage] + kSpTileFloats;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const SpVoxel q = sp_voxel(dm, c, j);
+      if (!q.inside) continue;
+      float out = 0.0f;
+      if (comp && !is_boundary(dm, q.x, q.y, q.z)) {
+        const uint32_t lx = q.x - c.x0, ly = q.y - c.y0, lz = q.z - c.z0;
+        const uint32_t t = (lx + 4u) + 16u * ((ly + 1u) + 10u * (lz + 1u));
+        const float s = T[t + 1u] + T[t - 1u] + T[t + 16u] + T[t - 16u] + T[t + 160u] + T[t - 160u];
+        out = div6(s - Dv[lx + 8u * (ly + 8u * lz)]);
+        if (mid_p) out = out + prolong_sample_at(mid, mid_p, (int)q.x, (int)q.y, (int)q.z);
+      }
+      dst[q.i] = out;
+    }
+    __syncthreads();  // the stage is read; the next iteration may reload it
+    stage ^= 1;
+  }
+}
+
+// Host: the tensor-map encoder of the driver (cuTensorMapEncodeTiled), reached
+// through the runtime so the library needs no link to libcuda.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                                   const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+      return (EncodeTiledFn) nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// A 3-D tensor map over a dense float field of dm (x fastest) with a bx x by x bz
+// box; false where the layout does not allow one (widths not divisible by 4).
+bool field_tensor_map(CUtensorMap* m, const float* base, Dims dm, uint32_t bx, uint32_t by, uint32_t bz) {
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc || dm.w % 4u != 0u || (reinterpret_cast<uintptr_t>(base) & 15u) != 0u) return false;
+  const cuuint64_t dims[3] = {dm.w, dm.h, dm.d};
+  const cuuint64_t strides[2] = {(cuuint64_t)dm.w * 4u, (cuuint64_t)dm.w * dm.h * 4u};
+  const cuuint32_t box[3] = {bx, by, bz};
+  const cuuint32_t es[3] = {1u, 1u, 1u};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}

@@ -1036,6 +1036,8 @@ fx_status fx_sim_synchronize(fx_sim* s) {
   if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_synchronize: NULL handle");
   FX_CUDA(s, cudaSetDevice(s->device));
   FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  if (fused_check_device_error(s->fw, s->stream) == FX_ERR_TIMEOUT)
+    return fail(s, FX_ERR_TIMEOUT, "a bounded wait of the sparse sweep ran out; the results of that step are invalid");
   return FX_OK;
 }
 
@@ -1512,6 +1514,17 @@ fx_status fx_test_march_plan(int32_t kind, uint32_t w, uint32_t h, uint32_t d, i
 fx_status fx_test_fail_allocations(int32_t nth) {
   if (nth < 0) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_test_fail_allocations: negative count");
   g_alloc_countdown.store(nth);
+  return FX_OK;
+}
+
+// Test entry (failure detection): the bound (ns) of every wait of the
+// TMA-staged sparse sweep and extra bytes its tile stages expect. With extra > 0
+// no stage ever completes, so each wait runs out after wait_ns, the kernel
+// records it and returns, and the next synchronizing call reports
+// FX_ERR_TIMEOUT. (0, 1e9) restores normal operation.
+fx_status fx_test_sparse_tma_wait(fx_sim* s, uint64_t wait_ns, uint32_t extra_tx) {
+  if (!s || wait_ns == 0) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_test_sparse_tma_wait: invalid argument");
+  fused_set_tma_test(s->fw, wait_ns, extra_tx);
   return FX_OK;
 }
 

@@ -8,11 +8,15 @@ f64, as one JSON object and as markdown tables.
 Legs:
   f16                 fused step, FP16 scalar storage (every stored scalar rounded to binary16)
   f32                 fused step, f32 storage
+  f16_sparse          the same in sparse mode (velocity passes on the active bricks only)
+  f32_sparse
   f32_once_f16        f32 storage, the start state's scalars rounded to binary16 once
   f32_perturbed       f32 storage, the start state's scalars multiplied once by
                       (1 + 2^-12 u), u uniform in [-1, 1] (seeded)
 The last two separate the amplification of one storage-sized perturbation by
-the flow from the rounding that FP16 storage adds at every step.
+the flow from the rounding that FP16 storage adds at every step. Sparse legs are
+compared with the f64 oracle in parity mode (sparse against the reference step)
+and with the f64 oracle in sparse mode (the precision of the sparse step).
 
 --solver vcycle runs every leg and the oracle with the FP64-norm V-cycle
 (5 levels, V(4,4), 20 coarse sweeps, warm start, stop at relative residual
@@ -38,7 +42,7 @@ FIELDS = ("density", "temperature", "fuel", "reaction", "velocity_x", "velocity_
 SCALARS = ("density", "temperature", "fuel", "reaction")
 VCYCLE = {"mode": "vcycle", "levels": 5, "preSweeps": 4, "postSweeps": 4, "coarseSweeps": 20, "maxCycles": 30,
           "warmStart": True, "omega": 2.0 / 3.0, "tolerance": 1e-5}
-LEGS = ("f16", "f32", "f32_once_f16", "f32_perturbed")
+LEGS = ("f16", "f32", "f32_once_f16", "f32_perturbed", "f16_sparse", "f32_sparse")
 
 
 def errors(got: np.ndarray, ref: np.ndarray) -> dict:
@@ -80,26 +84,36 @@ def main() -> int:
 
     orc_mod.set_threads(args.threads)
     wl = workloads.plume_256(size=args.size)
+    if args.solver == "vcycle" and any(l.endswith("_sparse") for l in legs):
+        raise SystemExit("sparse mode has no V-cycle form")
     sims = {}
     for leg in legs:
-        s = createCombustionVolumeSimulation(wl.options, device=0, storage="f16" if leg == "f16" else "f32")
+        s = createCombustionVolumeSimulation(wl.options, device=0, storage="f16" if leg.startswith("f16") else "f32",
+                                             sparse=leg.endswith("_sparse"))
         s.updateSources(wl.sources)
         if args.solver == "vcycle":
             s.setSolver(VCYCLE)
         workloads.load_state(s, leg_state(leg, wl.state))
         sims[leg] = s
-    ref = OracleSimulation(wl.options, precision=64)
-    ref.updateSources(wl.sources)
-    if args.solver == "vcycle":
-        ref.setSolver(VCYCLE, norms=True)
-    workloads.load_state(ref, wl.state)
+    refs_sim = {}
+    for name, sparse in (("f64", False), ("f64_sparse", True)):
+        if sparse and not any(l.endswith("_sparse") for l in legs):
+            continue
+        ref = OracleSimulation(wl.options, precision=64)
+        ref.updateSources(wl.sources)
+        if args.solver == "vcycle":
+            ref.setSolver(VCYCLE, norms=True)
+        ref.setSparse(sparse)
+        workloads.load_state(ref, wl.state)
+        refs_sim[name] = ref
     out = {"workload": f"plume_{args.size}", "solver": VCYCLE if args.solver == "vcycle" else "reference schedule",
            "steps": marks, "dt": wl.dt, "against": "f64 oracle, same start state and steps", "threads": args.threads,
            "legs": legs, "at": {}, "cycles": {}}
     t0 = time.time()
     step = 0
     cycles = {leg: 0 for leg in legs}
-    cycles["f64"] = 0
+    for name in refs_sim:
+        cycles[name] = 0
     for mark in marks:
         while step < mark:
             t = step * wl.dt
@@ -107,14 +121,18 @@ def main() -> int:
                 s.step(t, wl.dt)
                 if args.solver == "vcycle":
                     cycles[leg] += s.readSolverStats()["cycles"]
-            ref.step(t, wl.dt)
-            if args.solver == "vcycle":
-                cycles["f64"] += ref.readSolverStats()["cycles"]
+            for name, ref in refs_sim.items():
+                ref.step(t, wl.dt)
+                if args.solver == "vcycle":
+                    cycles[name] += ref.readSolverStats()["cycles"]
             step += 1
         row = {}
-        refs = {f: ref.readField(f) for f in FIELDS}
+        fields_of = {name: {f: ref.readField(f) for f in FIELDS} for name, ref in refs_sim.items()}
         for leg, s in sims.items():
-            row[leg] = {f: errors(s.readField(f), refs[f]) for f in FIELDS}
+            got = {f: s.readField(f) for f in FIELDS}
+            row[leg] = {f: errors(got[f], fields_of["f64"][f]) for f in FIELDS}
+            if leg.endswith("_sparse"):
+                row[leg + " vs f64_sparse"] = {f: errors(got[f], fields_of["f64_sparse"][f]) for f in FIELDS}
         out["at"][str(mark)] = row
         out["cycles"][str(mark)] = dict(cycles)
         print(f"step {mark} done ({time.time() - t0:.0f} s)", file=sys.stderr, flush=True)

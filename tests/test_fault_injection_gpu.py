@@ -101,3 +101,39 @@ def test_fault_injection_entry_rejects_negative_counts():
     assert lib.fx_test_fail_allocations(-1) == _lib.FX_ERR_INVALID_ARGUMENT
     assert lib.fx_test_fail_allocations(0) == _lib.FX_OK
     assert isinstance(lib.fx_last_error(), (bytes, ctypes.c_char_p, type(None)))
+
+
+@pytest.mark.gpu
+def test_a_tma_wait_that_runs_out_reports_timeout_and_the_context_stays_usable(lib):
+    """The TMA-staged sparse sweep bounds every wait for a tile (globaltimer). With
+    the test hook its stages expect more bytes than the loads deliver, so no wait
+    ever completes: each block records the timeout after 2 ms, lets its loads
+    land and returns; the host reads FX_ERR_TIMEOUT at the next synchronize. The
+    loads themselves complete, so nothing is left in flight."""
+    from oracle.oracle import OracleSimulation
+
+    opts = {"resolution": (64, 48, 40), "worldSize": 1.5}
+    sim = createCombustionVolumeSimulation(opts, device=0, sparse=True)
+    sim.updateSources(all_kind_sources(seed=3.0))
+    for k in range(3):
+        sim.step(k * DT, DT)
+    sim.synchronize()
+    assert lib.fx_test_sparse_tma_wait(sim._h, 2_000_000, 64) == _lib.FX_OK
+    sim.step(3 * DT, DT)
+    assert lib.fx_sim_synchronize(sim._h) == _lib.FX_ERR_TIMEOUT
+    assert b"bounded wait" in lib.fx_sim_last_error(sim._h)
+    assert lib.fx_sim_step(sim._h, 4 * DT, DT) == _lib.FX_ERR_STATE
+    sim.dispose()
+
+    sim = createCombustionVolumeSimulation(opts, device=0, sparse=True)
+    orc = OracleSimulation(opts, precision=32)
+    orc.setSparse(True)
+    for s in (sim, orc):
+        s.updateSources(all_kind_sources(seed=3.0))
+    for k in range(3):
+        sim.step(k * DT, DT)
+        orc.step(k * DT, DT)
+    for name in ("density", "velocity_x", "pressure"):
+        assert_bit_equal(sim.readField(name), orc.readField(name), name)
+    sim.dispose()
+    orc.dispose()
