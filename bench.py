@@ -670,7 +670,7 @@ def main():
             tt = torch.tensor([e2e_s], device="cuda")
             pg.all_reduce(tt, op=pg.ReduceOp.MAX)
             e2e_s = float(tt.item())
-        e2e = {"value": (active_mean * args.steps * world) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(packed.nbytes + 80),
+        e2e = {"value": (active_mean * args.steps * world) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(packed.nbytes + 88),
                "d2h_bytes_per_step": 16, "ms_per_step": e2e_s * 1e3 / args.steps}
 
     sim.dispose()

@@ -30,6 +30,7 @@ FX_OPT_DEBUG_FIELDS = 1 << 0
 FX_OPT_NO_GRAPHS = 1 << 1
 FX_OPT_SCALARS_F16 = 1 << 2
 FX_OPT_SPARSE = 1 << 3
+FX_OPT_F16_ROUND_NEAREST = 1 << 4
 
 FX_DTYPE_F32 = 0
 FX_DTYPE_F16 = 1
@@ -290,6 +291,7 @@ TEST_PROTOTYPES = [
     ("fx_test_march_plan", c_int32, [c_int32, c_uint32, c_uint32, c_uint32, c_int32, POINTER(c_int32)]),
     ("fx_test_fail_allocations", c_int32, [c_int32]),
     ("fx_test_sparse_tma_wait", c_int32, [c_void_p, c_uint64, c_uint32]),
+    ("fx_test_sr_half", c_int32, [POINTER(c_float), POINTER(c_float), c_uint32, c_uint32, c_uint32]),
     ("fx_test_pinned_exp_pow", c_int32, [POINTER(c_float), POINTER(c_float), POINTER(c_float), POINTER(c_float), c_uint32]),
 ]
 

@@ -38,7 +38,7 @@ constexpr int kBrickThreads = 256;
 // ------------------------------------------------------------- scalar storage
 // The scalar sets (density, temperature, fuel, reaction) are stored as float or,
 // with FP16 storage, as binary16. The kernels compute in f32 either way. Each
-// value the reference stores into one of those buffers goes through qS first
+// value the reference stores into one of those buffers goes through qS_at first
 // (round to the storage type and back), so everything read afterwards (the
 // brick summaries, the non-zero bits, later fields) sees the stored value.
 template <typename S>
@@ -60,15 +60,18 @@ FX_DEV float rdS(const __half* p, uint32_t i) { return __half2float(p[i]); }
 FX_DEV void stS(float* p, uint32_t i, float v) { p[i] = v; }
 FX_DEV void stS(__half* p, uint32_t i, float v) { p[i] = __float2half_rn(v); }
 
+// The value a pass stores for voxel i at store site `site` (numbered as the
+// oracle's Sim::qs_at): itself in f32 storage; in binary16 storage rounded to
+// nearest, or stochastically (sr_half) when the step's uniform asks for it.
 template <typename S>
-FX_DEV float qS(float v);
+FX_DEV float qS_at(float v, const Params& P, uint32_t i, uint32_t site);
 template <>
-FX_DEV float qS<float>(float v) {
+FX_DEV float qS_at<float>(float v, const Params&, uint32_t, uint32_t) {
   return v;
 }
 template <>
-FX_DEV float qS<__half>(float v) {
-  return __half2float(__float2half_rn(v));
+FX_DEV float qS_at<__half>(float v, const Params& P, uint32_t i, uint32_t site) {
+  return P.half_round ? sr_half(v, sr_draw(i, site, P.step_index)) : __half2float(__float2half_rn(v));
 }
 
 // tri_interp (sampling-scalar.wgsl.ts:11-34) over a stored scalar field.
@@ -292,9 +295,9 @@ __global__ void __launch_bounds__(kBrickThreads) k_inject(Dims dm, uint3 bc, con
         r = rdS(set.f[3], i);
         inject_scalar_voxel(P, src, nsrc, px, py, pz, d, t, f);
         // inject-scalar stores d, T, f here; inject-igniter reads them back
-        d = qS<S>(d);
-        t = qS<S>(t);
-        f = qS<S>(f);
+        d = qS_at<S>(d, P, i, 0);
+        t = qS_at<S>(t, P, i, 1);
+        f = qS_at<S>(f, P, i, 2);
         float vx = v.c[0][i], vy = v.c[1][i], vz = v.c[2][i];
         inject_velocity_voxel(P, src, nsrc, px, py, pz, vx, vy, vz);
         const float lim = speed_limit(P);
@@ -302,8 +305,8 @@ __global__ void __launch_bounds__(kBrickThreads) k_inject(Dims dm, uint3 bc, con
         v.c[1][i] = clampv(vy, -lim, lim);
         v.c[2][i] = clampv(vz, -lim, lim);
         inject_igniter_voxel(P, src, nsrc, px, py, pz, f, r, t);
-        r = qS<S>(r);
-        t = qS<S>(t);
+        r = qS_at<S>(r, P, i, 3);
+        t = qS_at<S>(t, P, i, 4);
         stS(set.f[0], i, d);
         stS(set.f[1], i, t);
         stS(set.f[2], i, f);
@@ -671,8 +674,9 @@ __global__ void __launch_bounds__(kBrickThreads) k_advect_scalars(Dims dm, uint3
           noise = thermal_noise(P, spx, spy, spz);
         }
         decay_scalars(P, ny, noise, out[0], out[1], out[2], out[3]);
+        const uint32_t iv = flat(dm, x, y, z);
 #pragma unroll
-        for (int f = 0; f < 4; ++f) out[f] = qS<S>(out[f]);
+        for (int f = 0; f < 4; ++f) out[f] = qS_at<S>(out[f], P, iv, 5u + (uint32_t)f);
         any = any || out[0] != 0.f || out[1] != 0.f || out[2] != 0.f || out[3] != 0.f;
       }
       if (inside) {
@@ -738,10 +742,10 @@ __global__ void __launch_bounds__(kBrickThreads) k_combustion(Dims dm, uint3 bc,
         const Nbr n = neighbours(dm, x, y, z, i);
         const float nsum = hot(n.xp) + hot(n.xm) + hot(n.yp) + hot(n.ym) + hot(n.zp) + hot(n.zm);
         combustion_voxel_c(P, thermal_cluster_ys(P, (float)x, (float)y, (float)z, ysin), ny, nsum, d, t, f, r);
-        d = qS<S>(d);
-        t = qS<S>(t);
-        f = qS<S>(f);
-        r = qS<S>(r);
+        d = qS_at<S>(d, P, i, 11);
+        t = qS_at<S>(t, P, i, 10);
+        f = qS_at<S>(f, P, i, 9);
+        r = qS_at<S>(r, P, i, 12);
         energy_vote(c, x, y, z, true, d, t, r, e);
       }
       stS(dst.f[0], i, d);

@@ -62,6 +62,9 @@ int device_sm_count();
 cudaError_t device_alloc(void** ptr, size_t bytes);
 cudaError_t host_alloc(void** ptr, size_t bytes);
 
+// Stochastic binary16 rounding over an array: out[i] = sr_half(x[i], sr_draw(i, site, step)).
+cudaError_t sr_half_array(const float* x, float* out, uint32_t n, uint32_t site, uint32_t step);
+
 // Pinned sin/cos over an array (tests compare it with the oracle bit for bit).
 void pinned_sincos_array(cudaStream_t s, const float* x, float* out, uint32_t n, int cosine);
 

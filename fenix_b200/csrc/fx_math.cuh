@@ -10,6 +10,8 @@
 
 #include <cstdint>
 
+#include <cuda_fp16.h>
+
 #define FX_DEV __device__ __forceinline__
 
 namespace fx {
@@ -133,14 +135,54 @@ FX_DEV bool is_boundary(const Dims& dm, uint32_t x, uint32_t y, uint32_t z) {
   return x == 0u || y == 0u || z == 0u || x == dm.w - 1u || y == dm.h - 1u || z == dm.d - 1u;
 }
 
-// The 80-byte uniform of shaders/common/simulation-params.wgsl.ts:2-14.
+// The 80-byte uniform of shaders/common/simulation-params.wgsl.ts:2-14, then two
+// words of this build: the step index and the rounding of binary16 scalar stores
+// (0 to nearest, 1 stochastic; see sr_half).
 struct Params {
   float time, dt, prev_time, scalar_set;
   float wind[4];
   float gravity[4];
   float buoyancy, vorticity_strength, dx, world_size;
   float vmask[4];
+  uint32_t step_index;
+  uint32_t half_round;
 };
+
+// Stochastic rounding to binary16 (an extension for FP16 scalar storage).
+// sr_draw is a 32-bit hash of a voxel index and a store site plus the step index
+// times 0x9E3779B9 (2^32 / golden ratio: a rank-1 sequence in time); sr_half
+// rounds a finite |v| < 65504 to the binary16 value below it (toward zero) or
+// the next one up, up when the distance from the lower one, in units of their
+// spacing, exceeds the top 24 bits of r read as a fraction. Every operation is
+// exact. A value that changes by less than half a binary16 spacing per step moves
+// by the right amount on average instead of staying put, which is the bias of
+// round-to-nearest on slowly decaying smoke. Other values round to nearest.
+FX_DEV uint32_t sr_draw(uint32_t i, uint32_t site, uint32_t step) {
+  uint32_t h = i * 0x9E3779B1u + site * 0x85EBCA77u;
+  h ^= h >> 16;
+  h *= 0x7FEB352Du;
+  h ^= h >> 15;
+  h *= 0x846CA68Bu;
+  h ^= h >> 16;
+  return h + step * 0x9E3779B9u;
+}
+
+FX_DEV float sr_half(float v, uint32_t r) {
+  const float a = fabsf(v);
+  if (!(a < 65504.0f)) return __half2float(__float2half_rn(v));
+  float lo, ulp;
+  if (a >= 0x1p-14f) {
+    const uint32_t b = __float_as_uint(a);
+    lo = __uint_as_float(b & ~0x1FFFu);
+    ulp = __uint_as_float((((b >> 23) & 0xFFu) - 10u) << 23);
+  } else {
+    lo = truncf(a * 0x1p24f) * 0x1p-24f;
+    ulp = 0x1p-24f;
+  }
+  const float frac = (a - lo) / ulp;
+  const float u = (float)(r >> 8) * 0x1p-24f;
+  return copysignf(frac > u ? lo + ulp : lo, v);
+}
 
 // Trilinear sampler of shaders/common/sampling-scalar.wgsl.ts:11-34. A NaN
 // position is sent to 0, like the oracle.

@@ -347,6 +347,11 @@ __global__ void k_velocity_magnitude(Dims dm, VelField v, float* __restrict__ ou
   out[i] = length3(v.c[0][i], v.c[1][i], v.c[2][i]);
 }
 
+__global__ void k_sr_half(const float* __restrict__ x, float* __restrict__ out, uint32_t n, uint32_t site, uint32_t step) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = sr_half(x[i], sr_draw(i, site, step));
+}
+
 __global__ void k_pinned_sincos(const float* __restrict__ x, float* __restrict__ out, uint32_t n, int cosine) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = cosine ? pcos(x[i]) : psin(x[i]);
@@ -406,6 +411,12 @@ void plain_velocity_magnitude(cudaStream_t s, Dims dm, VelField v, float* out) {
 void pinned_sincos_array(cudaStream_t s, const float* x, float* out, uint32_t n, int cosine) {
   if (n == 0) return;
   k_pinned_sincos<<<(n + 255) / 256, 256, 0, s>>>(x, out, n, cosine);
+}
+
+cudaError_t sr_half_array(const float* x, float* out, uint32_t n, uint32_t site, uint32_t step) {
+  if (n == 0) return cudaSuccess;
+  k_sr_half<<<(n + 255) / 256, 256>>>(x, out, n, site, step);
+  return cudaGetLastError();
 }
 
 }  // namespace fx

@@ -98,6 +98,7 @@ struct fx_sim {
   uint32_t opt_flags = 0;
   bool half = false;  // FX_OPT_SCALARS_F16: the scalar sets are binary16 buffers
   bool sparse = false;  // FX_OPT_SPARSE / fx_sim_set_sparse
+  bool half_nearest = false;  // FX_OPT_F16_ROUND_NEAREST
   fx_solver_settings solver{};
   uint32_t last_cycle_launches = 0;  // kernels per V-cycle in the latest step
   int sweep_variant[3] = {-1, -1, -1};  // sweep kernel per pressure level, chosen by fx_sim_autotune
@@ -331,6 +332,8 @@ Params make_params(const fx_sim* s, double elapsed, double step_s) {
   P.vmask[1] = (float)s->rp.vorticity_velocity_mask;
   P.vmask[2] = (float)s->rp.vorticity_heat_mask;
   P.vmask[3] = (float)s->rp.vorticity_density_mask;
+  P.step_index = (uint32_t)s->step_index;
+  P.half_round = (s->half && !s->half_nearest) ? 1u : 0u;
   return P;
 }
 
@@ -711,6 +714,7 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
   s->opt_flags = opt.flags;
   s->half = (opt.flags & FX_OPT_SCALARS_F16) != 0;
   s->sparse = (opt.flags & FX_OPT_SPARSE) != 0;
+  s->half_nearest = (opt.flags & FX_OPT_F16_ROUND_NEAREST) != 0;
   s->dm = Dims{w, h, d};
   s->n = w * h * d;
   s->bricks = make_uint3((w + 7) / 8, (h + 7) / 8, (d + 7) / 8);
@@ -1526,6 +1530,19 @@ fx_status fx_test_sparse_tma_wait(fx_sim* s, uint64_t wait_ns, uint32_t extra_tx
   if (!s || wait_ns == 0) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_test_sparse_tma_wait: invalid argument");
   fused_set_tma_test(s->fw, wait_ns, extra_tx);
   return FX_OK;
+}
+
+// Test entry: sr_half(x[i], sr_draw(i, site, step)) on the device for host arrays
+// (compared with the oracle's stochastic binary16 rounding bit for bit).
+fx_status fx_test_sr_half(const float* host_x, float* host_out, uint32_t n, uint32_t site, uint32_t step) {
+  if (!host_x || !host_out) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_test_sr_half: NULL argument");
+  float* d = nullptr;
+  if (cudaMalloc(&d, (size_t)n * 2 * sizeof(float)) != cudaSuccess) return FX_ERR_OUT_OF_MEMORY;
+  cudaError_t e = cudaMemcpy(d, host_x, (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = sr_half_array(d, d + n, n, site, step);
+  if (e == cudaSuccess) e = cudaMemcpy(host_out, d + n, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return e == cudaSuccess ? FX_OK : FX_ERR_CUDA;
 }
 
 fx_status fx_test_div6_exhaustive(unsigned long long* bad) {

@@ -388,7 +388,9 @@ class CombustionVolumeSimulation:
             pass
 
 
-STORAGE = {"f32": 0, "f16": _lib.FX_OPT_SCALARS_F16}
+# Scalar storage: f32; binary16 with stochastic rounding of the stores ("f16");
+# binary16 rounded to nearest ("f16-nearest").
+STORAGE = {"f32": 0, "f16": _lib.FX_OPT_SCALARS_F16, "f16-nearest": _lib.FX_OPT_SCALARS_F16 | _lib.FX_OPT_F16_ROUND_NEAREST}
 
 # Pressure solver settings (extension): "reference" is PressureSolvePass's fixed
 # schedule, "vcycle" the weighted-Jacobi V-cycle with an FP64 stopping test.

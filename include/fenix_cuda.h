@@ -115,6 +115,14 @@ typedef struct fx_runtime_params {
  * and writes still exchange f32 (writes are rounded), and the render buffers
  * report FX_DTYPE_F16. */
 #define FX_OPT_SCALARS_F16 (1u << 2)
+/* With FX_OPT_SCALARS_F16: round every binary16 scalar store to nearest (ties to
+ * even). Without it the stores round stochastically: to one of the two
+ * neighbouring binary16 values, up with probability equal to the distance from
+ * the lower one in units of their spacing, by a hash of the voxel, the store
+ * site and the step index. Round-to-nearest holds a value still when a step
+ * changes it by less than half a binary16 spacing (slow smoke decay), a bias
+ * that stochastic rounding removes. */
+#define FX_OPT_F16_ROUND_NEAREST (1u << 4)
 /* Sparse mode (extension; fused kernels and the reference pressure schedule
  * only). The reference computes velocity advection, curl, confinement,
  * divergence, the fine pressure sweeps and the projection over the whole grid

@@ -334,6 +334,42 @@ struct SolverStats {
   int cycles = 0, converged = 0;
 };
 
+// Stochastic rounding to binary16 (extension). sr_draw is a 32-bit hash of a
+// voxel index and a store site plus the step index times 0x9E3779B9 (2^32 /
+// golden ratio); sr_half rounds a finite |v| < 65504 to the binary16 value below
+// it (toward zero) or the next one up, up when the distance from the lower one,
+// in units of their spacing, exceeds the top 24 bits of r read as a fraction.
+// Every operation is exact, so the CUDA kernels reproduce it bit for bit. Other
+// values round to nearest.
+inline uint32_t sr_draw(uint32_t i, uint32_t site, uint32_t step) {
+  uint32_t h = i * 0x9E3779B1u + site * 0x85EBCA77u;
+  h ^= h >> 16;
+  h *= 0x7FEB352Du;
+  h ^= h >> 15;
+  h *= 0x846CA68Bu;
+  h ^= h >> 16;
+  return h + step * 0x9E3779B9u;
+}
+
+inline float sr_half(float v, uint32_t r) {
+  const float a = std::fabs(v);
+  if (!(a < 65504.0f)) return (float)(_Float16)v;
+  float lo, ulp;
+  if (a >= 0x1p-14f) {
+    uint32_t b;
+    std::memcpy(&b, &a, 4);
+    const uint32_t lb = b & ~0x1FFFu, ub = (((b >> 23) & 0xFFu) - 10u) << 23;
+    std::memcpy(&lo, &lb, 4);
+    std::memcpy(&ulp, &ub, 4);
+  } else {
+    lo = std::trunc(a * 0x1p24f) * 0x1p-24f;
+    ulp = 0x1p-24f;
+  }
+  const float frac = (a - lo) / ulp;
+  const float u = (float)(r >> 8) * 0x1p-24f;
+  return std::copysign(frac > u ? lo + ulp : lo, v);
+}
+
 template <class R> class Sim {
  public:
   Dims dm;
@@ -378,6 +414,23 @@ template <class R> class Sim {
   R qs(R v) const {
     if constexpr (is_tan<R>::value) return v;
     else return half_storage ? (R)(_Float16)v : v;
+  }
+  // Stochastic rounding of the binary16 stores (extension; orc_set_half_rounding):
+  // a pass's store of voxel i rounds to one of the two neighbouring binary16
+  // values, up with probability equal to the distance from the lower one in
+  // units of their spacing. The draw is the voxel's and store site's hash plus
+  // the step index times 2^32 / golden ratio (a rank-1 sequence in time): a value
+  // that changes by less than half a binary16 spacing per step then moves by the
+  // right amount on average over a few steps, where round-to-nearest would hold
+  // it still every step.
+  bool half_sr = false;
+  R qs_at(R v, size_t i, uint32_t site) const {
+    if constexpr (is_tan<R>::value) return v;
+    else {
+      if (!half_storage) return v;
+      if (!half_sr) return (R)(_Float16)v;
+      return (R)sr_half((float)v, sr_draw((uint32_t)i, site, (uint32_t)step_index));
+    }
   }
   // Extension with no reference counterpart: a patch of per-voxel inflow
   // velocity. After inject-velocity, velocity.y at (x0 + i, y, z0 + k) is set to
@@ -593,9 +646,9 @@ template <class R> class Sim {
         tt = clamp01(tt + s.yt * contribution);
         ff = clamp01(ff + s.yf * contribution);
       }
-      D[i] = qs(dd);
-      T[i] = qs(tt);
-      Fu[i] = qs(ff);
+      D[i] = qs_at(dd, i, 0);
+      T[i] = qs_at(tt, i, 1);
+      Fu[i] = qs_at(ff, i, 2);
     });
   }
 
@@ -692,8 +745,8 @@ template <class R> class Sim {
         rr = clamp01(rr + seed);
         tt = clamp01(tt + intensity * weight * R(P.dt) * K(4.0));
       }
-      Re[i] = qs(rr);
-      T[i] = qs(tt);
+      Re[i] = qs_at(rr, i, 3);
+      T[i] = qs_at(tt, i, 4);
     });
   }
 
@@ -799,10 +852,10 @@ template <class R> class Sim {
     const R cold_breakup = dt * density * (R(1) - smoothstepv(K(0.2), K(0.86), hot)) * smoothstepv(K(0.18), K(0.72), density) *
                            smoothstepv(K(0.34), K(0.92), noise) * K(0.34);
     const R clearing = dt * density * hot * mixv(K(0.1), K(0.72), noise);
-    sc[dst][0][i] = qs(clamp01(mx(R(0), density * (R(1) - smoke_loss) - clearing - cold_breakup)));
-    sc[dst][1][i] = qs(clamp01(mx(R(0), temperature - cooling)));
-    sc[dst][2][i] = qs(clamp01(mx(R(0), fuel - dt * mixv(K(0.012), K(0.034), noise))));
-    sc[dst][3][i] = qs(clamp01(mx(R(0), reaction - dt * mixv(K(0.46), K(0.82), noise))));
+    sc[dst][0][i] = qs_at(clamp01(mx(R(0), density * (R(1) - smoke_loss) - clearing - cold_breakup)), i, 5);
+    sc[dst][1][i] = qs_at(clamp01(mx(R(0), temperature - cooling)), i, 6);
+    sc[dst][2][i] = qs_at(clamp01(mx(R(0), fuel - dt * mixv(K(0.012), K(0.034), noise))), i, 7);
+    sc[dst][3][i] = qs_at(clamp01(mx(R(0), reaction - dt * mixv(K(0.46), K(0.82), noise))), i, 8);
   }
 
   // shaders/passes/advect-scalar-maccormack.wgsl.ts:33-101 (set src -> set dst,
@@ -908,10 +961,10 @@ template <class R> class Sim {
       const R clearing = d * smoothstepv(K(0.18), K(0.82), t + r * K(0.22) + f * K(0.1)) * dt * mixv(K(0.55), K(2.45), hot_pocket);
       const R cooling_smoke = d * t * (cooling_pocket + hot_soot * K(0.32)) * dt * K(0.16);
       const R reaction_decay = r * (R(1) - dt * mixv(K(0.68), K(0.22), hot_pocket));
-      sc[set][2][i] = qs(clamp01(f - burn));
-      sc[set][1][i] = qs(clamp01(t + burn * mixv(K(2.1), K(3.25), hot_pocket) + radiative - heat_loss));
-      sc[set][0][i] = qs(clamp01(mx(R(0), d + smoke_yield + cooling_smoke - density_loss - clearing * K(0.72))));
-      sc[set][3][i] = qs(clamp01(mx(reaction_decay, burn * mixv(K(4.0), K(7.5), hot_pocket) + radiative * K(1.8))));
+      sc[set][2][i] = qs_at(clamp01(f - burn), i, 9);
+      sc[set][1][i] = qs_at(clamp01(t + burn * mixv(K(2.1), K(3.25), hot_pocket) + radiative - heat_loss), i, 10);
+      sc[set][0][i] = qs_at(clamp01(mx(R(0), d + smoke_yield + cooling_smoke - density_loss - clearing * K(0.72))), i, 11);
+      sc[set][3][i] = qs_at(clamp01(mx(reaction_decay, burn * mixv(K(4.0), K(7.5), hot_pocket) + radiative * K(1.8))), i, 12);
     });
   }
 
@@ -1683,6 +1736,20 @@ int orc_set_sparse(void* hv, int on) {
   return dispatch(static_cast<Handle*>(hv), [&](auto* s) -> int {
     if (on && s->sv.mode == 1) return -1;
     s->sparse = on != 0;
+    return 0;
+  });
+}
+
+// sr_half(x[i], sr_draw(i, site, step)) for i < n (tests compare it with the CUDA one).
+void orc_sr_half_array(const float* x, float* out, long n, uint32_t site, uint32_t step) {
+  for (long i = 0; i < n; ++i) out[i] = sr_half(x[i], sr_draw((uint32_t)i, site, step));
+}
+
+// Rounding of the binary16 stores: 0 to nearest (ties to even), 1 stochastic
+// (see Sim::qs_at).
+void orc_set_half_rounding(void* hv, int mode) {
+  dispatch(static_cast<Handle*>(hv), [&](auto* s) {
+    s->half_sr = mode == 1;
     return 0;
   });
 }

@@ -42,6 +42,8 @@ def load() -> ctypes.CDLL:
         lib.orc_set_advection_mode.argtypes = [c_void_p, c_int]
         lib.orc_set_emit_dead_residual.argtypes = [c_void_p, c_int]
         lib.orc_set_half_storage.argtypes = [c_void_p, c_int]
+        lib.orc_set_half_rounding.argtypes = [c_void_p, c_int]
+        lib.orc_sr_half_array.argtypes = [POINTER(c_float), POINTER(c_float), c_long, c_uint32, c_uint32]
         lib.orc_set_sparse.restype = c_int
         lib.orc_set_sparse.argtypes = [c_void_p, c_int]
         lib.orc_raymarch.argtypes = [POINTER(c_float)] * 4 + [POINTER(c_uint32), c_uint32, c_uint32, c_uint32, POINTER(c_double), c_int,
@@ -121,7 +123,8 @@ class OracleSimulation:
     (precision=66).
 
     storage="f16" stores the scalar sets in binary16: every value a pass writes to
-    density, temperature, fuel or reaction is rounded to the nearest binary16."""
+    density, temperature, fuel or reaction is rounded to binary16, stochastically
+    (Sim::qs_at), or to nearest with storage="f16-nearest"."""
 
     def __init__(self, options: Optional[Mapping[str, Any]] = None, precision: int = 32, storage: str = "f32"):
         self._lib = load()
@@ -132,10 +135,11 @@ class OracleSimulation:
         self._h = self._lib.orc_create(precision, w, h, d)
         if not self._h:
             raise ValueError("orc_create rejected the arguments")
-        if storage not in ("f32", "f16"):
+        if storage not in ("f32", "f16", "f16-nearest"):
             raise ValueError(f"unknown storage {storage!r}")
         self.storage = storage
-        self._lib.orc_set_half_storage(self._h, 1 if storage == "f16" else 0)
+        self._lib.orc_set_half_storage(self._h, 0 if storage == "f32" else 1)
+        self._lib.orc_set_half_rounding(self._h, 1 if storage == "f16" else 0)
         self._runtime = dict(DEFAULT_RUNTIME)
         mode = options.pop("scalarAdvectionMode", None)
         self._mode = "maccormack"
@@ -158,6 +162,19 @@ class OracleSimulation:
                          int(full["coarseSweeps"]), int(full["maxCycles"]), 1 if full["warmStart"] else 0)
         dv = (c_double * 2)(float(full["omega"]), float(full["tolerance"]))
         self._lib.orc_set_solver(self._h, iv, dv, 1 if norms else 0)
+
+    @staticmethod
+    def srHalfArray(values: np.ndarray, site: int, step: int) -> np.ndarray:
+        """The stochastic binary16 rounding of values[i] as a store of voxel i at
+        store site `site` in step `step` (float32 in and out)."""
+        x = np.ascontiguousarray(values, dtype=np.float32).ravel()
+        out = np.empty_like(x)
+        load().orc_sr_half_array(x.ctypes.data_as(POINTER(c_float)), out.ctypes.data_as(POINTER(c_float)), x.size, site, step)
+        return out
+
+    def setHalfRounding(self, mode: str) -> None:
+        """Rounding of the binary16 scalar stores: "nearest" or "stochastic"."""
+        self._lib.orc_set_half_rounding(self._h, {"nearest": 0, "stochastic": 1}[mode])
 
     def setSparse(self, on: bool) -> None:
         """Sparse mode (extension): velocity and the fine pressure computed on the

@@ -2,7 +2,8 @@
 with binary16 storage, bit for bit.
 
 Both round every value a reference pass stores into density, temperature, fuel
-or reaction to the nearest binary16 (ties to even) and compute in f32, so the
+or reaction to binary16, stochastically by the same hash of voxel, store site and
+step (the default), or to nearest (ties to even), and compute in f32, so the
 results are identical. The error of FP16 storage against the f64 oracle is
 checked in test_precision.py.
 """
@@ -19,15 +20,17 @@ pytestmark = pytest.mark.gpu
 DT = 1.0 / 60.0
 
 
-def make_pair(options, debug=False):
-    sim = createCombustionVolumeSimulation(options, device=0, kernels="fused", debug_fields=debug, storage="f16")
-    orc = OracleSimulation(options, precision=32, storage="f16")
+def make_pair(options, debug=False, storage="f16"):
+    sim = createCombustionVolumeSimulation(options, device=0, kernels="fused", debug_fields=debug, storage=storage)
+    orc = OracleSimulation(options, precision=32, storage=storage)
     return sim, orc
 
 
-def test_f16_all_emitter_kinds_ragged_grid():
+@pytest.mark.parametrize("storage", ["f16", "f16-nearest"])
+def test_f16_all_emitter_kinds_ragged_grid(storage):
+    """Both roundings of the binary16 stores: stochastic (the default) and to nearest."""
     opts = {"resolution": (17, 33, 9), "worldSize": 1.3}
-    sim, orc = make_pair(opts, debug=True)
+    sim, orc = make_pair(opts, debug=True, storage=storage)
     for s in (sim, orc):
         s.updateSources(all_kind_sources())
     run_lockstep(sim, orc, 10, DT, EXPOSED_FIELDS + DEBUG_FIELDS, "f16 ragged")
@@ -83,3 +86,28 @@ def test_f16_plume_256_full_size():
         s.updateSources(wl.sources)
         workloads.load_state(s, wl.state)
     run_lockstep(sim, orc, 2, wl.dt, EXPOSED_FIELDS, "f16 plume256")
+
+
+def test_stochastic_rounding_function_matches_the_oracle():
+    """sr_half on the device against the oracle's, bit for bit: random values over
+    the binary16 normal and subnormal ranges, both signs, the grid itself, 0."""
+    import ctypes
+
+    from fenix_b200 import _lib
+
+    rng = np.random.default_rng(12)
+    x = np.concatenate([
+        rng.random(40000, dtype=np.float32),
+        (rng.random(20000) * 2.0**-14).astype(np.float32),  # binary16 subnormal range
+        -rng.random(5000, dtype=np.float32),
+        np.float32([0.0, -0.0, 1.0, 2.0**-24, 0.5, 65503.0, 70000.0]),
+        rng.random(1000, dtype=np.float32).astype(np.float16).astype(np.float32),
+    ]).astype(np.float32)
+    lib = _lib.load()
+    for site, step in ((0, 0), (7, 123), (12, 4000000)):
+        got = np.empty_like(x)
+        st = lib.fx_test_sr_half(x.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), got.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                 x.size, site, step)
+        assert st == _lib.FX_OK
+        want = OracleSimulation.srHalfArray(x, site, step)
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))

@@ -26,7 +26,7 @@ def test_oracle_half_storage_rounds_to_nearest_even():
     flat[:4] = np.float32([6.1e-5, 3e-8, 2.98e-8, 1.0 - 2.0**-12])  # subnormal half, ties, near-one
     # exact ties between two binary16 neighbours: 1 + (2k+1) * 2^-11
     flat[4:8] = np.float32(1.0) + np.float32(2.0**-11) * np.float32([1, 3, 5, 7])
-    orc = OracleSimulation({"resolution": (10, 9, 8)}, precision=32, storage="f16")
+    orc = OracleSimulation({"resolution": (10, 9, 8)}, precision=32, storage="f16-nearest")
     for name in SCALARS:
         orc.writeField(name, vals)
         got = orc.readField(name)
@@ -36,10 +36,27 @@ def test_oracle_half_storage_rounds_to_nearest_even():
     np.testing.assert_array_equal(orc.readField("velocity_x"), vals.ravel())
 
 
+def test_stochastic_rounding_is_unbiased_and_exact():
+    """sr_half (oracle): the result is one of the two binary16 neighbours of the
+    value, and over many draws the mean equals the value; round-to-nearest would
+    return the lower neighbour every time for these values."""
+    n = 20000
+    v = np.float32(0.7001)  # between binary16 neighbours, 0.0001 above the lower in units of 4.9e-4 -> p(up) ~ 0.2
+    lo = np.float32(np.float16(v)) if np.float32(np.float16(v)) <= v else np.float32(np.nextafter(np.float16(v), np.float16(0)))
+    hi = np.float32(np.nextafter(np.float16(lo), np.float16(1)))
+    assert lo < v < hi
+    got = OracleSimulation.srHalfArray(np.full(n, v, np.float32), site=5, step=0)
+    assert set(np.unique(got)) <= {lo, hi}
+    assert abs(float(got.astype(np.float64).mean()) - float(v)) < 4 * float(hi - lo) * 0.5 / np.sqrt(n)
+    # values on the binary16 grid stay; so do 0, and the sign is kept
+    grid = np.float32([0.0, -0.0, 1.0, 0.5, 2.0**-24, -(2.0**-20), 0.69970703125])
+    np.testing.assert_array_equal(OracleSimulation.srHalfArray(grid, site=1, step=3).view(np.uint32), grid.view(np.uint32))
+
+
 def test_storage_error_against_f64_plume64():
     wl = workloads.plume_64()
     sims = {}
-    for tag, prec, storage in (("f64", 64, "f32"), ("f32", 32, "f32"), ("f16", 32, "f16")):
+    for tag, prec, storage in (("f64", 64, "f32"), ("f32", 32, "f32"), ("f16", 32, "f16"), ("f16n", 32, "f16-nearest")):
         o = OracleSimulation(wl.options, precision=prec, storage=storage)
         o.updateSources(wl.sources)
         workloads.load_state(o, wl.state)
@@ -48,13 +65,18 @@ def test_storage_error_against_f64_plume64():
         for o in sims.values():
             o.step(k * wl.dt, wl.dt)
     ref = {n: sims["f64"].readField(n) for n in SCALARS}
-    err = {tag: {n: rel_l2(sims[tag].readField(n), ref[n]) for n in SCALARS} for tag in ("f32", "f16")}
+    err = {tag: {n: rel_l2(sims[tag].readField(n), ref[n]) for n in SCALARS} for tag in ("f32", "f16", "f16n")}
     # every stored scalar is a binary16 value
-    for n in SCALARS:
-        v = sims["f16"].readField(n)
-        assert np.array_equal(v.astype(np.float16).astype(np.float32), v), n
+    for tag in ("f16", "f16n"):
+        for n in SCALARS:
+            v = sims[tag].readField(n)
+            assert np.array_equal(v.astype(np.float16).astype(np.float32), v), (tag, n)
     # tolerances: f32 arithmetic 1e-5 relative L2; binary16 storage 1e-3 for density
-    # (the stated bar) and 3e-3 for the other scalars
+    # (the stated bar) and 3e-3 for the other scalars, with either rounding here;
+    # stochastic rounding has the smaller density error (round-to-nearest stalls
+    # the slow decay of smoke)
     assert max(err["f32"].values()) < 1e-5, err
-    assert err["f16"]["density"] < 1e-3, err
-    assert max(err["f16"].values()) < 3e-3, err
+    for tag in ("f16", "f16n"):
+        assert err[tag]["density"] < 1e-3, err
+        assert max(err[tag].values()) < 3e-3, err
+    assert err["f16"]["density"] < err["f16n"]["density"], err
