@@ -236,10 +236,10 @@ PARITY_FIELDS = ("density", "temperature", "fuel", "reaction", "velocity_x", "ve
 ERROR_FIELDS = ("density", "temperature", "fuel", "reaction", "velocity_x", "velocity_y", "velocity_z")
 
 
-def cpu_baseline_and_parity(args, wl, counts, kernels, storage):
+def cpu_baseline_and_parity(args, wl, counts, kernels, storage, sparse=False):
     """Times the f32 oracle on a bounded sample, checks the CUDA step bit for bit
-    against the oracle of the same storage, and states the error of the CUDA
-    step (and of the f32 fused step) against the f64 oracle."""
+    against the oracle of the same storage (and mode), and states the error of the
+    CUDA step (and of the f32 fused step) against the f64 oracle in parity mode."""
     from fenix_b200 import createCombustionVolumeSimulation, workloads
     from oracle import build as orc_build
     from oracle.oracle import OracleSimulation, num_threads
@@ -247,8 +247,10 @@ def cpu_baseline_and_parity(args, wl, counts, kernels, storage):
     orc_build.build()
     orc = OracleSimulation(wl.options, precision=32)
     orc64 = OracleSimulation(wl.options, precision=64)
-    orc_same = orc if storage == "f32" else OracleSimulation(wl.options, precision=32, storage=storage)
-    sim = createCombustionVolumeSimulation(wl.options, device=0, kernels=kernels, storage=storage)
+    orc_same = orc if (storage == "f32" and not sparse) else OracleSimulation(wl.options, precision=32, storage=storage)
+    if sparse:
+        orc_same.setSparse(True)
+    sim = createCombustionVolumeSimulation(wl.options, device=0, kernels=kernels, storage=storage, sparse=sparse)
     sim32 = None if storage == "f32" else createCombustionVolumeSimulation(wl.options, device=0, kernels="fused")
     everyone = [s for s in (orc, orc64, orc_same, sim, sim32) if s is not None]
     for s in set(everyone):
@@ -287,7 +289,8 @@ def cpu_baseline_and_parity(args, wl, counts, kernels, storage):
         "nproc": os.cpu_count(), "per_step": [round(v) for v in per_step],
         "sample": f"{args.cpu_steps} full steps of the same workload from the same start state (f32 restatement, OpenMP); "
                   "value = median of the per-step rates",
-    }, {"steps": args.cpu_steps, "bit_exact_vs_oracle": parity, "oracle": f"f32 arithmetic, {storage} storage"}, {
+    }, {"steps": args.cpu_steps, "bit_exact_vs_oracle": parity,
+        "oracle": f"f32 arithmetic, {storage} storage" + (", sparse mode" if sparse else "")}, {
         "steps": args.cpu_steps, "against": "f64 oracle (same start state and steps)", "fields": err}
 
 
@@ -508,7 +511,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="fenix", choices=["fenix", "reference"])
     ap.add_argument("--kernels", default="fused", choices=["fused", "plain"])
-    ap.add_argument("--storage", default="f16", choices=["f16", "f32"], help="scalar-set storage of the headline step")
+    ap.add_argument("--storage", default="f16", choices=["f16", "f16-nearest", "f32"],
+                    help="scalar-set storage of the headline step (f16: binary16 with stochastic rounding of the stores)")
+    ap.add_argument("--sparse", action="store_true", help="run the headline step in sparse mode (an extension)")
     ap.add_argument("--no-compare", action="store_true", help="skip timing the FP32 plain and fused steps")
     ap.add_argument("--no-c3", action="store_true", help="skip the batched 64-simulation configuration")
     ap.add_argument("--c3-steps", type=int, default=100)
@@ -559,9 +564,9 @@ def main():
     n = res[0] * res[1] * res[2]
     counts = workloads.brick_voxel_counts(res)
     nb = counts.size
-    if args.storage == "f16" and args.kernels != "fused":
+    if args.storage != "f32" and args.kernels != "fused":
         raise SystemExit("FP16 storage runs on the fused kernels only")
-    sim = createCombustionVolumeSimulation(wl.options, device=local, kernels=args.kernels, storage=args.storage)
+    sim = createCombustionVolumeSimulation(wl.options, device=local, kernels=args.kernels, storage=args.storage, sparse=args.sparse)
     sim.updateSources(wl.sources)
     workloads.load_state(sim, wl.state)
     sim.setInstrumentation(count_active=True)
@@ -705,7 +710,7 @@ def main():
     parity = None
     error = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu, parity, error = cpu_baseline_and_parity(args, wl, counts, args.kernels, args.storage)
+        cpu, parity, error = cpu_baseline_and_parity(args, wl, counts, args.kernels, args.storage, args.sparse)
 
     if pg:
         pg.barrier()
