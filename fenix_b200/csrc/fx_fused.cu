@@ -1301,6 +1301,9 @@ fx_status fused_init(FusedWork& w, cudaStream_t) {
   if (host_alloc((void**)&w.host_list_inj, ((size_t)w.nb + 1) * 4) != cudaSuccess) return FX_ERR_OUT_OF_MEMORY;
   if (host_alloc((void**)&w.host_cont, sizeof(int)) != cudaSuccess) return FX_ERR_OUT_OF_MEMORY;
   if (cudaStreamCreateWithFlags(&w.aux, cudaStreamNonBlocking) != cudaSuccess) return FX_ERR_CUDA;
+  if (cudaStreamCreateWithFlags(&w.aux2, cudaStreamNonBlocking) != cudaSuccess) return FX_ERR_CUDA;
+  if (cudaEventCreateWithFlags(&w.fork_ev, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
+  if (cudaEventCreateWithFlags(&w.join_ev, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
   w.valid = true;  // the arena starts cleared: every brick is zero
   return FX_OK;
 }
@@ -1331,6 +1334,11 @@ void fused_release(FusedWork& w) {
   w.host_cont = nullptr;
   if (w.aux) cudaStreamDestroy(w.aux);
   w.aux = nullptr;
+  if (w.aux2) cudaStreamDestroy(w.aux2);
+  w.aux2 = nullptr;
+  if (w.fork_ev) cudaEventDestroy(w.fork_ev);
+  if (w.join_ev) cudaEventDestroy(w.join_ev);
+  w.fork_ev = w.join_ev = nullptr;
   for (auto& ev : w.timing_events) cudaEventDestroy(ev);
   w.timing_events.clear();
 }
@@ -1602,6 +1610,61 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   uint32_t* c_adv = w.counters + 0;
   uint32_t* c_next = w.counters + 1;
   uint32_t* c_inj = w.counters + 3;
+  // The mid and coarse part of PressureSolvePass.solve (:73-82), sweep by sweep
+  // (inside the step's CUDA graph the launch gaps are short): mid pre-smoothing,
+  // restriction to coarse, coarse smoothing, prolongation into mid pressureA,
+  // mid post-smoothing. The first sweep of a level reads the cleared buffer, so
+  // it is computed from the divergence alone. With `side`, the chain runs on the
+  // second stream, forked after the restriction into the mid level and joined by
+  // join_ev; *mid gets the mid buffer holding the result.
+  auto lower_levels = [&](bool side, int& mid) -> cudaError_t {
+    const LevelBuf& M = st.lv[1];
+    const LevelBuf& C = st.lv[2];
+    cudaStream_t ls = s;
+    if (side) {
+      cudaError_t e = cudaEventRecord(w.fork_ev, s);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(w.aux2, w.fork_ev, 0);
+      if (e != cudaSuccess) return e;
+      ls = w.aux2;
+    }
+    int a = 0;
+    for (int k = 0; k < st.q[4]; ++k) {
+      Timed tm(w, ls, "fused_sweep_mid");
+      cudaError_t e = lean_sweep_variant(ls, st.sweep_variant[1], M.dm, M.div, k == 0 ? nullptr : M.p[a], M.p[a ^ 1], M.dm, nullptr);
+      if (e != cudaSuccess) return e;
+      a ^= 1;
+      ++launches;
+    }
+    const int mid_pre = a;
+    {
+      Timed tm(w, ls, "fused_restrict");
+      plain_restrict(ls, M.dm, C.dm, M.div, C.div);
+      ++launches;
+    }
+    int coarse = 0;
+    for (int k = 0; k < st.q[6]; ++k) {
+      Timed tm(w, ls, "fused_sweep_coarse");
+      cudaError_t e = lean_sweep_variant(ls, st.sweep_variant[2], C.dm, C.div, k == 0 ? nullptr : C.p[coarse], C.p[coarse ^ 1], C.dm, nullptr);
+      if (e != cudaSuccess) return e;
+      coarse ^= 1;
+      ++launches;
+    }
+    {
+      Timed tm(w, ls, "fused_prolong");
+      plain_prolong(ls, C.dm, M.dm, C.p[coarse], M.p[0]);
+      ++launches;
+    }
+    mid = mid_pre;
+    for (int k = 0; k < st.q[5]; ++k) {
+      Timed tm(w, ls, "fused_sweep_mid");
+      cudaError_t e = lean_sweep_variant(ls, st.sweep_variant[1], M.dm, M.div, M.p[mid], M.p[mid ^ 1], M.dm, nullptr);
+      if (e != cudaSuccess) return e;
+      mid ^= 1;
+      ++launches;
+    }
+    if (side) return cudaEventRecord(w.join_ev, w.aux2);
+    return cudaGetLastError();
+  };
   if (ninj) {
     Timed tm(w, s, "fused_inject");
     by_storage(st.half_storage, [&](auto tag) {
@@ -1827,41 +1890,9 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       ++launches;
     }
     if (m >= 1) chain = outs[wi++];
+    const bool overlap = prolong_live && m >= 3;
     int mid = 0;
-    if (prolong_live) {
-      int a = 0;
-      for (int k = 0; k < st.q[4]; ++k) {
-        Timed tm(w, s, "fused_sweep_mid");
-        FX_CK(lean_sweep_variant(s, st.sweep_variant[1], M.dm, M.div, k == 0 ? nullptr : M.p[a], M.p[a ^ 1], M.dm, nullptr));
-        a ^= 1;
-        ++launches;
-      }
-      const int mid_pre = a;
-      {
-        Timed tm(w, s, "fused_restrict");
-        plain_restrict(s, M.dm, C.dm, M.div, C.div);
-        ++launches;
-      }
-      int coarse = 0;
-      for (int k = 0; k < st.q[6]; ++k) {
-        Timed tm(w, s, "fused_sweep_coarse");
-        FX_CK(lean_sweep_variant(s, st.sweep_variant[2], C.dm, C.div, k == 0 ? nullptr : C.p[coarse], C.p[coarse ^ 1], C.dm, nullptr));
-        coarse ^= 1;
-        ++launches;
-      }
-      {
-        Timed tm(w, s, "fused_prolong");
-        plain_prolong(s, C.dm, M.dm, C.p[coarse], M.p[0]);
-        ++launches;
-      }
-      mid = mid_pre;
-      for (int k = 0; k < st.q[5]; ++k) {
-        Timed tm(w, s, "fused_sweep_mid");
-        FX_CK(lean_sweep_variant(s, st.sweep_variant[1], M.dm, M.div, M.p[mid], M.p[mid ^ 1], M.dm, nullptr));
-        mid ^= 1;
-        ++launches;
-      }
-    }
+    if (prolong_live) FX_CK(lower_levels(overlap, mid));
     // The fine sweeps: TMA-staged where tensor maps of the buffers exist.
     static const bool use_tma = [] {
       const char* v = std::getenv("FENIX_SPARSE_TMA");
@@ -1887,6 +1918,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     };
     for (int k = 2; k <= m; ++k) {
       const bool add = prolong_live && k == m;
+      if (add && overlap) FX_CK(cudaStreamWaitEvent(s, w.join_ev, 0));
       sweep(chain, outs[wi], add ? M.p[mid] : nullptr, add ? "sparse_sweep_prolong" : "sparse_sweep");
       chain = outs[wi++];
     }
@@ -1944,53 +1976,14 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       plain_restrict(s, F.dm, M.dm, F.div, M.div);
       ++launches;
     }
+    // The mid and coarse levels run on a second stream while the fine
+    // pre-sweeps before the last one (which adds their prolongation) run here.
+    const bool overlap = prolong_live && m >= 3;
     int mid = 0;
-    if (prolong_live) {
-      // Mid and coarse levels sweep by sweep (inside the step's CUDA graph the
-      // launch gaps are short). The first sweep of a level reads the cleared
-      // buffer, so it is computed from the divergence alone.
-      int mid_pre = 0;
-      {
-        int a = 0;
-        for (int k = 0; k < st.q[4]; ++k) {
-          Timed tm(w, s, "fused_sweep_mid");
-          FX_CK(lean_sweep_variant(s, st.sweep_variant[1], M.dm, M.div, k == 0 ? nullptr : M.p[a], M.p[a ^ 1], M.dm, nullptr));
-          a ^= 1;
-          ++launches;
-        }
-        mid_pre = a;
-      }
-      {
-        Timed tm(w, s, "fused_restrict");
-        plain_restrict(s, M.dm, C.dm, M.div, C.div);
-        ++launches;
-      }
-      int coarse = 0;
-      {
-        int a = 0;
-        for (int k = 0; k < st.q[6]; ++k) {
-          Timed tm(w, s, "fused_sweep_coarse");
-          FX_CK(lean_sweep_variant(s, st.sweep_variant[2], C.dm, C.div, k == 0 ? nullptr : C.p[a], C.p[a ^ 1], C.dm, nullptr));
-          a ^= 1;
-          ++launches;
-        }
-        coarse = a;
-      }
-      {
-        Timed tm(w, s, "fused_prolong");
-        plain_prolong(s, C.dm, M.dm, C.p[coarse], M.p[0]);
-        ++launches;
-      }
-      mid = mid_pre;
-      for (int k = 0; k < st.q[5]; ++k) {
-        Timed tm(w, s, "fused_sweep_mid");
-        FX_CK(lean_sweep_variant(s, st.sweep_variant[1], M.dm, M.div, M.p[mid], M.p[mid ^ 1], M.dm, nullptr));
-        mid ^= 1;
-        ++launches;
-      }
-    }
+    if (prolong_live) FX_CK(lower_levels(overlap, mid));
     for (int k = 2; k <= m; ++k) {
       const bool add = prolong_live && k == m;
+      if (add && overlap) FX_CK(cudaStreamWaitEvent(s, w.join_ev, 0));
       Timed tm(w, s, add ? "fused_sweep_prolong" : "fused_sweep");
       FX_CK(lean_sweep_variant(s, st.sweep_variant[0], dm, F.div, chain, outs[wi], M.dm, add ? M.p[mid] : nullptr));
       chain = outs[wi++];

@@ -67,6 +67,8 @@ struct FusedWork {
   SolverDev* solver = nullptr;     // FP64 solver statistics and the V-cycle loop state
   unsigned* vmax = nullptr;        // max |v| of the current velocity (float bits; all ones = unknown)
   cudaStream_t aux = nullptr;      // captures the V-cycle body graph
+  cudaStream_t aux2 = nullptr;     // the mid and coarse pressure levels, beside the fine pre-sweeps
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   int* host_cont = nullptr;        // pinned: the continue flag, read by the host loop without graphs
   uint32_t* host_list_inj = nullptr;  // pinned staging for list_inj (+ count at [nb])
   cudaEvent_t inj_event = nullptr;

@@ -167,21 +167,28 @@ FX_DEV uint32_t sr_draw(uint32_t i, uint32_t site, uint32_t step) {
   return h + step * 0x9E3779B9u;
 }
 
+//
+// Computed here without a division: in the binary16 normal range the distance
+// from the lower value in units of the spacing is the 13 low significand bits of
+// the float over 2^13, so "frac > u" is the integer test (bits << 11) > (r >> 8),
+// and the upper value is the lower one's bit pattern plus 2^13 (a carry into the
+// exponent gives the next binade's first value, as it should). Below 2^-14 the
+// spacing is 2^-24 and a * 2^24 and its truncation are exact. The results equal
+// the oracle's formulation bit for bit.
 FX_DEV float sr_half(float v, uint32_t r) {
   const float a = fabsf(v);
   if (!(a < 65504.0f)) return __half2float(__float2half_rn(v));
-  float lo, ulp;
+  const uint32_t rb = r >> 8;
   if (a >= 0x1p-14f) {
     const uint32_t b = __float_as_uint(a);
-    lo = __uint_as_float(b & ~0x1FFFu);
-    ulp = __uint_as_float((((b >> 23) & 0xFFu) - 10u) << 23);
-  } else {
-    lo = truncf(a * 0x1p24f) * 0x1p-24f;
-    ulp = 0x1p-24f;
+    const uint32_t lo = b & ~0x1FFFu;
+    const uint32_t m = ((b & 0x1FFFu) << 11) > rb ? lo + 0x2000u : lo;
+    return copysignf(__uint_as_float(m), v);
   }
-  const float frac = (a - lo) / ulp;
-  const float u = (float)(r >> 8) * 0x1p-24f;
-  return copysignf(frac > u ? lo + ulp : lo, v);
+  const float q = a * 0x1p24f;
+  const float t = truncf(q);
+  const float u = (float)rb * 0x1p-24f;
+  return copysignf(((q - t) > u ? t + 1.0f : t) * 0x1p-24f, v);
 }
 
 // Trilinear sampler of shaders/common/sampling-scalar.wgsl.ts:11-34. A NaN

@@ -422,6 +422,119 @@ __global__ void __launch_bounds__(256, 4) k_resid_norm_march(Dims f, const float
   block_sum_to(s2, part);
 }
 
+// The lower part of a V-cycle in one block of 1024 threads: from level k0 (its
+// right-hand side restricted and its p[0] cleared by the caller) down to the
+// coarsest level and back, as level_cycle runs it: pre-sweeps, residual
+// restriction, clearing, the coarsest sweeps, prolongation and post-sweeps, with a
+// block barrier between passes. Each voxel is computed as in k_wjacobi,
+// k_resid_restrict and k_prolong_add, in their operation order, so the results
+// are the same bits. Small levels are bound by launch latency when every pass is
+// its own kernel; here they cost one launch. Buffers written in the kernel are
+// read with plain loads (never the read-only path) after the barrier.
+constexpr uint32_t kTailVoxels = 40000;  // a level at most this large runs in the tail kernel
+constexpr int kTailThreads = 1024;
+
+FX_DEV void tail_sweep(const LevelBuf& B, const float* src, float* dst, float w, bool one) {
+  const Dims d = B.dm;
+  const uint32_t n = d.w * d.h * d.d, sy = d.w, sz = d.w * d.h;
+  for (uint32_t i = threadIdx.x; i < n; i += kTailThreads) {
+    const uint32_t x = i % d.w, y = (i / d.w) % d.h, z = i / sz;
+    float v = 0.0f;
+    if (!is_boundary(d, x, y, z)) {
+      const float s = src[i + 1] + src[i - 1] + src[i + sy] + src[i - sy] + src[i + sz] + src[i - sz];
+      const float j = div6(s - B.div[i]);
+      const float cm = src[i];
+      v = one ? j : cm + w * (j - cm);
+    }
+    dst[i] = v;
+  }
+}
+
+FX_DEV float tail_resid_at(const Dims& f, const float* rhs, const float* e, uint32_t x, uint32_t y, uint32_t z) {
+  if (is_boundary(f, x, y, z)) return 0.0f;
+  const uint32_t W1 = f.w - 1u, H1 = f.h - 1u, D1 = f.d - 1u;
+  const uint32_t i = flat(f, x, y, z);
+  const float s = e[flat(f, inc(x, W1), y, z)] + e[flat(f, dec(x), y, z)] + e[flat(f, x, inc(y, H1), z)] + e[flat(f, x, dec(y), z)] +
+                  e[flat(f, x, y, inc(z, D1))] + e[flat(f, x, y, dec(z))];
+  const float lap = s - e[i] * 6.0f;
+  return rhs[i] - lap;
+}
+
+FX_DEV void tail_resid_restrict(const LevelBuf& B, const float* e, const LevelBuf& C) {
+  const Dims f = B.dm, c = C.dm;
+  const uint32_t n = c.w * c.h * c.d;
+  for (uint32_t i = threadIdx.x; i < n; i += kTailThreads) {
+    const uint32_t x = i % c.w, y = (i / c.w) % c.h, z = i / (c.w * c.h);
+    if (x == 0u || y == 0u || z == 0u || x == c.w - 1u || y == c.h - 1u || z == c.d - 1u) {
+      C.div[i] = 0.0f;
+      continue;
+    }
+    float sum = 0.0f;
+    for (uint32_t dz = 0; dz < 2; ++dz)
+      for (uint32_t dy = 0; dy < 2; ++dy)
+        for (uint32_t dx = 0; dx < 2; ++dx)
+          sum += tail_resid_at(f, B.div, e, min(2u * x + dx, f.w - 1u), min(2u * y + dy, f.h - 1u), min(2u * z + dz, f.d - 1u));
+    C.div[i] = (sum * 0.125f) * 4.0f;
+  }
+}
+
+FX_DEV float tail_interp(const float* f, const Tri& c) {
+  const float x00 = mixv(f[c.i000], f[c.i100], c.fx);
+  const float x10 = mixv(f[c.i010], f[c.i110], c.fx);
+  const float x01 = mixv(f[c.i001], f[c.i101], c.fx);
+  const float x11 = mixv(f[c.i011], f[c.i111], c.fx);
+  return mixv(mixv(x00, x10, c.fy), mixv(x01, x11, c.fy), c.fz);
+}
+
+FX_DEV void tail_prolong_add(const LevelBuf& C, const float* ec, const LevelBuf& B, const float* src, float* dst) {
+  const Dims f = B.dm;
+  const uint32_t n = f.w * f.h * f.d;
+  for (uint32_t i = threadIdx.x; i < n; i += kTailThreads) {
+    const uint32_t x = i % f.w, y = (i / f.w) % f.h, z = i / (f.w * f.h);
+    const float v = src[i];
+    if (x == 0u || y == 0u || z == 0u || x == f.w - 1u || y == f.h - 1u || z == f.d - 1u) {
+      dst[i] = v;
+      continue;
+    }
+    const float px = ((float)x + 0.5f) * 0.5f - 0.5f;
+    const float py = ((float)y + 0.5f) * 0.5f - 0.5f;
+    const float pz = ((float)z + 0.5f) * 0.5f - 0.5f;
+    dst[i] = v + tail_interp(ec, tri_corners(C.dm, px, py, pz));
+  }
+}
+
+FX_DEV int tail_smooth(const LevelBuf& B, int sweeps, int start, const VCycleConfig& c) {
+  int a = start;
+  for (int k = 0; k < sweeps; ++k) {
+    tail_sweep(B, B.p[a], B.p[a ^ 1], c.omega, c.omega_one);
+    __syncthreads();
+    a ^= 1;
+  }
+  return a;
+}
+
+__global__ void __launch_bounds__(kTailThreads) k_vcycle_tail(VCycleLevels L, VCycleConfig c, int k0) {
+  int a[kMaxVLevels];
+  for (int k = k0; k < c.levels - 1; ++k) {
+    const LevelBuf& B = L.lv[k];
+    const LevelBuf& C = L.lv[k + 1];
+    a[k] = tail_smooth(B, c.pre, 0, c);
+    tail_resid_restrict(B, B.p[a[k]], C);
+    const uint32_t nc = C.dm.w * C.dm.h * C.dm.d;
+    for (uint32_t i = threadIdx.x; i < nc; i += kTailThreads) C.p[0][i] = 0.0f;
+    __syncthreads();
+  }
+  int e = tail_smooth(L.lv[c.levels - 1], c.coarse, 0, c);
+  for (int k = c.levels - 2; k >= k0; --k) {
+    const LevelBuf& B = L.lv[k];
+    const LevelBuf& C = L.lv[k + 1];
+    const int b = ((c.pre + c.post) & 1) ? a[k] ^ 1 : a[k];
+    tail_prolong_add(C, C.p[e], B, B.p[a[k]], B.p[b]);
+    __syncthreads();
+    e = tail_smooth(B, c.post, b, c);
+  }
+}
+
 __global__ void __launch_bounds__(256) k_fill0(float* __restrict__ p, uint32_t n) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0.0f;
 }
@@ -570,8 +683,23 @@ int resid_norm(cudaStream_t s, Dims dm, const float* rhs, const float* p, double
   return (int)reduce_blocks();
 }
 
+// The buffer id that level_cycle(k, start) ends in (host arithmetic).
+int cycle_end_id(const VCycleConfig& c, int k, int start) {
+  if (k == c.levels - 1) return start ^ (c.coarse & 1);
+  const int a = start ^ (c.pre & 1);
+  const int b = ((c.pre + c.post) & 1) ? a ^ 1 : a;
+  return b ^ (c.post & 1);
+}
+
 int level_cycle(cudaStream_t s, const VCycleLevels& L, const VCycleConfig& c, int k, int start, uint32_t* launches) {
   const LevelBuf& B = L.lv[k];
+  // A small level and everything below it: one block, one launch (the caller has
+  // restricted its right-hand side and cleared p[0], so start is 0).
+  if (!c.plain && k > 0 && start == 0 && count_of(B.dm) <= kTailVoxels) {
+    k_vcycle_tail<<<1, kTailThreads, 0, s>>>(L, c, k);
+    ++*launches;
+    return cycle_end_id(c, k, 0);
+  }
   if (k == c.levels - 1) return smooth(s, B, c.coarse, start, c, launches);
   const int a = smooth(s, B, c.pre, start, c, launches);
   const LevelBuf& C = L.lv[k + 1];
