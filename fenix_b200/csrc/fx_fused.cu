@@ -1717,7 +1717,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     L.nz[0] = w.nz_sp[SP_VSCR];
     {
       Timed tm(w, s, "sparse_lists");
-      k_sp_lists<<<(nb + 255) / 256, 256, 0, s>>>(nb, st.flags_cur, nullptr, L, nullptr);
+      k_sp_lists<<<(nb + 255) / 256, 256, 0, s>>>(bc, nb, st.flags_cur, nullptr, L, nullptr);
       ++launches;
     }
     Timed tm(w, s, "sparse_advect_velocity");
@@ -1780,7 +1780,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       L.nz[k] = w.nz_sp[fams[k]];
     }
     Timed tm(w, s, "sparse_lists");
-    k_sp_lists<<<(nb + 255) / 256, 256, 0, s>>>(nb, st.flags_cur, st.flags_next, L, w.nz_sp[SP_VSCR]);
+    k_sp_lists<<<(nb + 255) / 256, 256, 0, s>>>(bc, nb, st.flags_cur, st.flags_next, L, w.nz_sp[SP_VSCR]);
     ++launches;
   }
   // 6. combustion T -> next set, 7. buoyancy
@@ -1909,8 +1909,9 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       Timed tm(w, s, name);
       if (use_tma && w.tmaps_ok && src) {
         const CUtensorMap& sm = src == F.p[0] ? w.tmap_p[0] : w.tmap_p[1];
-        k_sp_sweep_tma<<<brick_grid, kBrickThreads, 0, s>>>(sm, w.tmap_div, dm, bc, dst, M.dm, mid_p, pl, pc, w.dev_err, w.tma_wait_ns,
-                                                            w.tma_extra_tx);
+        const uint32_t sweep_grid = std::max<uint32_t>(1, std::min<uint32_t>(nb, (uint32_t)device_sm_count() * 8u));
+        k_sp_sweep_tma<<<sweep_grid, kSpSweepThreads, 0, s>>>(sm, w.tmap_div, dm, bc, dst, M.dm, mid_p, pl, pc, w.dev_err, w.tma_wait_ns,
+                                                              w.tma_extra_tx);
       } else {
         k_sp_sweep<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, F.div, src, dst, M.dm, mid_p, 0, pl, pc);
       }

@@ -19,11 +19,31 @@
 // Fields keep their dense layout: a gather or stencil that leaves the set reads
 // the zeros stored there, with no indirection. Per-brick "may be non-zero" bits
 // of each buffer family tell which bricks outside the set still hold values of
-// an earlier step; the lists the kernels walk are the set plus those bricks,
-// each entry the brick index with bit 31 set where the brick is computed and
-// clear where it is only zeroed.
+// an earlier step; the lists the kernels walk are the set plus those bricks.
+// An entry holds the brick's coordinates (10 bits each: x, then y, then z; at
+// most 1024 bricks per axis) with bit 31 set where the brick is computed and
+// clear where it is only zeroed, so no kernel divides to locate its brick.
 constexpr uint32_t kSpCompute = 0x80000000u;
-constexpr uint32_t kSpIndex = 0x7FFFFFFFu;
+constexpr uint32_t kSpMaxBricksPerAxis = 1024;
+
+FX_DEV uint32_t sp_pack(uint3 bc, uint32_t b, bool comp) {
+  const uint32_t bx = b % bc.x, by = (b / bc.x) % bc.y, bz = b / (bc.x * bc.y);
+  return bx | (by << 10) | (bz << 20) | (comp ? kSpCompute : 0u);
+}
+FX_DEV BrickCtx sp_ctx(const Dims& dm, uint32_t e) {
+  BrickCtx c;
+  c.bx = e & 1023u;
+  c.by = (e >> 10) & 1023u;
+  c.bz = (e >> 20) & 1023u;
+  c.x0 = c.bx * 8u;
+  c.y0 = c.by * 8u;
+  c.z0 = c.bz * 8u;
+  c.cx = min(c.x0 + 4u, dm.w - 1u);
+  c.cy = min(c.y0 + 4u, dm.h - 1u);
+  c.cz = min(c.z0 + 4u, dm.d - 1u);
+  return c;
+}
+FX_DEV uint32_t sp_brick_index(uint3 bc, const BrickCtx& c) { return c.bx + bc.x * (c.by + bc.y * c.bz); }
 
 // Buffer families with their own non-zero bits (FusedWork::nz_sp).
 enum SpFamily { SP_VSCR = 0, SP_CURL = 1, SP_PRESSURE = 2, SP_VCUR = 3, kSpFamilies = 4 };
@@ -39,8 +59,8 @@ struct SpLists {
   uint8_t* nz[3];
 };
 
-__global__ void __launch_bounds__(256) k_sp_lists(uint32_t nb, const uint32_t* __restrict__ flags_a, const uint32_t* __restrict__ flags_b,
-                                                  SpLists L, uint8_t* __restrict__ extra) {
+__global__ void __launch_bounds__(256) k_sp_lists(uint3 bc, uint32_t nb, const uint32_t* __restrict__ flags_a,
+                                                  const uint32_t* __restrict__ flags_b, SpLists L, uint8_t* __restrict__ extra) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t lane = threadIdx.x & 31u;
   const bool live = b < nb;
@@ -54,7 +74,7 @@ __global__ void __launch_bounds__(256) k_sp_lists(uint32_t nb, const uint32_t* _
     uint32_t base = 0;
     if (lane == 0 && ballot) base = atomicAdd(L.count[k], (uint32_t)__popc(ballot));
     base = __shfl_sync(0xffffffffu, base, 0);
-    if (take) L.list[k][base + __popc(ballot & ((1u << lane) - 1u))] = b | (comp ? kSpCompute : 0u);
+    if (take) L.list[k][base + __popc(ballot & ((1u << lane) - 1u))] = sp_pack(bc, b, comp);
     if (live) L.nz[k][b] = comp ? 1 : 0;
   }
 }
@@ -102,7 +122,7 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_advect_velocity(Dims dm, u
   for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
     const uint32_t e = list[li];
     const bool comp = (e & kSpCompute) != 0u;
-    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+    const BrickCtx c = sp_ctx(dm, e);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       const SpVoxel v = sp_voxel(dm, c, j);
@@ -136,7 +156,7 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_vorticity(Dims dm, uint3 b
   for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
     const uint32_t e = list[li];
     const bool comp = (e & kSpCompute) != 0u;
-    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+    const BrickCtx c = sp_ctx(dm, e);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       const SpVoxel q = sp_voxel(dm, c, j);
@@ -168,8 +188,8 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_confinement(Dims dm, uint3
   for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
     const uint32_t e = list[li];
     const bool comp = (e & kSpCompute) != 0u;
-    const uint32_t b = e & kSpIndex;
-    const BrickCtx c = brick_ctx(dm, bc, b);
+    const BrickCtx c = sp_ctx(dm, e);
+    const uint32_t b = sp_brick_index(bc, c);
     const bool scal = __ldg(nz + b) != 0;
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
@@ -229,7 +249,7 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_div_first(Dims dm, uint3 b
   for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
     const uint32_t e = list[li];
     const bool comp = (e & kSpCompute) != 0u;
-    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+    const BrickCtx c = sp_ctx(dm, e);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       const SpVoxel q = sp_voxel(dm, c, j);
@@ -283,7 +303,7 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_sweep(Dims dm, uint3 bc, c
   for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
     const uint32_t e = list[li];
     const bool comp = (e & kSpCompute) != 0u;
-    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+    const BrickCtx c = sp_ctx(dm, e);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       const SpVoxel q = sp_voxel(dm, c, j);
@@ -314,7 +334,7 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_project(Dims dm, uint3 bc,
   for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
     const uint32_t e = list[li];
     const bool comp = (e & kSpCompute) != 0u;
-    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+    const BrickCtx c = sp_ctx(dm, e);
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       const SpVoxel q = sp_voxel(dm, c, j);
@@ -401,21 +421,27 @@ FX_DEV void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, 
 }
 
 // k_sp_sweep (src given) from TMA-staged tiles; the same operations in the same
-// order, so the same bits. `wait_ns` bounds every wait on a tile: when one runs
-// out the block sets *err, waits (bounded again) for its loads in flight and
+// order, so the same bits. A block of 128 threads takes a brick at a time; a
+// thread owns one (x, y) of it and four consecutive z, so the brick's decoding,
+// tests and index arithmetic are shared by four voxels and the z neighbours of
+// its column are read once. Three stages: the loads of the next two entries are
+// in flight while one is computed. `wait_ns` bounds every wait on a tile: when one
+// runs out the block sets *err, waits (bounded again) for its loads in flight and
 // returns. `extra_tx` adds to the bytes a stage expects and is 0 except in the
 // test of that timeout path, where the stage then never completes.
-__global__ void __launch_bounds__(kBrickThreads) k_sp_sweep_tma(const __grid_constant__ CUtensorMap src_map,
-                                                                const __grid_constant__ CUtensorMap div_map, Dims dm, uint3 bc,
-                                                                float* __restrict__ dst, Dims mid, const float* __restrict__ mid_p,
-                                                                const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
-                                                                uint32_t* __restrict__ err, uint64_t wait_ns, uint32_t extra_tx) {
-  __shared__ __align__(128) float tile[2][kSpTileFloats + kSpDivFloats];
-  __shared__ __align__(8) uint64_t bar[2];
+constexpr int kSpSweepThreads = 128;
+constexpr int kSpStages = 3;
+
+__global__ void __launch_bounds__(kSpSweepThreads) k_sp_sweep_tma(const __grid_constant__ CUtensorMap src_map,
+                                                                  const __grid_constant__ CUtensorMap div_map, Dims dm, uint3 bc,
+                                                                  float* __restrict__ dst, Dims mid, const float* __restrict__ mid_p,
+                                                                  const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
+                                                                  uint32_t* __restrict__ err, uint64_t wait_ns, uint32_t extra_tx) {
+  __shared__ __align__(128) float tile[kSpStages][kSpTileFloats + kSpDivFloats];
+  __shared__ __align__(8) uint64_t bar[kSpStages];
   const uint32_t n = *count;
   if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int k = 0; k < kSpStages; ++k) mbar_init(&bar[k], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
@@ -423,22 +449,30 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_sweep_tma(const __grid_con
   auto issue = [&](uint32_t li, int stage) {
     const uint32_t e = list[li];
     if (!(e & kSpCompute)) return false;
-    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+    const BrickCtx c = sp_ctx(dm, e);
     mbar_arrive_expect_tx(&bar[stage], kSpStageBytes + extra_tx);
     tma_load_3d(&tile[stage][0], &src_map, (int)c.x0 - 4, (int)c.y0 - 1, (int)c.z0 - 1, &bar[stage]);
     tma_load_3d(&tile[stage][kSpTileFloats], &div_map, (int)c.x0, (int)c.y0, (int)c.z0, &bar[stage]);
     return true;
   };
-  uint32_t parity = 0u;  // bit k: the phase stage k waits for next
+  // bit k of `issued`: stage k has loads in flight; bit k of `parity`: the phase it waits for
+  uint32_t issued = 0u, parity = 0u;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < kSpStages - 1; ++k) {
+      const uint32_t li = blockIdx.x + (uint32_t)k * gridDim.x;
+      if (li < n && issue(li, k)) issued |= 1u << k;
+    }
+  const uint32_t lx = threadIdx.x & 7u, ly = (threadIdx.x >> 3) & 7u, lz0 = (threadIdx.x >> 6) * 4u;
+  const uint32_t sz = dm.w * dm.h;
   int stage = 0;
-  if (threadIdx.x == 0 && blockIdx.x < n) issue(blockIdx.x, 0);
   for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
-    const uint32_t nli = li + gridDim.x;
-    bool next_issued = false;
-    if (threadIdx.x == 0 && nli < n) next_issued = issue(nli, stage ^ 1);
+    // keep kSpStages - 1 entries ahead in flight (that stage was read two iterations ago)
+    const uint32_t ahead = li + (uint32_t)(kSpStages - 1) * gridDim.x;
+    const int ast = (stage + kSpStages - 1) % kSpStages;
+    if (threadIdx.x == 0 && ahead < n && issue(ahead, ast)) issued |= 1u << ast;
     const uint32_t e = list[li];
     const bool comp = (e & kSpCompute) != 0u;
-    const BrickCtx c = brick_ctx(dm, bc, e & kSpIndex);
+    const BrickCtx c = sp_ctx(dm, e);
     if (comp) {
       const uint32_t ph = (parity >> stage) & 1u;
       const bool ok = mbar_wait_bounded(&bar[stage], ph, wait_ns);
@@ -446,32 +480,43 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_sweep_tma(const __grid_con
         // A tile never arrived: record it, let the loads in flight land, leave.
         if (threadIdx.x == 0) {
           atomicOr(err, 1u);
-          mbar_wait_bounded(&bar[stage], ph, wait_ns);
-          if (next_issued) mbar_wait_bounded(&bar[stage ^ 1], (parity >> (stage ^ 1)) & 1u, wait_ns);
+          for (int k = 0; k < kSpStages; ++k)
+            if (issued & (1u << k)) mbar_wait_bounded(&bar[k], (parity >> k) & 1u, wait_ns);
         }
         __syncthreads();
         return;
       }
       parity ^= 1u << stage;
+      issued &= ~(1u << stage);
     }
-    const float* T = tile[stage];
-    const float* Dv = tile[stage] + kSpTileFloats;
+    const uint32_t x = c.x0 + lx, y = c.y0 + ly;
+    if (x < dm.w && y < dm.h) {
+      const bool xyint = comp && x > 0u && y > 0u && x < dm.w - 1u && y < dm.h - 1u;
+      const float* T = tile[stage];
+      const float* Dv = tile[stage] + kSpTileFloats;
+      const uint32_t col = (lx + 4u) + 16u * (ly + 1u);  // tile index of (x, y) at tile plane 0
+      const uint32_t base = x + dm.w * y;
+      float zc[6];
+      if (xyint) {
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const SpVoxel q = sp_voxel(dm, c, j);
-      if (!q.inside) continue;
-      float out = 0.0f;
-      if (comp && !is_boundary(dm, q.x, q.y, q.z)) {
-        const uint32_t lx = q.x - c.x0, ly = q.y - c.y0, lz = q.z - c.z0;
-        const uint32_t t = (lx + 4u) + 16u * ((ly + 1u) + 10u * (lz + 1u));
-        const float s = T[t + 1u] + T[t - 1u] + T[t + 16u] + T[t - 16u] + T[t + 160u] + T[t - 160u];
-        out = div6(s - Dv[lx + 8u * (ly + 8u * lz)]);
-        if (mid_p) out = out + prolong_sample_at(mid, mid_p, (int)q.x, (int)q.y, (int)q.z);
+        for (int k = 0; k < 6; ++k) zc[k] = T[col + 160u * (lz0 + (uint32_t)k)];  // planes lz0 - 1 .. lz0 + 4
       }
-      dst[q.i] = out;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint32_t lz = lz0 + (uint32_t)k, z = c.z0 + lz;
+        if (z >= dm.d) break;
+        float out = 0.0f;
+        if (xyint && z > 0u && z < dm.d - 1u) {
+          const uint32_t t = col + 160u * (lz + 1u);
+          const float s = T[t + 1u] + T[t - 1u] + T[t + 16u] + T[t - 16u] + zc[k + 2] + zc[k];
+          out = div6(s - Dv[lx + 8u * (ly + 8u * lz)]);
+          if (mid_p) out = out + prolong_sample_at(mid, mid_p, (int)x, (int)y, (int)z);
+        }
+        dst[base + sz * z] = out;
+      }
     }
-    __syncthreads();  // the stage is read; the next iteration may reload it
-    stage ^= 1;
+    __syncthreads();  // the stage is read; a later iteration may reload it
+    stage = (stage + 1) % kSpStages;
   }
 }
 

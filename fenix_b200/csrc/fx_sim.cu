@@ -701,6 +701,8 @@ fx_status fx_sim_create(const fx_sim_options* opt_in, fx_sim** out) {
     return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_sim_create: FP16 scalar storage needs the fused kernels");
   if ((opt.flags & FX_OPT_SPARSE) && opt.kernels != FX_KERNELS_FUSED)
     return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_sim_create: sparse mode needs the fused kernels");
+  if ((opt.flags & FX_OPT_SPARSE) && (opt.width > 8192u || opt.height > 8192u || opt.depth > 8192u))
+    return fail(nullptr, FX_ERR_UNSUPPORTED, "fx_sim_create: sparse mode supports at most 8192 voxels (1024 bricks) per axis");
 
   fx_sim* s = new (std::nothrow) fx_sim;
   if (!s) return fail(nullptr, FX_ERR_OUT_OF_MEMORY, "fx_sim_create: host allocation failed");
@@ -1265,6 +1267,8 @@ fx_status fx_sim_set_sparse(fx_sim* s, int32_t on) {
   if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_sparse: NULL handle");
   if (on && s->kernels != FX_KERNELS_FUSED) return fail(s, FX_ERR_UNSUPPORTED, "fx_sim_set_sparse: sparse mode needs the fused kernels");
   if (on && s->solver.mode == FX_SOLVER_VCYCLE) return fail(s, FX_ERR_UNSUPPORTED, "fx_sim_set_sparse: sparse mode has no V-cycle form");
+  if (on && (s->bricks.x > 1024u || s->bricks.y > 1024u || s->bricks.z > 1024u))
+    return fail(s, FX_ERR_UNSUPPORTED, "fx_sim_set_sparse: sparse mode supports at most 1024 bricks (8192 voxels) per axis");
   s->sparse = on != 0;
   return FX_OK;
 }

@@ -431,22 +431,47 @@ __global__ void __launch_bounds__(256, 4) k_resid_norm_march(Dims f, const float
 // are the same bits. Small levels are bound by launch latency when every pass is
 // its own kernel; here they cost one launch. Buffers written in the kernel are
 // read with plain loads (never the read-only path) after the barrier.
-constexpr uint32_t kTailVoxels = 40000;  // a level at most this large runs in the tail kernel
+// A level at most this large runs in the tail kernel: at most 8 voxels per
+// thread, whose loads are issued together (one block has too few warps to hide
+// the latency of longer chains; 32^3 levels measured slower there than launched).
+constexpr uint32_t kTailVoxels = 8192;
 constexpr int kTailThreads = 1024;
+constexpr int kTailVox = 4;  // voxels per thread per round, loads issued before the arithmetic
 
 FX_DEV void tail_sweep(const LevelBuf& B, const float* src, float* dst, float w, bool one) {
   const Dims d = B.dm;
   const uint32_t n = d.w * d.h * d.d, sy = d.w, sz = d.w * d.h;
-  for (uint32_t i = threadIdx.x; i < n; i += kTailThreads) {
-    const uint32_t x = i % d.w, y = (i / d.w) % d.h, z = i / sz;
-    float v = 0.0f;
-    if (!is_boundary(d, x, y, z)) {
-      const float s = src[i + 1] + src[i - 1] + src[i + sy] + src[i - sy] + src[i + sz] + src[i - sz];
-      const float j = div6(s - B.div[i]);
-      const float cm = src[i];
-      v = one ? j : cm + w * (j - cm);
+  for (uint32_t i0 = threadIdx.x; i0 < n; i0 += kTailThreads * kTailVox) {
+    float nb[kTailVox][7];
+    bool in[kTailVox];
+#pragma unroll
+    for (int k = 0; k < kTailVox; ++k) {
+      const uint32_t i = i0 + (uint32_t)k * kTailThreads;
+      const uint32_t x = i % d.w, y = (i / d.w) % d.h, z = i / sz;
+      in[k] = i < n && !is_boundary(d, x, y, z);
+      if (in[k]) {
+        nb[k][0] = src[i + 1];
+        nb[k][1] = src[i - 1];
+        nb[k][2] = src[i + sy];
+        nb[k][3] = src[i - sy];
+        nb[k][4] = src[i + sz];
+        nb[k][5] = src[i - sz];
+        nb[k][6] = B.div[i];
+      }
     }
-    dst[i] = v;
+#pragma unroll
+    for (int k = 0; k < kTailVox; ++k) {
+      const uint32_t i = i0 + (uint32_t)k * kTailThreads;
+      if (i >= n) continue;
+      float v = 0.0f;
+      if (in[k]) {
+        const float s = nb[k][0] + nb[k][1] + nb[k][2] + nb[k][3] + nb[k][4] + nb[k][5];
+        const float j = div6(s - nb[k][6]);
+        const float cm = src[i];
+        v = one ? j : cm + w * (j - cm);
+      }
+      dst[i] = v;
+    }
   }
 }
 
