@@ -294,14 +294,15 @@ def cpu_baseline_and_parity(args, wl, counts, kernels, storage, sparse=False):
         "steps": args.cpu_steps, "against": "f64 oracle (same start state and steps)", "fields": err}
 
 
-def time_steps(args, wl, local, kernels, storage, pg, solver=None, sparse=False):
-    """K steps of (kernels, storage[, solver][, sparse mode]) on a fresh simulation,
-    device time on its stream (max over ranks), after the warm-up steps."""
+def time_steps(args, wl, local, kernels, storage, pg, solver=None, sparse=False, fast_math=False):
+    """K steps of (kernels, storage[, solver][, sparse mode][, fast-arithmetic build])
+    on a fresh simulation, device time on its stream (max over ranks), after the
+    warm-up steps."""
     import torch
 
     from fenix_b200 import createCombustionVolumeSimulation, workloads
 
-    sim = createCombustionVolumeSimulation(wl.options, device=local, kernels=kernels, storage=storage, sparse=sparse)
+    sim = createCombustionVolumeSimulation(wl.options, device=local, kernels=kernels, storage=storage, sparse=sparse, fast_math=fast_math)
     sim.updateSources(wl.sources)
     workloads.load_state(sim, wl.state)
     sim.setInstrumentation(count_active=True)
@@ -339,6 +340,8 @@ def time_steps(args, wl, local, kernels, storage, pg, solver=None, sparse=False)
     out = {"value": voxel_steps / (ms / 1e3), "ms_per_step": ms / args.steps, "kernels": kernels, "storage": storage}
     if sparse:
         out["sparse"] = True
+    if fast_math:
+        out["fast_math"] = True
     if solver:
         out["solver"] = dict(solver)
         out["last_step_solver_stats"] = solver_stats
@@ -697,11 +700,16 @@ def main():
             r["ratio"] = value / r["value"]
             compare[f"{storage}_{kernels}_vcycle"] = r
         compare["c2_mixed_over_plain_f32"] = compare["f16_fused_vcycle"]["value"] / compare["f32_plain_vcycle"]["value"]
-        # sparse mode (extension): the velocity passes on the active bricks only
+        # sparse mode (extension): the velocity passes on the active bricks only;
+        # and the fast-arithmetic build (FMA contraction, CUDA sin/cos; not bit-exact)
         for storage in ("f16", "f32"):
             r = time_steps(args, wl, local, "fused", storage, pg, sparse=True)
             r["ratio"] = value / r["value"]
             compare[f"{storage}_fused_sparse"] = r
+        for sparse in (False, True):
+            r = time_steps(args, wl, local, "fused", "f16", pg, sparse=sparse, fast_math=True)
+            r["ratio"] = value / r["value"]
+            compare["f16_fused" + ("_sparse" if sparse else "") + "_fast"] = r
 
     batch_c3 = None if args.no_c3 else run_batch_c3(args, local, rank, world, pg)
     adjoint = None if args.no_adjoint else run_adjoint_c4(args, local, pg)

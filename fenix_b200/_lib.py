@@ -11,6 +11,9 @@ from ctypes import POINTER, Structure, c_char_p, c_double, c_float, c_int32, c_i
 
 PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PACKAGE_DIR, "libfenixcuda.so")
+# The fast-arithmetic build of the same sources (FMA contraction, CUDA sin/cos,
+# approximate division): results are stated against f64, not bit-exact.
+LIB_PATH_FAST = os.path.join(PACKAGE_DIR, "libfenixcuda_fast.so")
 
 FX_OK = 0
 FX_ERR_INVALID_ARGUMENT = -1
@@ -306,12 +309,18 @@ class FenixError(RuntimeError):
         self.status = status
 
 
-def load(path: str | None = None) -> ctypes.CDLL:
-    """Loads the CUDA library once. Raises if it is missing: no fallback exists."""
-    global _LIB
-    if _LIB is not None and path is None:
+_LIB_FAST = None
+
+
+def load(path: str | None = None, fast: bool = False) -> ctypes.CDLL:
+    """Loads the CUDA library once (the fast-arithmetic build with fast=True).
+    Raises if it is missing: no fallback exists."""
+    global _LIB, _LIB_FAST
+    if path is None and fast and _LIB_FAST is not None:
+        return _LIB_FAST
+    if _LIB is not None and path is None and not fast:
         return _LIB
-    p = path or LIB_PATH
+    p = path or (LIB_PATH_FAST if fast else LIB_PATH)
     if not os.path.exists(p):
         raise RuntimeError(
             f"libfenixcuda.so not found at {p}: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
@@ -322,14 +331,18 @@ def load(path: str | None = None) -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if path is None:
+    if path is None and fast:
+        _LIB_FAST = lib
+    elif path is None:
         _LIB = lib
     return lib
 
 
-def check(status: int, sim_handle=None) -> None:
+def check(status: int, sim_handle=None, lib: ctypes.CDLL | None = None) -> None:
+    """Raises FenixError for a negative status, with the handle's message (or the
+    library's last error; `lib` is the library that made the call)."""
     if status == FX_OK:
         return
-    lib = load()
+    lib = lib or load()
     msg = lib.fx_sim_last_error(sim_handle) if sim_handle else lib.fx_last_error()
     raise FenixError(status, (msg or b"").decode(errors="replace"))

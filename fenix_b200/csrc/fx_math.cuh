@@ -57,8 +57,16 @@ FX_DEV float pinned_sincos(float x, int quadrant_offset) {
   return (q & 2) ? -s : s;
 }
 
+// The fast-arithmetic build (FX_FAST_MATH; libfenixcuda_fast.so, compiled with
+// contraction into FMA and approximate division and square root) calls CUDA's
+// sinf/cosf instead: not the oracle's bits, a stated error against f64.
+#ifdef FX_FAST_MATH
+FX_DEV float psin(float x) { return sinf(x); }
+FX_DEV float pcos(float x) { return cosf(x); }
+#else
 FX_DEV float psin(float x) { return pinned_sincos(x, 0); }
 FX_DEV float pcos(float x) { return pinned_sincos(x, 1); }
+#endif
 
 // ---------------------------------------------------------------------------
 // WGSL builtins (spec formulas), written as the same comparisons and operations
@@ -79,6 +87,9 @@ FX_DEV float stepv(float e, float x) { return x >= e ? 1.0f : 0.0f; }
 // (tests/native/divconst_check.c, run by tests/test_exact_division.py); other x
 // take the IEEE division. With literal edges c and r fold at compile time.
 FX_DEV float div_const(float x, float c) {
+#ifdef FX_FAST_MATH
+  return x * (1.0f / c);
+#endif
   const float r = 1.0f / c;
   const float ax = fabsf(x);
   if (ax >= 0x1p-100f && ax <= 0x1p100f) {
@@ -120,6 +131,9 @@ FX_DEV uint32_t inc(uint32_t v, uint32_t m) { return min(v + 1u, m); }
 // quotient. Having no division keeps a slow path and its call out of the sweep
 // kernels, whose pressure tails reach the subnormal range.
 FX_DEV float div6(float x) {
+#ifdef FX_FAST_MATH
+  return x * 0x1.555556p-3f;
+#endif
   const float ax = fabsf(x);
   const float r6 = 0x1.555556p-3f;  // RN(1/6)
   const float q0 = x * r6;
@@ -149,8 +163,9 @@ struct Params {
 };
 
 // Stochastic rounding to binary16 (an extension for FP16 scalar storage).
-// sr_draw is a 32-bit hash of a voxel index and a store site plus the step index
-// times 0x9E3779B9 (2^32 / golden ratio: a rank-1 sequence in time); sr_half
+// sr_draw is a 32-bit hash of a voxel index (one per voxel, shared by its store
+// sites) plus the store site times 0x85EBCA77 plus the step index times
+// 0x9E3779B9 (2^32 / golden ratio: a rank-1 sequence in time); sr_half
 // rounds a finite |v| < 65504 to the binary16 value below it (toward zero) or
 // the next one up, up when the distance from the lower one, in units of their
 // spacing, exceeds the top 24 bits of r read as a fraction. Every operation is
@@ -158,13 +173,13 @@ struct Params {
 // by the right amount on average instead of staying put, which is the bias of
 // round-to-nearest on slowly decaying smoke. Other values round to nearest.
 FX_DEV uint32_t sr_draw(uint32_t i, uint32_t site, uint32_t step) {
-  uint32_t h = i * 0x9E3779B1u + site * 0x85EBCA77u;
+  uint32_t h = i * 0x9E3779B1u;
   h ^= h >> 16;
   h *= 0x7FEB352Du;
   h ^= h >> 15;
   h *= 0x846CA68Bu;
   h ^= h >> 16;
-  return h + step * 0x9E3779B9u;
+  return h + site * 0x85EBCA77u + step * 0x9E3779B9u;
 }
 
 //

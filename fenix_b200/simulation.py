@@ -437,13 +437,13 @@ def solver_dict(st: "_lib.FxSolverSettings") -> Dict[str, Any]:
 
 def build_options(options: Optional[Mapping[str, Any]] = None, *, device: int = 0, kernels: str = "fused",
                   debug_fields: bool = False, use_graphs: bool = True, storage: str = "f32", stream: int = 0,
-                  sparse: bool = False) -> FxSimOptions:
+                  sparse: bool = False, lib=None) -> FxSimOptions:
     """CombustionVolumeSimulationOptions -> fx_sim_options. storage="f16" stores the
     scalar sets in binary16 and sparse=True runs the velocity passes on the active
     bricks only (both fused kernels only)."""
     if storage not in STORAGE:
         raise ValueError(f"unknown storage {storage!r}; expected one of {sorted(STORAGE)}")
-    lib = _lib.load()
+    lib = lib or _lib.load()
     opt = FxSimOptions()
     lib.fx_sim_options_default(ctypes.byref(opt))
     options = dict(options or {})
@@ -476,14 +476,16 @@ def build_options(options: Optional[Mapping[str, Any]] = None, *, device: int = 
 
 def createCombustionVolumeSimulation(options: Optional[Mapping[str, Any]] = None, *, device: int = 0, kernels: str = "fused",
                                      debug_fields: bool = False, use_graphs: bool = True, storage: str = "f32",
-                                     stream: int = 0, sparse: bool = False) -> CombustionVolumeSimulation:
+                                     stream: int = 0, sparse: bool = False, fast_math: bool = False) -> CombustionVolumeSimulation:
     """createCombustionVolumeSimulation.ts:50-401 on CUDA device `device`. `stream`
-    (a cudaStream_t as an integer, 0 = the simulation's own) is where it enqueues."""
-    lib = _lib.load()
+    (a cudaStream_t as an integer, 0 = the simulation's own) is where it enqueues.
+    fast_math=True uses the fast-arithmetic build (libfenixcuda_fast.so): FMA
+    contraction and CUDA's sin/cos, results stated against f64 instead of bit-exact."""
+    lib = _lib.load(fast=fast_math)
     opt = build_options(options, device=device, kernels=kernels, debug_fields=debug_fields, use_graphs=use_graphs, storage=storage,
-                        stream=stream, sparse=sparse)
+                        stream=stream, sparse=sparse, lib=lib)
     handle = ctypes.c_void_p()
-    check(lib.fx_sim_create(ctypes.byref(opt), ctypes.byref(handle)))
+    check(lib.fx_sim_create(ctypes.byref(opt), ctypes.byref(handle)), lib=lib)
     return CombustionVolumeSimulation(handle, lib)
 
 

@@ -335,20 +335,20 @@ struct SolverStats {
 };
 
 // Stochastic rounding to binary16 (extension). sr_draw is a 32-bit hash of a
-// voxel index and a store site plus the step index times 0x9E3779B9 (2^32 /
-// golden ratio); sr_half rounds a finite |v| < 65504 to the binary16 value below
+// voxel index plus the store site times 0x85EBCA77 plus the step index times
+// 0x9E3779B9 (2^32 / golden ratio); sr_half rounds a finite |v| < 65504 to the binary16 value below
 // it (toward zero) or the next one up, up when the distance from the lower one,
 // in units of their spacing, exceeds the top 24 bits of r read as a fraction.
 // Every operation is exact, so the CUDA kernels reproduce it bit for bit. Other
 // values round to nearest.
 inline uint32_t sr_draw(uint32_t i, uint32_t site, uint32_t step) {
-  uint32_t h = i * 0x9E3779B1u + site * 0x85EBCA77u;
+  uint32_t h = i * 0x9E3779B1u;
   h ^= h >> 16;
   h *= 0x7FEB352Du;
   h ^= h >> 15;
   h *= 0x846CA68Bu;
   h ^= h >> 16;
-  return h + step * 0x9E3779B9u;
+  return h + site * 0x85EBCA77u + step * 0x9E3779B9u;
 }
 
 inline float sr_half(float v, uint32_t r) {
@@ -1736,6 +1736,19 @@ int orc_set_sparse(void* hv, int on) {
   return dispatch(static_cast<Handle*>(hv), [&](auto* s) -> int {
     if (on && s->sv.mode == 1) return -1;
     s->sparse = on != 0;
+    return 0;
+  });
+}
+
+// The host clock of a simulation (createCombustionVolumeSimulation.ts:180-204):
+// the elapsed time of its first step, of its latest step and the step index, so
+// a fresh oracle can take a step in the middle of another simulation's run.
+void orc_set_clock(void* hv, double start_s, double last_elapsed_s, long step_index) {
+  dispatch(static_cast<Handle*>(hv), [&](auto* s) {
+    s->initialized = true;
+    s->start_s = start_s;
+    s->last_elapsed_s = last_elapsed_s;
+    s->step_index = step_index;
     return 0;
   });
 }

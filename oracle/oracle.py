@@ -43,6 +43,7 @@ def load() -> ctypes.CDLL:
         lib.orc_set_emit_dead_residual.argtypes = [c_void_p, c_int]
         lib.orc_set_half_storage.argtypes = [c_void_p, c_int]
         lib.orc_set_half_rounding.argtypes = [c_void_p, c_int]
+        lib.orc_set_clock.argtypes = [c_void_p, c_double, c_double, c_long]
         lib.orc_sr_half_array.argtypes = [POINTER(c_float), POINTER(c_float), c_long, c_uint32, c_uint32]
         lib.orc_set_sparse.restype = c_int
         lib.orc_set_sparse.argtypes = [c_void_p, c_int]
@@ -171,6 +172,11 @@ class OracleSimulation:
         out = np.empty_like(x)
         load().orc_sr_half_array(x.ctypes.data_as(POINTER(c_float)), out.ctypes.data_as(POINTER(c_float)), x.size, site, step)
         return out
+
+    def setClock(self, start: float, lastElapsed: float, stepIndex: int) -> None:
+        """The host clock (elapsed time of the first and the latest step, step index),
+        so this oracle can take a step in the middle of another simulation's run."""
+        self._lib.orc_set_clock(self._h, float(start), float(lastElapsed), int(stepIndex))
 
     def setHalfRounding(self, mode: str) -> None:
         """Rounding of the binary16 scalar stores: "nearest" or "stochastic"."""

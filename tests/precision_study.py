@@ -12,6 +12,8 @@ Legs:
   f32                 fused step, f32 storage
   f16_sparse          the same in sparse mode (velocity passes on the active bricks only)
   f32_sparse
+  f16_fast            f16 on the fast-arithmetic build (FMA contraction, CUDA sin/cos)
+  f16_sparse_fast
   f32_once_f16        f32 storage, the start state's scalars rounded to binary16 once
   f32_perturbed       f32 storage, the start state's scalars multiplied once by
                       (1 + 2^-12 u), u uniform in [-1, 1] (seeded)
@@ -44,7 +46,7 @@ FIELDS = ("density", "temperature", "fuel", "reaction", "velocity_x", "velocity_
 SCALARS = ("density", "temperature", "fuel", "reaction")
 VCYCLE = {"mode": "vcycle", "levels": 5, "preSweeps": 4, "postSweeps": 4, "coarseSweeps": 20, "maxCycles": 30,
           "warmStart": True, "omega": 2.0 / 3.0, "tolerance": 1e-5}
-LEGS = ("f16", "f16_nearest", "f32", "f32_once_f16", "f32_perturbed", "f16_sparse", "f32_sparse")
+LEGS = ("f16", "f16_nearest", "f32", "f32_once_f16", "f32_perturbed", "f16_sparse", "f32_sparse", "f16_fast", "f16_sparse_fast")
 
 
 def errors(got: np.ndarray, ref: np.ndarray) -> dict:
@@ -86,12 +88,13 @@ def main() -> int:
 
     orc_mod.set_threads(args.threads)
     wl = workloads.plume_256(size=args.size)
-    if args.solver == "vcycle" and any(l.endswith("_sparse") for l in legs):
+    if args.solver == "vcycle" and any("_sparse" in l for l in legs):
         raise SystemExit("sparse mode has no V-cycle form")
     sims = {}
     for leg in legs:
         storage = "f16-nearest" if leg.startswith("f16_nearest") else ("f16" if leg.startswith("f16") else "f32")
-        s = createCombustionVolumeSimulation(wl.options, device=0, storage=storage, sparse=leg.endswith("_sparse"))
+        sparse = "_sparse" in leg
+        s = createCombustionVolumeSimulation(wl.options, device=0, storage=storage, sparse=sparse, fast_math=leg.endswith("_fast"))
         s.updateSources(wl.sources)
         if args.solver == "vcycle":
             s.setSolver(VCYCLE)
@@ -99,7 +102,7 @@ def main() -> int:
         sims[leg] = s
     refs_sim = {}
     for name, sparse in (("f64", False), ("f64_sparse", True)):
-        if sparse and not any(l.endswith("_sparse") for l in legs):
+        if sparse and not any("_sparse" in l for l in legs):
             continue
         ref = OracleSimulation(wl.options, precision=64)
         ref.updateSources(wl.sources)
@@ -133,7 +136,7 @@ def main() -> int:
         for leg, s in sims.items():
             got = {f: s.readField(f) for f in FIELDS}
             row[leg] = {f: errors(got[f], fields_of["f64"][f]) for f in FIELDS}
-            if leg.endswith("_sparse"):
+            if "_sparse" in leg:
                 row[leg + " vs f64_sparse"] = {f: errors(got[f], fields_of["f64_sparse"][f]) for f in FIELDS}
         out["at"][str(mark)] = row
         out["cycles"][str(mark)] = dict(cycles)
