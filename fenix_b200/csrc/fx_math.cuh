@@ -283,9 +283,15 @@ FX_DEV float source_feather(const Params& P, float r) {
   return mx(r * 0.24f, voxel_width * 3.0f);
 }
 FX_DEV float source_outer_limit(const Params& P, float r) { return r + source_feather(P, r); }
+// The emitter hash fract(sin(dot(p, (127.1, 311.7, 74.7))) * 43758.5453) turns
+// the last bit of its sine into about 2^-9 of output, so it is always evaluated
+// with the pinned sine and with products and sums that are never contracted into
+// FMA (the _rn intrinsics): the fast-arithmetic build keeps the same hash values
+// (the same lattice noise) as the parity build and the oracle.
 FX_DEV float hash31(float x, float y, float z) {
-  const float d = x * 127.1f + y * 311.7f + z * 74.7f;
-  return fractv(psin(d) * 43758.5453123f);
+  const float d = __fadd_rn(__fadd_rn(__fmul_rn(x, 127.1f), __fmul_rn(y, 311.7f)), __fmul_rn(z, 74.7f));
+  const float v = __fmul_rn(pinned_sincos(d, 0), 43758.5453123f);
+  return __fsub_rn(v, floorf(v));
 }
 FX_DEV float value_noise3(float px, float py, float pz) {
   const float cx = floorf(px), cy = floorf(py), cz = floorf(pz);
