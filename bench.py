@@ -720,6 +720,13 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu, parity, error = cpu_baseline_and_parity(args, wl, counts, args.kernels, args.storage, args.sparse)
 
+    # the same-storage ratios to the CPU baseline: the headline and the f32 fused
+    # step (the CPU port stores f32)
+    cpu_ratios = None
+    if cpu:
+        cpu_ratios = {"headline_over_cpu": value / cpu["value"], "headline_e2e_over_cpu": (e2e or {}).get("value", 0.0) / cpu["value"]}
+        if "f32_fused" in compare:
+            cpu_ratios["f32_fused_over_cpu"] = compare["f32_fused"]["value"] / cpu["value"]
     if pg:
         pg.barrier()
     if rank == 0:
@@ -730,12 +737,13 @@ def main():
             "config": {
                 "workload": f"plume_{args.size}: {args.size}^3 grid, 4 floor plumes (scalar+velocity+igniter each), seeded "
                             f"developed-plume start, 4/4/4/4/20 sweeps, dt 1/60, f32 arithmetic, {args.storage} scalar storage, "
-                            f"reference semantics",
+                            + ("sparse mode (velocity passes on the active bricks)" if args.sparse else "reference semantics"),
+                "sparse": args.sparse,
                 "kernels": args.kernels, "scalar_storage": args.storage, "autotune": tuned, "cuda_graph": bool(st_timed.get("graphReplay")), "active_fraction": active_mean / n, "global_batch": world, "seq_len": 0,
                 "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (about 2 GB of fields per step)",
             },
             "roofline": roofline, "kernels": kernel_table, "cpu_baseline": cpu, "parity_full_size": parity, "e2e": e2e,
-            "compare": compare, "error_vs_f64": error, "batch_c3": batch_c3, "adjoint_c4": adjoint,
+            "compare": compare, "cpu_ratios": cpu_ratios, "error_vs_f64": error, "batch_c3": batch_c3, "adjoint_c4": adjoint,
             "gpu_launches": int(kernels_last * args.steps), "clocks": clock_info,
         }
         print(json.dumps(line))

@@ -109,9 +109,16 @@ FX_DEV SpVoxel sp_voxel(const Dims& dm, const BrickCtx& c, int j) {
   return v;
 }
 
+// Column walk of the sparse kernels below: a block of 256 threads takes four list
+// entries at a time, and thread t takes the (x, y) column (t & 7, (t >> 3) & 7) of
+// entry 4 * block + (t >> 6) and its 8 z, so a brick's decoding and tests serve 8
+// voxels and z neighbours stay in registers. A warp holds four rows of one brick.
+constexpr uint32_t kSpColBricks = 4;
+
 // advect-velocity-semilagrangian.wgsl.ts:23-41 in computed bricks, over
 // vCurrent clamped to +-80/dx on read (advect_velocity_column<true>'s
-// arithmetic); 0 in zeroed bricks.
+// arithmetic); 0 in zeroed bricks. The next voxel's velocity is loaded before
+// the current voxel's 24 gathers are issued.
 __global__ void __launch_bounds__(kBrickThreads) k_sp_advect_velocity(Dims dm, uint3 bc, const Params* __restrict__ Pp, VelField src,
                                                                       VelField dst, const uint32_t* __restrict__ list,
                                                                       const uint32_t* __restrict__ count) {
@@ -119,29 +126,44 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_advect_velocity(Dims dm, u
   const float lim = speed_limit(*Pp);
   const float damp = 1.0f - dt * 0.025f;
   const uint32_t n = *count;
-  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+  const uint32_t lx = threadIdx.x & 7u, ly = (threadIdx.x >> 3) & 7u;
+  const uint32_t sz = dm.w * dm.h;
+  for (uint32_t li = blockIdx.x * kSpColBricks + (threadIdx.x >> 6); li < n; li += gridDim.x * kSpColBricks) {
     const uint32_t e = list[li];
-    const bool comp = (e & kSpCompute) != 0u;
     const BrickCtx c = sp_ctx(dm, e);
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const SpVoxel v = sp_voxel(dm, c, j);
-      if (!v.inside) continue;
+    const uint32_t x = c.x0 + lx, y = c.y0 + ly;
+    if (x >= dm.w || y >= dm.h) continue;
+    const uint32_t ze = min(c.z0 + 8u, dm.d);
+    uint32_t i = x + dm.w * (y + dm.h * c.z0);
+    const bool xyint = (e & kSpCompute) != 0u && x > 0u && y > 0u && x < dm.w - 1u && y < dm.h - 1u;
+    if (!xyint) {
+      for (uint32_t z = c.z0; z < ze; ++z, i += sz) {
+        dst.c[0][i] = 0.0f;
+        dst.c[1][i] = 0.0f;
+        dst.c[2][i] = 0.0f;
+      }
+      continue;
+    }
+    float ax = __ldg(src.c[0] + i), ay = __ldg(src.c[1] + i), az = __ldg(src.c[2] + i);
+    for (uint32_t z = c.z0; z < ze; ++z, i += sz) {
+      const uint32_t in = z + 1u < ze ? i + sz : i;
+      const float nx = __ldg(src.c[0] + in), ny = __ldg(src.c[1] + in), nz = __ldg(src.c[2] + in);
       float ox = 0.f, oy = 0.f, oz = 0.f;
-      if (comp && !is_boundary(dm, v.x, v.y, v.z)) {
-        const float cx = (float)v.x + 0.5f, cy = (float)v.y + 0.5f, cz = (float)v.z + 0.5f;
-        const float v0x = clampv(__ldg(src.c[0] + v.i), -lim, lim);
-        const float v0y = clampv(__ldg(src.c[1] + v.i), -lim, lim);
-        const float v0z = clampv(__ldg(src.c[2] + v.i), -lim, lim);
+      if (z > 0u && z < dm.d - 1u) {
+        const float cx = (float)x + 0.5f, cy = (float)y + 0.5f, cz = (float)z + 0.5f;
+        const float v0x = clampv(ax, -lim, lim), v0y = clampv(ay, -lim, lim), v0z = clampv(az, -lim, lim);
         const float bx = cx - v0x * dt, by = cy - v0y * dt, bz = cz - v0z * dt;
         const Tri c1 = tri_corners(dm, bx - 0.5f, by - 0.5f, bz - 0.5f);
         ox = tri_interp_clamped(src.c[0], c1, lim) * damp;
         oy = tri_interp_clamped(src.c[1], c1, lim) * damp;
         oz = tri_interp_clamped(src.c[2], c1, lim) * damp;
       }
-      dst.c[0][v.i] = ox;
-      dst.c[1][v.i] = oy;
-      dst.c[2][v.i] = oz;
+      dst.c[0][i] = ox;
+      dst.c[1][i] = oy;
+      dst.c[2][i] = oz;
+      ax = nx;
+      ay = ny;
+      az = nz;
     }
   }
 }
@@ -176,7 +198,9 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_vorticity(Dims dm, uint3 b
 
 // apply-vorticity-confinement.wgsl.ts:30-66 in computed bricks (k_confinement's
 // arithmetic, out = vScratch + F dt clamped); the boundary passes vScratch
-// through, and zeroed bricks get 0 (vScratch is 0 there).
+// through, and zeroed bricks get 0 (vScratch is 0 there). Column walk: the z
+// neighbours of |w|, vx and vy (the gradient's and the curl's z terms) stay in
+// registers; each voxel's values and operations are k_confinement's.
 template <typename S, bool FMAG>
 __global__ void __launch_bounds__(kBrickThreads) k_sp_confinement(Dims dm, uint3 bc, const Params* __restrict__ Pp, VelField v,
                                                                   const float* __restrict__ wmag, SSet<S> set, const uint8_t* __restrict__ nz,
@@ -185,51 +209,76 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_confinement(Dims dm, uint3
   const Params P = *Pp;
   const uint32_t n = *count;
   const uint32_t sy = dm.w, sz = dm.w * dm.h;
-  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+  const uint32_t lx = threadIdx.x & 7u, ly = (threadIdx.x >> 3) & 7u;
+  for (uint32_t li = blockIdx.x * kSpColBricks + (threadIdx.x >> 6); li < n; li += gridDim.x * kSpColBricks) {
     const uint32_t e = list[li];
-    const bool comp = (e & kSpCompute) != 0u;
     const BrickCtx c = sp_ctx(dm, e);
-    const uint32_t b = sp_brick_index(bc, c);
-    const bool scal = __ldg(nz + b) != 0;
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const SpVoxel q = sp_voxel(dm, c, j);
-      if (!q.inside) continue;
-      if (!comp) {
-        out.c[0][q.i] = 0.0f;
-        out.c[1][q.i] = 0.0f;
-        out.c[2][q.i] = 0.0f;
-        if (FMAG) fmag[q.i] = 0.0f;
-        continue;
+    const uint32_t x = c.x0 + lx, y = c.y0 + ly;
+    if (x >= dm.w || y >= dm.h) continue;
+    const uint32_t ze = min(c.z0 + 8u, dm.d);
+    uint32_t i = x + dm.w * (y + dm.h * c.z0);
+    if (!(e & kSpCompute)) {
+      for (uint32_t z = c.z0; z < ze; ++z, i += sz) {
+        out.c[0][i] = 0.0f;
+        out.c[1][i] = 0.0f;
+        out.c[2][i] = 0.0f;
+        if (FMAG) fmag[i] = 0.0f;
       }
-      float vx = __ldg(v.c[0] + q.i), vy = __ldg(v.c[1] + q.i), vz = __ldg(v.c[2] + q.i);
-      if (is_boundary(dm, q.x, q.y, q.z)) {
-        out.c[0][q.i] = vx;
-        out.c[1][q.i] = vy;
-        out.c[2][q.i] = vz;
-        if (FMAG) fmag[q.i] = 0.0f;
-        continue;
+      continue;
+    }
+    const bool xyint = x > 0u && y > 0u && x < dm.w - 1u && y < dm.h - 1u;
+    if (!xyint) {  // boundary column: vScratch passes through
+      for (uint32_t z = c.z0; z < ze; ++z, i += sz) {
+        out.c[0][i] = __ldg(v.c[0] + i);
+        out.c[1][i] = __ldg(v.c[1] + i);
+        out.c[2][i] = __ldg(v.c[2] + i);
+        if (FMAG) fmag[i] = 0.0f;
       }
-      const uint32_t i = q.i;
-      const float gx = (__ldg(wmag + i + 1u) - __ldg(wmag + i - 1u)) * 0.5f;
-      const float gy = (__ldg(wmag + i + sy) - __ldg(wmag + i - sy)) * 0.5f;
-      const float gz = (__ldg(wmag + i + sz) - __ldg(wmag + i - sz)) * 0.5f;
-      float wx, wy, wz;
-      curl_at(v, i, sy, sz, wx, wy, wz);
-      float d = 0.f, t = 0.f, r = 0.f;
-      if (scal) {
-        d = ldS(set.f[0], i);
-        t = ldS(set.f[1], i);
-        r = ldS(set.f[3], i);
-      }
-      if (FMAG) {
-        fmag[i] = confinement_voxel(P, gx, gy, gz, wx, wy, wz, __ldg(wmag + i), d, t, r, vx, vy, vz);
+      continue;
+    }
+    const bool scal = __ldg(nz + sp_brick_index(bc, c)) != 0;
+    // planes z - 1, z, z + 1 of |w|, vx and vy (reads at z - 1 < 0 or z + 1 >= d are never used)
+    auto at = [&](const float* f, uint32_t z) { return z < dm.d ? __ldg(f + x + dm.w * (y + dm.h * z)) : 0.0f; };
+    float wm = c.z0 > 0u ? at(wmag, c.z0 - 1u) : 0.0f, w0 = at(wmag, c.z0);
+    float xm = c.z0 > 0u ? at(v.c[0], c.z0 - 1u) : 0.0f, x0 = at(v.c[0], c.z0);
+    float ym = c.z0 > 0u ? at(v.c[1], c.z0 - 1u) : 0.0f, y0 = at(v.c[1], c.z0);
+    for (uint32_t z = c.z0; z < ze; ++z, i += sz) {
+      const float wp = at(wmag, z + 1u), xp = at(v.c[0], z + 1u), yp = at(v.c[1], z + 1u);
+      float vx = x0, vy = y0, vz = __ldg(v.c[2] + i);
+      if (z == 0u || z == dm.d - 1u) {
+        out.c[0][i] = vx;
+        out.c[1][i] = vy;
+        out.c[2][i] = vz;
+        if (FMAG) fmag[i] = 0.0f;
       } else {
-        confinement_voxel_v(P, gx, gy, gz, wx, wy, wz, __ldg(wmag + i), d, t, r, vx, vy, vz);
+        const float gx = (__ldg(wmag + i + 1u) - __ldg(wmag + i - 1u)) * 0.5f;
+        const float gy = (__ldg(wmag + i + sy) - __ldg(wmag + i - sy)) * 0.5f;
+        const float gz = (wp - wm) * 0.5f;
+        // curl_at with the z terms from the column
+        const float wx = ((__ldg(v.c[2] + i + sy) - __ldg(v.c[2] + i - sy)) - (yp - ym)) * 0.5f;
+        const float wy = ((xp - xm) - (__ldg(v.c[2] + i + 1u) - __ldg(v.c[2] + i - 1u))) * 0.5f;
+        const float wz = ((__ldg(v.c[1] + i + 1u) - __ldg(v.c[1] + i - 1u)) - (__ldg(v.c[0] + i + sy) - __ldg(v.c[0] + i - sy))) * 0.5f;
+        float d = 0.f, t = 0.f, r = 0.f;
+        if (scal) {
+          d = ldS(set.f[0], i);
+          t = ldS(set.f[1], i);
+          r = ldS(set.f[3], i);
+        }
+        if (FMAG) {
+          fmag[i] = confinement_voxel(P, gx, gy, gz, wx, wy, wz, w0, d, t, r, vx, vy, vz);
+        } else {
+          confinement_voxel_v(P, gx, gy, gz, wx, wy, wz, w0, d, t, r, vx, vy, vz);
+        }
+        out.c[0][i] = vx;
+        out.c[1][i] = vy;
+        out.c[2][i] = vz;
       }
-      out.c[0][i] = vx;
-      out.c[1][i] = vy;
-      out.c[2][i] = vz;
+      wm = w0;
+      w0 = wp;
+      xm = x0;
+      x0 = xp;
+      ym = y0;
+      y0 = yp;
     }
   }
 }
