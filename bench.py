@@ -700,6 +700,14 @@ def main():
             r["ratio"] = value / r["value"]
             compare[f"{storage}_{kernels}_vcycle"] = r
         compare["c2_mixed_over_plain_f32"] = compare["f16_fused_vcycle"]["value"] / compare["f32_plain_vcycle"]["value"]
+        # config C1's solver: a fixed schedule of one 5-level V-cycle per step
+        # (4 pre-, 4 post-sweeps, 20 on the coarsest level), plain FP32 kernels,
+        # with the mixed-storage fused step on the same schedule beside it
+        c1 = {"mode": "vcycle", "levels": 5, "maxCycles": 1, "tolerance": 0.0}
+        for kernels, storage in (("plain", "f32"), ("fused", "f16")):
+            r = time_steps(args, wl, local, kernels, storage, pg, solver=c1)
+            r["ratio"] = value / r["value"]
+            compare[f"{storage}_{kernels}_vcycle5_fixed"] = r
         # sparse mode (extension): the velocity passes on the active bricks only;
         # and the fast-arithmetic build (FMA contraction, CUDA sin/cos; not bit-exact)
         for storage in ("f16", "f32"):

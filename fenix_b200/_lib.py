@@ -247,6 +247,9 @@ PROTOTYPES = [
     ("fx_sim_field_size", c_int32, [c_void_p, c_int32, POINTER(c_size_t)]),
     ("fx_sim_read_field", c_int32, [c_void_p, c_int32, c_void_p, c_size_t]),
     ("fx_sim_write_field", c_int32, [c_void_p, c_int32, c_void_p, c_size_t]),
+    ("fx_sim_state_bytes", c_int32, [c_void_p, POINTER(c_uint64)]),
+    ("fx_sim_save_state", c_int32, [c_void_p, c_void_p, c_uint64]),
+    ("fx_sim_load_state", c_int32, [c_void_p, c_void_p, c_uint64]),
     ("fx_sim_synchronize", c_int32, [c_void_p]),
     ("fx_sim_get_stats", c_int32, [c_void_p, POINTER(FxStats)]),
     ("fx_sim_set_instrumentation", c_int32, [c_void_p, c_uint32]),

@@ -1038,6 +1038,118 @@ fx_status fx_sim_write_field(fx_sim* s, int32_t id, const void* src, size_t byte
   return fused_invalidate(s->fw, s->stream);
 }
 
+namespace {
+
+// The saved state's layout: this header, then the current scalar set as stored
+// (4 fields of n elements of scalar_bytes each), the velocity (3 f32 fields),
+// the fine pressure of the latest solve (n f32) and the brick flags of the
+// current and the other set (2 x nb u32), each part starting on 16 bytes.
+struct StateHeader {
+  uint32_t magic;
+  uint32_t version;
+  uint32_t w, h, d;
+  uint32_t scalar_bytes;
+  int32_t cur, last_p;
+  int64_t step_index;
+  double start_s, last_elapsed_s;
+  uint32_t initialized, reserved;
+};
+constexpr uint32_t kStateMagic = 0x54535846u;  // "FXST"
+constexpr uint32_t kStateVersion = 1;
+
+size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
+
+struct StateLayout {
+  size_t scalar, vel, pressure, flags, total;
+};
+
+StateLayout state_layout(const fx_sim* s) {
+  StateLayout L;
+  const size_t es = s->half ? sizeof(__half) : sizeof(float);
+  L.scalar = align16(sizeof(StateHeader));
+  L.vel = L.scalar + 4 * align16(s->n * es);
+  L.pressure = L.vel + 3 * align16(s->n * sizeof(float));
+  L.flags = L.pressure + align16(s->n * sizeof(float));
+  L.total = L.flags + 2 * align16(s->nb * sizeof(uint32_t));
+  return L;
+}
+
+}  // namespace
+
+fx_status fx_sim_state_bytes(fx_sim* s, uint64_t* bytes) {
+  if (!s || !bytes) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_state_bytes: NULL argument");
+  *bytes = state_layout(s).total;
+  return FX_OK;
+}
+
+fx_status fx_sim_save_state(fx_sim* s, void* dst, uint64_t bytes) {
+  if (!s || !dst) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_save_state: NULL argument");
+  if (!s->err.empty()) return FX_ERR_STATE;
+  const StateLayout L = state_layout(s);
+  if (bytes != L.total) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_save_state: byte count does not match fx_sim_state_bytes");
+  FX_CUDA(s, cudaSetDevice(s->device));
+  StateHeader h{};
+  h.magic = kStateMagic;
+  h.version = kStateVersion;
+  h.w = s->dm.w, h.h = s->dm.h, h.d = s->dm.d;
+  h.scalar_bytes = s->half ? 2 : 4;
+  h.cur = s->cur, h.last_p = s->last_p;
+  h.step_index = s->step_index;
+  h.start_s = s->start_s, h.last_elapsed_s = s->last_elapsed_s;
+  h.initialized = s->initialized ? 1u : 0u;
+  char* o = static_cast<char*>(dst);
+  const size_t sb = s->n * (size_t)h.scalar_bytes, fb = s->n * sizeof(float), gb = s->nb * sizeof(uint32_t);
+  FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  FX_CUDA(s, cudaMemcpy(o, &h, sizeof h, cudaMemcpyDefault));
+  for (int k = 0; k < 4; ++k)
+    FX_CUDA(s, cudaMemcpyAsync(o + L.scalar + k * align16(sb), s->sets[s->cur].f[k], sb, cudaMemcpyDefault, s->stream));
+  for (int k = 0; k < 3; ++k)
+    FX_CUDA(s, cudaMemcpyAsync(o + L.vel + k * align16(fb), s->vcur.c[k], fb, cudaMemcpyDefault, s->stream));
+  FX_CUDA(s, cudaMemcpyAsync(o + L.pressure, s->lv[0].p[s->last_p], fb, cudaMemcpyDefault, s->stream));
+  for (int k = 0; k < 2; ++k)
+    FX_CUDA(s, cudaMemcpyAsync(o + L.flags + k * align16(gb), s->flags[s->cur ^ k], gb, cudaMemcpyDefault, s->stream));
+  FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  return FX_OK;
+}
+
+fx_status fx_sim_load_state(fx_sim* s, const void* src, uint64_t bytes) {
+  if (!s || !src) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: NULL argument");
+  if (!s->err.empty()) return FX_ERR_STATE;
+  const StateLayout L = state_layout(s);
+  if (bytes != L.total) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: byte count does not match fx_sim_state_bytes");
+  FX_CUDA(s, cudaSetDevice(s->device));
+  StateHeader h{};
+  FX_CUDA(s, cudaMemcpy(&h, src, sizeof h, cudaMemcpyDefault));
+  if (h.magic != kStateMagic || h.version != kStateVersion)
+    return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: not a saved state of this version");
+  if (h.w != s->dm.w || h.h != s->dm.h || h.d != s->dm.d || h.scalar_bytes != (s->half ? 2u : 4u))
+    return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: the state has another resolution or scalar storage");
+  if ((h.cur != 0 && h.cur != 1) || (h.last_p != 0 && h.last_p != 1) || h.step_index < 0)
+    return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: corrupt header");
+  // doReset's clears (a superset), then the saved parts
+  fx_status st = zero_state(s);
+  if (st != FX_OK) return st;
+  if ((st = fused_reset(s->fw, s->stream)) != FX_OK) return st;
+  s->cur = h.cur;
+  s->last_p = h.last_p;
+  s->step_index = h.step_index;
+  s->start_s = h.start_s;
+  s->last_elapsed_s = h.last_elapsed_s;
+  s->initialized = h.initialized != 0;
+  const char* in = static_cast<const char*>(src);
+  const size_t sb = s->n * (size_t)h.scalar_bytes, fb = s->n * sizeof(float), gb = s->nb * sizeof(uint32_t);
+  for (int k = 0; k < 4; ++k)
+    FX_CUDA(s, cudaMemcpyAsync(s->sets[s->cur].f[k], in + L.scalar + k * align16(sb), sb, cudaMemcpyDefault, s->stream));
+  for (int k = 0; k < 3; ++k)
+    FX_CUDA(s, cudaMemcpyAsync(s->vcur.c[k], in + L.vel + k * align16(fb), fb, cudaMemcpyDefault, s->stream));
+  FX_CUDA(s, cudaMemcpyAsync(s->lv[0].p[s->last_p], in + L.pressure, fb, cudaMemcpyDefault, s->stream));
+  for (int k = 0; k < 2; ++k)
+    FX_CUDA(s, cudaMemcpyAsync(s->flags[s->cur ^ k], in + L.flags + k * align16(gb), gb, cudaMemcpyDefault, s->stream));
+  if ((st = fused_invalidate(s->fw, s->stream)) != FX_OK) return st;
+  FX_CUDA(s, cudaStreamSynchronize(s->stream));
+  return FX_OK;
+}
+
 fx_status fx_sim_synchronize(fx_sim* s) {
   if (!s) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_synchronize: NULL handle");
   FX_CUDA(s, cudaSetDevice(s->device));

@@ -171,21 +171,21 @@ class CombustionVolumeSimulation:
         self._lib = lib
         self._owned = owned  # False for the members of a batch, which the batch destroys
         w, h, d = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
-        check(lib.fx_sim_get_resolution(self._h, ctypes.byref(w), ctypes.byref(h), ctypes.byref(d)), self._h)
+        check(lib.fx_sim_get_resolution(self._h, ctypes.byref(w), ctypes.byref(h), ctypes.byref(d)), self._h, self._lib)
         self.resolution = {"width": w.value, "height": h.value, "depth": d.value}
 
     # -- CombustionVolumeSimulation --------------------------------------------
     def step(self, elapsedSeconds: float, stepSeconds: float) -> None:
-        check(self._lib.fx_sim_step(self._h, float(elapsedSeconds), float(stepSeconds)), self._h)
+        check(self._lib.fx_sim_step(self._h, float(elapsedSeconds), float(stepSeconds)), self._h, self._lib)
 
     def getRenderBuffers(self) -> Dict[str, Any]:
         rb = FxRenderBuffers()
-        check(self._lib.fx_sim_get_render_buffers(self._h, ctypes.byref(rb)), self._h)
+        check(self._lib.fx_sim_get_render_buffers(self._h, ctypes.byref(rb)), self._h, self._lib)
         return _pointer_dict(rb)
 
     def getDebugBuffers(self) -> Dict[str, Any]:
         db = FxDebugBuffers()
-        check(self._lib.fx_sim_get_debug_buffers(self._h, ctypes.byref(db)), self._h)
+        check(self._lib.fx_sim_get_debug_buffers(self._h, ctypes.byref(db)), self._h, self._lib)
         out = _pointer_dict(db.render)
         out.update(
             velocityMagnitude=db.velocity_magnitude,
@@ -198,35 +198,35 @@ class CombustionVolumeSimulation:
 
     def getScalarAdvectionMode(self) -> str:
         m = ctypes.c_int32()
-        check(self._lib.fx_sim_get_scalar_advection_mode(self._h, ctypes.byref(m)), self._h)
+        check(self._lib.fx_sim_get_scalar_advection_mode(self._h, ctypes.byref(m)), self._h, self._lib)
         return ADVECTION_NAMES[m.value]
 
     def setScalarAdvectionMode(self, mode: str) -> None:
-        check(self._lib.fx_sim_set_scalar_advection_mode(self._h, ADVECTION_MODES[mode]), self._h)
+        check(self._lib.fx_sim_set_scalar_advection_mode(self._h, ADVECTION_MODES[mode]), self._h, self._lib)
 
     def getRuntimeParams(self) -> Dict[str, Any]:
         st = FxRuntimeParams()
-        check(self._lib.fx_sim_get_runtime_params(self._h, ctypes.byref(st)), self._h)
+        check(self._lib.fx_sim_get_runtime_params(self._h, ctypes.byref(st)), self._h, self._lib)
         return runtime_params_dict(st)
 
     def setRuntimeParams(self, params: Mapping[str, Any]) -> None:
         st, mask = runtime_params_struct(params)
-        check(self._lib.fx_sim_set_runtime_params(self._h, ctypes.byref(st), mask), self._h)
+        check(self._lib.fx_sim_set_runtime_params(self._h, ctypes.byref(st), mask), self._h, self._lib)
 
     def getQualitySettings(self) -> Dict[str, int]:
         st = FxQuality()
-        check(self._lib.fx_sim_get_quality(self._h, ctypes.byref(st)), self._h)
+        check(self._lib.fx_sim_get_quality(self._h, ctypes.byref(st)), self._h, self._lib)
         return {k: int(getattr(st, f)) for k, f in zip(QUALITY_KEYS, _QUALITY_FIELDS)}
 
     def setQualitySettings(self, settings: Mapping[str, Any]) -> None:
         st, mask = quality_struct(settings)
-        check(self._lib.fx_sim_set_quality(self._h, ctypes.byref(st), mask), self._h)
+        check(self._lib.fx_sim_set_quality(self._h, ctypes.byref(st), mask), self._h, self._lib)
 
     def updateSources(self, sources: Sequence[EmitterSource]) -> None:
         self.updatePackedSources(packEmitterSources(sources), len(sources))
 
     def reset(self) -> None:
-        check(self._lib.fx_sim_reset(self._h), self._h)
+        check(self._lib.fx_sim_reset(self._h), self._h, self._lib)
 
     def dispose(self) -> None:
         if self._h:
@@ -241,31 +241,47 @@ class CombustionVolumeSimulation:
         if arr.size != count * 32:
             raise ValueError("packed sources must hold count * 32 floats")
         ptr = arr.ctypes.data_as(ctypes.POINTER(ctypes.c_float)) if count else None
-        check(self._lib.fx_sim_update_sources(self._h, ptr, count), self._h)
+        check(self._lib.fx_sim_update_sources(self._h, ptr, count), self._h, self._lib)
 
     def readField(self, name: str) -> np.ndarray:
         """Copies one field to the host (waits for the stream). Volumes come back
         with shape (depth, height, width) of their level; flags as uint32[bricks]."""
         fid = _lib.FIELD_IDS[name]
         nbytes = ctypes.c_size_t()
-        check(self._lib.fx_sim_field_size(self._h, fid, ctypes.byref(nbytes)), self._h)
+        check(self._lib.fx_sim_field_size(self._h, fid, ctypes.byref(nbytes)), self._h, self._lib)
         dtype = np.uint32 if name in _lib.UINT_FIELDS else np.float32
         out = np.empty(nbytes.value // 4, dtype=dtype)
-        check(self._lib.fx_sim_read_field(self._h, fid, out.ctypes.data_as(ctypes.c_void_p), nbytes.value), self._h)
+        check(self._lib.fx_sim_read_field(self._h, fid, out.ctypes.data_as(ctypes.c_void_p), nbytes.value), self._h, self._lib)
         return out
 
     def writeField(self, name: str, values: np.ndarray) -> None:
         fid = _lib.FIELD_IDS[name]
         dtype = np.uint32 if name in _lib.UINT_FIELDS else np.float32
         arr = np.ascontiguousarray(values, dtype=dtype).ravel()
-        check(self._lib.fx_sim_write_field(self._h, fid, arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes), self._h)
+        check(self._lib.fx_sim_write_field(self._h, fid, arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes), self._h, self._lib)
+
+    def saveState(self) -> np.ndarray:
+        """The simulation's state as a byte array (fx_sim_save_state): the clock,
+        the current scalar set as stored, the velocity, the latest fine pressure
+        and the brick flags. Settings and sources are not part of it."""
+        n = ctypes.c_uint64()
+        check(self._lib.fx_sim_state_bytes(self._h, ctypes.byref(n)), self._h, self._lib)
+        out = np.empty(n.value, dtype=np.uint8)
+        check(self._lib.fx_sim_save_state(self._h, out.ctypes.data_as(ctypes.c_void_p), out.nbytes), self._h, self._lib)
+        return out
+
+    def loadState(self, state: np.ndarray) -> None:
+        """Restores a saveState() of a simulation with the same resolution and
+        scalar storage; the following steps repeat the saved run's bits."""
+        arr = np.ascontiguousarray(state, dtype=np.uint8).ravel()
+        check(self._lib.fx_sim_load_state(self._h, arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes), self._h, self._lib)
 
     def synchronize(self) -> None:
-        check(self._lib.fx_sim_synchronize(self._h), self._h)
+        check(self._lib.fx_sim_synchronize(self._h), self._h, self._lib)
 
     def stats(self) -> Dict[str, int]:
         st = FxStats()
-        check(self._lib.fx_sim_get_stats(self._h, ctypes.byref(st)), self._h)
+        check(self._lib.fx_sim_get_stats(self._h, ctypes.byref(st)), self._h, self._lib)
         return {
             "stepIndex": st.step_index,
             "currentScalarSet": st.current_scalar_set,
@@ -280,18 +296,18 @@ class CombustionVolumeSimulation:
     def setInstrumentation(self, kernel_times: bool = False, count_active: bool = False, solver_norms: bool = False) -> None:
         flags = ((_lib.FX_INSTR_KERNEL_TIMES if kernel_times else 0) | (_lib.FX_INSTR_COUNT_ACTIVE if count_active else 0)
                  | (_lib.FX_INSTR_SOLVER_NORMS if solver_norms else 0))
-        check(self._lib.fx_sim_set_instrumentation(self._h, flags), self._h)
+        check(self._lib.fx_sim_set_instrumentation(self._h, flags), self._h, self._lib)
 
     # -- pressure solver (extension) ---------------------------------------------
     def setSolver(self, settings: Mapping[str, Any]) -> None:
         """Partial solver settings (keys of SOLVER_DEFAULTS); the rest keep their values."""
         cur = self.getSolver()
         cur.update(settings)
-        check(self._lib.fx_sim_set_solver(self._h, ctypes.byref(solver_struct(cur))), self._h)
+        check(self._lib.fx_sim_set_solver(self._h, ctypes.byref(solver_struct(cur))), self._h, self._lib)
 
     def getSolver(self) -> Dict[str, Any]:
         st = _lib.FxSolverSettings()
-        check(self._lib.fx_sim_get_solver(self._h, ctypes.byref(st)), self._h)
+        check(self._lib.fx_sim_get_solver(self._h, ctypes.byref(st)), self._h, self._lib)
         return solver_dict(st)
 
     def autotune(self, cache: Optional[str] = None, key: Optional[str] = None) -> Dict[str, Any]:
@@ -313,7 +329,7 @@ class CombustionVolumeSimulation:
                 self.setSweepVariants(table[key]["sweepVariant"])
                 return {**table[key], "cached": True}
         r = _lib.FxAutotuneReport()
-        check(self._lib.fx_sim_autotune(self._h, ctypes.byref(r)), self._h)
+        check(self._lib.fx_sim_autotune(self._h, ctypes.byref(r)), self._h, self._lib)
         rep = {"sweepVariant": list(r.sweep_variant), "sweepUs": list(r.sweep_us), "defaultUs": list(r.default_us)}
         if cache:
             table[key] = rep
@@ -336,28 +352,28 @@ class CombustionVolumeSimulation:
     def setSweepVariants(self, variants: Sequence[int]) -> None:
         """The sweep kernel per pressure level (fine, mid, coarse); -1 keeps the default."""
         arr = (ctypes.c_int32 * 3)(*[int(v) for v in variants])
-        check(self._lib.fx_sim_set_sweep_variants(self._h, arr), None)
+        check(self._lib.fx_sim_set_sweep_variants(self._h, arr), None, self._lib)
 
     def getSweepVariants(self) -> list:
         arr = (ctypes.c_int32 * 3)()
-        check(self._lib.fx_sim_get_sweep_variants(self._h, arr), None)
+        check(self._lib.fx_sim_get_sweep_variants(self._h, arr), None, self._lib)
         return list(arr)
 
     # -- sparse mode (extension) ---------------------------------------------------
     def setSparse(self, on: bool) -> None:
         """Velocity passes on the active bricks only, zero elsewhere (FX_OPT_SPARSE),
         from the next step."""
-        check(self._lib.fx_sim_set_sparse(self._h, 1 if on else 0), self._h)
+        check(self._lib.fx_sim_set_sparse(self._h, 1 if on else 0), self._h, self._lib)
 
     def getSparse(self) -> bool:
         v = ctypes.c_int32()
-        check(self._lib.fx_sim_get_sparse(self._h, ctypes.byref(v)), self._h)
+        check(self._lib.fx_sim_get_sparse(self._h, ctypes.byref(v)), self._h, self._lib)
         return bool(v.value)
 
     def readSolverStats(self) -> Dict[str, Any]:
         """FP64 statistics of the latest solve (waits for the stream)."""
         st = _lib.FxSolverStats()
-        check(self._lib.fx_sim_read_solver_stats(self._h, ctypes.byref(st)), self._h)
+        check(self._lib.fx_sim_read_solver_stats(self._h, ctypes.byref(st)), self._h, self._lib)
         return {"rhsL2": st.rhs_l2, "residualL2": st.residual_l2, "relativeResidual": st.relative_residual,
                 "maxAbsDivergence": st.max_abs_divergence, "cycles": st.cycles, "converged": bool(st.converged)}
 
@@ -366,19 +382,19 @@ class CombustionVolumeSimulation:
         cap = 64
         arr = (_lib.FxKernelTime * cap)()
         n = ctypes.c_uint32()
-        check(self._lib.fx_sim_read_kernel_times(self._h, arr, cap, ctypes.byref(n)), self._h)
+        check(self._lib.fx_sim_read_kernel_times(self._h, arr, cap, ctypes.byref(n)), self._h, self._lib)
         return {arr[i].name.decode(): {"launches": arr[i].launches, "total_ms": arr[i].total_ms} for i in range(min(n.value, cap))}
 
     def readActiveCounters(self) -> Dict[str, int]:
         """Active brick-steps and voxel-steps since the last call (waits for the stream)."""
         b, v = ctypes.c_uint64(), ctypes.c_uint64()
-        check(self._lib.fx_sim_read_active_counters(self._h, ctypes.byref(b), ctypes.byref(v)), self._h)
+        check(self._lib.fx_sim_read_active_counters(self._h, ctypes.byref(b), ctypes.byref(v)), self._h, self._lib)
         return {"brickSteps": b.value, "voxelSteps": v.value}
 
     @property
     def stream(self) -> int:
         s = ctypes.c_void_p()
-        check(self._lib.fx_sim_get_stream(self._h, ctypes.byref(s)), self._h)
+        check(self._lib.fx_sim_get_stream(self._h, ctypes.byref(s)), self._h, self._lib)
         return s.value or 0
 
     def __del__(self):  # pragma: no cover - interpreter shutdown order

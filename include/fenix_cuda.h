@@ -272,6 +272,22 @@ fx_status fx_sim_field_size(fx_sim* sim, int32_t field_id, size_t* bytes);
 fx_status fx_sim_read_field(fx_sim* sim, int32_t field_id, void* host_dst, size_t bytes);
 fx_status fx_sim_write_field(fx_sim* sim, int32_t field_id, const void* host_src, size_t bytes);
 
+/* Saved state (extension). The state is what doReset of
+ * createCombustionVolumeSimulation.ts:206-226 re-initialises and the next step
+ * reads: the host clock (current scalar set, step index, start and last elapsed
+ * seconds, the initialized flag, the latest pressure buffer), the current scalar
+ * set as stored (f32 or binary16), the velocity, the fine pressure of the latest
+ * solve (the V-cycle's warm start) and the brick flags of both sets. Settings
+ * (quality, runtime parameters, sources, solver, kernels) are not part of it.
+ * fx_sim_state_bytes gives the size of the blob; save copies it to `dst` (host
+ * or device memory, waits for the stream). Load accepts a blob of a simulation
+ * with the same resolution and scalar storage (else FX_ERR_INVALID_ARGUMENT and
+ * the simulation is unchanged), clears everything else as fx_sim_reset does, and
+ * the steps that follow give the same bits as the steps that followed the save. */
+fx_status fx_sim_state_bytes(fx_sim* sim, uint64_t* bytes);
+fx_status fx_sim_save_state(fx_sim* sim, void* dst, uint64_t bytes);
+fx_status fx_sim_load_state(fx_sim* sim, const void* src, uint64_t bytes);
+
 /* Waits until all enqueued work of the simulation has finished. */
 fx_status fx_sim_synchronize(fx_sim* sim);
 
@@ -318,8 +334,10 @@ const char* fx_sim_last_error(fx_sim* sim);
  * right-hand side 4 x the mean of the 8 fine residuals, the reference's
  * trilinear prolongation. It stops when ||div - A p||_2 <= tolerance * ||div||_2
  * (both FP64, on the device) or after max_cycles cycles, and can start from the
- * previous step's pressure. Fused kernels only. Under CUDA graphs the loop is a
- * conditional WHILE node decided on the device. */
+ * previous step's pressure. Both kernel paths: the fused one's loop is a
+ * conditional WHILE node decided on the device under CUDA graphs; the plain
+ * one's is a host loop over one-voxel kernels. tolerance 0 with max_cycles N
+ * is a fixed schedule of N cycles per step. Not in sparse mode. */
 #define FX_SOLVER_REFERENCE 0
 #define FX_SOLVER_VCYCLE 1
 
