@@ -405,6 +405,7 @@ def run_batch_c3(args, local, rank, world, pg):
         sim.setInstrumentation(count_active=True)
         if not args.no_autotune:
             sim.autotune()  # sweeps per level, chosen per simulation size
+            sim.autotuneBricks(dt, steps=2)  # CTAs per SM of the brick kernels
     bstream = torch.cuda.ExternalStream(batch.stream, device=dev)
     batched = timed(lambda t: batch.step(t, dt), bstream, batch.sims)
     batch.dispose()
@@ -578,7 +579,13 @@ def main():
     # The autotuner runs before the warm-up: its choice enters the step's
     # CUDA-graph key, so the warm-up steps capture the graphs (both ping-pong
     # parities) that the timed steps replay.
-    tuned = None if args.no_autotune or args.kernels != "fused" else sim.autotune()
+    tuned = None
+    if not args.no_autotune and args.kernels == "fused":
+        tuned = sim.autotune()  # sweep kernel per pressure level
+        # CTAs per SM of each brick kernel, timed on a clone from the start state:
+        # {kernel: [chosen, us per step, us per step at the default 8]}
+        tuned["brickCtas"] = {k: [v["ctasPerSM"], round(v["us"], 2), round(v["defaultUs"], 2)]
+                              for k, v in sim.autotuneBricks(wl.dt, steps=4).items() if v["defaultUs"] > 0}
     for _ in range(args.warmup):
         sim.step(t, wl.dt)
         t += wl.dt

@@ -176,6 +176,14 @@ class FxAutotuneReport(Structure):
     _fields_ = [("sweep_variant", c_int32 * 3), ("sweep_us", c_float * 3), ("default_us", c_float * 3)]
 
 
+BRICK_KERNELS = ("inject", "advect_scalars", "combustion", "buoyancy", "sparse_advect_velocity", "sparse_vorticity",
+                 "sparse_confinement", "sparse_div_first_sweep", "sparse_sweep", "sparse_prolong_fine", "sparse_project")
+
+
+class FxBrickTuneReport(Structure):
+    _fields_ = [("ctas_per_sm", c_int32 * 11), ("us", c_float * 11), ("default_us", c_float * 11)]
+
+
 class FxRolloutDesc(Structure):
     _fields_ = [("struct_size", c_uint32), ("steps", c_uint32), ("checkpoint_interval", c_uint32), ("reserved0", c_uint32),
                 ("start_elapsed", c_double), ("step_seconds", c_double), ("inflow_x0", c_uint32), ("inflow_y", c_uint32),
@@ -266,6 +274,9 @@ PROTOTYPES = [
     ("fx_sim_autotune", c_int32, [c_void_p, POINTER(FxAutotuneReport)]),
     ("fx_sim_set_sweep_variants", c_int32, [c_void_p, POINTER(c_int32)]),
     ("fx_sim_get_sweep_variants", c_int32, [c_void_p, POINTER(c_int32)]),
+    ("fx_sim_set_brick_ctas", c_int32, [c_void_p, POINTER(c_int32)]),
+    ("fx_sim_get_brick_ctas", c_int32, [c_void_p, POINTER(c_int32)]),
+    ("fx_sim_autotune_bricks", c_int32, [c_void_p, c_double, c_int32, POINTER(FxBrickTuneReport)]),
     ("fx_rollout_desc_default", None, [POINTER(FxRolloutDesc)]),
     ("fx_rollout_create", c_int32, [c_void_p, POINTER(FxRolloutDesc), POINTER(c_void_p)]),
     ("fx_rollout_destroy", None, [c_void_p]),
@@ -347,5 +358,6 @@ def check(status: int, sim_handle=None, lib: ctypes.CDLL | None = None) -> None:
     if status == FX_OK:
         return
     lib = lib or load()
-    msg = lib.fx_sim_last_error(sim_handle) if sim_handle else lib.fx_last_error()
+    # argument errors that leave a handle usable are reported through fx_last_error
+    msg = (lib.fx_sim_last_error(sim_handle) if sim_handle else b"") or lib.fx_last_error()
     raise FenixError(status, (msg or b"").decode(errors="replace"))

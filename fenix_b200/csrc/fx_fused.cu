@@ -1397,6 +1397,12 @@ int FusedWork::next_event() {
 
 fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, FusedResult& out);
 
+// The grid of brick kernel k: SMs x its CTAs per SM, at most one block per brick.
+uint32_t brick_grid_of(const FusedStep& st, uint32_t nb, BrickKernel k) {
+  const uint32_t m = st.brick_ctas[k] ? st.brick_ctas[k] : (uint32_t)kBrickCtasDefault;
+  return std::max<uint32_t>(1, std::min<uint32_t>(nb, (uint32_t)device_sm_count() * m));
+}
+
 fx_status fused_prepare(FusedWork& w, const FusedStep& st, uint32_t* ninj_out, FusedResult& out) {
   cudaStream_t s = st.stream;
   const Dims dm = st.dm;
@@ -1465,6 +1471,7 @@ uint64_t fused_key(const FusedStep& st, uint32_t ninj) {
   for (int l = 0; l < 3; ++l) mix_key((uint64_t)(st.sweep_variant[l] + 1));
   mix_key(st.solver_norms);
   mix_key(st.sparse);
+  for (int k = 0; k < kBrickKernels; ++k) mix_key(st.brick_ctas[k]);
   mix_key((uint64_t)(uintptr_t)st.inflow);
   if (st.inflow)
     for (uint32_t v : {st.inflow_patch.x0, st.inflow_patch.y, st.inflow_patch.z0, st.inflow_patch.nx, st.inflow_patch.nz}) mix_key(v);
@@ -1606,7 +1613,6 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   const uint32_t nb = w.nb;
   const int cur = st.cur_index, next = cur ^ 1;
   uint32_t launches = 0;
-  const uint32_t brick_grid = std::max<uint32_t>(1, std::min<uint32_t>(nb, (uint32_t)device_sm_count() * 8u));
   uint32_t* c_adv = w.counters + 0;
   uint32_t* c_next = w.counters + 1;
   uint32_t* c_inj = w.counters + 3;
@@ -1669,7 +1675,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     Timed tm(w, s, "fused_inject");
     by_storage(st.half_storage, [&](auto tag) {
       using S = typename decltype(tag)::type;
-      k_inject<S><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.sources, st.nsrc, w.list_inj, c_inj, sset<S>(st.cur), st.vcur,
+      k_inject<S><<<brick_grid_of(st, nb, BK_INJECT), kBrickThreads, 0, s>>>(dm, bc, st.params, st.sources, st.nsrc, w.list_inj, c_inj, sset<S>(st.cur), st.vcur,
                                                        w.summary_set[cur], w.nz_set[cur]);
     });
     ++launches;
@@ -1721,7 +1727,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       ++launches;
     }
     Timed tm(w, s, "sparse_advect_velocity");
-    k_sp_advect_velocity<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.vcur, st.vscr, L.list[0], L.count[0]);
+    k_sp_advect_velocity<<<brick_grid_of(st, nb, BK_SP_ADVECT_VELOCITY), kBrickThreads, 0, s>>>(dm, bc, st.params, st.vcur, st.vscr, L.list[0], L.count[0]);
     ++launches;
   } else {
     Timed tm(w, s, "fused_advect_velocity");
@@ -1752,7 +1758,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     Timed tm(w, s, "fused_advect_scalars");
     by_storage(st.half_storage, [&](auto tag) {
       using S = typename decltype(tag)::type;
-      k_advect_scalars<S><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.advect_mode,
+      k_advect_scalars<S><<<brick_grid_of(st, nb, BK_ADVECT_SCALARS), kBrickThreads, 0, s>>>(dm, bc, st.params, st.advect_mode,
                                                                static_cast<const typename Aos<S>::T*>(w.aos), st.vscr, st.flags_cur,
                                                                w.list_adv, c_adv, sset<S>(st.scratch), w.summary_t, w.nz_t);
     });
@@ -1789,7 +1795,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     Timed tm(w, s, "fused_combustion");
     by_storage(st.half_storage, [&](auto tag) {
       using S = typename decltype(tag)::type;
-      k_combustion<S><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, sset<S>(st.scratch), st.flags_next, w.list_next, c_next, w.nz_t,
+      k_combustion<S><<<brick_grid_of(st, nb, BK_COMBUSTION), kBrickThreads, 0, s>>>(dm, bc, st.params, sset<S>(st.scratch), st.flags_next, w.list_next, c_next, w.nz_t,
                                                            w.summary_t, sset<S>(st.next), w.summary_set[next], w.nz_set[next]);
     });
     ++launches;
@@ -1798,7 +1804,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     Timed tm(w, s, "fused_buoyancy");
     by_storage(st.half_storage, [&](auto tag) {
       using S = typename decltype(tag)::type;
-      k_buoyancy<S><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, sset<S>(st.next), st.flags_next, w.list_next, c_next, st.vscr);
+      k_buoyancy<S><<<brick_grid_of(st, nb, BK_BUOYANCY), kBrickThreads, 0, s>>>(dm, bc, st.params, sset<S>(st.next), st.flags_next, w.list_next, c_next, st.vscr);
     });
     ++launches;
   }
@@ -1807,7 +1813,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   if (st.vort_on && st.sparse) {
     {
       Timed tm(w, s, "sparse_vorticity");
-      k_sp_vorticity<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.vscr, st.vort_mag, st.vort, st.debug_fields ? 1 : 0, sp_list(SP_CURL),
+      k_sp_vorticity<<<brick_grid_of(st, nb, BK_SP_VORTICITY), kBrickThreads, 0, s>>>(dm, bc, st.vscr, st.vort_mag, st.vort, st.debug_fields ? 1 : 0, sp_list(SP_CURL),
                                                           sp_count(SP_CURL));
       ++launches;
     }
@@ -1816,10 +1822,10 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       by_storage(st.half_storage, [&](auto tag) {
         using S = typename decltype(tag)::type;
         if (st.debug_fields)
-          k_sp_confinement<S, true><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.vscr, st.vort_mag, sset<S>(st.next), w.nz_set[next],
+          k_sp_confinement<S, true><<<brick_grid_of(st, nb, BK_SP_CONFINEMENT), kBrickThreads, 0, s>>>(dm, bc, st.params, st.vscr, st.vort_mag, sset<S>(st.next), w.nz_set[next],
                                                                          st.vscr2, st.conf_mag, sp_list(SP_CURL), sp_count(SP_CURL));
         else
-          k_sp_confinement<S, false><<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, st.params, st.vscr, st.vort_mag, sset<S>(st.next),
+          k_sp_confinement<S, false><<<brick_grid_of(st, nb, BK_SP_CONFINEMENT), kBrickThreads, 0, s>>>(dm, bc, st.params, st.vscr, st.vort_mag, sset<S>(st.next),
                                                                           w.nz_set[next], st.vscr2, st.conf_mag, sp_list(SP_CURL),
                                                                           sp_count(SP_CURL));
       });
@@ -1886,7 +1892,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     const uint32_t* pc = sp_count(SP_PRESSURE);
     {
       Timed tm(w, s, "sparse_div_first_sweep");
-      k_sp_div_first<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, *vfinal, F.div, m >= 1 ? outs[0] : nullptr, M.dm, M.div, pl, pc);
+      k_sp_div_first<<<brick_grid_of(st, nb, BK_SP_DIV_FIRST), kBrickThreads, 0, s>>>(dm, bc, *vfinal, F.div, m >= 1 ? outs[0] : nullptr, M.dm, M.div, pl, pc);
       ++launches;
     }
     if (m >= 1) chain = outs[wi++];
@@ -1909,11 +1915,11 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       Timed tm(w, s, name);
       if (use_tma && w.tmaps_ok && src) {
         const CUtensorMap& sm = src == F.p[0] ? w.tmap_p[0] : w.tmap_p[1];
-        const uint32_t sweep_grid = std::max<uint32_t>(1, std::min<uint32_t>(nb, (uint32_t)device_sm_count() * 8u));
+        const uint32_t sweep_grid = brick_grid_of(st, nb, BK_SP_SWEEP);
         k_sp_sweep_tma<<<sweep_grid, kSpSweepThreads, 0, s>>>(sm, w.tmap_div, dm, bc, dst, M.dm, mid_p, pl, pc, w.dev_err, w.tma_wait_ns,
                                                               w.tma_extra_tx);
       } else {
-        k_sp_sweep<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, F.div, src, dst, M.dm, mid_p, 0, pl, pc);
+        k_sp_sweep<<<brick_grid_of(st, nb, BK_SP_SWEEP), kBrickThreads, 0, s>>>(dm, bc, F.div, src, dst, M.dm, mid_p, 0, pl, pc);
       }
       ++launches;
     };
@@ -1925,7 +1931,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     }
     if (m == 0) {
       Timed tm(w, s, "sparse_prolong_fine");
-      k_sp_sweep<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, F.div, nullptr, outs[wi], M.dm, M.p[mid], 1, pl, pc);
+      k_sp_sweep<<<brick_grid_of(st, nb, BK_SP_PROLONG_FINE), kBrickThreads, 0, s>>>(dm, bc, F.div, nullptr, outs[wi], M.dm, M.p[mid], 1, pl, pc);
       chain = outs[wi++];
       ++launches;
     }
@@ -1935,7 +1941,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     }
     {
       Timed tm(w, s, "sparse_project");
-      k_sp_project<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, *vfinal, F.p[last_p], st.vcur, sp_list(SP_VCUR), sp_count(SP_VCUR));
+      k_sp_project<<<brick_grid_of(st, nb, BK_SP_PROJECT), kBrickThreads, 0, s>>>(dm, bc, *vfinal, F.p[last_p], st.vcur, sp_list(SP_VCUR), sp_count(SP_VCUR));
       ++launches;
     }
   } else if (st.pressure_on) {
@@ -2010,7 +2016,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     }
   } else if (st.sparse) {
     Timed tm(w, s, "sparse_project");
-    k_sp_project<<<brick_grid, kBrickThreads, 0, s>>>(dm, bc, *vfinal, st.lv[0].p[last_p], st.vcur, sp_list(SP_VCUR), sp_count(SP_VCUR));
+    k_sp_project<<<brick_grid_of(st, nb, BK_SP_PROJECT), kBrickThreads, 0, s>>>(dm, bc, *vfinal, st.lv[0].p[last_p], st.vcur, sp_list(SP_VCUR), sp_count(SP_VCUR));
     ++launches;
   } else {
     // 10. projection with the pressure of the last solve (+ |v|)

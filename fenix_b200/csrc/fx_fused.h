@@ -98,6 +98,17 @@ struct FusedWork {
   int next_event();
 };
 
+// The brick-list kernels whose grid is tunable (fx_sim_autotune_bricks): each
+// block walks the brick list with a stride of the grid, so any grid gives the
+// same results. The grid is SMs x CTAs per SM, at most one block per brick.
+enum BrickKernel {
+  BK_INJECT, BK_ADVECT_SCALARS, BK_COMBUSTION, BK_BUOYANCY,
+  BK_SP_ADVECT_VELOCITY, BK_SP_VORTICITY, BK_SP_CONFINEMENT, BK_SP_DIV_FIRST, BK_SP_SWEEP, BK_SP_PROLONG_FINE, BK_SP_PROJECT,
+  kBrickKernels
+};
+constexpr int kBrickCtasDefault = 8;
+constexpr int kBrickCtasMax = 64;
+
 struct FusedStep {
   cudaStream_t stream;
   const float* inflow = nullptr;  // device values of the inflow patch (NULL: none)
@@ -121,6 +132,7 @@ struct FusedStep {
   LevelBuf xlv[3];  // V-cycle levels 3..5
   int q[7];
   int sweep_variant[3];  // sweep kernel of the fine, mid and coarse level (-1 = default)
+  uint8_t brick_ctas[kBrickKernels] = {};  // CTAs per SM of each brick kernel (0 = kBrickCtasDefault)
   int solver_mode;    // 0: the reference schedule, 1: the V-cycle
   VCycleConfig vc;
   bool solver_norms;  // FP64 statistics after the reference schedule too

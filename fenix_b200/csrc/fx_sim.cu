@@ -102,6 +102,7 @@ struct fx_sim {
   fx_solver_settings solver{};
   uint32_t last_cycle_launches = 0;  // kernels per V-cycle in the latest step
   int sweep_variant[3] = {-1, -1, -1};  // sweep kernel per pressure level, chosen by fx_sim_autotune
+  uint8_t brick_ctas[kBrickKernels] = {};  // CTAs per SM of the brick kernels (0 = default), fx_sim_autotune_bricks
   int last_solver_mode = 0;
 
   // device memory
@@ -576,6 +577,7 @@ fx_status step_begin(fx_sim* s, double elapsed, double step_s, StepPlan& sp) {
   for (int l = 0; l < 3; ++l) fs.xlv[l] = s->xlv[l];
   for (int k = 0; k < 7; ++k) fs.q[k] = s->qi[k];
   for (int l = 0; l < 3; ++l) fs.sweep_variant[l] = s->sweep_variant[l];
+  for (int k = 0; k < kBrickKernels; ++k) fs.brick_ctas[k] = s->brick_ctas[k];
   fs.solver_mode = s->solver.mode;
   fs.vc = vcycle_config(s, false);
   fs.solver_norms = (s->instr & FX_INSTR_SOLVER_NORMS) != 0;
@@ -1086,7 +1088,7 @@ fx_status fx_sim_save_state(fx_sim* s, void* dst, uint64_t bytes) {
   if (!s || !dst) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_save_state: NULL argument");
   if (!s->err.empty()) return FX_ERR_STATE;
   const StateLayout L = state_layout(s);
-  if (bytes != L.total) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_save_state: byte count does not match fx_sim_state_bytes");
+  if (bytes != L.total) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_save_state: byte count does not match fx_sim_state_bytes");
   FX_CUDA(s, cudaSetDevice(s->device));
   StateHeader h{};
   h.magic = kStateMagic;
@@ -1116,16 +1118,16 @@ fx_status fx_sim_load_state(fx_sim* s, const void* src, uint64_t bytes) {
   if (!s || !src) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: NULL argument");
   if (!s->err.empty()) return FX_ERR_STATE;
   const StateLayout L = state_layout(s);
-  if (bytes != L.total) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: byte count does not match fx_sim_state_bytes");
+  if (bytes != L.total) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: byte count does not match fx_sim_state_bytes");
   FX_CUDA(s, cudaSetDevice(s->device));
   StateHeader h{};
   FX_CUDA(s, cudaMemcpy(&h, src, sizeof h, cudaMemcpyDefault));
   if (h.magic != kStateMagic || h.version != kStateVersion)
-    return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: not a saved state of this version");
+    return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: not a saved state of this version");
   if (h.w != s->dm.w || h.h != s->dm.h || h.d != s->dm.d || h.scalar_bytes != (s->half ? 2u : 4u))
-    return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: the state has another resolution or scalar storage");
+    return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: the state has another resolution or scalar storage");
   if ((h.cur != 0 && h.cur != 1) || (h.last_p != 0 && h.last_p != 1) || h.step_index < 0)
-    return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: corrupt header");
+    return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_load_state: corrupt header");
   // doReset's clears (a superset), then the saved parts
   fx_status st = zero_state(s);
   if (st != FX_OK) return st;
@@ -1372,6 +1374,130 @@ fx_status fx_sim_autotune(fx_sim* s, fx_autotune_report* o) {
   cudaEventDestroy(ev[1]);
   if (st != FX_OK) return st;
   FX_CUDA(s, cudaGetLastError());
+  return FX_OK;
+}
+
+static_assert(FX_BRICK_KERNELS == kBrickKernels && FX_BK_INJECT == BK_INJECT && FX_BK_ADVECT_SCALARS == BK_ADVECT_SCALARS &&
+                  FX_BK_COMBUSTION == BK_COMBUSTION && FX_BK_BUOYANCY == BK_BUOYANCY &&
+                  FX_BK_SPARSE_ADVECT_VELOCITY == BK_SP_ADVECT_VELOCITY && FX_BK_SPARSE_VORTICITY == BK_SP_VORTICITY &&
+                  FX_BK_SPARSE_CONFINEMENT == BK_SP_CONFINEMENT && FX_BK_SPARSE_DIV_FIRST_SWEEP == BK_SP_DIV_FIRST &&
+                  FX_BK_SPARSE_SWEEP == BK_SP_SWEEP && FX_BK_SPARSE_PROLONG_FINE == BK_SP_PROLONG_FINE &&
+                  FX_BK_SPARSE_PROJECT == BK_SP_PROJECT,
+              "the ABI's brick kernel indices follow BrickKernel");
+
+fx_status fx_sim_set_brick_ctas(fx_sim* s, const int32_t* v) {
+  if (!s || !v) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_brick_ctas: NULL argument");
+  for (int k = 0; k < kBrickKernels; ++k)
+    if (v[k] < 0 || v[k] > kBrickCtasMax)
+      return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_set_brick_ctas: CTAs per SM must be 0 (default) or 1.." + std::to_string(kBrickCtasMax));
+  for (int k = 0; k < kBrickKernels; ++k) s->brick_ctas[k] = (uint8_t)v[k];
+  return FX_OK;
+}
+
+fx_status fx_sim_get_brick_ctas(fx_sim* s, int32_t* v) {
+  if (!s || !v) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_get_brick_ctas: NULL argument");
+  for (int k = 0; k < kBrickKernels; ++k) v[k] = s->brick_ctas[k];
+  return FX_OK;
+}
+
+namespace {
+
+// The timer names of each brick kernel's launches (fused_sequence's Timed labels).
+const char* const kBrickKernelTimers[kBrickKernels][2] = {
+    {"fused_inject", nullptr},
+    {"fused_advect_scalars", nullptr},
+    {"fused_combustion", nullptr},
+    {"fused_buoyancy", nullptr},
+    {"sparse_advect_velocity", nullptr},
+    {"sparse_vorticity", nullptr},
+    {"sparse_confinement", nullptr},
+    {"sparse_div_first_sweep", nullptr},
+    {"sparse_sweep", "sparse_sweep_prolong"},
+    {"sparse_prolong_fine", nullptr},
+    {"sparse_project", nullptr},
+};
+
+// A second simulation with s's settings and sources (not its state).
+fx_status clone_settings(fx_sim* s, fx_sim** out) {
+  fx_sim_options o;
+  fx_sim_options_default(&o);
+  o.width = s->dm.w, o.height = s->dm.h, o.depth = s->dm.d;
+  o.scalar_advection_mode = s->advect_mode;
+  o.runtime_mask = FX_PARAM_ALL;
+  o.runtime = s->rp;
+  o.quality_mask = FX_QUALITY_ALL;
+  o.quality = s->quality;
+  o.device = s->device;
+  o.kernels = s->kernels;
+  o.flags = s->opt_flags & ~FX_OPT_SPARSE;
+  fx_sim* c = nullptr;
+  fx_status st = fx_sim_create(&o, &c);
+  if (st != FX_OK) return st;
+  const uint32_t nsrc = (uint32_t)(s->host_sources.size() / 32);
+  if ((st = fx_sim_update_sources(c, nsrc ? s->host_sources.data() : nullptr, nsrc)) == FX_OK &&
+      (st = fx_sim_set_solver(c, &s->solver)) == FX_OK && (st = fx_sim_set_sparse(c, s->sparse ? 1 : 0)) == FX_OK) {
+    for (int l = 0; l < 3; ++l) c->sweep_variant[l] = s->sweep_variant[l];
+    c->debug_requested = s->debug_requested;
+    *out = c;
+    return FX_OK;
+  }
+  g_last_error = "fx_sim_autotune_bricks: clone: " + (c->err.empty() ? g_last_error : c->err);
+  fx_sim_destroy(c);
+  return st;
+}
+
+}  // namespace
+
+fx_status fx_sim_autotune_bricks(fx_sim* s, double step_seconds, int32_t steps, fx_brick_tune_report* o) {
+  if (!s || !o) return fail(s, FX_ERR_INVALID_ARGUMENT, "fx_sim_autotune_bricks: NULL argument");
+  if (!s->err.empty()) return FX_ERR_STATE;
+  if (s->kernels != FX_KERNELS_FUSED) return fail(s, FX_ERR_UNSUPPORTED, "fx_sim_autotune_bricks: the plain kernels have no brick lists");
+  if (!(step_seconds > 0.0) || !std::isfinite(step_seconds) || steps < 1 || steps > 64)
+    return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_sim_autotune_bricks: step_seconds must be > 0 and steps in 1..64");
+  std::memset(o, 0, sizeof *o);
+  FX_CUDA(s, cudaSetDevice(s->device));
+  uint64_t bytes = 0;
+  fx_sim_state_bytes(s, &bytes);
+  void* blob = nullptr;
+  FX_CUDA(s, device_alloc(&blob, bytes));
+  fx_sim* c = nullptr;
+  fx_status st = fx_sim_save_state(s, blob, bytes);
+  if (st == FX_OK) st = clone_settings(s, &c);
+  static const int kCandidates[] = {2, 4, 8, 16, 32};
+  float us[5][kBrickKernels] = {};
+  std::vector<fx_kernel_time> kt(128);
+  for (int ci = 0; ci < 5 && st == FX_OK; ++ci) {
+    for (int k = 0; k < kBrickKernels; ++k) c->brick_ctas[k] = (uint8_t)kCandidates[ci];
+    // every candidate steps the same state, so every candidate does the same work
+    if ((st = fx_sim_load_state(c, blob, bytes)) != FX_OK) break;
+    double t = c->last_elapsed_s;
+    if ((st = fx_sim_set_instrumentation(c, 0)) != FX_OK || (st = fx_sim_step(c, t += step_seconds, step_seconds)) != FX_OK) break;
+    if ((st = fx_sim_set_instrumentation(c, FX_INSTR_KERNEL_TIMES)) != FX_OK) break;
+    for (int k = 0; k < steps && st == FX_OK; ++k) st = fx_sim_step(c, t += step_seconds, step_seconds);
+    uint32_t n = 0;
+    if (st != FX_OK || (st = fx_sim_read_kernel_times(c, kt.data(), (uint32_t)kt.size(), &n)) != FX_OK) break;
+    for (uint32_t i = 0; i < std::min<uint32_t>(n, (uint32_t)kt.size()); ++i)
+      for (int k = 0; k < kBrickKernels; ++k)
+        for (const char* name : kBrickKernelTimers[k])
+          if (name && std::strcmp(kt[i].name, name) == 0) us[ci][k] += (float)(kt[i].total_ms * 1000.0 / steps);
+  }
+  if (st != FX_OK && c && !c->err.empty() && s->err.empty()) g_last_error = "fx_sim_autotune_bricks: " + c->err;
+  if (c) fx_sim_destroy(c);
+  cudaFree(blob);
+  if (st != FX_OK) return st;
+  const int dflt = 2;  // kCandidates[2] == kBrickCtasDefault
+  static_assert(kBrickCtasDefault == 8, "the default grid is a candidate");
+  for (int k = 0; k < kBrickKernels; ++k) {
+    o->default_us[k] = us[dflt][k];
+    int best = dflt;
+    for (int ci = 0; ci < 5; ++ci)
+      if (us[ci][k] > 0.0f && us[ci][k] < us[best][k]) best = ci;
+    // closer than 3 % is within the run-to-run noise of a few steps
+    if (!(us[dflt][k] > 0.0f) || us[best][k] > 0.97f * us[dflt][k]) best = dflt;
+    o->ctas_per_sm[k] = kCandidates[best];
+    o->us[k] = us[best][k];
+    s->brick_ctas[k] = best == dflt ? 0 : (uint8_t)kCandidates[best];
+  }
   return FX_OK;
 }
 

@@ -274,7 +274,8 @@ class CombustionVolumeSimulation:
         """Restores a saveState() of a simulation with the same resolution and
         scalar storage; the following steps repeat the saved run's bits."""
         arr = np.ascontiguousarray(state, dtype=np.uint8).ravel()
-        check(self._lib.fx_sim_load_state(self._h, arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes), self._h, self._lib)
+        # a refused state is reported through fx_last_error; the handle stays usable
+        check(self._lib.fx_sim_load_state(self._h, arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes), None, self._lib)
 
     def synchronize(self) -> None:
         check(self._lib.fx_sim_synchronize(self._h), self._h, self._lib)
@@ -358,6 +359,35 @@ class CombustionVolumeSimulation:
         arr = (ctypes.c_int32 * 3)()
         check(self._lib.fx_sim_get_sweep_variants(self._h, arr), None, self._lib)
         return list(arr)
+
+    def setBrickCtas(self, ctas_per_sm) -> None:
+        """CTAs per SM of each brick kernel (a sequence in _lib.BRICK_KERNELS order, or
+        a {name: value} mapping; 0 keeps the default 8). Results do not change."""
+        cur = self.getBrickCtas()
+        if isinstance(ctas_per_sm, Mapping):
+            for k, v in ctas_per_sm.items():
+                cur[k] = int(v)
+            vals = [cur[k] for k in _lib.BRICK_KERNELS]
+        else:
+            vals = [int(v) for v in ctas_per_sm]
+            if len(vals) != len(_lib.BRICK_KERNELS):
+                raise ValueError(f"expected {len(_lib.BRICK_KERNELS)} values")
+        arr = (ctypes.c_int32 * len(vals))(*vals)
+        check(self._lib.fx_sim_set_brick_ctas(self._h, arr), None, self._lib)
+
+    def getBrickCtas(self) -> Dict[str, int]:
+        arr = (ctypes.c_int32 * len(_lib.BRICK_KERNELS))()
+        check(self._lib.fx_sim_get_brick_ctas(self._h, arr), None, self._lib)
+        return dict(zip(_lib.BRICK_KERNELS, list(arr)))
+
+    def autotuneBricks(self, stepSeconds: float = 1.0 / 60.0, steps: int = 4) -> Dict[str, Any]:
+        """Times 2, 4, 8, 16 and 32 CTAs per SM for every brick kernel on a clone of
+        this simulation (same settings, sources and state) and keeps the fastest
+        per kernel (fx_sim_autotune_bricks; results do not change)."""
+        r = _lib.FxBrickTuneReport()
+        check(self._lib.fx_sim_autotune_bricks(self._h, float(stepSeconds), int(steps), ctypes.byref(r)), self._h, self._lib)
+        return {name: {"ctasPerSM": r.ctas_per_sm[i], "us": r.us[i], "defaultUs": r.default_us[i]}
+                for i, name in enumerate(_lib.BRICK_KERNELS)}
 
     # -- sparse mode (extension) ---------------------------------------------------
     def setSparse(self, on: bool) -> None:

@@ -110,8 +110,9 @@ typedef struct fx_runtime_params {
 #define FX_OPT_NO_GRAPHS (1u << 1)    /* launch kernels directly instead of CUDA graphs */
 /* FP16 storage of the scalar sets (density, temperature, fuel, reaction); fused
  * kernels only (FX_ERR_UNSUPPORTED with FX_KERNELS_PLAIN). Arithmetic stays f32;
- * every value a reference pass stores into a scalar buffer is rounded to the
- * nearest binary16 (ties to even). Velocity and pressure stay f32. Field reads
+ * every value a reference pass stores into a scalar buffer is rounded to
+ * binary16, stochastically unless FX_OPT_F16_ROUND_NEAREST (below) is given.
+ * Velocity and pressure stay f32. Field reads
  * and writes still exchange f32 (writes are rounded), and the render buffers
  * report FX_DTYPE_F16. */
 #define FX_OPT_SCALARS_F16 (1u << 2)
@@ -281,8 +282,9 @@ fx_status fx_sim_write_field(fx_sim* sim, int32_t field_id, const void* host_src
  * (quality, runtime parameters, sources, solver, kernels) are not part of it.
  * fx_sim_state_bytes gives the size of the blob; save copies it to `dst` (host
  * or device memory, waits for the stream). Load accepts a blob of a simulation
- * with the same resolution and scalar storage (else FX_ERR_INVALID_ARGUMENT and
- * the simulation is unchanged), clears everything else as fx_sim_reset does, and
+ * with the same resolution and scalar storage (else FX_ERR_INVALID_ARGUMENT,
+ * reported through fx_last_error, and the simulation is unchanged and usable),
+ * clears everything else as fx_sim_reset does, and
  * the steps that follow give the same bits as the steps that followed the save. */
 fx_status fx_sim_state_bytes(fx_sim* sim, uint64_t* bytes);
 fx_status fx_sim_save_state(fx_sim* sim, void* dst, uint64_t bytes);
@@ -402,6 +404,45 @@ fx_status fx_sim_autotune(fx_sim* sim, fx_autotune_report* out);
  * of planes with the next plane's loads in flight (widths divisible by 4). */
 fx_status fx_sim_set_sweep_variants(fx_sim* sim, const int32_t variants[3]);
 fx_status fx_sim_get_sweep_variants(fx_sim* sim, int32_t variants[3]);
+
+/* Grids of the brick-list kernels (extension; the reference dispatches one
+ * workgroup of 4^3 threads per 4^3 voxels, runtime/combustion-volume-simulation/
+ * constants.ts:3 and runtime/shared/createVolumeDispatch.ts:5-38). Each such
+ * kernel runs SMs x ctas_per_sm blocks (at most one per brick), every block
+ * walking the brick list with a stride of the grid, so the results do not
+ * depend on the choice. Index: FX_BK_*. 0 keeps the default (8); else 1..64. */
+#define FX_BRICK_KERNELS 11
+#define FX_BK_INJECT 0
+#define FX_BK_ADVECT_SCALARS 1
+#define FX_BK_COMBUSTION 2
+#define FX_BK_BUOYANCY 3
+#define FX_BK_SPARSE_ADVECT_VELOCITY 4
+#define FX_BK_SPARSE_VORTICITY 5
+#define FX_BK_SPARSE_CONFINEMENT 6
+#define FX_BK_SPARSE_DIV_FIRST_SWEEP 7
+#define FX_BK_SPARSE_SWEEP 8
+#define FX_BK_SPARSE_PROLONG_FINE 9
+#define FX_BK_SPARSE_PROJECT 10
+fx_status fx_sim_set_brick_ctas(fx_sim* sim, const int32_t ctas_per_sm[FX_BRICK_KERNELS]);
+fx_status fx_sim_get_brick_ctas(fx_sim* sim, int32_t ctas_per_sm[FX_BRICK_KERNELS]);
+
+/* Times the brick kernels' grids and keeps the fastest per kernel (extension).
+ * The timing runs on a clone: a second simulation with this one's settings,
+ * sources and saved state (fx_sim_save_state), stepped `steps` times (1..64,
+ * after one warm-up step) from that state for each of 2, 4, 8, 16 and 32 CTAs
+ * per SM, with per-kernel CUDA events. The simulation itself is only read (its
+ * stream is waited for), and the clone is destroyed before the call returns;
+ * it needs the memory of a second simulation for that time. A grid replaces the
+ * default only when it is at least 3 % faster. Kernels that did not run (the
+ * sparse ones in dense mode) keep the default and report 0 us. Fused kernels
+ * only. The choice enters the step's CUDA-graph key. */
+typedef struct fx_brick_tune_report {
+  int32_t ctas_per_sm[FX_BRICK_KERNELS]; /* chosen (8 where the default stays) */
+  float us[FX_BRICK_KERNELS];            /* its time per step */
+  float default_us[FX_BRICK_KERNELS];    /* the default grid's time per step */
+} fx_brick_tune_report;
+
+fx_status fx_sim_autotune_bricks(fx_sim* sim, double step_seconds, int32_t steps, fx_brick_tune_report* out);
 
 /* Batches (extension; the reference steps one simulation per device): many
  * independent simulations, each with its own options (sizes may differ), stepped

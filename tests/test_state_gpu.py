@@ -141,6 +141,8 @@ def test_mismatched_states_are_refused():
             a.loadState(bad)
         assert e.value.status == _lib.FX_ERR_INVALID_ARGUMENT
     same(before, snapshot(a), "after refused loads")
+    a.step(wl.dt, wl.dt)  # a refused load leaves the handle usable
+    a.synchronize()
     other = workloads.plume_box((64, 48, 48))
     b = createCombustionVolumeSimulation(other.options, device=0)
     c = createCombustionVolumeSimulation(wl.options, device=0, storage="f16")
