@@ -82,10 +82,17 @@ FX_DEV void tri_dpos(const float* __restrict__ f, const Tri& c, float& gx, float
 struct Sample {
   Tri t;
   float mx, my, mz;
+  int bx, by, bz, ux, uy, uz;  // the lower and upper corner coordinates (tri_corners')
 };
 FX_DEV Sample sample_at(const Dims& dm, float px, float py, float pz) {
   Sample s;
   s.t = tri_corners(dm, px, py, pz);
+  s.bx = (int)floorf(clamp_pos(px, (float)(dm.w - 1u)));
+  s.by = (int)floorf(clamp_pos(py, (float)(dm.h - 1u)));
+  s.bz = (int)floorf(clamp_pos(pz, (float)(dm.d - 1u)));
+  s.ux = min(s.bx + 1, (int)dm.w - 1);
+  s.uy = min(s.by + 1, (int)dm.h - 1);
+  s.uz = min(s.bz + 1, (int)dm.d - 1);
   s.mx = pass_mask(px, (float)(dm.w - 1u));
   s.my = pass_mask(py, (float)(dm.h - 1u));
   s.mz = pass_mask(pz, (float)(dm.d - 1u));
@@ -98,6 +105,77 @@ FX_DEV void add_dpos(const float* __restrict__ f, const Sample& s, float w, floa
   g[0] += w * gx * s.mx;
   g[1] += w * gy * s.my;
   g[2] += w * gz * s.mz;
+}
+
+// Brick-local accumulation of the advections' transposed trilinear scatters.
+// A block owns one 8^3 brick (two voxels per thread) and keeps, per adjoint
+// field, a shared-memory tile of the brick with a halo of kAccHalo voxels. A
+// sample whose eight corners lie in the tile adds to it with shared-memory
+// atomics; any other goes to global memory directly. At the end the block adds
+// each touched tile cell to global memory once, instead of one global atomic
+// per (sample, corner): a back-traced sample lies within a voxel or two of its
+// voxel wherever the flow is slow, so neighbouring voxels hit the same cells.
+constexpr int kAccHalo = 2;
+constexpr int kAccEdge = 8 + 2 * kAccHalo;
+constexpr int kAccCells = kAccEdge * kAccEdge * kAccEdge;
+constexpr int kAccThreads = 256;
+static_assert(7 * kAccCells * sizeof(float) <= 48 * 1024, "the scalar adjoint's tiles fit the default shared memory");
+
+struct TileOrigin {
+  int x, y, z;
+};
+
+FX_DEV TileOrigin brick_tile(uint3 bc, uint32_t b) {
+  const uint32_t bx = b % bc.x, by = (b / bc.x) % bc.y, bz = b / (bc.x * bc.y);
+  return {(int)(bx * 8u) - kAccHalo, (int)(by * 8u) - kAccHalo, (int)(bz * 8u) - kAccHalo};
+}
+
+FX_DEV void tile_clear(float* sh, int fields) {
+  for (int j = threadIdx.x; j < fields * kAccCells; j += blockDim.x) sh[j] = 0.0f;
+  __syncthreads();
+}
+
+// tri_scatter of g at sample s into the field's tile `sh` (or `lam` when a
+// corner lies outside the tile).
+FX_DEV void tile_scatter(const TileOrigin& o, float* sh, float* lam, const Sample& s, float g) {
+  if (g == 0.0f) return;
+  const int lx = s.bx - o.x, ly = s.by - o.y, lz = s.bz - o.z;
+  const int hx = s.ux - o.x, hy = s.uy - o.y, hz = s.uz - o.z;
+  if (lx < 0 || ly < 0 || lz < 0 || hx >= kAccEdge || hy >= kAccEdge || hz >= kAccEdge) {
+    tri_scatter(lam, s.t, g);
+    return;
+  }
+  const Tri& c = s.t;
+  const float ax = 1.0f - c.fx, ay = 1.0f - c.fy, az = 1.0f - c.fz;
+  const int r00 = kAccEdge * (ly + kAccEdge * lz), r10 = kAccEdge * (hy + kAccEdge * lz);
+  const int r01 = kAccEdge * (ly + kAccEdge * hz), r11 = kAccEdge * (hy + kAccEdge * hz);
+  atomicAdd(sh + lx + r00, g * (ax * ay * az));
+  atomicAdd(sh + hx + r00, g * (c.fx * ay * az));
+  atomicAdd(sh + lx + r10, g * (ax * c.fy * az));
+  atomicAdd(sh + hx + r10, g * (c.fx * c.fy * az));
+  atomicAdd(sh + lx + r01, g * (ax * ay * c.fz));
+  atomicAdd(sh + hx + r01, g * (c.fx * ay * c.fz));
+  atomicAdd(sh + lx + r11, g * (ax * c.fy * c.fz));
+  atomicAdd(sh + hx + r11, g * (c.fx * c.fy * c.fz));
+}
+
+// v added at voxel (x, y, z) of the block's own brick.
+FX_DEV void tile_point(const TileOrigin& o, float* sh, uint32_t x, uint32_t y, uint32_t z, float v) {
+  if (v != 0.0f) atomicAdd(sh + ((int)x - o.x) + kAccEdge * (((int)y - o.y) + kAccEdge * ((int)z - o.z)), v);
+}
+
+// Adds the block's tiles to their global fields (after a barrier).
+FX_DEV void tile_flush(const Dims& dm, const TileOrigin& o, const float* sh, float* const* lam, int fields) {
+  __syncthreads();
+  for (int j = threadIdx.x; j < kAccCells; j += blockDim.x) {
+    const int x = o.x + j % kAccEdge, y = o.y + (j / kAccEdge) % kAccEdge, z = o.z + j / (kAccEdge * kAccEdge);
+    if (x < 0 || y < 0 || z < 0 || x >= (int)dm.w || y >= (int)dm.h || z >= (int)dm.d) continue;
+    const uint32_t gi = flat(dm, (uint32_t)x, (uint32_t)y, (uint32_t)z);
+    for (int f = 0; f < fields; ++f) {
+      const float v = sh[f * kAccCells + j];
+      if (v != 0.0f) atomicAdd(lam[f] + gi, v);
+    }
+  }
 }
 
 // ------------------------------------------------------------------ kernels
@@ -371,12 +449,12 @@ __global__ void k_adj_combustion_fold(Dims dm, ScalarSet snap, ScalarSet lam_set
   hot[i] = 0.0f;
 }
 
-// advect-scalar-maccormack.wgsl.ts:33-101 at active voxels (velocity = vel).
-__global__ void k_adj_advect_scalars(Dims dm, uint3 bc, const Params* __restrict__ Pp, ScalarSet src, VelField vel,
-                                     const uint32_t* __restrict__ flags, ScalarSet lam_out, ScalarSet lam_src, VelField lam_vel) {
-  FX_VOXEL_PROLOGUE(dm);
-  if (!active_coord(flags, bc, x, y, z)) return;
-  const Params P = *Pp;
+// advect-scalar-maccormack.wgsl.ts:33-101 at one voxel of an active brick
+// (velocity = vel). Tiles 0-3: lam_src's fields; 4-6: lam_vel's components.
+FX_DEV void adj_advect_scalars_voxel(const Dims& dm, const Params& P, const ScalarSet& src, const VelField& vel, const ScalarSet& lam_out,
+                                     const ScalarSet& lam_src, const VelField& lam_vel, uint32_t x, uint32_t y, uint32_t z,
+                                     const TileOrigin& o, float* sh) {
+  const uint32_t i = flat(dm, x, y, z);
   const float dt = P.dt;
   const float cx = (float)x + 0.5f, cy = (float)y + 0.5f, cz = (float)z + 0.5f;
   const Tri c0 = tri_corners(dm, cx - 0.5f, cy - 0.5f, cz - 0.5f);
@@ -426,11 +504,11 @@ __global__ void k_adj_advect_scalars(Dims dm, uint3 bc, const Params* __restrict
       lorig = l;
     }
     if (lpred != 0.0f) {
-      tri_scatter(lam_src.f[f], cs.t, lpred);
+      tile_scatter(o, sh + f * kAccCells, lam_src.f[f], cs, lpred);
       add_dpos(src.f[f], cs, lpred, gsp);
     }
     if (lrec != 0.0f) {
-      tri_scatter(lam_src.f[f], cr.t, lrec);
+      tile_scatter(o, sh + f * kAccCells, lam_src.f[f], cr, lrec);
       float gr[3] = {0.0f, 0.0f, 0.0f};
       add_dpos(src.f[f], cr, lrec, gr);
 #pragma unroll
@@ -439,26 +517,45 @@ __global__ void k_adj_advect_scalars(Dims dm, uint3 bc, const Params* __restrict
         gfv[k] += gr[k] * dt;
       }
     }
-    if (lorig != 0.0f) atomicAdd(lam_src.f[f] + i, lorig);
+    tile_point(o, sh + f * kAccCells, x, y, z, lorig);
   }
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     if (gfv[k] == 0.0f) continue;
-    tri_scatter(lam_vel.c[k], cs.t, gfv[k]);
+    tile_scatter(o, sh + (4 + k) * kAccCells, lam_vel.c[k], cs, gfv[k]);
     add_dpos(vel.c[k], cs, gfv[k], gsp);
   }
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const float g = -dt * (gb[k] + gsp[k]);
-    if (g != 0.0f) atomicAdd(lam_vel.c[k] + i, g);
+    tile_point(o, sh + (4 + k) * kAccCells, x, y, z, g);
   }
 }
 
-// advect-velocity-semilagrangian.wgsl.ts:23-41 at interior voxels.
-__global__ void k_adj_advect_velocity(Dims dm, const Params* __restrict__ Pp, VelField src, VelField lam_dst, VelField lam_src) {
-  FX_VOXEL_PROLOGUE(dm);
+__global__ void __launch_bounds__(kAccThreads) k_adj_advect_scalars(Dims dm, uint3 bc, const Params* __restrict__ Pp, ScalarSet src,
+                                                                    VelField vel, const uint32_t* __restrict__ flags, ScalarSet lam_out,
+                                                                    ScalarSet lam_src, VelField lam_vel) {
+  extern __shared__ float sh[];
+  const uint32_t b = blockIdx.x;
+  if (flags[b] == 0u) return;
+  const TileOrigin o = brick_tile(bc, b);
+  tile_clear(sh, 7);
+  const Params P = *Pp;
+  for (uint32_t v = threadIdx.x; v < 512u; v += kAccThreads) {
+    const uint32_t x = (uint32_t)(o.x + kAccHalo) + (v & 7u), y = (uint32_t)(o.y + kAccHalo) + ((v >> 3) & 7u),
+                   z = (uint32_t)(o.z + kAccHalo) + (v >> 6);
+    if (x < dm.w && y < dm.h && z < dm.d) adj_advect_scalars_voxel(dm, P, src, vel, lam_out, lam_src, lam_vel, x, y, z, o, sh);
+  }
+  float* const lam[7] = {lam_src.f[0], lam_src.f[1], lam_src.f[2], lam_src.f[3], lam_vel.c[0], lam_vel.c[1], lam_vel.c[2]};
+  tile_flush(dm, o, sh, lam, 7);
+}
+
+// advect-velocity-semilagrangian.wgsl.ts:23-41 at one interior voxel; tiles
+// 0-2: lam_src's components.
+FX_DEV void adj_advect_velocity_voxel(const Dims& dm, float dt, const VelField& src, const VelField& lam_dst, const VelField& lam_src,
+                                      uint32_t x, uint32_t y, uint32_t z, const TileOrigin& o, float* sh) {
   if (is_boundary(dm, x, y, z)) return;
-  const float dt = Pp->dt;
+  const uint32_t i = flat(dm, x, y, z);
   const float damp = 1.0f - dt * 0.025f;
   float la[3];
   bool any = false;
@@ -477,12 +574,26 @@ __global__ void k_adj_advect_velocity(Dims dm, const Params* __restrict__ Pp, Ve
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     if (la[k] == 0.0f) continue;
-    tri_scatter(lam_src.c[k], c1.t, la[k]);
+    tile_scatter(o, sh + k * kAccCells, lam_src.c[k], c1, la[k]);
     add_dpos(src.c[k], c1, la[k], gp);
   }
 #pragma unroll
-  for (int k = 0; k < 3; ++k)
-    if (gp[k] != 0.0f) atomicAdd(lam_src.c[k] + i, -dt * gp[k]);
+  for (int k = 0; k < 3; ++k) tile_point(o, sh + k * kAccCells, x, y, z, -dt * gp[k]);
+}
+
+__global__ void __launch_bounds__(kAccThreads) k_adj_advect_velocity(Dims dm, uint3 bc, const Params* __restrict__ Pp, VelField src,
+                                                                     VelField lam_dst, VelField lam_src) {
+  extern __shared__ float sh[];
+  const TileOrigin o = brick_tile(bc, blockIdx.x);
+  tile_clear(sh, 3);
+  const float dt = Pp->dt;
+  for (uint32_t v = threadIdx.x; v < 512u; v += kAccThreads) {
+    const uint32_t x = (uint32_t)(o.x + kAccHalo) + (v & 7u), y = (uint32_t)(o.y + kAccHalo) + ((v >> 3) & 7u),
+                   z = (uint32_t)(o.z + kAccHalo) + (v >> 6);
+    if (x < dm.w && y < dm.h && z < dm.d) adj_advect_velocity_voxel(dm, dt, src, lam_dst, lam_src, x, y, z, o, sh);
+  }
+  float* const lam[3] = {lam_src.c[0], lam_src.c[1], lam_src.c[2]};
+  tile_flush(dm, o, sh, lam, 3);
 }
 
 // inject-igniter.wgsl.ts:32-66.
@@ -590,10 +701,13 @@ void adj_combustion(cudaStream_t s, Dims dm, uint3 bricks, const Params* P, Scal
 }
 void adj_advect_scalars(cudaStream_t s, Dims dm, uint3 bricks, const Params* P, ScalarSet src, VelField vel, const uint32_t* flags,
                         ScalarSet lam_out, ScalarSet lam_src, VelField lam_vel) {
-  k_adj_advect_scalars<<<grid_for(dm), kBlock, 0, s>>>(dm, bricks, P, src, vel, flags, lam_out, lam_src, lam_vel);
+  const size_t smem = 7 * kAccCells * sizeof(float);  // 48,384 B: within the default 48 KiB
+  k_adj_advect_scalars<<<bricks.x * bricks.y * bricks.z, kAccThreads, smem, s>>>(dm, bricks, P, src, vel, flags, lam_out, lam_src, lam_vel);
 }
 void adj_advect_velocity(cudaStream_t s, Dims dm, const Params* P, VelField src, VelField lam_dst, VelField lam_src) {
-  k_adj_advect_velocity<<<grid_for(dm), kBlock, 0, s>>>(dm, P, src, lam_dst, lam_src);
+  const uint3 bc = make_uint3((dm.w + 7) / 8, (dm.h + 7) / 8, (dm.d + 7) / 8);
+  const size_t smem = 3 * kAccCells * sizeof(float);
+  k_adj_advect_velocity<<<bc.x * bc.y * bc.z, kAccThreads, smem, s>>>(dm, bc, P, src, lam_dst, lam_src);
 }
 void adj_inject_igniter(cudaStream_t s, Dims dm, const Params* P, const float* src, uint32_t nsrc, const float* t_before, const float* fuel,
                         const float* r_before, ScalarSet lam_set) {
