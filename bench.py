@@ -63,18 +63,28 @@ KERNEL_BYTES = {
 
 
 # DRAM bytes (read + written) per launch measured by ncu on plume_256 with FP16
-# storage (the launch-list summary under profiles/), per kernel of the fused
-# path, for roofline.traffic. fused_sweep is the marching fine sweep.
+# storage (profiles/sparse_step_plume256_f16_launches.md), per kernel timer name,
+# dense and sparse mode, for roofline.traffic. fused_sweep is the marching fine
+# sweep, sparse_sweep the TMA-staged sparse one.
 NCU_TRAFFIC = {
-    "fused_sweep": 176.3e6,
-    "fused_advect_velocity": 360.8e6,
-    "fused_advect_scalars": 109.5e6,
-    "fused_combustion": 50.7e6,
-    "fused_buoyancy": 84.8e6,
-    "fused_vorticity": 248.1e6,
-    "fused_confinement": 456.4e6,
-    "fused_div_first_sweep": 312.9e6,
-    "fused_project": 426.7e6,
+    "fused_sweep": 176.2e6,
+    "fused_sweep_prolong": 186.7e6,
+    "fused_advect_velocity": 359.8e6,
+    "fused_advect_scalars": 97.3e6,
+    "fused_combustion": 50.1e6,
+    "fused_buoyancy": 85.8e6,
+    "fused_vorticity": 247.9e6,
+    "fused_confinement": 458.7e6,
+    "fused_div_first_sweep": 310.7e6,
+    "fused_project": 439.4e6,
+    "fused_inject": 7.0e6,
+    "fused_pack_aos": 31.1e6,
+    "sparse_sweep": 33.7e6,
+    "sparse_confinement": 108.9e6,
+    "sparse_advect_velocity": 59.2e6,
+    "sparse_vorticity": 51.5e6,
+    "sparse_div_first_sweep": 50.0e6,
+    "sparse_project": 72.6e6,
 }
 
 

@@ -169,87 +169,29 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_advect_velocity(Dims dm, u
 }
 
 // compute-vorticity.wgsl.ts:23-50: |w| (w itself with debug fields) in computed
-// bricks, 0 in zeroed bricks and on the boundary. Column walk: planes z - 1, z and
-// z + 1 of vx and vy stay in registers; each component is curl_at's operations in
-// its order.
+// bricks, 0 in zeroed bricks and on the boundary.
 __global__ void __launch_bounds__(kBrickThreads) k_sp_vorticity(Dims dm, uint3 bc, VelField v, float* __restrict__ wmag, VelField w,
                                                                 int write_w, const uint32_t* __restrict__ list,
                                                                 const uint32_t* __restrict__ count) {
   const uint32_t n = *count;
   const uint32_t sy = dm.w, sz = dm.w * dm.h;
-  const uint32_t lx = threadIdx.x & 7u, ly = (threadIdx.x >> 3) & 7u;
-  for (uint32_t li = blockIdx.x * kSpColBricks + (threadIdx.x >> 6); li < n; li += gridDim.x * kSpColBricks) {
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
     const uint32_t e = list[li];
+    const bool comp = (e & kSpCompute) != 0u;
     const BrickCtx c = sp_ctx(dm, e);
-    const uint32_t x = c.x0 + lx, y = c.y0 + ly;
-    if (x >= dm.w || y >= dm.h) continue;
-    const uint32_t ze = min(c.z0 + 8u, dm.d);
-    uint32_t i = x + dm.w * (y + dm.h * c.z0);
-    const bool xyint = (e & kSpCompute) != 0u && x > 0u && y > 0u && x < dm.w - 1u && y < dm.h - 1u;
-    // reads outside [0, d) give 0 and are only used at boundary planes, which are not computed
-    auto at = [&](const float* f, uint32_t z) { return (xyint && z < dm.d) ? __ldg(f + x + dm.w * (y + dm.h * z)) : 0.0f; };
-    float xm = c.z0 > 0u ? at(v.c[0], c.z0 - 1u) : 0.0f, xc = at(v.c[0], c.z0), xp = at(v.c[0], c.z0 + 1u);
-    float ym = c.z0 > 0u ? at(v.c[1], c.z0 - 1u) : 0.0f, yc = at(v.c[1], c.z0), yp = at(v.c[1], c.z0 + 1u);
-    for (uint32_t z = c.z0; z < ze; ++z, i += sz) {
-      const float xn = at(v.c[0], z + 2u), yn = at(v.c[1], z + 2u);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const SpVoxel q = sp_voxel(dm, c, j);
+      if (!q.inside) continue;
       float cx = 0.f, cy = 0.f, cz = 0.f;
-      const bool live = xyint && z > 0u && z < dm.d - 1u;
-      if (live) {
-        cx = ((__ldg(v.c[2] + i + sy) - __ldg(v.c[2] + i - sy)) - (yp - ym)) * 0.5f;
-        cy = ((xp - xm) - (__ldg(v.c[2] + i + 1u) - __ldg(v.c[2] + i - 1u))) * 0.5f;
-        cz = ((__ldg(v.c[1] + i + 1u) - __ldg(v.c[1] + i - 1u)) - (__ldg(v.c[0] + i + sy) - __ldg(v.c[0] + i - sy))) * 0.5f;
-      }
-      wmag[i] = live ? length3(cx, cy, cz) : 0.0f;
+      const bool live = comp && !is_boundary(dm, q.x, q.y, q.z);
+      if (live) curl_at(v, q.i, sy, sz, cx, cy, cz);
+      wmag[q.i] = live ? length3(cx, cy, cz) : 0.0f;
       if (write_w) {
-        w.c[0][i] = cx;
-        w.c[1][i] = cy;
-        w.c[2][i] = cz;
+        w.c[0][q.i] = cx;
+        w.c[1][q.i] = cy;
+        w.c[2][q.i] = cz;
       }
-      xm = xc;
-      xc = xp;
-      xp = xn;
-      ym = yc;
-      yc = yp;
-      yp = yn;
-    }
-  }
-}
-
-// project-velocity.wgsl.ts:21-43 in computed bricks (vCurrent = vScratch - the
-// central pressure gradient), 0 in zeroed bricks and on the boundary. Column walk:
-// planes z - 1, z and z + 1 of the pressure stay in registers.
-__global__ void __launch_bounds__(kBrickThreads) k_sp_project(Dims dm, uint3 bc, VelField vs, const float* __restrict__ p, VelField vd,
-                                                              const uint32_t* __restrict__ list, const uint32_t* __restrict__ count) {
-  const uint32_t n = *count;
-  const uint32_t sy = dm.w, sz = dm.w * dm.h;
-  const uint32_t lx = threadIdx.x & 7u, ly = (threadIdx.x >> 3) & 7u;
-  for (uint32_t li = blockIdx.x * kSpColBricks + (threadIdx.x >> 6); li < n; li += gridDim.x * kSpColBricks) {
-    const uint32_t e = list[li];
-    const BrickCtx c = sp_ctx(dm, e);
-    const uint32_t x = c.x0 + lx, y = c.y0 + ly;
-    if (x >= dm.w || y >= dm.h) continue;
-    const uint32_t ze = min(c.z0 + 8u, dm.d);
-    uint32_t i = x + dm.w * (y + dm.h * c.z0);
-    const bool xyint = (e & kSpCompute) != 0u && x > 0u && y > 0u && x < dm.w - 1u && y < dm.h - 1u;
-    auto at = [&](uint32_t z) { return (xyint && z < dm.d) ? __ldg(p + x + dm.w * (y + dm.h * z)) : 0.0f; };
-    float pm = c.z0 > 0u ? at(c.z0 - 1u) : 0.0f, pc = at(c.z0), pp = at(c.z0 + 1u);
-    for (uint32_t z = c.z0; z < ze; ++z, i += sz) {
-      const float pn = at(z + 2u);
-      float ox = 0.f, oy = 0.f, oz = 0.f;
-      if (xyint && z > 0u && z < dm.d - 1u) {
-        const float gx = (__ldg(p + i + 1u) - __ldg(p + i - 1u)) * 0.5f;
-        const float gy = (__ldg(p + i + sy) - __ldg(p + i - sy)) * 0.5f;
-        const float gz = (pp - pm) * 0.5f;
-        ox = __ldg(vs.c[0] + i) - gx;
-        oy = __ldg(vs.c[1] + i) - gy;
-        oz = __ldg(vs.c[2] + i) - gz;
-      }
-      vd.c[0][i] = ox;
-      vd.c[1][i] = oy;
-      vd.c[2][i] = oz;
-      pm = pc;
-      pc = pp;
-      pp = pn;
     }
   }
 }
@@ -347,56 +289,39 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_confinement(Dims dm, uint3
 // divergence into the mid cells it covers (pressure-restriction.wgsl.ts:27-50:
 // the mean of the clamped 2x2x2 children, 0 on the mid boundary). Every mid cell
 // m lies in fine brick m >> 2 (the mid level is at most half the fine one, or 4
-// cells on a grid under 8), and so do its clamped children. Column walk (planes
-// z - 1, z, z + 1 of vz in registers) over groups of four entries, so the block
-// barrier around the restriction is reached by every thread the same number of
-// times; each quarter of the block then restricts its own brick from shared memory.
+// cells on a grid under 8), and so do its clamped children.
 __global__ void __launch_bounds__(kBrickThreads) k_sp_div_first(Dims dm, uint3 bc, VelField v, float* __restrict__ div, float* __restrict__ p1,
                                                                 Dims mid, float* __restrict__ mid_div, const uint32_t* __restrict__ list,
                                                                 const uint32_t* __restrict__ count) {
-  __shared__ float sd[kSpColBricks][512];
+  __shared__ float sd[512];
   const uint32_t n = *count;
-  const uint32_t q = threadIdx.x >> 6, lx = threadIdx.x & 7u, ly = (threadIdx.x >> 3) & 7u;
-  const uint32_t sy = dm.w, sz = dm.w * dm.h;
-  for (uint32_t base = blockIdx.x * kSpColBricks; base < n; base += gridDim.x * kSpColBricks) {
-    const uint32_t li = base + q;
-    const bool valid = li < n;
-    const uint32_t e = valid ? list[li] : 0u;
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t e = list[li];
+    const bool comp = (e & kSpCompute) != 0u;
     const BrickCtx c = sp_ctx(dm, e);
-    const uint32_t x = c.x0 + lx, y = c.y0 + ly;
-    const bool xyin = valid && x < dm.w && y < dm.h;
-    const bool xyint = xyin && (e & kSpCompute) != 0u && x > 0u && y > 0u && x < dm.w - 1u && y < dm.h - 1u;
-    auto at = [&](uint32_t z) { return (xyint && z < dm.d) ? __ldg(v.c[2] + x + dm.w * (y + dm.h * z)) : 0.0f; };
-    float zm = c.z0 > 0u ? at(c.z0 - 1u) : 0.0f, zc = at(c.z0), zp = at(c.z0 + 1u);
-    uint32_t i = xyin ? x + dm.w * (y + dm.h * c.z0) : 0u;
 #pragma unroll
-    for (uint32_t k = 0; k < 8u; ++k) {
-      const uint32_t z = c.z0 + k;
-      const float zn = at(z + 2u);
+    for (int j = 0; j < 2; ++j) {
+      const SpVoxel q = sp_voxel(dm, c, j);
       float dv = 0.0f;
-      if (xyin && z < dm.d) {
-        const bool live = xyint && z > 0u && z < dm.d - 1u;
+      if (q.inside) {
+        const bool live = comp && !is_boundary(dm, q.x, q.y, q.z);
         if (live) {
-          const float ddx = __ldg(v.c[0] + i + 1u) - __ldg(v.c[0] + i - 1u);
-          const float ddy = __ldg(v.c[1] + i + sy) - __ldg(v.c[1] + i - sy);
-          const float ddz = zp - zm;
+          const Nbr nb = neighbours(dm, q.x, q.y, q.z, q.i);
+          const float ddx = __ldg(v.c[0] + nb.xp) - __ldg(v.c[0] + nb.xm);
+          const float ddy = __ldg(v.c[1] + nb.yp) - __ldg(v.c[1] + nb.ym);
+          const float ddz = __ldg(v.c[2] + nb.zp) - __ldg(v.c[2] + nb.zm);
           dv = (ddx + ddy + ddz) * 0.5f;
         }
-        div[i] = dv;
-        if (p1) p1[i] = live ? div6(0.0f - dv) : 0.0f;
-        i += sz;
+        div[q.i] = dv;
+        if (p1) p1[q.i] = live ? div6(0.0f - dv) : 0.0f;
       }
-      sd[q][lx + 8u * (ly + 8u * k)] = dv;
-      zm = zc;
-      zc = zp;
-      zp = zn;
+      sd[threadIdx.x + kBrickThreads * j] = dv;
     }
     __syncthreads();
-    if (valid) {
-      const uint32_t cell = threadIdx.x & 63u;
-      const uint32_t mx = c.bx * 4u + (cell & 3u), my = c.by * 4u + ((cell >> 2) & 3u), mz = c.bz * 4u + (cell >> 4);
+    if (threadIdx.x < 64u) {
+      const uint32_t mx = c.bx * 4u + (threadIdx.x & 3u), my = c.by * 4u + ((threadIdx.x >> 2) & 3u), mz = c.bz * 4u + (threadIdx.x >> 4);
       if (mx < mid.w && my < mid.h && mz < mid.d) {
-        float outv = 0.0f;
+        float out = 0.0f;
         if (mx != 0u && my != 0u && mz != 0u && mx != mid.w - 1u && my != mid.h - 1u && mz != mid.d - 1u) {
           float sum = 0.0f;
           for (uint32_t dz = 0; dz < 2u; ++dz)
@@ -404,11 +329,11 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_div_first(Dims dm, uint3 b
               for (uint32_t dx = 0; dx < 2u; ++dx) {
                 const uint32_t fx = min(2u * mx + dx, dm.w - 1u) - c.x0, fy = min(2u * my + dy, dm.h - 1u) - c.y0,
                                fz = min(2u * mz + dz, dm.d - 1u) - c.z0;
-                sum += sd[q][fx + 8u * (fy + 8u * fz)];
+                sum += sd[fx + 8u * (fy + 8u * fz)];
               }
-          outv = sum * 0.125f;
+          out = sum * 0.125f;
         }
-        mid_div[flat(mid, mx, my, mz)] = outv;
+        mid_div[flat(mid, mx, my, mz)] = out;
       }
     }
     __syncthreads();
@@ -445,6 +370,37 @@ __global__ void __launch_bounds__(kBrickThreads) k_sp_sweep(Dims dm, uint3 bc, c
         }
       }
       dst[q.i] = out;
+    }
+  }
+}
+
+// project-velocity.wgsl.ts:21-43 in computed bricks (vCurrent = vScratch - the
+// central pressure gradient), 0 in zeroed bricks and on the boundary.
+__global__ void __launch_bounds__(kBrickThreads) k_sp_project(Dims dm, uint3 bc, VelField vs, const float* __restrict__ p, VelField vd,
+                                                              const uint32_t* __restrict__ list, const uint32_t* __restrict__ count) {
+  const uint32_t n = *count;
+  const uint32_t sy = dm.w, sz = dm.w * dm.h;
+  for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
+    const uint32_t e = list[li];
+    const bool comp = (e & kSpCompute) != 0u;
+    const BrickCtx c = sp_ctx(dm, e);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const SpVoxel q = sp_voxel(dm, c, j);
+      if (!q.inside) continue;
+      float ox = 0.f, oy = 0.f, oz = 0.f;
+      if (comp && !is_boundary(dm, q.x, q.y, q.z)) {
+        const uint32_t i = q.i;
+        const float gx = (__ldg(p + i + 1u) - __ldg(p + i - 1u)) * 0.5f;
+        const float gy = (__ldg(p + i + sy) - __ldg(p + i - sy)) * 0.5f;
+        const float gz = (__ldg(p + i + sz) - __ldg(p + i - sz)) * 0.5f;
+        ox = __ldg(vs.c[0] + i) - gx;
+        oy = __ldg(vs.c[1] + i) - gy;
+        oz = __ldg(vs.c[2] + i) - gz;
+      }
+      vd.c[0][q.i] = ox;
+      vd.c[1][q.i] = oy;
+      vd.c[2][q.i] = oz;
     }
   }
 }
