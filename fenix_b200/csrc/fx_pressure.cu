@@ -766,7 +766,7 @@ int march_plan_waves(Dims dm, int tx, int ty, int slots) {
   return best;
 }
 
-static cudaError_t march_run(Dims dm, int* run);
+static cudaError_t march_run(Dims dm, int* run, int slot_pct = 100);
 
 // The variant used when none was chosen: four x per thread marching in z where
 // the width allows and a thread marches at least 8 planes (the 256^3 level of
@@ -809,11 +809,11 @@ static cudaError_t march_slots(int* slots) {
 
 // Planes per thread of k_sweep_march on a level: runs of planes such that the
 // row tiles times the runs fill the resident slots once.
-static cudaError_t march_run(Dims dm, int* run) {
+static cudaError_t march_run(Dims dm, int* run, int slot_pct) {
   int slots = 0;
   const cudaError_t e = march_slots(&slots);
   if (e != cudaSuccess) return e;
-  *run = march_plan_one_wave(dm, slots);
+  *run = march_plan_one_wave(dm, std::max(1, slots * slot_pct / 100));
   return cudaSuccess;
 }
 
@@ -839,8 +839,13 @@ static cudaError_t march_run_of(K kernel, Dims dm, int* run) {
   return cudaSuccess;
 }
 
+int march_share_pct() {
+  static const int pct = env_int("FENIX_MARCH_SHARE", 50, 10, 100);
+  return pct;
+}
+
 cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float* div, const float* src, float* dst, Dims mid,
-                               const float* mid_p) {
+                               const float* mid_p, int slot_pct) {
   if (!sweep_variant_valid(variant, dm)) variant = sweep_variant_default(dm);
   auto grid = [&](int x_per_block, int z) { return dim3((dm.w + x_per_block - 1) / x_per_block, (dm.h + 7) / 8, (dm.d + z - 1) / z); };
   const dim3 block(32, 8, 1);
@@ -855,7 +860,7 @@ cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float
     case SWEEP_VEC4_Z1: k_sweep_v4<1><<<grid(128, 1), block, 0, s>>>(dm, div, src, dst, mid, mid_p); break;
     default: {
       int run = 0;
-      const cudaError_t e = march_run(dm, &run);
+      const cudaError_t e = march_run(dm, &run, slot_pct);
       if (e != cudaSuccess) return e;
       // FENIX_PROLONG_MARCH=0 keeps k_sweep_v4<2> for the sweep with the prolongation
       static const bool prolong_march = env_int("FENIX_PROLONG_MARCH", 1, 0, 1) == 1;

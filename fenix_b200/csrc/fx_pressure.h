@@ -47,8 +47,14 @@ cudaError_t march_wsweep(cudaStream_t s, Dims dm, const float* rhs, const float*
 
 bool sweep_variant_valid(int variant, Dims dm);
 int sweep_variant_default(Dims dm);
+// slot_pct < 100 plans the marching sweep for that share of the resident blocks
+// (longer runs, the rest of each SM free for another stream's kernels); the
+// results are the same bits.
 cudaError_t lean_sweep_variant(cudaStream_t s, int variant, Dims dm, const float* div, const float* src, float* dst, Dims mid,
-                               const float* mid_p);
+                               const float* mid_p, int slot_pct = 100);
+// The share of the resident blocks for the fine sweeps that run beside the mid
+// and coarse levels (FENIX_MARCH_SHARE, percent; default 50).
+int march_share_pct();
 cudaError_t lean_prolong_zero(cudaStream_t s, Dims dm, float* dst, Dims mid, const float* mid_p);
 
 // Counts the floats x (all 2^32 bit patterns, NaNs excluded) for which the
