@@ -1304,6 +1304,9 @@ fx_status fused_init(FusedWork& w, cudaStream_t) {
   if (cudaStreamCreateWithFlags(&w.aux2, cudaStreamNonBlocking) != cudaSuccess) return FX_ERR_CUDA;
   if (cudaEventCreateWithFlags(&w.fork_ev, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
   if (cudaEventCreateWithFlags(&w.join_ev, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
+  if (cudaStreamCreateWithFlags(&w.aux3, cudaStreamNonBlocking) != cudaSuccess) return FX_ERR_CUDA;
+  if (cudaEventCreateWithFlags(&w.fork2_ev, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
+  if (cudaEventCreateWithFlags(&w.join2_ev, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
   w.valid = true;  // the arena starts cleared: every brick is zero
   return FX_OK;
 }
@@ -1339,6 +1342,11 @@ void fused_release(FusedWork& w) {
   if (w.fork_ev) cudaEventDestroy(w.fork_ev);
   if (w.join_ev) cudaEventDestroy(w.join_ev);
   w.fork_ev = w.join_ev = nullptr;
+  if (w.aux3) cudaStreamDestroy(w.aux3);
+  w.aux3 = nullptr;
+  if (w.fork2_ev) cudaEventDestroy(w.fork2_ev);
+  if (w.join2_ev) cudaEventDestroy(w.join2_ev);
+  w.fork2_ev = w.join2_ev = nullptr;
   for (auto& ev : w.timing_events) cudaEventDestroy(ev);
   w.timing_events.clear();
 }
@@ -1633,6 +1641,16 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
       if (e != cudaSuccess) return e;
       ls = w.aux2;
     }
+    // The coarse level needs the restricted divergence, not the mid
+    // pre-sweeps: beside the fine sweeps it runs on a third stream next to
+    // them, and the prolongation into the mid level waits for both.
+    cudaStream_t cs = ls;
+    if (side) {
+      cudaError_t e = cudaEventRecord(w.fork2_ev, ls);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(w.aux3, w.fork2_ev, 0);
+      if (e != cudaSuccess) return e;
+      cs = w.aux3;
+    }
     int a = 0;
     for (int k = 0; k < st.q[4]; ++k) {
       Timed tm(w, ls, "fused_sweep_mid");
@@ -1643,17 +1661,22 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     }
     const int mid_pre = a;
     {
-      Timed tm(w, ls, "fused_restrict");
-      plain_restrict(ls, M.dm, C.dm, M.div, C.div);
+      Timed tm(w, cs, "fused_restrict");
+      plain_restrict(cs, M.dm, C.dm, M.div, C.div);
       ++launches;
     }
     int coarse = 0;
     for (int k = 0; k < st.q[6]; ++k) {
-      Timed tm(w, ls, "fused_sweep_coarse");
-      cudaError_t e = lean_sweep_variant(ls, st.sweep_variant[2], C.dm, C.div, k == 0 ? nullptr : C.p[coarse], C.p[coarse ^ 1], C.dm, nullptr);
+      Timed tm(w, cs, "fused_sweep_coarse");
+      cudaError_t e = lean_sweep_variant(cs, st.sweep_variant[2], C.dm, C.div, k == 0 ? nullptr : C.p[coarse], C.p[coarse ^ 1], C.dm, nullptr);
       if (e != cudaSuccess) return e;
       coarse ^= 1;
       ++launches;
+    }
+    if (side) {
+      cudaError_t e = cudaEventRecord(w.join2_ev, cs);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(ls, w.join2_ev, 0);
+      if (e != cudaSuccess) return e;
     }
     {
       Timed tm(w, ls, "fused_prolong");

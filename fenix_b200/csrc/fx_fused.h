@@ -69,6 +69,8 @@ struct FusedWork {
   cudaStream_t aux = nullptr;      // captures the V-cycle body graph
   cudaStream_t aux2 = nullptr;     // the mid and coarse pressure levels, beside the fine pre-sweeps
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  cudaStream_t aux3 = nullptr;     // the coarse level, beside the mid pre-sweeps on aux2
+  cudaEvent_t fork2_ev = nullptr, join2_ev = nullptr;
   int* host_cont = nullptr;        // pinned: the continue flag, read by the host loop without graphs
   uint32_t* host_list_inj = nullptr;  // pinned staging for list_inj (+ count at [nb])
   cudaEvent_t inj_event = nullptr;
