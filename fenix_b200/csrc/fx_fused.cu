@@ -2014,7 +2014,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     for (int k = 2; k <= m; ++k) {
       const bool add = prolong_live && k == m;
       if (add && overlap) FX_CK(cudaStreamWaitEvent(s, w.join_ev, 0));
-      Timed tm(w, s, add ? "fused_sweep_prolong" : "fused_sweep");
+      Timed tm(w, s, add ? "fused_sweep_prolong" : (overlap ? "fused_sweep_shared" : "fused_sweep"));
       // The sweeps beside the lower levels take part of each SM: at 64
       // registers four marching blocks fill an SM's register file, and the
       // second stream's small sweeps would otherwise wait for a whole sweep to

@@ -16,6 +16,8 @@ def kernel_bytes_table(storage: str = "f32") -> dict:
     return {
         # p 4 + div 4 read, p 4 written
         "fused_sweep": ("dense", 12.0),
+        # the same kernel beside the mid and coarse levels, on half the resident blocks
+        "fused_sweep_shared": ("dense", 12.0),
         # the same plus the mid-level pressure (one mid value per 8 fine voxels)
         "fused_sweep_prolong": ("dense", 12.5),
         # velocity 12 read; divergence 4, first sweep 4, mid divergence 0.5 written
