@@ -42,7 +42,26 @@ FX_DEV float poly_cos(float r) {
   return fmaf(p, r2, 1.0f);
 }
 
+// Below |x| = 8192 the reduction runs in f32 (four fused multiply-adds with a
+// Cody-Waite split of pi/2 into three 12-bit parts and the rounded rest; Cody and
+// Waite, "Software Manual for the Elementary Functions", 1980): with |k| < 2^13
+// the first two steps are exact and the split's error stays below 2^-50, so the
+// reduced argument is within about one unit in the last place. Larger and
+// non-finite arguments take the double reduction.
+FX_DEV float pinned_quadrant(float r, int q) {
+  const float s = (q & 1) ? poly_cos(r) : poly_sin(r);
+  return (q & 2) ? -s : s;
+}
+
 FX_DEV float pinned_sincos(float x, int quadrant_offset) {
+  if (fabsf(x) < 8192.0f) {
+    const float kf = rintf(x * 0x1.45f306p-1f);
+    float r = fmaf(-kf, 0x1.92p+0f, x);
+    r = fmaf(-kf, 0x1.fb4p-12f, r);
+    r = fmaf(-kf, 0x1.444p-24f, r);
+    r = fmaf(-kf, 0x1.68c234p-39f, r);
+    return pinned_quadrant(r, (int)kf + quadrant_offset);
+  }
   const double xd = (double)x;
   const double k = rint(xd * 0x1.45f306dc9c883p-1);
   double r = fma(-k, 0x1.921fb544p+0, xd);

@@ -87,8 +87,41 @@ inline float poly_cos(float r) {
   return std::fma(p, r2, 1.0f);
 }
 
+// Below |x| = 8192 the reduction runs in f32: k = rint(x * RN(2/pi)), then
+// r = x - k*P1 - k*P2 - k*P3 - k*P4 by four fused multiply-adds with a Cody-Waite
+// split of pi/2 into three 12-bit parts and the rounded rest (pi/2 - sum < 2^-63).
+// With |k| < 2^13 the first two steps are exact (x and the products share a
+// 2^-24 grid and the differences are below 1), the third is exact whenever
+// |r| < 2^-11, and the split's error k * 2^-63 stays below 2^-50; the reduced
+// argument is within about one unit in the last place, as in Cody and Waite,
+// "Software Manual for the Elementary Functions" (1980). k may be off by one
+// at quadrant boundaries; |r| then slightly exceeds pi/4, where the polynomials
+// are still accurate. Larger and non-finite arguments take the double path.
+constexpr float kTwoOverPiF = 0x1.45f306p-1f;
+constexpr float kPio2F_1 = 0x1.92p+0f;
+constexpr float kPio2F_2 = 0x1.fb4p-12f;
+constexpr float kPio2F_3 = 0x1.444p-24f;
+constexpr float kPio2F_4 = 0x1.68c234p-39f;
+
+inline float poly_quadrant(float r, int q) {
+  switch (q & 3) {
+    case 0: return poly_sin(r);
+    case 1: return poly_cos(r);
+    case 2: return -poly_sin(r);
+    default: return -poly_cos(r);
+  }
+}
+
 // quadrant_offset: 0 for sin, 1 for cos (cos x = sin(x + pi/2)).
 inline float pinned_sincos(float x, int quadrant_offset) {
+  if (std::fabs(x) < 8192.0f) {
+    const float kf = std::rint(x * kTwoOverPiF);
+    float r = std::fma(-kf, kPio2F_1, x);
+    r = std::fma(-kf, kPio2F_2, r);
+    r = std::fma(-kf, kPio2F_3, r);
+    r = std::fma(-kf, kPio2F_4, r);
+    return poly_quadrant(r, (int)kf + quadrant_offset);
+  }
   const double xd = (double)x;
   const double k = std::rint(xd * kTwoOverPi);
   double r = std::fma(-k, kPio2_1, xd);

@@ -226,13 +226,22 @@ def test_constant_velocity_advects_to_itself():
 
 
 def test_pinned_sin_cos_accuracy():
-    x = np.concatenate([np.linspace(-10, 10, 20001), RNG.uniform(-1e4, 1e4, 50000), RNG.uniform(-2e7, 2e7, 50000)]).astype(F)
+    """The pinned sine and cosine against double libm: below 2.5 units in the last
+    place, also at the floats nearest to multiples of pi/2 (where the f32 reduction
+    cancels most) on both sides of the |x| = 8192 switch to the double reduction.
+    WGSL itself only bounds sin/cos by an absolute error of 2^-11 on [-pi, pi]."""
+    near = []
+    for k in np.concatenate([np.arange(-5300, 5301), RNG.integers(-13_000_000, 13_000_000, 20000)]):
+        c = np.float32(k * np.pi / 2)
+        near += [c, np.nextafter(c, F(np.inf)), np.nextafter(c, F(-np.inf))]
+    x = np.concatenate([np.linspace(-10, 10, 20001), RNG.uniform(-1e4, 1e4, 200000), RNG.uniform(-2e7, 2e7, 50000),
+                        np.array(near, F)]).astype(F)
     xd = x.astype(np.float64)
     for fn, ref_fn in ((pinned_sin, np.sin), (pinned_cos, np.cos)):
         got = fn(x).astype(np.float64)
         exact = ref_fn(xd)
         ulp = np.spacing(np.abs(exact).astype(F)).astype(np.float64)
-        assert np.max(np.abs(got - exact) / ulp) < 2.0
+        assert np.max(np.abs(got - exact) / ulp) < 2.5
     assert pinned_sin(np.array([0.0], F))[0] == 0.0 and pinned_cos(np.array([0.0], F))[0] == 1.0
 
 
