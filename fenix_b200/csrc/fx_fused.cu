@@ -1307,6 +1307,7 @@ fx_status fused_init(FusedWork& w, cudaStream_t) {
   if (cudaStreamCreateWithFlags(&w.aux3, cudaStreamNonBlocking) != cudaSuccess) return FX_ERR_CUDA;
   if (cudaEventCreateWithFlags(&w.fork2_ev, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
   if (cudaEventCreateWithFlags(&w.join2_ev, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
+  if (vcycle_init() != cudaSuccess) return FX_ERR_CUDA;
   w.valid = true;  // the arena starts cleared: every brick is zero
   return FX_OK;
 }

@@ -538,7 +538,62 @@ FX_DEV int tail_smooth(const LevelBuf& B, int sweeps, int start, const VCycleCon
   return a;
 }
 
-__global__ void __launch_bounds__(kTailThreads) k_vcycle_tail(VCycleLevels L, VCycleConfig c, int k0) {
+// The coarsest level's sweeps with its two buffers and right-hand side held in
+// shared memory (up to kTailSharedVox voxels): each thread's voxel indices and
+// boundary tests are worked out once, and a sweep reads only shared memory. Each
+// voxel is computed as in tail_sweep, in its operation order, so the results are
+// the same bits; both buffers are written back, as the ping-pong leaves them.
+constexpr uint32_t kTailSharedVox = 8192;
+constexpr int kTailSharedPer = (int)(kTailSharedVox / kTailThreads);
+
+FX_DEV int tail_smooth_shared(const LevelBuf& B, int sweeps, int start, const VCycleConfig& c, float* sm) {
+  const Dims d = B.dm;
+  const uint32_t n = d.w * d.h * d.d, sy = d.w, sz = d.w * d.h;
+  float* P[2] = {sm, sm + n};
+  float* R = sm + 2 * n;
+  for (uint32_t i = threadIdx.x; i < n; i += kTailThreads) {
+    P[0][i] = B.p[start][i];
+    P[1][i] = B.p[start ^ 1][i];
+    R[i] = B.div[i];
+  }
+  bool valid[kTailSharedPer], inner[kTailSharedPer];
+#pragma unroll
+  for (int k = 0; k < kTailSharedPer; ++k) {
+    const uint32_t i = threadIdx.x + (uint32_t)k * kTailThreads;
+    valid[k] = i < n;
+    const uint32_t x = i % d.w, y = (i / d.w) % d.h, z = i / sz;
+    inner[k] = valid[k] && !is_boundary(d, x, y, z);
+  }
+  __syncthreads();
+  int a = 0;
+  for (int it = 0; it < sweeps; ++it) {
+    const float* src = P[a];
+    float* dst = P[a ^ 1];
+#pragma unroll
+    for (int k = 0; k < kTailSharedPer; ++k) {
+      if (!valid[k]) continue;
+      const uint32_t i = threadIdx.x + (uint32_t)k * kTailThreads;
+      float v = 0.0f;
+      if (inner[k]) {
+        const float t = src[i + 1] + src[i - 1] + src[i + sy] + src[i - sy] + src[i + sz] + src[i - sz];
+        const float j = div6(t - R[i]);
+        const float cm = src[i];
+        v = c.omega_one ? j : cm + c.omega * (j - cm);
+      }
+      dst[i] = v;
+    }
+    __syncthreads();
+    a ^= 1;
+  }
+  for (uint32_t i = threadIdx.x; i < n; i += kTailThreads) {
+    B.p[start][i] = P[0][i];
+    B.p[start ^ 1][i] = P[1][i];
+  }
+  __syncthreads();
+  return start ^ (sweeps & 1);
+}
+
+__global__ void __launch_bounds__(kTailThreads) k_vcycle_tail(VCycleLevels L, VCycleConfig c, int k0, int coarse_shared) {
   int a[kMaxVLevels];
   for (int k = k0; k < c.levels - 1; ++k) {
     const LevelBuf& B = L.lv[k];
@@ -549,7 +604,9 @@ __global__ void __launch_bounds__(kTailThreads) k_vcycle_tail(VCycleLevels L, VC
     for (uint32_t i = threadIdx.x; i < nc; i += kTailThreads) C.p[0][i] = 0.0f;
     __syncthreads();
   }
-  int e = tail_smooth(L.lv[c.levels - 1], c.coarse, 0, c);
+  extern __shared__ float tail_sm[];
+  int e = coarse_shared ? tail_smooth_shared(L.lv[c.levels - 1], c.coarse, 0, c, tail_sm)
+                        : tail_smooth(L.lv[c.levels - 1], c.coarse, 0, c);
   for (int k = c.levels - 2; k >= k0; --k) {
     const LevelBuf& B = L.lv[k];
     const LevelBuf& C = L.lv[k + 1];
@@ -721,7 +778,9 @@ int level_cycle(cudaStream_t s, const VCycleLevels& L, const VCycleConfig& c, in
   // A small level and everything below it: one block, one launch (the caller has
   // restricted its right-hand side and cleared p[0], so start is 0).
   if (!c.plain && k > 0 && start == 0 && count_of(B.dm) <= kTailVoxels) {
-    k_vcycle_tail<<<1, kTailThreads, 0, s>>>(L, c, k);
+    const uint32_t nc = count_of(L.lv[c.levels - 1].dm);
+    const int shared = nc <= kTailSharedVox ? 1 : 0;
+    k_vcycle_tail<<<1, kTailThreads, shared ? 3 * nc * sizeof(float) : 0, s>>>(L, c, k, shared);
     ++*launches;
     return cycle_end_id(c, k, 0);
   }
@@ -770,6 +829,10 @@ cudaError_t solver_norms(cudaStream_t s, Dims dm, const float* div, const float*
   const int nres = resid_norm(s, dm, div, p, st->part_res, false);
   k_finalize<<<1, 256, 0, s>>>(st, tol, 0, 0, nres, (int)reduce_blocks(), 0);
   return cudaGetLastError();
+}
+
+cudaError_t vcycle_init() {
+  return cudaFuncSetAttribute(k_vcycle_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(3 * kTailSharedVox * sizeof(float)));
 }
 
 cudaError_t max_divergence(cudaStream_t s, Dims dm, VelField v, SolverDev* st) {

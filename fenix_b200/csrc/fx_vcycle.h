@@ -63,5 +63,7 @@ cudaError_t solver_norms(cudaStream_t s, Dims dm, const float* div, const float*
 
 // max |0.5 (central differences of v)| over interior voxels, in FP64.
 cudaError_t max_divergence(cudaStream_t s, Dims dm, VelField v, SolverDev* st);
+// Once per device before the first V-cycle (the tail kernel's shared memory).
+cudaError_t vcycle_init();
 
 }  // namespace fx
