@@ -442,9 +442,33 @@ __global__ void __launch_bounds__(256) k_sweep_v4(Dims dm, const float* __restri
 // WEIGHTED is the V-cycle's weighted sweep (an extension, fx_vcycle.cu): each
 // interior value becomes c + w (j - c), with j the Jacobi value above and c the
 // source value, in that operation order; the boundary stays 0.
-template <bool WEIGHTED>
+// With NORM the kernel also adds up, in FP64, the squared residual
+// rhs - (sum of the 6 neighbours - 6 p) of its source over the interior voxels it
+// visits (the residual norm of k_resid_norm_march, per voxel in the same
+// operations), one deterministic partial per block into norm_part.
+FX_DEV void block_sum_double(double v, double* part) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __shared__ double warp_sums[8];  // blocks of 32 x 8 threads
+  if (threadIdx.x == 0) warp_sums[threadIdx.y] = v;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    double t = 0.0;
+    for (int k = 0; k < 8; ++k) t += warp_sums[k];
+    part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = t;
+  }
+}
+
+FX_DEV double resid_sq(float xp, float xm, float yp, float ym, float zp, float zm, float c, float rh) {
+  const double s = (double)xp + (double)xm + (double)yp + (double)ym + (double)zp + (double)zm;
+  const double r = (double)rh - (s - 6.0 * (double)c);
+  return r * r;
+}
+
+template <bool WEIGHTED, bool NORM = false>
 __global__ void __launch_bounds__(256, 4) k_sweep_march(Dims dm, const float* __restrict__ div, const float* __restrict__ src,
-                                                        float* __restrict__ dst, int run, float w) {
+                                                        float* __restrict__ dst, int run, float w, double* norm_part = nullptr) {
+  double s2 = 0.0;
+  [&]() {
   const uint32_t lane = threadIdx.x;
   const uint32_t x0 = blockIdx.x * 128 + 4 * lane, y = blockIdx.y * 8 + threadIdx.y;
   const int zb = (int)blockIdx.z * run, ze = min(zb + run, (int)dm.d);
@@ -511,6 +535,12 @@ __global__ void __launch_bounds__(256, 4) k_sweep_march(Dims dm, const float* __
           v.z = c0.z + w * (v.z - c0.z);
           if (int3) v.w = c0.w + w * (v.w - c0.w);
         }
+        if (NORM) {
+          if (int0) s2 += resid_sq(c0.y, left, yp.x, ym.x, cp.x, cm.x, c0.x, dv.x);
+          s2 += resid_sq(c0.z, c0.x, yp.y, ym.y, cp.y, cm.y, c0.y, dv.y);
+          s2 += resid_sq(c0.w, c0.y, yp.z, ym.z, cp.z, cm.z, c0.z, dv.z);
+          if (int3) s2 += resid_sq(right, c0.z, yp.w, ym.w, cp.w, cm.w, c0.w, dv.w);
+        }
       }
       dst4[(base + sz * (uint32_t)z) >> 2] = v;
     }
@@ -523,6 +553,8 @@ __global__ void __launch_bounds__(256, 4) k_sweep_march(Dims dm, const float* __
     xle = n_xle;
     xre = n_xre;
   }
+  }();
+  if constexpr (NORM) block_sum_double(s2, norm_part);
 }
 
 // k_sweep_march with the prolongation of mid_p added (the first fine post-sweep),
@@ -901,6 +933,32 @@ cudaError_t march_wsweep(cudaStream_t s, Dims dm, const float* rhs, const float*
     k_sweep_march<false><<<g, dim3(32, 8, 1), 0, s>>>(dm, rhs, src, dst, run, 1.0f);
   else
     k_sweep_march<true><<<g, dim3(32, 8, 1), 0, s>>>(dm, rhs, src, dst, run, w);
+  return cudaGetLastError();
+}
+
+cudaError_t march_wsweep_norm(cudaStream_t s, Dims dm, const float* rhs, const float* src, float* dst, float w, bool one,
+                              double* part, int* nparts) {
+  if (dm.w % 4 != 0 || dm.w < 8 || !src) return cudaErrorNotSupported;
+  static int slots[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  int n = (dev >= 0 && dev < 64) ? slots[dev] : 0;
+  if (n <= 0) {
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_march<true, true>, 256, 0);
+    if (e != cudaSuccess) return e;
+    n = std::max(1, per_sm) * device_sm_count();
+    if (dev >= 0 && dev < 64) slots[dev] = n;
+  }
+  const int run = march_plan_one_wave(dm, n);
+  const dim3 g((dm.w + 127) / 128, (dm.h + 7) / 8, (dm.d + run - 1) / run);
+  if ((int)(g.x * g.y * g.z) > *nparts) return cudaErrorNotSupported;
+  *nparts = (int)(g.x * g.y * g.z);
+  if (one)
+    k_sweep_march<false, true><<<g, dim3(32, 8, 1), 0, s>>>(dm, rhs, src, dst, run, 1.0f, part);
+  else
+    k_sweep_march<true, true><<<g, dim3(32, 8, 1), 0, s>>>(dm, rhs, src, dst, run, w, part);
   return cudaGetLastError();
 }
 

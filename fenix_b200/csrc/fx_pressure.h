@@ -44,6 +44,11 @@ int march_plan_waves(Dims dm, int tx, int ty, int slots);
 // when `one`) as the marching four-x kernel: same bits as the V-cycle's
 // one-x kernel. cudaErrorNotSupported where the width is not a multiple of 4.
 cudaError_t march_wsweep(cudaStream_t s, Dims dm, const float* rhs, const float* src, float* dst, float w, bool one);
+// march_wsweep that also writes the FP64 squared residual norm of src, one
+// partial per block, into part (at most *nparts; *nparts gets the count).
+// cudaErrorNotSupported where march_wsweep refuses or the blocks outnumber *nparts.
+cudaError_t march_wsweep_norm(cudaStream_t s, Dims dm, const float* rhs, const float* src, float* dst, float w, bool one,
+                              double* part, int* nparts);
 
 bool sweep_variant_valid(int variant, Dims dm);
 int sweep_variant_default(Dims dm);

@@ -773,7 +773,10 @@ int cycle_end_id(const VCycleConfig& c, int k, int start) {
   return b ^ (c.post & 1);
 }
 
-int level_cycle(cudaStream_t s, const VCycleLevels& L, const VCycleConfig& c, int k, int start, uint32_t* launches) {
+// first_done: the level's first pre-sweep has already run (fused with the
+// residual norm, see fused_norm_sweep), from p[start] into p[start ^ 1].
+int level_cycle(cudaStream_t s, const VCycleLevels& L, const VCycleConfig& c, int k, int start, uint32_t* launches,
+                bool first_done = false) {
   const LevelBuf& B = L.lv[k];
   // A small level and everything below it: one block, one launch (the caller has
   // restricted its right-hand side and cleared p[0], so start is 0).
@@ -785,7 +788,7 @@ int level_cycle(cudaStream_t s, const VCycleLevels& L, const VCycleConfig& c, in
     return cycle_end_id(c, k, 0);
   }
   if (k == c.levels - 1) return smooth(s, B, c.coarse, start, c, launches);
-  const int a = smooth(s, B, c.pre, start, c, launches);
+  const int a = first_done ? smooth(s, B, c.pre - 1, start ^ 1, c, launches) : smooth(s, B, c.pre, start, c, launches);
   const LevelBuf& C = L.lv[k + 1];
   resid_restrict(s, B, B.p[a], C, c.plain);
   fill0(s, C.p[0], C.dm);
@@ -799,6 +802,37 @@ int level_cycle(cudaStream_t s, const VCycleLevels& L, const VCycleConfig& c, in
 
 }  // namespace
 
+// Whether the fine level's residual norm rides on the next cycle's first
+// pre-sweep: the marching kernels, at least one pre-sweep and a fine level with
+// more than one level below it (a cycle's fine pre-smoothing starts from p[start]).
+bool fuse_norm(const VCycleLevels& L, const VCycleConfig& c) {
+  return !c.plain && c.pre >= 1 && c.levels >= 2 && L.lv[0].dm.w % 4 == 0 && L.lv[0].dm.w >= 8;
+}
+
+// The residual norm of p[start] (its partials into st->part_res) and, in the same
+// pass, the first pre-sweep of the next cycle from p[start] into p[start ^ 1]:
+// both read the same neighbours. When the norm stops the loop, the sweep's output
+// is left unused in p[start ^ 1] (the result stays in p[start]). Returns the
+// partial count, or 0 where the fused kernel refuses.
+int fused_norm_sweep(cudaStream_t s, const LevelBuf& F, const VCycleConfig& c, int start, SolverDev* st) {
+  int n = kNormParts;
+  if (march_wsweep_norm(s, F.dm, F.div, F.p[start], F.p[start ^ 1], c.omega, c.omega_one, st->part_res, &n) != cudaSuccess) {
+    (void)cudaGetLastError();  // a host-side refusal: nothing was launched
+    return 0;
+  }
+  return n;
+}
+
+// The fused pass, or where the kernel refuses, the norm and the first pre-sweep
+// apart (the next cycle expects that sweep done either way).
+int norm_and_first_sweep(cudaStream_t s, const LevelBuf& F, const VCycleConfig& c, int start, SolverDev* st, uint32_t* launches) {
+  int n = fused_norm_sweep(s, F, c, start, st);
+  if (n > 0) return n;
+  n = resid_norm(s, F.dm, F.div, F.p[start], st->part_res, c.plain);
+  smooth(s, F, 1, start, c, launches);
+  return n;
+}
+
 cudaError_t vcycle_prologue(cudaStream_t s, const VCycleLevels& L, const VCycleConfig& c, int start, SolverDev* st,
                             cudaGraphConditionalHandle cond) {
   const LevelBuf& F = L.lv[0];
@@ -806,7 +840,8 @@ cudaError_t vcycle_prologue(cudaStream_t s, const VCycleLevels& L, const VCycleC
   if (e != cudaSuccess) return e;
   if (!c.warm) fill0(s, F.p[start], F.dm);
   k_sumsq<<<reduce_blocks(), 256, 0, s>>>(F.div, count_of(F.dm), st->part_rhs);
-  const int nres = resid_norm(s, F.dm, F.div, F.p[start], st->part_res, c.plain);
+  uint32_t extra = 0;
+  const int nres = fuse_norm(L, c) ? norm_and_first_sweep(s, F, c, start, st, &extra) : resid_norm(s, F.dm, F.div, F.p[start], st->part_res, c.plain);
   k_finalize<<<1, 256, 0, s>>>(st, c.tol, c.max_cycles, 0, nres, (int)reduce_blocks(), cond);
   return cudaGetLastError();
 }
@@ -814,9 +849,12 @@ cudaError_t vcycle_prologue(cudaStream_t s, const VCycleLevels& L, const VCycleC
 cudaError_t vcycle_body(cudaStream_t s, const VCycleLevels& L, const VCycleConfig& c, int start, SolverDev* st,
                         cudaGraphConditionalHandle cond, uint32_t* launches) {
   const LevelBuf& F = L.lv[0];
-  const int fin = level_cycle(s, L, c, 0, start, launches);
+  // The prologue and every body end with the fused norm and first pre-sweep
+  // whenever fuse_norm holds (the host decides both the same way).
+  const bool fused = fuse_norm(L, c);
+  const int fin = level_cycle(s, L, c, 0, start, launches, fused);
   (void)fin;  // == start: the fine level ends in the buffer it started from
-  const int nres = resid_norm(s, F.dm, F.div, F.p[start], st->part_res, c.plain);
+  const int nres = fused ? norm_and_first_sweep(s, F, c, start, st, launches) : resid_norm(s, F.dm, F.div, F.p[start], st->part_res, c.plain);
   k_finalize<<<1, 256, 0, s>>>(st, c.tol, c.max_cycles, 1, nres, 0, cond);
   *launches += 2;
   return cudaGetLastError();
