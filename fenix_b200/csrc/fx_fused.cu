@@ -1307,6 +1307,8 @@ fx_status fused_init(FusedWork& w, cudaStream_t) {
   if (cudaStreamCreateWithFlags(&w.aux3, cudaStreamNonBlocking) != cudaSuccess) return FX_ERR_CUDA;
   if (cudaEventCreateWithFlags(&w.fork2_ev, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
   if (cudaEventCreateWithFlags(&w.join2_ev, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
+  if (cudaEventCreateWithFlags(&w.prep_fork_ev, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
+  if (cudaEventCreateWithFlags(&w.prep_join_ev, cudaEventDisableTiming) != cudaSuccess) return FX_ERR_CUDA;
   if (vcycle_init() != cudaSuccess) return FX_ERR_CUDA;
   w.valid = true;  // the arena starts cleared: every brick is zero
   return FX_OK;
@@ -1348,6 +1350,9 @@ void fused_release(FusedWork& w) {
   if (w.fork2_ev) cudaEventDestroy(w.fork2_ev);
   if (w.join2_ev) cudaEventDestroy(w.join2_ev);
   w.fork2_ev = w.join2_ev = nullptr;
+  if (w.prep_fork_ev) cudaEventDestroy(w.prep_fork_ev);
+  if (w.prep_join_ev) cudaEventDestroy(w.prep_join_ev);
+  w.prep_fork_ev = w.prep_join_ev = nullptr;
   for (auto& ev : w.timing_events) cudaEventDestroy(ev);
   w.timing_events.clear();
 }
@@ -1719,25 +1724,36 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     ++launches;
   }
 
+  // In dense mode the interleaved copy and the current flags do not feed the
+  // velocity advection: they run on the second stream beside it, joined before
+  // the scalar advection. (Sparse mode's velocity advection needs the flags.)
+  const bool side_prep = !st.sparse;
+  cudaStream_t ps = s;
+  if (side_prep) {
+    FX_CK(cudaEventRecord(w.prep_fork_ev, s));
+    FX_CK(cudaStreamWaitEvent(w.aux2, w.prep_fork_ev, 0));
+    ps = w.aux2;
+  }
   // the interleaved copy of the current set for the scalar advection
   {
-    Timed tm(w, s, "fused_pack_aos");
+    Timed tm(w, ps, "fused_pack_aos");
     by_storage(st.half_storage, [&](auto tag) {
       using S = typename decltype(tag)::type;
-      k_pack_aos<S><<<(nb + 7) / 8, dim3(32, 8), 0, s>>>(dm, bc, sset<S>(st.cur), w.nz_set[cur], w.nz_aos,
-                                                         static_cast<typename Aos<S>::T*>(w.aos));
+      k_pack_aos<S><<<(nb + 7) / 8, dim3(32, 8), 0, ps>>>(dm, bc, sset<S>(st.cur), w.nz_set[cur], w.nz_aos,
+                                                          static_cast<typename Aos<S>::T*>(w.aos));
     });
     ++launches;
   }
 
   // 2. flags of the current set, list of bricks for scalar advection
-  FX_CK(cudaMemsetAsync(w.counters, 0, 3 * sizeof(uint32_t), s));
-  if (st.sparse) FX_CK(cudaMemsetAsync(w.counters + 4, 0, 4 * sizeof(uint32_t), s));
+  FX_CK(cudaMemsetAsync(w.counters, 0, 3 * sizeof(uint32_t), ps));
+  if (st.sparse) FX_CK(cudaMemsetAsync(w.counters + 4, 0, 4 * sizeof(uint32_t), ps));
   {
-    Timed tm(w, s, "fused_dilate");
-    k_dilate<<<(nb + 255) / 256, 256, 0, s>>>(bc, w.summary_set[cur], st.flags_cur, w.nz_t, nullptr, w.list_adv, c_adv);
+    Timed tm(w, ps, "fused_dilate");
+    k_dilate<<<(nb + 255) / 256, 256, 0, ps>>>(bc, w.summary_set[cur], st.flags_cur, w.nz_t, nullptr, w.list_adv, c_adv);
     ++launches;
   }
+  if (side_prep) FX_CK(cudaEventRecord(w.prep_join_ev, ps));
   // 3. velocity advection (dense; sparse mode: over the current flags)
   if (st.sparse) {
     if (st.solver_mode != 0) return FX_ERR_UNSUPPORTED;
@@ -1777,6 +1793,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     ++launches;
   }
   // 4. scalar advection over the list
+  if (side_prep) FX_CK(cudaStreamWaitEvent(s, w.prep_join_ev, 0));
   FX_CK(cudaMemsetAsync(w.summary_t, 0, nb, s));
   {
     Timed tm(w, s, "fused_advect_scalars");

@@ -71,6 +71,7 @@ struct FusedWork {
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   cudaStream_t aux3 = nullptr;     // the coarse level, beside the mid pre-sweeps on aux2
   cudaEvent_t fork2_ev = nullptr, join2_ev = nullptr;
+  cudaEvent_t prep_fork_ev = nullptr, prep_join_ev = nullptr;  // the copy and flags beside the velocity advection
   int* host_cont = nullptr;        // pinned: the continue flag, read by the host loop without graphs
   uint32_t* host_list_inj = nullptr;  // pinned staging for list_inj (+ count at [nb])
   cudaEvent_t inj_event = nullptr;
