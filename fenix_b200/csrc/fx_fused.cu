@@ -1724,16 +1724,14 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     ++launches;
   }
 
-  // In dense mode the interleaved copy and the current flags do not feed the
-  // velocity advection: they run on the second stream beside it, joined before
-  // the scalar advection. (Sparse mode's velocity advection needs the flags.)
-  const bool side_prep = !st.sparse;
-  cudaStream_t ps = s;
-  if (side_prep) {
-    FX_CK(cudaEventRecord(w.prep_fork_ev, s));
-    FX_CK(cudaStreamWaitEvent(w.aux2, w.prep_fork_ev, 0));
-    ps = w.aux2;
-  }
+  // The interleaved copy, and in dense mode the current flags too, do not feed
+  // the velocity advection: they run on the second stream beside it, joined
+  // before the scalar advection. (Sparse mode's velocity advection walks the
+  // current flags, so there they stay on the step's stream.)
+  FX_CK(cudaEventRecord(w.prep_fork_ev, s));
+  FX_CK(cudaStreamWaitEvent(w.aux2, w.prep_fork_ev, 0));
+  const cudaStream_t ps = w.aux2;
+  const cudaStream_t fs = st.sparse ? s : w.aux2;
   // the interleaved copy of the current set for the scalar advection
   {
     Timed tm(w, ps, "fused_pack_aos");
@@ -1746,14 +1744,14 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
   }
 
   // 2. flags of the current set, list of bricks for scalar advection
-  FX_CK(cudaMemsetAsync(w.counters, 0, 3 * sizeof(uint32_t), ps));
-  if (st.sparse) FX_CK(cudaMemsetAsync(w.counters + 4, 0, 4 * sizeof(uint32_t), ps));
+  FX_CK(cudaMemsetAsync(w.counters, 0, 3 * sizeof(uint32_t), fs));
+  if (st.sparse) FX_CK(cudaMemsetAsync(w.counters + 4, 0, 4 * sizeof(uint32_t), fs));
   {
-    Timed tm(w, ps, "fused_dilate");
-    k_dilate<<<(nb + 255) / 256, 256, 0, ps>>>(bc, w.summary_set[cur], st.flags_cur, w.nz_t, nullptr, w.list_adv, c_adv);
+    Timed tm(w, fs, "fused_dilate");
+    k_dilate<<<(nb + 255) / 256, 256, 0, fs>>>(bc, w.summary_set[cur], st.flags_cur, w.nz_t, nullptr, w.list_adv, c_adv);
     ++launches;
   }
-  if (side_prep) FX_CK(cudaEventRecord(w.prep_join_ev, ps));
+  FX_CK(cudaEventRecord(w.prep_join_ev, ps));
   // 3. velocity advection (dense; sparse mode: over the current flags)
   if (st.sparse) {
     if (st.solver_mode != 0) return FX_ERR_UNSUPPORTED;
@@ -1793,7 +1791,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     ++launches;
   }
   // 4. scalar advection over the list
-  if (side_prep) FX_CK(cudaStreamWaitEvent(s, w.prep_join_ev, 0));
+  FX_CK(cudaStreamWaitEvent(s, w.prep_join_ev, 0));
   FX_CK(cudaMemsetAsync(w.summary_t, 0, nb, s));
   {
     Timed tm(w, s, "fused_advect_scalars");
