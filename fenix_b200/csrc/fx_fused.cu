@@ -272,7 +272,8 @@ FX_DEV uint8_t summary_of(const Energy& e) {
 template <typename S>
 __global__ void __launch_bounds__(kBrickThreads) k_inject(Dims dm, uint3 bc, const Params* __restrict__ Pp, const float* __restrict__ src,
                                                           uint32_t nsrc, const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
-                                                          SSet<S> set, VelField v, uint8_t* __restrict__ summary, uint8_t* __restrict__ nz) {
+                                                          SSet<S> set, VelField v, uint8_t* __restrict__ summary, uint8_t* __restrict__ nz,
+                                                          float* __restrict__ tape_t1, float* __restrict__ tape_r1) {
   const Params P = *Pp;
   const uint32_t n = *count;
   for (uint32_t li = blockIdx.x; li < n; li += gridDim.x) {
@@ -298,6 +299,10 @@ __global__ void __launch_bounds__(kBrickThreads) k_inject(Dims dm, uint3 bc, con
         d = qS_at<S>(d, P, i, 0);
         t = qS_at<S>(t, P, i, 1);
         f = qS_at<S>(f, P, i, 2);
+        if (tape_t1) {  // the rollout's tape: after the scalar injection, before the igniter
+          tape_t1[i] = t;
+          tape_r1[i] = r;
+        }
         float vx = v.c[0][i], vy = v.c[1][i], vz = v.c[2][i];
         inject_velocity_voxel(P, src, nsrc, px, py, pz, vx, vy, vz);
         const float lim = speed_limit(P);
@@ -1486,6 +1491,9 @@ uint64_t fused_key(const FusedStep& st, uint32_t ninj) {
   mix_key(st.solver_norms);
   mix_key(st.sparse);
   for (int k = 0; k < kBrickKernels; ++k) mix_key(st.brick_ctas[k]);
+  for (const void* p : {(const void*)st.tape_t1, (const void*)st.tape_r1, (const void*)st.tape_v1.c[0], (const void*)st.tape_a.c[0],
+                        (const void*)st.tape_b.c[0]})
+    mix_key((uint64_t)(uintptr_t)p);
   mix_key((uint64_t)(uintptr_t)st.inflow);
   if (st.inflow)
     for (uint32_t v : {st.inflow_patch.x0, st.inflow_patch.y, st.inflow_patch.z0, st.inflow_patch.nx, st.inflow_patch.nz}) mix_key(v);
@@ -1700,12 +1708,30 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     if (side) return cudaEventRecord(w.join_ev, w.aux2);
     return cudaGetLastError();
   };
+  // The rollout's tape (f32 storage): copies of the velocity at three points of
+  // the step, and temperature and reaction before the igniter, which equal the
+  // fields before the injection outside the emitters' reach and are written by the
+  // injection kernel inside it.
+  const bool taped = st.tape_t1 != nullptr && !st.half_storage;
+  const size_t field_bytes = (size_t)dm.w * dm.h * dm.d * sizeof(float);
+  auto tape_vel = [&](const VelField& dst, const VelField& src) -> cudaError_t {
+    for (int k = 0; k < 3 && dst.c[0]; ++k) {
+      const cudaError_t e = cudaMemcpyAsync(dst.c[k], src.c[k], field_bytes, cudaMemcpyDeviceToDevice, s);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
+  if (taped) {
+    FX_CK(cudaMemcpyAsync(st.tape_t1, st.cur.f[1], field_bytes, cudaMemcpyDeviceToDevice, s));
+    FX_CK(cudaMemcpyAsync(st.tape_r1, st.cur.f[3], field_bytes, cudaMemcpyDeviceToDevice, s));
+  }
   if (ninj) {
     Timed tm(w, s, "fused_inject");
     by_storage(st.half_storage, [&](auto tag) {
       using S = typename decltype(tag)::type;
       k_inject<S><<<brick_grid_of(st, nb, BK_INJECT), kBrickThreads, 0, s>>>(dm, bc, st.params, st.sources, st.nsrc, w.list_inj, c_inj, sset<S>(st.cur), st.vcur,
-                                                       w.summary_set[cur], w.nz_set[cur]);
+                                                       w.summary_set[cur], w.nz_set[cur], taped ? st.tape_t1 : nullptr,
+                                                       taped ? st.tape_r1 : nullptr);
     });
     ++launches;
   }
@@ -1723,6 +1749,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     FX_CK(cudaMemsetAsync(w.vmax, 0xFF, sizeof(unsigned), s));
     ++launches;
   }
+  if (taped) FX_CK(tape_vel(st.tape_v1, st.vcur));
 
   // The interleaved copy, and in dense mode the current flags too, do not feed
   // the velocity advection: they run on the second stream beside it, joined
@@ -1791,6 +1818,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     ++launches;
   }
   // 4. scalar advection over the list
+  if (taped) FX_CK(tape_vel(st.tape_a, st.vscr));
   FX_CK(cudaStreamWaitEvent(s, w.prep_join_ev, 0));
   FX_CK(cudaMemsetAsync(w.summary_t, 0, nb, s));
   {
@@ -1847,6 +1875,7 @@ fx_status fused_sequence(FusedWork& w, const FusedStep& st, uint32_t ninj, Fused
     });
     ++launches;
   }
+  if (taped) FX_CK(tape_vel(st.tape_b, st.vscr));
   // 8. vorticity confinement
   const VelField* vfinal = &st.vscr;
   if (st.vort_on && st.sparse) {

@@ -141,6 +141,13 @@ struct FusedStep {
   bool solver_norms;  // FP64 statistics after the reference schedule too
   bool vort_on, pressure_on, debug_on, debug_fields;
   bool sparse = false;  // sparse mode (extension): velocity passes on the active bricks only
+  // The differentiable rollout's tape (f32 storage, dense mode; all NULL otherwise):
+  // temperature and reaction after the scalar injection and before the igniter,
+  // and the velocity after the injection and inflow, after advection and after
+  // buoyancy, as the plain step records them.
+  float* tape_t1 = nullptr;
+  float* tape_r1 = nullptr;
+  VelField tape_v1{}, tape_a{}, tape_b{};
   int last_p;
 };
 

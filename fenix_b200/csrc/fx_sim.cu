@@ -1851,6 +1851,9 @@ struct fx_rollout {
   // within the speed limit (the fused velocity advection clamps on read, where
   // the plain step leaves the inflow values as they are); both give the same bits.
   bool fused_steps = false;
+  // The taped re-runs of the backward use the fused step too (fused_steps), with
+  // the tape recorded inside it; plain_tape (a test entry) keeps them plain.
+  bool plain_tape = false;
 };
 
 namespace {
@@ -1915,9 +1918,18 @@ fx_status rollout_step(fx_rollout* r, uint32_t k, const PlainHooks& hk) {
   fx_status st = step_begin(s, elapsed, r->d.step_seconds, sp);
   if (st != FX_OK) return st;
   const bool taped = hk.t1 || hk.r1 || hk.v1.c[0] || hk.a.c[0] || hk.b.c[0];
-  if (r->fused_steps && !taped) {
+  const bool full_tape = hk.t1 && hk.r1 && hk.v1.c[0] && hk.a.c[0] && hk.b.c[0];
+  if (r->fused_steps && (!taped || (full_tape && !r->plain_tape))) {
     sp.fs.inflow = hk.inflow;
     sp.fs.inflow_patch = hk.patch;
+    if (taped) {
+      sp.fs.tape_t1 = hk.t1;
+      sp.fs.tape_r1 = hk.r1;
+      sp.fs.tape_v1 = hk.v1;
+      sp.fs.tape_a = hk.a;
+      sp.fs.tape_b = hk.b;
+      sp.fs.debug_fields = true;  // the adjoint reads the curl w of the step
+    }
     FusedResult fr;
     st = fused_step(s->fw, sp.fs, fr);
     if (st != FX_OK) fail(s, st, "fx_rollout: fused step failed: " + fr.error);
@@ -2155,6 +2167,15 @@ fx_status fx_rollout_forward(fx_rollout* r, const float* inflow, double* loss) {
   FX_CUDA(s, cudaMemcpyAsync(loss, r->loss, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   FX_CUDA(s, cudaStreamSynchronize(s->stream));
   r->forward_done = true;
+  return FX_OK;
+}
+
+// Test entry: 1 makes the rollout's taped re-runs use the plain step (the fused
+// step records the same tape; the test compares the gradients of both), 0 the
+// default.
+fx_status fx_test_rollout_plain_tape(fx_rollout* r, int32_t on) {
+  if (!r) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_test_rollout_plain_tape: NULL rollout");
+  r->plain_tape = on != 0;
   return FX_OK;
 }
 

@@ -138,6 +138,24 @@ def test_full_size_gradient_against_the_fixture():
     assert worst_fd <= 1e-3
 
 
+def test_fused_tape_matches_the_plain_tape():
+    """On the fused kernels the backward's taped re-runs are fused steps that record
+    the plain step's tape (temperature and reaction before the igniter, the velocity
+    after the inflow, after advection and after buoyancy, the curl w). The same
+    rollout with the re-runs forced plain gives the same gradient up to the order
+    of the float atomics of the adjoint kernels."""
+    fsim, fro, floss, ffinal, fgi, fgv = run_rollout(AW, fused=True)
+    assert fro._lib.fx_test_rollout_plain_tape(fro._h, 1) == 0
+    start_from(fsim, AW.workload.state)
+    ploss = fro.forward(AW.inflow)
+    pgi, pgv = fro.backward()
+    assert abs(ploss - floss) <= 1e-12 * floss  # the loss is an FP64 atomic sum
+    np.testing.assert_allclose(fgi, pgi, rtol=1e-5, atol=1e-7 * float(np.abs(pgi).max()))
+    np.testing.assert_allclose(fgv.reshape(3, -1), pgv.reshape(3, -1), rtol=1e-4, atol=1e-6 * float(np.abs(pgv).max()))
+    fro.dispose()
+    fsim.dispose()
+
+
 def test_fused_simulation_gives_the_same_rollout(rolled):
     """The fused kernels run the forward and the recomputed steps: the final
     state is the plain rollout's bits, the loss equals it up to the order of the
