@@ -219,12 +219,20 @@ __global__ void k_adj_project(Dims dm, VelField lam_v, VelField lam_c, float* __
 }
 
 // pressure-jacobi.wgsl.ts:15-36: dst = (sum of the 6 neighbours of src - div) / 6.
+// ACCUMULATE false: lam_src holds no adjoint yet (it is treated as zero and
+// written whole), which gives the accumulated bits: 0 + q is q, or +0 for a
+// q that is -0.
+template <bool ACCUMULATE>
 __global__ void k_adj_jacobi(Dims dm, const float* __restrict__ lam_dst, float* __restrict__ lam_src, float* __restrict__ lam_div) {
   FX_VOXEL_PROLOGUE(dm);
   const int X = (int)x, Y = (int)y, Z = (int)z;
   const float acc = interior_val(lam_dst, dm, X + 1, Y, Z) + interior_val(lam_dst, dm, X - 1, Y, Z) + interior_val(lam_dst, dm, X, Y + 1, Z) +
                     interior_val(lam_dst, dm, X, Y - 1, Z) + interior_val(lam_dst, dm, X, Y, Z + 1) + interior_val(lam_dst, dm, X, Y, Z - 1);
-  if (acc != 0.0f) lam_src[i] += acc / 6.0f;
+  if (ACCUMULATE) {
+    if (acc != 0.0f) lam_src[i] += acc / 6.0f;
+  } else {
+    lam_src[i] = acc != 0.0f ? 0.0f + acc / 6.0f : 0.0f;
+  }
   if (!is_boundary(dm, x, y, z)) {
     const float l = lam_dst[i];
     if (l != 0.0f) lam_div[i] += -l / 6.0f;
@@ -668,8 +676,11 @@ void adj_loss(cudaStream_t s, uint32_t n, const float* d, const float* target, f
 void adj_project(cudaStream_t s, Dims dm, VelField lam_v, VelField lam_c, float* lam_p) {
   k_adj_project<<<grid_for(dm), kBlock, 0, s>>>(dm, lam_v, lam_c, lam_p);
 }
-void adj_jacobi(cudaStream_t s, Dims dm, const float* lam_dst, float* lam_src, float* lam_div) {
-  k_adj_jacobi<<<grid_for(dm), kBlock, 0, s>>>(dm, lam_dst, lam_src, lam_div);
+void adj_jacobi(cudaStream_t s, Dims dm, const float* lam_dst, float* lam_src, float* lam_div, bool accumulate) {
+  if (accumulate)
+    k_adj_jacobi<true><<<grid_for(dm), kBlock, 0, s>>>(dm, lam_dst, lam_src, lam_div);
+  else
+    k_adj_jacobi<false><<<grid_for(dm), kBlock, 0, s>>>(dm, lam_dst, lam_src, lam_div);
 }
 void adj_restrict(cudaStream_t s, Dims fine, Dims coarse, const float* lam_coarse, float* lam_fine) {
   k_adj_restrict<<<grid_for(coarse), kBlock, 0, s>>>(fine, coarse, lam_coarse, lam_fine);

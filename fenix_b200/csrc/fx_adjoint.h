@@ -21,7 +21,8 @@ void adj_loss(cudaStream_t s, uint32_t n, const float* d, const float* target, f
 // (0 on the boundary); lam_p = its pressure part (both assigned).
 void adj_project(cudaStream_t s, Dims dm, VelField lam_v, VelField lam_c, float* lam_p);
 // pressure-jacobi (src -> dst): lam_src += J^T lam_dst, lam_div += -lam_dst / 6.
-void adj_jacobi(cudaStream_t s, Dims dm, const float* lam_dst, float* lam_src, float* lam_div);
+// accumulate false: lam_src is taken as zero and written whole (lam_src = J^T lam_dst).
+void adj_jacobi(cudaStream_t s, Dims dm, const float* lam_dst, float* lam_src, float* lam_div, bool accumulate);
 // pressure-restriction (fine.div -> coarse.div): lam_fine += scatter (atomics).
 void adj_restrict(cudaStream_t s, Dims fine, Dims coarse, const float* lam_coarse, float* lam_fine);
 // pressure-prolongation (coarse p -> fine pressureA +=): lam_cp += scatter

@@ -1854,6 +1854,9 @@ struct fx_rollout {
   // The taped re-runs of the backward use the fused step too (fused_steps), with
   // the tape recorded inside it; plain_tape (a test entry) keeps them plain.
   bool plain_tape = false;
+  // reverse_pressure captured as a graph, for the schedule counts rp_key (qi[2..6])
+  cudaGraphExec_t rp_exec = nullptr;
+  int rp_key[5]{};
 };
 
 namespace {
@@ -1948,13 +1951,18 @@ float speed_limit_of(const fx_sim* s) {
 }
 
 // PressureSolvePass.smooth (:129-143) in reverse.
+// Each sweep's adjoint moves lam from the buffer the sweep wrote to the one it
+// read, and that written buffer's adjoint is then spent. The first sweep
+// undone adds to what its read buffer holds; every later one writes its read
+// buffer whole, since that buffer's adjoint was spent by the sweep undone just
+// before. The buffer left over at the end is cleared.
 void reverse_smooth(fx_rollout* r, int l, int iters, int start) {
   fx_sim* s = r->s;
   const Dims dm = s->lv[l].dm;
   for (int k = iters - 1; k >= 0; --k) {
     const int a = start ^ (k & 1);
-    adj_jacobi(s->stream, dm, r->lam_p[l][a ^ 1], r->lam_p[l][a], r->lam_div[l]);
-    cudaMemsetAsync(r->lam_p[l][a ^ 1], 0, count_of(dm) * sizeof(float), s->stream);
+    adj_jacobi(s->stream, dm, r->lam_p[l][a ^ 1], r->lam_p[l][a], r->lam_div[l], k == iters - 1);
+    if (k == 0) cudaMemsetAsync(r->lam_p[l][a ^ 1], 0, count_of(dm) * sizeof(float), s->stream);
   }
 }
 
@@ -1974,6 +1982,33 @@ void reverse_pressure(fx_rollout* r) {
   reverse_smooth(r, 1, q[4], 0);
   adj_restrict(s->stream, s->lv[0].dm, s->lv[1].dm, r->lam_div[1], r->lam_div[0]);
   reverse_smooth(r, 0, q[2], 0);
+}
+
+// reverse_pressure as one CUDA graph: its launches (45 small kernels and clears
+// at the three levels for the 4/4/4/4/20 schedule) and their buffers are the
+// same every step, so
+// the graph is captured on first use and again only when the solve's schedule
+// changes.
+fx_status launch_reverse_pressure(fx_rollout* r) {
+  fx_sim* s = r->s;
+  const int* q = s->qi;
+  if (!r->rp_exec || !std::equal(q + 2, q + 7, r->rp_key)) {
+    if (r->rp_exec) {
+      cudaGraphExecDestroy(r->rp_exec);
+      r->rp_exec = nullptr;
+    }
+    FX_CUDA(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    reverse_pressure(r);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&r->rp_exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) r->rp_exec = nullptr;
+    FX_CUDA(s, e);
+    std::copy(q + 2, q + 7, r->rp_key);
+  }
+  FX_CUDA(s, cudaGraphLaunch(r->rp_exec, s->stream));
+  return FX_OK;
 }
 
 // The adjoint of one step that was just re-run with the tape hooks from the
@@ -2001,7 +2036,8 @@ fx_status reverse_step(fx_rollout* r, int cur, const float* state0, int o) {
     FX_CUDA(s, cudaMemsetAsync(r->lam_div[l], 0, c, st));
   }
   adj_project(st, dm, lvo, r->lam_c, r->lam_p[0][s->last_p]);
-  reverse_pressure(r);
+  fx_status ps = launch_reverse_pressure(r);
+  if (ps != FX_OK) return ps;
   adj_divergence(st, dm, r->lam_div[0], r->lam_c);
   adj_confinement(st, dm, P, s->vort, s->vort_mag, s->sets[next], r->b, r->lam_c, r->lam_w, r->lam_wmag, r->lam_g, lo);
   adj_vorticity(st, dm, s->vort, s->vort_mag, r->lam_w, r->lam_wmag, r->lam_g, r->lam_c);
@@ -2124,6 +2160,7 @@ fx_status fx_rollout_create(fx_sim* s, const fx_rollout_desc* d, fx_rollout** ou
 void fx_rollout_destroy(fx_rollout* r) {
   if (!r) return;
   cudaSetDevice(r->device);
+  if (r->rp_exec) cudaGraphExecDestroy(r->rp_exec);
   if (r->arena) cudaFree(r->arena);
   delete r;
 }
