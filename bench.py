@@ -494,8 +494,8 @@ def run_adjoint_c4(args, local, pg):
     n = int(np.prod(aw.target.shape))
     out = {
         "workload": f"adjoint_{args.adjoint_size}: {args.adjoint_size}^3 four-plume start (about 30 % of bricks active), "
-                    f"16 x 16 inflow patch at y = 1 (2 + N(0, 0.1^2)), {aw.steps} f32 steps at dt 1/60 (fused forward, "
-                    f"recomputation and taped re-runs), "
+                    f"16 x 16 inflow patch at y = 1 (2 + N(0, 0.1^2)), {aw.steps} f32 steps at dt 1/60 (fused forward, and "
+                    f"a fused taped recomputation of each segment that records every step's tape), "
                     f"loss |density - target|^2 (3 seeded Gaussians), checkpoint every {aw.checkpoint_interval}",
         "loss": loss, "forward_ms": f_ms, "backward_ms": b_ms, "backward_over_forward": b_ms / f_ms,
         "voxel_steps_per_s_forward": n * aw.steps / (f_ms / 1e3),

@@ -309,6 +309,7 @@ TEST_PROTOTYPES = [
     ("fx_test_fail_allocations", c_int32, [c_int32]),
     ("fx_test_sparse_tma_wait", c_int32, [c_void_p, c_uint64, c_uint32]),
     ("fx_test_rollout_plain_tape", c_int32, [c_void_p, c_int32]),
+    ("fx_test_rollout_rerun_tape", c_int32, [c_void_p, c_int32, POINTER(c_int32)]),
     ("fx_test_sr_half", c_int32, [POINTER(c_float), POINTER(c_float), c_uint32, c_uint32, c_uint32]),
     ("fx_test_pinned_exp_pow", c_int32, [POINTER(c_float), POINTER(c_float), POINTER(c_float), POINTER(c_float), c_uint32]),
 ]

@@ -1816,6 +1816,24 @@ struct HostState {
 
 }  // namespace
 
+// What the adjoint of one step reads of that step's forward: its tape (the
+// fields the plain step's hooks record) and the fields the step leaves in the
+// simulation (the input set after the injections, the output set, the set
+// before combustion, the curl and its length, both brick flag arrays, the step
+// uniform and the final pressure buffer's index).
+struct StepTape {
+  float* t1 = nullptr;
+  float* r1 = nullptr;
+  VelField v1{}, a{}, b{};
+  ScalarSet in{}, out{}, snap{};
+  VelField w{};
+  float* wmag = nullptr;
+  uint32_t* flags_in = nullptr;
+  uint32_t* flags_out = nullptr;
+  Params* P = nullptr;
+  int last_p = 0;
+};
+
 struct fx_rollout {
   fx_sim* s = nullptr;
   int device = 0;
@@ -1857,6 +1875,12 @@ struct fx_rollout {
   // reverse_pressure captured as a graph, for the schedule counts rp_key (qi[2..6])
   cudaGraphExec_t rp_exec = nullptr;
   int rp_key[5]{};
+  // One StepTape per step of a segment, recorded while the segment is
+  // recomputed; empty when they did not fit, and then each step is re-run taped
+  // just before its adjoint. rerun_tape (a test entry) forces the re-runs.
+  void* slot_arena = nullptr;
+  std::vector<StepTape> slots;
+  bool rerun_tape = false;
 };
 
 namespace {
@@ -2011,17 +2035,93 @@ fx_status launch_reverse_pressure(fx_rollout* r) {
   return FX_OK;
 }
 
-// The adjoint of one step that was just re-run with the tape hooks from the
-// state `state0` (whose current set index was `cur`): lam_s[o], lam_v[o] hold
-// the adjoint of the step's output state; lam_s[o ^ 1], lam_v[o ^ 1] receive
-// the adjoint of its input state.
-fx_status reverse_step(fx_rollout* r, int cur, const float* state0, int o) {
+// The tape of the step just run from a state whose current set index was
+// `cur`, in place in the simulation and the rollout's single tape.
+StepTape sim_tape(fx_rollout* r, int cur) {
+  fx_sim* s = r->s;
+  StepTape t;
+  t.t1 = r->t1;
+  t.r1 = r->r1;
+  t.v1 = r->v1;
+  t.a = r->a;
+  t.b = r->b;
+  t.in = s->sets[cur];
+  t.out = s->sets[cur ^ 1];
+  t.snap = s->sets[2];
+  t.w = s->vort;
+  t.wmag = s->vort_mag;
+  t.flags_in = s->flags[cur];
+  t.flags_out = s->flags[cur ^ 1];
+  t.P = s->d_params;
+  t.last_p = s->last_p;
+  return t;
+}
+
+// Copies into the slot `t` (whose t1, r1, v1, a, b the step already wrote) the
+// fields of the step just run from a state whose current set index was `cur`.
+fx_status record_tape(fx_rollout* r, int cur, StepTape& t) {
+  fx_sim* s = r->s;
+  const StepTape src = sim_tape(r, cur);
+  cudaStream_t st = s->stream;
+  const size_t b = r->n * sizeof(float), fb = (size_t)s->nb * sizeof(uint32_t);
+  for (int k = 0; k < 4; ++k) {
+    FX_CUDA(s, cudaMemcpyAsync(t.in.f[k], src.in.f[k], b, cudaMemcpyDeviceToDevice, st));
+    FX_CUDA(s, cudaMemcpyAsync(t.out.f[k], src.out.f[k], b, cudaMemcpyDeviceToDevice, st));
+    FX_CUDA(s, cudaMemcpyAsync(t.snap.f[k], src.snap.f[k], b, cudaMemcpyDeviceToDevice, st));
+  }
+  for (int c = 0; c < 3; ++c) FX_CUDA(s, cudaMemcpyAsync(t.w.c[c], src.w.c[c], b, cudaMemcpyDeviceToDevice, st));
+  FX_CUDA(s, cudaMemcpyAsync(t.wmag, src.wmag, b, cudaMemcpyDeviceToDevice, st));
+  FX_CUDA(s, cudaMemcpyAsync(t.flags_in, src.flags_in, fb, cudaMemcpyDeviceToDevice, st));
+  FX_CUDA(s, cudaMemcpyAsync(t.flags_out, src.flags_out, fb, cudaMemcpyDeviceToDevice, st));
+  FX_CUDA(s, cudaMemcpyAsync(t.P, src.P, sizeof(Params), cudaMemcpyDeviceToDevice, st));
+  t.last_p = src.last_p;
+  return FX_OK;
+}
+
+// Device bytes of one StepTape slot: 27 fields of n floats, two brick flag
+// arrays and the step uniform, each start 256-byte aligned.
+size_t slot_bytes(size_t n, size_t nb) {
+  auto al = [](size_t v) { return (v + 255) / 256 * 256; };
+  return 27 * al(n * sizeof(float)) + 2 * al(nb * sizeof(uint32_t)) + al(sizeof(Params));
+}
+
+// Carves `count` slots out of the arena at `base`.
+void carve_slots(fx_rollout* r, char* base, uint32_t count) {
+  const size_t nb = r->s->nb;
+  auto al = [](size_t v) { return (v + 255) / 256 * 256; };
+  char* p = base;
+  auto fl = [&]() {
+    float* q = reinterpret_cast<float*>(p);
+    p += al(r->n * sizeof(float));
+    return q;
+  };
+  r->slots.assign(count, StepTape{});
+  for (StepTape& t : r->slots) {
+    t.t1 = fl();
+    t.r1 = fl();
+    for (VelField* v : {&t.v1, &t.a, &t.b, &t.w})
+      for (int c = 0; c < 3; ++c) v->c[c] = fl();
+    for (ScalarSet* q : {&t.in, &t.out, &t.snap})
+      for (int k = 0; k < 4; ++k) q->f[k] = fl();
+    t.wmag = fl();
+    t.flags_in = reinterpret_cast<uint32_t*>(p);
+    p += al(nb * sizeof(uint32_t));
+    t.flags_out = reinterpret_cast<uint32_t*>(p);
+    p += al(nb * sizeof(uint32_t));
+    t.P = reinterpret_cast<Params*>(p);
+    p += al(sizeof(Params));
+  }
+}
+
+// The adjoint of one step from the state `state0`, whose forward fields are in
+// `t`: lam_s[o], lam_v[o] hold the adjoint of the step's output state;
+// lam_s[o ^ 1], lam_v[o ^ 1] receive the adjoint of its input state.
+fx_status reverse_step(fx_rollout* r, const StepTape& t, const float* state0, int o) {
   fx_sim* s = r->s;
   cudaStream_t st = s->stream;
   const Dims dm = s->dm;
-  const int next = cur ^ 1;
   const size_t n = r->n;
-  const Params* P = s->d_params;
+  const Params* P = t.P;
   const uint32_t nsrc = std::max<uint32_t>(s->src_count, 1);
   ScalarSet S0;
   for (int k = 0; k < 4; ++k) S0.f[k] = const_cast<float*>(state0) + k * n;
@@ -2035,19 +2135,19 @@ fx_status reverse_step(fx_rollout* r, int cur, const float* state0, int o) {
     FX_CUDA(s, cudaMemsetAsync(r->lam_p[l][1], 0, c, st));
     FX_CUDA(s, cudaMemsetAsync(r->lam_div[l], 0, c, st));
   }
-  adj_project(st, dm, lvo, r->lam_c, r->lam_p[0][s->last_p]);
+  adj_project(st, dm, lvo, r->lam_c, r->lam_p[0][t.last_p]);
   fx_status ps = launch_reverse_pressure(r);
   if (ps != FX_OK) return ps;
   adj_divergence(st, dm, r->lam_div[0], r->lam_c);
-  adj_confinement(st, dm, P, s->vort, s->vort_mag, s->sets[next], r->b, r->lam_c, r->lam_w, r->lam_wmag, r->lam_g, lo);
-  adj_vorticity(st, dm, s->vort, s->vort_mag, r->lam_w, r->lam_wmag, r->lam_g, r->lam_c);
-  adj_buoyancy(st, dm, s->bricks, P, s->sets[next], s->flags[next], r->a, r->lam_c, lo, r->hot, r->dens);
-  adj_combustion(st, dm, s->bricks, P, s->sets[2], s->flags[next], lo, r->hot);
+  adj_confinement(st, dm, P, t.w, t.wmag, t.out, t.b, r->lam_c, r->lam_w, r->lam_wmag, r->lam_g, lo);
+  adj_vorticity(st, dm, t.w, t.wmag, r->lam_w, r->lam_wmag, r->lam_g, r->lam_c);
+  adj_buoyancy(st, dm, s->bricks, P, t.out, t.flags_out, t.a, r->lam_c, lo, r->hot, r->dens);
+  adj_combustion(st, dm, s->bricks, P, t.snap, t.flags_out, lo, r->hot);
   for (int k = 0; k < 4; ++k) FX_CUDA(s, cudaMemsetAsync(li.f[k], 0, n * sizeof(float), st));
   for (int k = 0; k < 3; ++k) FX_CUDA(s, cudaMemsetAsync(lvi.c[k], 0, n * sizeof(float), st));
-  adj_advect_scalars(st, dm, s->bricks, P, s->sets[cur], r->a, s->flags[cur], lo, li, r->lam_c);
-  adj_advect_velocity(st, dm, P, r->v1, r->lam_c, lvi);
-  adj_inject_igniter(st, dm, P, s->d_sources, nsrc, r->t1, s->sets[cur].f[2], r->r1, li);
+  adj_advect_scalars(st, dm, s->bricks, P, t.in, t.a, t.flags_in, lo, li, r->lam_c);
+  adj_advect_velocity(st, dm, P, t.v1, r->lam_c, lvi);
+  adj_inject_igniter(st, dm, P, s->d_sources, nsrc, t.t1, t.in.f[2], t.r1, li);
   adj_inflow(st, dm, r->patch, lvi, r->grad_inflow);
   adj_inject_velocity(st, dm, P, s->d_sources, nsrc, V0, lvi);
   adj_inject_scalar(st, dm, P, s->d_sources, nsrc, S0, li);
@@ -2151,6 +2251,19 @@ fx_status fx_rollout_create(fx_sim* s, const fx_rollout_desc* d, fx_rollout** ou
     delete r;
     return fail(nullptr, FX_ERR_CUDA, "fx_rollout_create: cudaMemsetAsync failed");
   }
+  // The per-step tapes of a segment, when they take at most half of the free
+  // device memory; without them the backward re-runs each step taped.
+  const uint32_t nslots = std::min(d->checkpoint_interval, d->steps);
+  const size_t sbytes = slot_bytes(n, s->nb) * nslots;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && sbytes <= free_b / 2) {
+    if (device_alloc(&r->slot_arena, sbytes) == cudaSuccess) {
+      carve_slots(r, static_cast<char*>(r->slot_arena), nslots);
+    } else {
+      r->slot_arena = nullptr;
+      cudaGetLastError();  // a refused slot allocation is not an error of the rollout
+    }
+  }
   *out = r;
   return FX_OK;
 }
@@ -2161,6 +2274,7 @@ void fx_rollout_destroy(fx_rollout* r) {
   if (!r) return;
   cudaSetDevice(r->device);
   if (r->rp_exec) cudaGraphExecDestroy(r->rp_exec);
+  if (r->slot_arena) cudaFree(r->slot_arena);
   if (r->arena) cudaFree(r->arena);
   delete r;
 }
@@ -2216,6 +2330,17 @@ fx_status fx_test_rollout_plain_tape(fx_rollout* r, int32_t on) {
   return FX_OK;
 }
 
+// Test entry: 1 makes the backward re-run each step taped just before its
+// adjoint instead of reading the tapes recorded while the segment was
+// recomputed, 0 the default. *has_slots (optional) receives whether the
+// recorded tapes were allocated.
+fx_status fx_test_rollout_rerun_tape(fx_rollout* r, int32_t on, int32_t* has_slots) {
+  if (!r) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_test_rollout_rerun_tape: NULL rollout");
+  r->rerun_tape = on != 0;
+  if (has_slots) *has_slots = r->slots.empty() ? 0 : 1;
+  return FX_OK;
+}
+
 fx_status fx_rollout_backward(fx_rollout* r, float* grad_inflow, float* grad_velocity) {
   if (!r || (!grad_inflow && r->npatch)) return fail(nullptr, FX_ERR_INVALID_ARGUMENT, "fx_rollout_backward: NULL argument");
   fx_sim* s = r->s;
@@ -2243,9 +2368,31 @@ fx_status fx_rollout_backward(fx_rollout* r, float* grad_inflow, float* grad_vel
   tape.a = r->a;
   tape.b = r->b;
   const uint32_t every = r->d.checkpoint_interval;
+  const bool slotted = !r->slots.empty() && !r->rerun_tape;
   for (int seg = (int)r->nck - 1; seg >= 0; --seg) {
     const uint32_t k0 = (uint32_t)seg * every, k1 = std::min(k0 + every, r->d.steps);
     if (restore_state(r, r->ck + (size_t)seg * 7 * n, r->ck_host[seg]) != FX_OK) return FX_ERR_CUDA;
+    if (slotted) {
+      // one taped pass over the segment records every step's tape
+      for (uint32_t k = k0; k < k1; ++k) {
+        if (save_state(r, r->seg + (size_t)(k - k0) * 7 * n, r->seg_host[k - k0]) != FX_OK) return FX_ERR_CUDA;
+        StepTape& t = r->slots[k - k0];
+        PlainHooks hk = run;
+        hk.t1 = t.t1;
+        hk.r1 = t.r1;
+        hk.v1 = t.v1;
+        hk.a = t.a;
+        hk.b = t.b;
+        const int cur = s->cur;
+        if ((st = rollout_step(r, k, hk)) != FX_OK) return st;
+        if ((st = record_tape(r, cur, t)) != FX_OK) return st;
+      }
+      for (int k = (int)k1 - 1; k >= (int)k0; --k) {
+        if ((st = reverse_step(r, r->slots[k - k0], r->seg + (size_t)(k - k0) * 7 * n, o)) != FX_OK) return st;
+        o ^= 1;
+      }
+      continue;
+    }
     for (uint32_t k = k0; k < k1; ++k) {
       if (save_state(r, r->seg + (size_t)(k - k0) * 7 * n, r->seg_host[k - k0]) != FX_OK) return FX_ERR_CUDA;
       if (k + 1 < k1 && (st = rollout_step(r, k, run)) != FX_OK) return st;
@@ -2255,7 +2402,7 @@ fx_status fx_rollout_backward(fx_rollout* r, float* grad_inflow, float* grad_vel
       if (restore_state(r, state0, r->seg_host[k - k0]) != FX_OK) return FX_ERR_CUDA;
       const int cur = s->cur;
       if ((st = rollout_step(r, (uint32_t)k, tape)) != FX_OK) return st;
-      if ((st = reverse_step(r, cur, state0, o)) != FX_OK) return st;
+      if ((st = reverse_step(r, sim_tape(r, cur), state0, o)) != FX_OK) return st;
       o ^= 1;
     }
   }

@@ -577,6 +577,10 @@ fx_status fx_bloom_render(fx_bloom* pass, const void* hdr, int32_t hdr_format, u
  * gradient of the loss with respect to the inflow values and the initial
  * velocity field by the adjoint of every pass, recomputing each segment from its
  * checkpoint, and leaves the simulation in the forward's final state again.
+ * The recomputation records each step's tape (27 fields of width * height *
+ * depth floats per step of a segment, allocated by fx_rollout_create when they
+ * take at most half of the device's free memory); without that allocation each
+ * step is re-run taped just before its adjoint, with the same result.
  * Brick flags, emitter sources and the step uniform are constants of the
  * differentiation; a branch (min, max, clamp, the MacCormack limiter) passes the
  * adjoint of the operand it selected. */

@@ -4,6 +4,7 @@ exact derivative of the f32 trajectory, and of the f64 one) and against central
 finite differences of the f64 oracle, on the 32^3 copy of the differentiation
 workload (64 steps, a checkpoint every 8) and, through the committed fixture,
 at its full 128^3 size."""
+import ctypes
 import json
 import os
 
@@ -154,6 +155,26 @@ def test_fused_tape_matches_the_plain_tape():
     np.testing.assert_allclose(fgv.reshape(3, -1), pgv.reshape(3, -1), rtol=1e-4, atol=1e-6 * float(np.abs(pgv).max()))
     fro.dispose()
     fsim.dispose()
+
+
+@pytest.mark.parametrize("fused", [False, True])
+def test_recorded_tapes_match_the_taped_re_runs(fused):
+    """The backward records every step's tape (and the fields the step leaves that
+    the adjoint reads) while it recomputes a segment, and runs the segment's
+    adjoints from those. Forcing a taped re-run of each step just before its
+    adjoint gives the same gradient up to the order of the float atomics."""
+    sim, ro, loss, final, gi, gv = run_rollout(AW, every=5, fused=fused)
+    has = ctypes.c_int32(-1)
+    assert ro._lib.fx_test_rollout_rerun_tape(ro._h, 1, ctypes.byref(has)) == 0
+    assert has.value == 1  # the recorded tapes fit: the first backward used them
+    start_from(sim, AW.workload.state)
+    rloss = ro.forward(AW.inflow)
+    rgi, rgv = ro.backward()
+    assert abs(rloss - loss) <= 1e-12 * loss
+    np.testing.assert_allclose(gi, rgi, rtol=1e-5, atol=1e-7 * float(np.abs(rgi).max()))
+    np.testing.assert_allclose(gv.reshape(3, -1), rgv.reshape(3, -1), rtol=1e-4, atol=1e-6 * float(np.abs(rgv).max()))
+    ro.dispose()
+    sim.dispose()
 
 
 def test_fused_simulation_gives_the_same_rollout(rolled):
