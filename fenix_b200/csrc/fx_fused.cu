@@ -1471,6 +1471,8 @@ fx_status fused_prepare(FusedWork& w, const FusedStep& st, uint32_t* ninj_out, F
   return FX_OK;
 }
 
+constexpr size_t kMaxTapedGraphs = 64;
+
 uint64_t fused_key(const FusedStep& st, uint32_t ninj) {
   uint64_t key = 0;
   auto mix_key = [&](uint64_t v) { key = (key ^ v) * 0x100000001b3ull; };
@@ -1548,7 +1550,23 @@ fx_status fused_step(FusedWork& w, const FusedStep& st, FusedResult& out) {
         w.graph_note = std::string("instantiate failed: ") + cudaGetErrorString(ie);
         return fused_sequence(w, st, ninj, out);
       }
-      it = w.graphs.emplace(key, FusedWork::GraphEntry{ex, tmp}).first;
+      const bool taped = st.tape_t1 != nullptr;
+      if (taped) {
+        // Every rollout records its tapes at its own addresses: keep the taped
+        // graphs of a few rollouts, not of every rollout ever made.
+        size_t count = 0;
+        for (const auto& kv : w.graphs) count += kv.second.taped;
+        if (count >= kMaxTapedGraphs)
+          for (auto g = w.graphs.begin(); g != w.graphs.end();) {
+            if (g->second.taped) {
+              cudaGraphExecDestroy(g->second.exec);
+              g = w.graphs.erase(g);
+            } else {
+              ++g;
+            }
+          }
+      }
+      it = w.graphs.emplace(key, FusedWork::GraphEntry{ex, tmp, taped}).first;
     }
     FX_CK(cudaGraphLaunch(it->second.exec, s));
     out = it->second.result;
@@ -2136,7 +2154,8 @@ fx_status fused_check_device_error(FusedWork& w, cudaStream_t s) {
 void fused_set_tma_test(FusedWork& w, uint64_t wait_ns, uint32_t extra_tx) {
   w.tma_wait_ns = wait_ns;
   w.tma_extra_tx = extra_tx;
-  w.graphs.clear();  // the values are captured in the graphs
+  for (auto& kv : w.graphs) cudaGraphExecDestroy(kv.second.exec);  // the values are captured in the graphs
+  w.graphs.clear();
 }
 
 fx_status fused_count_active(FusedWork& w, cudaStream_t s, const uint32_t* flags, uint32_t nb, uint32_t* out) {

@@ -85,6 +85,7 @@ struct FusedWork {
   struct GraphEntry {
     cudaGraphExec_t exec;
     FusedResult result;
+    bool taped;  // writes a rollout's tape (its key holds the tape's pointers)
   };
   bool use_graphs = true;
   std::string graph_note;

@@ -177,6 +177,27 @@ def test_recorded_tapes_match_the_taped_re_runs(fused):
     sim.dispose()
 
 
+def test_many_rollouts_on_one_simulation():
+    """Each rollout on the fused kernels captures the fused step once per tape
+    slot; past a bound the simulation drops those graphs and captures again.
+    Ten rollouts of 16 steps (8 slots each) cross the bound, and the last one's
+    gradient equals the first one's up to the order of the float atomics."""
+    sim = createCombustionVolumeSimulation(AW.workload.options, device=0, kernels="fused")
+    sim.updateSources(AW.workload.sources)
+    grads = []
+    for _ in range(10):
+        ro = Rollout(sim, steps=16, checkpoint_interval=8, patch=AW.patch)
+        ro.setTarget(AW.target)
+        start_from(sim, AW.workload.state)
+        ro.forward(AW.inflow)
+        grads.append(ro.backward())
+        ro.dispose()
+    (gi0, gv0), (gi9, gv9) = grads[0], grads[-1]
+    np.testing.assert_allclose(gi9, gi0, rtol=1e-5, atol=1e-7 * float(np.abs(gi0).max()))
+    np.testing.assert_allclose(gv9.reshape(3, -1), gv0.reshape(3, -1), rtol=1e-4, atol=1e-6 * float(np.abs(gv0).max()))
+    sim.dispose()
+
+
 def test_fused_simulation_gives_the_same_rollout(rolled):
     """The fused kernels run the forward and the recomputed steps: the final
     state is the plain rollout's bits, the loss equals it up to the order of the
