@@ -1,7 +1,7 @@
 """FP16 storage of the scalar sets: rounding, and error against the f64 oracle.
 
-The north star states the bar for this mode: density relative L2 <= 1e-3
-against f64 after 200 steps of the 256^3 plume. Here a 64^3 plume runs 60 steps
+The accuracy bar for this mode: density relative L2 <= 1e-3 against f64
+after 200 steps of the 256^3 plume. Here a 64^3 plume runs 60 steps
 on the CPU, and the bar is asserted beside the f32 path's own error.
 """
 import numpy as np
