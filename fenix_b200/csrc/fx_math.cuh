@@ -169,8 +169,8 @@ FX_DEV bool is_boundary(const Dims& dm, uint32_t x, uint32_t y, uint32_t z) {
 }
 
 // The 80-byte uniform of shaders/common/simulation-params.wgsl.ts:2-14, then two
-// words of this build: the step index and the rounding of binary16 scalar stores
-// (0 to nearest, 1 stochastic; see sr_half).
+// words the reference does not have: the step index and the rounding of binary16
+// scalar stores (0 to nearest, 1 stochastic; see sr_half).
 struct Params {
   float time, dt, prev_time, scalar_set;
   float wind[4];
