@@ -4,6 +4,7 @@
 // quality handling, and the multilevel pressure schedule
 // (runtime/passes/PressureSolvePass.ts:62-158).
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <map>
@@ -1881,6 +1882,9 @@ struct fx_rollout {
   void* slot_arena = nullptr;
   std::vector<StepTape> slots;
   bool rerun_tape = false;
+  // reverse_step of each (slot, o) as a graph, and the inputs it was captured for
+  std::vector<cudaGraphExec_t> rs_exec;
+  std::vector<std::array<uint64_t, 8>> rs_key;
 };
 
 namespace {
@@ -2116,7 +2120,7 @@ void carve_slots(fx_rollout* r, char* base, uint32_t count) {
 // The adjoint of one step from the state `state0`, whose forward fields are in
 // `t`: lam_s[o], lam_v[o] hold the adjoint of the step's output state;
 // lam_s[o ^ 1], lam_v[o ^ 1] receive the adjoint of its input state.
-fx_status reverse_step(fx_rollout* r, const StepTape& t, const float* state0, int o) {
+fx_status reverse_step(fx_rollout* r, const StepTape& t, const float* state0, int o, bool in_graph = false) {
   fx_sim* s = r->s;
   cudaStream_t st = s->stream;
   const Dims dm = s->dm;
@@ -2136,8 +2140,12 @@ fx_status reverse_step(fx_rollout* r, const StepTape& t, const float* state0, in
     FX_CUDA(s, cudaMemsetAsync(r->lam_div[l], 0, c, st));
   }
   adj_project(st, dm, lvo, r->lam_c, r->lam_p[0][t.last_p]);
-  fx_status ps = launch_reverse_pressure(r);
-  if (ps != FX_OK) return ps;
+  if (in_graph) {
+    reverse_pressure(r);
+  } else {
+    fx_status ps = launch_reverse_pressure(r);
+    if (ps != FX_OK) return ps;
+  }
   adj_divergence(st, dm, r->lam_div[0], r->lam_c);
   adj_confinement(st, dm, P, t.w, t.wmag, t.out, t.b, r->lam_c, r->lam_w, r->lam_wmag, r->lam_g, lo);
   adj_vorticity(st, dm, t.w, t.wmag, r->lam_w, r->lam_wmag, r->lam_g, r->lam_c);
@@ -2152,6 +2160,48 @@ fx_status reverse_step(fx_rollout* r, const StepTape& t, const float* state0, in
   adj_inject_velocity(st, dm, P, s->d_sources, nsrc, V0, lvi);
   adj_inject_scalar(st, dm, P, s->d_sources, nsrc, S0, li);
   FX_CUDA(s, cudaGetLastError());
+  return FX_OK;
+}
+
+// The inputs of a captured reverse step that can change between backward calls.
+std::array<uint64_t, 8> reverse_key(fx_rollout* r, const StepTape& t) {
+  const fx_sim* s = r->s;
+  return {(uint64_t)(uintptr_t)s->d_sources, s->src_count, (uint64_t)s->qi[2], (uint64_t)s->qi[3], (uint64_t)s->qi[4],
+          (uint64_t)s->qi[5], (uint64_t)s->qi[6], (uint64_t)t.last_p};
+}
+
+// reverse_step of slot j as one CUDA graph per (slot, o): within a segment the
+// adjoint steps run back to back from the slots, with the same buffers every
+// backward call, so each is captured on first use and replayed.
+fx_status reverse_step_slot(fx_rollout* r, uint32_t j, int o) {
+  fx_sim* s = r->s;
+  const StepTape& t = r->slots[j];
+  const float* state0 = r->seg + (size_t)j * 7 * r->n;
+  const std::array<uint64_t, 8> key = reverse_key(r, t);
+  const size_t idx = (size_t)j * 2 + (size_t)o;
+  if (r->rs_exec.size() != r->slots.size() * 2) r->rs_exec.assign(r->slots.size() * 2, nullptr);
+  if (r->rs_key.size() != r->rs_exec.size()) r->rs_key.assign(r->rs_exec.size(), {});
+  cudaGraphExec_t& ex = r->rs_exec[idx];
+  if (ex && r->rs_key[idx] != key) {
+    cudaGraphExecDestroy(ex);
+    ex = nullptr;
+  }
+  if (!ex) {
+    FX_CUDA(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    const fx_status st = reverse_step(r, t, state0, o, true);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (st != FX_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ex, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) ex = nullptr;
+    FX_CUDA(s, e);
+    r->rs_key[idx] = key;
+  }
+  FX_CUDA(s, cudaGraphLaunch(ex, s->stream));
   return FX_OK;
 }
 
@@ -2274,6 +2324,8 @@ void fx_rollout_destroy(fx_rollout* r) {
   if (!r) return;
   cudaSetDevice(r->device);
   if (r->rp_exec) cudaGraphExecDestroy(r->rp_exec);
+  for (cudaGraphExec_t ex : r->rs_exec)
+    if (ex) cudaGraphExecDestroy(ex);
   if (r->slot_arena) cudaFree(r->slot_arena);
   if (r->arena) cudaFree(r->arena);
   delete r;
@@ -2388,7 +2440,7 @@ fx_status fx_rollout_backward(fx_rollout* r, float* grad_inflow, float* grad_vel
         if ((st = record_tape(r, cur, t)) != FX_OK) return st;
       }
       for (int k = (int)k1 - 1; k >= (int)k0; --k) {
-        if ((st = reverse_step(r, r->slots[k - k0], r->seg + (size_t)(k - k0) * 7 * n, o)) != FX_OK) return st;
+        if ((st = reverse_step_slot(r, k - k0, o)) != FX_OK) return st;
         o ^= 1;
       }
       continue;
