@@ -451,7 +451,7 @@ def run_adjoint_c4(args, local, pg):
     """The differentiation configuration: 64 plain FP32 steps at 128^3 with a
     16 x 16 inflow patch as the control, loss = |density_64 - target|^2, a
     checkpoint every 8 steps. Times the forward (with checkpoints) and the
-    backward (segment recomputation, tape re-runs and the adjoint kernels) with
+    backward (the taped recomputation of each segment and the adjoint kernels) with
     CUDA events on the simulation's stream, host copies of the control, loss and
     gradients included; checks the gradient against the committed oracle
     references of this workload (f32-trajectory tangents, f64 central
