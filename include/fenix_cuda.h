@@ -570,8 +570,9 @@ fx_status fx_bloom_render(fx_bloom* pass, const void* hdr, int32_t hdr_format, u
  * at elapsed = start_elapsed + k * step_seconds with step = step_seconds.
  *
  * The adjoint differentiates the plain step; with FX_KERNELS_FUSED the forward
- * and the recomputed steps run the fused kernels, which give the same bits
- * (unless an inflow value exceeds the speed limit, when every step is plain).
+ * and the recomputed (taped) steps run the fused kernels, which give the same
+ * bits (unless an inflow value exceeds the speed limit, when every step is
+ * plain).
  * fx_rollout_forward leaves the simulation in its final state and keeps a state
  * checkpoint every checkpoint_interval steps; fx_rollout_backward returns the
  * gradient of the loss with respect to the inflow values and the initial
